@@ -1,0 +1,213 @@
+/* vulcan_b200.h -- C ABI of libvulcan_b200.so, the sm_100a DDA search hot path.
+ *
+ * Conventions
+ *   - Every pointer argument is a DEVICE pointer unless its comment says "host".
+ *   - `stream` is a cudaStream_t passed as void*; launches are asynchronous on it.
+ *   - Every function returns 0 on success, a cudaError_t code (> 0) if a launch failed, or a negative VK_E_* code
+ *     for a rejected argument.  Nothing allocates device memory unless its comment says so: the caller sizes every
+ *     buffer (the *_count / *_plan calls report the sizes).
+ *   - No hidden global state except the process-wide constants of the reference-compatible entry points
+ *     (vk_set_params / vk_set_nterm / vk_set_tol_da, per device, as in the reference).  The B200 entry points take
+ *     their fragment constants by value (vk_frag_params), so threads with their own streams can call them
+ *     concurrently.
+ *
+ * Part 1 keeps the reference's exported names and argument lists (vulcan/gpu/_lib.py:22-35 binds them with
+ * ctypes), so the reference's own engine can load this library unchanged.  Part 2 is the B200 layout: a tiled
+ * fragment index (row tiles, postings sorted by exact f32 fragment m/z, per-tile CSR over integer coarse m/z bins)
+ * and the device stages of the search.
+ */
+#ifndef VULCAN_B200_H
+#define VULCAN_B200_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VK_E_ARG (-1)       /* invalid argument (size, alignment, layout limit) */
+#define VK_E_CAPACITY (-2)  /* an output buffer is too small; the needed size was written where documented */
+
+/* ============================================================ Part 1: reference-compatible entry points */
+
+/* Replaces vulcan/gpu/kernels.cu:381-385: Sage f32 residue masses (26, by letter), static and variable
+ * modification deltas (26 each); host pointers; copied to this device's constant memory. */
+int vk_set_params(const float* mono, const float* stat, const float* var);
+/* Replaces kernels.cu:387: variable peptide-N-term delta (mask bit 63). */
+int vk_set_nterm(float nterm);
+/* Replaces kernels.cu:389: fragment tolerance unit, 0 = ppm, 1 = Da. */
+int vk_set_tol_da(int da);
+
+/* Replaces kernels.cu:391-399 (frag_count_kernel): index fragments per row (ion index > min_ion_index and
+ * fmin <= neutral fragment mass <= fmax). */
+int vk_frag_count(int64_t n, const int64_t* seq_off, const uint8_t* len, const uint64_t* mask, const float* mass32,
+                  const uint8_t* res, int min_ion_index, float fmin, float fmax, int32_t* count, void* stream);
+/* Replaces kernels.cu:401-411 (frag_emit_kernel): int64 keys chunk<<50 | logbin<<32 | local<<16 | fine. */
+int vk_frag_emit(int64_t n, const int64_t* seq_off, const uint8_t* len, const uint64_t* mask, const float* mass32,
+                 const uint8_t* res, int min_ion_index, float fmin, float fmax, double inv_logw, int chunk_size,
+                 int64_t row0, const int64_t* out_off, int64_t* keys, void* stream);
+/* Replaces kernels.cu:413-431 (k1_kernel): K1 counts over the reference's (chunk, log bin) CSR; appends
+ * (hyp, row, count) for count >= thr at atomicAdd(n_out) (entries beyond cap are dropped, n_out still counts them);
+ * hyp_scored / hyp_matched accumulate. */
+int vk_k1(int n_items, const int32_t* it_hyp, const int32_t* it_chunk, const int32_t* it_lo, const int32_t* it_hi,
+          const int32_t* hyp_spec, const int8_t* hyp_maxfz, const int64_t* pk_off, const float* pk_mass,
+          const uint32_t* offsets, const uint32_t* entries, int n_bins, int chunk0, int chunk_size, int tile,
+          float tol_lo, float tol_hi, float fmin, double inv_logw, int thr, int64_t cap,
+          unsigned long long* n_out, int32_t* out_hyp, int32_t* out_row, int32_t* out_cnt,
+          unsigned int* hyp_scored, unsigned long long* hyp_matched, void* stream);
+/* Replaces kernels.cu:433-445 (k1_brute_kernel): brute-force K1 count of each (hyp, row) pair. */
+int vk_k1_brute(int64_t n, const int32_t* c_hyp, const int32_t* c_row, const int32_t* hyp_spec,
+                const int8_t* hyp_maxfz, const int64_t* pk_off, const float* pk_mass, const int64_t* seq_off,
+                const uint8_t* len, const uint64_t* mask, const float* mass32, const uint8_t* res,
+                int min_ion_index, float fmin, float fmax, float tol_lo, float tol_hi, double inv_logw,
+                int32_t* out_cnt, void* stream);
+/* Replaces kernels.cu:447-458 (k2_kernel, closed mode): exact b/y rescoring of candidates grouped by spectrum
+ * (cand_off[n_spec+1]); spectrum bs uses peaks of spec_ids[bs] (first 512 mass-sorted peaks).  `threads` is
+ * accepted for signature compatibility; the launch shape is chosen here. */
+int vk_k2(int n_spec, const int64_t* cand_off, const int32_t* c_row, const int8_t* c_maxfz, const int32_t* spec_ids,
+          const int64_t* pk_off, const float* pk_mass, const float* pk_int, const int64_t* seq_off,
+          const uint8_t* len, const uint64_t* mask, const float* mass32, const uint8_t* res, float tol_lo,
+          float tol_hi, double* o_hs, float* o_sb, float* o_sy, float* o_ppm, int16_t* o_mb, int16_t* o_my,
+          int16_t* o_lb, int16_t* o_ly, int threads, void* stream);
+/* Replaces kernels.cu:461-472: K2 with a per-candidate precursor delta (shifted + unshifted ions, best site). */
+int vk_k2_shift(int n_spec, const int64_t* cand_off, const int32_t* c_row, const int8_t* c_maxfz,
+                const int32_t* spec_ids, const int64_t* pk_off, const float* pk_mass, const float* pk_int,
+                const int64_t* seq_off, const uint8_t* len, const uint64_t* mask, const float* mass32,
+                const uint8_t* res, float tol_lo, float tol_hi, const float* c_shift, double* o_hs, float* o_sb,
+                float* o_sy, float* o_ppm, int16_t* o_mb, int16_t* o_my, int16_t* o_lb, int16_t* o_ly,
+                int threads, void* stream);
+
+/* ============================================================ Part 2: B200 layout and device stages */
+
+/* Fragment constants by value (what vk_set_params/vk_set_nterm/vk_set_tol_da hold globally in Part 1). */
+typedef struct {
+  float mono[26];
+  float stat[26];
+  float var[26];
+  float nterm;
+  int tol_da;
+} vk_frag_params;
+
+/* Tiled fragment index.  Rows (mass-sorted peptidoforms) are cut into tiles of tile_rows = 2^tile_shift rows.
+ * A posting is one u32: (f32bits(fragment) - f32bits(fmin)) << row_bits | (row - tile*tile_rows), where
+ * row_bits = 32 - mass_bits and mass_bits = bit length of f32bits(fmax) - f32bits(fmin).  A tile's postings are
+ * sorted ascending, i.e. by exact f32 fragment mass, then row.  The coarse m/z bin of a posting is its top
+ * cbin_bits bits (an integer bin in f32-bit space); cbin_off[tile*(n_cbins+1) + b] (u16, relative to the tile's
+ * first posting) is the CSR over those bins.  tile_off[n_tiles+1] (i64) locates each tile's postings. */
+typedef struct {
+  int64_t n_rows;
+  int64_t n_tiles;
+  int64_t n_postings;
+  int32_t tile_shift;       /* log2(tile_rows) */
+  int32_t row_bits;
+  int32_t mass_bits;
+  int32_t cbin_bits;        /* coarse bins per tile = 2^cbin_bits */
+  uint32_t fmin_bits;
+  uint32_t fmax_bits;
+  int32_t min_ion_index;
+  int32_t max_tile_postings;
+  const int64_t* tile_off;
+  const uint16_t* cbin_off;
+  const uint32_t* postings;
+} vk_tindex;
+
+/* Layout of a tiled index for tile_rows/fmin/fmax: fills tile_shift, row_bits, mass_bits, cbin_bits, fmin_bits,
+ * fmax_bits, n_tiles (host struct).  VK_E_ARG if tile_rows is not a power of two or does not fit row_bits. */
+int vk_tindex_layout(int64_t n_rows, int tile_rows, float fmin, float fmax, int min_ion_index, int cbin_bits,
+                     vk_tindex* ix);
+/* Postings per tile: tile_count[n_tiles] (i64) from the peptidoform table. */
+int vk_tindex_count(const vk_tindex* ix, const vk_frag_params* fp, const int64_t* seq_off, const uint8_t* len,
+                    const uint64_t* mask, const float* mass32, const uint8_t* res, int64_t* tile_count,
+                    void* stream);
+/* Fill postings and cbin_off of a tiled index whose tile_off (exclusive scan of tile_count) is in place.
+ * max_tile_postings (host, from tile_count) sizes the per-tile sort; it must be <= 16384. */
+int vk_tindex_emit(const vk_tindex* ix, const vk_frag_params* fp, const int64_t* seq_off, const uint8_t* len,
+                   const uint64_t* mask, const float* mass32, const uint8_t* res, uint32_t* postings,
+                   uint16_t* cbin_off, void* stream);
+
+/* Exclusive scan of n int64 values: out[0] = 0, out[i+1] = sum(in[0..i]) (out has n+1 entries; in == out+1
+ * is allowed).  Uses `tmp` of vk_scan_tmp_bytes(n) bytes. */
+int64_t vk_scan_tmp_bytes(int64_t n);
+int vk_scan_i64(const int64_t* in, int64_t n, int64_t* out, void* tmp, void* stream);
+
+/* K0 peak view (reference vulcan/gpu/engine.py:171-210), two calls: vk_k0_count writes kept[n_spec] (i64) =
+ * min(#peaks with fmin <= mz <= fmax and not NaN, max_peaks); after the caller's scan into pk_off[n_spec+1],
+ * vk_k0_fill writes mass-sorted peaks (mass = mz - PROTON) of the top max_peaks by (intensity desc, mass desc),
+ * tic[n_spec] (f32 of the f64 sum) and valid[n_spec] (u8, kept >= min_peaks).  max_raw (host) = the largest raw
+ * peak count of a spectrum, at most 16384 (one CTA sorts a spectrum in shared memory). */
+int vk_k0_count(int n_spec, const int64_t* raw_off, const float* raw_mz, float fmin, float fmax, int max_peaks,
+                int64_t* kept, void* stream);
+int vk_k0_fill(int n_spec, const int64_t* raw_off, const float* raw_mz, const float* raw_int, float fmin,
+               float fmax, int max_peaks, int min_peaks, const int64_t* pk_off, float* pk_mass, float* pk_int,
+               float* tic, uint8_t* valid, int max_raw, void* stream);
+
+/* Hypotheses (reference vulcan/gpu/host.py:64-91), two calls like K0: vk_hyp_count writes n_hyp[n_spec] (i64);
+ * vk_hyp_fill writes, at hyp_off[s], the spectrum's hypotheses in (charge, isotope) order with f32 Sage
+ * arithmetic and the row window [lo, hi) by binary search of the mass-sorted index masses. */
+int vk_hyp_count(int n_spec, const uint8_t* valid, const double* precursor_mz, const int8_t* charge, int z_lo,
+                 int z_hi, int iso_lo, int iso_hi, int64_t* n_hyp, void* stream);
+int vk_hyp_fill(int n_spec, const uint8_t* valid, const double* precursor_mz, const int8_t* charge, int z_lo,
+                int z_hi, int iso_lo, int iso_hi, float ppm_lo, float ppm_hi, int max_fragment_charge,
+                const float* idx_mass32, int64_t n_rows, const int64_t* hyp_off, int32_t* h_spec, int8_t* h_z,
+                int8_t* h_iso, float* h_pm, float* h_M, int64_t* h_lo, int64_t* h_hi, int8_t* h_maxfz,
+                void* stream);
+
+/* K1 on the tiled index.  Work items are (tile, hypothesis) pairs grouped by tile:
+ *   vk_k1_plan_count: items per tile (tile_items[n_tiles], i64, zeroed by the call) and window sizes
+ *                     (win_len[n_hyp], i64);
+ *   vk_k1_plan_fill:  with tile_item_off (scan of tile_items) in place, writes item_hyp[n_items] (i32) grouped by
+ *                     tile (order inside a tile is unspecified; results do not depend on it);  `cursor` is an
+ *                     n_tiles i64 scratch;
+ *   vk_k1_tiles:      dense counts cnt[win_off[h] + row - lo[h]] (i32) for every window row of every hypothesis.
+ * Counts equal the reference's brute force (kernels.cu:195-232): #(peak p, fragment charge z < maxfz, index
+ * fragment f) with tol_bound(p*z, tol_lo) <= f <= tol_bound(p*z, tol_hi) in f32.  `status` (device i32, zeroed by
+ * the caller) gets VK_STATUS_WAIT_TIMEOUT if a tile copy did not complete within the bounded wait. */
+int vk_k1_plan_count(const vk_tindex* ix, int64_t n_hyp, const int64_t* h_lo, const int64_t* h_hi,
+                     int64_t* tile_items, int64_t* win_len, void* stream);
+int vk_k1_plan_fill(const vk_tindex* ix, int64_t n_hyp, const int64_t* h_lo, const int64_t* h_hi,
+                    const int64_t* tile_item_off, int64_t* cursor, int32_t* item_hyp, void* stream);
+int vk_k1_tiles(const vk_tindex* ix, const vk_frag_params* fp, float tol_lo, float tol_hi,
+                const int64_t* tile_item_off, const int32_t* item_hyp, const int32_t* h_spec,
+                const int8_t* h_maxfz, const int64_t* h_lo, const int64_t* h_hi, const int64_t* win_off,
+                const int64_t* pk_off, const float* pk_mass, int32_t* cnt, int32_t* status, void* stream);
+
+/* Top-K + pair closure (reference vulcan/gpu/engine.py:284-312) per spectrum, from the dense K1 counts.
+ * Spectrum s owns hypotheses [spec_hyp_off[s], spec_hyp_off[s+1]).  Per spectrum: entries with count >= thr,
+ * ranked by (count desc, row desc, hypothesis asc), the first topk kept; with pair_closure their partner rows are
+ * added with count -1; duplicates of (spectrum, row) merge to the lowest hypothesis and highest count.  Output
+ * slots: spectrum s writes n_cand[s] candidates sorted by row at [s*cap, s*cap + n_cand[s]) of c_hyp (i64),
+ * c_row (i64), c_cnt (i64); cap >= (pair_closure ? 2 : 1) * topk.  Also hyp_scored (u32, #rows with count > 0)
+ * and hyp_matched (u64, sum of counts) per hypothesis, and their sums per spectrum (spec_scored, spec_matched,
+ * i64; may be NULL). */
+int vk_select_topk(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo, const int64_t* h_hi,
+                   const int64_t* win_off, const int32_t* cnt, const int64_t* partner, int thr, int topk,
+                   int pair_closure, int cap, int64_t* c_hyp, int64_t* c_row, int64_t* c_cnt, int64_t* n_cand,
+                   uint32_t* hyp_scored, uint64_t* hyp_matched, int64_t* spec_scored, int64_t* spec_matched,
+                   void* stream);
+
+/* Compaction of per-spectrum slots into a flat candidate list: with cand_off = scan(n_cand), copies slot s to
+ * [cand_off[s], cand_off[s+1]) and writes c_maxfz from h_maxfz[c_hyp]. */
+int vk_compact_cands(int n_spec, int cap, const int64_t* n_cand, const int64_t* cand_off, const int64_t* s_hyp,
+                     const int64_t* s_row, const int64_t* s_cnt, const int8_t* h_maxfz, int64_t* c_hyp,
+                     int64_t* c_row, int64_t* c_cnt, int32_t* c_row32, int8_t* c_maxfz, void* stream);
+
+/* K2 exact rescoring (reference kernels.cu:263-376, closed mode), B200 launch: one warp per spectrum, lanes over
+ * candidates, the spectrum's (first 512) peaks in shared memory.  Candidates of spectrum s are
+ * [cand_off[s], cand_off[s+1]) (cand_off has n_spec+1 entries, spectrum ids are 0..n_spec-1). */
+int vk_k2_spectra(const vk_frag_params* fp, int n_spec, const int64_t* cand_off, const int32_t* c_row,
+                  const int8_t* c_maxfz, const int64_t* pk_off, const float* pk_mass, const float* pk_int,
+                  const int64_t* seq_off, const uint8_t* len, const uint64_t* mask, const float* mass32,
+                  const uint8_t* res, float tol_lo, float tol_hi, const float* c_shift, double* o_hs, float* o_sb,
+                  float* o_sy, float* o_ppm, int16_t* o_mb, int16_t* o_my, int16_t* o_lb, int16_t* o_ly,
+                  void* stream);
+
+/* PSM ranking (reference vulcan/gpu/engine.py:366-392): per spectrum, candidates with matched_b + matched_y >=
+ * min_matched ranked by (hyperscore desc, row asc); the first `report` go to slots [s*report, ...): psm_cand (i64,
+ * candidate index or -1), psm_rank (i32, 1-based), psm_dnext, psm_dbest (f64).  n_psm[s] = number written. */
+int vk_psm_rank(int n_spec, const int64_t* cand_off, const int64_t* c_row, const double* hs, const int16_t* mb,
+                const int16_t* my, int min_matched, int report, int64_t* psm_cand, int32_t* psm_rank,
+                double* psm_dnext, double* psm_dbest, int32_t* n_psm, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VULCAN_B200_H */

@@ -1,0 +1,228 @@
+// K0 peak view and precursor hypotheses on the device.
+//
+// K0 (reference vulcan/gpu/engine.py:171-210, global peak mode): peaks with fmin <= m/z <= fmax (not NaN), mass =
+// m/z - PROTON in f32, the top max_peaks by (intensity desc, mass desc), then mass ascending.  One CTA per
+// spectrum sorts 64-bit keys that carry both values (no payload): (~ord(intensity), ~ord(mass)) for the selection
+// and (ord(mass), ~ord(intensity)) for the final order, where ord() maps a float to an order-preserving u32.  Peaks
+// with equal intensity and mass are indistinguishable, so the reference's remaining tie order (input position)
+// cannot change any output.  TIC = f64 sum of the kept intensities (fixed-order tree), stored as f32.
+//
+// Hypotheses (reference vulcan/gpu/host.py:64-91): per valid spectrum with a finite precursor m/z, charges (the
+// known one, else the configured range) x isotope errors in (charge, isotope) order, Sage f32 arithmetic, row
+// window [lower_bound(lo), upper_bound(hi)) over the mass-sorted index masses.
+#include "common.cuh"
+
+namespace {
+
+__device__ __forceinline__ uint32_t ord_f32(float x) {
+  uint32_t u = __float_as_uint(x);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float unord_f32(uint32_t o) {
+  uint32_t u = (o & 0x80000000u) ? (o & 0x7fffffffu) : ~o;
+  return __uint_as_float(u);
+}
+__device__ __forceinline__ bool in_range(float mz, float fmin, float fmax) {
+  return mz >= fmin && mz <= fmax;   // false for NaN
+}
+
+__global__ void k0_count_k(int n_spec, const int64_t* raw_off, const float* raw_mz, float fmin, float fmax,
+                           int max_peaks, int64_t* kept) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= n_spec) return;
+  long long c = 0;
+  for (int64_t i = raw_off[warp] + lane; i < raw_off[warp + 1]; i += 32) c += in_range(raw_mz[i], fmin, fmax);
+  c = vk::warp_sum(c);
+  if (lane == 0) kept[warp] = min(c, (long long)max_peaks);
+}
+
+__device__ __forceinline__ void block_bitonic_u64(uint64_t* v, int n_pow2) {
+  for (int k = 2; k <= n_pow2; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = threadIdx.x; i < n_pow2; i += blockDim.x) {
+        int p = i ^ j;
+        if (p > i) {
+          uint64_t a = v[i], b = v[p];
+          bool up = (i & k) == 0;
+          if ((a > b) == up) { v[i] = b; v[p] = a; }
+        }
+      }
+      __syncthreads();
+    }
+}
+
+constexpr int K0_THREADS = 256;
+
+__global__ void __launch_bounds__(K0_THREADS)
+k0_fill_k(int n_spec, const int64_t* raw_off, const float* raw_mz, const float* raw_int, float fmin, float fmax,
+          int max_peaks, int min_peaks, const int64_t* pk_off, float* pk_mass, float* pk_int, float* tic,
+          uint8_t* valid) {
+  extern __shared__ uint64_t k0_keys[];
+  __shared__ double red[K0_THREADS / 32];
+  const int s = blockIdx.x;
+  const int64_t r0 = raw_off[s];
+  const int n = (int)(raw_off[s + 1] - r0);
+  int n_pow2 = 1;
+  while (n_pow2 < n) n_pow2 <<= 1;
+  for (int i = threadIdx.x; i < n_pow2; i += blockDim.x) {
+    uint64_t k = ~0ull;
+    if (i < n) {
+      float mz = raw_mz[r0 + i];
+      if (in_range(mz, fmin, fmax)) {
+        float mass = __fsub_rn(mz, VK_PROTON);
+        k = ((uint64_t)(~ord_f32(raw_int[r0 + i])) << 32) | (uint64_t)(~ord_f32(mass));
+      }
+    }
+    k0_keys[i] = k;
+  }
+  __syncthreads();
+  block_bitonic_u64(k0_keys, n_pow2);   // in-range peaks first, by (intensity desc, mass desc)
+  const int64_t o0 = pk_off[s];
+  const int kept = (int)(pk_off[s + 1] - o0);
+  int m_pow2 = 1;
+  while (m_pow2 < kept) m_pow2 <<= 1;
+  // re-key the kept peaks for the mass order (each thread rewrites only the elements it reads)
+  for (int i = threadIdx.x; i < m_pow2; i += blockDim.x) {
+    uint64_t k = ~0ull;
+    if (i < kept) {
+      uint64_t a = k0_keys[i];
+      float it = unord_f32(~(uint32_t)(a >> 32));
+      float mass = unord_f32(~(uint32_t)a);
+      k = ((uint64_t)ord_f32(mass) << 32) | (uint64_t)(~ord_f32(it));
+    }
+    k0_keys[i] = k;
+  }
+  __syncthreads();
+  block_bitonic_u64(k0_keys, m_pow2);
+  double part = 0.0;
+  for (int i = threadIdx.x; i < kept; i += blockDim.x) {
+    uint64_t k = k0_keys[i];
+    float mass = unord_f32((uint32_t)(k >> 32));
+    float it = unord_f32(~(uint32_t)k);
+    pk_mass[o0 + i] = mass;
+    pk_int[o0 + i] = it;
+    part += (double)it;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(VK_FULL, part, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = part;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < K0_THREADS / 32; ++w) t += red[w];
+    tic[s] = (float)t;
+    valid[s] = kept >= min_peaks;
+  }
+}
+
+__global__ void hyp_count_k(int n_spec, const uint8_t* valid, const double* pmz, const int8_t* charge, int n_z,
+                            int n_iso, int64_t* n_hyp) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n_spec) return;
+  bool ok = valid[s] && isfinite(pmz[s]);
+  n_hyp[s] = ok ? (int64_t)(charge[s] > 0 ? 1 : n_z) * n_iso : 0;
+}
+
+__device__ __forceinline__ int64_t lower_bound_g(const float* a, int64_t n, float x) {
+  int64_t lo = 0, hi = n;
+  while (lo < hi) {
+    int64_t m = (lo + hi) >> 1;
+    if (a[m] < x) lo = m + 1; else hi = m;
+  }
+  return lo;
+}
+__device__ __forceinline__ int64_t upper_bound_g(const float* a, int64_t n, float x) {
+  int64_t lo = 0, hi = n;
+  while (lo < hi) {
+    int64_t m = (lo + hi) >> 1;
+    if (a[m] <= x) lo = m + 1; else hi = m;
+  }
+  return lo;
+}
+
+__global__ void hyp_fill_k(int n_spec, const uint8_t* valid, const double* pmz, const int8_t* charge, int z_lo,
+                           int z_hi, int iso_lo, int iso_hi, float ppm_lo, float ppm_hi, int mfc,
+                           const float* idx_mass32, int64_t n_rows, const int64_t* hyp_off, int32_t* h_spec,
+                           int8_t* h_z, int8_t* h_iso, float* h_pm, float* h_M, int64_t* h_lo, int64_t* h_hi,
+                           int8_t* h_maxfz) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n_spec) return;
+  if (!(valid[s] && isfinite(pmz[s]))) return;
+  int64_t o = hyp_off[s];
+  const int zk = charge[s];
+  const int za = zk > 0 ? zk : z_lo, zb = zk > 0 ? zk : z_hi;
+  const float mz = __fsub_rn(__double2float_rn(pmz[s]), VK_PROTON);
+  for (int z = za; z <= zb; ++z) {
+    const float pm = __fmul_rn(mz, (float)z);
+    int mf = z;
+    if (mfc > 0) mf = min(z, mfc + 1);
+    mf = max(mf, 2);
+    for (int iso = iso_lo; iso <= iso_hi; ++iso) {
+      const float M = __fsub_rn(pm, __fmul_rn((float)iso, VK_NEUTRON));
+      const float lo = __fadd_rn(M, __fdiv_rn(__fmul_rn(M, ppm_lo), 1000000.0f));
+      const float hi = __fadd_rn(M, __fdiv_rn(__fmul_rn(M, ppm_hi), 1000000.0f));
+      h_spec[o] = s;
+      h_z[o] = (int8_t)z;
+      h_iso[o] = (int8_t)iso;
+      h_pm[o] = pm;
+      h_M[o] = M;
+      h_lo[o] = lower_bound_g(idx_mass32, n_rows, lo);
+      h_hi[o] = upper_bound_g(idx_mass32, n_rows, hi);
+      h_maxfz[o] = (int8_t)mf;
+      ++o;
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int vk_k0_count(int n_spec, const int64_t* raw_off, const float* raw_mz, float fmin, float fmax, int max_peaks,
+                int64_t* kept, void* stream) {
+  if (n_spec == 0) return 0;
+  int64_t threads = (int64_t)n_spec * 32;
+  k0_count_k<<<(unsigned)((threads + 255) / 256), 256, 0, (cudaStream_t)stream>>>(n_spec, raw_off, raw_mz, fmin, fmax,
+                                                                                  max_peaks, kept);
+  return vk_launch_status();
+}
+
+int vk_k0_fill(int n_spec, const int64_t* raw_off, const float* raw_mz, const float* raw_int, float fmin,
+               float fmax, int max_peaks, int min_peaks, const int64_t* pk_off, float* pk_mass, float* pk_int,
+               float* tic, uint8_t* valid, int max_raw, void* stream) {
+  if (n_spec == 0) return 0;
+  if (max_raw < 0 || max_raw > 16384) return VK_E_ARG;
+  int n_pow2 = 1;
+  while (n_pow2 < max_raw) n_pow2 <<= 1;
+  size_t sh = (size_t)n_pow2 * sizeof(uint64_t);
+  cudaError_t e = cudaFuncSetAttribute(k0_fill_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  if (e != cudaSuccess) return vk_err(e);
+  k0_fill_k<<<n_spec, K0_THREADS, sh, (cudaStream_t)stream>>>(n_spec, raw_off, raw_mz, raw_int, fmin, fmax,
+                                                               max_peaks, min_peaks, pk_off, pk_mass, pk_int, tic,
+                                                               valid);
+  return vk_launch_status();
+}
+
+int vk_hyp_count(int n_spec, const uint8_t* valid, const double* precursor_mz, const int8_t* charge, int z_lo,
+                 int z_hi, int iso_lo, int iso_hi, int64_t* n_hyp, void* stream) {
+  if (n_spec == 0) return 0;
+  if (z_hi < z_lo || iso_hi < iso_lo) return VK_E_ARG;
+  hyp_count_k<<<(unsigned)((n_spec + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
+      n_spec, valid, precursor_mz, charge, z_hi - z_lo + 1, iso_hi - iso_lo + 1, n_hyp);
+  return vk_launch_status();
+}
+
+int vk_hyp_fill(int n_spec, const uint8_t* valid, const double* precursor_mz, const int8_t* charge, int z_lo,
+                int z_hi, int iso_lo, int iso_hi, float ppm_lo, float ppm_hi, int max_fragment_charge,
+                const float* idx_mass32, int64_t n_rows, const int64_t* hyp_off, int32_t* h_spec, int8_t* h_z,
+                int8_t* h_iso, float* h_pm, float* h_M, int64_t* h_lo, int64_t* h_hi, int8_t* h_maxfz,
+                void* stream) {
+  if (n_spec == 0) return 0;
+  if (z_hi < z_lo || iso_hi < iso_lo) return VK_E_ARG;
+  hyp_fill_k<<<(unsigned)((n_spec + 127) / 128), 128, 0, (cudaStream_t)stream>>>(
+      n_spec, valid, precursor_mz, charge, z_lo, z_hi, iso_lo, iso_hi, ppm_lo, ppm_hi, max_fragment_charge,
+      idx_mass32, n_rows, hyp_off, h_spec, h_z, h_iso, h_pm, h_M, h_lo, h_hi, h_maxfz);
+  return vk_launch_status();
+}
+
+}  // extern "C"

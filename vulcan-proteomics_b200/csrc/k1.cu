@@ -1,0 +1,192 @@
+// K1 shared-peak counting on the tiled fragment index.
+//
+// Work items are (tile, hypothesis) pairs grouped by tile.  One CTA owns one tile: thread 0 stages the tile's
+// postings and its coarse-bin CSR into shared memory with two bulk (TMA) copies completing on one mbarrier; then
+// each warp takes the tile's hypotheses in turn.  For a hypothesis the lanes stride over the spectrum's peaks x
+// fragment charges; a peak's tolerance window [a, bd] (Sage f32 arithmetic) is the posting key range
+// [bits(a) - bits(fmin), bits(bd) - bits(fmin)] << row_bits, found through the coarse bins and a binary search in
+// shared memory; every posting in range whose row lies in the hypothesis window bumps a warp-private shared-memory
+// histogram.  Matches of the same row inside a warp are combined (match_any) before the shared atomic.
+// The histogram is written to the hypothesis' dense count slice.
+//
+// Result = the reference's brute-force count (vulcan/gpu/kernels.cu:195-232) for every window row: a posting key
+// compares exactly like its f32 fragment mass, so f == a and f == bd are both counted.
+#include "common.cuh"
+
+namespace {
+
+constexpr int K1_WARPS = 4;
+constexpr uint32_t WAIT_LIMIT = 1u << 22;
+
+__global__ void plan_count_k(int64_t n_hyp, int shift, const int64_t* h_lo, const int64_t* h_hi,
+                             unsigned long long* tile_items, int64_t* win_len) {
+  int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (h >= n_hyp) return;
+  int64_t lo = h_lo[h], hi = h_hi[h];
+  win_len[h] = hi > lo ? hi - lo : 0;
+  if (hi <= lo) return;
+  for (int64_t t = lo >> shift; t <= (hi - 1) >> shift; ++t) atomicAdd(&tile_items[t], 1ull);
+}
+
+__global__ void plan_fill_k(int64_t n_hyp, int shift, const int64_t* h_lo, const int64_t* h_hi,
+                            const int64_t* tile_item_off, unsigned long long* cursor, int32_t* item_hyp) {
+  int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (h >= n_hyp) return;
+  int64_t lo = h_lo[h], hi = h_hi[h];
+  if (hi <= lo) return;
+  for (int64_t t = lo >> shift; t <= (hi - 1) >> shift; ++t) {
+    unsigned long long pos = atomicAdd(&cursor[t], 1ull);
+    item_hyp[tile_item_off[t] + (int64_t)pos] = (int32_t)h;
+  }
+}
+
+__global__ void __launch_bounds__(K1_WARPS * 32)
+k1_tiles_k(vk_tindex ix, float tol_lo, float tol_hi, int tol_da, int post_cap, const int64_t* tile_item_off,
+           const int32_t* item_hyp, const int32_t* h_spec, const int8_t* h_maxfz, const int64_t* h_lo,
+           const int64_t* h_hi, const int64_t* win_off, const int64_t* pk_off, const float* pk_mass, int32_t* cnt,
+           int32_t* status) {
+  extern __shared__ __align__(16) uint8_t k1_smem[];
+  __shared__ __align__(8) uint64_t bar;
+  const int64_t t = blockIdx.x;
+  const int64_t i0 = tile_item_off[t], i1 = tile_item_off[t + 1];
+  if (i0 == i1) return;
+  const int T = 1 << ix.tile_shift;
+  const int nb = 1 << ix.cbin_bits;
+  const int stride = (nb + 1 + 7) & ~7;
+  uint32_t* post = reinterpret_cast<uint32_t*>(k1_smem);
+  uint16_t* cb = reinterpret_cast<uint16_t*>(k1_smem + (size_t)post_cap * 4);
+  uint32_t* hist = reinterpret_cast<uint32_t*>(k1_smem + (size_t)post_cap * 4 + (size_t)stride * 2);
+  const int64_t po = ix.tile_off[t];
+  const uint32_t post_bytes = (uint32_t)((ix.tile_off[t + 1] - po) * 4);
+  const uint32_t cb_bytes = (uint32_t)stride * 2;
+  if (threadIdx.x == 0) {
+    vk::mbar_init(&bar, 1);
+    vk::fence_mbar_init();
+    vk::mbar_expect_tx(&bar, post_bytes + cb_bytes);
+    if (post_bytes) vk::bulk_g2s(post, ix.postings + po, post_bytes, &bar);
+    vk::bulk_g2s(cb, ix.cbin_off + t * stride, cb_bytes, &bar);
+  }
+  __syncthreads();
+  if (!vk::mbar_wait(&bar, 0, WAIT_LIMIT)) {
+    // give up on this tile, but do not leave while the copies may still land in shared memory
+    if (threadIdx.x == 0) atomicOr(status, VK_STATUS_WAIT_TIMEOUT);
+    vk::mbar_wait(&bar, 0, WAIT_LIMIT);
+    return;
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint32_t* hw = hist + warp * T;
+  const int row_bits = ix.row_bits;
+  const uint32_t rowmask = (1u << row_bits) - 1u;
+  const int sh = 32 - ix.cbin_bits;
+  const float fmin = __uint_as_float(ix.fmin_bits), fmax = __uint_as_float(ix.fmax_bits);
+  const uint32_t krange = ix.fmax_bits - ix.fmin_bits;
+  const int64_t r0 = t << ix.tile_shift;
+  for (int64_t it = i0 + warp; it < i1; it += K1_WARPS) {
+    const int h = item_hyp[it];
+    const int64_t lo = h_lo[h], hi = h_hi[h];
+    const int rlo = (int)max(lo - r0, (int64_t)0), rhi = (int)min(hi - r0, (int64_t)T);
+    for (int j = lane; j < T; j += 32) hw[j] = 0;
+    __syncwarp();
+    const int s = h_spec[h], maxfz = h_maxfz[h];
+    const int64_t p0 = pk_off[s], p1 = pk_off[s + 1];
+    const int64_t n_iter = (p1 - p0 + 31) & ~31ll;
+    for (int64_t q = lane; q < n_iter; q += 32) {
+      const int64_t p = p0 + q;
+      const float pm = p < p1 ? pk_mass[p] : 0.f;
+      for (int z = 1; z < maxfz; ++z) {
+        int e = 0, e1 = 0;
+        uint32_t hi_key = 0;
+        if (p < p1) {
+          const float m = __fmul_rn(pm, (float)z);
+          const float a = vk::tol_bound(m, tol_lo, tol_da), bd = vk::tol_bound(m, tol_hi, tol_da);
+          if (bd >= fmin && a <= fmax) {
+            const uint32_t ka = a <= fmin ? 0u : __float_as_uint(a) - ix.fmin_bits;
+            const uint32_t kb = bd >= fmax ? krange : __float_as_uint(bd) - ix.fmin_bits;
+            const uint32_t lo_key = ka << row_bits;
+            hi_key = (kb << row_bits) | rowmask;
+            e = cb[lo_key >> sh];
+            e1 = cb[(hi_key >> sh) + 1];
+            int R = e1;
+            while (e < R) {
+              int M = (e + R) >> 1;
+              if (post[M] < lo_key) e = M + 1; else R = M;
+            }
+          }
+        }
+        // scan the key range; all lanes step together so equal rows can be merged before the shared atomic
+        while (__any_sync(VK_FULL, e < e1)) {
+          int local = -1;
+          if (e < e1) {
+            const uint32_t v = post[e];
+            if (v <= hi_key) {
+              const int l = (int)(v & rowmask);
+              if (l >= rlo && l < rhi) local = l;
+              ++e;
+            } else {
+              e = e1;
+            }
+          }
+          const unsigned peers = __match_any_sync(VK_FULL, local);
+          if (local >= 0 && (__ffs(peers) - 1) == lane) atomicAdd(&hw[local], (uint32_t)__popc(peers));
+        }
+      }
+    }
+    __syncwarp();
+    const int64_t base = win_off[h] + (r0 - lo);
+    for (int j = rlo + lane; j < rhi; j += 32) cnt[base + j] = (int32_t)hw[j];
+    __syncwarp();
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int vk_k1_plan_count(const vk_tindex* ix, int64_t n_hyp, const int64_t* h_lo, const int64_t* h_hi,
+                     int64_t* tile_items, int64_t* win_len, void* stream) {
+  if (!ix) return VK_E_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (ix->n_tiles > 0) {
+    cudaError_t e = cudaMemsetAsync(tile_items, 0, sizeof(int64_t) * ix->n_tiles, st);
+    if (e != cudaSuccess) return vk_err(e);
+  }
+  if (n_hyp == 0) return 0;
+  plan_count_k<<<(unsigned)((n_hyp + 255) / 256), 256, 0, st>>>(n_hyp, ix->tile_shift, h_lo, h_hi,
+                                                                 (unsigned long long*)tile_items, win_len);
+  return vk_launch_status();
+}
+
+int vk_k1_plan_fill(const vk_tindex* ix, int64_t n_hyp, const int64_t* h_lo, const int64_t* h_hi,
+                    const int64_t* tile_item_off, int64_t* cursor, int32_t* item_hyp, void* stream) {
+  if (!ix) return VK_E_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (ix->n_tiles > 0) {
+    cudaError_t e = cudaMemsetAsync(cursor, 0, sizeof(int64_t) * ix->n_tiles, st);
+    if (e != cudaSuccess) return vk_err(e);
+  }
+  if (n_hyp == 0) return 0;
+  plan_fill_k<<<(unsigned)((n_hyp + 255) / 256), 256, 0, st>>>(n_hyp, ix->tile_shift, h_lo, h_hi, tile_item_off,
+                                                                (unsigned long long*)cursor, item_hyp);
+  return vk_launch_status();
+}
+
+int vk_k1_tiles(const vk_tindex* ix, const vk_frag_params* fp, float tol_lo, float tol_hi,
+                const int64_t* tile_item_off, const int32_t* item_hyp, const int32_t* h_spec,
+                const int8_t* h_maxfz, const int64_t* h_lo, const int64_t* h_hi, const int64_t* win_off,
+                const int64_t* pk_off, const float* pk_mass, int32_t* cnt, int32_t* status, void* stream) {
+  if (!ix || !fp || !status) return VK_E_ARG;
+  if (ix->n_tiles == 0) return 0;
+  if ((ix->max_tile_postings & 3) || ix->max_tile_postings < 0) return VK_E_ARG;
+  const int T = 1 << ix->tile_shift;
+  const int stride = ((1 << ix->cbin_bits) + 1 + 7) & ~7;
+  size_t sh = (size_t)ix->max_tile_postings * 4 + (size_t)stride * 2 + (size_t)K1_WARPS * T * 4;
+  if (sh > 200 * 1024) return VK_E_ARG;
+  cudaError_t e = cudaFuncSetAttribute(k1_tiles_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  if (e != cudaSuccess) return vk_err(e);
+  k1_tiles_k<<<(unsigned)ix->n_tiles, K1_WARPS * 32, sh, (cudaStream_t)stream>>>(
+      *ix, tol_lo, tol_hi, fp->tol_da, ix->max_tile_postings, tile_item_off, item_hyp, h_spec, h_maxfz, h_lo, h_hi,
+      win_off, pk_off, pk_mass, cnt, status);
+  return vk_launch_status();
+}
+
+}  // extern "C"

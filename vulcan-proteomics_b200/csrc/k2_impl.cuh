@@ -1,0 +1,177 @@
+// K2 exact rescoring body (Sage score_candidate semantics, reference vulcan/gpu/kernels.cu:240-376).
+//
+// B200 launch shape: one warp per spectrum, K2_WARPS spectra per CTA.  The warp stages its spectrum's first 512
+// mass-sorted peaks in shared memory; each lane scores whole candidates (the f32 sums are sequential in ion order:
+// b ions k ascending, fragment charge ascending, then y ions), so the per-candidate arithmetic is the reference's
+// operation for operation and the outputs are bit-identical.
+#pragma once
+#include "common.cuh"
+
+namespace vk {
+
+constexpr int K2_WARPS = 8;
+
+struct K2Out {
+  double* hs;
+  float* sb;
+  float* sy;
+  float* ppm;
+  int16_t* mb;
+  int16_t* my;
+  int16_t* lb;
+  int16_t* ly;
+};
+
+struct RunLen {
+  int start, length, last, longest;
+};
+
+// Longest run of consecutive matched ion indices (kernels.cu:252-258)
+__device__ __forceinline__ void run_matched(RunLen& r, int idx) {
+  if (r.last == idx) return;
+  if (r.start + r.length == idx) {
+    r.length += 1;
+  } else {
+    r.start = idx;
+    r.length = 1;
+  }
+  r.longest = max(r.longest, r.length);
+  r.last = idx;
+}
+
+__device__ __forceinline__ int lower_bound_smem(const float* v, int n, float x) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    int m = (lo + hi) >> 1;
+    if (v[m] < x) lo = m + 1; else hi = m;
+  }
+  return lo;
+}
+
+template <bool SHIFT>
+__device__ __forceinline__ void k2_score(const SmemFrag& fp, const float* sm, const float* si, int np, int r,
+                                         int maxfz, const int64_t* seq_off, const uint8_t* len,
+                                         const uint64_t* mask, const float* mass32, const uint8_t* res,
+                                         float tol_lo, float tol_hi, float shift, const K2Out& out, int64_t c) {
+  const uint8_t* sq = res + seq_off[r];
+  int L = len[r];
+  uint64_t mk = mask[r];
+  float sb = 0.f, sy = 0.f, ppm = 0.f;
+  int mb = 0, my = 0;
+  RunLen rb = {0, 0, 0, 0}, ry = {0, 0, 0, 0};
+  const int da = fp.tol_da;
+  int n_alt = 1;
+  float iu[2][SHIFT ? VK_K2_MAXLEN : 1], is_[2][SHIFT ? VK_K2_MAXLEN : 1];
+  unsigned char nu[2][SHIFT ? VK_K2_MAXLEN : 1], ns[2][SHIFT ? VK_K2_MAXLEN : 1];
+  if (SHIFT) {
+    n_alt = shift != 0.f ? 2 : 1;
+    if (n_alt == 2) {
+      for (int k = 0; k < (SHIFT ? VK_K2_MAXLEN : 1); ++k) {
+        iu[0][k] = iu[1][k] = is_[0][k] = is_[1][k] = 0.f;
+        nu[0][k] = nu[1][k] = ns[0][k] = ns[1][k] = 0;
+      }
+    }
+  }
+  for (int kind = 0; kind < 2; ++kind) {
+    float cum = kind == 0 ? nterm_of(fp, mk) : __fsub_rn(mass32[r], nterm_of(fp, mk));
+    for (int k = 0; k + 1 < L; ++k) {
+      float rm = resmass(fp, sq[k], k, mk);
+      cum = kind == 0 ? __fadd_rn(cum, rm) : __fsub_rn(cum, rm);
+      for (int z = 1; z < maxfz; ++z) {
+        int best = -1;
+        float mx = 0.f, best_mz = 0.f;
+        for (int alt = 0; alt < n_alt; ++alt) {
+          int best_a = -1;
+          float mx_a = 0.f;
+          float base = alt == 0 ? cum : __fadd_rn(cum, shift);
+          float mz = __fdiv_rn(base, (float)z);
+          float a = tol_bound(mz, tol_lo, da), bd = tol_bound(mz, tol_hi, da);
+          for (int j = lower_bound_smem(sm, np, a); j < np && sm[j] <= bd; ++j) {
+            float it = si[j];
+            if (it >= mx) { mx = it; best = j; best_mz = mz; }
+            if (SHIFT && it >= mx_a) { mx_a = it; best_a = j; }
+          }
+          if (SHIFT && n_alt == 2 && best_a >= 0 && k < VK_K2_MAXLEN) {
+            if (alt == 0) { iu[kind][k] = __fadd_rn(iu[kind][k], si[best_a]); nu[kind][k] += 1; }
+            else { is_[kind][k] = __fadd_rn(is_[kind][k], si[best_a]); ns[kind][k] += 1; }
+          }
+        }
+        if (best >= 0) {
+          float pmass = sm[best], pint = si[best];
+          float num = __fmul_rn(__fmul_rn(pint, fabsf(__fsub_rn(best_mz, pmass))), 2.0e6f);
+          ppm = __fadd_rn(ppm, __fdiv_rn(num, __fadd_rn(best_mz, pmass)));
+          if (kind == 0) { mb += 1; sb = __fadd_rn(sb, pint); run_matched(rb, k); }
+          else { my += 1; sy = __fadd_rn(sy, pint); run_matched(ry, k); }
+        }
+      }
+    }
+  }
+  if (SHIFT && n_alt == 2) {
+    // best site of the delta (kernels.cu:343-363): b_k shifted iff k >= site, y_k iff k < site
+    int Lk = min(L - 1, VK_K2_MAXLEN);
+    float b_u = 0.f, y_s = 0.f, b_s = 0.f, y_u = 0.f;
+    int nb_u = 0, ny_s = 0, nb_s = 0, ny_u = 0;
+    for (int k = 0; k < Lk; ++k) {
+      b_s = __fadd_rn(b_s, is_[0][k]); nb_s += ns[0][k];
+      y_u = __fadd_rn(y_u, iu[1][k]); ny_u += nu[1][k];
+    }
+    double best_hs = -1e300;
+    for (int st = 0; st < L; ++st) {
+      if (st > 0 && st - 1 < Lk) {
+        int k = st - 1;
+        b_u = __fadd_rn(b_u, iu[0][k]); nb_u += nu[0][k]; b_s = __fsub_rn(b_s, is_[0][k]); nb_s -= ns[0][k];
+        y_s = __fadd_rn(y_s, is_[1][k]); ny_s += ns[1][k]; y_u = __fsub_rn(y_u, iu[1][k]); ny_u -= nu[1][k];
+      }
+      float sb2 = __fadd_rn(b_u, b_s), sy2 = __fadd_rn(y_u, y_s);
+      int mb2 = nb_u + nb_s, my2 = ny_u + ny_s;
+      double h2 = log((double)__fadd_rn(fmaxf(sb2, 0.f), 1.0f) * (double)__fadd_rn(fmaxf(sy2, 0.f), 1.0f)) +
+                  lnfact(mb2) + lnfact(my2);
+      if (h2 > best_hs) { best_hs = h2; mb = mb2; my = my2; sb = fmaxf(sb2, 0.f); sy = fmaxf(sy2, 0.f); }
+    }
+  }
+  double i2 = (double)__fadd_rn(sb, 1.0f) * (double)__fadd_rn(sy, 1.0f);
+  double hs = log(i2) + lnfact(mb) + lnfact(my);
+  if (!isfinite(hs)) hs = 255.0;
+  out.hs[c] = hs;
+  out.sb[c] = sb;
+  out.sy[c] = sy;
+  out.ppm[c] = __fdiv_rn(ppm, __fadd_rn(sb, sy));
+  out.mb[c] = (int16_t)mb;
+  out.my[c] = (int16_t)my;
+  out.lb[c] = (int16_t)rb.longest;
+  out.ly[c] = (int16_t)ry.longest;
+}
+
+// Warp-per-spectrum driver.  spec_ids == nullptr: spectrum bs uses peaks of spectrum bs.
+template <bool SHIFT>
+__device__ __forceinline__ void k2_body(const SmemFrag& fp, int n_spec, const int64_t* cand_off,
+                                        const int32_t* c_row, const int8_t* c_maxfz, const int32_t* spec_ids,
+                                        const int64_t* pk_off, const float* pk_mass, const float* pk_int,
+                                        const int64_t* seq_off, const uint8_t* len, const uint64_t* mask,
+                                        const float* mass32, const uint8_t* res, float tol_lo, float tol_hi,
+                                        const float* c_shift, const K2Out& out) {
+  __shared__ float s_mass[K2_WARPS][VK_K2_MAXPK];
+  __shared__ float s_int[K2_WARPS][VK_K2_MAXPK];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int bs = blockIdx.x * K2_WARPS + warp; bs < n_spec; bs += gridDim.x * K2_WARPS) {
+    int s = spec_ids ? spec_ids[bs] : bs;
+    int64_t p0 = pk_off[s];
+    int np = (int)min((int64_t)VK_K2_MAXPK, pk_off[s + 1] - p0);
+    float* sm = s_mass[warp];
+    float* si = s_int[warp];
+    __syncwarp();
+    for (int j = lane; j < np; j += 32) {
+      sm[j] = pk_mass[p0 + j];
+      si[j] = pk_int[p0 + j];
+    }
+    __syncwarp();
+    int64_t c1 = cand_off[bs + 1];
+    for (int64_t c = cand_off[bs] + lane; c < c1; c += 32) {
+      float shift = SHIFT ? c_shift[c] : 0.f;
+      k2_score<SHIFT>(fp, sm, si, np, c_row[c], c_maxfz[c], seq_off, len, mask, mass32, res, tol_lo, tol_hi, shift,
+                      out, c);
+    }
+  }
+}
+
+}  // namespace vk

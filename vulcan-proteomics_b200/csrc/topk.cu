@@ -1,0 +1,249 @@
+// Per-spectrum top-K with pair closure (reference vulcan/gpu/engine.py:284-312), one warp per spectrum.
+//
+// The reference sorts every appended (hyp, row, count) of the run by a packed key
+// (spectrum, 32767 - min(count, 32767), 2^28 - 1 - row) and keeps rank < topk per spectrum, then adds partner rows
+// and merges duplicates of (spectrum, row) to the lowest hypothesis and highest count.  Here a warp reads its
+// spectrum's dense K1 counts, computes the per-hypothesis scored/matched statistics, and
+//   - if at most topk entries pass the threshold, takes them all (ballot compaction);
+//   - otherwise finds the topk-th largest 63-bit key (min(count,32767), row, -hypothesis) by an 8-bit radix select
+//     in shared memory and keeps the keys at or above it (keys are unique, so exactly topk);
+// then appends the partners, sorts by (row, hypothesis) with a warp bitonic sort and merges duplicates.
+#include "common.cuh"
+
+namespace {
+
+constexpr int TK_WARPS = 4;
+
+struct WarpLists {
+  uint64_t* key;   // sort keys
+  int32_t* row;
+  int32_t* hl;     // hypothesis index within the spectrum
+  int32_t* cnt;
+  uint32_t* hist;  // 256 radix counters
+};
+
+__device__ __forceinline__ uint64_t sel_key(int c, int64_t r, int hl) {
+  uint64_t kc = (uint64_t)min(c, 32767);
+  return (kc << 48) | ((uint64_t)r << 18) | (uint64_t)((1 << 18) - 1 - hl);
+}
+
+__device__ __forceinline__ void warp_bitonic_u64(uint64_t* v, int n_pow2, int lane) {
+  for (int k = 2; k <= n_pow2; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = lane; i < n_pow2; i += 32) {
+        int p = i ^ j;
+        if (p > i) {
+          uint64_t a = v[i], b = v[p];
+          bool up = (i & k) == 0;
+          if ((a > b) == up) { v[i] = b; v[p] = a; }
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+__global__ void __launch_bounds__(TK_WARPS * 32)
+select_topk_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo, const int64_t* h_hi,
+              const int64_t* win_off, const int32_t* cnt, const int64_t* partner, int thr, int topk, int pair_closure,
+              int cap, int list_pow2, int64_t* c_hyp, int64_t* c_row, int64_t* c_cnt, int64_t* n_cand,
+              uint32_t* hyp_scored, uint64_t* hyp_matched, int64_t* spec_scored, int64_t* spec_matched) {
+  extern __shared__ __align__(16) uint8_t tk_smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int s = blockIdx.x * TK_WARPS + warp;
+  if (s >= n_spec) return;
+  const size_t per_warp = (size_t)list_pow2 * (8 + 4 + 4 + 4) + 256 * 4;
+  uint8_t* base = tk_smem + per_warp * warp;
+  WarpLists W;
+  W.key = reinterpret_cast<uint64_t*>(base);
+  W.row = reinterpret_cast<int32_t*>(base + (size_t)list_pow2 * 8);
+  W.hl = W.row + list_pow2;
+  W.cnt = W.hl + list_pow2;
+  W.hist = reinterpret_cast<uint32_t*>(W.cnt + list_pow2);
+  const unsigned lt_mask = (1u << lane) - 1u;
+
+  const int64_t hb = spec_hyp_off[s], he = spec_hyp_off[s + 1];
+  // pass A: per-hypothesis statistics and the number of appended entries
+  long long n_app = 0, s_sc = 0, s_mt = 0;
+  for (int64_t h = hb; h < he; ++h) {
+    const int64_t w0 = win_off[h], n = h_hi[h] - h_lo[h];
+    long long sc = 0, mt = 0, ap = 0;
+    for (int64_t j = lane; j < n; j += 32) {
+      int c = cnt[w0 + j];
+      sc += c > 0;
+      mt += c;
+      ap += c >= thr;
+    }
+    sc = vk::warp_sum(sc);
+    mt = vk::warp_sum(mt);
+    ap = vk::warp_sum(ap);
+    if (lane == 0) {
+      hyp_scored[h] = (uint32_t)sc;
+      hyp_matched[h] = (uint64_t)mt;
+    }
+    n_app += ap;
+    s_sc += sc;
+    s_mt += mt;
+  }
+  if (lane == 0 && spec_scored) {
+    spec_scored[s] = s_sc;
+    spec_matched[s] = s_mt;
+  }
+  // threshold key: every entry with key >= kth is selected
+  uint64_t kth = 0;
+  const bool limit = n_app > topk;
+  if (limit) {
+    uint64_t prefix = 0, pmask = 0;
+    long long need = topk;   // how many still to take from the entries matching prefix
+    for (int shift = 56; shift >= 0; shift -= 8) {
+      for (int i = lane; i < 256; i += 32) W.hist[i] = 0;
+      __syncwarp();
+      for (int64_t h = hb; h < he; ++h) {
+        const int64_t w0 = win_off[h], lo = h_lo[h], n = h_hi[h] - lo;
+        for (int64_t j = lane; j < n; j += 32) {
+          int c = cnt[w0 + j];
+          if (c < thr) continue;
+          uint64_t k = sel_key(c, lo + j, (int)(h - hb));
+          if ((k & pmask) == prefix) atomicAdd(&W.hist[(k >> shift) & 255], 1u);
+        }
+      }
+      __syncwarp();
+      // digit d from the top such that the entries with digit > d number < need <= those with digit >= d
+      long long above = 0;
+      int dsel = 0;
+      for (int d0 = 255; d0 >= 0; d0 -= 32) {
+        int d = d0 - lane;
+        long long v = W.hist[d];
+        // inclusive scan from the top digit downwards across the lanes of this group of 32 digits
+        long long inc = vk::warp_incl_scan(v);
+        unsigned hit = __ballot_sync(VK_FULL, above + inc >= need);
+        if (hit) {
+          int l = __ffs(hit) - 1;
+          long long inc_l = __shfl_sync(VK_FULL, inc, l);
+          long long v_l = __shfl_sync(VK_FULL, v, l);
+          dsel = d0 - l;
+          need -= above + inc_l - v_l;
+          break;
+        }
+        above += __shfl_sync(VK_FULL, inc, 31);
+      }
+      prefix |= (uint64_t)dsel << shift;
+      pmask |= 255ull << shift;
+      __syncwarp();
+    }
+    kth = prefix;
+  }
+  // gather the selected entries (ballot compaction, order: hypothesis, row)
+  int n_sel = 0;
+  for (int64_t h = hb; h < he; ++h) {
+    const int64_t w0 = win_off[h], lo = h_lo[h], n = h_hi[h] - lo;
+    for (int64_t j0 = 0; j0 < n; j0 += 32) {
+      const int64_t j = j0 + lane;
+      int c = j < n ? cnt[w0 + j] : -1;
+      bool take = j < n && c >= thr && (!limit || sel_key(c, lo + j, (int)(h - hb)) >= kth);
+      unsigned m = __ballot_sync(VK_FULL, take);
+      if (take) {
+        int pos = n_sel + __popc(m & lt_mask);
+        W.row[pos] = (int32_t)(lo + j);
+        W.hl[pos] = (int32_t)(h - hb);
+        W.cnt[pos] = c;
+      }
+      n_sel += __popc(m);
+    }
+  }
+  __syncwarp();
+  int n_list = n_sel;
+  if (pair_closure) {
+    for (int i = lane; i < n_sel; i += 32) {
+      W.row[n_sel + i] = (int32_t)partner[W.row[i]];
+      W.hl[n_sel + i] = W.hl[i];
+      W.cnt[n_sel + i] = -1;
+    }
+    n_list = 2 * n_sel;
+  }
+  __syncwarp();
+  // sort by (row, hypothesis); the low 16 bits carry the list index
+  int n_pow2 = 1;
+  while (n_pow2 < n_list) n_pow2 <<= 1;
+  for (int i = lane; i < n_pow2; i += 32)
+    W.key[i] = i < n_list ? (((uint64_t)W.row[i] << 34) | ((uint64_t)W.hl[i] << 16) | (uint64_t)i) : ~0ull;
+  __syncwarp();
+  warp_bitonic_u64(W.key, n_pow2, lane);
+  // merge equal rows: head = first of a run of equal rows (lowest hypothesis); count = max over the run
+  int n_out = 0;
+  int64_t slot = (int64_t)s * cap;
+  for (int i0 = 0; i0 < n_list; i0 += 32) {
+    int i = i0 + lane;
+    bool head = false;
+    int64_t r = 0;
+    if (i < n_list) {
+      r = (int64_t)(W.key[i] >> 34);
+      head = i == 0 || (int64_t)(W.key[i - 1] >> 34) != r;
+    }
+    unsigned m = __ballot_sync(VK_FULL, head);
+    if (head) {
+      int idx = (int)(W.key[i] & 0xffff);
+      int best = W.cnt[idx];
+      for (int k = i + 1; k < n_list && (int64_t)(W.key[k] >> 34) == r; ++k) best = max(best, W.cnt[W.key[k] & 0xffff]);
+      int pos = n_out + __popc(m & lt_mask);
+      c_hyp[slot + pos] = hb + (int)((W.key[i] >> 16) & 0x3ffff);
+      c_row[slot + pos] = r;
+      c_cnt[slot + pos] = best;
+    }
+    n_out += __popc(m);
+  }
+  if (lane == 0) n_cand[s] = n_out;
+}
+
+__global__ void compact_k(int n_spec, int cap, const int64_t* n_cand, const int64_t* cand_off, const int64_t* s_hyp,
+                          const int64_t* s_row, const int64_t* s_cnt, const int8_t* h_maxfz, int64_t* c_hyp,
+                          int64_t* c_row, int64_t* c_cnt, int32_t* c_row32, int8_t* c_maxfz) {
+  int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  int64_t s = g / cap;
+  int j = (int)(g % cap);
+  if (s >= n_spec || j >= n_cand[s]) return;
+  int64_t src = s * cap + j, dst = cand_off[s] + j;
+  int64_t h = s_hyp[src];
+  c_hyp[dst] = h;
+  c_row[dst] = s_row[src];
+  c_cnt[dst] = s_cnt[src];
+  c_row32[dst] = (int32_t)s_row[src];
+  c_maxfz[dst] = h_maxfz[h];
+}
+
+}  // namespace
+
+extern "C" {
+
+int vk_select_topk(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo, const int64_t* h_hi,
+                   const int64_t* win_off, const int32_t* cnt, const int64_t* partner, int thr, int topk,
+                   int pair_closure, int cap, int64_t* c_hyp, int64_t* c_row, int64_t* c_cnt, int64_t* n_cand,
+                   uint32_t* hyp_scored, uint64_t* hyp_matched, int64_t* spec_scored, int64_t* spec_matched,
+                   void* stream) {
+  if (n_spec == 0) return 0;
+  if (topk < 1 || topk > 8192 || cap < (pair_closure ? 2 : 1) * topk) return VK_E_ARG;
+  int list_pow2 = 32;
+  while (list_pow2 < (pair_closure ? 2 : 1) * topk) list_pow2 <<= 1;
+  size_t per_warp = (size_t)list_pow2 * 20 + 1024;
+  size_t sh = per_warp * TK_WARPS;
+  if (sh > 220 * 1024) return VK_E_ARG;
+  cudaError_t e = cudaFuncSetAttribute(select_topk_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  if (e != cudaSuccess) return vk_err(e);
+  select_topk_k<<<(unsigned)((n_spec + TK_WARPS - 1) / TK_WARPS), TK_WARPS * 32, sh, (cudaStream_t)stream>>>(
+      n_spec, spec_hyp_off, h_lo, h_hi, win_off, cnt, partner, thr, topk, pair_closure, cap, list_pow2, c_hyp, c_row,
+      c_cnt, n_cand, hyp_scored, hyp_matched, spec_scored, spec_matched);
+  return vk_launch_status();
+}
+
+int vk_compact_cands(int n_spec, int cap, const int64_t* n_cand, const int64_t* cand_off, const int64_t* s_hyp,
+                     const int64_t* s_row, const int64_t* s_cnt, const int8_t* h_maxfz, int64_t* c_hyp,
+                     int64_t* c_row, int64_t* c_cnt, int32_t* c_row32, int8_t* c_maxfz, void* stream) {
+  if (n_spec == 0) return 0;
+  int64_t n = (int64_t)n_spec * cap;
+  compact_k<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(n_spec, cap, n_cand, cand_off, s_hyp,
+                                                                           s_row, s_cnt, h_maxfz, c_hyp, c_row, c_cnt,
+                                                                           c_row32, c_maxfz);
+  return vk_launch_status();
+}
+
+}  // extern "C"

@@ -1,0 +1,106 @@
+"""ctypes binding of ``vulcan/lib/libvulcan_b200.so`` (built from ``csrc/`` for sm_100a).
+
+Mirrors the reference's ``vulcan/gpu/_lib.py`` (``lib()``, ``ptr()``, ``stream()``, ``check()``; the reference
+signatures of ``_SIGS`` are kept name for name) and adds the B200 entry points of ``include/vulcan_b200.h``.
+There is no fallback: if the library is missing, ``lib()`` raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import sys
+
+import torch
+
+from .._native import GPU_SO, _load
+
+P = C.c_void_p
+I32, I64, F32, F64, U32 = C.c_int, C.c_int64, C.c_float, C.c_double, C.c_uint32
+
+
+class FragParams(C.Structure):
+    """vk_frag_params"""
+    _fields_ = [("mono", C.c_float * 26), ("stat", C.c_float * 26), ("var", C.c_float * 26),
+                ("nterm", C.c_float), ("tol_da", C.c_int)]
+
+
+class TIndex(C.Structure):
+    """vk_tindex"""
+    _fields_ = [("n_rows", C.c_int64), ("n_tiles", C.c_int64), ("n_postings", C.c_int64),
+                ("tile_shift", C.c_int32), ("row_bits", C.c_int32), ("mass_bits", C.c_int32),
+                ("cbin_bits", C.c_int32), ("fmin_bits", C.c_uint32), ("fmax_bits", C.c_uint32),
+                ("min_ion_index", C.c_int32), ("max_tile_postings", C.c_int32),
+                ("tile_off", P), ("cbin_off", P), ("postings", P)]
+
+
+# reference-compatible signatures (vulcan/gpu/_lib.py:22-35 of the reference)
+_SIGS = {
+    "vk_set_params": [P, P, P],
+    "vk_frag_count": [I64, P, P, P, P, P, I32, F32, F32, P, P],
+    "vk_frag_emit": [I64, P, P, P, P, P, I32, F32, F32, F64, I32, I64, P, P, P],
+    "vk_k1": [I32, P, P, P, P, P, P, P, P, P, P, I32, I32, I32, I32, F32, F32, F32, F64, I32, I64, P, P, P, P,
+              P, P, P],
+    "vk_k1_brute": [I64, P, P, P, P, P, P, P, P, P, P, P, I32, F32, F32, F32, F32, F64, P, P],
+    "vk_k2": [I32, P, P, P, P, P, P, P, P, P, P, P, P, F32, F32, P, P, P, P, P, P, P, P, I32, P],
+    "vk_set_nterm": [F32],
+    "vk_k2_shift": [I32, P, P, P, P, P, P, P, P, P, P, P, P, F32, F32, P, P, P, P, P, P, P, P, P, I32, P],
+    "vk_set_tol_da": [I32],
+}
+# B200 entry points
+_SIGS_B200 = {
+    "vk_tindex_layout": [I64, I32, F32, F32, I32, I32, P],
+    "vk_tindex_count": [P, P, P, P, P, P, P, P, P],
+    "vk_tindex_emit": [P, P, P, P, P, P, P, P, P, P],
+    "vk_scan_i64": [P, I64, P, P, P],
+    "vk_k0_count": [I32, P, P, F32, F32, I32, P, P],
+    "vk_k0_fill": [I32, P, P, P, F32, F32, I32, I32, P, P, P, P, P, I32, P],
+    "vk_hyp_count": [I32, P, P, P, I32, I32, I32, I32, P, P],
+    "vk_hyp_fill": [I32, P, P, P, I32, I32, I32, I32, F32, F32, I32, P, I64, P, P, P, P, P, P, P, P, P, P],
+    "vk_k1_plan_count": [P, I64, P, P, P, P, P],
+    "vk_k1_plan_fill": [P, I64, P, P, P, P, P, P],
+    "vk_k1_tiles": [P, P, F32, F32, P, P, P, P, P, P, P, P, P, P, P, P],
+    "vk_select_topk": [I32, P, P, P, P, P, P, I32, I32, I32, I32, P, P, P, P, P, P, P, P, P],
+    "vk_compact_cands": [I32, I32, P, P, P, P, P, P, P, P, P, P, P, P],
+    "vk_k2_spectra": [P, I32, P, P, P, P, P, P, P, P, P, P, P, F32, F32, P, P, P, P, P, P, P, P, P, P],
+    "vk_psm_rank": [I32, P, P, P, P, P, I32, I32, P, P, P, P, P, P],
+}
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    torch.cuda.init()
+    L = _load(GPU_SO, "CUDA kernel library")
+    for name, args in {**_SIGS, **_SIGS_B200}.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = C.c_int
+    L.vk_scan_tmp_bytes.argtypes = [I64]
+    L.vk_scan_tmp_bytes.restype = I64
+    _lib = L
+    return L
+
+
+def ptr(t: torch.Tensor | None):
+    if t is None:
+        return None
+    assert t.is_cuda and t.is_contiguous(), "kernels need contiguous CUDA tensors"
+    return t.data_ptr()
+
+
+def stream():
+    return torch.cuda.current_stream().cuda_stream
+
+
+_TRACE = os.environ.get("VK_TRACE") == "1"
+
+
+def check(code: int, what: str):
+    if code != 0:
+        raise RuntimeError(f"{what}: CUDA error {code}" if code > 0 else f"{what}: rejected argument ({code})")
+    if _TRACE:   # debugging aid: finish every launch and report the stage before the next one
+        torch.cuda.synchronize()
+        print(f"[vk] {what} ok", file=sys.stderr, flush=True)

@@ -1,0 +1,707 @@
+"""GPU closed search on B200: K0 peak view -> hypotheses -> K1 (tiled fragment index) -> top-K + pair closure
+-> K2 exact rescoring -> PSM ranking.  Mirror of the reference's ``vulcan/gpu/engine.py``: the same public names
+(``SAGE_MONO``, ``Stats``, ``GpuIndex``, ``k0_preprocess``, ``work_items``, ``Timer``, ``run_k1``, ``select_topk``,
+``run_k2``, ``lnfact``, ``psm_table``, ``search``, ``window_candidates``, ``k1_brute``, ``search_exhaustive``) with
+the same arguments and results.
+
+Where the work runs: every stage of ``search`` is a kernel of ``libvulcan_b200.so`` (``include/vulcan_b200.h``);
+torch only allocates device memory and hands pointers across.  Scoring semantics are the reference's (Sage f32
+arithmetic; candidate order and tie rules of ``engine.py:284-312`` and ``:366-392``).  Nothing reads labels.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import resource
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+import pyarrow as pa
+import torch
+
+from . import _lib as K
+from .host import NEUTRON, PROTON, SearchParams, Spectra, make_hypotheses, max_fragment_z, pre_hypotheses  # noqa: F401
+
+SAGE_MONO = np.array([71.03711, 0.0, 103.00919, 115.02694, 129.04259, 147.0684, 57.02146, 137.05891, 113.08406,
+                      0.0, 128.09496, 113.08406, 131.0405, 114.04293, 237.14774, 97.05276, 128.05858, 156.1011,
+                      87.03203, 101.04768, 150.95363, 99.06841, 186.07932, 0.0, 163.06332, 0.0], np.float32)
+
+ROW_BITS = 28   # candidate rows < 2^28 (top-K key packing of the reference, engine.py:35)
+CBIN_BITS = 8   # coarse m/z bins per index tile
+
+
+@dataclass
+class Slice:
+    """One slice of the reference-layout (chunk, log bin) CSR, for the reference-compatible ``vk_k1``."""
+    chunk0: int
+    chunk1: int
+    offsets: torch.Tensor
+    entries: torch.Tensor
+
+
+@dataclass
+class Stats:
+    h2d_bytes: int = 0
+    d2h_bytes: int = 0
+    gpu_ms: dict = field(default_factory=dict)
+    wall_s: dict = field(default_factory=dict)
+    counts: dict = field(default_factory=dict)
+
+
+def frag_params(static_mods: dict, var_mods: dict, fragment_unit: str = "ppm") -> K.FragParams:
+    fp = K.FragParams()
+    stat = np.zeros(26, np.float32)
+    var = np.zeros(26, np.float32)
+    nterm = 0.0
+    for r, m in static_mods.items():
+        stat[ord(r) - 65] = np.float32(m)
+    for r, m in var_mods.items():
+        if r == "^":
+            nterm = float(np.float32(m))
+            continue
+        var[ord(r) - 65] = np.float32(m)
+    for i in range(26):
+        fp.mono[i] = float(SAGE_MONO[i])
+        fp.stat[i] = float(stat[i])
+        fp.var[i] = float(var[i])
+    fp.nterm = nterm
+    if fragment_unit not in ("ppm", "da"):
+        raise ValueError("fragment_unit must be 'ppm' or 'da'")
+    fp.tol_da = int(fragment_unit == "da")
+    return fp
+
+
+def _scan(x: torch.Tensor) -> torch.Tensor:
+    """Exclusive scan (n+1 entries) of an int64 device vector, on the device."""
+    L = K.lib()
+    n = x.numel()
+    out = torch.empty(n + 1, dtype=torch.int64, device=x.device)
+    tmp = torch.empty((L.vk_scan_tmp_bytes(n) + 7) // 8, dtype=torch.int64, device=x.device)
+    K.check(L.vk_scan_i64(K.ptr(x), n, K.ptr(out), K.ptr(tmp), K.stream()), "scan")
+    return out
+
+
+class GpuIndex:
+    """Device-resident peptidoform table + tiled fragment index.
+
+    Tiles of ``params.tile_rows`` mass-sorted rows; postings are u32 (f32 fragment bits - f32 bits of fmin) <<
+    row_bits | local row, sorted per tile, with a coarse-bin CSR per tile (``include/vulcan_b200.h``).  The
+    reference-layout CSR slices (``slices``) used by the reference-compatible ``vk_k1`` are built on first use.
+    """
+
+    def __init__(self, l1, params: SearchParams, static_mods: dict, var_mods: dict, device="cuda"):
+        t0 = time.perf_counter()
+        self.p = params
+        self.dev = torch.device(device)
+        L = K.lib()
+        self.static_mods, self.var_mods = dict(static_mods), dict(var_mods)
+        self.fp = frag_params(static_mods, var_mods, params.fragment_unit)
+        # process-wide constants of the reference-compatible entry points (as the reference sets them)
+        stat = np.array(self.fp.stat[:], np.float32)
+        var = np.array(self.fp.var[:], np.float32)
+        with torch.cuda.device(self.dev):
+            K.check(L.vk_set_params(SAGE_MONO.ctypes.data, stat.ctypes.data, var.ctypes.data), "set_params")
+            K.check(L.vk_set_nterm(self.fp.nterm), "set_nterm")
+            K.check(L.vk_set_tol_da(self.fp.tol_da), "set_tol_da")
+        self.n = len(l1)
+        d = self.dev
+        self.h2d = 0
+
+        def up(a):
+            t = torch.from_numpy(np.array(a, copy=True)).to(d)
+            self.h2d += t.numel() * t.element_size()
+            return t
+        self.mass32_np = l1.mass32
+        self.seq_off = up(l1.seq_off.astype(np.int64))
+        self.length = up(l1.length.astype(np.uint8))
+        self.mask = up(l1.mask.view(np.int64))
+        self.mass32 = up(l1.mass32.astype(np.float32))
+        self.residues = up(l1.residues.astype(np.uint8))
+        self.partner = up(l1.partner.astype(np.int64))
+        if self.n >= 2 ** ROW_BITS:
+            raise ValueError("index rows must be < 2^28")
+        # reference layout constants (used by the compatible entry points)
+        self.inv_logw = 1.0 / math.log1p(params.bin_ppm * 1e-6)
+        self.n_bins = int(math.floor(math.log(params.fragment_max_mz / params.fragment_min_mz) * self.inv_logw)) + 2
+        self.n_chunks = (self.n + params.chunk_size - 1) // params.chunk_size
+        self._slices = None
+        with torch.cuda.device(d):
+            self._build_tiles()
+        torch.cuda.synchronize(d)
+        self.build_s = time.perf_counter() - t0
+        self.device_bytes = sum(t.numel() * t.element_size() for t in
+                                [self.seq_off, self.length, self.mask, self.mass32, self.residues, self.partner,
+                                 self.tile_off, self.cbin_off, self.postings])
+
+    def table_ptrs(self):
+        return (K.ptr(self.seq_off), K.ptr(self.length), K.ptr(self.mask), K.ptr(self.mass32), K.ptr(self.residues))
+
+    def _build_tiles(self):
+        L = K.lib()
+        p = self.p
+        ix = K.TIndex()
+        K.check(L.vk_tindex_layout(self.n, p.tile_rows, p.fragment_min_mz, p.fragment_max_mz, p.min_ion_index,
+                                   CBIN_BITS, C.byref(ix)), "tindex_layout")
+        d = self.dev
+        nt = ix.n_tiles
+        tile_count = torch.empty(max(nt, 1), dtype=torch.int64, device=d)
+        K.check(L.vk_tindex_count(C.byref(ix), C.byref(self.fp), *self.table_ptrs(), K.ptr(tile_count), K.stream()),
+                "tindex_count")
+        self.tile_off = _scan(tile_count[:nt])
+        stats = torch.stack([tile_count[:nt].max() if nt else torch.zeros((), dtype=torch.int64, device=d),
+                             self.tile_off[-1]]).cpu().tolist()
+        ix.max_tile_postings = int(stats[0])
+        ix.n_postings = int(stats[1])
+        stride = ((1 << CBIN_BITS) + 1 + 7) & ~7
+        self.postings = torch.empty(max(ix.n_postings, 4), dtype=torch.int32, device=d)
+        self.cbin_off = torch.empty(max(nt * stride, 8), dtype=torch.int16, device=d)
+        ix.tile_off = K.ptr(self.tile_off)
+        K.check(L.vk_tindex_emit(C.byref(ix), C.byref(self.fp), *self.table_ptrs(), K.ptr(self.postings),
+                                 K.ptr(self.cbin_off), K.stream()), "tindex_emit")
+        ix.cbin_off = K.ptr(self.cbin_off)
+        ix.postings = K.ptr(self.postings)
+        self.tix = ix
+        self.n_postings = ix.n_postings
+
+    # ------------------------------------------------------------------ reference-layout CSR (compatible vk_k1)
+    @property
+    def slices(self) -> list[Slice]:
+        if self._slices is None:
+            with torch.cuda.device(self.dev):
+                self._slices = self._build_compat_slices()
+        return self._slices
+
+    def _build_compat_slices(self):
+        """The reference's (chunk, log-ppm bin) CSR (engine.py:101-148), built with the compatible kernels."""
+        L = K.lib()
+        p, d = self.p, self.dev
+        Cs = p.chunk_size
+        cnt = torch.empty(self.n, dtype=torch.int32, device=d)
+        K.check(L.vk_frag_count(self.n, *self.table_ptrs(), p.min_ion_index, p.fragment_min_mz, p.fragment_max_mz,
+                                K.ptr(cnt), K.stream()), "frag_count")
+        per_chunk = torch.zeros(self.n_chunks, dtype=torch.int64, device=d)
+        per_chunk.index_add_(0, torch.arange(self.n, device=d) // Cs, cnt.to(torch.int64))
+        pcs = per_chunk.cpu().numpy()
+        bounds, acc, c0 = [], 0, 0
+        for c, v in enumerate(pcs):
+            if acc + v > p.max_slice_entries and c > c0:
+                bounds.append((c0, c))
+                c0, acc = c, 0
+            acc += int(v)
+        bounds.append((c0, self.n_chunks))
+        out = []
+        for c0, c1 in bounds:
+            r0, r1 = c0 * Cs, min(c1 * Cs, self.n)
+            off = torch.zeros(r1 - r0 + 1, dtype=torch.int64, device=d)
+            torch.cumsum(cnt[r0:r1].to(torch.int64), 0, out=off[1:])
+            keys = torch.empty(int(off[-1]), dtype=torch.int64, device=d)
+            K.check(L.vk_frag_emit(r1 - r0, K.ptr(self.seq_off[r0:r1]), K.ptr(self.length[r0:r1]),
+                                   K.ptr(self.mask[r0:r1]), K.ptr(self.mass32[r0:r1]), K.ptr(self.residues),
+                                   p.min_ion_index, p.fragment_min_mz, p.fragment_max_mz, self.inv_logw, Cs, r0,
+                                   K.ptr(off), K.ptr(keys), K.stream()), "frag_emit")
+            keys = torch.sort(keys).values
+            entries = (keys & 0xFFFFFFFF).to(torch.int64)
+            entries = torch.where(entries >= 2 ** 31, entries - 2 ** 32, entries).to(torch.int32)
+            lin = ((keys >> 50) - c0) * self.n_bins + ((keys >> 32) & 0x3FFFF)
+            nb = (c1 - c0) * self.n_bins
+            offs = torch.zeros(nb + 1, dtype=torch.int64, device=d)
+            torch.cumsum(torch.bincount(lin, minlength=nb), 0, out=offs[1:])
+            offs = torch.where(offs >= 2 ** 31, offs - 2 ** 32, offs).to(torch.int32)
+            out.append(Slice(c0, c1, offs, entries))
+        return out
+
+
+# ------------------------------------------------------------------------------------------------ spectra
+class DeviceRun:
+    """One run's raw spectra on the device (the inputs of K0 and of the hypotheses)."""
+
+    def __init__(self, sp: Spectra, dev, stats: Stats | None = None, pinned: bool = True):
+        def up(a, dt):
+            a = np.ascontiguousarray(a, dtype=dt)
+            t = torch.from_numpy(a)
+            if pinned and dev.type == "cuda":
+                t = t.pin_memory()
+            g = t.to(dev, non_blocking=True)
+            if stats is not None:
+                stats.h2d_bytes += g.numel() * g.element_size()
+            return g
+        self.n = len(sp)
+        self.mz = up(sp.mz, np.float32)
+        self.intensity = up(sp.intensity, np.float32)
+        self.offsets = up(sp.offsets, np.int64)
+        self.precursor_mz = up(sp.precursor_mz, np.float64)
+        self.charge = up(sp.charge, np.int8)
+        lens = np.diff(np.asarray(sp.offsets, np.int64))
+        self.max_raw = int(lens.max()) if len(lens) else 0
+        self.n_raw = int(np.asarray(sp.offsets)[-1]) if len(sp.offsets) else 0
+        self.charge_np = np.asarray(sp.charge)
+
+
+def _k0_device(run: DeviceRun, p: SearchParams, dev):
+    L = K.lib()
+    n = run.n
+    kept = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
+    K.check(L.vk_k0_count(n, K.ptr(run.offsets), K.ptr(run.mz), p.fragment_min_mz, p.fragment_max_mz, p.max_peaks,
+                          K.ptr(kept), K.stream()), "k0_count")
+    off = _scan(kept[:n])
+    cap = max(run.n_raw, 1)
+    mass = torch.empty(cap, dtype=torch.float32, device=dev)
+    inten = torch.empty(cap, dtype=torch.float32, device=dev)
+    tic = torch.empty(max(n, 1), dtype=torch.float32, device=dev)
+    valid = torch.empty(max(n, 1), dtype=torch.uint8, device=dev)
+    K.check(L.vk_k0_fill(n, K.ptr(run.offsets), K.ptr(run.mz), K.ptr(run.intensity), p.fragment_min_mz,
+                         p.fragment_max_mz, p.max_peaks, p.min_peaks, K.ptr(off), K.ptr(mass), K.ptr(inten),
+                         K.ptr(tic), K.ptr(valid), run.max_raw, K.stream()), "k0_fill")
+    return {"off": off, "mass": mass, "int": inten, "tic": tic[:n], "valid_d": valid[:n]}
+
+
+def k0_preprocess(sp: Spectra, p: SearchParams, dev, stats: Stats):
+    """K0 on the GPU (reference engine.py:171-210): device peaks + host validity mask."""
+    if p.peak_mode != "global":
+        raise NotImplementedError("only the global peak view (Sage) is implemented")
+    run = DeviceRun(sp, torch.device(dev), stats)
+    pk = _k0_device(run, p, torch.device(dev))
+    n_kept = int(pk["off"][-1])
+    pk["mass"] = pk["mass"][:n_kept]
+    pk["int"] = pk["int"][:n_kept]
+    pk["valid"] = pk["valid_d"].bool().cpu().numpy()
+    return pk
+
+
+def _hyp_device(run: DeviceRun, peaks, gi: GpuIndex, p: SearchParams):
+    """Hypotheses on the device; capacity = the host-known upper bound (charge known or the charge range)."""
+    L = K.lib()
+    dev = gi.dev
+    n = run.n
+    z0, z1 = p.precursor_charge
+    i0, i1 = p.isotope_errors
+    n_iso = i1 - i0 + 1
+    n_max = int(np.where(run.charge_np > 0, 1, z1 - z0 + 1).sum()) * n_iso
+    cnt = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
+    K.check(L.vk_hyp_count(n, K.ptr(peaks["valid_d"]), K.ptr(run.precursor_mz), K.ptr(run.charge), z0, z1, i0, i1,
+                           K.ptr(cnt), K.stream()), "hyp_count")
+    off = _scan(cnt[:n])
+    cap = max(n_max, 1)
+    h = {"spec": torch.zeros(cap, dtype=torch.int32, device=dev),
+         "z": torch.zeros(cap, dtype=torch.int8, device=dev),
+         "iso": torch.zeros(cap, dtype=torch.int8, device=dev),
+         "pm": torch.zeros(cap, dtype=torch.float32, device=dev),
+         "M": torch.zeros(cap, dtype=torch.float32, device=dev),
+         "lo": torch.zeros(cap, dtype=torch.int64, device=dev),
+         "hi": torch.zeros(cap, dtype=torch.int64, device=dev),
+         "maxfz": torch.zeros(cap, dtype=torch.int8, device=dev)}
+    mfc = p.max_fragment_charge or 0
+    K.check(L.vk_hyp_fill(n, K.ptr(peaks["valid_d"]), K.ptr(run.precursor_mz), K.ptr(run.charge), z0, z1, i0, i1,
+                          float(p.precursor_ppm[0]), float(p.precursor_ppm[1]), int(mfc), K.ptr(gi.mass32), gi.n,
+                          K.ptr(off), K.ptr(h["spec"]), K.ptr(h["z"]), K.ptr(h["iso"]), K.ptr(h["pm"]), K.ptr(h["M"]),
+                          K.ptr(h["lo"]), K.ptr(h["hi"]), K.ptr(h["maxfz"]), K.stream()), "hyp_fill")
+    h["spec_off"] = off
+    h["n_max"] = n_max
+    return h
+
+
+def work_items(hyp, p: SearchParams):
+    """Reference work items (engine.py:213-229) for the compatible ``vk_k1``: tile-aligned pieces of each
+    window that never cross a chunk boundary."""
+    lo, hi = np.asarray(hyp["lo"]), np.asarray(hyp["hi"])
+    T = p.tile
+    nz = hi > lo
+    h = np.nonzero(nz)[0]
+    t0 = lo[h] // T
+    t1 = (hi[h] - 1) // T
+    nt = (t1 - t0 + 1)
+    hh = np.repeat(h, nt)
+    tt = np.repeat(t0, nt) + (np.arange(nt.sum()) - np.repeat(np.cumsum(nt) - nt, nt))
+    a = np.maximum(lo[hh], tt * T)
+    b = np.minimum(hi[hh], (tt + 1) * T)
+    chunk = (tt * T) // p.chunk_size
+    base = chunk * p.chunk_size
+    return {"hyp": hh.astype(np.int32), "chunk": chunk.astype(np.int32), "lo": (a - base).astype(np.int32),
+            "hi": (b - base).astype(np.int32), "n_window": int((hi - lo)[nz].sum())}
+
+
+class Timer:
+    """CUDA-event + wall time of a phase, recorded on the current stream."""
+
+    def __init__(self, stats: Stats, name: str):
+        self.stats, self.name = stats, name
+
+    def __enter__(self):
+        self.e0 = torch.cuda.Event(enable_timing=True)
+        self.e1 = torch.cuda.Event(enable_timing=True)
+        self.e0.record()
+        self.t0 = time.perf_counter()
+        return self
+
+    def __exit__(self, *a):
+        self.e1.record()
+        self.e1.synchronize()
+        self.stats.gpu_ms[self.name] = self.stats.gpu_ms.get(self.name, 0.0) + self.e0.elapsed_time(self.e1)
+        self.stats.wall_s[self.name] = self.stats.wall_s.get(self.name, 0.0) + time.perf_counter() - self.t0
+
+
+def _as_dev(hyp, dev):
+    out = {}
+    for k in ("spec", "z", "iso", "pm", "M", "lo", "hi", "maxfz"):
+        v = hyp[k]
+        out[k] = v if isinstance(v, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(v)).to(dev)
+    return out
+
+
+def _k1_dense(gi: GpuIndex, dh, peaks, p: SearchParams, n_hyp: int, stats: Stats | None = None):
+    """Tiled K1: dense counts of every window row.  Returns (win_off, cnt)."""
+    L = K.lib()
+    dev = gi.dev
+    ix = gi.tix
+    nt = ix.n_tiles
+    tile_items = torch.empty(max(nt, 1), dtype=torch.int64, device=dev)
+    win_len = torch.empty(max(n_hyp, 1), dtype=torch.int64, device=dev)
+    K.check(L.vk_k1_plan_count(C.byref(ix), n_hyp, K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(tile_items),
+                               K.ptr(win_len), K.stream()), "k1_plan_count")
+    item_off = _scan(tile_items[:nt])
+    win_off = _scan(win_len[:n_hyp])
+    n_items, n_win = torch.stack([item_off[-1], win_off[-1]]).cpu().tolist()
+    cursor = torch.empty(max(nt, 1), dtype=torch.int64, device=dev)
+    item_hyp = torch.empty(max(n_items, 1), dtype=torch.int32, device=dev)
+    K.check(L.vk_k1_plan_fill(C.byref(ix), n_hyp, K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(item_off),
+                              K.ptr(cursor), K.ptr(item_hyp), K.stream()), "k1_plan_fill")
+    cnt = torch.empty(max(n_win, 1), dtype=torch.int32, device=dev)
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
+    K.check(L.vk_k1_tiles(C.byref(ix), C.byref(gi.fp), float(p.fragment_ppm[0]), float(p.fragment_ppm[1]),
+                          K.ptr(item_off), K.ptr(item_hyp), K.ptr(dh["spec"]), K.ptr(dh["maxfz"]), K.ptr(dh["lo"]),
+                          K.ptr(dh["hi"]), K.ptr(win_off), K.ptr(peaks["off"]), K.ptr(peaks["mass"]), K.ptr(cnt),
+                          K.ptr(status), K.stream()), "k1_tiles")
+    if stats is not None:
+        stats.counts["k1_work_items"] = stats.counts.get("k1_work_items", 0) + n_items
+        stats.counts["k1_window_candidates"] = stats.counts.get("k1_window_candidates", 0) + n_win
+    return win_off, cnt[:n_win], status
+
+
+def run_k1(gi: GpuIndex, hyp, peaks, p: SearchParams, stats: Stats):
+    """K1 (reference engine.py:250-281): returns (o_h, o_r, o_c, scored, matched, d_spec, d_maxfz) with the appended
+    (hyp, row, count) entries sorted by (hyp, row)."""
+    dev = gi.dev
+    dh = _as_dev(hyp, dev)
+    n_h = len(hyp["spec"])
+    win_off, cnt, status = _k1_dense(gi, dh, peaks, p, n_h, stats)
+    if int(status.item()):
+        raise RuntimeError("k1_tiles: a tile copy did not complete")
+    win_len = (dh["hi"] - dh["lo"]).clamp(min=0)
+    hh = torch.repeat_interleave(torch.arange(n_h, device=dev), win_len)
+    rr = dh["lo"][hh] + (torch.arange(len(hh), device=dev) - win_off[:-1][hh])
+    keep = cnt >= p.k1_threshold
+    scored = torch.zeros(n_h, dtype=torch.int32, device=dev).index_add_(0, hh, (cnt > 0).to(torch.int32))
+    matched = torch.zeros(n_h, dtype=torch.int64, device=dev).index_add_(0, hh, cnt.to(torch.int64))
+    n = int(keep.sum())
+    stats.counts["k1_appended"] = stats.counts.get("k1_appended", 0) + n
+    return (hh[keep].to(torch.int32), rr[keep].to(torch.int32), cnt[keep], scored, matched, dh["spec"], dh["maxfz"])
+
+
+def select_topk(o_h, o_r, o_c, d_spec, gi: GpuIndex, p: SearchParams):
+    """Top-K per spectrum then pair closure from appended lists (reference engine.py:284-312), tie (count, row)
+    broken by the lower hypothesis.  ``search`` runs the same selection in the ``vk_select_topk`` kernel."""
+    dev = gi.dev
+    spec = d_spec[o_h.long()].long()
+    key = (spec << 43) | ((32767 - o_c.long().clamp(max=32767)) << ROW_BITS) | ((2 ** ROW_BITS - 1) - o_r.long())
+    o = torch.argsort(o_h.long(), stable=True)
+    o = o[torch.argsort(key[o], stable=True)]
+    ss = spec[o]
+    first = torch.searchsorted(ss, ss, side="left")
+    rank = torch.arange(len(ss), device=dev) - first
+    sel = o[rank < p.topk]
+    h, r, c = o_h[sel].long(), o_r[sel].long(), o_c[sel].long()
+    if p.pair_closure:
+        pr = gi.partner[r]
+        h = torch.cat([h, h])
+        r = torch.cat([r, pr])
+        c = torch.cat([c, torch.full_like(c, -1)])
+    sp = d_spec[h].long()
+    k = (sp << ROW_BITS) | r
+    uk, inv = torch.unique(k, sorted=True, return_inverse=True)
+    hh = torch.full((len(uk),), 2 ** 62, dtype=torch.int64, device=dev).scatter_reduce_(0, inv, h, reduce="amin")
+    cc = torch.full((len(uk),), -1, dtype=torch.int64, device=dev).scatter_reduce_(0, inv, c, reduce="amax")
+    rr = uk & (2 ** ROW_BITS - 1)
+    return hh, rr, cc
+
+
+def _k2_outputs(n, dev):
+    out = {"hyperscore": torch.empty(n, dtype=torch.float64, device=dev)}
+    for k in ("summed_b", "summed_y", "ppm"):
+        out[k] = torch.empty(n, dtype=torch.float32, device=dev)
+    for k in ("matched_b", "matched_y", "longest_b", "longest_y"):
+        out[k] = torch.empty(n, dtype=torch.int16, device=dev)
+    return out
+
+
+def _k2_ptrs(out):
+    return [K.ptr(out[k]) for k in ("hyperscore", "summed_b", "summed_y", "ppm", "matched_b", "matched_y",
+                                    "longest_b", "longest_y")]
+
+
+def run_k2(gi: GpuIndex, h, r, d_spec, d_maxfz, peaks, p: SearchParams, shift: torch.Tensor | None = None):
+    """K2 over candidates sorted by spectrum (reference engine.py:315-351), through the reference-compatible
+    ``vk_k2`` / ``vk_k2_shift`` entry points.  Returns a dict of device tensors, one row per candidate."""
+    L = K.lib()
+    dev = gi.dev
+    spec = d_spec[h].long()
+    us, cnts = torch.unique_consecutive(spec, return_counts=True)
+    off = torch.zeros(len(us) + 1, dtype=torch.int64, device=dev)
+    torch.cumsum(cnts, 0, out=off[1:])
+    n = len(r)
+    row = r.to(torch.int32).contiguous()
+    mfz = d_maxfz[h].contiguous()
+    out = _k2_outputs(n, dev)
+    sid = us.to(torch.int32).contiguous()
+    args = [len(us), K.ptr(off), K.ptr(row), K.ptr(mfz), K.ptr(sid), K.ptr(peaks["off"]), K.ptr(peaks["mass"]),
+            K.ptr(peaks["int"]), *gi.table_ptrs(), p.fragment_ppm[0], p.fragment_ppm[1]]
+    if shift is None:
+        K.check(L.vk_k2(*args, *_k2_ptrs(out), p.k2_threads, K.stream()), "k2")
+    else:
+        sh = shift.to(torch.float32).contiguous()
+        K.check(L.vk_k2_shift(*args, K.ptr(sh), *_k2_ptrs(out), p.k2_threads, K.stream()), "k2_shift")
+    out["spec"] = spec
+    return out
+
+
+def lnfact(n):
+    n = np.asarray(n, np.float64)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        v = n * np.log(n) - n + 0.5 * np.log(n) + 0.5 * np.log(2 * np.pi * n)
+    return np.where(n == 0, 1.0, v)
+
+
+def _rank_device(n_spec, cand_off, rows, k2, p: SearchParams, report: int, dev):
+    L = K.lib()
+    slots = max(n_spec * report, 1)
+    psm_cand = torch.empty(slots, dtype=torch.int64, device=dev)
+    psm_rank = torch.empty(slots, dtype=torch.int32, device=dev)
+    dnext = torch.empty(slots, dtype=torch.float64, device=dev)
+    dbest = torch.empty(slots, dtype=torch.float64, device=dev)
+    n_psm = torch.empty(max(n_spec, 1), dtype=torch.int32, device=dev)
+    K.check(L.vk_psm_rank(n_spec, K.ptr(cand_off), K.ptr(rows), K.ptr(k2["hyperscore"]), K.ptr(k2["matched_b"]),
+                          K.ptr(k2["matched_y"]), p.min_matched_peaks, report, K.ptr(psm_cand), K.ptr(psm_rank),
+                          K.ptr(dnext), K.ptr(dbest), K.ptr(n_psm), K.stream()), "psm_rank")
+    return psm_cand[:n_spec * report], psm_rank[:n_spec * report], dnext[:n_spec * report], dbest[:n_spec * report]
+
+
+def _psm_columns(sp: Spectra, l1, rec: dict, p: SearchParams) -> pa.Table:
+    """Host part of the PSM table (reference engine.py:396-432) from the gathered per-PSM records."""
+    s = rec["spec"]
+    rows = rec["row"]
+    mbk, myk = rec["matched_b"].astype(np.int64), rec["matched_y"].astype(np.int64)
+    kk = mbk + myk
+    sc, mt = rec["spec_scored"], rec["spec_matched"]
+    with np.errstate(divide="ignore", invalid="ignore", over="ignore"):
+        lam = mt / sc
+        pois = lam ** kk * np.exp(-lam) / np.exp(lnfact(kk))
+        pois = np.where(np.isinf(pois), 1e-325, pois)
+        log_pois = np.log10(pois)
+    z = rec["z"].astype(np.int64)
+    iso = rec["iso"].astype(np.int64)
+    pm = rec["pm"]
+    calc = l1.mass32[rows]
+    ie = (iso.astype(np.float32) * NEUTRON).astype(np.float32)
+    dm = (np.abs(pm - calc - ie) * np.float32(2e6) / (pm - ie + calc)).astype(np.float32)
+    plen = l1.length[rows].astype(np.int64)
+    sbs = (rec["summed_b"] + rec["summed_y"]).astype(np.float32)
+    cols = {
+        "run": pa.array([sp.run] * len(s)),
+        "spec_idx": s.astype(np.int64), "scan": sp.scan[s], "rt": sp.rt[s],
+        "rank": rec["rank"].astype(np.int32), "pf_row": rows.astype(np.int64), "pf_id": l1.pf_id[rows],
+        "charge": z.astype(np.int8), "isotope_error": iso.astype(np.int8),
+        "expmass": pm.astype(np.float32), "calcmass": calc.astype(np.float32), "delta_mass_ppm": dm,
+        "hyperscore": rec["hyperscore"], "delta_next": rec["dnext"], "delta_best": rec["dbest"],
+        "matched_b": mbk.astype(np.int16), "matched_y": myk.astype(np.int16), "matched_peaks": kk.astype(np.int16),
+        "summed_intensity": sbs,
+        "matched_intensity_pct": (100.0 * sbs / rec["tic"]).astype(np.float32),
+        "average_ppm": rec["ppm"], "longest_b": rec["longest_b"], "longest_y": rec["longest_y"],
+        "longest_y_pct": (rec["longest_y"] / plen).astype(np.float32),
+        "peptide_len": plen.astype(np.int16), "missed_cleavages": l1.missed[rows], "n_var": l1.n_var[rows],
+        "k1_count": rec["k1"].astype(np.int32), "scored_candidates": sc.astype(np.int32), "poisson": log_pois,
+    }
+    return pa.table(cols)
+
+
+def _gather_psms(psm_cand, psm_rank, dnext, dbest, c_hyp, c_row, c_cnt, k2, dh, spec_scored, spec_matched, tic,
+                 report, stats: Stats | None = None):
+    """Device gather of the reported PSMs, one D2H copy per column."""
+    ok = psm_cand >= 0
+    sel = psm_cand[ok]
+    slot = torch.nonzero(ok).squeeze(1)
+    s = slot // report
+    hh = c_hyp[sel].long()
+    cols = {"spec": s, "rank": psm_rank[ok], "dnext": dnext[ok], "dbest": dbest[ok], "row": c_row[sel],
+            "hyp": hh, "k1": c_cnt[sel], "z": dh["z"][hh], "iso": dh["iso"][hh], "pm": dh["pm"][hh],
+            "spec_scored": spec_scored[s], "spec_matched": spec_matched[s], "tic": tic[s]}
+    for k in ("hyperscore", "summed_b", "summed_y", "ppm", "matched_b", "matched_y", "longest_b", "longest_y"):
+        cols[k] = k2[k][sel]
+    out = {}
+    for k, v in cols.items():
+        out[k] = v.cpu().numpy()
+        if stats is not None:
+            stats.d2h_bytes += v.numel() * v.element_size()
+    return out
+
+
+def psm_table(sp: Spectra, gi: GpuIndex, l1, hyp, h, r, k1c, k2, scored, matched, peaks, p: SearchParams,
+              report: int | None = None) -> pa.Table:
+    """Rank candidates per spectrum by hyperscore (label-blind), Sage-style features, top ``report``
+    (reference engine.py:361-432).  h, r, k1c: candidates sorted by (spectrum, row)."""
+    report = p.report_psms if report is None else report
+    dev = gi.dev
+    dh = _as_dev(hyp, dev)
+    n_spec = len(sp)
+    spec = dh["spec"][h].long()
+    cand_off = torch.zeros(n_spec + 1, dtype=torch.int64, device=dev)
+    torch.cumsum(torch.bincount(spec, minlength=n_spec), 0, out=cand_off[1:])
+    rows = r.long().contiguous()
+    psm = _rank_device(n_spec, cand_off, rows, k2, p, report, dev)
+    hs_spec = dh["spec"].long()
+    sc = torch.zeros(n_spec, dtype=torch.int64, device=dev).index_add_(0, hs_spec, scored.long())
+    mt = torch.zeros(n_spec, dtype=torch.int64, device=dev).index_add_(0, hs_spec, matched.long())
+    rec = _gather_psms(*psm, h.long(), rows, k1c.long(), k2, dh, sc, mt, peaks["tic"], report)
+    return _psm_columns(sp, l1, rec, p)
+
+
+def _search_device(run: DeviceRun, gi: GpuIndex, p: SearchParams, report: int, st: Stats, timers: bool = False):
+    """The whole hot path on the device for one run whose raw spectra are already resident.  Returns the device
+    PSM slots and the intermediates."""
+    L = K.lib()
+    dev = gi.dev
+    n = run.n
+
+    def phase(name):
+        return Timer(st, name) if timers else _NoTimer()
+    with phase("k0"):
+        peaks = _k0_device(run, p, dev)
+    with phase("hyp"):
+        dh = _hyp_device(run, peaks, gi, p)
+    n_h = dh["n_max"]
+    with phase("k1"):
+        win_off, cnt, status = _k1_dense(gi, dh, peaks, p, n_h, st)
+    cap = (2 if p.pair_closure else 1) * p.topk
+    with phase("topk"):
+        s_hyp = torch.empty(max(n * cap, 1), dtype=torch.int64, device=dev)
+        s_row = torch.empty_like(s_hyp)
+        s_cnt = torch.empty_like(s_hyp)
+        n_cand = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
+        hyp_scored = torch.empty(max(n_h, 1), dtype=torch.int32, device=dev)
+        hyp_matched = torch.empty(max(n_h, 1), dtype=torch.int64, device=dev)
+        spec_scored = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
+        spec_matched = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
+        K.check(L.vk_select_topk(n, K.ptr(dh["spec_off"]), K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(win_off),
+                                 K.ptr(cnt), K.ptr(gi.partner), p.k1_threshold, p.topk, int(p.pair_closure), cap,
+                                 K.ptr(s_hyp), K.ptr(s_row), K.ptr(s_cnt), K.ptr(n_cand), K.ptr(hyp_scored),
+                                 K.ptr(hyp_matched), K.ptr(spec_scored), K.ptr(spec_matched), K.stream()),
+                "select_topk")
+        cand_off = _scan(n_cand[:n])
+        c_hyp = torch.empty_like(s_hyp)
+        c_row = torch.empty_like(s_hyp)
+        c_cnt = torch.empty_like(s_hyp)
+        c_row32 = torch.empty(max(n * cap, 1), dtype=torch.int32, device=dev)
+        c_maxfz = torch.empty(max(n * cap, 1), dtype=torch.int8, device=dev)
+        K.check(L.vk_compact_cands(n, cap, K.ptr(n_cand), K.ptr(cand_off), K.ptr(s_hyp), K.ptr(s_row), K.ptr(s_cnt),
+                                   K.ptr(dh["maxfz"]), K.ptr(c_hyp), K.ptr(c_row), K.ptr(c_cnt), K.ptr(c_row32),
+                                   K.ptr(c_maxfz), K.stream()), "compact_cands")
+    with phase("k2"):
+        k2 = _k2_outputs(max(n * cap, 1), dev)
+        K.check(L.vk_k2_spectra(C.byref(gi.fp), n, K.ptr(cand_off), K.ptr(c_row32), K.ptr(c_maxfz),
+                                K.ptr(peaks["off"]), K.ptr(peaks["mass"]), K.ptr(peaks["int"]), *gi.table_ptrs(),
+                                float(p.fragment_ppm[0]), float(p.fragment_ppm[1]), None, *_k2_ptrs(k2), K.stream()),
+                "k2_spectra")
+    with phase("rank"):
+        psm = _rank_device(n, cand_off, c_row, k2, p, report, dev)
+    return {"peaks": peaks, "dh": dh, "win_off": win_off, "cnt": cnt, "status": status, "cand_off": cand_off,
+            "c_hyp": c_hyp, "c_row": c_row, "c_cnt": c_cnt, "k2": k2, "psm": psm, "hyp_scored": hyp_scored,
+            "hyp_matched": hyp_matched, "spec_scored": spec_scored, "spec_matched": spec_matched}
+
+
+class _NoTimer:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        return False
+
+
+def search(sp: Spectra, gi: GpuIndex, l1, p: SearchParams, report: int | None = None, pre_hyp=None,
+           timers: bool = False):
+    """Full closed search of one run (reference engine.py:435-464).  Returns (PSM table, stats, debug).
+    ``pre_hyp`` is accepted for signature compatibility; hypotheses are always computed on the device (they equal
+    ``make_hypotheses`` on K0's validity mask)."""
+    report = p.report_psms if report is None else report
+    st = Stats()
+    ru0 = resource.getrusage(resource.RUSAGE_SELF)
+    t0 = time.perf_counter()
+    with torch.cuda.device(gi.dev):
+        run = DeviceRun(sp, gi.dev, st)
+        out = _search_device(run, gi, p, report, st, timers)
+        if int(out["status"].item()):
+            raise RuntimeError("k1_tiles: a tile copy did not complete")
+        rec = _gather_psms(*out["psm"], out["c_hyp"], out["c_row"], out["c_cnt"], out["k2"], out["dh"],
+                           out["spec_scored"], out["spec_matched"], out["peaks"]["tic"], report, st)
+    tbl = _psm_columns(sp, l1, rec, p)
+    ru1 = resource.getrusage(resource.RUSAGE_SELF)
+    st.wall_s["total"] = time.perf_counter() - t0
+    n_rescored = int(out["cand_off"][-1])
+    st.counts.update(n_spectra=len(sp), n_searched=int(out["peaks"]["valid_d"].sum()),
+                     n_hypotheses=int(out["dh"]["spec_off"][-1]), n_rescored=n_rescored, n_psms=tbl.num_rows)
+    st.counts["cpu_core_s"] = (ru1.ru_utime - ru0.ru_utime) + (ru1.ru_stime - ru0.ru_stime)
+    return tbl, st, out
+
+
+# ------------------------------------------------------------------------------------------------ references
+def window_candidates(hyp, dev, spec_subset: np.ndarray | None = None):
+    """Every (hypothesis, row) in the precursor windows, sorted by (spectrum, row) (reference engine.py:468-480)."""
+    lo, hi = np.asarray(hyp["lo"]), np.asarray(hyp["hi"])
+    hs = np.asarray(hyp["spec"])
+    hsel = np.arange(len(lo))
+    if spec_subset is not None:
+        hsel = hsel[np.isin(hs, spec_subset)]
+    n = (hi - lo)[hsel]
+    hh = np.repeat(hsel, n)
+    rr = np.repeat(lo[hsel], n) + (np.arange(n.sum()) - np.repeat(np.cumsum(n) - n, n))
+    s = hs[hh]
+    o = np.lexsort((rr, s))
+    return torch.from_numpy(hh[o].astype(np.int64)).to(dev), torch.from_numpy(rr[o].astype(np.int64)).to(dev)
+
+
+def k1_brute(gi: GpuIndex, hyp, peaks, h: torch.Tensor, r: torch.Tensor, p: SearchParams) -> torch.Tensor:
+    """Brute-force preliminary counts for (hyp, row) pairs, no index (reference engine.py:483-497)."""
+    L = K.lib()
+    dev = gi.dev
+    dh = _as_dev(hyp, dev)
+    out = torch.empty(len(h), dtype=torch.int32, device=dev)
+    hh = h.to(torch.int32).contiguous()
+    rr = r.to(torch.int32).contiguous()
+    K.check(L.vk_k1_brute(len(h), K.ptr(hh), K.ptr(rr), K.ptr(dh["spec"]), K.ptr(dh["maxfz"]), K.ptr(peaks["off"]),
+                          K.ptr(peaks["mass"]), *gi.table_ptrs(), p.min_ion_index, p.fragment_min_mz,
+                          p.fragment_max_mz, p.fragment_ppm[0], p.fragment_ppm[1], gi.inv_logw, K.ptr(out),
+                          K.stream()), "k1_brute")
+    return out
+
+
+def search_exhaustive(sp: Spectra, gi: GpuIndex, l1, p: SearchParams, report: int | None = None,
+                      spec_subset: np.ndarray | None = None, batch: int = 20_000_000):
+    """K2 over EVERY candidate of the precursor windows, no K1 shortlist (reference engine.py:500-523)."""
+    st = Stats()
+    dev = gi.dev
+    peaks = k0_preprocess(sp, p, dev, st)
+    hyp = make_hypotheses(sp, peaks["valid"], gi.mass32_np, p)
+    o_h, o_r, o_c, scored, matched, d_spec, d_maxfz = run_k1(gi, hyp, peaks, p, st)
+    h, r = window_candidates(hyp, dev, spec_subset)
+    spec = d_spec[h].long()
+    parts = []
+    i = 0
+    n = len(h)
+    while i < n:
+        j = min(n, i + batch)
+        if j < n:
+            j = int(torch.searchsorted(spec, spec[j - 1], side="right"))
+        parts.append(run_k2(gi, h[i:j], r[i:j], d_spec, d_maxfz, peaks, p))
+        i = j
+    k2 = {k: torch.cat([q[k] for q in parts]) for k in parts[0]} if parts else None
+    c = torch.full((len(h),), -1, dtype=torch.int64, device=dev)
+    tbl = psm_table(sp, gi, l1, hyp, h, r, c, k2, scored, matched, peaks, p, report)
+    return tbl, st, {"peaks": peaks, "hyp": hyp, "h": h, "r": r, "k2": k2}
