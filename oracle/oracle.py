@@ -11,7 +11,7 @@ Pieces (each cites the reference lines it restates):
   k1_appended        vulcan/gpu/kernels.cu:170-189  threshold append + per-hypothesis scored / matched
   select_topk        vulcan/gpu/engine.py:284-312   per-spectrum top-K + pair closure + unique (spectrum, row)
   k2                 vulcan/gpu/kernels.cu:263-376  exact rescoring (C)
-  k2_f64             same algorithm in FP64         hyperscore oracle (C)
+  k2_f64             same matches, FP64 sums        hyperscore oracle (C)
   psm_rank           vulcan/gpu/engine.py:366-392   filter, rank by (hyperscore desc, row asc), delta_next/best
   lnfact             vulcan/gpu/engine.py:354-358
 """

@@ -10,7 +10,7 @@
  *   - K1 brute-force counts               vulcan/gpu/kernels.cu:195-232
  *   - K1 per-hypothesis window counts     same semantics, faster search (sorted fragments per row)
  *   - K2 exact rescoring (+ shift mode)   vulcan/gpu/kernels.cu:240-376
- *   - K2 in FP64 (hyperscore oracle)      same algorithm with f64 ion masses, bounds and sums
+ *   - K2 with FP64 accumulation           same matches, intensity sums and hyperscore in double (hyperscore oracle)
  *
  * Build: gcc -O2 -fopenmp -ffp-contract=off (no FMA contraction: every f32 operation rounds once, as the
  * reference's -fmad=false kernels and Sage's Rust code do).
@@ -355,8 +355,10 @@ void or_k2(int n_spec, const int64_t* cand_off, const int32_t* c_row, const int8
   }
 }
 
-/* K2 closed mode in FP64: ion masses, tolerance bounds, intensity sums and the hyperscore in double precision,
- * same match rule (most intense peak in the window, later peak on ties).  The hyperscore oracle. */
+/* K2 closed mode with FP64 accumulation: the matches are decided exactly as the reference decides them (f32 ion
+ * masses and tolerance bounds, most intense peak in the window, later peak on ties), then the matched intensities
+ * are summed and the hyperscore evaluated in double precision.  The hyperscore oracle: it isolates the rounding of
+ * the f32 accumulation from the (defined) f32 match semantics. */
 void or_k2_f64(int n_spec, const int64_t* cand_off, const int32_t* c_row, const int8_t* c_maxfz,
                const int32_t* spec_ids, const int64_t* pk_off, const float* pk_mass, const float* pk_int,
                const int64_t* seq_off, const uint8_t* len, const uint64_t* mask, const float* mass32,
@@ -376,26 +378,20 @@ void or_k2_f64(int n_spec, const int64_t* cand_off, const int32_t* c_row, const 
       const uint8_t* sq = res + seq_off[r];
       int L = len[r];
       uint64_t mk = mask[r];
-      double nt = (mk & NTERM_BIT) ? (double)P->nterm : 0.0;
       double sb = 0.0, sy = 0.0;
       int mb = 0, my = 0;
       for (int kind = 0; kind < 2; ++kind) {
-        double cum = kind == 0 ? nt : (double)mass32[r] - nt;
+        float cum = kind == 0 ? nterm_of(P, mk) : mass32[r] - nterm_of(P, mk);
         for (int k = 0; k < L - 1; ++k) {
-          int i = sq[k] - 'A';
-          double rm = (double)P->mono[i] + (double)(((mk >> k) & 1ull) ? P->var[i] : P->stat[i]);
+          float rm = resmass(P, sq[k], k, mk);
           cum = kind == 0 ? cum + rm : cum - rm;
           for (int z = 1; z < maxfz; ++z) {
-            double mz = cum / (double)z;
-            double a = P->tol_da ? mz + tol_lo : mz + mz * tol_lo / 1e6;
-            double bd = P->tol_da ? mz + tol_hi : mz + mz * tol_hi / 1e6;
+            float mz = cum / (float)z;
+            float a = tol_bound(P, mz, (float)tol_lo), bd = tol_bound(P, mz, (float)tol_hi);
             int best = -1;
             float mx = 0.f;
-            for (int j = 0; j < np; ++j) {
-              if ((double)sm[j] < a) continue;
-              if ((double)sm[j] > bd) break;
+            for (int j = lower_bound_f(sm, np, a); j < np && sm[j] <= bd; ++j)
               if (si[j] >= mx) { mx = si[j]; best = j; }
-            }
             if (best >= 0) {
               if (kind == 0) { mb += 1; sb += (double)si[best]; }
               else { my += 1; sy += (double)si[best]; }

@@ -1,0 +1,184 @@
+"""The CPU oracle against the reference: its own Python code (golden_ref_py.npz, made by
+tests/golden/make_golden.py) and its own CUDA kernels (golden_ref_kernels.npz, made by
+tests/golden/make_golden_ref.py on a B200).  These pins make the oracle trustworthy before it judges the kernels."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+STATIC = {"C": 57.021464}
+VAR = {"M": 15.9949}
+SETS = ("da", "ppm", "ppm_mfz")
+
+
+def _peaks(g, name):
+    return {k: g[f"{name}/k0_{k}"] for k in ("off", "mass", "int", "tic")}
+
+
+def _hyp(g, name):
+    return {k: g[f"{name}/hyp_{k}"] for k in ("spec", "z", "iso", "pm", "M", "lo", "hi", "maxfz")}
+
+
+@pytest.mark.parametrize("name", SETS)
+def test_k0_view_equals_reference(mini, golden_py, param_sets, name):
+    l1, sp, _ = mini
+    pk = O.k0_view(sp, param_sets[name])
+    g = golden_py
+    assert np.array_equal(pk["off"], g[f"{name}/k0_off"])
+    assert np.array_equal(pk["mass"], g[f"{name}/k0_mass"])
+    assert np.array_equal(pk["int"], g[f"{name}/k0_int"])
+    assert np.array_equal(pk["valid"], g[f"{name}/k0_valid"])
+    np.testing.assert_allclose(pk["tic"], g[f"{name}/k0_tic"], rtol=1e-7)
+
+
+@pytest.mark.parametrize("name", SETS)
+def test_hypotheses_equal_reference(mini, golden_py, param_sets, name):
+    l1, sp, _ = mini
+    g = golden_py
+    hyp = O.make_hypotheses(sp, g[f"{name}/k0_valid"], l1.mass32, param_sets[name])
+    for k in ("spec", "z", "iso", "pm", "M", "lo", "hi", "maxfz"):
+        assert np.array_equal(hyp[k], g[f"{name}/hyp_{k}"]), k
+
+
+@pytest.mark.parametrize("name", SETS)
+def test_window_candidates_equal_reference(golden_py, name):
+    g = golden_py
+    h, r = O.window_candidates(_hyp(g, name))
+    assert np.array_equal(h, g[f"{name}/win_h"]) and np.array_equal(r, g[f"{name}/win_r"])
+
+
+@pytest.mark.parametrize("name", SETS)
+def test_select_topk_equals_reference(mini, golden_py, param_sets, name):
+    l1, sp, _ = mini
+    g = golden_py
+    p = param_sets[name]
+    hyp = _hyp(g, name)
+    P = O.make_params(STATIC, VAR, p.fragment_unit)
+    win_off, cnt, sc, mt = O.k1_windows(l1, hyp, _peaks(g, name), p, P)
+    oh, orr, oc = O.k1_appended(hyp, win_off, cnt, p.k1_threshold)
+    assert len(oh) > p.topk * 10       # enough entries that the per-spectrum cut is exercised
+    h, r, c = O.select_topk(oh, orr, oc, hyp["spec"], l1.partner, p.topk)
+    assert np.array_equal(h, g[f"{name}/topk_h"])
+    assert np.array_equal(r, g[f"{name}/topk_r"])
+    assert np.array_equal(c, g[f"{name}/topk_c"])
+
+
+@pytest.mark.parametrize("name", SETS)
+def test_psm_rank_equals_reference(mini, golden_py, param_sets, name):
+    """Ranking, delta_next / delta_best and the reported candidates equal the reference's psm_table."""
+    l1, sp, _ = mini
+    g = golden_py
+    p = param_sets[name]
+    hyp = _hyp(g, name)
+    P = O.make_params(STATIC, VAR, p.fragment_unit)
+    h, r = g[f"{name}/topk_h"], g[f"{name}/topk_r"]
+    k2 = O.k2(l1, hyp, _peaks(g, name), h, r, p, P)
+    rk = O.psm_rank(k2, r, p.min_matched_peaks, 3)
+    assert np.array_equal(rk["spec"], g[f"{name}/psm_spec_idx"])
+    assert np.array_equal(rk["rank"], g[f"{name}/psm_rank"])
+    assert np.array_equal(r[rk["cand"]], g[f"{name}/psm_pf_row"])
+    assert np.array_equal(rk["hyperscore"], g[f"{name}/psm_hyperscore"])
+    assert np.array_equal(rk["delta_next"], g[f"{name}/psm_delta_next"])
+    assert np.array_equal(rk["delta_best"], g[f"{name}/psm_delta_best"])
+
+
+def test_lnfact_equals_reference(golden_py):
+    assert np.array_equal(O.lnfact(golden_py["lnfact_n"]), golden_py["lnfact_v"])
+
+
+# ---------------------------------------------------------------------------------- against the reference kernels
+@pytest.mark.parametrize("name", SETS)
+def test_frag_count_and_keys_equal_reference_kernels(mini, golden_kernels, param_sets, name):
+    import math
+    l1, _, _ = mini
+    p = param_sets[name]
+    P = O.make_params(STATIC, VAR, p.fragment_unit)
+    n = len(l1)
+    cnt = np.empty(n, np.int32)
+    import ctypes as C
+    L = O.lib()
+    a = [O._p(O._c(getattr(l1, k), dt)) for k, dt in (("seq_off", np.int64), ("length", np.uint8),
+                                                      ("mask", np.uint64), ("mass32", np.float32),
+                                                      ("residues", np.uint8))]
+    L.or_frag_count(C.c_int64(n), *a, C.c_int(p.min_ion_index), C.c_float(p.fragment_min_mz),
+                    C.c_float(p.fragment_max_mz), O._p(cnt), C.byref(P))
+    assert np.array_equal(cnt, golden_kernels[f"{name}/frag_count"])
+    off = np.zeros(n + 1, np.int64)
+    np.cumsum(cnt, out=off[1:])
+    keys = np.empty(off[-1], np.int64)
+    inv_logw = 1.0 / math.log1p(p.bin_ppm * 1e-6)
+    L.or_frag_emit(C.c_int64(n), *a, C.c_int(p.min_ion_index), C.c_float(p.fragment_min_mz),
+                   C.c_float(p.fragment_max_mz), C.c_double(inv_logw), C.c_int(p.chunk_size), C.c_int64(0),
+                   O._p(off), O._p(keys), C.byref(P))
+    # host log() may differ from the device's by an ulp; a key can then move across a quantum boundary
+    ref = golden_kernels[f"{name}/frag_keys"]
+    assert len(keys) == len(ref)
+    assert np.mean(np.sort(keys) == ref) > 0.999
+
+
+@pytest.mark.parametrize("name", SETS)
+def test_k1_brute_equals_reference_kernels(mini, golden_py, golden_kernels, param_sets, name):
+    l1, _, _ = mini
+    g = golden_py
+    p = param_sets[name]
+    P = O.make_params(STATIC, VAR, p.fragment_unit)
+    cnt = O.k1_brute(l1, _hyp(g, name), _peaks(g, name), g[f"{name}/win_h"], g[f"{name}/win_r"], p, P)
+    assert np.array_equal(cnt, golden_kernels[f"{name}/brute"])
+
+
+@pytest.mark.parametrize("name", SETS)
+def test_k1_windows_equal_reference_k1(mini, golden_py, golden_kernels, param_sets, name):
+    """The oracle's window counts == the reference's indexed K1 append set, scored and matched (and so equal its
+    brute force, as the reference's own test asserts)."""
+    l1, _, _ = mini
+    g = golden_py
+    p = param_sets[name]
+    hyp = _hyp(g, name)
+    P = O.make_params(STATIC, VAR, p.fragment_unit)
+    win_off, cnt, sc, mt = O.k1_windows(l1, hyp, _peaks(g, name), p, P)
+    oh, orr, oc = O.k1_appended(hyp, win_off, cnt, p.k1_threshold)
+    key = (oh << 32) | orr
+    o = np.argsort(key)
+    assert np.array_equal(key[o], golden_kernels[f"{name}/k1_key"])
+    assert np.array_equal(oc[o], golden_kernels[f"{name}/k1_cnt"])
+    assert np.array_equal(sc.astype(np.int64), golden_kernels[f"{name}/k1_scored"].astype(np.int64))
+    assert np.array_equal(mt.astype(np.int64), golden_kernels[f"{name}/k1_matched"].astype(np.int64))
+    # window counts restricted to the brute-force pairs
+    bc = golden_kernels[f"{name}/brute"]
+    nz = bc > 0
+    bkey = (g[f"{name}/win_h"][nz].astype(np.int64) << 32) | g[f"{name}/win_r"][nz]
+    assert np.array_equal(np.sort(bkey), golden_kernels[f"{name}/k1_key"])
+
+
+@pytest.mark.parametrize("name", SETS)
+@pytest.mark.parametrize("mode", ("closed", "shift"))
+def test_k2_equals_reference_kernels(mini, golden_py, golden_kernels, param_sets, name, mode):
+    l1, _, _ = mini
+    g = golden_py
+    p = param_sets[name]
+    P = O.make_params(STATIC, VAR, p.fragment_unit)
+    shift = golden_kernels[f"{name}/k2shift_delta"] if mode == "shift" else None
+    out = O.k2(l1, _hyp(g, name), _peaks(g, name), g[f"{name}/win_h"], g[f"{name}/win_r"], p, P, shift=shift)
+    ref = {k: golden_kernels[f"{name}/k2{mode}_{k}"] for k in ("hs", "sb", "sy", "ppm", "mb", "my", "lb", "ly")}
+    for a, b in (("summed_b", "sb"), ("summed_y", "sy"), ("matched_b", "mb"), ("matched_y", "my"),
+                 ("longest_b", "lb"), ("longest_y", "ly")):
+        assert np.array_equal(out[a], ref[b]), a
+    assert np.array_equal(out["ppm"], ref["ppm"], equal_nan=True)
+    # host and device log() agree to an ulp or so
+    np.testing.assert_allclose(out["hyperscore"], ref["hs"], rtol=1e-13, atol=0)
+
+
+@pytest.mark.parametrize("name", SETS)
+def test_k2_hyperscore_within_fp64_oracle(mini, golden_py, param_sets, name):
+    """f32 K2 hyperscores within 1e-5 relative of the all-FP64 oracle wherever both match the same ions."""
+    l1, _, _ = mini
+    g = golden_py
+    p = param_sets[name]
+    P = O.make_params(STATIC, VAR, p.fragment_unit)
+    h, r = g[f"{name}/win_h"], g[f"{name}/win_r"]
+    a = O.k2(l1, _hyp(g, name), _peaks(g, name), h, r, p, P)
+    b = O.k2_f64(l1, _hyp(g, name), _peaks(g, name), h, r, p, P)
+    same = (a["matched_b"] == b["matched_b"]) & (a["matched_y"] == b["matched_y"])
+    assert same.mean() > 0.999
+    rel = np.abs(a["hyperscore"][same] - b["hyperscore"][same]) / np.abs(b["hyperscore"][same])
+    assert rel.max() <= 1e-5
