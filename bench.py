@@ -1,0 +1,420 @@
+#!/usr/bin/env python3
+"""Benchmark of the DDA search hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload human|small]
+
+One step = one pass of the search over one MS2 run of the workload (human: 40,000 simulated spectra of uneven
+peak counts, 20-600, against the ~5.5M-peptidoform human-scale index, top-k 100): K0 peak view, hypotheses, K1
+fragment-index counting, top-K + pair closure, K2 exact rescoring, PSM ranking.
+
+  value      spectra/s with the run's raw spectra already in HBM (device pass, CUDA events on the stream, L2
+             flushed between steps), summed over ranks (each rank searches its own run: weak scaling)
+  e2e        spectra/s through the public API engine.search(Spectra) with host buffers: H2D of the raw spectra,
+             the device pass, D2H of the PSM rows and the host PSM table (wall clock around each call)
+  roofline   the dominant kernel's algorithmic bytes per launch / its mean CUDA-event duration vs the measured
+             HBM copy bandwidth
+  cpu_baseline  the CPU oracle (C/OpenMP restatement of the reference kernels) on a bounded sample, all cores
+
+--impl reference times the CPU path of the reference (its C restatement: the reference ships no CPU search of
+its own; its CPU comparator is the external Sage binary) on the same workload, a bounded sample per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "vulcan-proteomics_b200"))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "spectra/s on 1 B200, learned-pruned vs exhaustive at ≥99.9% top-1 recall"
+STATIC = {"C": 57.021464}
+VAR = {"M": 15.9949}
+CACHE = os.environ.get("VULCAN_BENCH_CACHE", os.path.join(tempfile.gettempdir(), "vulcan_bench_cache"))
+
+
+def _peaks_json():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _workload_setup(name: str, rank: int):
+    from vulcan import synth
+    from vulcan.index.build import L1Index, read_labels
+    w = synth.WORKLOADS[name]
+    t0 = time.perf_counter()
+    d = synth.build_index(w, CACHE)
+    t_build = time.perf_counter() - t0
+    l1 = L1Index(d)
+    sp, rows = synth.simulate_run(l1, read_labels(d), w, seed=w.spectra_seed + 1000 * rank, run=f"run{rank}")
+    return w, l1, sp, t_build
+
+
+def _config(w, p, extra=None):
+    cfg = {"workload": f"{w.name}: {w.n_proteins} random proteins (<= {w.missed_cleavages} missed cleavages, "
+                       f"length {w.min_len}-{w.max_len}, CAM-C, Met-ox <= {w.max_var}, pseudo-reverse decoys); "
+                       f"runs of {w.n_spectra} simulated MS2 spectra, charge {w.charges[0]}-{w.charges[1]}",
+           "path": "plain exhaustive search (K1 -> top-k -> K2), no learned pruner",
+           "precursor_ppm": list(p.precursor_ppm), "fragment_tol": f"+-{p.fragment_ppm[1]} {p.fragment_unit}",
+           "topk": p.topk, "max_peaks": p.max_peaks, "l2": "flushed between steps (256 MiB write)"}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples every 200 ms while running."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200", "-i", str(device_index)], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [ln.split(",") for ln in self.f.read().strip().splitlines() if ln.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in rows:
+            r = [x.strip() for x in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_oracle_pass(l1, sp_sub, p):
+    """The oracle's search of a run (K0, hypotheses, K1, top-K + closure, K2, ranking) on the host cores."""
+    from oracle import oracle as O
+    P = O.make_params(STATIC, VAR, p.fragment_unit)
+    pk = O.k0_view(sp_sub, p)
+    hyp = O.make_hypotheses(sp_sub, pk["valid"], l1.mass32, p)
+    win_off, cnt, sc, mt = O.k1_windows(l1, hyp, pk, p, P, arrays=_ARR.get(id(l1)))
+    oh, orr, oc = O.k1_appended(hyp, win_off, cnt, p.k1_threshold)
+    h, r, c = O.select_topk(oh, orr, oc, hyp["spec"], l1.partner, p.topk, p.pair_closure)
+    k2 = O.k2(l1, hyp, pk, h, r, p, P)
+    return O.psm_rank(k2, r, p.min_matched_peaks, p.report_psms)
+
+
+_ARR = {}
+
+
+def _subset(sp, n):
+    from vulcan.gpu.host import Spectra
+    n = min(n, len(sp))
+    o = sp.offsets[:n + 1]
+    return Spectra(sp.run, sp.scan[:n], sp.index[:n], sp.rt[:n], sp.precursor_mz[:n], sp.charge[:n],
+                   sp.mz[:o[-1]], sp.intensity[:o[-1]], o.copy())
+
+
+def cpu_rate(l1, sp, p, budget_s: float):
+    """spectra/s of the CPU oracle on a sample sized to take about budget_s."""
+    from oracle import oracle as O
+    _ARR[id(l1)] = {k: np.ascontiguousarray(getattr(l1, k)) for k in ("seq_off", "length", "mask", "mass32",
+                                                                         "residues")}
+    n = 500
+    t0 = time.perf_counter()
+    cpu_oracle_pass(l1, _subset(sp, n), p)
+    t = time.perf_counter() - t0
+    n2 = int(min(len(sp), max(n, n * budget_s / max(t, 1e-3))))
+    t0 = time.perf_counter()
+    cpu_oracle_pass(l1, _subset(sp, n2), p)
+    t2 = time.perf_counter() - t0
+    return n2 / t2, n2, t2, O.n_threads()
+
+
+def k1_algorithmic_bytes(gi, dh, peaks, win_off, item_off, item_hyp):
+    """Bytes K1 must move per launch in this layout: each tile with work is read once (postings + coarse-bin CSR);
+    per work item the spectrum's peak masses (4 B each) and the hypothesis record (spec 4, maxfz 1, lo/hi 16,
+    peak offsets 16, item id 4); per window row one 4-byte count written."""
+    import torch
+    nt = gi.tix.n_tiles
+    stride = ((1 << gi.tix.cbin_bits) + 1 + 7) & ~7
+    items_per_tile = item_off[1:] - item_off[:-1]
+    busy = items_per_tile > 0
+    tile_bytes = ((gi.tile_off[1:nt + 1] - gi.tile_off[:nt]) * 4 + stride * 2)[busy].sum()
+    h = item_hyp.long()
+    s = dh["spec"][h].long()
+    npk = (peaks["off"][s + 1] - peaks["off"][s])
+    item_bytes = (npk * 4 + 41).sum()
+    out_bytes = win_off[-1] * 4
+    return int((tile_bytes + item_bytes + out_bytes).item())
+
+
+def run_b200(a):
+    import torch
+    import torch.distributed as dist
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+    from vulcan.gpu import _lib as K
+    from vulcan.gpu import engine as E
+    w, l1, sp, t_build = _workload_setup(a.workload, rank)
+    p = w.search_params()
+    gi = E.GpuIndex(l1, p, STATIC, VAR, device=dev)
+    run = E.DeviceRun(sp, dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device=dev)   # 256 MiB > 126 MB L2
+    st = E.Stats()
+
+    def step():
+        return E._search_device(run, gi, p, 1, st)
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+    # device pass, timed with events on the launching stream
+    clocks = ClockSampler(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    K.LAUNCHES["n"] = 0
+    evs = []
+    for _ in range(a.steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        out = step()
+        e1.record()
+        evs.append((e0, e1))
+    torch.cuda.synchronize()
+    launches = K.LAUNCHES["n"]
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = sum(e0.elapsed_time(e1) for e0, e1 in evs)
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    ms_per_step = ms_max / a.steps
+    value = len(sp) * world * a.steps / (ms_max / 1e3)
+
+    # end to end through the public API (host Spectra in, PSM table out)
+    e2e_steps = max(3, min(a.steps, 20))
+    E.search(sp, gi, l1, p)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    h2d = d2h = 0
+    for _ in range(e2e_steps):
+        tbl, s2, _ = E.search(sp, gi, l1, p)
+        h2d, d2h = s2.h2d_bytes, s2.d2h_bytes
+    torch.cuda.synchronize()
+    e2e_s = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(e2e_s, op=dist.ReduceOp.MAX)
+    e2e = len(sp) * world * e2e_steps / float(e2e_s.item())
+
+    # per-phase device times (separate pass, phases synchronised) -> dominant kernel
+    st_ph = E.Stats()
+    for _ in range(3):
+        flush.zero_()
+        E._search_device(run, gi, p, 1, st_ph, timers=True)
+    phase_ms = {k: v / 3 for k, v in st_ph.gpu_ms.items()}
+    # the K1 kernel alone: mean launch duration with the plan of this run
+    dh = out["dh"]
+    win_off, cnt = out["win_off"], out["cnt"]
+    import ctypes as C
+    L = K.lib()
+    nt = gi.tix.n_tiles
+    tile_items = torch.empty(nt, dtype=torch.int64, device=dev)
+    win_len = torch.empty(dh["n_max"], dtype=torch.int64, device=dev)
+    K.check(L.vk_k1_plan_count(C.byref(gi.tix), dh["n_max"], K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(tile_items),
+                               K.ptr(win_len), K.stream()), "k1_plan_count")
+    item_off = E._scan(tile_items)
+    n_items = int(item_off[-1])
+    cursor = torch.empty(nt, dtype=torch.int64, device=dev)
+    item_hyp = torch.empty(max(n_items, 1), dtype=torch.int32, device=dev)
+    K.check(L.vk_k1_plan_fill(C.byref(gi.tix), dh["n_max"], K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(item_off),
+                              K.ptr(cursor), K.ptr(item_hyp), K.stream()), "k1_plan_fill")
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
+    peaks = out["peaks"]
+    k1_ms = []
+    for _ in range(10):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        K.check(L.vk_k1_tiles(C.byref(gi.tix), C.byref(gi.fp), float(p.fragment_ppm[0]), float(p.fragment_ppm[1]),
+                              K.ptr(item_off), K.ptr(item_hyp), K.ptr(dh["spec"]), K.ptr(dh["maxfz"]),
+                              K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(win_off), K.ptr(peaks["off"]),
+                              K.ptr(peaks["mass"]), K.ptr(cnt), K.ptr(status), K.stream()), "k1_tiles")
+        e1.record()
+        torch.cuda.synchronize()
+        k1_ms.append(e0.elapsed_time(e1))
+    k1_mean = sum(k1_ms[2:]) / len(k1_ms[2:])
+    algo = k1_algorithmic_bytes(gi, dh, peaks, win_off, item_off, item_hyp)
+    peak_gbs, peak_kind = _peaks_json()
+    achieved = algo / (k1_mean / 1e3) / 1e9
+    traffic = _traffic_from_profiles("k1_tiles")
+
+    if rank == 0:
+        cpu = None
+        if world == 1:
+            rate, n_s, t_s, cores = cpu_rate(l1, sp, p, a.cpu_budget)
+            cpu = {"value": round(rate, 1), "unit": "spectra/s", "cores": cores, "kind": "port",
+                   "sample": f"first {n_s} spectra of the run through the oracle's K0->hypotheses->K1->top-k->K2->"
+                             f"ranking ({t_s:.1f} s)"}
+        counts = st.counts
+        line = {
+            "metric": METRIC, "value": round(value, 1), "unit": "spectra/s", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": _config(w, p, {"spectra_per_step_per_gpu": len(sp), "index_rows": len(l1),
+                                     "index_postings": gi.n_postings, "tile_rows": p.tile_rows,
+                                     "parallelism": f"replicas x{world} (one run per GPU)"}),
+            "e2e": {"value": round(e2e, 1), "unit": "spectra/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "kernel": "k1_tiles", "achieved": round(achieved, 1),
+                         "peak": peak_gbs, "unit": "GB/s", "frac": round(achieved / peak_gbs, 4),
+                         "peak_source": peak_kind, "traffic": traffic, "algorithmic_bytes": algo,
+                         "mean_launch_ms": round(k1_mean, 4)},
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "phase_ms": {k: round(v, 4) for k, v in phase_ms.items()},
+            "index_build_s": round(t_build, 1),
+            "per_step": {"hypotheses": counts.get("n_hypotheses"), "k1_work_items": n_items,
+                         "k1_window_rows": int(win_off[-1]), "rescored": int(out["cand_off"][-1])},
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def _traffic_from_profiles(kernel: str):
+    """DRAM bytes per launch of `kernel` recorded from an ncu capture in profiles/<kernel>_*.md (a line
+    'dram_bytes_per_launch: N'), or None."""
+    d = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(d):
+        return None
+    for f in sorted(os.listdir(d)):
+        if f.startswith(kernel) and f.endswith(".md"):
+            for ln in open(os.path.join(d, f)):
+                if ln.strip().startswith("dram_bytes_per_launch:"):
+                    try:
+                        return int(float(ln.split(":", 1)[1].strip().split()[0]))
+                    except ValueError:
+                        return None
+    return None
+
+
+def run_profile(a):
+    import torch
+    from vulcan.gpu import engine as E
+    dev = torch.device("cuda", 0)
+    w, l1, sp, _ = _workload_setup(a.workload, 0)
+    p = w.search_params()
+    gi = E.GpuIndex(l1, p, STATIC, VAR, device=dev)
+    run = E.DeviceRun(sp, dev)
+    st = E.Stats()
+    for _ in range(2):
+        E._search_device(run, gi, p, 1, st)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_passes": 2, "spectra": len(sp), "index_rows": len(l1)}), flush=True)
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    w, l1, sp, _ = _workload_setup(a.workload, 0)
+    p = w.search_params()
+    _ARR[id(l1)] = {k: np.ascontiguousarray(getattr(l1, k)) for k in ("seq_off", "length", "mask", "mass32",
+                                                                         "residues")}
+    # per-step sample sized so warmup + steps take about a.cpu_total seconds
+    t0 = time.perf_counter()
+    cpu_oracle_pass(l1, _subset(sp, 300), p)
+    per_spec = (time.perf_counter() - t0) / 300
+    n_step = int(max(100, min(len(sp), a.cpu_total / max(1, a.steps + a.warmup) / max(per_spec, 1e-6))))
+    for i in range(a.warmup):
+        cpu_oracle_pass(l1, _subset(sp, n_step), p)
+    t0 = time.perf_counter()
+    for i in range(a.steps):
+        cpu_oracle_pass(l1, _subset(sp, n_step), p)
+    t = time.perf_counter() - t0
+    value = n_step * a.steps / t
+    cores = O.n_threads()
+    line = {
+        "metric": METRIC, "value": round(value, 1), "unit": "spectra/s", "n_gpus": int(os.environ.get("WORLD_SIZE", 1)),
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(t / a.steps * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+        "config": _config(w, p, {"spectra_per_step": n_step}),
+        "cpu_baseline": {"value": round(value, 1), "unit": "spectra/s", "cores": cores, "kind": "port",
+                         "sample": f"{n_step} spectra per step of the same simulated run"},
+        "e2e": {"value": round(value, 1), "unit": "spectra/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
+    ap.add_argument("--workload", choices=("human", "small"), default="human")
+    ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of CPU-baseline work (rank 0, N=1)")
+    ap.add_argument("--cpu-total", type=float, default=120.0, help="seconds of the reference arm in total")
+    ap.add_argument("--mode", choices=("bench", "profile"), default="bench",
+                    help="profile: set up the workload and run two device passes only (for an ncu capture of one "
+                         "kernel launch of the second pass, e.g. -k regex:k1_tiles -s 1 -c 1)")
+    a = ap.parse_args()
+    if a.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if a.impl == "reference":
+        run_reference(a)
+    elif a.mode == "profile":
+        run_profile(a)
+    else:
+        run_b200(a)
+
+
+if __name__ == "__main__":
+    main()

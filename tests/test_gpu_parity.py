@@ -1,0 +1,228 @@
+"""Parity of the sm_100a kernels with the oracle and with the reference's own kernels, on the mini fixture
+(three parameter sets: Da tolerance, ppm tolerance, ppm with fragment charges up to z-1 and isotope errors -1..2).
+
+Integer, index and f32 outputs must be bit-identical; hyperscores (f64 log on the device vs the host libm) within
+1e-12 relative of the oracle and bit-identical to the reference's kernels (same device log)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+SETS = ("da", "ppm", "ppm_mfz")
+STATIC = {"C": 57.021464}
+VAR = {"M": 15.9949}
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    assert torch.cuda.is_available(), "needs a CUDA device"
+    return torch
+
+
+@pytest.fixture(scope="module")
+def indexes(mini, param_sets, torch_cuda):
+    from vulcan.gpu import engine as E
+    l1, _, _ = mini
+    return {name: E.GpuIndex(l1, p, STATIC, VAR) for name, p in param_sets.items()}
+
+
+def _hyp(g, name):
+    return {k: g[f"{name}/hyp_{k}"] for k in ("spec", "z", "iso", "pm", "M", "lo", "hi", "maxfz")}
+
+
+@pytest.mark.parametrize("name", SETS)
+def test_k0_device_equals_reference(mini, golden_py, param_sets, indexes, name):
+    from vulcan.gpu import engine as E
+    _, sp, _ = mini
+    st = E.Stats()
+    pk = E.k0_preprocess(sp, param_sets[name], indexes[name].dev, st)
+    g = golden_py
+    assert np.array_equal(pk["off"].cpu().numpy(), g[f"{name}/k0_off"])
+    assert np.array_equal(pk["mass"].cpu().numpy(), g[f"{name}/k0_mass"])
+    assert np.array_equal(pk["int"].cpu().numpy(), g[f"{name}/k0_int"])
+    assert np.array_equal(pk["valid"], g[f"{name}/k0_valid"])
+    np.testing.assert_allclose(pk["tic"].cpu().numpy(), g[f"{name}/k0_tic"], rtol=1e-7)
+
+
+@pytest.mark.parametrize("name", SETS)
+def test_search_stages_equal_reference(mini, golden_py, golden_kernels, param_sets, indexes, name, torch_cuda):
+    """Device hypotheses, dense K1 counts, top-K + closure and K2 of engine.search equal the references."""
+    from oracle import oracle as O
+    from vulcan.gpu import engine as E
+    l1, sp, _ = mini
+    p = param_sets[name]
+    g = golden_py
+    tbl, st, out = E.search(sp, indexes[name], l1, p, report=3)
+    dh = out["dh"]
+    nh = int(dh["spec_off"][-1])
+    for k in ("spec", "z", "iso", "pm", "M", "lo", "hi", "maxfz"):
+        assert np.array_equal(dh[k][:nh].cpu().numpy(), g[f"{name}/hyp_{k}"]), k
+    # dense K1 counts == oracle window counts; nonzero set == the reference kernels' K1 append set
+    hyp = _hyp(g, name)
+    P = O.make_params(STATIC, VAR, p.fragment_unit)
+    peaks = {k: g[f"{name}/k0_{k}"] for k in ("off", "mass", "int")}
+    win_off, cnt, sc, mt = O.k1_windows(l1, hyp, peaks, p, P)
+    assert np.array_equal(out["cnt"].cpu().numpy(), cnt)
+    assert np.array_equal(out["hyp_scored"][:nh].cpu().numpy().astype(np.int64), golden_kernels[f"{name}/k1_scored"])
+    assert np.array_equal(out["hyp_matched"][:nh].cpu().numpy().astype(np.int64),
+                          golden_kernels[f"{name}/k1_matched"])
+    # top-K + pair closure == the reference's select_topk
+    nc = int(out["cand_off"][-1])
+    assert np.array_equal(out["c_hyp"][:nc].cpu().numpy(), g[f"{name}/topk_h"])
+    assert np.array_equal(out["c_row"][:nc].cpu().numpy(), g[f"{name}/topk_r"])
+    assert np.array_equal(out["c_cnt"][:nc].cpu().numpy(), g[f"{name}/topk_c"])
+    # K2 == oracle (bit-exact f32 / integer outputs)
+    k2o = O.k2(l1, hyp, peaks, g[f"{name}/topk_h"], g[f"{name}/topk_r"], p, P)
+    for k in ("summed_b", "summed_y", "matched_b", "matched_y", "longest_b", "longest_y"):
+        assert np.array_equal(out["k2"][k][:nc].cpu().numpy(), k2o[k]), k
+    assert np.array_equal(out["k2"]["ppm"][:nc].cpu().numpy(), k2o["ppm"], equal_nan=True)
+    np.testing.assert_allclose(out["k2"]["hyperscore"][:nc].cpu().numpy(), k2o["hyperscore"], rtol=1e-12)
+    # the PSM table == the reference's psm_table
+    cols = ("spec_idx", "rank", "pf_row", "pf_id", "charge", "isotope_error", "expmass", "calcmass",
+            "delta_mass_ppm", "matched_b", "matched_y", "matched_peaks", "summed_intensity", "longest_b",
+            "longest_y", "longest_y_pct", "peptide_len", "missed_cleavages", "n_var", "k1_count",
+            "scored_candidates", "average_ppm")
+    for c in cols:
+        assert np.array_equal(tbl.column(c).to_numpy(), g[f"{name}/psm_{c}"], equal_nan=True), c
+    for c in ("hyperscore", "delta_next", "delta_best", "poisson"):
+        np.testing.assert_allclose(tbl.column(c).to_numpy(), g[f"{name}/psm_{c}"], rtol=1e-9, atol=1e-12)
+    # the TIC is an f64 sum rounded to f32 whose summation order differs from the reference's
+    np.testing.assert_allclose(tbl.column("matched_intensity_pct").to_numpy(), g[f"{name}/psm_matched_intensity_pct"],
+                               rtol=1e-6)
+
+
+@pytest.mark.parametrize("name", SETS)
+def test_compat_entry_points_equal_reference_kernels(mini, golden_py, golden_kernels, param_sets, indexes, name,
+                                                     torch_cuda):
+    """The reference-named entry points (vk_frag_count/emit, vk_k1 over the reference CSR, vk_k1_brute,
+    vk_k2, vk_k2_shift) reproduce the reference's kernels exactly."""
+    torch = torch_cuda
+    from vulcan.gpu import _lib as K
+    from vulcan.gpu import engine as E
+    l1, sp, _ = mini
+    p = param_sets[name]
+    gi = indexes[name]
+    g = golden_py
+    L = K.lib()
+    # the process-wide constants of the compatible entry points follow the last index built; set this one's
+    stat = np.array(gi.fp.stat[:], np.float32)
+    var = np.array(gi.fp.var[:], np.float32)
+    K.check(L.vk_set_params(E.SAGE_MONO.ctypes.data, stat.ctypes.data, var.ctypes.data), "set_params")
+    K.check(L.vk_set_tol_da(gi.fp.tol_da), "set_tol_da")
+    n = gi.n
+    cnt = torch.empty(n, dtype=torch.int32, device=gi.dev)
+    K.check(L.vk_frag_count(n, *gi.table_ptrs(), p.min_ion_index, p.fragment_min_mz, p.fragment_max_mz, K.ptr(cnt),
+                            K.stream()), "frag_count")
+    assert np.array_equal(cnt.cpu().numpy(), golden_kernels[f"{name}/frag_count"])
+    gi._slices = None
+    sl = gi.slices
+    assert len(sl) == 1
+    dev = gi.dev
+    up = lambda a, dt: torch.from_numpy(np.ascontiguousarray(a, dtype=dt)).to(dev)
+    pk_off, pk_mass = up(g[f"{name}/k0_off"], np.int64), up(g[f"{name}/k0_mass"], np.float32)
+    pk_int = up(g[f"{name}/k0_int"], np.float32)
+    d_spec, d_maxfz = up(g[f"{name}/hyp_spec"], np.int32), up(g[f"{name}/hyp_maxfz"], np.int8)
+    wi = {k: up(g[f"{name}/wi_{k}"], np.int32) for k in ("hyp", "chunk", "lo", "hi")}
+    cap = max(1, int((g[f"{name}/hyp_hi"] - g[f"{name}/hyp_lo"]).clip(0).sum()))
+    n_out = torch.zeros(1, dtype=torch.int64, device=dev)
+    o_h, o_r, o_c = (torch.empty(cap, dtype=torch.int32, device=dev) for _ in range(3))
+    n_h = len(g[f"{name}/hyp_spec"])
+    scored = torch.zeros(n_h, dtype=torch.int32, device=dev)
+    matched = torch.zeros(n_h, dtype=torch.int64, device=dev)
+    K.check(L.vk_k1(len(g[f"{name}/wi_hyp"]), K.ptr(wi["hyp"]), K.ptr(wi["chunk"]), K.ptr(wi["lo"]), K.ptr(wi["hi"]),
+                    K.ptr(d_spec), K.ptr(d_maxfz), K.ptr(pk_off), K.ptr(pk_mass), K.ptr(sl[0].offsets),
+                    K.ptr(sl[0].entries), gi.n_bins, 0, p.chunk_size, p.tile, p.fragment_ppm[0], p.fragment_ppm[1],
+                    p.fragment_min_mz, gi.inv_logw, 1, cap, K.ptr(n_out), K.ptr(o_h), K.ptr(o_r), K.ptr(o_c),
+                    K.ptr(scored), K.ptr(matched), K.stream()), "k1")
+    m = int(n_out.item())
+    key = (o_h[:m].long() << 32) | o_r[:m].long()
+    o = torch.argsort(key)
+    assert np.array_equal(key[o].cpu().numpy(), golden_kernels[f"{name}/k1_key"])
+    assert np.array_equal(o_c[:m][o].cpu().numpy(), golden_kernels[f"{name}/k1_cnt"])
+    assert np.array_equal(scored.cpu().numpy(), golden_kernels[f"{name}/k1_scored"])
+    assert np.array_equal(matched.cpu().numpy(), golden_kernels[f"{name}/k1_matched"])
+    h, r = up(g[f"{name}/win_h"], np.int64), up(g[f"{name}/win_r"], np.int64)
+    bc = E.k1_brute(gi, _hyp(g, name), {"off": pk_off, "mass": pk_mass}, h, r, p)
+    assert np.array_equal(bc.cpu().numpy(), golden_kernels[f"{name}/brute"])
+    peaks = {"off": pk_off, "mass": pk_mass, "int": pk_int}
+    for mode in ("closed", "shift"):
+        shift = up(golden_kernels[f"{name}/k2shift_delta"], np.float32) if mode == "shift" else None
+        k2 = E.run_k2(gi, h, r, d_spec, d_maxfz, peaks, p, shift=shift)
+        for a, b in (("summed_b", "sb"), ("summed_y", "sy"), ("matched_b", "mb"), ("matched_y", "my"),
+                     ("longest_b", "lb"), ("longest_y", "ly"), ("hyperscore", "hs")):
+            assert np.array_equal(k2[a].cpu().numpy(), golden_kernels[f"{name}/k2{mode}_{b}"]), (mode, a)
+        assert np.array_equal(k2["ppm"].cpu().numpy(), golden_kernels[f"{name}/k2{mode}_ppm"], equal_nan=True)
+
+
+@pytest.mark.parametrize("name", SETS)
+def test_k2_spectra_shift_equals_reference(mini, golden_py, golden_kernels, param_sets, indexes, name, torch_cuda):
+    """The B200 K2 entry point (constants by value) in shifted mode == the reference's vk_k2_shift."""
+    torch = torch_cuda
+    from vulcan.gpu import _lib as K
+    from vulcan.gpu import engine as E
+    gi = indexes[name]
+    p = param_sets[name]
+    g = golden_py
+    dev = gi.dev
+    up = lambda a, dt: torch.from_numpy(np.ascontiguousarray(a, dtype=dt)).to(dev)
+    h = g[f"{name}/win_h"]
+    spec = g[f"{name}/hyp_spec"][h].astype(np.int64)
+    n_spec = len(g[f"{name}/k0_off"]) - 1
+    cand_off = np.zeros(n_spec + 1, np.int64)
+    np.cumsum(np.bincount(spec, minlength=n_spec), out=cand_off[1:])
+    out = E._k2_outputs(len(h), dev)
+    # every device array stays referenced until the asynchronous launch has finished
+    d_off, d_row = up(cand_off, np.int64), up(g[f"{name}/win_r"], np.int32)
+    d_mfz, d_pko = up(g[f"{name}/hyp_maxfz"][h], np.int8), up(g[f"{name}/k0_off"], np.int64)
+    d_pkm, d_pki = up(g[f"{name}/k0_mass"], np.float32), up(g[f"{name}/k0_int"], np.float32)
+    d_shift = up(golden_kernels[f"{name}/k2shift_delta"], np.float32)
+    K.check(K.lib().vk_k2_spectra(C.byref(gi.fp), n_spec, K.ptr(d_off), K.ptr(d_row), K.ptr(d_mfz), K.ptr(d_pko),
+                                  K.ptr(d_pkm), K.ptr(d_pki), *gi.table_ptrs(), p.fragment_ppm[0], p.fragment_ppm[1],
+                                  K.ptr(d_shift), *E._k2_ptrs(out), K.stream()), "k2_spectra")
+    torch.cuda.synchronize()
+    for a, b in (("summed_b", "sb"), ("summed_y", "sy"), ("matched_b", "mb"), ("matched_y", "my"),
+                 ("longest_b", "lb"), ("longest_y", "ly"), ("hyperscore", "hs")):
+        assert np.array_equal(out[a].cpu().numpy(), golden_kernels[f"{name}/k2shift_{b}"]), a
+
+
+def test_topk_radix_selection_path(mini, param_sets, torch_cuda):
+    """topk far below the appended count forces the radix-select path; result == oracle select_topk."""
+    from oracle import oracle as O
+    from vulcan.gpu import engine as E
+    import dataclasses
+    l1, sp, _ = mini
+    for k in (1, 2, 3):
+        p = dataclasses.replace(param_sets["ppm"], topk=k)
+        gi = E.GpuIndex(l1, p, STATIC, VAR)
+        tbl, st, out = E.search(sp, gi, l1, p)
+        pk = O.k0_view(sp, p)
+        hyp = O.make_hypotheses(sp, pk["valid"], l1.mass32, p)
+        P = O.make_params(STATIC, VAR, p.fragment_unit)
+        win_off, cnt, sc, mt = O.k1_windows(l1, hyp, pk, p, P)
+        oh, orr, oc = O.k1_appended(hyp, win_off, cnt, p.k1_threshold)
+        H, R, Cc = O.select_topk(oh, orr, oc, hyp["spec"], l1.partner, p.topk)
+        nc = int(out["cand_off"][-1])
+        assert np.array_equal(out["c_hyp"][:nc].cpu().numpy(), H)
+        assert np.array_equal(out["c_row"][:nc].cpu().numpy(), R)
+        assert np.array_equal(out["c_cnt"][:nc].cpu().numpy(), Cc)
+
+
+def test_search_finds_planted_truth(mini, param_sets, indexes):
+    from vulcan.gpu import engine as E
+    l1, sp, fx = mini
+    tbl, _, _ = E.search(sp, indexes["da"], l1, param_sets["da"])
+    top = dict(zip(tbl.column("spec_idx").to_pylist(), tbl.column("pf_row").to_pylist()))
+    rows = fx["truth_rows"]
+    hit = np.mean([top.get(i) == r for i, r in enumerate(rows)])
+    assert hit > 0.9
+
+
+def test_search_is_deterministic(mini, param_sets, indexes):
+    from vulcan.gpu import engine as E
+    l1, sp, _ = mini
+    a = E.search(sp, indexes["ppm"], l1, param_sets["ppm"], report=5)[0]
+    b = E.search(sp, indexes["ppm"], l1, param_sets["ppm"], report=5)[0]
+    assert a.equals(b)

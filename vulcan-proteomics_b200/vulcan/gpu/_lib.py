@@ -96,9 +96,13 @@ def stream():
 
 
 _TRACE = os.environ.get("VK_TRACE") == "1"
+# kernels launched by one successful call of an entry point (default 1); `LAUNCHES` counts them
+_KERNELS_PER_CALL = {"scan": 3, "set_params": 0, "set_nterm": 0, "set_tol_da": 0, "tindex_layout": 0}
+LAUNCHES = {"n": 0}
 
 
 def check(code: int, what: str):
+    LAUNCHES["n"] += _KERNELS_PER_CALL.get(what, 1) if code == 0 else 0
     if code != 0:
         raise RuntimeError(f"{what}: CUDA error {code}" if code > 0 else f"{what}: rejected argument ({code})")
     if _TRACE:   # debugging aid: finish every launch and report the stage before the next one

@@ -77,42 +77,80 @@ def cleavage_sites(seq: str, cleave_at: str, restrict: str | None, c_terminal: b
 
 def digest_fasta(fasta_text: str, missed_cleavages: int, min_len: int, max_len: int, cleave_at: str,
                  restrict: str | None, c_terminal: bool) -> dict:
+    """Tryptic-style digestion of every protein (vectorised over the whole proteome)."""
     prots = parse_fasta(fasta_text)
     accessions = [a for a, _ in prots]
-    best: dict[str, list] = {}
-    nonstd: set[str] = set()
-    for pi, (_, seq) in enumerate(prots):
-        sites = cleavage_sites(seq, cleave_at, restrict, c_terminal)
-        ns = len(sites)
-        all_std = _is_standard(seq)
-        for a in range(ns - 1):
-            for m in range(missed_cleavages + 1):
-                b = a + 1 + m
-                if b >= ns:
-                    break
-                pep = seq[sites[a]:sites[b]]
-                if not (min_len <= len(pep) <= max_len):
-                    continue
-                if not all_std and not _is_standard(pep):
-                    nonstd.add(pep)
-                    continue
-                key = pep.replace("I", "L")
-                e = best.get(key)
-                if e is None:
-                    best[key] = [m, [pi]]
-                else:
-                    e[0] = min(e[0], m)
-                    e[1].append(pi)
-    keys = sorted(best)
-    missed = np.array([best[k][0] for k in keys], np.uint8)
-    prot_off = np.zeros(len(keys) + 1, np.int64)
-    idx = []
-    for i, k in enumerate(keys):
-        ps = sorted(set(best[k][1]))
-        idx.extend(ps)
-        prot_off[i + 1] = len(idx)
-    return {"keys": keys, "missed": missed, "prot_off": prot_off, "prot_idx": np.array(idx, np.uint32),
-            "accessions": accessions, "n_nonstandard": len(nonstd)}
+    seqs = [q for _, q in prots]
+    n_prot = len(seqs)
+    plen = np.fromiter((len(q) for q in seqs), np.int64, n_prot)
+    buf = np.frombuffer("".join(seqs).encode(), np.uint8)
+    pstart = np.zeros(n_prot + 1, np.int64)
+    np.cumsum(plen, out=pstart[1:])
+    pid = np.repeat(np.arange(n_prot), plen)
+    cut = np.zeros(256, bool)
+    cut[np.frombuffer(cleave_at.encode(), np.uint8)] = True
+    rst = np.zeros(256, bool)
+    if restrict:
+        rst[np.frombuffer(restrict.encode(), np.uint8)] = True
+    nb = len(buf)
+    if c_terminal:
+        # site after position i when buf[i] cleaves, buf[i+1] is not restricted, and i+1 is in the same protein
+        ok = cut[buf[:-1]] & ~rst[buf[1:]] & (pid[:-1] == pid[1:]) if nb > 1 else np.zeros(0, bool)
+        site_g = np.flatnonzero(ok) + 1
+    else:
+        ok = cut[buf[1:]] & ~rst[buf[:-1]] & (pid[:-1] == pid[1:]) if nb > 1 else np.zeros(0, bool)
+        site_g = np.flatnonzero(ok) + 1
+    # sites per protein: start, internal sites, end; ordered by (protein, position)
+    s_pos = np.concatenate([pstart[:-1], site_g, pstart[1:]])
+    s_pid = np.concatenate([np.arange(n_prot), pid[site_g], np.arange(n_prot)])
+    s_end = np.concatenate([np.zeros(n_prot, bool), np.zeros(len(site_g), bool), np.ones(n_prot, bool)])
+    o = np.lexsort((s_end, s_pos, s_pid))
+    s_pos, s_pid = s_pos[o], s_pid[o]
+    starts, ends, miss = [], [], []
+    ns = len(s_pos)
+    for m in range(missed_cleavages + 1):
+        if ns <= 1 + m:
+            break
+        a = np.arange(ns - 1 - m)
+        b = a + 1 + m
+        same = s_pid[a] == s_pid[b]
+        a, b = a[same], b[same]
+        ln = s_pos[b] - s_pos[a]
+        keep = (ln >= min_len) & (ln <= max_len)
+        starts.append(s_pos[a][keep])
+        ends.append(s_pos[b][keep])
+        miss.append(np.full(int(keep.sum()), m, np.int64))
+    st = np.concatenate(starts) if starts else np.zeros(0, np.int64)
+    en = np.concatenate(ends) if ends else np.zeros(0, np.int64)
+    mi = np.concatenate(miss) if miss else np.zeros(0, np.int64)
+    pp = pid[st] if len(st) else np.zeros(0, np.int64)
+    # non-standard residues
+    bad = np.concatenate([[0], np.cumsum(~_STD[buf])])
+    nonstd = (bad[en] - bad[st]) > 0
+    width = int((en - st).max()) if len(st) else 1
+    col = np.arange(width)
+    lens = en - st
+
+    def fixed(sel, table):
+        idx = st[sel][:, None] + col[None, :]
+        valid = col[None, :] < lens[sel][:, None]
+        mat = np.where(valid, table[np.minimum(idx, nb - 1)], 0).astype(np.uint8)
+        return np.ascontiguousarray(mat).view(f"S{width}").ravel()
+    n_nonstd = len(np.unique(fixed(nonstd, buf))) if nonstd.any() else 0
+    il = buf.copy()
+    il[il == ord("I")] = ord("L")
+    good = ~nonstd
+    keys_b = fixed(good, il)
+    uk, inv = np.unique(keys_b, return_inverse=True)
+    missed = np.full(len(uk), 255, np.int64)
+    np.minimum.at(missed, inv, mi[good])
+    pk = np.unique(inv.astype(np.int64) * (n_prot + 1) + pp[good])
+    ki, pi = pk // (n_prot + 1), pk % (n_prot + 1)
+    prot_off = np.zeros(len(uk) + 1, np.int64)
+    np.cumsum(np.bincount(ki, minlength=len(uk)), out=prot_off[1:])
+    keys = [k.decode() for k in uk.tolist()]
+    return {"keys": keys, "missed": missed.astype(np.uint8), "prot_off": prot_off,
+            "prot_idx": pi.astype(np.uint32), "accessions": accessions, "n_nonstandard": int(n_nonstd)}
 
 
 def _mod_tables(static_mods, var_mods):

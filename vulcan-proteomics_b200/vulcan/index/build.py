@@ -69,10 +69,25 @@ def content_hash(fasta_paths, params) -> str:
 
 
 def _pair_perm(fwd: str, perm) -> np.ndarray:
+    """Explicit permutation array of a pair (the pseudo-reverse one when perm is None)."""
     if perm is not None:
         return np.asarray(perm, np.uint8)
     n = len(fwd)
     return np.array([n - 2 - j for j in range(n - 1)] + [n - 1], np.uint8)
+
+
+def _string_column(strs: list[str], order: np.ndarray) -> pa.Array:
+    """Arrow string column of strs[order] built from one byte buffer and an offsets buffer."""
+    data = np.frombuffer("".join(strs).encode(), np.uint8)
+    ln = np.fromiter((len(q) for q in strs), np.int64, len(strs))
+    off = np.zeros(len(strs) + 1, np.int64)
+    np.cumsum(ln, out=off[1:])
+    ln_s = ln[order]
+    off_s = np.zeros(len(order) + 1, np.int64)
+    np.cumsum(ln_s, out=off_s[1:])
+    gather = np.repeat(off[:-1][order] - off_s[:-1], ln_s) + np.arange(off_s[-1])
+    body = data[gather]
+    return pa.Array.from_buffers(pa.large_string(), len(order), [None, pa.py_buffer(off_s), pa.py_buffer(body)])
 
 
 def build(fasta_paths, out_dir: str, params: dict | None = None, workers: int | None = None,
@@ -88,7 +103,6 @@ def build(fasta_paths, out_dir: str, params: dict | None = None, workers: int | 
     dg = core.digest_fasta(text, e["missed_cleavages"], e["min_len"], e["max_len"], e["cleave_at"],
                            e["restrict"], e["c_terminal"])
     targets = list(dg["keys"])
-    t_missed = dict(zip(targets, dg["missed"].tolist()))
     timing["digest_s"] = time.perf_counter() - t0
 
     t1 = time.perf_counter()
@@ -108,23 +122,28 @@ def build(fasta_paths, out_dir: str, params: dict | None = None, workers: int | 
     t2 = time.perf_counter()
     fw = forward
     dc = [dec[f][0] for f in fw]
-    perms = [_pair_perm(f, dec[f][1]) for f in fw]
     order = np.arange(len(fw))
     if shuffle_rows_seed is not None:
         order = np.random.default_rng(shuffle_rows_seed).permutation(len(fw))
     a_seq = [fw[i] for i in order]
     b_seq = [dc[i] for i in order]
-    pr = [perms[i] for i in order]
+    # explicit permutations only for shuffled decoys; an empty slice is the pseudo-reverse
+    perm_lists = [dec[fw[i]][1] for i in order]
     if swap_labels:
         a_seq, b_seq = b_seq, a_seq
-        pr = [np.argsort(q).astype(np.uint8) for q in pr]
-    poff = np.zeros(len(pr) + 1, np.int64)
-    np.cumsum([len(q) for q in pr], out=poff[1:])
-    pflat = np.concatenate(pr).astype(np.uint8) if pr else np.zeros(0, np.uint8)
+        perm_lists = [np.argsort(_pair_perm(b_seq[j], q)).astype(np.uint8) if q is not None else None
+                      for j, q in enumerate(perm_lists)]
+        # the inverse of the pseudo-reverse permutation is itself, so None stays None
+    plens = np.fromiter((0 if q is None else len(q) for q in perm_lists), np.int64, len(perm_lists))
+    poff = np.zeros(len(perm_lists) + 1, np.int64)
+    np.cumsum(plens, out=poff[1:])
+    explicit = [q for q in perm_lists if q is not None]
+    pflat = np.concatenate(explicit).astype(np.uint8) if explicit else np.zeros(0, np.uint8)
     smods = sorted(p["static_mods"].items())
     vmods = sorted(p["variable_mods"].items())
     r = core.expand_pairs(a_seq, b_seq, pflat, poff, smods, vmods, p["max_variable_mods"],
-                          p["peptide_min_mass"], p["peptide_max_mass"], p["id_seed"])
+                          p["peptide_min_mass"], p["peptide_max_mass"], p["id_seed"],
+                          site_limits=p.get("site_limits"))
     timing["expand_s"] = time.perf_counter() - t2
 
     t3 = time.perf_counter()
@@ -132,7 +151,7 @@ def build(fasta_paths, out_dir: str, params: dict | None = None, workers: int | 
     seq_i = r["seq"].astype(np.int64)
     a_bytes = np.frombuffer("".join(a_seq).encode(), np.uint8)
     b_bytes = np.frombuffer("".join(b_seq).encode(), np.uint8)
-    lens = np.array([len(s) for s in a_seq], np.int64)
+    lens = np.fromiter((len(q) for q in a_seq), np.int64, len(a_seq))
     a_off = np.zeros(len(a_seq) + 1, np.int64)
     np.cumsum(lens, out=a_off[1:])
     residues = np.concatenate([a_bytes, b_bytes])
@@ -142,8 +161,12 @@ def build(fasta_paths, out_dir: str, params: dict | None = None, workers: int | 
     length = np.concatenate([lens[seq_i], lens[seq_i]]).astype(np.uint8)
     mask = np.concatenate([r["mask_f"], r["mask_d"]])
     n_var = np.concatenate([r["n_var"], r["n_var"]])
-    fwd_of = [x if not swap_labels else y for x, y in zip(a_seq, b_seq)]
-    missed_seq = np.array([t_missed[fwd_fam[f][2]] for f in fwd_of], np.uint8)
+    # missed cleavages: the forward target's digest count, a pair attribute
+    fw_arr = np.asarray(fw, dtype=object)
+    tgt_of_fw = np.asarray([fwd_fam[f][2] for f in fw], dtype=object) if ent_stats else fw_arr
+    tgt_index = {t: i for i, t in enumerate(targets)}
+    missed_fw = dg["missed"][np.fromiter((tgt_index[t] for t in tgt_of_fw), np.int64, len(fw))]
+    missed_seq = missed_fw[order]
     missed = np.concatenate([missed_seq[seq_i], missed_seq[seq_i]])
     side_b = np.concatenate([np.zeros(n_pairs, bool), np.ones(n_pairs, bool)])
     if len(np.unique(pf_id)) != len(pf_id):
@@ -170,18 +193,22 @@ def build(fasta_paths, out_dir: str, params: dict | None = None, workers: int | 
     })
     timing["arrays_s"] = time.perf_counter() - t3
 
-    fam_fwd = np.array([FAMILY[fwd_fam[f][0]] for f in fw], np.uint8)[order]
-    seed_fwd = np.array([fwd_fam[f][1] for f in fw], np.int32)[order]
-    tgt_fwd = np.array([fwd_fam[f][2] for f in fw], dtype=object)[order]
-    fwd_seq = np.array(fw, dtype=object)[order]
+    fam_fw = np.fromiter((FAMILY[fwd_fam[f][0]] for f in fw), np.uint8, len(fw)) if ent_stats else \
+        np.zeros(len(fw), np.uint8)
+    seed_fw = np.fromiter((fwd_fam[f][1] for f in fw), np.int32, len(fw)) if ent_stats else np.zeros(len(fw), np.int32)
+    fam_fwd, seed_fwd = fam_fw[order], seed_fw[order]
     is_dec = side_b if not swap_labels else ~side_b
     fam_side = np.concatenate([fam_fwd[seq_i], fam_fwd[seq_i]])
     fam = np.where(is_dec, fam_side + 2, fam_side)
     fwd_member_id = np.where(is_dec, pf_id[partner_unsorted], pf_id)
-    tseq = np.concatenate([tgt_fwd[seq_i], tgt_fwd[seq_i]])
-    ep = np.array([int.from_bytes(hashlib.blake2b(t.encode(), digest_size=8).digest(), "little")
-                   for t in tgt_fwd], np.uint64)
+    tgt_pairs = [tgt_of_fw[i] for i in order.tolist()]
+    ep = np.fromiter((int.from_bytes(hashlib.blake2b(t.encode(), digest_size=8).digest(), "little")
+                      for t in tgt_pairs), np.uint64, len(tgt_pairs))
     ep = np.concatenate([ep[seq_i], ep[seq_i]])
+    # string columns straight from byte buffers: the forward (true-label) sequence and its target of every row
+    fwd_strs = [x if not swap_labels else y for x, y in zip(a_seq, b_seq)]
+    fwd_col = _string_column([fwd_strs[i] for i in seq_i.tolist()] * 2, srt)
+    tgt_col = _string_column([tgt_pairs[i] for i in seq_i.tolist()] * 2, srt)
     lab = pa.table({
         "pf_id": pa.array(pf_id[srt], pa.uint64()),
         "family": pa.array(fam[srt].astype(np.uint8)),
@@ -190,8 +217,8 @@ def build(fasta_paths, out_dir: str, params: dict | None = None, workers: int | 
         "is_entrapment": pa.array((fam[srt] % 2) == 1),
         "tdc_pair": pa.array(fwd_member_id[srt], pa.uint64()),
         "entrap_pair": pa.array(ep[srt], pa.uint64()),
-        "fwd_seq": pa.array(np.concatenate([fwd_seq[seq_i], fwd_seq[seq_i]])[srt].tolist(), pa.string()),
-        "target_seq": pa.array(tseq[srt].tolist(), pa.string()),
+        "fwd_seq": fwd_col,
+        "target_seq": tgt_col,
     })
     prot = pa.table({
         "peptide": pa.array(targets, pa.string()),

@@ -49,13 +49,24 @@ def hash_shuffle(pep: str, seed: int, attempt: int = 0) -> str:
     return apply_perm(pep, hash_shuffle_perm(pep, seed, attempt))
 
 
-def make_decoys(forward: list[str], seed: int = DECOY_SEED, max_tries: int = 50):
-    """Pseudo-reverse decoys of every forward peptide, hash shuffles on collision.
+def _pseudo_reverse_all(peps: list[str]) -> list[str]:
+    """pseudo_reverse of every peptide, vectorised over a fixed-width byte matrix."""
+    if not peps:
+        return []
+    lens = np.fromiter((len(q) for q in peps), np.int64, len(peps))
+    w = int(lens.max())
+    flat = np.frombuffer("".join(peps).encode(), np.uint8)
+    off = np.zeros(len(peps) + 1, np.int64)
+    np.cumsum(lens, out=off[1:])
+    col = np.arange(w)
+    # source column of output column j: n-2-j for j < n-1, n-1 for j = n-1
+    src = np.where(col[None, :] < lens[:, None] - 1, lens[:, None] - 2 - col[None, :], lens[:, None] - 1)
+    valid = col[None, :] < lens[:, None]
+    mat = np.where(valid, flat[np.clip(off[:-1, None] + src, 0, len(flat) - 1)], 0).astype(np.uint8)
+    return [x.decode() for x in np.ascontiguousarray(mat).view(f"S{w}").ravel().tolist()]
 
-    Returns ``({forward: (decoy, perm or None)}, n_shuffled)``; ``perm`` None means the pseudo-reverse.
-    Follows ``vulcan/index/decoys.py:109-132``: attempts ``k = 0 .. max_tries-1`` are tried in turn and a peptide
-    whose every attempt collides gets no decoy.
-    """
+
+def _make_decoys_sequential(forward: list[str], seed: int, max_tries: int):
     fwd = set(forward)
     used: set[str] = set()
     out: dict[str, tuple[str, np.ndarray | None]] = {}
@@ -76,6 +87,47 @@ def make_decoys(forward: list[str], seed: int = DECOY_SEED, max_tries: int = 50)
             out[pep] = (dec, perm)
             used.add(dec)
     return out, n_shuffled
+
+
+def make_decoys(forward: list[str], seed: int = DECOY_SEED, max_tries: int = 50):
+    """Pseudo-reverse decoys of every forward peptide, hash shuffles on collision.
+
+    Returns ``({forward: (decoy, perm or None)}, n_shuffled)``; ``perm`` None means the pseudo-reverse.
+    Follows ``vulcan/index/decoys.py:109-132``: peptides in sorted order; a decoy that equals its peptide, any
+    forward peptide, or an earlier decoy is replaced by shuffle attempts ``k = 0 .. max_tries-1``; a peptide whose
+    every attempt collides gets no decoy.  Pseudo-reverses of distinct peptides are distinct, so only the colliding
+    peptides need the sequential rule; if a shuffle lands on a later peptide's pseudo-reverse, the whole list is
+    redone sequentially.
+    """
+    srt = sorted(set(forward))
+    rev = _pseudo_reverse_all(srt)
+    fwd = set(srt)
+    bad = [i for i, (q, d) in enumerate(zip(srt, rev)) if d == q or d in fwd]
+    out = {q: (d, None) for q, d in zip(srt, rev)}
+    if not bad:
+        return out, 0
+    rev_pos = {d: i for i, d in enumerate(rev)}
+    bad_set = set(bad)
+    shuffled: set[str] = set()
+    for i in bad:
+        pep = srt[i]
+        dec, perm, attempt = rev[i], None, 0
+        while (dec == pep or dec in fwd or dec in shuffled or
+               (dec in rev_pos and rev_pos[dec] < i and rev_pos[dec] not in bad_set)):
+            if attempt >= max_tries:
+                dec = None
+                break
+            perm = hash_shuffle_perm(pep, seed, attempt)
+            dec = apply_perm(pep, perm)
+            attempt += 1
+        if dec is None:
+            del out[pep]
+            continue
+        if dec in rev_pos and rev_pos[dec] > i and rev_pos[dec] not in bad_set:
+            return _make_decoys_sequential(srt, seed, max_tries)
+        out[pep] = (dec, perm)
+        shuffled.add(dec)
+    return out, len(bad)
 
 
 def make_entrapment(targets: list[str], seed: int, taken: set[str], workers: int = 1, max_tries: int = 200):
