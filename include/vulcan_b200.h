@@ -26,6 +26,7 @@ extern "C" {
 
 #define VK_E_ARG (-1)       /* invalid argument (size, alignment, layout limit) */
 #define VK_E_CAPACITY (-2)  /* an output buffer is too small; the needed size was written where documented */
+#define VK_E_TOO_LARGE (-3) /* the input is larger than a fixed-size internal buffer allows */
 
 /* ============================================================ Part 1: reference-compatible entry points */
 
@@ -128,6 +129,22 @@ int vk_tindex_emit(const vk_tindex* ix, const vk_frag_params* fp, const int64_t*
  * is allowed).  Uses `tmp` of vk_scan_tmp_bytes(n) bytes. */
 int64_t vk_scan_tmp_bytes(int64_t n);
 int vk_scan_i64(const int64_t* in, int64_t n, int64_t* out, void* tmp, void* stream);
+
+/* The same exclusive scan without the caller's scratch buffer; it allocates nothing.  No counterpart in the
+ * reference.  For callers that cannot allocate device memory on this path: a foreign-language binding (cgo, JNI,
+ * plain C) that holds only the input and output buffers and has no device allocator to hand out scratch, or a
+ * stage thread that must not call cudaMalloc / cudaFree because they synchronise the whole device and would stall
+ * the other streams' searches.
+ *   - Scratch: the block partial sums live in one fixed device array inside the library (64 KiB on every device
+ *     that loads it, held until the process exits).  n may be at most vk_scan_noalloc_max_n() = 33,554,432;
+ *     larger n returns VK_E_TOO_LARGE and launches nothing.
+ *   - Set-up: the first call on a device looks up the array's device address (cudaGetSymbolAddress) with that
+ *     device current and keeps it; make that first call before any stream capture.
+ *   - Sharing: every call on a device uses the same array.  Calls whose kernels may overlap on the GPU (other
+ *     streams, other host threads) race on it and give wrong sums; order them (one stream, or events).
+ *     Nothing in the array has to start at zero; each call overwrites what it reads. */
+int64_t vk_scan_noalloc_max_n(void);
+int vk_scan_i64_noalloc(const int64_t* in, int64_t n, int64_t* out, void* stream);
 
 /* K0 peak view (reference vulcan/gpu/engine.py:171-210), two calls: vk_k0_count writes kept[n_spec] (i64) =
  * min(#peaks with fmin <= mz <= fmax and not NaN, max_peaks); after the caller's scan into pk_off[n_spec+1],

@@ -6,6 +6,8 @@
 // [a, bd] is exactly the key range [bits(a) - base, bits(bd) - base] (shifted): no quantisation, no edge loss.
 // Each tile's postings start at a multiple of 4 entries (16 bytes) so the search can stage a tile with one bulk
 // copy; the padding entries are 0xffffffff and are never inside a key range (see vk_tindex_layout).
+#include <mutex>
+
 #include "common.cuh"
 
 namespace {
@@ -217,6 +219,34 @@ scan_apply_k(const int64_t* in, int64_t n, const int64_t* block_sums, int64_t* o
   if (blockIdx.x == 0 && threadIdx.x == 0) out[0] = 0;
 }
 
+// Scratch of vk_scan_i64_noalloc: the per-block partial sums, in a fixed device array instead of a caller buffer.
+// 8192 blocks of SCAN_TILE (4096) elements: inputs of up to 33,554,432 values; 64 KiB held on every device that
+// loads the library, until the process exits.
+constexpr int64_t NOALLOC_SCAN_BLOCKS = 8192;
+static __device__ __align__(256) int64_t g_scan_scratch[NOALLOC_SCAN_BLOCKS];
+
+// Device address of g_scan_scratch per device.  In host code the array's name is only a stand-in; the address a
+// kernel may use comes from cudaGetSymbolAddress, taken once per device with that device current.
+constexpr int NOALLOC_MAX_DEVICES = 64;
+int64_t* g_scan_scratch_dev[NOALLOC_MAX_DEVICES] = {};
+std::mutex g_scan_scratch_mu;
+
+int scan_scratch_address(int64_t** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return vk_err(e);
+  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return VK_E_ARG;
+  std::lock_guard<std::mutex> lock(g_scan_scratch_mu);
+  if (!g_scan_scratch_dev[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_scan_scratch);
+    if (e != cudaSuccess) return vk_err(e);
+    g_scan_scratch_dev[dev] = static_cast<int64_t*>(p);
+  }
+  *out = g_scan_scratch_dev[dev];
+  return 0;
+}
+
 }  // namespace
 
 extern "C" {
@@ -271,6 +301,24 @@ int vk_tindex_emit(const vk_tindex* ix, const vk_frag_params* fp, const int64_t*
   if (e != cudaSuccess) return vk_err(e);
   tindex_emit_k<<<(unsigned)ix->n_tiles, 512, sh, (cudaStream_t)stream>>>(*ix, *fp, seq_off, len, mask, mass32, res,
                                                                           postings, cbin_off, n_pow2);
+  return vk_launch_status();
+}
+
+int64_t vk_scan_noalloc_max_n(void) { return NOALLOC_SCAN_BLOCKS * SCAN_TILE; }
+
+int vk_scan_i64_noalloc(const int64_t* in, int64_t n, int64_t* out, void* stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  if (n < 0) return VK_E_ARG;
+  if (n > NOALLOC_SCAN_BLOCKS * SCAN_TILE) return VK_E_TOO_LARGE;
+  int64_t* bs = nullptr;
+  int rc = scan_scratch_address(&bs);
+  if (rc != 0) return rc;
+  if (n == 0) return vk_err(cudaMemsetAsync(out, 0, sizeof(int64_t), st));
+  // every block sum is written by scan_reduce_k before it is read: nothing in the scratch has to start at zero
+  int64_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;
+  scan_reduce_k<<<(unsigned)nb, SCAN_THREADS, 0, st>>>(in, n, bs);
+  scan_blocks_k<<<1, SCAN_THREADS, 0, st>>>(bs, nb);
+  scan_apply_k<<<(unsigned)nb, SCAN_THREADS, 0, st>>>(in, n, bs, out);
   return vk_launch_status();
 }
 

@@ -52,6 +52,7 @@ _SIGS_B200 = {
     "vk_tindex_count": [P, P, P, P, P, P, P, P, P],
     "vk_tindex_emit": [P, P, P, P, P, P, P, P, P, P],
     "vk_scan_i64": [P, I64, P, P, P],
+    "vk_scan_i64_noalloc": [P, I64, P, P],
     "vk_k0_count": [I32, P, P, F32, F32, I32, P, P],
     "vk_k0_fill": [I32, P, P, P, F32, F32, I32, I32, P, P, P, P, P, I32, P],
     "vk_hyp_count": [I32, P, P, P, I32, I32, I32, I32, P, P],
@@ -80,6 +81,8 @@ def lib():
         f.restype = C.c_int
     L.vk_scan_tmp_bytes.argtypes = [I64]
     L.vk_scan_tmp_bytes.restype = I64
+    L.vk_scan_noalloc_max_n.argtypes = []
+    L.vk_scan_noalloc_max_n.restype = I64
     _lib = L
     return L
 
