@@ -62,13 +62,25 @@ def _workload_setup(name: str, rank: int):
     return w, l1, sp, t_build
 
 
+def _params(w, a):
+    kw = {"k1_merge": a.k1 == "merge", "search_method": a.method}
+    if a.tile_rows:
+        kw["tile_rows"] = a.tile_rows
+    if a.warps:
+        kw["fused_warps"] = a.warps
+    return w.search_params(**kw)
+
+
 def _config(w, p, extra=None):
     cfg = {"workload": f"{w.name}: {w.n_proteins} random proteins (<= {w.missed_cleavages} missed cleavages, "
                        f"length {w.min_len}-{w.max_len}, CAM-C, Met-ox <= {w.max_var}, pseudo-reverse decoys); "
                        f"runs of {w.n_spectra} simulated MS2 spectra, charge {w.charges[0]}-{w.charges[1]}",
            "path": "plain exhaustive search (K1 -> top-k -> K2), no learned pruner",
+           "method": ("fused persistent kernel (K1+top-k+K2+ranking per spectrum)" if p.search_method == "fused"
+                      else "staged kernels"),
            "precursor_ppm": list(p.precursor_ppm), "fragment_tol": f"+-{p.fragment_ppm[1]} {p.fragment_unit}",
-           "topk": p.topk, "max_peaks": p.max_peaks, "l2": "flushed between steps (256 MiB write)"}
+           "topk": p.topk, "max_peaks": p.max_peaks, "k1": "merge join" if p.k1_merge else "per-peak search",
+           "l2": "flushed between steps (256 MiB write)"}
     if extra:
         cfg.update(extra)
     return cfg
@@ -163,21 +175,49 @@ def cpu_rate(l1, sp, p, budget_s: float):
 
 
 def k1_algorithmic_bytes(gi, dh, peaks, win_off, item_off, item_hyp):
-    """Bytes K1 must move per launch in this layout: each tile with work is read once (postings + coarse-bin CSR);
-    per work item the spectrum's peak masses (4 B each) and the hypothesis record (spec 4, maxfz 1, lo/hi 16,
-    peak offsets 16, item id 4); per window row one 4-byte count written."""
-    import torch
+    """Bytes K1 must move per launch: each tile with work is read once (postings + coarse-bin CSR); per work item
+    the spectrum's peak masses (4 B each) and the hypothesis record (spec 4, maxfz 1, lo/hi 16, peak offsets 16,
+    item id 4); per window row one 4-byte count written."""
     nt = gi.tix.n_tiles
     stride = ((1 << gi.tix.cbin_bits) + 1 + 7) & ~7
-    items_per_tile = item_off[1:] - item_off[:-1]
-    busy = items_per_tile > 0
+    busy = (item_off[1:] - item_off[:-1]) > 0
     tile_bytes = ((gi.tile_off[1:nt + 1] - gi.tile_off[:nt]) * 4 + stride * 2)[busy].sum()
-    h = item_hyp.long()
-    s = dh["spec"][h].long()
-    npk = (peaks["off"][s + 1] - peaks["off"][s])
-    item_bytes = (npk * 4 + 41).sum()
-    out_bytes = win_off[-1] * 4
-    return int((tile_bytes + item_bytes + out_bytes).item())
+    s = dh["spec"][item_hyp.long()].long()
+    item_bytes = ((peaks["off"][s + 1] - peaks["off"][s]) * 4 + 41).sum()
+    return int((tile_bytes + item_bytes + win_off[-1] * 4).item())
+
+
+def fused_algorithmic_bytes(gi, dh, peaks, oc, n_spec):
+    """Bytes the fused search moves per launch: per (hypothesis, tile) item the staged tile (postings + coarse CSR)
+    and the spectrum's peak masses read by the per-peak search (4 B each); per spectrum its peaks staged for K2
+    (8 B each, at most 512) and the hypothesis records (33 B each); per candidate the row gather of K2 (seq_off 8,
+    length 1, mask 8, mass32 4, residues L) and, for the selected entries, the partner row (8); per spectrum the PSM
+    slot written (~100 B)."""
+    import torch
+    ix = gi.tix
+    sh = ix.tile_shift
+    cb = (((1 << ix.cbin_bits) + 1 + 7) & ~7) * 2
+    nh = int(dh["spec_off"][-1])
+    lo, hi = dh["lo"][:nh], dh["hi"][:nh]
+    ok = hi > lo
+    t0 = lo[ok] >> sh
+    t1 = (hi[ok] - 1) >> sh
+    tiles = (t1 - t0 + 1)
+    tile_b = ((gi.tile_off[t1 + 1] - gi.tile_off[t0]) * 4 + tiles * cb).sum()
+    s = dh["spec"][:nh][ok].long()
+    npk = peaks["off"][s + 1] - peaks["off"][s]
+    peak_item_b = (npk * tiles * 4).sum()
+    npk_all = (peaks["off"][1:n_spec + 1] - peaks["off"][:n_spec]).clamp(max=512)
+    spec_b = (npk_all * 8).sum() + nh * 33 + n_spec * 100
+    cd, cap = oc["cand"], oc["cand_cap"]
+    n_cand = cd["n_cand"][:n_spec].clamp(min=0)
+    idx = torch.arange(cap, device=n_cand.device)[None, :] < n_cand[:, None]
+    rows = cd["c_row"][:n_spec * cap].view(n_spec, cap)[idx]
+    cand_b = (21 + gi.length[rows].long()).sum() + n_cand.sum() * 4
+    total = int((tile_b + peak_item_b + spec_b + cand_b).item())
+    return {"total": total, "tiles": int(tile_b.item()), "peaks_per_item": int(peak_item_b.item()),
+            "spectra": int(spec_b.item()), "candidates_gather": int(cand_b.item()), "items": int(tiles.sum().item()),
+            "candidates": int(n_cand.sum().item())}
 
 
 def run_b200(a):
@@ -194,13 +234,15 @@ def run_b200(a):
     from vulcan.gpu import _lib as K
     from vulcan.gpu import engine as E
     w, l1, sp, t_build = _workload_setup(a.workload, rank)
-    p = w.search_params()
+    p = _params(w, a)
     gi = E.GpuIndex(l1, p, STATIC, VAR, device=dev)
     run = E.DeviceRun(sp, dev)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device=dev)   # 256 MiB > 126 MB L2
     st = E.Stats()
 
     def step():
+        if p.search_method == "fused":
+            return E._search_fused_device(run, gi, p, 1, st)
         return E._search_device(run, gi, p, 1, st)
 
     for _ in range(a.warmup):
@@ -232,6 +274,10 @@ def run_b200(a):
     ms_max = float(t.item())
     ms_per_step = ms_max / a.steps
     value = len(sp) * world * a.steps / (ms_max / 1e3)
+    if p.search_method == "fused":
+        st_ok = int(out["status"][:len(sp)].max())
+        if st_ok:
+            raise RuntimeError(f"fused search status {st_ok}: spectra over the window capacity or a copy timeout")
 
     # end to end through the public API (host Spectra in, PSM table out)
     e2e_steps = max(3, min(a.steps, 20))
@@ -250,17 +296,34 @@ def run_b200(a):
         dist.all_reduce(e2e_s, op=dist.ReduceOp.MAX)
     e2e = len(sp) * world * e2e_steps / float(e2e_s.item())
 
-    # per-phase device times (separate pass, phases synchronised) -> dominant kernel
-    st_ph = E.Stats()
-    for _ in range(3):
-        flush.zero_()
-        E._search_device(run, gi, p, 1, st_ph, timers=True)
-    phase_ms = {k: v / 3 for k, v in st_ph.gpu_ms.items()}
-    # the K1 kernel alone: mean launch duration with the plan of this run
-    dh = out["dh"]
-    win_off, cnt = out["win_off"], out["cnt"]
+    # per-phase device times of both methods (separate passes, phases synchronised)
+    phase_ms = {}
+    for method in ("fused", "staged"):
+        st_ph = E.Stats()
+        q = E._replace(p, search_method=method)
+        for _ in range(3):
+            flush.zero_()
+            (E._search_fused_device if method == "fused" else E._search_device)(run, gi, q, 1, st_ph, timers=True)
+        phase_ms[method] = {k: round(v / 3, 4) for k, v in st_ph.gpu_ms.items()}
+    # each main kernel alone (mean CUDA-event duration over 8 launches after 2 warm-up launches, L2 flushed before
+    # each), with its algorithmic bytes; the dominant one goes into `roofline`
     import ctypes as C
     L = K.lib()
+    so = E._search_device(run, gi, p, 1, st)
+    peaks, dh = so["peaks"], so["dh"]
+    peak_gbs, peak_kind = _peaks_json()
+
+    def timed(fn, n=10):
+        ts = []
+        for _ in range(n):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return sum(ts[2:]) / len(ts[2:])
     nt = gi.tix.n_tiles
     tile_items = torch.empty(nt, dtype=torch.int64, device=dev)
     win_len = torch.empty(dh["n_max"], dtype=torch.int64, device=dev)
@@ -273,24 +336,49 @@ def run_b200(a):
     K.check(L.vk_k1_plan_fill(C.byref(gi.tix), dh["n_max"], K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(item_off),
                               K.ptr(cursor), K.ptr(item_hyp), K.stream()), "k1_plan_fill")
     status = torch.zeros(1, dtype=torch.int32, device=dev)
-    peaks = out["peaks"]
-    k1_ms = []
-    for _ in range(10):
-        flush.zero_()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        K.check(L.vk_k1_tiles(C.byref(gi.tix), C.byref(gi.fp), float(p.fragment_ppm[0]), float(p.fragment_ppm[1]),
-                              K.ptr(item_off), K.ptr(item_hyp), K.ptr(dh["spec"]), K.ptr(dh["maxfz"]),
-                              K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(win_off), K.ptr(peaks["off"]),
-                              K.ptr(peaks["mass"]), K.ptr(cnt), K.ptr(status), K.stream()), "k1_tiles")
-        e1.record()
-        torch.cuda.synchronize()
-        k1_ms.append(e0.elapsed_time(e1))
-    k1_mean = sum(k1_ms[2:]) / len(k1_ms[2:])
-    algo = k1_algorithmic_bytes(gi, dh, peaks, win_off, item_off, item_hyp)
-    peak_gbs, peak_kind = _peaks_json()
-    achieved = algo / (k1_mean / 1e3) / 1e9
-    traffic = _traffic_from_profiles("k1_tiles")
+    win_off, cnt = so["win_off"], so["cnt"]
+    kern = {}
+    ms_k1 = timed(lambda: K.check(L.vk_k1_tiles(
+        C.byref(gi.tix), C.byref(gi.fp), float(p.fragment_ppm[0]), float(p.fragment_ppm[1]), E.k1_max_win(p),
+        K.ptr(item_off), K.ptr(item_hyp), K.ptr(dh["spec"]), K.ptr(dh["maxfz"]), K.ptr(dh["lo"]), K.ptr(dh["hi"]),
+        K.ptr(win_off), K.ptr(peaks["off"]), K.ptr(peaks["mass"]), K.ptr(cnt), K.ptr(status), K.stream()),
+        "k1_tiles"))
+    kern["k1_tiles_k"] = (ms_k1, k1_algorithmic_bytes(gi, dh, peaks, win_off, item_off, item_hyp))
+    n = run.n
+    cap = so["cap"]
+    tk = {k: torch.empty(max(n * cap, 1), dtype=torch.int64, device=dev) for k in ("h", "r", "c")}
+    tk_n = torch.empty(n, dtype=torch.int64, device=dev)
+    hs_ = torch.empty(dh["n_max"], dtype=torch.int32, device=dev)
+    hm_ = torch.empty(dh["n_max"], dtype=torch.int64, device=dev)
+    ss_ = torch.empty(n, dtype=torch.int64, device=dev)
+    sm_ = torch.empty(n, dtype=torch.int64, device=dev)
+    ms_tk = timed(lambda: K.check(L.vk_select_topk(
+        n, K.ptr(dh["spec_off"]), K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(win_off), K.ptr(cnt), K.ptr(gi.partner),
+        p.k1_threshold, p.topk, int(p.pair_closure), cap, K.ptr(tk["h"]), K.ptr(tk["r"]), K.ptr(tk["c"]),
+        K.ptr(tk_n), K.ptr(hs_), K.ptr(hm_), K.ptr(ss_), K.ptr(sm_), K.stream()), "select_topk"))
+    n_cand = int(so["cand_off"][-1])
+    n_sel = int(((so["c_cnt"][:n_cand] >= 0)).sum())
+    kern["select_topk_k"] = (ms_tk, int(win_off[-1]) * 4 + n_sel * 8 + n_cand * 24 + dh["n_max"] * 12 + n * 16)
+    k2o = E._k2_outputs(max(n_cand, 1), dev)
+    ms_k2 = timed(lambda: K.check(L.vk_k2_spectra(
+        C.byref(gi.fp), n, K.ptr(so["cand_off"]), K.ptr(so["c_row32"]), K.ptr(so["c_maxfz"]), K.ptr(peaks["off"]),
+        K.ptr(peaks["mass"]), K.ptr(peaks["int"]), *gi.table_ptrs(), float(p.fragment_ppm[0]),
+        float(p.fragment_ppm[1]), None, *E._k2_ptrs(k2o), K.stream()), "k2_spectra"))
+    rows = so["c_row"][:n_cand]
+    npk = (peaks["off"][1:n + 1] - peaks["off"][:n]).clamp(max=512)
+    k2_bytes = int(((21 + gi.length[rows].long() + 5 + 28).sum() + npk.sum() * 8 + n * 16).item())
+    kern["k2_spectra_k"] = (ms_k2, k2_bytes)
+    if p.search_method == "fused":
+        kern = {"fused_search_k": (timed(lambda: E._fused_device(gi, p, 1, peaks, dh, run.n)),
+                                   fused_algorithmic_bytes(gi, dh, peaks, E._fused_device(gi, p, 1, peaks, dh, run.n,
+                                                                                          cand=True), n)["total"])}
+    dom = max(kern, key=lambda k: kern[k][0])
+    k_mean, algo = kern[dom]
+    achieved = algo / (k_mean / 1e3) / 1e9
+    traffic = _traffic_from_profiles(dom[:-2] if dom.endswith("_k") else dom)
+    kernels = {k: {"mean_launch_ms": round(v[0], 4), "algorithmic_bytes": v[1],
+                   "algorithmic_gbs": round(v[1] / (v[0] / 1e3) / 1e9, 1)} for k, v in kern.items()}
+    n_rescored = n_cand
 
     if rank == 0:
         cpu = None
@@ -299,7 +387,6 @@ def run_b200(a):
             cpu = {"value": round(rate, 1), "unit": "spectra/s", "cores": cores, "kind": "port",
                    "sample": f"first {n_s} spectra of the run through the oracle's K0->hypotheses->K1->top-k->K2->"
                              f"ranking ({t_s:.1f} s)"}
-        counts = st.counts
         line = {
             "metric": METRIC, "value": round(value, 1), "unit": "spectra/s", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True, "scaling": "weak",
@@ -310,16 +397,17 @@ def run_b200(a):
             "e2e": {"value": round(e2e, 1), "unit": "spectra/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "hbm", "kernel": "k1_tiles", "achieved": round(achieved, 1),
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1),
                          "peak": peak_gbs, "unit": "GB/s", "frac": round(achieved / peak_gbs, 4),
                          "peak_source": peak_kind, "traffic": traffic, "algorithmic_bytes": algo,
-                         "mean_launch_ms": round(k1_mean, 4)},
+                         "mean_launch_ms": round(k_mean, 4)},
+            "kernels": kernels,
             "cpu_baseline": cpu,
             "clocks": clk,
-            "phase_ms": {k: round(v, 4) for k, v in phase_ms.items()},
+            "phase_ms": phase_ms,
             "index_build_s": round(t_build, 1),
-            "per_step": {"hypotheses": counts.get("n_hypotheses"), "k1_work_items": n_items,
-                         "k1_window_rows": int(win_off[-1]), "rescored": int(out["cand_off"][-1])},
+            "per_step": {"hypotheses": int(dh["spec_off"][-1]), "k1_work_items": n_items,
+                         "k1_window_rows": int(win_off[-1]), "rescored": n_rescored},
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -349,12 +437,15 @@ def run_profile(a):
     from vulcan.gpu import engine as E
     dev = torch.device("cuda", 0)
     w, l1, sp, _ = _workload_setup(a.workload, 0)
-    p = w.search_params()
+    p = _params(w, a)
     gi = E.GpuIndex(l1, p, STATIC, VAR, device=dev)
     run = E.DeviceRun(sp, dev)
     st = E.Stats()
     for _ in range(2):
-        E._search_device(run, gi, p, 1, st)
+        if p.search_method == "fused":
+            E._search_fused_device(run, gi, p, 1, st)
+        else:
+            E._search_device(run, gi, p, 1, st)
     torch.cuda.synchronize()
     print(json.dumps({"profile_passes": 2, "spectra": len(sp), "index_rows": len(l1)}), flush=True)
 
@@ -402,6 +493,11 @@ def main():
     ap.add_argument("--workload", choices=("human", "small"), default="human")
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of CPU-baseline work (rank 0, N=1)")
     ap.add_argument("--cpu-total", type=float, default=120.0, help="seconds of the reference arm in total")
+    ap.add_argument("--method", choices=("staged", "fused"), default="staged",
+                    help="staged: a kernel per stage; fused: one persistent kernel per run after K0 and hypotheses")
+    ap.add_argument("--k1", choices=("merge", "per-peak"), default="per-peak", help="staged K1 search method")
+    ap.add_argument("--warps", type=int, default=None, help="warps per fused-search CTA")
+    ap.add_argument("--tile-rows", type=int, default=None, help="rows per fragment-index tile")
     ap.add_argument("--mode", choices=("bench", "profile"), default="bench",
                     help="profile: set up the workload and run two device passes only (for an ncu capture of one "
                          "kernel launch of the second pass, e.g. -k regex:k1_tiles -s 1 -c 1)")

@@ -177,12 +177,14 @@ int vk_hyp_fill(int n_spec, const uint8_t* valid, const double* precursor_mz, co
  *   vk_k1_tiles:      dense counts cnt[win_off[h] + row - lo[h]] (i32) for every window row of every hypothesis.
  * Counts equal the reference's brute force (kernels.cu:195-232): #(peak p, fragment charge z < maxfz, index
  * fragment f) with tol_bound(p*z, tol_lo) <= f <= tol_bound(p*z, tol_hi) in f32.  `status` (device i32, zeroed by
- * the caller) gets VK_STATUS_WAIT_TIMEOUT if a tile copy did not complete within the bounded wait. */
+ * the caller) gets VK_STATUS_WAIT_TIMEOUT if a tile copy did not complete within the bounded wait.  max_win
+ * (<= 4096) sizes the per-warp window buffer of the merge join: spectra with more peaks use the per-peak search;
+ * 0 selects the per-peak search for every item. */
 int vk_k1_plan_count(const vk_tindex* ix, int64_t n_hyp, const int64_t* h_lo, const int64_t* h_hi,
                      int64_t* tile_items, int64_t* win_len, void* stream);
 int vk_k1_plan_fill(const vk_tindex* ix, int64_t n_hyp, const int64_t* h_lo, const int64_t* h_hi,
                     const int64_t* tile_item_off, int64_t* cursor, int32_t* item_hyp, void* stream);
-int vk_k1_tiles(const vk_tindex* ix, const vk_frag_params* fp, float tol_lo, float tol_hi,
+int vk_k1_tiles(const vk_tindex* ix, const vk_frag_params* fp, float tol_lo, float tol_hi, int max_win,
                 const int64_t* tile_item_off, const int32_t* item_hyp, const int32_t* h_spec,
                 const int8_t* h_maxfz, const int64_t* h_lo, const int64_t* h_hi, const int64_t* win_off,
                 const int64_t* pk_off, const float* pk_mass, int32_t* cnt, int32_t* status, void* stream);
@@ -223,6 +225,81 @@ int vk_k2_spectra(const vk_frag_params* fp, int n_spec, const int64_t* cand_off,
 int vk_psm_rank(int n_spec, const int64_t* cand_off, const int64_t* c_row, const double* hs, const int16_t* mb,
                 const int16_t* my, int min_matched, int report, int64_t* psm_cand, int32_t* psm_rank,
                 double* psm_dnext, double* psm_dbest, int32_t* n_psm, void* stream);
+
+/* ============================================================ Part 3: fused persistent search */
+
+/* Inputs of the fused search.  Spectra are the batch's (global ids 0..n_spec-1, peaks and hypotheses grouped by
+ * spectrum as vk_k0_fill / vk_hyp_fill write them); spec_ids (may be NULL) selects the n_work spectra to search. */
+typedef struct {
+  int n_spec;
+  int n_work;
+  const int32_t* spec_ids;
+  const int64_t* pk_off;
+  const float* pk_mass;
+  const float* pk_int;
+  const int64_t* spec_hyp_off;
+  const int64_t* h_lo;
+  const int64_t* h_hi;
+  const int8_t* h_maxfz;
+  const int64_t* partner;
+  const int64_t* seq_off;
+  const uint8_t* len;
+  const uint64_t* mask;
+  const float* mass32;
+  const uint8_t* res;
+  float tol_lo, tol_hi;
+  int thr, topk, pair_closure, min_matched, report;
+} vk_fused_in;
+
+/* Reported PSMs, slot s*report + k (k < n_psm[s]); row = -1 in unused slots. */
+typedef struct {
+  int64_t* row;
+  int64_t* hyp;
+  int64_t* k1;
+  int32_t* rank;
+  double* dnext;
+  double* dbest;
+  double* hs;
+  float* sb;
+  float* sy;
+  float* ppm;
+  int16_t* mb;
+  int16_t* my;
+  int16_t* lb;
+  int16_t* ly;
+} vk_psm_out;
+
+/* Optional per-candidate outputs, slot s*cap + j (j < n_cand[s], sorted by row); n_cand == NULL: not written;
+ * hs == NULL: K2 outputs not written.  cap >= (pair_closure ? 2 : 1) * topk. */
+typedef struct {
+  int cap;
+  int64_t* n_cand;
+  int64_t* c_hyp;
+  int64_t* c_row;
+  int64_t* c_cnt;
+  double* hs;
+  float* sb;
+  float* sy;
+  float* ppm;
+  int16_t* mb;
+  int16_t* my;
+  int16_t* lb;
+  int16_t* ly;
+} vk_cand_out;
+
+/* Fused search of every work spectrum: K1 -> top-K + pair closure -> K2 -> ranking in one persistent kernel (one
+ * CTA of `warps` warps per spectrum at a time, intermediate state in shared memory; `grid` CTAs, see
+ * vk_search_fused_grid).  Same results as the staged entry points.  cnt_cap = window rows a spectrum may span in
+ * total; spectra over it (or with more than 32 hypotheses) get status bit 1 and no PSMs -- search them with the
+ * staged entry points.  status bit 2: a tile copy timed out.  work_counter (u32) and status (i32[n_spec]) are
+ * zeroed by the call.  hyp_scored / hyp_matched may be NULL. */
+int vk_search_fused(const vk_tindex* ix, const vk_frag_params* fp, const vk_fused_in* in, int warps, int cnt_cap,
+                    int grid, unsigned int* work_counter, int32_t* status, int32_t* n_psm, int64_t* spec_scored,
+                    int64_t* spec_matched, const vk_psm_out* psm, const vk_cand_out* cand, uint32_t* hyp_scored,
+                    uint64_t* hyp_matched, void* stream);
+/* Dynamic shared memory per CTA and the persistent grid size (CTAs resident per SM x SMs) of the fused search. */
+int vk_search_fused_smem(const vk_tindex* ix, int warps, int topk, int pair_closure, int cnt_cap, int64_t* bytes);
+int vk_search_fused_grid(const vk_tindex* ix, int warps, int topk, int pair_closure, int cnt_cap, int* grid);
 
 #ifdef __cplusplus
 }

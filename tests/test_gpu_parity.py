@@ -52,8 +52,9 @@ def test_search_stages_equal_reference(mini, golden_py, golden_kernels, param_se
     """Device hypotheses, dense K1 counts, top-K + closure and K2 of engine.search equal the references."""
     from oracle import oracle as O
     from vulcan.gpu import engine as E
+    import dataclasses
     l1, sp, _ = mini
-    p = param_sets[name]
+    p = dataclasses.replace(param_sets[name], search_method="staged")
     g = golden_py
     tbl, st, out = E.search(sp, indexes[name], l1, p, report=3)
     dh = out["dh"]
@@ -195,7 +196,7 @@ def test_topk_radix_selection_path(mini, param_sets, torch_cuda):
     import dataclasses
     l1, sp, _ = mini
     for k in (1, 2, 3):
-        p = dataclasses.replace(param_sets["ppm"], topk=k)
+        p = dataclasses.replace(param_sets["ppm"], topk=k, search_method="staged")
         gi = E.GpuIndex(l1, p, STATIC, VAR)
         tbl, st, out = E.search(sp, gi, l1, p)
         pk = O.k0_view(sp, p)
@@ -226,3 +227,81 @@ def test_search_is_deterministic(mini, param_sets, indexes):
     a = E.search(sp, indexes["ppm"], l1, param_sets["ppm"], report=5)[0]
     b = E.search(sp, indexes["ppm"], l1, param_sets["ppm"], report=5)[0]
     assert a.equals(b)
+
+
+def test_k1_per_peak_path_equals_merge_join(mini, param_sets, torch_cuda):
+    """The per-peak K1 search (used when windows are not monotone or a spectrum has more peaks than the window
+    buffer) gives the same dense counts as the merge join, for every parameter set."""
+    import dataclasses
+    from vulcan.gpu import engine as E
+    l1, sp, _ = mini
+    for name, p in param_sets.items():
+        outs = []
+        for merge in (True, False):
+            q = dataclasses.replace(p, k1_merge=merge, search_method="staged")
+            gi = E.GpuIndex(l1, q, STATIC, VAR)
+            outs.append(E.search(sp, gi, l1, q)[2]["cnt"].cpu().numpy())
+        assert np.array_equal(outs[0], outs[1]), name
+
+
+def test_k0_cta_path_for_large_spectra(mini, param_sets, torch_cuda):
+    """Runs with a spectrum of more than 2048 raw peaks use the CTA sort kernel; it equals the oracle too."""
+    from oracle import oracle as O
+    from vulcan.gpu import engine as E
+    from vulcan.gpu.host import Spectra
+    l1, sp, _ = mini
+    rng = np.random.default_rng(9)
+    big = np.sort(rng.uniform(100, 2100, 3000)).astype(np.float32)
+    mz = np.concatenate([sp.mz, big])
+    it = np.concatenate([sp.intensity, rng.lognormal(7, 1, 3000).astype(np.float32)])
+    off = np.concatenate([sp.offsets, [len(mz)]])
+    n = len(sp) + 1
+    sp2 = Spectra("big", np.arange(n, dtype=np.uint32), np.arange(n, dtype=np.uint32), np.zeros(n),
+                  np.concatenate([sp.precursor_mz, [800.0]]), np.concatenate([sp.charge, [2]]).astype(np.int8), mz, it,
+                  off.astype(np.int64))
+    for name in ("da", "ppm"):
+        p = param_sets[name]
+        pk = E.k0_preprocess(sp2, p, "cuda", E.Stats())
+        ref = O.k0_view(sp2, p)
+        assert np.array_equal(pk["off"].cpu().numpy(), ref["off"])
+        assert np.array_equal(pk["mass"].cpu().numpy(), ref["mass"])
+        assert np.array_equal(pk["int"].cpu().numpy(), ref["int"])
+        assert np.array_equal(pk["valid"], ref["valid"])
+
+
+@pytest.mark.parametrize("name", SETS)
+@pytest.mark.parametrize("topk", (None, 2))
+def test_fused_search_equals_staged_and_reference(mini, golden_py, param_sets, indexes, name, topk, torch_cuda):
+    """The fused persistent kernel gives the staged path's candidates (with K2 outputs) and PSM table, and the
+    reference's select_topk / psm_table on the golden fixture."""
+    import dataclasses
+    from vulcan.gpu import engine as E
+    l1, sp, _ = mini
+    p = param_sets[name] if topk is None else dataclasses.replace(param_sets[name], topk=topk)
+    gi = indexes[name] if topk is None else E.GpuIndex(l1, p, STATIC, VAR)
+    staged = dataclasses.replace(p, search_method="staged")
+    t_s, _, o_s = E.search(sp, gi, l1, staged, report=3)
+    t_f, _, o_f = E.search(sp, gi, l1, p, report=3)
+    assert t_f.equals(t_s)
+    # candidate-level outputs of the fused kernel
+    st = E.Stats()
+    run = E.DeviceRun(sp, gi.dev, st)
+    of = E._search_fused_device(run, gi, p, 3, st, cand=True)
+    cd, cap = of["cand"], of["cand_cap"]
+    n_cand = cd["n_cand"].cpu().numpy()
+    assert (n_cand >= 0).all()
+    sel = np.concatenate([np.arange(s * cap, s * cap + n_cand[s]) for s in range(len(n_cand))]).astype(np.int64)
+    nc = int(o_s["cand_off"][-1])
+    assert len(sel) == nc
+    for a, b in (("c_hyp", "c_hyp"), ("c_row", "c_row"), ("c_cnt", "c_cnt")):
+        assert np.array_equal(cd[a].cpu().numpy()[sel], o_s[b][:nc].cpu().numpy()), a
+    for k, name2, _ in E._K2_KEYS:
+        x, y = cd[k].cpu().numpy()[sel], o_s["k2"][name2][:nc].cpu().numpy()
+        assert np.array_equal(x, y, equal_nan=True), k
+    assert np.array_equal(of["hyp_scored"][:len(golden_py[f"{name}/hyp_spec"])].cpu().numpy(),
+                          o_s["hyp_scored"][:len(golden_py[f"{name}/hyp_spec"])].cpu().numpy())
+    if topk is None:
+        g = golden_py
+        assert np.array_equal(cd["c_hyp"].cpu().numpy()[sel], g[f"{name}/topk_h"])
+        assert np.array_equal(cd["c_row"].cpu().numpy()[sel], g[f"{name}/topk_r"])
+        assert np.array_equal(t_f.column("pf_row").to_numpy(), g[f"{name}/psm_pf_row"])

@@ -1,9 +1,10 @@
 // K2 exact rescoring body (Sage score_candidate semantics, reference vulcan/gpu/kernels.cu:240-376).
 //
 // B200 launch shape: one warp per spectrum, K2_WARPS spectra per CTA.  The warp stages its spectrum's first 512
-// mass-sorted peaks in shared memory; each lane scores whole candidates (the f32 sums are sequential in ion order:
-// b ions k ascending, fragment charge ascending, then y ions), so the per-candidate arithmetic is the reference's
-// operation for operation and the outputs are bit-identical.
+// mass-sorted peaks in shared memory with a bucket table of start indices (one lookup + a short walk replaces the
+// reference's binary search; same index found); each lane scores whole candidates (the f32 sums are sequential in
+// ion order: b ions k ascending, fragment charge ascending, then y ions), so the per-candidate arithmetic is the
+// reference's operation for operation and the outputs are bit-identical.
 #pragma once
 #include "common.cuh"
 
@@ -48,11 +49,60 @@ __device__ __forceinline__ int lower_bound_smem(const float* v, int n, float x) 
   return lo;
 }
 
+// Bucket table of a spectrum's sorted peak masses: start[b] = first peak j with bucket(sm[j]) >= b, where
+// bucket(x) = clamp((int)((x - m0) * inv_w), 0, K2_BUCKETS - 1) is monotone in x.  For a bound a with bucket b,
+// every peak >= a has bucket >= b, so the first peak >= a is found by starting at start[b] and stepping while
+// sm[j] < a: the same index the binary search returns, in one lookup and a short walk.
+constexpr int K2_BUCKETS = 512;
+
+struct PeakTable {
+  const float* sm;
+  const float* si;
+  const uint16_t* start;
+  int np;
+  float m0, inv_w;
+
+  __device__ __forceinline__ int bucket(float x) const {
+    float t = __fmul_rn(__fsub_rn(x, m0), inv_w);
+    int b = t <= 0.f ? 0 : (t >= (float)(K2_BUCKETS - 1) ? K2_BUCKETS - 1 : (int)t);
+    return b;
+  }
+  __device__ __forceinline__ int first_ge(float a) const {
+    int j = start[bucket(a)];
+    while (j < np && sm[j] < a) ++j;
+    return j;
+  }
+};
+
+// Build the table for the warp's spectrum (peaks already in shared memory).
+__device__ __forceinline__ PeakTable build_table(const float* sm, const float* si, uint16_t* start, int np, int lane) {
+  PeakTable t;
+  t.sm = sm;
+  t.si = si;
+  t.start = start;
+  t.np = np;
+  t.m0 = np > 0 ? sm[0] : 0.f;
+  float span = np > 0 ? __fsub_rn(sm[np - 1], t.m0) : 0.f;
+  t.inv_w = span > 0.f ? __fdiv_rn((float)K2_BUCKETS, span) : 0.f;
+  for (int j = lane; j < np; j += 32) {
+    int b = t.bucket(sm[j]);
+    int bp = j > 0 ? t.bucket(sm[j - 1]) : -1;
+    for (int q = bp + 1; q <= b; ++q) start[q] = (uint16_t)j;
+  }
+  int blast = np > 0 ? t.bucket(sm[np - 1]) : -1;
+  for (int q = blast + 1 + lane; q < K2_BUCKETS; q += 32) start[q] = (uint16_t)np;
+  __syncwarp();
+  return t;
+}
+
 template <bool SHIFT>
-__device__ __forceinline__ void k2_score(const SmemFrag& fp, const float* sm, const float* si, int np, int r,
+__device__ __forceinline__ void k2_score(const SmemFrag& fp, const PeakTable& pt, int r,
                                          int maxfz, const int64_t* seq_off, const uint8_t* len,
                                          const uint64_t* mask, const float* mass32, const uint8_t* res,
                                          float tol_lo, float tol_hi, float shift, const K2Out& out, int64_t c) {
+  const float* sm = pt.sm;
+  const float* si = pt.si;
+  const int np = pt.np;
   const uint8_t* sq = res + seq_off[r];
   int L = len[r];
   uint64_t mk = mask[r];
@@ -86,7 +136,7 @@ __device__ __forceinline__ void k2_score(const SmemFrag& fp, const float* sm, co
           float base = alt == 0 ? cum : __fadd_rn(cum, shift);
           float mz = __fdiv_rn(base, (float)z);
           float a = tol_bound(mz, tol_lo, da), bd = tol_bound(mz, tol_hi, da);
-          for (int j = lower_bound_smem(sm, np, a); j < np && sm[j] <= bd; ++j) {
+          for (int j = pt.first_ge(a); j < np && sm[j] <= bd; ++j) {
             float it = si[j];
             if (it >= mx) { mx = it; best = j; best_mz = mz; }
             if (SHIFT && it >= mx_a) { mx_a = it; best_a = j; }
@@ -152,6 +202,7 @@ __device__ __forceinline__ void k2_body(const SmemFrag& fp, int n_spec, const in
                                         const float* c_shift, const K2Out& out) {
   __shared__ float s_mass[K2_WARPS][VK_K2_MAXPK];
   __shared__ float s_int[K2_WARPS][VK_K2_MAXPK];
+  __shared__ uint16_t s_start[K2_WARPS][K2_BUCKETS];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int bs = blockIdx.x * K2_WARPS + warp; bs < n_spec; bs += gridDim.x * K2_WARPS) {
     int s = spec_ids ? spec_ids[bs] : bs;
@@ -165,11 +216,11 @@ __device__ __forceinline__ void k2_body(const SmemFrag& fp, int n_spec, const in
       si[j] = pk_int[p0 + j];
     }
     __syncwarp();
+    const PeakTable pt = build_table(sm, si, s_start[warp], np, lane);
     int64_t c1 = cand_off[bs + 1];
     for (int64_t c = cand_off[bs] + lane; c < c1; c += 32) {
       float shift = SHIFT ? c_shift[c] : 0.f;
-      k2_score<SHIFT>(fp, sm, si, np, c_row[c], c_maxfz[c], seq_off, len, mask, mass32, res, tol_lo, tol_hi, shift,
-                      out, c);
+      k2_score<SHIFT>(fp, pt, c_row[c], c_maxfz[c], seq_off, len, mask, mass32, res, tol_lo, tol_hi, shift, out, c);
     }
   }
 }

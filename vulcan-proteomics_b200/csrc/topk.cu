@@ -5,8 +5,9 @@
 // and merges duplicates of (spectrum, row) to the lowest hypothesis and highest count.  Here a warp reads its
 // spectrum's dense K1 counts, computes the per-hypothesis scored/matched statistics, and
 //   - if at most topk entries pass the threshold, takes them all (ballot compaction);
-//   - otherwise finds the topk-th largest 63-bit key (min(count,32767), row, -hypothesis) by an 8-bit radix select
-//     in shared memory and keeps the keys at or above it (keys are unique, so exactly topk);
+//   - otherwise finds the topk-th largest 63-bit key (min(count,32767), row, -hypothesis) -- by a warp bitonic sort
+//     of the appended keys when at most 512 pass, else by an 8-bit radix select -- and keeps the keys at or above
+//     it (keys are unique, so exactly topk);
 // then appends the partners, sorts by (row, hypothesis) with a warp bitonic sort and merges duplicates.
 #include "common.cuh"
 
@@ -46,17 +47,17 @@ __device__ __forceinline__ void warp_bitonic_u64(uint64_t* v, int n_pow2, int la
 __global__ void __launch_bounds__(TK_WARPS * 32)
 select_topk_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo, const int64_t* h_hi,
               const int64_t* win_off, const int32_t* cnt, const int64_t* partner, int thr, int topk, int pair_closure,
-              int cap, int list_pow2, int64_t* c_hyp, int64_t* c_row, int64_t* c_cnt, int64_t* n_cand,
+              int cap, int list_pow2, int key_cap, int64_t* c_hyp, int64_t* c_row, int64_t* c_cnt, int64_t* n_cand,
               uint32_t* hyp_scored, uint64_t* hyp_matched, int64_t* spec_scored, int64_t* spec_matched) {
   extern __shared__ __align__(16) uint8_t tk_smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int s = blockIdx.x * TK_WARPS + warp;
   if (s >= n_spec) return;
-  const size_t per_warp = (size_t)list_pow2 * (8 + 4 + 4 + 4) + 256 * 4;
+  const size_t per_warp = (size_t)key_cap * 8 + (size_t)list_pow2 * (4 + 4 + 4) + 256 * 4;
   uint8_t* base = tk_smem + per_warp * warp;
   WarpLists W;
   W.key = reinterpret_cast<uint64_t*>(base);
-  W.row = reinterpret_cast<int32_t*>(base + (size_t)list_pow2 * 8);
+  W.row = reinterpret_cast<int32_t*>(base + (size_t)key_cap * 8);
   W.hl = W.row + list_pow2;
   W.cnt = W.hl + list_pow2;
   W.hist = reinterpret_cast<uint32_t*>(W.cnt + list_pow2);
@@ -92,7 +93,28 @@ select_topk_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo, cons
   // threshold key: every entry with key >= kth is selected
   uint64_t kth = 0;
   const bool limit = n_app > topk;
-  if (limit) {
+  if (limit && n_app <= key_cap) {
+    // sort path: every appended key into shared memory, bitonic sort, the topk-th largest is the threshold
+    int n_k = 0;
+    for (int64_t h = hb; h < he; ++h) {
+      const int64_t w0 = win_off[h], lo = h_lo[h], n = h_hi[h] - lo;
+      for (int64_t j0 = 0; j0 < n; j0 += 32) {
+        const int64_t j = j0 + lane;
+        const int c = j < n ? cnt[w0 + j] : -1;
+        const bool take = j < n && c >= thr;
+        const unsigned m = __ballot_sync(VK_FULL, take);
+        if (take) W.key[n_k + __popc(m & lt_mask)] = sel_key(c, lo + j, (int)(h - hb));
+        n_k += __popc(m);
+      }
+    }
+    int n_pow2 = 32;
+    while (n_pow2 < n_k) n_pow2 <<= 1;
+    for (int i = n_k + lane; i < n_pow2; i += 32) W.key[i] = 0ull;   // smaller than every real key
+    __syncwarp();
+    warp_bitonic_u64(W.key, n_pow2, lane);
+    kth = W.key[n_pow2 - topk];
+    __syncwarp();
+  } else if (limit) {
     uint64_t prefix = 0, pmask = 0;
     long long need = topk;   // how many still to take from the entries matching prefix
     for (int shift = 56; shift >= 0; shift -= 8) {
@@ -224,13 +246,15 @@ int vk_select_topk(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo,
   if (topk < 1 || topk > 8192 || cap < (pair_closure ? 2 : 1) * topk) return VK_E_ARG;
   int list_pow2 = 32;
   while (list_pow2 < (pair_closure ? 2 : 1) * topk) list_pow2 <<= 1;
-  size_t per_warp = (size_t)list_pow2 * 20 + 1024;
+  const int key_cap = list_pow2 > 512 ? list_pow2 : 512;   // sort path up to 512 appended entries
+  size_t per_warp = (size_t)key_cap * 8 + (size_t)list_pow2 * 12 + 1024;
   size_t sh = per_warp * TK_WARPS;
   if (sh > 220 * 1024) return VK_E_ARG;
   cudaError_t e = cudaFuncSetAttribute(select_topk_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
   if (e != cudaSuccess) return vk_err(e);
   select_topk_k<<<(unsigned)((n_spec + TK_WARPS - 1) / TK_WARPS), TK_WARPS * 32, sh, (cudaStream_t)stream>>>(
-      n_spec, spec_hyp_off, h_lo, h_hi, win_off, cnt, partner, thr, topk, pair_closure, cap, list_pow2, c_hyp, c_row,
+      n_spec, spec_hyp_off, h_lo, h_hi, win_off, cnt, partner, thr, topk, pair_closure, cap, list_pow2, key_cap, c_hyp,
+      c_row,
       c_cnt, n_cand, hyp_scored, hyp_matched, spec_scored, spec_matched);
   return vk_launch_status();
 }

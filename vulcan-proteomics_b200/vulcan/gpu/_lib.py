@@ -33,6 +33,28 @@ class TIndex(C.Structure):
                 ("tile_off", P), ("cbin_off", P), ("postings", P)]
 
 
+class FusedIn(C.Structure):
+    """vk_fused_in"""
+    _fields_ = [("n_spec", C.c_int), ("n_work", C.c_int), ("spec_ids", P), ("pk_off", P), ("pk_mass", P),
+                ("pk_int", P), ("spec_hyp_off", P), ("h_lo", P), ("h_hi", P), ("h_maxfz", P), ("partner", P),
+                ("seq_off", P), ("len", P), ("mask", P), ("mass32", P), ("res", P), ("tol_lo", C.c_float),
+                ("tol_hi", C.c_float), ("thr", C.c_int), ("topk", C.c_int), ("pair_closure", C.c_int),
+                ("min_matched", C.c_int), ("report", C.c_int)]
+
+
+_K2_FIELDS = [("hs", P), ("sb", P), ("sy", P), ("ppm", P), ("mb", P), ("my", P), ("lb", P), ("ly", P)]
+
+
+class PsmOut(C.Structure):
+    """vk_psm_out"""
+    _fields_ = [("row", P), ("hyp", P), ("k1", P), ("rank", P), ("dnext", P), ("dbest", P)] + _K2_FIELDS
+
+
+class CandOut(C.Structure):
+    """vk_cand_out"""
+    _fields_ = [("cap", C.c_int), ("n_cand", P), ("c_hyp", P), ("c_row", P), ("c_cnt", P)] + _K2_FIELDS
+
+
 # reference-compatible signatures (vulcan/gpu/_lib.py:22-35 of the reference)
 _SIGS = {
     "vk_set_params": [P, P, P],
@@ -59,11 +81,14 @@ _SIGS_B200 = {
     "vk_hyp_fill": [I32, P, P, P, I32, I32, I32, I32, F32, F32, I32, P, I64, P, P, P, P, P, P, P, P, P, P],
     "vk_k1_plan_count": [P, I64, P, P, P, P, P],
     "vk_k1_plan_fill": [P, I64, P, P, P, P, P, P],
-    "vk_k1_tiles": [P, P, F32, F32, P, P, P, P, P, P, P, P, P, P, P, P],
+    "vk_k1_tiles": [P, P, F32, F32, I32, P, P, P, P, P, P, P, P, P, P, P, P],
     "vk_select_topk": [I32, P, P, P, P, P, P, I32, I32, I32, I32, P, P, P, P, P, P, P, P, P],
     "vk_compact_cands": [I32, I32, P, P, P, P, P, P, P, P, P, P, P, P],
     "vk_k2_spectra": [P, I32, P, P, P, P, P, P, P, P, P, P, P, F32, F32, P, P, P, P, P, P, P, P, P, P],
     "vk_psm_rank": [I32, P, P, P, P, P, I32, I32, P, P, P, P, P, P],
+    "vk_search_fused": [P, P, P, I32, I32, I32, P, P, P, P, P, P, P, P, P, P],
+    "vk_search_fused_smem": [P, I32, I32, I32, I32, P],
+    "vk_search_fused_grid": [P, I32, I32, I32, I32, P],
 }
 
 _lib = None

@@ -349,6 +349,11 @@ def _as_dev(hyp, dev):
     return out
 
 
+def k1_max_win(p: SearchParams) -> int:
+    """Window buffer of the K1 merge join: K0 keeps at most max_peaks peaks per spectrum (0 = per-peak search)."""
+    return int(min(4096, max(0, p.max_peaks))) if p.k1_merge else 0
+
+
 def _k1_dense(gi: GpuIndex, dh, peaks, p: SearchParams, n_hyp: int, stats: Stats | None = None):
     """Tiled K1: dense counts of every window row.  Returns (win_off, cnt)."""
     L = K.lib()
@@ -369,7 +374,7 @@ def _k1_dense(gi: GpuIndex, dh, peaks, p: SearchParams, n_hyp: int, stats: Stats
     cnt = torch.empty(max(n_win, 1), dtype=torch.int32, device=dev)
     status = torch.zeros(1, dtype=torch.int32, device=dev)
     K.check(L.vk_k1_tiles(C.byref(ix), C.byref(gi.fp), float(p.fragment_ppm[0]), float(p.fragment_ppm[1]),
-                          K.ptr(item_off), K.ptr(item_hyp), K.ptr(dh["spec"]), K.ptr(dh["maxfz"]), K.ptr(dh["lo"]),
+                          k1_max_win(p), K.ptr(item_off), K.ptr(item_hyp), K.ptr(dh["spec"]), K.ptr(dh["maxfz"]), K.ptr(dh["lo"]),
                           K.ptr(dh["hi"]), K.ptr(win_off), K.ptr(peaks["off"]), K.ptr(peaks["mass"]), K.ptr(cnt),
                           K.ptr(status), K.stream()), "k1_tiles")
     if stats is not None:
@@ -613,8 +618,122 @@ def _search_device(run: DeviceRun, gi: GpuIndex, p: SearchParams, report: int, s
     with phase("rank"):
         psm = _rank_device(n, cand_off, c_row, k2, p, report, dev)
     return {"peaks": peaks, "dh": dh, "win_off": win_off, "cnt": cnt, "status": status, "cand_off": cand_off,
-            "c_hyp": c_hyp, "c_row": c_row, "c_cnt": c_cnt, "k2": k2, "psm": psm, "hyp_scored": hyp_scored,
+            "c_hyp": c_hyp, "c_row": c_row, "c_cnt": c_cnt, "c_row32": c_row32, "c_maxfz": c_maxfz, "cap": cap,
+            "n_cand": n_cand, "k2": k2, "psm": psm, "hyp_scored": hyp_scored,
             "hyp_matched": hyp_matched, "spec_scored": spec_scored, "spec_matched": spec_matched}
+
+
+_K2_KEYS = (("hs", "hyperscore", torch.float64), ("sb", "summed_b", torch.float32),
+            ("sy", "summed_y", torch.float32), ("ppm", "ppm", torch.float32), ("mb", "matched_b", torch.int16),
+            ("my", "matched_y", torch.int16), ("lb", "longest_b", torch.int16), ("ly", "longest_y", torch.int16))
+_FUSED_GRID = {}
+
+
+def fused_grid(gi: GpuIndex, p: SearchParams) -> int:
+    """Persistent grid of the fused search (resident CTAs per SM x SMs) for this index and parameters."""
+    key = (id(gi), p.fused_warps, p.topk, p.pair_closure, p.fused_cnt_cap)
+    if key not in _FUSED_GRID:
+        g = C.c_int(0)
+        with torch.cuda.device(gi.dev):
+            K.check(K.lib().vk_search_fused_grid(C.byref(gi.tix), p.fused_warps, p.topk, int(p.pair_closure),
+                                                 p.fused_cnt_cap, C.byref(g)), "fused_grid")
+        _FUSED_GRID[key] = g.value
+    return _FUSED_GRID[key]
+
+
+def _fused_device(gi: GpuIndex, p: SearchParams, report: int, peaks, dh, n: int, cand: bool = False,
+                  spec_ids: torch.Tensor | None = None, warps: int | None = None):
+    """The fused persistent search (K1 -> top-K + closure -> K2 -> ranking) over spectra 0..n-1 (or spec_ids)."""
+    L = K.lib()
+    dev = gi.dev
+    slots = max(n * report, 1)
+    o = {"status": torch.empty(max(n, 1), dtype=torch.int32, device=dev),
+         "n_psm": torch.empty(max(n, 1), dtype=torch.int32, device=dev),
+         "spec_scored": torch.zeros(max(n, 1), dtype=torch.int64, device=dev),
+         "spec_matched": torch.zeros(max(n, 1), dtype=torch.int64, device=dev),
+         "work": torch.empty(1, dtype=torch.int32, device=dev)}
+    psm = {"row": torch.full((slots,), -1, dtype=torch.int64, device=dev),
+           "hyp": torch.empty(slots, dtype=torch.int64, device=dev),
+           "k1": torch.empty(slots, dtype=torch.int64, device=dev),
+           "rank": torch.empty(slots, dtype=torch.int32, device=dev),
+           "dnext": torch.empty(slots, dtype=torch.float64, device=dev),
+           "dbest": torch.empty(slots, dtype=torch.float64, device=dev)}
+    for k, _, dt in _K2_KEYS:
+        psm[k] = torch.empty(slots, dtype=dt, device=dev)
+    po = K.PsmOut(*[K.ptr(psm[f]) for f, _ in K.PsmOut._fields_])
+    co = None
+    if cand:
+        cap = (2 if p.pair_closure else 1) * p.topk
+        cs = max(n * cap, 1)
+        cd = {"n_cand": torch.full((max(n, 1),), -1, dtype=torch.int64, device=dev),
+              "c_hyp": torch.empty(cs, dtype=torch.int64, device=dev),
+              "c_row": torch.empty(cs, dtype=torch.int64, device=dev),
+              "c_cnt": torch.empty(cs, dtype=torch.int64, device=dev)}
+        for k, _, dt in _K2_KEYS:
+            cd[k] = torch.empty(cs, dtype=dt, device=dev)
+        co = K.CandOut(cap, *[K.ptr(cd[f]) for f, _ in K.CandOut._fields_[1:]])
+        o["cand"] = cd
+        o["cand_cap"] = cap
+    n_h = dh["n_max"]
+    o["hyp_scored"] = torch.empty(max(n_h, 1), dtype=torch.int32, device=dev)
+    o["hyp_matched"] = torch.empty(max(n_h, 1), dtype=torch.int64, device=dev)
+    fin = K.FusedIn(n, n if spec_ids is None else int(spec_ids.numel()), K.ptr(spec_ids), K.ptr(peaks["off"]),
+                    K.ptr(peaks["mass"]), K.ptr(peaks["int"]), K.ptr(dh["spec_off"]), K.ptr(dh["lo"]),
+                    K.ptr(dh["hi"]), K.ptr(dh["maxfz"]), K.ptr(gi.partner), *gi.table_ptrs(),
+                    float(p.fragment_ppm[0]), float(p.fragment_ppm[1]), p.k1_threshold, p.topk, int(p.pair_closure),
+                    p.min_matched_peaks, report)
+    w = warps or p.fused_warps
+    q = p if w == p.fused_warps else _replace(p, fused_warps=w)
+    K.check(L.vk_search_fused(C.byref(gi.tix), C.byref(gi.fp), C.byref(fin), w, p.fused_cnt_cap, fused_grid(gi, q),
+                              K.ptr(o["work"]), K.ptr(o["status"]), K.ptr(o["n_psm"]), K.ptr(o["spec_scored"]),
+                              K.ptr(o["spec_matched"]), C.byref(po), C.byref(co) if co is not None else None,
+                              K.ptr(o["hyp_scored"]), K.ptr(o["hyp_matched"]), K.stream()), "search_fused")
+    o["psm"] = psm
+    return o
+
+
+def _replace(p: SearchParams, **kw) -> SearchParams:
+    import dataclasses
+    return dataclasses.replace(p, **kw)
+
+
+def _search_fused_device(run: DeviceRun, gi: GpuIndex, p: SearchParams, report: int, st: Stats,
+                         timers: bool = False, cand: bool = False):
+    """K0, hypotheses and the fused search of one run whose raw spectra are already resident."""
+    dev = gi.dev
+
+    def phase(name):
+        return Timer(st, name) if timers else _NoTimer()
+    with phase("k0"):
+        peaks = _k0_device(run, p, dev)
+    with phase("hyp"):
+        dh = _hyp_device(run, peaks, gi, p)
+    with phase("fused"):
+        o = _fused_device(gi, p, report, peaks, dh, run.n, cand=cand)
+    o["peaks"] = peaks
+    o["dh"] = dh
+    return o
+
+
+def _gather_fused(o, report, stats: Stats | None = None):
+    """Device gather of the fused search's reported PSMs, one D2H copy per column."""
+    psm, dh = o["psm"], o["dh"]
+    ok = psm["row"] >= 0
+    slot = torch.nonzero(ok).squeeze(1)
+    s = slot // report
+    hh = psm["hyp"][ok]
+    cols = {"spec": s, "rank": psm["rank"][ok], "dnext": psm["dnext"][ok], "dbest": psm["dbest"][ok],
+            "row": psm["row"][ok], "hyp": hh, "k1": psm["k1"][ok], "z": dh["z"][hh], "iso": dh["iso"][hh],
+            "pm": dh["pm"][hh], "spec_scored": o["spec_scored"][s], "spec_matched": o["spec_matched"][s],
+            "tic": o["peaks"]["tic"][s]}
+    for k, name, _ in _K2_KEYS:
+        cols[name] = psm[k][ok]
+    out = {}
+    for k, v in cols.items():
+        out[k] = v.cpu().numpy()
+        if stats is not None:
+            stats.d2h_bytes += v.numel() * v.element_size()
+    return out
 
 
 class _NoTimer:
@@ -636,15 +755,28 @@ def search(sp: Spectra, gi: GpuIndex, l1, p: SearchParams, report: int | None = 
     t0 = time.perf_counter()
     with torch.cuda.device(gi.dev):
         run = DeviceRun(sp, gi.dev, st)
-        out = _search_device(run, gi, p, report, st, timers)
-        if int(out["status"].item()):
-            raise RuntimeError("k1_tiles: a tile copy did not complete")
-        rec = _gather_psms(*out["psm"], out["c_hyp"], out["c_row"], out["c_cnt"], out["k2"], out["dh"],
-                           out["spec_scored"], out["spec_matched"], out["peaks"]["tic"], report, st)
+        method = p.search_method
+        if method == "fused":
+            out = _search_fused_device(run, gi, p, report, st, timers)
+            stat = int(out["status"][:run.n].max()) if run.n else 0
+            if stat & 2:
+                raise RuntimeError("search_fused: a tile copy did not complete")
+            if stat & 1:   # a spectrum spans more window rows than the fused kernel holds: staged path for the run
+                method = "staged"
+            else:
+                rec = _gather_fused(out, report, st)
+        if method == "staged":
+            out = _search_device(run, gi, p, report, st, timers)
+            if int(out["status"].item()):
+                raise RuntimeError("k1_tiles: a tile copy did not complete")
+            rec = _gather_psms(*out["psm"], out["c_hyp"], out["c_row"], out["c_cnt"], out["k2"], out["dh"],
+                               out["spec_scored"], out["spec_matched"], out["peaks"]["tic"], report, st)
+        elif method != "fused":
+            raise ValueError(f"unknown search_method {method!r}")
     tbl = _psm_columns(sp, l1, rec, p)
     ru1 = resource.getrusage(resource.RUSAGE_SELF)
     st.wall_s["total"] = time.perf_counter() - t0
-    n_rescored = int(out["cand_off"][-1])
+    n_rescored = int(out["cand_off"][-1]) if "cand_off" in out else -1
     st.counts.update(n_spectra=len(sp), n_searched=int(out["peaks"]["valid_d"].sum()),
                      n_hypotheses=int(out["dh"]["spec_off"][-1]), n_rescored=n_rescored, n_psms=tbl.num_rows)
     st.counts["cpu_core_s"] = (ru1.ru_utime - ru0.ru_utime) + (ru1.ru_stime - ru0.ru_stime)

@@ -43,9 +43,12 @@ class SearchParams:
     tile: int = 1024
     k2_threads: int = 128
     max_slice_entries: int = 2 ** 31 - 1
-    # B200 layout knobs: rows per fragment-index tile (power of two <= 2^row_bits) and coarse m/z bin width
+    # B200 layout knobs: rows per fragment-index tile (power of two, 32 <= tile_rows < 2^row_bits) and K1 method
     tile_rows: int = 64
-    coarse_bin_th: float = 8.0
+    k1_merge: bool = False                  # staged K1: merge join instead of the per-peak search
+    search_method: str = "staged"           # "staged" (a kernel per stage) or "fused" (one persistent kernel)
+    fused_warps: int = 4                    # warps of a fused-search CTA (one spectrum at a time)
+    fused_cnt_cap: int = 4096               # window rows a spectrum may span in the fused search
 
     def to_dict(self):
         return asdict(self)
