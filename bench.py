@@ -341,8 +341,8 @@ def run_b200(a):
     ms_k1 = timed(lambda: K.check(L.vk_k1_tiles(
         C.byref(gi.tix), C.byref(gi.fp), float(p.fragment_ppm[0]), float(p.fragment_ppm[1]), E.k1_max_win(p),
         K.ptr(item_off), K.ptr(item_hyp), K.ptr(dh["spec"]), K.ptr(dh["maxfz"]), K.ptr(dh["lo"]), K.ptr(dh["hi"]),
-        K.ptr(win_off), K.ptr(peaks["off"]), K.ptr(peaks["mass"]), K.ptr(cnt), K.ptr(status), K.stream()),
-        "k1_tiles"))
+        K.ptr(win_off), K.ptr(peaks["off"]), K.ptr(peaks["mass"]), K.ptr(cnt), K.ptr(status), None, None, None,
+        K.stream()), "k1_tiles"))
     kern["k1_tiles_k"] = (ms_k1, k1_algorithmic_bytes(gi, dh, peaks, win_off, item_off, item_hyp))
     n = run.n
     cap = so["cap"]

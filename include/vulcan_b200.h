@@ -179,7 +179,9 @@ int vk_hyp_fill(int n_spec, const uint8_t* valid, const double* precursor_mz, co
  * fragment f) with tol_bound(p*z, tol_lo) <= f <= tol_bound(p*z, tol_hi) in f32.  `status` (device i32, zeroed by
  * the caller) gets VK_STATUS_WAIT_TIMEOUT if a tile copy did not complete within the bounded wait.  max_win
  * (<= 4096) sizes the per-warp window buffer of the merge join: spectra with more peaks use the per-peak search;
- * 0 selects the per-peak search for every item. */
+ * 0 selects the per-peak search for every item.  isum (may be NULL; then pk_int and tic may be NULL too): per
+ * window row the summed intensity of its matches, u32 fixed point = sum of round(intensity * 2^24 / tic[s]), for
+ * the candidate pruner's features (the per-peak search is used when isum is given). */
 int vk_k1_plan_count(const vk_tindex* ix, int64_t n_hyp, const int64_t* h_lo, const int64_t* h_hi,
                      int64_t* tile_items, int64_t* win_len, void* stream);
 int vk_k1_plan_fill(const vk_tindex* ix, int64_t n_hyp, const int64_t* h_lo, const int64_t* h_hi,
@@ -187,7 +189,8 @@ int vk_k1_plan_fill(const vk_tindex* ix, int64_t n_hyp, const int64_t* h_lo, con
 int vk_k1_tiles(const vk_tindex* ix, const vk_frag_params* fp, float tol_lo, float tol_hi, int max_win,
                 const int64_t* tile_item_off, const int32_t* item_hyp, const int32_t* h_spec,
                 const int8_t* h_maxfz, const int64_t* h_lo, const int64_t* h_hi, const int64_t* win_off,
-                const int64_t* pk_off, const float* pk_mass, int32_t* cnt, int32_t* status, void* stream);
+                const int64_t* pk_off, const float* pk_mass, int32_t* cnt, int32_t* status, const float* pk_int,
+                const float* tic, uint32_t* isum, void* stream);
 
 /* Top-K + pair closure (reference vulcan/gpu/engine.py:284-312) per spectrum, from the dense K1 counts.
  * Spectrum s owns hypotheses [spec_hyp_off[s], spec_hyp_off[s+1]).  Per spectrum: entries with count >= thr,
@@ -300,6 +303,49 @@ int vk_search_fused(const vk_tindex* ix, const vk_frag_params* fp, const vk_fuse
 /* Dynamic shared memory per CTA and the persistent grid size (CTAs resident per SM x SMs) of the fused search. */
 int vk_search_fused_smem(const vk_tindex* ix, int warps, int topk, int pair_closure, int cnt_cap, int64_t* bytes);
 int vk_search_fused_grid(const vk_tindex* ix, int warps, int topk, int pair_closure, int cnt_cap, int* grid);
+
+/* ============================================================ Part 4: learned candidate pruner */
+
+/* Features of n candidate hits (hypothesis, row, K1 count; e.g. the top-K shortlist of vk_select_topk with
+ * pair_closure = 0, compacted): 16 BF16 per hit = the standardised (x - mu) / sd of K1 count, summed matched
+ * intensity (isum of vk_k1_tiles / 2^24, a fraction of the TIC), precursor error in ppm
+ * ((M_hyp - mass32[row]) / mass32[row] * 1e6), charge, peptide length, missed cleavages; zero padded.
+ * n bounds the buffers; when n_dev is given the device count *n_dev (<= n) is used instead (no host sync). */
+int vk_cand_features(int64_t n, const int64_t* n_dev, const int64_t* c_hyp, const int64_t* c_row,
+                     const int64_t* c_cnt, const int64_t* win_off, const int64_t* h_lo, const uint32_t* isum,
+                     const float* h_M, const int8_t* h_z, const float* mass32, const uint8_t* len,
+                     const uint8_t* missed, const float* mu, const float* sd, void* feat_bf16, void* stream);
+/* MLP logits of n feature rows (16 BF16 each; n_dev as above): W1 [256 x 16] and W2 [256 x 256] BF16 row-major,
+ * b1, b2, w3 (256) FP32, scalar b3; tensor cores (mma.sync BF16, FP32 accumulate); `grid` persistent CTAs of 256
+ * threads, each holding the weights in vk_mlp_infer_smem() bytes of shared memory. */
+int64_t vk_mlp_infer_smem(void);
+int vk_mlp_infer(int64_t n, const int64_t* n_dev, const void* feat_bf16, const void* W1_bf16, const float* b1, const void* W2_bf16,
+                 const float* b2, const float* w3, float b3, float* logit, int grid, void* stream);
+/* Pruned candidate selection per spectrum: hits with logit >= tau plus the min_keep best by (logit, count, hit
+ * order) descending, at most max_keep (a power of two >= 16); pair closure; candidates sorted by row with duplicate
+ * rows merged (lowest hypothesis, highest count) into slots s*cap (cap >= (pair_closure ? 2 : 1) * max_keep), the
+ * layout of vk_select_topk. */
+int vk_select_pruned(int n_spec, const int64_t* spec_hyp_off, const int64_t* hit_off, const int64_t* hit_hyp,
+                     const int32_t* hit_row, const int64_t* hit_cnt, const float* logit, float tau, int min_keep,
+                     int max_keep, int pair_closure, const int64_t* partner, int cap, int64_t* c_hyp, int64_t* c_row,
+                     int64_t* c_cnt, int64_t* n_cand, void* stream);
+
+/* Training kernels.  vk_gemm: C[m*scm + n*scn] = sum_k A[m*sam + k*sak] * B[k*sbk + n*sbn] (+ bias[n]) (ReLU)
+ * (rounded to a BF16 value); B is BF16 when b_bf16 != 0, else FP32; deterministic (fixed summation order). */
+int vk_gemm(int M, int N, int K, const float* A, int64_t sam, int64_t sak, const void* B, int b_bf16, int64_t sbk,
+            int64_t sbn, const float* bias, int relu, int round_bf16, float* C, int64_t scm, int64_t scn,
+            void* stream);
+int vk_colsum(int n, int o, const float* dY, float* db, void* stream);                 /* db[j] = sum_i dY[i, j] */
+int vk_relu_mask(int64_t n, const float* Y, float* dY, void* stream);                  /* dY *= (Y > 0) */
+/* weighted BCE with logits: dz = w (sigmoid(z) - y) inv_wsum; loss_part[ceil(n/256)] block partial sums */
+int vk_bce(int n, const float* z, const float* y, const float* w, float inv_wsum, float* dz, float* loss_part,
+           void* stream);
+/* Adam step (step >= 1) on FP32 master weights, L2 term wd * p added to the gradient; writes the BF16 copy if
+ * given */
+int vk_adam(int64_t n, float* p, const float* g, float* m, float* v, float lr, float b1, float b2, float eps,
+            int step, float wd, void* p_bf16, void* stream);
+int vk_to_bf16(int64_t n, const float* x, void* y, void* stream);
+int vk_bf16_to_f32(int64_t n, const void* x, float* y, void* stream);
 
 #ifdef __cplusplus
 }

@@ -175,8 +175,10 @@ def k1_brute(l1, hyp, peaks, h, r, p, P, nthreads=None):
     return out
 
 
-def k1_windows(l1, hyp, peaks, p, P, nthreads=None, arrays=None):
-    """Dense K1 counts of every window row; returns (win_off, cnt, scored, matched)."""
+def k1_windows(l1, hyp, peaks, p, P, nthreads=None, arrays=None, tic=None):
+    """Dense K1 counts of every window row; returns (win_off, cnt, scored, matched), plus, when ``tic`` (f32 per
+    spectrum) is given, the summed matched intensity of every window row: u32 sum over the matches of
+    round_half_even(intensity * f32(2^24 / tic)) (the pruner's intensity feature)."""
     a = arrays or {k: getattr(l1, k) for k in ("seq_off", "length", "mask", "mass32", "residues")}
     lo = _c(hyp["lo"], np.int64)
     hi = _c(hyp["hi"], np.int64)
@@ -186,13 +188,18 @@ def k1_windows(l1, hyp, peaks, p, P, nthreads=None, arrays=None):
     cnt = np.empty(int(win_off[-1]), np.int32)
     scored = np.zeros(n_h, np.uint32)
     matched = np.zeros(n_h, np.uint64)
+    isum = np.zeros(len(cnt), np.uint32) if tic is not None else None
     lib().or_k1_windows(C.c_int64(n_h), _p(_c(hyp["spec"], np.int32)), _p(_c(hyp["maxfz"], np.int8)), _p(lo), _p(hi),
                         _p(win_off), _p(_c(peaks["off"], np.int64)), _p(_c(peaks["mass"], np.float32)),
                         _p(_c(a["seq_off"], np.int64)), _p(_c(a["length"], np.uint8)), _p(_c(a["mask"], np.uint64)),
                         _p(_c(a["mass32"], np.float32)), _p(_c(a["residues"], np.uint8)), C.c_int(p.min_ion_index),
                         C.c_float(p.fragment_min_mz), C.c_float(p.fragment_max_mz), C.c_float(p.fragment_ppm[0]),
-                        C.c_float(p.fragment_ppm[1]), _p(cnt), _p(scored), _p(matched), C.byref(P),
-                        C.c_int(nthreads or n_threads()))
+                        C.c_float(p.fragment_ppm[1]), _p(cnt), _p(scored), _p(matched),
+                        _p(_c(peaks["int"], np.float32)) if tic is not None else None,
+                        _p(_c(tic, np.float32)) if tic is not None else None,
+                        _p(isum) if tic is not None else None, C.byref(P), C.c_int(nthreads or n_threads()))
+    if tic is not None:
+        return win_off, cnt, scored, matched, isum
     return win_off, cnt, scored, matched
 
 
@@ -234,6 +241,49 @@ def select_topk(o_h, o_r, o_c, hyp_spec, partner, topk, pair_closure=True):
     cc = np.full(len(uk), -1, np.int64)
     np.maximum.at(cc, inv, c)
     return hh, uk & (2 ** ROW_BITS - 1), cc
+
+
+def _ord_f32(x):
+    """Order-preserving u32 image of f32 values (total order, -0 below +0)."""
+    u = np.ascontiguousarray(x, np.float32).view(np.uint32).astype(np.uint64)
+    return np.where(u & 0x80000000, (~u) & 0xFFFFFFFF, u | 0x80000000)
+
+
+def select_pruned(spec_hyp_off, hit_off, hit_hyp, hit_row, hit_cnt, logit, tau, min_keep, max_keep, partner,
+                  pair_closure=True, sort_cap=1024):
+    """The pruned selection of the learned pruner, per spectrum s over its hits [hit_off[s], hit_off[s+1]) (in
+    (row, hypothesis) order): rank by (logit, min(count, 4095), hit position) descending; keep rank < min_keep or
+    logit >= tau, at most max_keep (more than sort_cap hits: the first max_keep hits with logit >= tau in hit
+    order); then pair closure (partner rows, same hypothesis, count -1) and duplicate rows merged (lowest
+    hypothesis, highest count).  Returns per spectrum the (hyp, row, count) lists sorted by row."""
+    hit_hyp = np.asarray(hit_hyp, np.int64)
+    hit_row = np.asarray(hit_row, np.int64)
+    hit_cnt = np.asarray(hit_cnt, np.int64)
+    logit = np.asarray(logit, np.float32)
+    partner = np.asarray(partner, np.int64)
+    out = []
+    for s in range(len(hit_off) - 1):
+        a, b = int(hit_off[s]), int(hit_off[s + 1])
+        n = b - a
+        if n > sort_cap:
+            ok = np.flatnonzero(logit[a:b] >= tau)[:max_keep]
+        else:
+            loc = np.arange(n, dtype=np.uint64)
+            key = (_ord_f32(logit[a:b]) << np.uint64(32)) | (np.minimum(hit_cnt[a:b], 4095).astype(np.uint64)
+                                                              << np.uint64(20)) | loc
+            order = np.argsort(key)[::-1][:max_keep]
+            rank = np.arange(len(order))
+            ok = order[(rank < min_keep) | (logit[a:b][order] >= tau)]
+        h, r, c = hit_hyp[a + ok], hit_row[a + ok], hit_cnt[a + ok]
+        if pair_closure:
+            h = np.concatenate([h, h])
+            r = np.concatenate([r, partner[r]])
+            c = np.concatenate([c, np.full(len(ok), -1, np.int64)])
+        rows = np.unique(r)
+        hh = np.array([h[r == x].min() for x in rows], np.int64)
+        cc = np.array([c[r == x].max() for x in rows], np.int64)
+        out.append((hh, rows, cc))
+    return out
 
 
 # ---------------------------------------------------------------------------------------------------- K2

@@ -177,13 +177,15 @@ void or_k1_windows(int64_t n_hyp, const int32_t* hyp_spec, const int8_t* hyp_max
                    const int64_t* hyp_hi, const int64_t* win_off, const int64_t* pk_off, const float* pk_mass,
                    const int64_t* seq_off, const uint8_t* len, const uint64_t* mask, const float* mass32,
                    const uint8_t* res, int min_ion_index, float fmin, float fmax, float tol_lo, float tol_hi,
-                   int32_t* cnt, uint32_t* scored, uint64_t* matched, const or_params* P, int nthreads) {
+                   int32_t* cnt, uint32_t* scored, uint64_t* matched, const float* pk_int, const float* tic,
+                   uint32_t* isum, const or_params* P, int nthreads) {
   set_threads(nthreads);
 #pragma omp parallel
   {
     float fr[2 * K2_MAXLEN];
     int wcap = 0;
     float *wa = NULL, *wb = NULL;
+    uint32_t* wg = NULL;
 #pragma omp for schedule(dynamic, 16)
     for (int64_t h = 0; h < n_hyp; ++h) {
       int s = hyp_spec[h], maxfz = hyp_maxfz[h];
@@ -193,13 +195,17 @@ void or_k1_windows(int64_t n_hyp, const int32_t* hyp_spec, const int8_t* hyp_max
         wcap = nw * 2 + 16;
         wa = (float*)realloc(wa, sizeof(float) * wcap);
         wb = (float*)realloc(wb, sizeof(float) * wcap);
+        wg = (uint32_t*)realloc(wg, sizeof(uint32_t) * wcap);
       }
+      /* intensity weight of a peak: round-to-nearest-even of intensity * (2^24 / TIC) in f32 */
+      float wscale = (isum && tic[s] > 0.f) ? 16777216.0f / tic[s] : 0.f;
       int w = 0;
       for (int64_t p = p0; p < p1; ++p)
         for (int z = 1; z < maxfz; ++z) {
           float m = pk_mass[p] * (float)z;
           wa[w] = tol_bound(P, m, tol_lo);
           wb[w] = tol_bound(P, m, tol_hi);
+          wg[w] = isum ? (uint32_t)lrintf(pk_int[p] * wscale) : 0u;
           ++w;
         }
       uint32_t sc = 0;
@@ -208,10 +214,15 @@ void or_k1_windows(int64_t n_hyp, const int32_t* hyp_spec, const int8_t* hyp_max
         int nf = row_fragments(P, seq_off, len, mask, mass32, res, r, min_ion_index, fmin, fmax, fr);
         qsort(fr, nf, sizeof(float), cmp_f32);
         int c = 0;
+        uint32_t is = 0;
         for (int j = 0; j < nw; ++j) {
-          for (int t = lower_bound_f(fr, nf, wa[j]); t < nf && fr[t] <= wb[j]; ++t) ++c;
+          for (int t = lower_bound_f(fr, nf, wa[j]); t < nf && fr[t] <= wb[j]; ++t) {
+            ++c;
+            is += wg[j];
+          }
         }
         cnt[win_off[h] + (r - hyp_lo[h])] = c;
+        if (isum) isum[win_off[h] + (r - hyp_lo[h])] = is;
         if (c > 0) { ++sc; mt += (uint64_t)c; }
       }
       scored[h] = sc;
@@ -219,6 +230,7 @@ void or_k1_windows(int64_t n_hyp, const int32_t* hyp_spec, const int8_t* hyp_max
     }
     free(wa);
     free(wb);
+    free(wg);
   }
 }
 

@@ -49,7 +49,8 @@ __global__ void __launch_bounds__(K1_WARPS * 32)
 k1_tiles_k(vk_tindex ix, float tol_lo, float tol_hi, int tol_da, int post_cap, int max_win,
            const int64_t* tile_item_off, const int32_t* item_hyp, const int32_t* h_spec, const int8_t* h_maxfz,
            const int64_t* h_lo, const int64_t* h_hi, const int64_t* win_off, const int64_t* pk_off,
-           const float* pk_mass, int32_t* cnt, int32_t* status) {
+           const float* pk_mass, int32_t* cnt, int32_t* status, const float* pk_int, const float* tic,
+           uint32_t* isum_out) {
   extern __shared__ __align__(16) uint8_t k1_smem[];
   __shared__ __align__(8) uint64_t bar;
   const int64_t t = blockIdx.x;
@@ -62,6 +63,7 @@ k1_tiles_k(vk_tindex ix, float tol_lo, float tol_hi, int tol_da, int post_cap, i
   uint16_t* cb = reinterpret_cast<uint16_t*>(k1_smem + (size_t)post_cap * 4);
   uint32_t* hist = reinterpret_cast<uint32_t*>(k1_smem + (size_t)post_cap * 4 + (size_t)stride * 2);
   uint32_t* wins = hist + K1_WARPS * T;   // per warp: max_win window starts, then max_win window ends
+  uint32_t* ihist = wins + (size_t)K1_WARPS * 2 * max_win;   // per warp T intensity sums (features only)
   const int64_t po = ix.tile_off[t];
   const uint32_t post_bytes = (uint32_t)((ix.tile_off[t + 1] - po) * 4);
   const uint32_t cb_bytes = (uint32_t)stride * 2;
@@ -81,6 +83,7 @@ k1_tiles_k(vk_tindex ix, float tol_lo, float tol_hi, int tol_da, int post_cap, i
   }
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint32_t* hw = hist + warp * T;
+  uint32_t* iw = isum_out ? ihist + warp * T : nullptr;
   uint32_t* wka = wins + (size_t)warp * 2 * max_win;
   uint32_t* wkb = wka + max_win;
   const int row_bits = ix.row_bits;
@@ -94,11 +97,14 @@ k1_tiles_k(vk_tindex ix, float tol_lo, float tol_hi, int tol_da, int post_cap, i
     const int h = item_hyp[it];
     const int64_t lo = h_lo[h], hi = h_hi[h];
     const int rlo = (int)max(lo - r0, (int64_t)0), rhi = (int)min(hi - r0, (int64_t)T);
-    for (int j = lane; j < T; j += 32) hw[j] = 0;
+    for (int j = lane; j < T; j += 32) {
+      hw[j] = 0;
+      if (iw) iw[j] = 0;
+    }
     __syncwarp();
     const int s = h_spec[h], maxfz = h_maxfz[h];
     const int64_t p0 = pk_off[s], p1 = pk_off[s + 1];
-    bool merged = (p1 - p0) <= max_win;
+    bool merged = (p1 - p0) <= max_win && !iw;   // the merge join does not accumulate intensities
     for (int z = 1; merged && z < maxfz; ++z) {
       // tolerance windows of this fragment charge, in key space, in peak (= mass) order; windows that miss
       // [fmin, fmax] are dropped, the others clamped to it
@@ -163,11 +169,16 @@ k1_tiles_k(vk_tindex ix, float tol_lo, float tol_hi, int tol_da, int post_cap, i
       __syncwarp();
       for (int j = lane; j < T; j += 32) hw[j] = 0;
       __syncwarp();
-      vk::k1_item_per_peak(post, cb, hw, 0, rlo, rhi, p0, p1, maxfz, pk_mass, tol_lo, tol_hi, tol_da, ix, lane);
+      const float ts = iw ? tic[s] : 0.f;
+      vk::k1_item_per_peak(post, cb, hw, 0, rlo, rhi, p0, p1, maxfz, pk_mass, tol_lo, tol_hi, tol_da, ix, lane, iw,
+                           pk_int, ts > 0.f ? __fdiv_rn(16777216.0f, ts) : 0.f);
     }
     __syncwarp();
     const int64_t base = win_off[h] + (r0 - lo);
-    for (int j = rlo + lane; j < rhi; j += 32) cnt[base + j] = (int32_t)hw[j];
+    for (int j = rlo + lane; j < rhi; j += 32) {
+      cnt[base + j] = (int32_t)hw[j];
+      if (iw) isum_out[base + j] = iw[j];
+    }
     __syncwarp();
   }
 }
@@ -207,20 +218,22 @@ int vk_k1_plan_fill(const vk_tindex* ix, int64_t n_hyp, const int64_t* h_lo, con
 int vk_k1_tiles(const vk_tindex* ix, const vk_frag_params* fp, float tol_lo, float tol_hi, int max_win,
                 const int64_t* tile_item_off, const int32_t* item_hyp, const int32_t* h_spec,
                 const int8_t* h_maxfz, const int64_t* h_lo, const int64_t* h_hi, const int64_t* win_off,
-                const int64_t* pk_off, const float* pk_mass, int32_t* cnt, int32_t* status, void* stream) {
+                const int64_t* pk_off, const float* pk_mass, int32_t* cnt, int32_t* status, const float* pk_int,
+                const float* tic, uint32_t* isum, void* stream) {
   if (!ix || !fp || !status) return VK_E_ARG;
   if (ix->n_tiles == 0) return 0;
   if ((ix->max_tile_postings & 3) || ix->max_tile_postings < 0 || max_win < 0 || max_win > 4096) return VK_E_ARG;
   const int T = 1 << ix->tile_shift;
   const int stride = ((1 << ix->cbin_bits) + 1 + 7) & ~7;
+  if (isum && (!pk_int || !tic)) return VK_E_ARG;
   size_t sh = (size_t)ix->max_tile_postings * 4 + (size_t)stride * 2 + (size_t)K1_WARPS * T * 4 +
-              (size_t)K1_WARPS * 2 * max_win * 4;
+              (size_t)K1_WARPS * 2 * max_win * 4 + (isum ? (size_t)K1_WARPS * T * 4 : 0);
   if (sh > 220 * 1024) return VK_E_ARG;
   cudaError_t e = cudaFuncSetAttribute(k1_tiles_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
   if (e != cudaSuccess) return vk_err(e);
   k1_tiles_k<<<(unsigned)ix->n_tiles, K1_WARPS * 32, sh, (cudaStream_t)stream>>>(
       *ix, tol_lo, tol_hi, fp->tol_da, ix->max_tile_postings, max_win, tile_item_off, item_hyp, h_spec, h_maxfz,
-      h_lo, h_hi, win_off, pk_off, pk_mass, cnt, status);
+      h_lo, h_hi, win_off, pk_off, pk_mass, cnt, status, pk_int, tic, isum);
   return vk_launch_status();
 }
 

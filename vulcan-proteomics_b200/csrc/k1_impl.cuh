@@ -10,12 +10,15 @@
 
 namespace vk {
 
-// cnt[hoff + l] is the count of tile row l (rows rlo <= l < rhi only).
+// cnt[hoff + l] is the count of tile row l (rows rlo <= l < rhi only).  With isum != nullptr, every match also adds
+// the peak's weight round(intensity * wscale) (u32, wscale = 2^24 / TIC of the spectrum) to isum[hoff + l]: the
+// summed matched intensity as a fixed-point fraction of the TIC, accumulated with integer atomics (deterministic).
 __device__ __forceinline__ void k1_item_per_peak(const uint32_t* post, const uint16_t* cb, uint32_t* cnt, int64_t hoff,
                                                  int rlo, int rhi,
                                                  int64_t p0, int64_t p1, int maxfz, const float* pk_mass,
                                                  float tol_lo, float tol_hi, int tol_da, const vk_tindex& ix,
-                                                 int lane) {
+                                                 int lane, uint32_t* isum = nullptr, const float* pk_int = nullptr,
+                                                 float wscale = 0.f) {
   const int row_bits = ix.row_bits;
   const uint32_t rowmask = (1u << row_bits) - 1u;
   const int sh = 32 - ix.cbin_bits;
@@ -25,6 +28,7 @@ __device__ __forceinline__ void k1_item_per_peak(const uint32_t* post, const uin
   for (int64_t q = lane; q < n_iter; q += 32) {
     const int64_t p = p0 + q;
     const float pm = p < p1 ? pk_mass[p] : 0.f;
+    const uint32_t wgt = (isum && p < p1) ? __float2uint_rn(__fmul_rn(pk_int[p], wscale)) : 0u;
     for (int z = 1; z < maxfz; ++z) {
       int e = 0, e1 = 0;
       uint32_t hi_key = 0;
@@ -49,7 +53,10 @@ __device__ __forceinline__ void k1_item_per_peak(const uint32_t* post, const uin
         const uint32_t v = post[e];
         if (v > hi_key) break;
         const int l = (int)(v & rowmask);
-        if (l >= rlo && l < rhi) atomicAdd(&cnt[hoff + l], 1u);
+        if (l >= rlo && l < rhi) {
+          atomicAdd(&cnt[hoff + l], 1u);
+          if (isum) atomicAdd(&isum[hoff + l], wgt);
+        }
       }
     }
   }

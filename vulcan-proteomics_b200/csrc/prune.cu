@@ -1,0 +1,359 @@
+// Learned candidate pruner: features of the K1 index hits, the BF16 MLP on tensor cores, and the selection of the
+// hits to rescore.
+//
+// The pruner sees the hits the plain path shortlists: the top-K of each spectrum before pair closure (vk_select_topk
+// with pair_closure = 0), so the pruned candidates are always a subset of the plain path's.  Features per hit
+// (label-free): K1 count, summed matched intensity (fraction of the TIC, from K1's fixed-point sums), precursor mass
+// error in ppm (hypothesis mass vs the row's Sage f32 mass), precursor charge, peptide length, missed cleavages,
+// standardised with the model's (mu, sd) and stored as 16 BF16 values (6 used).
+//
+// MLP: x(16) -> 256 (ReLU) -> 256 (ReLU) -> 1 logit; BF16 weights, FP32 accumulation.  Inference uses mma.sync
+// m16n8k16 (BF16 in, FP32 accumulate): a warp scores 16 hits; the layer-1 accumulators are repacked in registers as
+// the layer-2 A fragments (BF16), layer 2 runs in chunks of 64 output columns whose ReLU output is dotted with the
+// layer-3 weights at once, so no activation leaves the registers.  The weights live in shared memory with padded
+// rows (no bank conflicts on the B fragments).
+//
+// Selection per spectrum (one warp): hits with logit >= tau plus the min_keep best (logit desc, count desc, hit
+// order desc), at most max_keep of them by the same order; then pair closure, sort by (row, hypothesis) and merge of
+// duplicate rows exactly as the top-K selection (topk.cu) -- only the ranking key differs.
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+
+namespace {
+
+constexpr int MLP_IN = 16;
+constexpr int MLP_H = 256;
+constexpr int W1_STRIDE = MLP_IN + 8;   // bf16 elements per W1 row in shared memory
+constexpr int W2_STRIDE = MLP_H + 8;    // bf16 elements per W2 row in shared memory
+constexpr int INF_WARPS = 8;
+
+// ------------------------------------------------------------------------------------------------ features
+// One thread per candidate hit (hypothesis, row, count): its window position is win_off[h] + row - lo[h].
+__global__ void cand_features_k(int64_t n, const int64_t* n_dev, const int64_t* c_hyp, const int64_t* c_row, const int64_t* c_cnt,
+                                const int64_t* win_off, const int64_t* h_lo, const uint32_t* isum, const float* h_M,
+                                const int8_t* h_z, const float* mass32, const uint8_t* len, const uint8_t* missed,
+                                const float* mu, const float* sd, __nv_bfloat16* feat) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n_dev) n = min(n, *n_dev);
+  if (i >= n) return;
+  const int64_t h = c_hyp[i], r = c_row[i];
+  const float mr = mass32[r];
+  float raw[6];
+  raw[0] = (float)c_cnt[i];
+  raw[1] = (float)isum[win_off[h] + (r - h_lo[h])] * (1.0f / 16777216.0f);
+  raw[2] = (h_M[h] - mr) / mr * 1.0e6f;
+  raw[3] = (float)h_z[h];
+  raw[4] = (float)len[r];
+  raw[5] = (float)missed[r];
+  uint32_t* f = reinterpret_cast<uint32_t*>(feat + i * MLP_IN);
+  __nv_bfloat162 v0 = __floats2bfloat162_rn((raw[0] - mu[0]) / sd[0], (raw[1] - mu[1]) / sd[1]);
+  __nv_bfloat162 v1 = __floats2bfloat162_rn((raw[2] - mu[2]) / sd[2], (raw[3] - mu[3]) / sd[3]);
+  __nv_bfloat162 v2 = __floats2bfloat162_rn((raw[4] - mu[4]) / sd[4], (raw[5] - mu[5]) / sd[5]);
+  f[0] = *reinterpret_cast<uint32_t*>(&v0);
+  f[1] = *reinterpret_cast<uint32_t*>(&v1);
+  f[2] = *reinterpret_cast<uint32_t*>(&v2);
+  for (int k = 3; k < MLP_IN / 2; ++k) f[k] = 0u;
+}
+
+// ------------------------------------------------------------------------------------------------ MLP inference
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+  __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<uint32_t*>(&v);
+}
+
+__device__ __forceinline__ void mma_bf16(float* c, const uint32_t* a, uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__global__ void __launch_bounds__(INF_WARPS * 32)
+mlp_infer_k(int64_t n, const int64_t* n_dev, const __nv_bfloat16* __restrict__ feat, const __nv_bfloat16* __restrict__ W1,
+            const float* __restrict__ b1, const __nv_bfloat16* __restrict__ W2, const float* __restrict__ b2,
+            const float* __restrict__ w3, float b3, float* __restrict__ logit) {
+  extern __shared__ __align__(16) uint8_t mlp_smem[];
+  __nv_bfloat16* sW2 = reinterpret_cast<__nv_bfloat16*>(mlp_smem);
+  __nv_bfloat16* sW1 = sW2 + MLP_H * W2_STRIDE;
+  float* sb1 = reinterpret_cast<float*>(sW1 + MLP_H * W1_STRIDE);
+  float* sb2 = sb1 + MLP_H;
+  float* sw3 = sb2 + MLP_H;
+  for (int i = threadIdx.x; i < MLP_H * MLP_H; i += blockDim.x) sW2[(i / MLP_H) * W2_STRIDE + (i % MLP_H)] = W2[i];
+  for (int i = threadIdx.x; i < MLP_H * MLP_IN; i += blockDim.x) sW1[(i / MLP_IN) * W1_STRIDE + (i % MLP_IN)] = W1[i];
+  for (int i = threadIdx.x; i < MLP_H; i += blockDim.x) {
+    sb1[i] = b1[i];
+    sb2[i] = b2[i];
+    sw3[i] = w3[i];
+  }
+  __syncthreads();
+  if (n_dev) n = min(n, *n_dev);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
+  const int64_t n_tiles = (n + 15) >> 4;
+  for (int64_t tile = (int64_t)blockIdx.x * INF_WARPS + warp; tile < n_tiles; tile += (int64_t)gridDim.x * INF_WARPS) {
+    const int64_t r0 = tile << 4;
+    // A fragment of the 16 x 16 input tile (rows beyond n read as zero)
+    uint32_t a[4];
+    {
+      const int64_t ra = r0 + g, rb = r0 + g + 8;
+      const uint32_t* fa = reinterpret_cast<const uint32_t*>(feat + ra * MLP_IN);
+      const uint32_t* fb = reinterpret_cast<const uint32_t*>(feat + rb * MLP_IN);
+      a[0] = ra < n ? fa[t] : 0u;
+      a[1] = rb < n ? fb[t] : 0u;
+      a[2] = ra < n ? fa[t + 4] : 0u;
+      a[3] = rb < n ? fb[t + 4] : 0u;
+    }
+    // layer 1: 32 n-tiles of 8 outputs; ReLU; repacked as layer-2 A fragments (16 k-steps x 4 regs)
+    uint32_t h1[16][4];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      float c[4] = {0.f, 0.f, 0.f, 0.f};
+      const __nv_bfloat16* wrow = sW1 + (8 * j + g) * W1_STRIDE;
+      const uint32_t b0 = *reinterpret_cast<const uint32_t*>(wrow + 2 * t);
+      const uint32_t bb = *reinterpret_cast<const uint32_t*>(wrow + 8 + 2 * t);
+      mma_bf16(c, a, b0, bb);
+      const int col = 8 * j + 2 * t;
+      const float x0 = fmaxf(c[0] + sb1[col], 0.f), x1 = fmaxf(c[1] + sb1[col + 1], 0.f);
+      const float x2 = fmaxf(c[2] + sb1[col], 0.f), x3 = fmaxf(c[3] + sb1[col + 1], 0.f);
+      const int kk = j >> 1;
+      if ((j & 1) == 0) {
+        h1[kk][0] = pack_bf16(x0, x1);
+        h1[kk][1] = pack_bf16(x2, x3);
+      } else {
+        h1[kk][2] = pack_bf16(x0, x1);
+        h1[kk][3] = pack_bf16(x2, x3);
+      }
+    }
+    // layers 2 + 3 in chunks of 64 output columns
+    float za = 0.f, zb = 0.f;   // partial logits of rows g and g + 8
+#pragma unroll 1
+    for (int ch = 0; ch < 4; ++ch) {
+      float c[8][4];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) c[j][0] = c[j][1] = c[j][2] = c[j][3] = 0.f;
+#pragma unroll
+      for (int kk = 0; kk < 16; ++kk) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const __nv_bfloat16* wrow = sW2 + (64 * ch + 8 * j + g) * W2_STRIDE + 16 * kk;
+          const uint32_t b0 = *reinterpret_cast<const uint32_t*>(wrow + 2 * t);
+          const uint32_t bb = *reinterpret_cast<const uint32_t*>(wrow + 8 + 2 * t);
+          mma_bf16(c[j], h1[kk], b0, bb);
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int col = 64 * ch + 8 * j + 2 * t;
+        za += fmaxf(c[j][0] + sb2[col], 0.f) * sw3[col] + fmaxf(c[j][1] + sb2[col + 1], 0.f) * sw3[col + 1];
+        zb += fmaxf(c[j][2] + sb2[col], 0.f) * sw3[col] + fmaxf(c[j][3] + sb2[col + 1], 0.f) * sw3[col + 1];
+      }
+    }
+    za += __shfl_xor_sync(VK_FULL, za, 1);
+    za += __shfl_xor_sync(VK_FULL, za, 2);
+    zb += __shfl_xor_sync(VK_FULL, zb, 1);
+    zb += __shfl_xor_sync(VK_FULL, zb, 2);
+    if (t == 0) {
+      if (r0 + g < n) logit[r0 + g] = za + b3;
+      if (r0 + g + 8 < n) logit[r0 + g + 8] = zb + b3;
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------------ selection
+__device__ __forceinline__ uint32_t ord_f32(float x) {
+  uint32_t u = __float_as_uint(x);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+// ranking key of a hit: logit, count, row (all descending), hypothesis ascending
+__device__ __forceinline__ unsigned long long prune_key_hi(float logit) { return ord_f32(logit); }
+
+constexpr int PS_WARPS = 4;
+
+__device__ __forceinline__ void warp_bitonic_u64(uint64_t* v, int n_pow2, int lane) {
+  for (int k = 2; k <= n_pow2; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = lane; i < n_pow2; i += 32) {
+        int p = i ^ j;
+        if (p > i) {
+          uint64_t a = v[i], b = v[p];
+          bool up = (i & k) == 0;
+          if ((a > b) == up) { v[i] = b; v[p] = a; }
+        }
+      }
+      __syncwarp();
+    }
+}
+
+// Per spectrum: rank hits by (logit, count, row) desc; keep those with logit >= tau or among the min_keep first,
+// at most max_keep; add partners; sort by (row, hypothesis); merge duplicates (lowest hypothesis, highest count).
+// The hits of spectrum s are [hit_off[s], hit_off[s+1]); hyp-local index = hit_hyp - first hypothesis of s.
+__global__ void __launch_bounds__(PS_WARPS * 32)
+select_pruned_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* hit_off, const int64_t* hit_hyp,
+                const int32_t* hit_row, const int64_t* hit_cnt, const float* logit, float tau, int min_keep,
+                int max_keep, int pair_closure, const int64_t* partner, int cap, int sort_cap, int64_t* c_hyp,
+                int64_t* c_row, int64_t* c_cnt, int64_t* n_cand) {
+  extern __shared__ __align__(16) uint8_t ps_smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int s = blockIdx.x * PS_WARPS + warp;
+  if (s >= n_spec) return;
+  const int list_cap = 2 * max_keep > 32 ? 2 * max_keep : 32;
+  uint64_t* key = reinterpret_cast<uint64_t*>(ps_smem) + (size_t)warp * (sort_cap + list_cap);
+  uint64_t* lst = key + sort_cap;          // (row << 34 | hl << 16 | idx) for the closure sort
+  int32_t* lcnt = reinterpret_cast<int32_t*>(reinterpret_cast<uint64_t*>(ps_smem) +
+                                             (size_t)PS_WARPS * (sort_cap + list_cap)) + (size_t)warp * list_cap;
+  const unsigned lt = (1u << lane) - 1u;
+  const int64_t h0 = spec_hyp_off[s];
+  const int64_t a = hit_off[s], b = hit_off[s + 1];
+  const int n = (int)(b - a);
+  // keys of the hits: ord(logit) << 32 | count(12 bits, saturated) << 20 | index (20 bits); the index order is
+  // (hypothesis, row) ascending, so among equal (logit, count) the later index = higher row wins on "desc"; the
+  // hypothesis tie (same row in two hypotheses) is resolved by the lower index first through the complement below
+  int n_keep = 0;
+  if (n > 0) {
+    if (n > sort_cap) {
+      // more hits than the sort buffer: keep those with logit >= tau by hit order, up to max_keep (rare)
+      for (int i0 = 0; i0 < n && n_keep < max_keep; i0 += 32) {
+        const int i = i0 + lane;
+        const bool take = i < n && logit[a + i] >= tau;
+        const unsigned m = __ballot_sync(VK_FULL, take);
+        if (take) {
+          const int pos = n_keep + __popc(m & lt);
+          if (pos < max_keep) {
+            lst[pos] = ((uint64_t)hit_row[a + i] << 34) | ((uint64_t)(hit_hyp[a + i] - h0) << 16) | (uint64_t)pos;
+            lcnt[pos] = (int32_t)hit_cnt[a + i];
+          }
+        }
+        n_keep = min(max_keep, n_keep + __popc(m));
+      }
+    } else {
+      int n_pow2 = 32;
+      while (n_pow2 < n) n_pow2 <<= 1;
+      for (int i = lane; i < n_pow2; i += 32) {
+        uint64_t k = 0ull;
+        if (i < n) {
+          const uint32_t c = (uint32_t)min(hit_cnt[a + i], (int64_t)4095);
+          const uint32_t rowpart = (uint32_t)i;   // hits are in (hyp, row) order: later index = higher row
+          k = (prune_key_hi(logit[a + i]) << 32) | ((uint64_t)c << 20) | (uint64_t)(rowpart & 0xfffff);
+        }
+        key[i] = k;
+      }
+      __syncwarp();
+      warp_bitonic_u64(key, n_pow2, lane);   // ascending: best hit last
+      for (int r0 = 0; r0 < n && r0 < max_keep; r0 += 32) {
+        const int r = r0 + lane;   // rank, 0 = best
+        bool take = false;
+        int i = 0;
+        if (r < n && r < max_keep) {
+          const uint64_t k = key[n_pow2 - 1 - r];
+          i = (int)(k & 0xfffff);
+          take = r < min_keep || logit[a + i] >= tau;
+        }
+        const unsigned m = __ballot_sync(VK_FULL, take);
+        if (take) {
+          const int pos = n_keep + __popc(m & lt);
+          lst[pos] = ((uint64_t)hit_row[a + i] << 34) | ((uint64_t)(hit_hyp[a + i] - h0) << 16) | (uint64_t)pos;
+          lcnt[pos] = (int32_t)hit_cnt[a + i];
+        }
+        n_keep += __popc(m);
+      }
+    }
+  }
+  __syncwarp();
+  int n_list = n_keep;
+  if (pair_closure) {
+    for (int i = lane; i < n_keep; i += 32) {
+      const uint64_t k = lst[i];
+      const int64_t r = (int64_t)(k >> 34);
+      const uint64_t hl = (k >> 16) & 0x3ffff;
+      lst[n_keep + i] = ((uint64_t)partner[r] << 34) | (hl << 16) | (uint64_t)(n_keep + i);
+      lcnt[n_keep + i] = -1;
+    }
+    n_list = 2 * n_keep;
+  }
+  __syncwarp();
+  int n_pow2 = 1;
+  while (n_pow2 < n_list) n_pow2 <<= 1;
+  for (int i = n_list + lane; i < n_pow2; i += 32) lst[i] = ~0ull;
+  __syncwarp();
+  warp_bitonic_u64(lst, n_pow2, lane);
+  int n_out = 0;
+  const int64_t slot = (int64_t)s * cap;
+  for (int i0 = 0; i0 < n_list; i0 += 32) {
+    const int i = i0 + lane;
+    bool head = false;
+    int64_t r = 0;
+    if (i < n_list) {
+      r = (int64_t)(lst[i] >> 34);
+      head = i == 0 || (int64_t)(lst[i - 1] >> 34) != r;
+    }
+    const unsigned m = __ballot_sync(VK_FULL, head);
+    if (head) {
+      int best = lcnt[lst[i] & 0xffff];
+      for (int k = i + 1; k < n_list && (int64_t)(lst[k] >> 34) == r; ++k) best = max(best, lcnt[lst[k] & 0xffff]);
+      const int pos = n_out + __popc(m & lt);
+      c_hyp[slot + pos] = h0 + (int64_t)((lst[i] >> 16) & 0x3ffff);
+      c_row[slot + pos] = r;
+      c_cnt[slot + pos] = best;
+    }
+    n_out += __popc(m);
+  }
+  if (lane == 0) n_cand[s] = n_out;
+}
+
+}  // namespace
+
+extern "C" {
+
+int vk_cand_features(int64_t n, const int64_t* n_dev, const int64_t* c_hyp, const int64_t* c_row,
+                     const int64_t* c_cnt, const int64_t* win_off, const int64_t* h_lo, const uint32_t* isum,
+                     const float* h_M, const int8_t* h_z, const float* mass32, const uint8_t* len,
+                     const uint8_t* missed, const float* mu, const float* sd, void* feat_bf16, void* stream) {
+  if (n <= 0) return 0;
+  cand_features_k<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
+      n, n_dev, c_hyp, c_row, c_cnt, win_off, h_lo, isum, h_M, h_z, mass32, len, missed, mu, sd,
+      reinterpret_cast<__nv_bfloat16*>(feat_bf16));
+  return vk_launch_status();
+}
+
+int64_t vk_mlp_infer_smem(void) {
+  return (int64_t)MLP_H * W2_STRIDE * 2 + (int64_t)MLP_H * W1_STRIDE * 2 + 3 * MLP_H * 4;
+}
+
+int vk_mlp_infer(int64_t n, const int64_t* n_dev, const void* feat_bf16, const void* W1_bf16, const float* b1, const void* W2_bf16,
+                 const float* b2, const float* w3, float b3, float* logit, int grid, void* stream) {
+  if (n <= 0) return 0;
+  if (grid < 1) return VK_E_ARG;
+  size_t sh = (size_t)vk_mlp_infer_smem();
+  cudaError_t e = cudaFuncSetAttribute(mlp_infer_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  if (e != cudaSuccess) return vk_err(e);
+  mlp_infer_k<<<grid, INF_WARPS * 32, sh, (cudaStream_t)stream>>>(
+      n, n_dev, reinterpret_cast<const __nv_bfloat16*>(feat_bf16), reinterpret_cast<const __nv_bfloat16*>(W1_bf16), b1,
+      reinterpret_cast<const __nv_bfloat16*>(W2_bf16), b2, w3, b3, logit);
+  return vk_launch_status();
+}
+
+int vk_select_pruned(int n_spec, const int64_t* spec_hyp_off, const int64_t* hit_off, const int64_t* hit_hyp,
+                     const int32_t* hit_row, const int64_t* hit_cnt, const float* logit, float tau, int min_keep,
+                     int max_keep, int pair_closure, const int64_t* partner, int cap, int64_t* c_hyp, int64_t* c_row,
+                     int64_t* c_cnt, int64_t* n_cand, void* stream) {
+  if (n_spec == 0) return 0;
+  if (max_keep < 1 || min_keep < 0 || min_keep > max_keep || cap < (pair_closure ? 2 : 1) * max_keep) return VK_E_ARG;
+  const int sort_cap = 1024;
+  const int list_cap = 2 * max_keep > 32 ? 2 * max_keep : 32;
+  int list_pow2 = 1;
+  while (list_pow2 < list_cap) list_pow2 <<= 1;
+  if (list_pow2 != list_cap) return VK_E_ARG;   // max_keep a power of two (>= 16)
+  size_t sh = (size_t)PS_WARPS * (sort_cap + list_cap) * 8 + (size_t)PS_WARPS * list_cap * 4;
+  if (sh > 200 * 1024) return VK_E_ARG;
+  cudaError_t e = cudaFuncSetAttribute(select_pruned_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  if (e != cudaSuccess) return vk_err(e);
+  select_pruned_k<<<(unsigned)((n_spec + PS_WARPS - 1) / PS_WARPS), PS_WARPS * 32, sh, (cudaStream_t)stream>>>(
+      n_spec, spec_hyp_off, hit_off, hit_hyp, hit_row, hit_cnt, logit, tau, min_keep, max_keep, pair_closure, partner,
+      cap, sort_cap, c_hyp, c_row, c_cnt, n_cand);
+  return vk_launch_status();
+}
+
+}  // extern "C"

@@ -81,7 +81,7 @@ _SIGS_B200 = {
     "vk_hyp_fill": [I32, P, P, P, I32, I32, I32, I32, F32, F32, I32, P, I64, P, P, P, P, P, P, P, P, P, P],
     "vk_k1_plan_count": [P, I64, P, P, P, P, P],
     "vk_k1_plan_fill": [P, I64, P, P, P, P, P, P],
-    "vk_k1_tiles": [P, P, F32, F32, I32, P, P, P, P, P, P, P, P, P, P, P, P],
+    "vk_k1_tiles": [P, P, F32, F32, I32, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P],
     "vk_select_topk": [I32, P, P, P, P, P, P, I32, I32, I32, I32, P, P, P, P, P, P, P, P, P],
     "vk_compact_cands": [I32, I32, P, P, P, P, P, P, P, P, P, P, P, P],
     "vk_k2_spectra": [P, I32, P, P, P, P, P, P, P, P, P, P, P, F32, F32, P, P, P, P, P, P, P, P, P, P],
@@ -89,6 +89,16 @@ _SIGS_B200 = {
     "vk_search_fused": [P, P, P, I32, I32, I32, P, P, P, P, P, P, P, P, P, P],
     "vk_search_fused_smem": [P, I32, I32, I32, I32, P],
     "vk_search_fused_grid": [P, I32, I32, I32, I32, P],
+    "vk_cand_features": [I64, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P],
+    "vk_mlp_infer": [I64, P, P, P, P, P, P, P, F32, P, I32, P],
+    "vk_select_pruned": [I32, P, P, P, P, P, P, F32, I32, I32, I32, P, I32, P, P, P, P, P],
+    "vk_gemm": [I32, I32, I32, P, I64, I64, P, I32, I64, I64, P, I32, I32, P, I64, I64, P],
+    "vk_colsum": [I32, I32, P, P, P],
+    "vk_relu_mask": [I64, P, P, P],
+    "vk_bce": [I32, P, P, P, F32, P, P, P],
+    "vk_adam": [I64, P, P, P, P, F32, F32, F32, F32, I32, F32, P, P],
+    "vk_to_bf16": [I64, P, P, P],
+    "vk_bf16_to_f32": [I64, P, P, P],
 }
 
 _lib = None
@@ -108,6 +118,8 @@ def lib():
     L.vk_scan_tmp_bytes.restype = I64
     L.vk_scan_noalloc_max_n.argtypes = []
     L.vk_scan_noalloc_max_n.restype = I64
+    L.vk_mlp_infer_smem.argtypes = []
+    L.vk_mlp_infer_smem.restype = I64
     _lib = L
     return L
 
@@ -125,7 +137,8 @@ def stream():
 
 _TRACE = os.environ.get("VK_TRACE") == "1"
 # kernels launched by one successful call of an entry point (default 1); `LAUNCHES` counts them
-_KERNELS_PER_CALL = {"scan": 3, "set_params": 0, "set_nterm": 0, "set_tol_da": 0, "tindex_layout": 0}
+_KERNELS_PER_CALL = {"scan": 3, "set_params": 0, "set_nterm": 0, "set_tol_da": 0, "tindex_layout": 0,
+                     "fused_grid": 0}
 LAUNCHES = {"n": 0}
 
 

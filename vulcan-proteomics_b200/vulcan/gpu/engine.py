@@ -119,6 +119,7 @@ class GpuIndex:
         self.mass32 = up(l1.mass32.astype(np.float32))
         self.residues = up(l1.residues.astype(np.uint8))
         self.partner = up(l1.partner.astype(np.int64))
+        self.missed = up(np.asarray(l1.missed).astype(np.uint8))
         if self.n >= 2 ** ROW_BITS:
             raise ValueError("index rows must be < 2^28")
         # reference layout constants (used by the compatible entry points)
@@ -132,7 +133,7 @@ class GpuIndex:
         self.build_s = time.perf_counter() - t0
         self.device_bytes = sum(t.numel() * t.element_size() for t in
                                 [self.seq_off, self.length, self.mask, self.mass32, self.residues, self.partner,
-                                 self.tile_off, self.cbin_off, self.postings])
+                                 self.missed, self.tile_off, self.cbin_off, self.postings])
 
     def table_ptrs(self):
         return (K.ptr(self.seq_off), K.ptr(self.length), K.ptr(self.mask), K.ptr(self.mass32), K.ptr(self.residues))
@@ -354,8 +355,10 @@ def k1_max_win(p: SearchParams) -> int:
     return int(min(4096, max(0, p.max_peaks))) if p.k1_merge else 0
 
 
-def _k1_dense(gi: GpuIndex, dh, peaks, p: SearchParams, n_hyp: int, stats: Stats | None = None):
-    """Tiled K1: dense counts of every window row.  Returns (win_off, cnt)."""
+def _k1_dense(gi: GpuIndex, dh, peaks, p: SearchParams, n_hyp: int, stats: Stats | None = None,
+              isum: bool = False):
+    """Tiled K1: dense counts of every window row.  Returns (win_off, cnt, status), plus the summed matched
+    intensity of every window row (u32, 2^24 = the spectrum's TIC) when ``isum``."""
     L = K.lib()
     dev = gi.dev
     ix = gi.tix
@@ -373,13 +376,17 @@ def _k1_dense(gi: GpuIndex, dh, peaks, p: SearchParams, n_hyp: int, stats: Stats
                               K.ptr(cursor), K.ptr(item_hyp), K.stream()), "k1_plan_fill")
     cnt = torch.empty(max(n_win, 1), dtype=torch.int32, device=dev)
     status = torch.zeros(1, dtype=torch.int32, device=dev)
+    isw = torch.empty(max(n_win, 1), dtype=torch.int32, device=dev) if isum else None
     K.check(L.vk_k1_tiles(C.byref(ix), C.byref(gi.fp), float(p.fragment_ppm[0]), float(p.fragment_ppm[1]),
                           k1_max_win(p), K.ptr(item_off), K.ptr(item_hyp), K.ptr(dh["spec"]), K.ptr(dh["maxfz"]), K.ptr(dh["lo"]),
                           K.ptr(dh["hi"]), K.ptr(win_off), K.ptr(peaks["off"]), K.ptr(peaks["mass"]), K.ptr(cnt),
-                          K.ptr(status), K.stream()), "k1_tiles")
+                          K.ptr(status), K.ptr(peaks["int"]) if isum else None, K.ptr(peaks["tic"]) if isum else None,
+                          K.ptr(isw) if isum else None, K.stream()), "k1_tiles")
     if stats is not None:
         stats.counts["k1_work_items"] = stats.counts.get("k1_work_items", 0) + n_items
         stats.counts["k1_window_candidates"] = stats.counts.get("k1_window_candidates", 0) + n_win
+    if isum:
+        return win_off, cnt[:n_win], status, isw[:n_win]
     return win_off, cnt[:n_win], status
 
 
@@ -569,10 +576,66 @@ def psm_table(sp: Spectra, gi: GpuIndex, l1, hyp, h, r, k1c, k2, scored, matched
     return _psm_columns(sp, l1, rec, p)
 
 
+def _shortlist(gi: GpuIndex, p: SearchParams, n: int, dh, win_off, cnt, topk: int, closure: bool,
+               thr: int | None = None):
+    """Top-k of every spectrum by K1 count among the rows with count >= thr (default ``p.k1_threshold``;
+    ``vk_select_topk``), optionally with pair closure, compacted to spectrum-ordered candidate lists.  Returns the
+    candidate dict and the per-hypothesis / per-spectrum K1 sums (which do not depend on thr)."""
+    L = K.lib()
+    dev = gi.dev
+    n_h = dh["n_max"]
+    cap = (2 if closure else 1) * topk
+    s_hyp = torch.empty(max(n * cap, 1), dtype=torch.int64, device=dev)
+    s_row = torch.empty_like(s_hyp)
+    s_cnt = torch.empty_like(s_hyp)
+    n_cand = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
+    hyp_scored = torch.empty(max(n_h, 1), dtype=torch.int32, device=dev)
+    hyp_matched = torch.empty(max(n_h, 1), dtype=torch.int64, device=dev)
+    spec_scored = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
+    spec_matched = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
+    K.check(L.vk_select_topk(n, K.ptr(dh["spec_off"]), K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(win_off),
+                             K.ptr(cnt), K.ptr(gi.partner), p.k1_threshold if thr is None else thr, topk,
+                             int(closure), cap,
+                             K.ptr(s_hyp), K.ptr(s_row), K.ptr(s_cnt), K.ptr(n_cand), K.ptr(hyp_scored),
+                             K.ptr(hyp_matched), K.ptr(spec_scored), K.ptr(spec_matched), K.stream()),
+            "select_topk")
+    cand = _compact(n, cap, n_cand, s_hyp, s_row, s_cnt, dh, dev)
+    sums = {"hyp_scored": hyp_scored, "hyp_matched": hyp_matched, "spec_scored": spec_scored,
+            "spec_matched": spec_matched}
+    return cand, sums
+
+
+def _compact(n: int, cap: int, n_cand, s_hyp, s_row, s_cnt, dh, dev):
+    """Per-spectrum candidate slots (``cap`` each) -> contiguous lists in spectrum order (``vk_compact_cands``)."""
+    L = K.lib()
+    cand_off = _scan(n_cand[:n])
+    c_hyp = torch.empty_like(s_hyp)
+    c_row = torch.empty_like(s_hyp)
+    c_cnt = torch.empty_like(s_hyp)
+    c_row32 = torch.empty(max(n * cap, 1), dtype=torch.int32, device=dev)
+    c_maxfz = torch.empty(max(n * cap, 1), dtype=torch.int8, device=dev)
+    K.check(L.vk_compact_cands(n, cap, K.ptr(n_cand), K.ptr(cand_off), K.ptr(s_hyp), K.ptr(s_row), K.ptr(s_cnt),
+                               K.ptr(dh["maxfz"]), K.ptr(c_hyp), K.ptr(c_row), K.ptr(c_cnt), K.ptr(c_row32),
+                               K.ptr(c_maxfz), K.stream()), "compact_cands")
+    return {"cand_off": cand_off, "c_hyp": c_hyp, "c_row": c_row, "c_cnt": c_cnt, "c_row32": c_row32,
+            "c_maxfz": c_maxfz, "cap": cap, "n_cand": n_cand}
+
+
+def _k2_cands(gi: GpuIndex, p: SearchParams, n: int, cand, peaks):
+    """K2 (``vk_k2_spectra``) over compacted candidate lists; one output row per candidate."""
+    L = K.lib()
+    dev = gi.dev
+    k2 = _k2_outputs(max(n * cand["cap"], 1), dev)
+    K.check(L.vk_k2_spectra(C.byref(gi.fp), n, K.ptr(cand["cand_off"]), K.ptr(cand["c_row32"]),
+                            K.ptr(cand["c_maxfz"]), K.ptr(peaks["off"]), K.ptr(peaks["mass"]), K.ptr(peaks["int"]),
+                            *gi.table_ptrs(), float(p.fragment_ppm[0]), float(p.fragment_ppm[1]), None,
+                            *_k2_ptrs(k2), K.stream()), "k2_spectra")
+    return k2
+
+
 def _search_device(run: DeviceRun, gi: GpuIndex, p: SearchParams, report: int, st: Stats, timers: bool = False):
     """The whole hot path on the device for one run whose raw spectra are already resident.  Returns the device
     PSM slots and the intermediates."""
-    L = K.lib()
     dev = gi.dev
     n = run.n
 
@@ -585,42 +648,14 @@ def _search_device(run: DeviceRun, gi: GpuIndex, p: SearchParams, report: int, s
     n_h = dh["n_max"]
     with phase("k1"):
         win_off, cnt, status = _k1_dense(gi, dh, peaks, p, n_h, st)
-    cap = (2 if p.pair_closure else 1) * p.topk
     with phase("topk"):
-        s_hyp = torch.empty(max(n * cap, 1), dtype=torch.int64, device=dev)
-        s_row = torch.empty_like(s_hyp)
-        s_cnt = torch.empty_like(s_hyp)
-        n_cand = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
-        hyp_scored = torch.empty(max(n_h, 1), dtype=torch.int32, device=dev)
-        hyp_matched = torch.empty(max(n_h, 1), dtype=torch.int64, device=dev)
-        spec_scored = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
-        spec_matched = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
-        K.check(L.vk_select_topk(n, K.ptr(dh["spec_off"]), K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(win_off),
-                                 K.ptr(cnt), K.ptr(gi.partner), p.k1_threshold, p.topk, int(p.pair_closure), cap,
-                                 K.ptr(s_hyp), K.ptr(s_row), K.ptr(s_cnt), K.ptr(n_cand), K.ptr(hyp_scored),
-                                 K.ptr(hyp_matched), K.ptr(spec_scored), K.ptr(spec_matched), K.stream()),
-                "select_topk")
-        cand_off = _scan(n_cand[:n])
-        c_hyp = torch.empty_like(s_hyp)
-        c_row = torch.empty_like(s_hyp)
-        c_cnt = torch.empty_like(s_hyp)
-        c_row32 = torch.empty(max(n * cap, 1), dtype=torch.int32, device=dev)
-        c_maxfz = torch.empty(max(n * cap, 1), dtype=torch.int8, device=dev)
-        K.check(L.vk_compact_cands(n, cap, K.ptr(n_cand), K.ptr(cand_off), K.ptr(s_hyp), K.ptr(s_row), K.ptr(s_cnt),
-                                   K.ptr(dh["maxfz"]), K.ptr(c_hyp), K.ptr(c_row), K.ptr(c_cnt), K.ptr(c_row32),
-                                   K.ptr(c_maxfz), K.stream()), "compact_cands")
+        cand, sums = _shortlist(gi, p, n, dh, win_off, cnt, p.topk, bool(p.pair_closure))
     with phase("k2"):
-        k2 = _k2_outputs(max(n * cap, 1), dev)
-        K.check(L.vk_k2_spectra(C.byref(gi.fp), n, K.ptr(cand_off), K.ptr(c_row32), K.ptr(c_maxfz),
-                                K.ptr(peaks["off"]), K.ptr(peaks["mass"]), K.ptr(peaks["int"]), *gi.table_ptrs(),
-                                float(p.fragment_ppm[0]), float(p.fragment_ppm[1]), None, *_k2_ptrs(k2), K.stream()),
-                "k2_spectra")
+        k2 = _k2_cands(gi, p, n, cand, peaks)
     with phase("rank"):
-        psm = _rank_device(n, cand_off, c_row, k2, p, report, dev)
-    return {"peaks": peaks, "dh": dh, "win_off": win_off, "cnt": cnt, "status": status, "cand_off": cand_off,
-            "c_hyp": c_hyp, "c_row": c_row, "c_cnt": c_cnt, "c_row32": c_row32, "c_maxfz": c_maxfz, "cap": cap,
-            "n_cand": n_cand, "k2": k2, "psm": psm, "hyp_scored": hyp_scored,
-            "hyp_matched": hyp_matched, "spec_scored": spec_scored, "spec_matched": spec_matched}
+        psm = _rank_device(n, cand["cand_off"], cand["c_row"], k2, p, report, dev)
+    return {"peaks": peaks, "dh": dh, "win_off": win_off, "cnt": cnt, "status": status, **cand, "k2": k2,
+            "psm": psm, **sums}
 
 
 _K2_KEYS = (("hs", "hyperscore", torch.float64), ("sb", "summed_b", torch.float32),
