@@ -4,15 +4,20 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload human|small]
 
 One step = one pass of the search over one MS2 run of the workload (human: 40,000 simulated spectra of uneven
-peak counts, 20-600, against the ~5.5M-peptidoform human-scale index, top-k 100): K0 peak view, hypotheses, K1
-fragment-index counting, top-K + pair closure, K2 exact rescoring, PSM ranking.
+peak counts, 20-600, against the ~5.5M-peptidoform human-scale index, top-k 100).  The headline path (--path
+pruned) is the learned-pruned search: K0 peak view, hypotheses, K1 fragment-index counting with intensity sums,
+top-k shortlist (count floor), BF16 MLP scores, calibrated selection + pair closure, K2 exact rescoring, PSM
+ranking.  Its pruner is trained first on the GPU (untimed) from 200,000 simulated spectra of other runs and
+calibrated on one more run to >= 99.95% top-1 recall; the plain exhaustive path (K1 -> top-k -> pair closure ->
+K2) is then timed the same way on the same run and the pruned path's top-1 recall and PSMs at 1% q are judged
+against it (`vs_plain`).
 
   value      spectra/s with the run's raw spectra already in HBM (device pass, CUDA events on the stream, L2
              flushed between steps), summed over ranks (each rank searches its own run: weak scaling)
-  e2e        spectra/s through the public API engine.search(Spectra) with host buffers: H2D of the raw spectra,
-             the device pass, D2H of the PSM rows and the host PSM table (wall clock around each call)
+  e2e        spectra/s through the public API (prune.search_pruned / engine.search) with host buffers: H2D of the
+             raw spectra, the device pass, D2H of the PSM rows and the host PSM table (wall clock around each call)
   roofline   the dominant kernel's algorithmic bytes per launch / its mean CUDA-event duration vs the measured
-             HBM copy bandwidth
+             HBM copy bandwidth; mlp_roofline: the MLP's FLOPs / duration vs the measured bf16 tensor peak
   cpu_baseline  the CPU oracle (C/OpenMP restatement of the reference kernels) on a bounded sample, all cores
 
 --impl reference times the CPU path of the reference (its C restatement: the reference ships no CPU search of
@@ -58,8 +63,9 @@ def _workload_setup(name: str, rank: int):
     d = synth.build_index(w, CACHE)
     t_build = time.perf_counter() - t0
     l1 = L1Index(d)
-    sp, rows = synth.simulate_run(l1, read_labels(d), w, seed=w.spectra_seed + 1000 * rank, run=f"run{rank}")
-    return w, l1, sp, t_build
+    lab = read_labels(d)
+    sp, rows = synth.simulate_run(l1, lab, w, seed=w.spectra_seed + 1000 * rank, run=f"run{rank}")
+    return w, l1, lab, sp, t_build
 
 
 def _params(w, a):
@@ -75,7 +81,7 @@ def _config(w, p, extra=None):
     cfg = {"workload": f"{w.name}: {w.n_proteins} random proteins (<= {w.missed_cleavages} missed cleavages, "
                        f"length {w.min_len}-{w.max_len}, CAM-C, Met-ox <= {w.max_var}, pseudo-reverse decoys); "
                        f"runs of {w.n_spectra} simulated MS2 spectra, charge {w.charges[0]}-{w.charges[1]}",
-           "path": "plain exhaustive search (K1 -> top-k -> K2), no learned pruner",
+           "path": "plain exhaustive search (K1 -> top-k -> pair closure -> K2), no learned pruner",
            "method": ("fused persistent kernel (K1+top-k+K2+ranking per spectrum)" if p.search_method == "fused"
                       else "staged kernels"),
            "precursor_ppm": list(p.precursor_ppm), "fragment_tol": f"+-{p.fragment_ppm[1]} {p.fragment_unit}",
@@ -220,6 +226,75 @@ def fused_algorithmic_bytes(gi, dh, peaks, oc, n_spec):
             "candidates": int(n_cand.sum().item())}
 
 
+def _pruner_setup(a, w, l1, lab, gi, p, rank):
+    """The learned pruner of the headline path: trained here on the GPU (untimed) from simulated runs disjoint
+    from the benchmark run (exhaustive rescoring labels), its threshold calibrated on one more run; or loaded."""
+    from vulcan import synth
+    from vulcan.gpu import prune as PR
+    if a.pruner != "train":
+        pr = PR.Pruner.load(a.pruner, gi.dev)
+        return pr, {"source": os.path.basename(a.pruner), "tau": pr.tau, "min_count": pr.min_count}
+    t0 = time.perf_counter()
+    n_left, runs, i = a.train_spectra, [], 0
+    while n_left > 0:
+        n = min(n_left, w.n_spectra)
+        runs.append(synth.simulate_run(l1, lab, w, n_spectra=n, seed=70000 + 100 * rank + i, run=f"train{i}")[0])
+        n_left -= n
+        i += 1
+    calib = [synth.simulate_run(l1, lab, w, seed=80000 + rank, run="calib")[0]]
+    t_sim = time.perf_counter() - t0
+    pr, info = PR.train(gi, p, runs, calib, seed=rank, epochs=a.epochs, batch=8192, target=a.target)
+    info.update(source="trained in this run", simulate_s=round(t_sim, 1), min_count=pr.min_count,
+                min_keep=pr.min_keep, max_keep=pr.max_keep, target=a.target,
+                losses=[round(x, 5) for x in info["losses"]])
+    return pr, info
+
+
+def _timed_passes(step, flush, steps, world, dist, K):
+    """CUDA-event time of `steps` device passes (L2 flushed before each), max over ranks; kernel launches counted."""
+    import torch
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    K.LAUNCHES["n"] = 0
+    evs = []
+    out = None
+    for _ in range(steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        out = step()
+        e1.record()
+        evs.append((e0, e1))
+    torch.cuda.synchronize()
+    launches = K.LAUNCHES["n"]
+    if world > 1:
+        dist.barrier()
+    ms = sum(e0.elapsed_time(e1) for e0, e1 in evs)
+    t = torch.tensor([ms], dtype=torch.float64, device=flush.device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item()), launches, out
+
+
+def _timed_e2e(call, n_spec, steps, world, dist, dev):
+    """Wall-clock spectra/s of `steps` calls through the public API (host buffers in, PSM table out)."""
+    import torch
+    call()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    st = None
+    for _ in range(steps):
+        st = call()[1]
+    torch.cuda.synchronize()
+    e2e_s = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(e2e_s, op=dist.ReduceOp.MAX)
+    return n_spec * world * steps / float(e2e_s.item()), st
+
+
 def run_b200(a):
     import torch
     import torch.distributed as dist
@@ -233,89 +308,154 @@ def run_b200(a):
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
     from vulcan.gpu import _lib as K
     from vulcan.gpu import engine as E
-    w, l1, sp, t_build = _workload_setup(a.workload, rank)
+    from vulcan.gpu import prune as PR
+    w, l1, lab, sp, t_build = _workload_setup(a.workload, rank)
     p = _params(w, a)
     gi = E.GpuIndex(l1, p, STATIC, VAR, device=dev)
+    pruned = a.path == "pruned"
+    pr, pr_info = _pruner_setup(a, w, l1, lab, gi, p, rank) if pruned else (None, None)
+    if pruned and a.save_pruner and rank == 0:
+        pr.save(a.save_pruner)
     run = E.DeviceRun(sp, dev)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device=dev)   # 256 MiB > 126 MB L2
     st = E.Stats()
 
-    def step():
+    def step_plain():
         if p.search_method == "fused":
             return E._search_fused_device(run, gi, p, 1, st)
         return E._search_device(run, gi, p, 1, st)
 
+    def step_pruned():
+        return PR._pruned_device(run, gi, p, pr, 1, st)
+    step = step_pruned if pruned else step_plain
     for _ in range(a.warmup):
         step()
     torch.cuda.synchronize()
-    # device pass, timed with events on the launching stream
     clocks = ClockSampler(local)
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    K.LAUNCHES["n"] = 0
-    evs = []
-    for _ in range(a.steps):
-        flush.zero_()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        out = step()
-        e1.record()
-        evs.append((e0, e1))
-    torch.cuda.synchronize()
-    launches = K.LAUNCHES["n"]
-    if world > 1:
-        dist.barrier()
+    ms_max, launches, out = _timed_passes(step, flush, a.steps, world, dist, K)
     clk = clocks.stop()
-    ms = sum(e0.elapsed_time(e1) for e0, e1 in evs)
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
     ms_per_step = ms_max / a.steps
     value = len(sp) * world * a.steps / (ms_max / 1e3)
-    if p.search_method == "fused":
+    if p.search_method == "fused" and not pruned:
         st_ok = int(out["status"][:len(sp)].max())
         if st_ok:
             raise RuntimeError(f"fused search status {st_ok}: spectra over the window capacity or a copy timeout")
-
-    # end to end through the public API (host Spectra in, PSM table out)
     e2e_steps = max(3, min(a.steps, 20))
-    E.search(sp, gi, l1, p)
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    t0 = time.perf_counter()
-    h2d = d2h = 0
-    for _ in range(e2e_steps):
-        tbl, s2, _ = E.search(sp, gi, l1, p)
-        h2d, d2h = s2.h2d_bytes, s2.d2h_bytes
-    torch.cuda.synchronize()
-    e2e_s = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(e2e_s, op=dist.ReduceOp.MAX)
-    e2e = len(sp) * world * e2e_steps / float(e2e_s.item())
+    if pruned:
+        e2e, s2 = _timed_e2e(lambda: PR.search_pruned(sp, gi, l1, p, pr), len(sp), e2e_steps, world, dist, dev)
+    else:
+        e2e, s2 = _timed_e2e(lambda: E.search(sp, gi, l1, p), len(sp), e2e_steps, world, dist, dev)
+    h2d, d2h = s2.h2d_bytes, s2.d2h_bytes
+    comparison = None
+    if pruned:
+        # the plain exhaustive path on the same run, same timing rules, and the pruned path's accuracy against it
+        for _ in range(a.warmup):
+            step_plain()
+        ms_plain, _, _ = _timed_passes(step_plain, flush, a.steps, world, dist, K)
+        e2e_plain, _ = _timed_e2e(lambda: E.search(sp, gi, l1, p), len(sp), e2e_steps, world, dist, dev)
+        ev = PR.evaluate(sp, gi, l1, lab, p, pr)
+        comparison = {"plain_value": round(len(sp) * world * a.steps / (ms_plain / 1e3), 1),
+                      "plain_ms_per_step": round(ms_plain / a.steps, 4), "plain_e2e": round(e2e_plain, 1),
+                      "speedup_device": round(ms_plain / ms_max, 3), "speedup_e2e": round(e2e / e2e_plain, 3),
+                      "top1_recall": round(ev["recall"], 6), "accepted_at_1pct_q_plain": ev["accepted_plain"],
+                      "accepted_at_1pct_q_pruned": ev["accepted_pruned"],
+                      "delta_accepted": round(ev["delta_accepted"], 6), "shortlist_hits": ev["hits"],
+                      "rescored_plain": ev["rescored_plain"], "rescored_pruned": ev["rescored_pruned"]}
 
-    # per-phase device times of both methods (separate passes, phases synchronised)
+    # per-phase device times of both paths (separate passes, phases synchronised)
     phase_ms = {}
-    for method in ("fused", "staged"):
+    paths = [("staged", lambda q, s: E._search_device(run, gi, q, 1, s, timers=True))]
+    if pruned:
+        paths.append(("pruned", lambda q, s: PR._pruned_device(run, gi, q, pr, 1, s, timers=True)))
+    else:
+        paths.append(("fused", lambda q, s: E._search_fused_device(run, gi, E._replace(q, search_method="fused"), 1,
+                                                                   s, timers=True)))
+    for name, fn in paths:
         st_ph = E.Stats()
-        q = E._replace(p, search_method=method)
         for _ in range(3):
             flush.zero_()
-            (E._search_fused_device if method == "fused" else E._search_device)(run, gi, q, 1, st_ph, timers=True)
-        phase_ms[method] = {k: round(v / 3, 4) for k, v in st_ph.gpu_ms.items()}
-    # each main kernel alone (mean CUDA-event duration over 8 launches after 2 warm-up launches, L2 flushed before
-    # each), with its algorithmic bytes; the dominant one goes into `roofline`
-    import ctypes as C
-    L = K.lib()
-    so = E._search_device(run, gi, p, 1, st)
-    peaks, dh = so["peaks"], so["dh"]
-    peak_gbs, peak_kind = _peaks_json()
+            fn(p, st_ph)
+        phase_ms[name] = {k: round(v / 3, 4) for k, v in st_ph.gpu_ms.items()}
 
-    def timed(fn, n=10):
+    peak_gbs, peak_kind = _peaks_json()
+    kern, mlp = _kernel_table(a, p, gi, run, flush, pr, dev)
+    dom = max(kern, key=lambda k: kern[k][0])
+    k_mean, algo = kern[dom]
+    achieved = algo / (k_mean / 1e3) / 1e9
+    traffic = _traffic_from_profiles(dom[:-2] if dom.endswith("_k") else dom)
+    kernels = {k: {"mean_launch_ms": round(v[0], 4), "algorithmic_bytes": v[1],
+                   "algorithmic_gbs": round(v[1] / (v[0] / 1e3) / 1e9, 1)} for k, v in kern.items()}
+
+    if rank == 0:
+        cpu = None
+        if world == 1:
+            rate, n_s, t_s, cores = cpu_rate(l1, sp, p, a.cpu_budget)
+            cpu = {"value": round(rate, 1), "unit": "spectra/s", "cores": cores, "kind": "port",
+                   "sample": f"first {n_s} spectra of the run through the oracle's plain path K0->hypotheses->K1->"
+                             f"top-k->K2->ranking ({t_s:.1f} s)"}
+        extra = {"spectra_per_step_per_gpu": len(sp), "index_rows": len(l1), "index_postings": gi.n_postings,
+                 "tile_rows": p.tile_rows, "parallelism": f"replicas x{world} (one run per GPU)"}
+        if pruned:
+            extra["path"] = ("learned-pruned search: K1 (+ intensity sums) -> top-k shortlist of hits with count >= "
+                             f"{pr.min_count} -> BF16 MLP 16-256-256-1 -> logit >= calibrated tau or best "
+                             f"{pr.min_keep} -> pair closure -> K2 -> ranking")
+            extra["pruner"] = pr_info
+        line = {
+            "metric": METRIC, "value": round(value, 1), "unit": "spectra/s", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (MLP: bf16 weights, fp32 accumulate)" if pruned else "f32",
+            "data": "synthetic",
+            "config": _config(w, p, extra),
+            "e2e": {"value": round(e2e, 1), "unit": "spectra/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1),
+                         "peak": peak_gbs, "unit": "GB/s", "frac": round(achieved / peak_gbs, 4),
+                         "peak_source": peak_kind, "traffic": traffic, "algorithmic_bytes": algo,
+                         "mean_launch_ms": round(k_mean, 4)},
+            "kernels": kernels,
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "phase_ms": phase_ms,
+            "index_build_s": round(t_build, 1),
+        }
+        if mlp:
+            line["mlp_roofline"] = mlp
+        if comparison:
+            line["vs_plain"] = comparison
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def _tensor_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d.get("bf16_tflops", 1590.0)), "measured (burst)"
+    return 1590.0, "fallback"
+
+
+def _kernel_table(a, p, gi, run, flush, pr, dev):
+    """Each main kernel of the timed path alone: mean CUDA-event duration over 8 launches after 2 warm-up launches
+    (L2 flushed before each) and its algorithmic bytes; for the pruned path also the MLP's tensor roofline."""
+    import ctypes as C
+    import torch
+    from vulcan.gpu import _lib as K
+    from vulcan.gpu import engine as E
+    from vulcan.gpu import prune as PR
+    L = K.lib()
+    st = E.Stats()
+    pruned = pr is not None
+    so = PR._pruned_device(run, gi, p, pr, 1, st) if pruned else E._search_device(run, gi, p, 1, st)
+    peaks, dh = so["peaks"], so["dh"]
+    n = run.n
+
+    def timed(fn, reps=10):
         ts = []
-        for _ in range(n):
+        for _ in range(reps):
             flush.zero_()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
@@ -337,15 +477,24 @@ def run_b200(a):
                               K.ptr(cursor), K.ptr(item_hyp), K.stream()), "k1_plan_fill")
     status = torch.zeros(1, dtype=torch.int32, device=dev)
     win_off, cnt = so["win_off"], so["cnt"]
+    n_win = int(win_off[-1])
+    isum = so.get("isum")
     kern = {}
     ms_k1 = timed(lambda: K.check(L.vk_k1_tiles(
         C.byref(gi.tix), C.byref(gi.fp), float(p.fragment_ppm[0]), float(p.fragment_ppm[1]), E.k1_max_win(p),
         K.ptr(item_off), K.ptr(item_hyp), K.ptr(dh["spec"]), K.ptr(dh["maxfz"]), K.ptr(dh["lo"]), K.ptr(dh["hi"]),
-        K.ptr(win_off), K.ptr(peaks["off"]), K.ptr(peaks["mass"]), K.ptr(cnt), K.ptr(status), None, None, None,
-        K.stream()), "k1_tiles"))
-    kern["k1_tiles_k"] = (ms_k1, k1_algorithmic_bytes(gi, dh, peaks, win_off, item_off, item_hyp))
-    n = run.n
-    cap = so["cap"]
+        K.ptr(win_off), K.ptr(peaks["off"]), K.ptr(peaks["mass"]), K.ptr(cnt), K.ptr(status),
+        K.ptr(peaks["int"]) if pruned else None, K.ptr(peaks["tic"]) if pruned else None,
+        K.ptr(isum) if pruned else None, K.stream()), "k1_tiles"))
+    k1b = k1_algorithmic_bytes(gi, dh, peaks, win_off, item_off, item_hyp)
+    if pruned:   # peak intensities per item and the window-row intensity sums
+        s_it = dh["spec"][item_hyp.long()].long()
+        k1b += int(((peaks["off"][s_it + 1] - peaks["off"][s_it]) * 4).sum().item()) + n_win * 4
+    kern["k1_tiles_k"] = (ms_k1, k1b)
+    hits = so["hits"] if pruned else so
+    thr = max(p.k1_threshold, pr.min_count) if pruned else p.k1_threshold
+    closure = 0 if pruned else int(p.pair_closure)
+    cap = hits["cap"]
     tk = {k: torch.empty(max(n * cap, 1), dtype=torch.int64, device=dev) for k in ("h", "r", "c")}
     tk_n = torch.empty(n, dtype=torch.int64, device=dev)
     hs_ = torch.empty(dh["n_max"], dtype=torch.int32, device=dev)
@@ -354,11 +503,26 @@ def run_b200(a):
     sm_ = torch.empty(n, dtype=torch.int64, device=dev)
     ms_tk = timed(lambda: K.check(L.vk_select_topk(
         n, K.ptr(dh["spec_off"]), K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(win_off), K.ptr(cnt), K.ptr(gi.partner),
-        p.k1_threshold, p.topk, int(p.pair_closure), cap, K.ptr(tk["h"]), K.ptr(tk["r"]), K.ptr(tk["c"]),
+        thr, p.topk, closure, cap, K.ptr(tk["h"]), K.ptr(tk["r"]), K.ptr(tk["c"]),
         K.ptr(tk_n), K.ptr(hs_), K.ptr(hm_), K.ptr(ss_), K.ptr(sm_), K.stream()), "select_topk"))
+    n_hit = int(hits["cand_off"][-1])
+    n_sel = int(((hits["c_cnt"][:n_hit] >= 0)).sum())
+    kern["select_topk_k"] = (ms_tk, n_win * 4 + n_sel * 8 + n_hit * 24 + dh["n_max"] * 12 + n * 16)
+    mlp = None
+    if pruned:
+        feat = so["feat"]
+        ms_f = timed(lambda: pr.features(gi, dh, win_off, isum, hits, n_hit))
+        kern["cand_features_k"] = (ms_f, n_hit * 87)
+        ms_m = timed(lambda: pr.logits(feat, n_hit))
+        flops = 2 * n_hit * (16 * 256 + 256 * 256 + 256)
+        kern["mlp_infer_k"] = (ms_m, n_hit * 36 + 2 * (256 * 16 + 256 * 256) + 4 * 256 * 3)
+        tpk, tkind = _tensor_peak()
+        ach = flops / (ms_m / 1e3) / 1e12
+        mlp = {"bound": "tensor", "kernel": "mlp_infer_k", "achieved": round(ach, 1), "peak": tpk,
+               "unit": "TFLOP/s", "frac": round(ach / tpk, 4), "peak_source": tkind, "flops_per_launch": flops,
+               "hits_per_launch": n_hit, "mean_launch_ms": round(ms_m, 4),
+               "instruction": "mma.sync m16n8k16 bf16 (fp32 accumulate)"}
     n_cand = int(so["cand_off"][-1])
-    n_sel = int(((so["c_cnt"][:n_cand] >= 0)).sum())
-    kern["select_topk_k"] = (ms_tk, int(win_off[-1]) * 4 + n_sel * 8 + n_cand * 24 + dh["n_max"] * 12 + n * 16)
     k2o = E._k2_outputs(max(n_cand, 1), dev)
     ms_k2 = timed(lambda: K.check(L.vk_k2_spectra(
         C.byref(gi.fp), n, K.ptr(so["cand_off"]), K.ptr(so["c_row32"]), K.ptr(so["c_maxfz"]), K.ptr(peaks["off"]),
@@ -368,51 +532,11 @@ def run_b200(a):
     npk = (peaks["off"][1:n + 1] - peaks["off"][:n]).clamp(max=512)
     k2_bytes = int(((21 + gi.length[rows].long() + 5 + 28).sum() + npk.sum() * 8 + n * 16).item())
     kern["k2_spectra_k"] = (ms_k2, k2_bytes)
-    if p.search_method == "fused":
+    if p.search_method == "fused" and not pruned:
         kern = {"fused_search_k": (timed(lambda: E._fused_device(gi, p, 1, peaks, dh, run.n)),
                                    fused_algorithmic_bytes(gi, dh, peaks, E._fused_device(gi, p, 1, peaks, dh, run.n,
                                                                                           cand=True), n)["total"])}
-    dom = max(kern, key=lambda k: kern[k][0])
-    k_mean, algo = kern[dom]
-    achieved = algo / (k_mean / 1e3) / 1e9
-    traffic = _traffic_from_profiles(dom[:-2] if dom.endswith("_k") else dom)
-    kernels = {k: {"mean_launch_ms": round(v[0], 4), "algorithmic_bytes": v[1],
-                   "algorithmic_gbs": round(v[1] / (v[0] / 1e3) / 1e9, 1)} for k, v in kern.items()}
-    n_rescored = n_cand
-
-    if rank == 0:
-        cpu = None
-        if world == 1:
-            rate, n_s, t_s, cores = cpu_rate(l1, sp, p, a.cpu_budget)
-            cpu = {"value": round(rate, 1), "unit": "spectra/s", "cores": cores, "kind": "port",
-                   "sample": f"first {n_s} spectra of the run through the oracle's K0->hypotheses->K1->top-k->K2->"
-                             f"ranking ({t_s:.1f} s)"}
-        line = {
-            "metric": METRIC, "value": round(value, 1), "unit": "spectra/s", "n_gpus": world, "steps": a.steps,
-            "warmup": a.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": _config(w, p, {"spectra_per_step_per_gpu": len(sp), "index_rows": len(l1),
-                                     "index_postings": gi.n_postings, "tile_rows": p.tile_rows,
-                                     "parallelism": f"replicas x{world} (one run per GPU)"}),
-            "e2e": {"value": round(e2e, 1), "unit": "spectra/s", "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h)},
-            "gpu_launches": int(launches),
-            "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1),
-                         "peak": peak_gbs, "unit": "GB/s", "frac": round(achieved / peak_gbs, 4),
-                         "peak_source": peak_kind, "traffic": traffic, "algorithmic_bytes": algo,
-                         "mean_launch_ms": round(k_mean, 4)},
-            "kernels": kernels,
-            "cpu_baseline": cpu,
-            "clocks": clk,
-            "phase_ms": phase_ms,
-            "index_build_s": round(t_build, 1),
-            "per_step": {"hypotheses": int(dh["spec_off"][-1]), "k1_work_items": n_items,
-                         "k1_window_rows": int(win_off[-1]), "rescored": n_rescored},
-        }
-        print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    return kern, mlp
 
 
 def _traffic_from_profiles(kernel: str):
@@ -436,18 +560,24 @@ def run_profile(a):
     import torch
     from vulcan.gpu import engine as E
     dev = torch.device("cuda", 0)
-    w, l1, sp, _ = _workload_setup(a.workload, 0)
+    w, l1, _, sp, _ = _workload_setup(a.workload, 0)
     p = _params(w, a)
     gi = E.GpuIndex(l1, p, STATIC, VAR, device=dev)
     run = E.DeviceRun(sp, dev)
     st = E.Stats()
+    pr = None
+    if a.path == "pruned":   # kernel shapes only: a saved pruner, or an untrained one with a typical count floor
+        from vulcan.gpu import prune as PR
+        pr = PR.Pruner.load(a.pruner, dev) if a.pruner != "train" else PR.Pruner(dev, tau=0.0, min_count=2)
     for _ in range(2):
-        if p.search_method == "fused":
+        if pr is not None:
+            PR._pruned_device(run, gi, p, pr, 1, st)
+        elif p.search_method == "fused":
             E._search_fused_device(run, gi, p, 1, st)
         else:
             E._search_device(run, gi, p, 1, st)
     torch.cuda.synchronize()
-    print(json.dumps({"profile_passes": 2, "spectra": len(sp), "index_rows": len(l1)}), flush=True)
+    print(json.dumps({"profile_passes": 2, "path": a.path, "spectra": len(sp), "index_rows": len(l1)}), flush=True)
 
 
 def run_reference(a):
@@ -455,7 +585,7 @@ def run_reference(a):
     if rank != 0:
         return
     from oracle import oracle as O
-    w, l1, sp, _ = _workload_setup(a.workload, 0)
+    w, l1, _, sp, _ = _workload_setup(a.workload, 0)
     p = w.search_params()
     _ARR[id(l1)] = {k: np.ascontiguousarray(getattr(l1, k)) for k in ("seq_off", "length", "mask", "mass32",
                                                                          "residues")}
@@ -498,6 +628,15 @@ def main():
     ap.add_argument("--k1", choices=("merge", "per-peak"), default="per-peak", help="staged K1 search method")
     ap.add_argument("--warps", type=int, default=None, help="warps per fused-search CTA")
     ap.add_argument("--tile-rows", type=int, default=None, help="rows per fragment-index tile")
+    ap.add_argument("--path", choices=("pruned", "plain"), default="pruned",
+                    help="pruned: the learned-pruned search (headline; the plain path is timed beside it); plain: "
+                         "the exhaustive K1 -> top-k -> K2 path alone")
+    ap.add_argument("--pruner", default="train",
+                    help="'train': train the pruner on the GPU before timing (untimed); else a saved pruner (.npz)")
+    ap.add_argument("--save-pruner", default=None, help="save the trained pruner (.npz) here")
+    ap.add_argument("--train-spectra", type=int, default=200000, help="simulated training spectra")
+    ap.add_argument("--epochs", type=int, default=3, help="training epochs")
+    ap.add_argument("--target", type=float, default=0.9995, help="calibration target of top-1 recall")
     ap.add_argument("--mode", choices=("bench", "profile"), default="bench",
                     help="profile: set up the workload and run two device passes only (for an ncu capture of one "
                          "kernel launch of the second pass, e.g. -k regex:k1_tiles -s 1 -c 1)")
