@@ -69,9 +69,13 @@ def _workload_setup(name: str, rank: int):
 
 
 def _params(w, a):
-    kw = {"k1_merge": a.k1 == "merge", "search_method": a.method}
+    kw = {"search_method": a.method}
     if a.tile_rows:
         kw["tile_rows"] = a.tile_rows
+    elif a.method == "fused":
+        kw["tile_rows"] = 64         # the fused kernel stages one tile per warp
+    if a.k1_warps:
+        kw["k1_warps"] = a.k1_warps
     if a.warps:
         kw["fused_warps"] = a.warps
     return w.search_params(**kw)
@@ -85,7 +89,7 @@ def _config(w, p, extra=None):
            "method": ("fused persistent kernel (K1+top-k+K2+ranking per spectrum)" if p.search_method == "fused"
                       else "staged kernels"),
            "precursor_ppm": list(p.precursor_ppm), "fragment_tol": f"+-{p.fragment_ppm[1]} {p.fragment_unit}",
-           "topk": p.topk, "max_peaks": p.max_peaks, "k1": "merge join" if p.k1_merge else "per-peak search",
+           "topk": p.topk, "max_peaks": p.max_peaks, "k1": f"per-peak search, {p.k1_warps} warps per tile CTA",
            "l2": "flushed between steps (256 MiB write)"}
     if extra:
         cfg.update(extra)
@@ -481,7 +485,7 @@ def _kernel_table(a, p, gi, run, flush, pr, dev):
     isum = so.get("isum")
     kern = {}
     ms_k1 = timed(lambda: K.check(L.vk_k1_tiles(
-        C.byref(gi.tix), C.byref(gi.fp), float(p.fragment_ppm[0]), float(p.fragment_ppm[1]), E.k1_max_win(p),
+        C.byref(gi.tix), C.byref(gi.fp), float(p.fragment_ppm[0]), float(p.fragment_ppm[1]), p.k1_warps,
         K.ptr(item_off), K.ptr(item_hyp), K.ptr(dh["spec"]), K.ptr(dh["maxfz"]), K.ptr(dh["lo"]), K.ptr(dh["hi"]),
         K.ptr(win_off), K.ptr(peaks["off"]), K.ptr(peaks["mass"]), K.ptr(cnt), K.ptr(status),
         K.ptr(peaks["int"]) if pruned else None, K.ptr(peaks["tic"]) if pruned else None,
@@ -625,7 +629,7 @@ def main():
     ap.add_argument("--cpu-total", type=float, default=120.0, help="seconds of the reference arm in total")
     ap.add_argument("--method", choices=("staged", "fused"), default="staged",
                     help="staged: a kernel per stage; fused: one persistent kernel per run after K0 and hypotheses")
-    ap.add_argument("--k1", choices=("merge", "per-peak"), default="per-peak", help="staged K1 search method")
+    ap.add_argument("--k1-warps", type=int, default=None, help="warps per K1 CTA (one CTA per index tile)")
     ap.add_argument("--warps", type=int, default=None, help="warps per fused-search CTA")
     ap.add_argument("--tile-rows", type=int, default=None, help="rows per fragment-index tile")
     ap.add_argument("--path", choices=("pruned", "plain"), default="pruned",

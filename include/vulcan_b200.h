@@ -89,11 +89,14 @@ typedef struct {
 } vk_frag_params;
 
 /* Tiled fragment index.  Rows (mass-sorted peptidoforms) are cut into tiles of tile_rows = 2^tile_shift rows.
- * A posting is one u32: (f32bits(fragment) - f32bits(fmin)) << row_bits | (row - tile*tile_rows), where
- * row_bits = 32 - mass_bits and mass_bits = bit length of f32bits(fmax) - f32bits(fmin).  A tile's postings are
- * sorted ascending, i.e. by exact f32 fragment mass, then row.  The coarse m/z bin of a posting is its top
- * cbin_bits bits (an integer bin in f32-bit space); cbin_off[tile*(n_cbins+1) + b] (u16, relative to the tile's
- * first posting) is the CSR over those bins.  tile_off[n_tiles+1] (i64) locates each tile's postings. */
+ * A fragment's key is f32bits(fragment) - f32bits(fmin), mass_bits = bit length of f32bits(fmax) - f32bits(fmin)
+ * wide; a tile's fragments are sorted by (key, row), i.e. by exact f32 mass, then row.  The coarse m/z bin of a
+ * fragment is the top cbin_bits bits of its key (an integer bin in f32-bit space); cbin_off[tile*stride + b]
+ * (u16, relative to the tile's first posting; stride = 2^cbin_bits + 1 rounded up to 8) is the CSR over those
+ * bins.  The bin being implicit in the position, a posting is one u32 holding the rest of the key and the local
+ * row: (key mod 2^(mass_bits - cbin_bits)) << row_bits | (row - tile*tile_rows), row_bits = 32 - mass_bits +
+ * cbin_bits.  tile_off[n_tiles+1] (i64) locates each tile's postings (16-byte aligned, padding 0xffffffff after
+ * the last bin). */
 typedef struct {
   int64_t n_rows;
   int64_t n_tiles;
@@ -112,7 +115,8 @@ typedef struct {
 } vk_tindex;
 
 /* Layout of a tiled index for tile_rows/fmin/fmax: fills tile_shift, row_bits, mass_bits, cbin_bits, fmin_bits,
- * fmax_bits, n_tiles (host struct).  VK_E_ARG if tile_rows is not a power of two or does not fit row_bits. */
+ * fmax_bits, n_tiles (host struct).  VK_E_ARG if tile_rows is not a power of two in [32, 1024] or does not fit
+ * row_bits, or cbin_bits is outside [1, min(12, mass_bits - 1)]. */
 int vk_tindex_layout(int64_t n_rows, int tile_rows, float fmin, float fmax, int min_ion_index, int cbin_bits,
                      vk_tindex* ix);
 /* Postings per tile: tile_count[n_tiles] (i64) from the peptidoform table. */
@@ -120,7 +124,7 @@ int vk_tindex_count(const vk_tindex* ix, const vk_frag_params* fp, const int64_t
                     const uint64_t* mask, const float* mass32, const uint8_t* res, int64_t* tile_count,
                     void* stream);
 /* Fill postings and cbin_off of a tiled index whose tile_off (exclusive scan of tile_count) is in place.
- * max_tile_postings (host, from tile_count) sizes the per-tile sort; it must be <= 16384. */
+ * max_tile_postings (host, from tile_count) sizes the per-tile sort; VK_E_TOO_LARGE above 16384. */
 int vk_tindex_emit(const vk_tindex* ix, const vk_frag_params* fp, const int64_t* seq_off, const uint8_t* len,
                    const uint64_t* mask, const float* mass32, const uint8_t* res, uint32_t* postings,
                    uint16_t* cbin_off, void* stream);
@@ -177,16 +181,15 @@ int vk_hyp_fill(int n_spec, const uint8_t* valid, const double* precursor_mz, co
  *   vk_k1_tiles:      dense counts cnt[win_off[h] + row - lo[h]] (i32) for every window row of every hypothesis.
  * Counts equal the reference's brute force (kernels.cu:195-232): #(peak p, fragment charge z < maxfz, index
  * fragment f) with tol_bound(p*z, tol_lo) <= f <= tol_bound(p*z, tol_hi) in f32.  `status` (device i32, zeroed by
- * the caller) gets VK_STATUS_WAIT_TIMEOUT if a tile copy did not complete within the bounded wait.  max_win
- * (<= 4096) sizes the per-warp window buffer of the merge join: spectra with more peaks use the per-peak search;
- * 0 selects the per-peak search for every item.  isum (may be NULL; then pk_int and tic may be NULL too): per
- * window row the summed intensity of its matches, u32 fixed point = sum of round(intensity * 2^24 / tic[s]), for
- * the candidate pruner's features (the per-peak search is used when isum is given). */
+ * the caller) gets VK_STATUS_WAIT_TIMEOUT if a tile copy did not complete within the bounded wait.  `warps`
+ * (1..16) per CTA, one CTA per tile.  isum (may be NULL; then pk_int and tic may be NULL too): per window row the
+ * summed intensity of its matches, u32 fixed point = sum of round(intensity * 2^24 / tic[s]), for the candidate
+ * pruner's features.  VK_E_TOO_LARGE if a tile and the histograms do not fit one CTA's shared memory. */
 int vk_k1_plan_count(const vk_tindex* ix, int64_t n_hyp, const int64_t* h_lo, const int64_t* h_hi,
                      int64_t* tile_items, int64_t* win_len, void* stream);
 int vk_k1_plan_fill(const vk_tindex* ix, int64_t n_hyp, const int64_t* h_lo, const int64_t* h_hi,
                     const int64_t* tile_item_off, int64_t* cursor, int32_t* item_hyp, void* stream);
-int vk_k1_tiles(const vk_tindex* ix, const vk_frag_params* fp, float tol_lo, float tol_hi, int max_win,
+int vk_k1_tiles(const vk_tindex* ix, const vk_frag_params* fp, float tol_lo, float tol_hi, int warps,
                 const int64_t* tile_item_off, const int32_t* item_hyp, const int32_t* h_spec,
                 const int8_t* h_maxfz, const int64_t* h_lo, const int64_t* h_hi, const int64_t* win_off,
                 const int64_t* pk_off, const float* pk_mass, int32_t* cnt, int32_t* status, const float* pk_int,

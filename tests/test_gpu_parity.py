@@ -229,19 +229,41 @@ def test_search_is_deterministic(mini, param_sets, indexes):
     assert a.equals(b)
 
 
-def test_k1_per_peak_path_equals_merge_join(mini, param_sets, torch_cuda):
-    """The per-peak K1 search (used when windows are not monotone or a spectrum has more peaks than the window
-    buffer) gives the same dense counts as the merge join, for every parameter set."""
+@pytest.mark.parametrize("layout", [(32, 12, 1), (64, 8, 4), (128, 2, 3), (256, 0, 8), (128, 1, 2),
+                                    (512, 11, 16)])
+def test_k1_counts_for_every_tile_layout(mini, param_sets, torch_cuda, layout):
+    """Dense K1 counts and intensity sums do not depend on the tile size, the coarse bins per tile or the warps
+    per CTA: the oracle's for every parameter set.  Many fine bins make tolerance windows straddle bin edges; a
+    single bin per half of the key range makes the binary searches long."""
+    import dataclasses
+    from oracle import oracle as O
+    from vulcan.gpu import engine as E
+    from vulcan.gpu import prune as PR
+    l1, sp, _ = mini
+    tile_rows, cbin, warps = layout
+    for name, p in param_sets.items():
+        q = dataclasses.replace(p, tile_rows=tile_rows, cbin_bits=cbin, k1_warps=warps, search_method="staged")
+        gi = E.GpuIndex(l1, q, STATIC, VAR)
+        st = E.Stats()
+        f = PR._front(E.DeviceRun(sp, gi.dev, st), gi, q, st, False)
+        hyp = {k: f["dh"][k].cpu().numpy() for k in ("spec", "maxfz", "lo", "hi")}
+        pk = {k: f["peaks"][k].cpu().numpy() for k in ("off", "mass", "int")}
+        P = O.make_params(STATIC, VAR, q.fragment_unit)
+        win_off, cnt, _, _, isum = O.k1_windows(l1, hyp, pk, q, P, tic=f["peaks"]["tic"].cpu().numpy())
+        assert np.array_equal(f["cnt"].cpu().numpy(), cnt), name
+        assert np.array_equal(f["isum"].cpu().numpy().view(np.uint32), isum), name
+        # the plain search's counts (no intensity sums) are the same
+        assert np.array_equal(E.search(sp, gi, l1, q)[2]["cnt"].cpu().numpy(), cnt), name
+
+
+def test_tiles_too_large_for_shared_memory_are_refused(mini, param_sets, torch_cuda):
+    """1024-row tiles of the mini index hold more postings than the build sorts in shared memory: refused."""
     import dataclasses
     from vulcan.gpu import engine as E
-    l1, sp, _ = mini
-    for name, p in param_sets.items():
-        outs = []
-        for merge in (True, False):
-            q = dataclasses.replace(p, k1_merge=merge, search_method="staged")
-            gi = E.GpuIndex(l1, q, STATIC, VAR)
-            outs.append(E.search(sp, gi, l1, q)[2]["cnt"].cpu().numpy())
-        assert np.array_equal(outs[0], outs[1]), name
+    l1, _, _ = mini
+    q = dataclasses.replace(param_sets["da"], tile_rows=1024)
+    with pytest.raises(RuntimeError, match="tindex_emit"):
+        E.GpuIndex(l1, q, STATIC, VAR)
 
 
 def test_k0_cta_path_for_large_spectra(mini, param_sets, torch_cuda):
@@ -277,8 +299,11 @@ def test_fused_search_equals_staged_and_reference(mini, golden_py, param_sets, i
     import dataclasses
     from vulcan.gpu import engine as E
     l1, sp, _ = mini
-    p = param_sets[name] if topk is None else dataclasses.replace(param_sets[name], topk=topk)
-    gi = indexes[name] if topk is None else E.GpuIndex(l1, p, STATIC, VAR)
+    # the fused kernel stages one index tile per warp: 64-row tiles
+    p = dataclasses.replace(param_sets[name], tile_rows=64)
+    if topk is not None:
+        p = dataclasses.replace(p, topk=topk)
+    gi = E.GpuIndex(l1, p, STATIC, VAR)
     staged = dataclasses.replace(p, search_method="staged")
     t_s, _, o_s = E.search(sp, gi, l1, staged, report=3)
     t_f, _, o_f = E.search(sp, gi, l1, p, report=3)

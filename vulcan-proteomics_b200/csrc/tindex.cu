@@ -1,11 +1,14 @@
 // Tiled fragment index build and the device exclusive scan.
 //
 // Layout (vk_tindex in vulcan_b200.h): rows (mass-sorted peptidoforms) are cut into tiles of 2^tile_shift rows.
-// A posting is the u32 (f32bits(f) - f32bits(fmin)) << row_bits | local_row.  For positive floats the bit pattern
-// is monotone in the value, so sorting postings sorts fragments by their exact f32 mass, and a tolerance window
-// [a, bd] is exactly the key range [bits(a) - base, bits(bd) - base] (shifted): no quantisation, no edge loss.
-// Each tile's postings start at a multiple of 4 entries (16 bytes) so the search can stage a tile with one bulk
-// copy; the padding entries are 0xffffffff and are never inside a key range (see vk_tindex_layout).
+// A fragment's key is f32bits(f) - f32bits(fmin) (mass_bits wide).  For positive floats the bit pattern is monotone
+// in the value, so sorting by key sorts fragments by their exact f32 mass, and a tolerance window [a, bd] is
+// exactly the key range [bits(a) - base, bits(bd) - base]: no quantisation, no edge loss.  A tile's fragments are
+// sorted by (key, row) and split into 2^cbin_bits coarse bins by the key's top cbin_bits bits (CSR cbin_off); the
+// bin is implicit in a posting's position, so the u32 posting keeps only the low mass_bits - cbin_bits key bits
+// and the local row: (key mod 2^(mass_bits - cbin_bits)) << row_bits | row.  Each tile's postings start at a
+// multiple of 4 entries (16 bytes) so the search can stage a tile with one bulk copy; the padding entries are
+// 0xffffffff, after the last bin.
 #include <mutex>
 
 #include "common.cuh"
@@ -48,13 +51,14 @@ tindex_count_k(vk_tindex ix, vk_frag_params fpv, const int64_t* seq_off, const u
   if (lane == 0) tile_count[t] = (c + 3) & ~3ll;
 }
 
-__device__ __forceinline__ void bitonic_sort_u32(uint32_t* v, int n_pow2) {
+
+__device__ __forceinline__ void bitonic_sort_u64(uint64_t* v, int n_pow2) {
   for (int k = 2; k <= n_pow2; k <<= 1) {
     for (int j = k >> 1; j > 0; j >>= 1) {
       for (int i = threadIdx.x; i < n_pow2; i += blockDim.x) {
         int p = i ^ j;
         if (p > i) {
-          uint32_t a = v[i], b = v[p];
+          uint64_t a = v[i], b = v[p];
           bool up = (i & k) == 0;
           if ((a > b) == up) { v[i] = b; v[p] = a; }
         }
@@ -64,11 +68,12 @@ __device__ __forceinline__ void bitonic_sort_u32(uint32_t* v, int n_pow2) {
   }
 }
 
-// One CTA per tile: generate the tile's postings in shared memory, sort them, write postings and coarse-bin CSR.
+// One CTA per tile: generate the tile's (key << 16 | row) entries in shared memory, sort them, write the postings
+// (low key bits and row) and the coarse-bin CSR.
 __global__ void __launch_bounds__(512)
 tindex_emit_k(vk_tindex ix, vk_frag_params fpv, const int64_t* seq_off, const uint8_t* len, const uint64_t* mask,
               const float* mass32, const uint8_t* res, uint32_t* postings, uint16_t* cbin_off, int n_pow2) {
-  extern __shared__ uint32_t ti_smem[];
+  extern __shared__ uint64_t ti_smem[];
   __shared__ vk::SmemFrag fp;
   __shared__ int row_off[1025];
   __shared__ long long warp_tot[16];
@@ -109,37 +114,45 @@ tindex_emit_k(vk_tindex ix, vk_frag_params fpv, const int64_t* seq_off, const ui
     int L = len[g];
     uint64_t mk = mask[g];
     float b = vk::nterm_of(fp, mk), y = __fsub_rn(mass32[g], vk::nterm_of(fp, mk));
-    uint32_t* o = ti_smem + row_off[r];
+    uint64_t* o = ti_smem + row_off[r];
     for (int k = 0; k + 1 < L; ++k) {
       float rm = vk::resmass(fp, s[k], k, mk);
       b = __fadd_rn(b, rm);
       y = __fsub_rn(y, rm);
       if (k + 1 > ix.min_ion_index && b >= fmin && b <= fmax)
-        *o++ = ((__float_as_uint(b) - ix.fmin_bits) << ix.row_bits) | (uint32_t)r;
+        *o++ = ((uint64_t)(__float_as_uint(b) - ix.fmin_bits) << 16) | (uint64_t)r;
       if (L - 1 - k > ix.min_ion_index && y >= fmin && y <= fmax)
-        *o++ = ((__float_as_uint(y) - ix.fmin_bits) << ix.row_bits) | (uint32_t)r;
+        *o++ = ((uint64_t)(__float_as_uint(y) - ix.fmin_bits) << 16) | (uint64_t)r;
     }
   }
-  for (int i = n_post + threadIdx.x; i < n_pow2; i += blockDim.x) ti_smem[i] = 0xffffffffu;
+  for (int i = n_post + threadIdx.x; i < n_pow2; i += blockDim.x) ti_smem[i] = ~0ull;
   __syncthreads();
-  bitonic_sort_u32(ti_smem, n_pow2);
+  bitonic_sort_u64(ti_smem, n_pow2);
+  const int low_bits = ix.mass_bits - ix.cbin_bits;
+  const uint64_t lowmask = (1ull << low_bits) - 1ull;
   const int64_t o0 = ix.tile_off[t];
   const int64_t o1 = ix.tile_off[t + 1];
-  for (int64_t i = threadIdx.x; i < o1 - o0; i += blockDim.x) postings[o0 + i] = ti_smem[i];
-  // coarse bins: CSR over the top cbin_bits bits, offsets relative to the tile start
+  for (int64_t i = threadIdx.x; i < o1 - o0; i += blockDim.x) {
+    uint32_t v = 0xffffffffu;
+    if (i < n_post) {
+      const uint64_t e = ti_smem[i];
+      v = (uint32_t)(((e >> 16) & lowmask) << ix.row_bits) | (uint32_t)(e & 0xffffull);
+    }
+    postings[o0 + i] = v;
+  }
+  // coarse bins: CSR over the top cbin_bits key bits, offsets relative to the tile start
   const int nb = 1 << ix.cbin_bits;
   const int stride = (nb + 1 + 7) & ~7;
-  const int sh = 32 - ix.cbin_bits;
   for (int b = threadIdx.x; b <= nb; b += blockDim.x) {
     int pos;
     if (b == nb) {
       pos = n_post;
     } else {
-      uint64_t key = (uint64_t)b << sh;
+      const uint64_t key = (uint64_t)b << low_bits;
       int lo = 0, hi = n_post;
       while (lo < hi) {
         int m = (lo + hi) >> 1;
-        if ((uint64_t)ti_smem[m] < key) lo = m + 1; else hi = m;
+        if ((ti_smem[m] >> 16) < key) lo = m + 1; else hi = m;
       }
       pos = lo;
     }
@@ -259,12 +272,13 @@ int vk_tindex_layout(int64_t n_rows, int tile_rows, float fmin, float fmax, int 
   uint32_t range = hi - lo;
   int mass_bits = 0;
   while (mass_bits < 32 && (range >> mass_bits) != 0) ++mass_bits;
-  int row_bits = 32 - mass_bits;
+  if (cbin_bits < 1 || cbin_bits >= mass_bits || cbin_bits > 12) return VK_E_ARG;
+  // a posting keeps the low mass_bits - cbin_bits key bits; the row gets the rest
+  int row_bits = 32 - (mass_bits - cbin_bits);
   int shift = 0;
   while ((1 << shift) < tile_rows) ++shift;
-  // local rows must leave the all-ones key (padding) unused: tile_rows < 2^row_bits
-  if (row_bits < 1 || shift >= row_bits) return VK_E_ARG;
-  if (cbin_bits < 1 || cbin_bits > mass_bits || cbin_bits > 12) return VK_E_ARG;
+  // local rows must leave the all-ones posting (padding) unused, and fit the emit's 16-bit row field
+  if (row_bits > 31 || shift >= row_bits || tile_rows > 1024) return VK_E_ARG;
   ix->n_rows = n_rows;
   ix->tile_shift = shift;
   ix->row_bits = row_bits;
@@ -293,10 +307,11 @@ int vk_tindex_emit(const vk_tindex* ix, const vk_frag_params* fp, const int64_t*
                    uint16_t* cbin_off, void* stream) {
   if (!ix || !fp || !ix->tile_off) return VK_E_ARG;
   if (ix->n_tiles == 0) return 0;
-  if (ix->max_tile_postings > 16384 || (1 << ix->tile_shift) > 1024) return VK_E_ARG;
+  if ((1 << ix->tile_shift) > 1024) return VK_E_ARG;
+  if (ix->max_tile_postings > 16384) return VK_E_TOO_LARGE;   // the sort of a tile in shared memory
   int n_pow2 = 16;
   while (n_pow2 < ix->max_tile_postings) n_pow2 <<= 1;
-  size_t sh = (size_t)n_pow2 * sizeof(uint32_t);
+  size_t sh = (size_t)n_pow2 * sizeof(uint64_t);
   cudaError_t e = cudaFuncSetAttribute(tindex_emit_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
   if (e != cudaSuccess) return vk_err(e);
   tindex_emit_k<<<(unsigned)ix->n_tiles, 512, sh, (cudaStream_t)stream>>>(*ix, *fp, seq_off, len, mask, mass32, res,

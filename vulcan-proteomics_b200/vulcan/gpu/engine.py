@@ -28,7 +28,13 @@ SAGE_MONO = np.array([71.03711, 0.0, 103.00919, 115.02694, 129.04259, 147.0684, 
                       87.03203, 101.04768, 150.95363, 99.06841, 186.07932, 0.0, 163.06332, 0.0], np.float32)
 
 ROW_BITS = 28   # candidate rows < 2^28 (top-K key packing of the reference, engine.py:35)
-CBIN_BITS = 8   # coarse m/z bins per index tile
+
+
+def cbin_bits(p: SearchParams) -> int:
+    """Coarse m/z bins per index tile (log2): p.cbin_bits, or 2^8 per 64 rows (~6 postings per bin)."""
+    if p.cbin_bits:
+        return int(p.cbin_bits)
+    return int(min(12, 8 + max(0, int(math.log2(p.tile_rows)) - 6)))
 
 
 @dataclass
@@ -85,8 +91,8 @@ def _scan(x: torch.Tensor) -> torch.Tensor:
 class GpuIndex:
     """Device-resident peptidoform table + tiled fragment index.
 
-    Tiles of ``params.tile_rows`` mass-sorted rows; postings are u32 (f32 fragment bits - f32 bits of fmin) <<
-    row_bits | local row, sorted per tile, with a coarse-bin CSR per tile (``include/vulcan_b200.h``).  The
+    Tiles of ``params.tile_rows`` mass-sorted rows; per tile the fragments sorted by exact f32 mass in coarse m/z
+    bins (CSR), each posting the low key bits and the local row (``include/vulcan_b200.h``).  The
     reference-layout CSR slices (``slices``) used by the reference-compatible ``vk_k1`` are built on first use.
     """
 
@@ -143,7 +149,7 @@ class GpuIndex:
         p = self.p
         ix = K.TIndex()
         K.check(L.vk_tindex_layout(self.n, p.tile_rows, p.fragment_min_mz, p.fragment_max_mz, p.min_ion_index,
-                                   CBIN_BITS, C.byref(ix)), "tindex_layout")
+                                   cbin_bits(p), C.byref(ix)), "tindex_layout")
         d = self.dev
         nt = ix.n_tiles
         tile_count = torch.empty(max(nt, 1), dtype=torch.int64, device=d)
@@ -154,7 +160,7 @@ class GpuIndex:
                              self.tile_off[-1]]).cpu().tolist()
         ix.max_tile_postings = int(stats[0])
         ix.n_postings = int(stats[1])
-        stride = ((1 << CBIN_BITS) + 1 + 7) & ~7
+        stride = ((1 << ix.cbin_bits) + 1 + 7) & ~7
         self.postings = torch.empty(max(ix.n_postings, 4), dtype=torch.int32, device=d)
         self.cbin_off = torch.empty(max(nt * stride, 8), dtype=torch.int16, device=d)
         ix.tile_off = K.ptr(self.tile_off)
@@ -350,11 +356,6 @@ def _as_dev(hyp, dev):
     return out
 
 
-def k1_max_win(p: SearchParams) -> int:
-    """Window buffer of the K1 merge join: K0 keeps at most max_peaks peaks per spectrum (0 = per-peak search)."""
-    return int(min(4096, max(0, p.max_peaks))) if p.k1_merge else 0
-
-
 def _k1_dense(gi: GpuIndex, dh, peaks, p: SearchParams, n_hyp: int, stats: Stats | None = None,
               isum: bool = False):
     """Tiled K1: dense counts of every window row.  Returns (win_off, cnt, status), plus the summed matched
@@ -378,7 +379,7 @@ def _k1_dense(gi: GpuIndex, dh, peaks, p: SearchParams, n_hyp: int, stats: Stats
     status = torch.zeros(1, dtype=torch.int32, device=dev)
     isw = torch.empty(max(n_win, 1), dtype=torch.int32, device=dev) if isum else None
     K.check(L.vk_k1_tiles(C.byref(ix), C.byref(gi.fp), float(p.fragment_ppm[0]), float(p.fragment_ppm[1]),
-                          k1_max_win(p), K.ptr(item_off), K.ptr(item_hyp), K.ptr(dh["spec"]), K.ptr(dh["maxfz"]), K.ptr(dh["lo"]),
+                          p.k1_warps, K.ptr(item_off), K.ptr(item_hyp), K.ptr(dh["spec"]), K.ptr(dh["maxfz"]), K.ptr(dh["lo"]),
                           K.ptr(dh["hi"]), K.ptr(win_off), K.ptr(peaks["off"]), K.ptr(peaks["mass"]), K.ptr(cnt),
                           K.ptr(status), K.ptr(peaks["int"]) if isum else None, K.ptr(peaks["tic"]) if isum else None,
                           K.ptr(isw) if isum else None, K.stream()), "k1_tiles")

@@ -43,9 +43,11 @@ class SearchParams:
     tile: int = 1024
     k2_threads: int = 128
     max_slice_entries: int = 2 ** 31 - 1
-    # B200 layout knobs: rows per fragment-index tile (power of two, 32 <= tile_rows < 2^row_bits) and K1 method
-    tile_rows: int = 64
-    k1_merge: bool = False                  # staged K1: merge join instead of the per-peak search
+    # B200 layout knobs: rows per fragment-index tile (power of two, 32..1024; the tile's postings must fit one
+    # CTA's shared memory), coarse m/z bins per tile (0 = 2^8 per 64 rows), warps per K1 CTA
+    tile_rows: int = 128
+    cbin_bits: int = 0
+    k1_warps: int = 8
     search_method: str = "staged"           # "staged" (a kernel per stage) or "fused" (one persistent kernel)
     fused_warps: int = 4                    # warps of a fused-search CTA (one spectrum at a time)
     fused_cnt_cap: int = 4096               # window rows a spectrum may span in the fused search
