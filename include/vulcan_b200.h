@@ -151,15 +151,20 @@ int64_t vk_scan_noalloc_max_n(void);
 int vk_scan_i64_noalloc(const int64_t* in, int64_t n, int64_t* out, void* stream);
 
 /* K0 peak view (reference vulcan/gpu/engine.py:171-210), two calls: vk_k0_count writes kept[n_spec] (i64) =
- * min(#peaks with fmin <= mz <= fmax and not NaN, max_peaks); after the caller's scan into pk_off[n_spec+1],
- * vk_k0_fill writes mass-sorted peaks (mass = mz - PROTON) of the top max_peaks by (intensity desc, mass desc),
- * tic[n_spec] (f32 of the f64 sum) and valid[n_spec] (u8, kept >= min_peaks).  max_raw (host) = the largest raw
- * peak count of a spectrum, at most 16384 (one CTA sorts a spectrum in shared memory). */
-int vk_k0_count(int n_spec, const int64_t* raw_off, const float* raw_mz, float fmin, float fmax, int max_peaks,
-                int64_t* kept, void* stream);
+ * min(#peaks with fmin <= mz <= fmax and not NaN, max_peaks), easy[n_spec] (u8: the raw peaks are already in
+ * (mass asc, intensity desc) order, no NaN, at most max_peaks in range) and the other spectra's indices into
+ * hard_list[n_spec] (i32, any order) with their number in *n_hard (device i32, zeroed by the call); after the
+ * caller's scan of kept into pk_off[n_spec+1], vk_k0_fill writes mass-sorted peaks (mass = mz - PROTON) of the top
+ * max_peaks by (intensity desc, mass desc), tic[n_spec] (f32 of the f64 sum) and valid[n_spec] (u8, kept >=
+ * min_peaks): easy spectra by a stream copy, the hard list by shared-memory sorts.  max_raw (host) = the largest
+ * raw peak count of a spectrum, at most 16384 (one CTA sorts a spectrum in shared memory). */
+int vk_k0_count(int n_spec, const int64_t* raw_off, const float* raw_mz, const float* raw_int, float fmin,
+                float fmax, int max_peaks, int64_t* kept, uint8_t* easy, int32_t* hard_list, int32_t* n_hard,
+                void* stream);
 int vk_k0_fill(int n_spec, const int64_t* raw_off, const float* raw_mz, const float* raw_int, float fmin,
                float fmax, int max_peaks, int min_peaks, const int64_t* pk_off, float* pk_mass, float* pk_int,
-               float* tic, uint8_t* valid, int max_raw, void* stream);
+               float* tic, uint8_t* valid, int max_raw, const uint8_t* easy, const int32_t* hard_list,
+               const int32_t* n_hard, void* stream);
 
 /* Hypotheses (reference vulcan/gpu/host.py:64-91), two calls like K0: vk_hyp_count writes n_hyp[n_spec] (i64);
  * vk_hyp_fill writes, at hyp_off[s], the spectrum's hypotheses in (charge, isotope) order with f32 Sage
@@ -324,6 +329,15 @@ int vk_cand_features(int64_t n, const int64_t* n_dev, const int64_t* c_hyp, cons
 int64_t vk_mlp_infer_smem(void);
 int vk_mlp_infer(int64_t n, const int64_t* n_dev, const void* feat_bf16, const void* W1_bf16, const float* b1, const void* W2_bf16,
                  const float* b2, const float* w3, float b3, float* logit, int grid, void* stream);
+/* The same logits on the 5th-generation tensor cores (tcgen05.mma, TMEM accumulators): tiles of 128 hits, layer 1
+ * (K 16) and layer 2 (K 256) as UMMA from shared memory, bias / ReLU / BF16 rounding and the layer-3 dot in the
+ * TMEM epilogues.  `grid` persistent CTAs of 512 threads (at most one per SM: vk_mlp_infer_tc_smem() bytes of
+ * shared memory each).  `status` (device i32, zeroed by the caller) gets VK_STATUS_WAIT_TIMEOUT if an MMA did not
+ * complete within the bounded wait. */
+int64_t vk_mlp_infer_tc_smem(void);
+int vk_mlp_infer_tc(int64_t n, const int64_t* n_dev, const void* feat_bf16, const void* W1_bf16, const float* b1,
+                    const void* W2_bf16, const float* b2, const float* w3, float b3, float* logit, int grid,
+                    int32_t* status, void* stream);
 /* Pruned candidate selection per spectrum: hits with logit >= tau plus the min_keep best by (logit, count, hit
  * order) descending, at most max_keep (a power of two >= 16); pair closure; candidates sorted by row with duplicate
  * rows merged (lowest hypothesis, highest count) into slots s*cap (cap >= (pair_closure ? 2 : 1) * max_keep), the

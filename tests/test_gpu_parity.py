@@ -266,6 +266,42 @@ def test_tiles_too_large_for_shared_memory_are_refused(mini, param_sets, torch_c
         E.GpuIndex(l1, q, STATIC, VAR)
 
 
+@pytest.mark.parametrize("name", ("da", "ppm"))
+def test_k0_easy_and_hard_spectra(mini, param_sets, name, torch_cuda):
+    """Sorted spectra take the stream-copy path; shuffled ones, ones with a NaN m/z and ones with more in-range
+    peaks than max_peaks take the sorting path: every spectrum equals the oracle's peak view."""
+    from oracle import oracle as O
+    from vulcan.gpu import engine as E
+    from vulcan.gpu.host import Spectra
+    _, sp, _ = mini
+    p = param_sets[name]
+    rng = np.random.default_rng(21)
+    mz, it, off = [], [], [0]
+    for s in range(len(sp)):
+        a, b = sp.offsets[s], sp.offsets[s + 1]
+        m, i = sp.mz[a:b].copy(), sp.intensity[a:b].copy()
+        kind = s % 4
+        if kind == 1 and len(m):          # shuffled
+            o = rng.permutation(len(m))
+            m, i = m[o], i[o]
+        elif kind == 2 and len(m):        # a NaN m/z in place
+            m[len(m) // 2] = np.nan
+        elif kind == 3 and len(m) > 2:    # every peak twice (ties in mass and intensity), still sorted
+            m, i = np.repeat(m, 2), np.repeat(i, 2)
+        mz.append(m)
+        it.append(i)
+        off.append(off[-1] + len(m))
+    sp2 = Spectra("mixed", sp.scan, sp.index, sp.rt, sp.precursor_mz, sp.charge, np.concatenate(mz).astype(np.float32),
+                  np.concatenate(it).astype(np.float32), np.array(off, np.int64))
+    pk = E.k0_preprocess(sp2, p, torch_cuda.device("cuda"), E.Stats())
+    ref = O.k0_view(sp2, p)
+    assert np.array_equal(pk["off"].cpu().numpy(), ref["off"])
+    assert np.array_equal(pk["mass"].cpu().numpy(), ref["mass"])
+    assert np.array_equal(pk["int"].cpu().numpy(), ref["int"])
+    assert np.array_equal(pk["valid"], ref["valid"])
+    np.testing.assert_allclose(pk["tic"].cpu().numpy(), ref["tic"], rtol=1e-7)
+
+
 def test_k0_cta_path_for_large_spectra(mini, param_sets, torch_cuda):
     """Runs with a spectrum of more than 2048 raw peaks use the CTA sort kernel; it equals the oracle too."""
     from oracle import oracle as O

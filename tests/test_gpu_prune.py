@@ -106,11 +106,13 @@ def _weights_np(pr, torch):
     return W1b, _np(pr.w["b1"]), W2b, _np(pr.w["b2"]), _np(pr.w["w3"]), _np(pr.w["b3"])
 
 
+@pytest.mark.parametrize("kernel", ["tcgen05", "mma.sync"])
 @pytest.mark.parametrize("n", [1, 16, 1037, 40000])
-def test_mlp_inference_matches_oracle(torch_cuda, n):
+def test_mlp_inference_matches_oracle(torch_cuda, n, kernel):
     torch = torch_cuda
     dev = torch.device("cuda")
     pr = _random_pruner(torch, dev, 7)
+    pr.tensor_cores = kernel
     g = torch.Generator(device="cpu").manual_seed(n)
     X = torch.zeros(n, 16)
     X[:, :6] = torch.randn(n, 6, generator=g) * 1.5
@@ -128,9 +130,14 @@ def test_mlp_inference_matches_oracle(torch_cuda, n):
         out = torch.full((n,), 123.0, device=dev)
         cnt = torch.tensor([n - 9], dtype=torch.int64, device=dev)
         from vulcan.gpu import _lib as K
-        K.check(K.lib().vk_mlp_infer(n, K.ptr(cnt), K.ptr(Xb), K.ptr(pr.bf["W1"]), K.ptr(pr.w["b1"]),
-                                     K.ptr(pr.bf["W2"]), K.ptr(pr.w["b2"]), K.ptr(pr.w["w3"]), pr._b3, K.ptr(out),
-                                     3, K.stream()), "mlp_infer")
+        args = (K.ptr(Xb), K.ptr(pr.bf["W1"]), K.ptr(pr.w["b1"]), K.ptr(pr.bf["W2"]), K.ptr(pr.w["b2"]),
+                K.ptr(pr.w["w3"]), pr._b3, K.ptr(out), 3)
+        if kernel == "tcgen05":
+            st = torch.zeros(1, dtype=torch.int32, device=dev)
+            K.check(K.lib().vk_mlp_infer_tc(n, K.ptr(cnt), *args, K.ptr(st), K.stream()), "mlp_infer_tc")
+            assert int(st.item()) == 0
+        else:
+            K.check(K.lib().vk_mlp_infer(n, K.ptr(cnt), *args, K.stream()), "mlp_infer")
         o = _np(out)
         np.testing.assert_array_equal(o[:n - 9], z[:n - 9])
         assert np.all(o[n - 9:] == 123.0)

@@ -26,14 +26,83 @@ __device__ __forceinline__ bool in_range(float mz, float fmin, float fmax) {
   return mz >= fmin && mz <= fmax;   // false for NaN
 }
 
-__global__ void k0_count_k(int n_spec, const int64_t* raw_off, const float* raw_mz, float fmin, float fmax,
-                           int max_peaks, int64_t* kept) {
+// mass-order key of a peak: ascending = mass ascending, then intensity descending
+__device__ __forceinline__ uint64_t mass_key(float mz, float it) {
+  return ((uint64_t)ord_f32(__fsub_rn(mz, VK_PROTON)) << 32) | (uint64_t)(~ord_f32(it));
+}
+
+// Warp per spectrum: kept = min(#in-range peaks, max_peaks); easy = the raw peaks are already in mass-key order
+// (no NaN) and at most max_peaks are in range, so the peak view is the in-range subsequence as it is.  Spectra that
+// are not easy are appended to hard_list (in any order: each is processed on its own).
+__global__ void k0_count_k(int n_spec, const int64_t* raw_off, const float* raw_mz, const float* raw_int, float fmin,
+                           float fmax, int max_peaks, int64_t* kept, uint8_t* easy, int32_t* hard_list,
+                           int32_t* n_hard) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (warp >= n_spec) return;
+  const int64_t r0 = raw_off[warp], r1 = raw_off[warp + 1];
   long long c = 0;
-  for (int64_t i = raw_off[warp] + lane; i < raw_off[warp + 1]; i += 32) c += in_range(raw_mz[i], fmin, fmax);
+  bool sorted = true;
+  uint64_t carry = 0;   // key of the previous chunk's last peak
+  for (int64_t i0 = r0; i0 < r1; i0 += 32) {
+    const int64_t i = i0 + lane;
+    uint64_t k = 0;
+    if (i < r1) {
+      const float mz = raw_mz[i];
+      c += in_range(mz, fmin, fmax);
+      sorted &= !isnan(mz);
+      k = mass_key(mz, raw_int[i]);
+    }
+    uint64_t prev = __shfl_up_sync(VK_FULL, k, 1);
+    if (lane == 0) prev = carry;
+    if (i < r1 && i > r0) sorted &= prev <= k;
+    carry = __shfl_sync(VK_FULL, k, 31);
+  }
   c = vk::warp_sum(c);
-  if (lane == 0) kept[warp] = min(c, (long long)max_peaks);
+  sorted = __all_sync(VK_FULL, sorted);
+  if (lane == 0) {
+    kept[warp] = min(c, (long long)max_peaks);
+    const bool e = sorted && c <= max_peaks;
+    easy[warp] = e;
+    if (!e) hard_list[atomicAdd(n_hard, 1)] = warp;
+  }
+}
+
+// Easy spectra: the in-range peaks in input order (ballot compaction), TIC as the f64 sum of lane partials
+// (lane order, then a butterfly), the same order as the sorting kernels use for sorted input.
+__global__ void k0_easy_k(int n_spec, const int64_t* raw_off, const float* raw_mz, const float* raw_int, float fmin,
+                          float fmax, int min_peaks, const int64_t* pk_off, float* pk_mass, float* pk_int, float* tic,
+                          uint8_t* valid, const uint8_t* easy) {
+  const int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (s >= n_spec || !easy[s]) return;
+  const unsigned lt_mask = (1u << lane) - 1u;
+  const int64_t r0 = raw_off[s], r1 = raw_off[s + 1];
+  const int64_t o0 = pk_off[s];
+  double part = 0.0;
+  int w = 0;
+  for (int64_t i0 = r0; i0 < r1; i0 += 32) {
+    const int64_t i = i0 + lane;
+    float mz = 0.f, it = 0.f;
+    bool take = false;
+    if (i < r1) {
+      mz = raw_mz[i];
+      take = in_range(mz, fmin, fmax);
+      if (take) it = raw_int[i];
+    }
+    const unsigned m = __ballot_sync(VK_FULL, take);
+    if (take) {
+      const int pos = w + __popc(m & lt_mask);
+      pk_mass[o0 + pos] = __fsub_rn(mz, VK_PROTON);
+      pk_int[o0 + pos] = it;
+      part += (double)it;
+    }
+    w += __popc(m);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(VK_FULL, part, o);
+  if (lane == 0) {
+    tic[s] = (float)part;
+    valid[s] = (int)(pk_off[s + 1] - o0) >= min_peaks;
+  }
 }
 
 __device__ __forceinline__ void block_bitonic_u64(uint64_t* v, int n_pow2) {
@@ -54,12 +123,14 @@ __device__ __forceinline__ void block_bitonic_u64(uint64_t* v, int n_pow2) {
 constexpr int K0_THREADS = 256;
 
 __global__ void __launch_bounds__(K0_THREADS)
-k0_fill_k(int n_spec, const int64_t* raw_off, const float* raw_mz, const float* raw_int, float fmin, float fmax,
-          int max_peaks, int min_peaks, const int64_t* pk_off, float* pk_mass, float* pk_int, float* tic,
-          uint8_t* valid) {
+k0_fill_k(const int32_t* hard_list, const int32_t* n_hard, const int64_t* raw_off, const float* raw_mz,
+          const float* raw_int, float fmin, float fmax, int max_peaks, int min_peaks, const int64_t* pk_off,
+          float* pk_mass, float* pk_int, float* tic, uint8_t* valid) {
   extern __shared__ uint64_t k0_keys[];
   __shared__ double red[K0_THREADS / 32];
-  const int s = blockIdx.x;
+  const int n_work = *n_hard;
+  for (int j = blockIdx.x; j < n_work; j += gridDim.x) {
+  const int s = hard_list[j];
   const int64_t r0 = raw_off[s];
   const int n = (int)(raw_off[s + 1] - r0);
   int n_pow2 = 1;
@@ -113,6 +184,8 @@ k0_fill_k(int n_spec, const int64_t* raw_off, const float* raw_mz, const float* 
     tic[s] = (float)t;
     valid[s] = kept >= min_peaks;
   }
+  __syncthreads();
+  }
 }
 
 // Warp-per-spectrum K0 for spectra of at most key_cap raw peaks (key_cap a power of two <= 2048).
@@ -145,13 +218,14 @@ __device__ __forceinline__ uint64_t sel_of(uint64_t k2) {
 }
 
 __global__ void __launch_bounds__(K0W_WARPS * 32)
-k0_fill_warp_k(int n_spec, const int64_t* raw_off, const float* raw_mz, const float* raw_int, float fmin, float fmax,
-               int max_peaks, int min_peaks, const int64_t* pk_off, float* pk_mass, float* pk_int, float* tic,
-               uint8_t* valid, int key_cap) {
+k0_fill_warp_k(const int32_t* hard_list, const int32_t* n_hard, const int64_t* raw_off, const float* raw_mz,
+               const float* raw_int, float fmin, float fmax, int max_peaks, int min_peaks, const int64_t* pk_off,
+               float* pk_mass, float* pk_int, float* tic, uint8_t* valid, int key_cap) {
   extern __shared__ uint64_t k0w_smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int s = blockIdx.x * K0W_WARPS + warp;
-  if (s >= n_spec) return;
+  const int n_work = *n_hard;
+  for (int j = blockIdx.x * K0W_WARPS + warp; j < n_work; j += gridDim.x * K0W_WARPS) {
+  const int s = hard_list[j];
   uint64_t* keys = k0w_smem + (size_t)warp * 2 * key_cap;
   uint64_t* sel = keys + key_cap;
   const unsigned lt_mask = (1u << lane) - 1u;
@@ -165,7 +239,7 @@ k0_fill_warp_k(int n_spec, const int64_t* raw_off, const float* raw_mz, const fl
     if (i < n) {
       const float mz = raw_mz[r0 + i];
       keep = in_range(mz, fmin, fmax);
-      if (keep) k = ((uint64_t)ord_f32(__fsub_rn(mz, VK_PROTON)) << 32) | (uint64_t)(~ord_f32(raw_int[r0 + i]));
+      if (keep) k = mass_key(mz, raw_int[r0 + i]);
     }
     const unsigned m = __ballot_sync(VK_FULL, keep);
     if (keep) keys[n_in + __popc(m & lt_mask)] = k;
@@ -229,6 +303,8 @@ k0_fill_warp_k(int n_spec, const int64_t* raw_off, const float* raw_mz, const fl
   if (lane == 0) {
     tic[s] = (float)part;
     valid[s] = kept >= min_peaks;
+  }
+  __syncwarp();
   }
 }
 
@@ -295,39 +371,53 @@ __global__ void hyp_fill_k(int n_spec, const uint8_t* valid, const double* pmz, 
 
 extern "C" {
 
-int vk_k0_count(int n_spec, const int64_t* raw_off, const float* raw_mz, float fmin, float fmax, int max_peaks,
-                int64_t* kept, void* stream) {
+int vk_k0_count(int n_spec, const int64_t* raw_off, const float* raw_mz, const float* raw_int, float fmin,
+                float fmax, int max_peaks, int64_t* kept, uint8_t* easy, int32_t* hard_list, int32_t* n_hard,
+                void* stream) {
+  cudaError_t e = cudaMemsetAsync(n_hard, 0, sizeof(int32_t), (cudaStream_t)stream);
+  if (e != cudaSuccess) return vk_err(e);
   if (n_spec == 0) return 0;
   int64_t threads = (int64_t)n_spec * 32;
-  k0_count_k<<<(unsigned)((threads + 255) / 256), 256, 0, (cudaStream_t)stream>>>(n_spec, raw_off, raw_mz, fmin, fmax,
-                                                                                  max_peaks, kept);
+  k0_count_k<<<(unsigned)((threads + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
+      n_spec, raw_off, raw_mz, raw_int, fmin, fmax, max_peaks, kept, easy, hard_list, n_hard);
   return vk_launch_status();
 }
 
 int vk_k0_fill(int n_spec, const int64_t* raw_off, const float* raw_mz, const float* raw_int, float fmin,
                float fmax, int max_peaks, int min_peaks, const int64_t* pk_off, float* pk_mass, float* pk_int,
-               float* tic, uint8_t* valid, int max_raw, void* stream) {
+               float* tic, uint8_t* valid, int max_raw, const uint8_t* easy, const int32_t* hard_list,
+               const int32_t* n_hard, void* stream) {
   if (n_spec == 0) return 0;
   if (max_raw < 0 || max_raw > 16384) return VK_E_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  int64_t threads = (int64_t)n_spec * 32;
+  k0_easy_k<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(n_spec, raw_off, raw_mz, raw_int, fmin, fmax,
+                                                                min_peaks, pk_off, pk_mass, pk_int, tic, valid, easy);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return vk_err(e);
+  int dev = 0, n_sm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
   if (max_raw <= 2048) {
     int key_cap = 32;
     while (key_cap < max_raw) key_cap <<= 1;
     size_t shw = (size_t)K0W_WARPS * 2 * key_cap * sizeof(uint64_t);
-    cudaError_t e = cudaFuncSetAttribute(k0_fill_warp_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shw);
+    e = cudaFuncSetAttribute(k0_fill_warp_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shw);
     if (e != cudaSuccess) return vk_err(e);
-    k0_fill_warp_k<<<(unsigned)((n_spec + K0W_WARPS - 1) / K0W_WARPS), K0W_WARPS * 32, shw, (cudaStream_t)stream>>>(
-        n_spec, raw_off, raw_mz, raw_int, fmin, fmax, max_peaks, min_peaks, pk_off, pk_mass, pk_int, tic, valid,
-        key_cap);
+    const int grid = (int)min((int64_t)n_sm * 4, ((int64_t)n_spec + K0W_WARPS - 1) / K0W_WARPS);
+    k0_fill_warp_k<<<grid, K0W_WARPS * 32, shw, st>>>(hard_list, n_hard, raw_off, raw_mz, raw_int, fmin, fmax,
+                                                     max_peaks, min_peaks, pk_off, pk_mass, pk_int, tic, valid,
+                                                     key_cap);
     return vk_launch_status();
   }
   int n_pow2 = 1;
   while (n_pow2 < max_raw) n_pow2 <<= 1;
   size_t sh = (size_t)n_pow2 * sizeof(uint64_t);
-  cudaError_t e = cudaFuncSetAttribute(k0_fill_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  e = cudaFuncSetAttribute(k0_fill_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
   if (e != cudaSuccess) return vk_err(e);
-  k0_fill_k<<<n_spec, K0_THREADS, sh, (cudaStream_t)stream>>>(n_spec, raw_off, raw_mz, raw_int, fmin, fmax,
-                                                               max_peaks, min_peaks, pk_off, pk_mass, pk_int, tic,
-                                                               valid);
+  const int grid = (int)min((int64_t)n_sm * 2, (int64_t)n_spec);
+  k0_fill_k<<<grid, K0_THREADS, sh, st>>>(hard_list, n_hard, raw_off, raw_mz, raw_int, fmin, fmax, max_peaks,
+                                          min_peaks, pk_off, pk_mass, pk_int, tic, valid);
   return vk_launch_status();
 }
 

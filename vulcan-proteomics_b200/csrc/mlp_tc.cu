@@ -1,0 +1,267 @@
+// Candidate-pruner MLP inference on the 5th-generation tensor cores (tcgen05 / UMMA, TMEM accumulators).
+//
+// Network: logit = w3 . relu(W2 relu(W1 x + b1) + b2) + b3; x 16 BF16 features, W1 [256 x 16], W2 [256 x 256] BF16,
+// b1, b2, w3 FP32.  The layer-1 activations are rounded to BF16 (the layer-2 operand), everything else stays FP32.
+//
+// Persistent CTAs of 16 warps, one per SM (the weights fill most of the shared memory).  Warp w reads TMEM lanes
+// 32*(w%4).. (hit rows; a warp may only touch its lane quarter) and columns 64*(w/4).. .  Per tile of 128 hits:
+//   1. the 128 x 16 feature tile is copied into shared memory in the UMMA canonical K-major layout;
+//   2. one thread issues D = X W1^T (M 128, N 256, K 16) into 256 TMEM columns and commits to an mbarrier;
+//   3. epilogue 1: every warp reads its 32 rows x 64 columns with tcgen05.ld, adds b1, applies ReLU, rounds to
+//      BF16 and writes them into shared memory as the layer-2 A operand;
+//   4. one thread issues D = H1 W2^T (K 256: 16 UMMAs) into the same TMEM columns and commits;
+//   5. epilogue 2: ReLU(D + b2) . w3 over the warp's 64 columns, the four column quarters of a row summed in a
+//      fixed order through shared memory, + b3, written to `logit`.
+// Shared-memory operands use the no-swizzle canonical layout: 8-row x 16-byte core matrices (128 contiguous bytes),
+// the two 16-byte K chunks of one UMMA K-step 128 bytes apart (leading byte offset), 8-row groups a whole K-row of
+// core matrices apart (stride byte offset).  Every mbarrier wait is bounded: on a timeout the CTA records
+// VK_STATUS_WAIT_TIMEOUT, waits once more for its own MMAs, frees its TMEM and stops.
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+
+namespace {
+
+constexpr int TC_M = 128;          // hits per tile (UMMA M)
+constexpr int TC_IN = 16;          // features (UMMA K of layer 1)
+constexpr int TC_H = 256;          // hidden width (UMMA N; K of layer 2)
+constexpr int TC_THREADS = 512;
+constexpr int TC_COLS_PER_WARP = 64;
+constexpr uint32_t TC_TMEM_COLS = 256;
+constexpr uint32_t TC_WAIT = 1u << 24;
+
+// shared-memory map (bytes)
+constexpr int OFF_W2 = 0;                                  // 256 x 256 bf16, K-major canonical: 128 KB
+constexpr int OFF_W1 = OFF_W2 + TC_H * TC_H * 2;           // 256 x 16: 8 KB
+constexpr int OFF_X = OFF_W1 + TC_H * TC_IN * 2;           // 128 x 16: 4 KB
+constexpr int OFF_H = OFF_X + TC_M * TC_IN * 2;            // 128 x 256: 64 KB
+constexpr int OFF_B1 = OFF_H + TC_M * TC_H * 2;
+constexpr int OFF_B2 = OFF_B1 + TC_H * 4;
+constexpr int OFF_W3 = OFF_B2 + TC_H * 4;
+constexpr int OFF_PART = OFF_W3 + TC_H * 4;                // 4 column quarters x 128 rows of partial logits
+constexpr int TC_SMEM = OFF_PART + 4 * TC_M * 4;           // + 128 for alignment slack at launch
+
+// byte offset of element (row r, k) of a K-major canonical operand whose K extent is kext elements
+__device__ __forceinline__ uint32_t canon_off(int r, int k, int kext) {
+  return (uint32_t)((r >> 3) * (kext / 8) * 128 + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2);
+}
+
+// UMMA shared-memory descriptor, no swizzle, K-major: start, leading byte offset (between the K chunks of one
+// K-step), stride byte offset (between 8-row groups), descriptor version 1.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// instruction descriptor of kind::f16: BF16 A and B (K-major), FP32 D, M x N
+__host__ __device__ constexpr uint32_t instr_desc(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+      :
+      : "r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(acc)
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  uint32_t b = (uint32_t)__cvta_generic_to_shared(bar);
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(b) : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void async_proxy_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t* v) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+        "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+        "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+      : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+__device__ __forceinline__ uint32_t pack2(float lo, float hi) {
+  __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<uint32_t*>(&v);
+}
+
+__global__ void __launch_bounds__(TC_THREADS, 1)
+mlp_infer_tc_k(int64_t n, const int64_t* n_dev, const __nv_bfloat16* __restrict__ feat,
+               const __nv_bfloat16* __restrict__ W1, const float* __restrict__ b1,
+               const __nv_bfloat16* __restrict__ W2, const float* __restrict__ b2, const float* __restrict__ w3,
+               float b3, float* __restrict__ logit, int32_t* status) {
+  extern __shared__ uint8_t tc_raw[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tmem_slot;
+  __shared__ int abort_flag;
+  uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(tc_raw) + 127) & ~uintptr_t(127));
+  const int tid = threadIdx.x, warp = tid >> 5;
+  if (n_dev) n = min(n, *n_dev);
+  // weights into the canonical layouts (16-byte chunks), biases and w3
+  for (int c = tid; c < TC_H * TC_H / 8; c += TC_THREADS) {
+    const int r = c / (TC_H / 8), k = (c % (TC_H / 8)) * 8;
+    *reinterpret_cast<uint4*>(sm + OFF_W2 + canon_off(r, k, TC_H)) =
+        *reinterpret_cast<const uint4*>(W2 + (size_t)r * TC_H + k);
+  }
+  for (int c = tid; c < TC_H * TC_IN / 8; c += TC_THREADS) {
+    const int r = c / (TC_IN / 8), k = (c % (TC_IN / 8)) * 8;
+    *reinterpret_cast<uint4*>(sm + OFF_W1 + canon_off(r, k, TC_IN)) =
+        *reinterpret_cast<const uint4*>(W1 + (size_t)r * TC_IN + k);
+  }
+  float* sb1 = reinterpret_cast<float*>(sm + OFF_B1);
+  float* sb2 = reinterpret_cast<float*>(sm + OFF_B2);
+  float* sw3 = reinterpret_cast<float*>(sm + OFF_W3);
+  for (int i = tid; i < TC_H; i += TC_THREADS) {
+    sb1[i] = b1[i];
+    sb2[i] = b2[i];
+    sw3[i] = w3[i];
+  }
+  if (tid == 0) {
+    abort_flag = 0;
+    vk::mbar_init(&bar, 1);
+    vk::fence_mbar_init();
+  }
+  if (warp == 0) {
+    const uint32_t slot = (uint32_t)__cvta_generic_to_shared(&tmem_slot);
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot),
+                 "r"(TC_TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+  }
+  async_proxy_fence();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_slot;
+  const uint32_t s_base = (uint32_t)__cvta_generic_to_shared(sm);
+  const uint32_t id_l = instr_desc(TC_M, TC_H);
+  const uint64_t dW1 = smem_desc(s_base + OFF_W1, 128, (TC_IN / 8) * 128);
+  const uint64_t dX = smem_desc(s_base + OFF_X, 128, (TC_IN / 8) * 128);
+  const int rq = warp & 3, cq = warp >> 2;                 // lane (row) quarter, column quarter
+  const int my_row = rq * 32 + (threadIdx.x & 31);
+  const int col0 = cq * TC_COLS_PER_WARP;
+  const uint32_t lane_base = tmem + ((uint32_t)(rq * 32) << 16);
+  float* part = reinterpret_cast<float*>(sm + OFF_PART);
+  uint32_t phase = 0;
+  const int64_t n_tiles = (n + TC_M - 1) / TC_M;
+  for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+    // 1. feature tile (one 16-byte half row per thread)
+    if (tid < 2 * TC_M) {
+      const int r = tid >> 1, k = (tid & 1) * 8;
+      const int64_t row = tile * TC_M + r;
+      uint4 v = make_uint4(0, 0, 0, 0);
+      if (row < n) v = *reinterpret_cast<const uint4*>(feat + row * TC_IN + k);
+      *reinterpret_cast<uint4*>(sm + OFF_X + canon_off(r, k, TC_IN)) = v;
+    }
+    async_proxy_fence();
+    tc_fence_before();
+    __syncthreads();
+    // 2. layer 1
+    if (tid == 0) {
+      tc_fence_after();
+      umma_bf16(tmem, dX, dW1, id_l, 0u);
+      umma_commit(&bar);
+    }
+    if (!vk::mbar_wait(&bar, phase, TC_WAIT)) atomicOr(&abort_flag, 1);
+    phase ^= 1u;
+    tc_fence_after();
+    // 3. epilogue 1: H1 = bf16(relu(D + b1)) into the layer-2 operand
+    for (int c0 = col0; c0 < col0 + TC_COLS_PER_WARP; c0 += 32) {
+      uint32_t v[32];
+      tmem_ld32(lane_base + (uint32_t)c0, v);
+      tmem_wait_ld();
+      uint8_t* dst = sm + OFF_H + canon_off(my_row, c0, TC_H);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        uint4 w;
+        const int c = c0 + 8 * q;
+        w.x = pack2(fmaxf(__uint_as_float(v[8 * q + 0]) + sb1[c + 0], 0.f),
+                    fmaxf(__uint_as_float(v[8 * q + 1]) + sb1[c + 1], 0.f));
+        w.y = pack2(fmaxf(__uint_as_float(v[8 * q + 2]) + sb1[c + 2], 0.f),
+                    fmaxf(__uint_as_float(v[8 * q + 3]) + sb1[c + 3], 0.f));
+        w.z = pack2(fmaxf(__uint_as_float(v[8 * q + 4]) + sb1[c + 4], 0.f),
+                    fmaxf(__uint_as_float(v[8 * q + 5]) + sb1[c + 5], 0.f));
+        w.w = pack2(fmaxf(__uint_as_float(v[8 * q + 6]) + sb1[c + 6], 0.f),
+                    fmaxf(__uint_as_float(v[8 * q + 7]) + sb1[c + 7], 0.f));
+        *reinterpret_cast<uint4*>(dst + q * 128) = w;    // k chunks 128 bytes apart
+      }
+    }
+    async_proxy_fence();
+    tc_fence_before();
+    __syncthreads();
+    if (abort_flag) break;
+    // 4. layer 2 (K = 256 in 16 steps of 16)
+    if (tid == 0) {
+      tc_fence_after();
+#pragma unroll 1
+      for (int ks = 0; ks < TC_H / 16; ++ks) {
+        const uint64_t dA = smem_desc(s_base + OFF_H + ks * 256, 128, (TC_H / 8) * 128);
+        const uint64_t dB = smem_desc(s_base + OFF_W2 + ks * 256, 128, (TC_H / 8) * 128);
+        umma_bf16(tmem, dA, dB, id_l, ks > 0 ? 1u : 0u);
+      }
+      umma_commit(&bar);
+    }
+    if (!vk::mbar_wait(&bar, phase, TC_WAIT)) atomicOr(&abort_flag, 1);
+    phase ^= 1u;
+    tc_fence_after();
+    // 5. epilogue 2: partial logit of this thread's row over the warp's columns, then the row's four quarters
+    float z = 0.f;
+    for (int c0 = col0; c0 < col0 + TC_COLS_PER_WARP; c0 += 32) {
+      uint32_t v[32];
+      tmem_ld32(lane_base + (uint32_t)c0, v);
+      tmem_wait_ld();
+#pragma unroll
+      for (int j = 0; j < 32; ++j) z += fmaxf(__uint_as_float(v[j]) + sb2[c0 + j], 0.f) * sw3[c0 + j];
+    }
+    part[cq * TC_M + my_row] = z;
+    tc_fence_before();
+    __syncthreads();
+    if (tid < TC_M) {
+      const int64_t row = tile * TC_M + tid;
+      if (row < n) logit[row] = ((part[tid] + part[TC_M + tid]) + (part[2 * TC_M + tid] + part[3 * TC_M + tid])) + b3;
+    }
+    if (abort_flag) break;
+  }
+  if (abort_flag) {
+    if (tid == 0) {
+      atomicOr(status, VK_STATUS_WAIT_TIMEOUT);
+      vk::mbar_wait(&bar, phase, TC_WAIT);   // the MMAs in flight, once more, bounded
+    }
+    __syncthreads();
+  }
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS));
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int64_t vk_mlp_infer_tc_smem(void) { return (int64_t)TC_SMEM + 128; }
+
+int vk_mlp_infer_tc(int64_t n, const int64_t* n_dev, const void* feat_bf16, const void* W1_bf16, const float* b1,
+                    const void* W2_bf16, const float* b2, const float* w3, float b3, float* logit, int grid,
+                    int32_t* status, void* stream) {
+  if (n <= 0) return 0;
+  if (grid < 1 || !status) return VK_E_ARG;
+  const size_t sh = (size_t)vk_mlp_infer_tc_smem();
+  cudaError_t e = cudaFuncSetAttribute(mlp_infer_tc_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  if (e != cudaSuccess) return vk_err(e);
+  mlp_infer_tc_k<<<grid, TC_THREADS, sh, (cudaStream_t)stream>>>(
+      n, n_dev, reinterpret_cast<const __nv_bfloat16*>(feat_bf16), reinterpret_cast<const __nv_bfloat16*>(W1_bf16), b1,
+      reinterpret_cast<const __nv_bfloat16*>(W2_bf16), b2, w3, b3, logit, status);
+  return vk_launch_status();
+}
+
+}  // extern "C"

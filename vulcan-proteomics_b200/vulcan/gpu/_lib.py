@@ -75,8 +75,8 @@ _SIGS_B200 = {
     "vk_tindex_emit": [P, P, P, P, P, P, P, P, P, P],
     "vk_scan_i64": [P, I64, P, P, P],
     "vk_scan_i64_noalloc": [P, I64, P, P],
-    "vk_k0_count": [I32, P, P, F32, F32, I32, P, P],
-    "vk_k0_fill": [I32, P, P, P, F32, F32, I32, I32, P, P, P, P, P, I32, P],
+    "vk_k0_count": [I32, P, P, P, F32, F32, I32, P, P, P, P, P],
+    "vk_k0_fill": [I32, P, P, P, F32, F32, I32, I32, P, P, P, P, P, I32, P, P, P, P],
     "vk_hyp_count": [I32, P, P, P, I32, I32, I32, I32, P, P],
     "vk_hyp_fill": [I32, P, P, P, I32, I32, I32, I32, F32, F32, I32, P, I64, P, P, P, P, P, P, P, P, P, P],
     "vk_k1_plan_count": [P, I64, P, P, P, P, P],
@@ -91,6 +91,7 @@ _SIGS_B200 = {
     "vk_search_fused_grid": [P, I32, I32, I32, I32, P],
     "vk_cand_features": [I64, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P],
     "vk_mlp_infer": [I64, P, P, P, P, P, P, P, F32, P, I32, P],
+    "vk_mlp_infer_tc": [I64, P, P, P, P, P, P, P, F32, P, I32, P, P],
     "vk_select_pruned": [I32, P, P, P, P, P, P, F32, I32, I32, I32, P, I32, P, P, P, P, P],
     "vk_gemm": [I32, I32, I32, P, I64, I64, P, I32, I64, I64, P, I32, I32, P, I64, I64, P],
     "vk_colsum": [I32, I32, P, P, P],
@@ -120,6 +121,8 @@ def lib():
     L.vk_scan_noalloc_max_n.restype = I64
     L.vk_mlp_infer_smem.argtypes = []
     L.vk_mlp_infer_smem.restype = I64
+    L.vk_mlp_infer_tc_smem.argtypes = []
+    L.vk_mlp_infer_tc_smem.restype = I64
     _lib = L
     return L
 
@@ -137,8 +140,9 @@ def stream():
 
 _TRACE = os.environ.get("VK_TRACE") == "1"
 # kernels launched by one successful call of an entry point (default 1); `LAUNCHES` counts them
+# kernels launched by one call of an entry point (counted by `check`; the default is 1)
 _KERNELS_PER_CALL = {"scan": 3, "set_params": 0, "set_nterm": 0, "set_tol_da": 0, "tindex_layout": 0,
-                     "fused_grid": 0}
+                     "fused_grid": 0, "k0_fill": 2}
 LAUNCHES = {"n": 0}
 
 

@@ -249,8 +249,12 @@ def _k0_device(run: DeviceRun, p: SearchParams, dev):
     L = K.lib()
     n = run.n
     kept = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
-    K.check(L.vk_k0_count(n, K.ptr(run.offsets), K.ptr(run.mz), p.fragment_min_mz, p.fragment_max_mz, p.max_peaks,
-                          K.ptr(kept), K.stream()), "k0_count")
+    easy = torch.empty(max(n, 1), dtype=torch.uint8, device=dev)
+    hard = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
+    n_hard = torch.empty(1, dtype=torch.int32, device=dev)
+    K.check(L.vk_k0_count(n, K.ptr(run.offsets), K.ptr(run.mz), K.ptr(run.intensity), p.fragment_min_mz,
+                          p.fragment_max_mz, p.max_peaks, K.ptr(kept), K.ptr(easy), K.ptr(hard), K.ptr(n_hard),
+                          K.stream()), "k0_count")
     off = _scan(kept[:n])
     cap = max(run.n_raw, 1)
     mass = torch.empty(cap, dtype=torch.float32, device=dev)
@@ -259,7 +263,8 @@ def _k0_device(run: DeviceRun, p: SearchParams, dev):
     valid = torch.empty(max(n, 1), dtype=torch.uint8, device=dev)
     K.check(L.vk_k0_fill(n, K.ptr(run.offsets), K.ptr(run.mz), K.ptr(run.intensity), p.fragment_min_mz,
                          p.fragment_max_mz, p.max_peaks, p.min_peaks, K.ptr(off), K.ptr(mass), K.ptr(inten),
-                         K.ptr(tic), K.ptr(valid), run.max_raw, K.stream()), "k0_fill")
+                         K.ptr(tic), K.ptr(valid), run.max_raw, K.ptr(easy), K.ptr(hard), K.ptr(n_hard),
+                         K.stream()), "k0_fill")
     return {"off": off, "mass": mass, "int": inten, "tic": tic[:n], "valid_d": valid[:n]}
 
 
@@ -290,14 +295,15 @@ def _hyp_device(run: DeviceRun, peaks, gi: GpuIndex, p: SearchParams):
                            K.ptr(cnt), K.stream()), "hyp_count")
     off = _scan(cnt[:n])
     cap = max(n_max, 1)
-    h = {"spec": torch.zeros(cap, dtype=torch.int32, device=dev),
-         "z": torch.zeros(cap, dtype=torch.int8, device=dev),
-         "iso": torch.zeros(cap, dtype=torch.int8, device=dev),
-         "pm": torch.zeros(cap, dtype=torch.float32, device=dev),
-         "M": torch.zeros(cap, dtype=torch.float32, device=dev),
-         "lo": torch.zeros(cap, dtype=torch.int64, device=dev),
-         "hi": torch.zeros(cap, dtype=torch.int64, device=dev),
-         "maxfz": torch.zeros(cap, dtype=torch.int8, device=dev)}
+    # one zeroed allocation for all hypothesis columns (slots past the spectra's hypotheses stay empty windows)
+    cols = (("lo", torch.int64), ("hi", torch.int64), ("spec", torch.int32), ("pm", torch.float32),
+            ("M", torch.float32), ("z", torch.int8), ("iso", torch.int8), ("maxfz", torch.int8))
+    sizes = [(cap * torch.empty(0, dtype=dt).element_size() + 15) & ~15 for _, dt in cols]
+    buf = torch.zeros(sum(sizes), dtype=torch.uint8, device=dev)
+    h, o = {}, 0
+    for (name, dt), sz in zip(cols, sizes):
+        h[name] = buf[o:o + sz].view(dt)[:cap]
+        o += sz
     mfc = p.max_fragment_charge or 0
     K.check(L.vk_hyp_fill(n, K.ptr(peaks["valid_d"]), K.ptr(run.precursor_mz), K.ptr(run.charge), z0, z1, i0, i1,
                           float(p.precursor_ppm[0]), float(p.precursor_ppm[1]), int(mfc), K.ptr(gi.mass32), gi.n,

@@ -11,7 +11,7 @@ label-free and pair closure runs after the pruning, so targets and decoys are tr
 Features per hit (``vk_cand_features``): K1 shared-peak count, summed matched intensity (fraction of the spectrum's
 TIC, K1's fixed-point sums), precursor error in ppm, precursor charge, peptide length, missed cleavages.
 Network: 16 -> 256 (ReLU) -> 256 (ReLU) -> 1, BF16 weights and layer-1 activations, FP32 accumulation; inference
-on tensor cores (``vk_mlp_infer``), training by the deterministic kernels of ``mlp_train.cu`` (forward, backward,
+on the tcgen05 tensor cores (``vk_mlp_infer_tc``; ``vk_mlp_infer`` is the mma.sync variant), training by the deterministic kernels of ``mlp_train.cu`` (forward, backward,
 weighted BCE, Adam) on the GPU.  Training target: the hit, itself or through its pair-closure partner, lands in the
 top 5 of the exhaustive rescoring of its spectrum (K2 over every row of the precursor windows).
 """
@@ -45,7 +45,7 @@ class Pruner:
     selection parameters (``tau``, ``min_keep``, ``max_keep``)."""
 
     def __init__(self, device="cuda", seed: int = 0, tau: float = -math.inf, min_keep: int = 1,
-                 max_keep: int = 128, min_count: int = 1):
+                 max_keep: int = 128, min_count: int = 1, tensor_cores: str = "tcgen05"):
         self.dev = torch.device(device)
         g = torch.Generator().manual_seed(seed)
         W1 = torch.zeros(HIDDEN, N_IN)
@@ -58,6 +58,9 @@ class Pruner:
         self.sd = torch.ones(N_IN, device=self.dev)
         self.tau, self.min_keep, self.max_keep = float(tau), int(min_keep), int(max_keep)
         self.min_count = int(min_count)     # shortlist only hits with K1 count >= min_count (calibrated)
+        if tensor_cores not in ("tcgen05", "mma.sync"):
+            raise ValueError("tensor_cores must be 'tcgen05' or 'mma.sync'")
+        self.tensor_cores = tensor_cores    # inference kernel: vk_mlp_infer_tc or vk_mlp_infer
         self.step = 0
         self._adam = None
         self._sync_bf16()
@@ -110,17 +113,25 @@ class Pruner:
                                          K.ptr(mu), K.ptr(sd), K.ptr(feat), K.stream()), "cand_features")
         return feat
 
-    def score(self, feat: torch.Tensor, hits, n: int, n_dev=None) -> torch.Tensor:
+    def score(self, feat: torch.Tensor, hits, n: int, n_dev=None, status=None) -> torch.Tensor:
         """Selection score of every hit: the MLP logit."""
-        return self.logits(feat, n, n_dev)
+        return self.logits(feat, n, n_dev, status)
 
-    def logits(self, feat: torch.Tensor, n: int, n_dev=None) -> torch.Tensor:
+    def logits(self, feat: torch.Tensor, n: int, n_dev=None, status=None) -> torch.Tensor:
+        """MLP logits of n feature rows.  With the tcgen05 kernel a wait timeout is ORed into ``status`` (device
+        i32) when given, else checked here (one host sync)."""
         out = torch.empty(max(n, 1), dtype=torch.float32, device=self.dev)
         grid = max(1, min(_n_sm(self.dev), (n + 127) // 128))
-        K.check(K.lib().vk_mlp_infer(n, K.ptr(n_dev) if n_dev is not None else None, K.ptr(feat),
-                                     K.ptr(self.bf["W1"]), K.ptr(self.w["b1"]), K.ptr(self.bf["W2"]),
-                                     K.ptr(self.w["b2"]), K.ptr(self.w["w3"]), self._b3, K.ptr(out), grid,
-                                     K.stream()), "mlp_infer")
+        nd = K.ptr(n_dev) if n_dev is not None else None
+        args = (K.ptr(feat), K.ptr(self.bf["W1"]), K.ptr(self.w["b1"]), K.ptr(self.bf["W2"]), K.ptr(self.w["b2"]),
+                K.ptr(self.w["w3"]), self._b3, K.ptr(out), grid)
+        if self.tensor_cores == "tcgen05":
+            st = status if status is not None else torch.zeros(1, dtype=torch.int32, device=self.dev)
+            K.check(K.lib().vk_mlp_infer_tc(n, nd, *args, K.ptr(st), K.stream()), "mlp_infer_tc")
+            if status is None and n > 0 and int(st.item()):
+                raise RuntimeError("mlp_infer_tc: a tensor-core MMA did not complete")
+        else:
+            K.check(K.lib().vk_mlp_infer(n, nd, *args, K.stream()), "mlp_infer")
         return out[:n]
 
     # ------------------------------------------------------------------ training (GPU kernels)
@@ -230,7 +241,7 @@ class CountRanker(Pruner):
     """The method without the network: hits ranked by K1 count alone, with the same calibrated threshold and
     selection (the baseline the learned pruner is compared against)."""
 
-    def score(self, feat, hits, n: int, n_dev=None) -> torch.Tensor:
+    def score(self, feat, hits, n: int, n_dev=None, status=None) -> torch.Tensor:
         return hits["c_cnt"][:n].to(torch.float32)
 
 
@@ -271,7 +282,7 @@ def _pruned_device(run: E.DeviceRun, gi: E.GpuIndex, p: SearchParams, pr: Pruner
         return E.Timer(st, name) if timers else E._NoTimer()
     with phase("prune"):
         feat = pr.features(gi, f["dh"], f["win_off"], f["isum"], hits, n_bound, n_dev=n_dev)
-        logit = pr.score(feat, hits, n_bound, n_dev=n_dev)
+        logit = pr.score(feat, hits, n_bound, n_dev=n_dev, status=f["status"])
         cap = (2 if p.pair_closure else 1) * pr.max_keep
         s_hyp = torch.empty(max(n * cap, 1), dtype=torch.int64, device=dev)
         s_row = torch.empty_like(s_hyp)
