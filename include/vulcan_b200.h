@@ -341,11 +341,13 @@ int vk_mlp_infer_tc(int64_t n, const int64_t* n_dev, const void* feat_bf16, cons
 /* Pruned candidate selection per spectrum: hits with logit >= tau plus the min_keep best by (logit, count, hit
  * order) descending, at most max_keep (a power of two >= 16); pair closure; candidates sorted by row with duplicate
  * rows merged (lowest hypothesis, highest count) into slots s*cap (cap >= (pair_closure ? 2 : 1) * max_keep), the
- * layout of vk_select_topk. */
+ * layout of vk_select_topk.  max_hits (1..4096) bounds the hits of one spectrum (e.g. the shortlist's top-k); it
+ * sizes the per-warp sort, and a spectrum with more hits keeps its first max_keep hits with logit >= tau in hit
+ * order instead. */
 int vk_select_pruned(int n_spec, const int64_t* spec_hyp_off, const int64_t* hit_off, const int64_t* hit_hyp,
                      const int32_t* hit_row, const int64_t* hit_cnt, const float* logit, float tau, int min_keep,
-                     int max_keep, int pair_closure, const int64_t* partner, int cap, int64_t* c_hyp, int64_t* c_row,
-                     int64_t* c_cnt, int64_t* n_cand, void* stream);
+                     int max_keep, int pair_closure, const int64_t* partner, int cap, int max_hits, int64_t* c_hyp,
+                     int64_t* c_row, int64_t* c_cnt, int64_t* n_cand, void* stream);
 
 /* Training kernels.  vk_gemm: C[m*scm + n*scn] = sum_k A[m*sam + k*sak] * B[k*sbk + n*sbn] (+ bias[n]) (ReLU)
  * (rounded to a BF16 value); B is BF16 when b_bf16 != 0, else FP32; deterministic (fixed summation order). */

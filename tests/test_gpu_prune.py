@@ -204,7 +204,7 @@ def test_select_pruned_equals_oracle(mini, param_sets, indexes, name, keep, torc
     K.check(K.lib().vk_select_pruned(n_spec, K.ptr(f["dh"]["spec_off"]), K.ptr(hits["cand_off"]),
                                      K.ptr(hits["c_hyp"]), K.ptr(hits["c_row32"]), K.ptr(hits["c_cnt"]),
                                      K.ptr(logit), tau, min_keep, max_keep, closure, K.ptr(gi.partner), cap,
-                                     K.ptr(out["h"]), K.ptr(out["r"]), K.ptr(out["c"]), K.ptr(n_cand), K.stream()),
+                                     p.topk, K.ptr(out["h"]), K.ptr(out["r"]), K.ptr(out["c"]), K.ptr(n_cand), K.stream()),
             "select_pruned")
     want = O.select_pruned(_np(f["dh"]["spec_off"]), _np(hits["cand_off"]), _np(hits["c_hyp"][:n]),
                            _np(hits["c_row"][:n]), _np(hits["c_cnt"][:n]), _np(logit[:n]), tau, min_keep, max_keep,

@@ -1,11 +1,13 @@
 // K0 peak view and precursor hypotheses on the device.
 //
 // K0 (reference vulcan/gpu/engine.py:171-210, global peak mode): peaks with fmin <= m/z <= fmax (not NaN), mass =
-// m/z - PROTON in f32, the top max_peaks by (intensity desc, mass desc), then mass ascending.  One CTA per
-// spectrum sorts 64-bit keys that carry both values (no payload): (~ord(intensity), ~ord(mass)) for the selection
-// and (ord(mass), ~ord(intensity)) for the final order, where ord() maps a float to an order-preserving u32.  Peaks
-// with equal intensity and mass are indistinguishable, so the reference's remaining tie order (input position)
-// cannot change any output.  TIC = f64 sum of the kept intensities (fixed-order tree), stored as f32.
+// m/z - PROTON in f32, the top max_peaks by (intensity desc, mass desc), then mass ascending.  Spectra whose raw
+// peaks already come in that final order with at most max_peaks in range (the usual case) are copied by a warp
+// with ballot compaction, no sort.  For the others one CTA sorts 64-bit keys that carry both values (no payload):
+// (~ord(intensity), ~ord(mass)) for the selection and (ord(mass), ~ord(intensity)) for the final order, where
+// ord() maps a float to an order-preserving u32.  Peaks with equal intensity and mass are indistinguishable, so the
+// reference's remaining tie order (input position) cannot change any output.  TIC = f64 sum of the kept
+// intensities (fixed-order tree), stored as f32.
 //
 // Hypotheses (reference vulcan/gpu/host.py:64-91): per valid spectrum with a finite precursor m/z, charges (the
 // known one, else the configured range) x isotope errors in (charge, isotope) order, Sage f32 arithmetic, row
@@ -188,126 +190,6 @@ k0_fill_k(const int32_t* hard_list, const int32_t* n_hard, const int64_t* raw_of
   }
 }
 
-// Warp-per-spectrum K0 for spectra of at most key_cap raw peaks (key_cap a power of two <= 2048).
-// 1. in-range peaks, in input order, as keys (ord(mass), ~ord(intensity)) -- ascending = mass asc, intensity desc;
-// 2. if that sequence is not already non-decreasing (unsorted input), a warp bitonic sort;
-// 3. if more than max_peaks remain: the max_peaks-th best by (intensity desc, mass desc) is found by sorting a copy
-//    of the selection keys; the peaks better than it plus the first ties (identical peaks, so which copies does not
-//    matter) are kept, in mass order.  No sort at all for sorted spectra with at most max_peaks peaks in range.
-constexpr int K0W_WARPS = 4;
-
-__device__ __forceinline__ void warp_bitonic_u64(uint64_t* v, int n_pow2, int lane) {
-  for (int k = 2; k <= n_pow2; k <<= 1)
-    for (int j = k >> 1; j > 0; j >>= 1) {
-      for (int i = lane; i < n_pow2; i += 32) {
-        int p = i ^ j;
-        if (p > i) {
-          uint64_t a = v[i], b = v[p];
-          bool up = (i & k) == 0;
-          if ((a > b) == up) { v[i] = b; v[p] = a; }
-        }
-      }
-      __syncwarp();
-    }
-}
-
-// selection key (ascending = intensity desc, mass desc) of a mass-order key
-__device__ __forceinline__ uint64_t sel_of(uint64_t k2) {
-  uint32_t om = (uint32_t)(k2 >> 32), nint = (uint32_t)k2;   // nint = ~ord(int)
-  return ((uint64_t)nint << 32) | (uint64_t)(~om);
-}
-
-__global__ void __launch_bounds__(K0W_WARPS * 32)
-k0_fill_warp_k(const int32_t* hard_list, const int32_t* n_hard, const int64_t* raw_off, const float* raw_mz,
-               const float* raw_int, float fmin, float fmax, int max_peaks, int min_peaks, const int64_t* pk_off,
-               float* pk_mass, float* pk_int, float* tic, uint8_t* valid, int key_cap) {
-  extern __shared__ uint64_t k0w_smem[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int n_work = *n_hard;
-  for (int j = blockIdx.x * K0W_WARPS + warp; j < n_work; j += gridDim.x * K0W_WARPS) {
-  const int s = hard_list[j];
-  uint64_t* keys = k0w_smem + (size_t)warp * 2 * key_cap;
-  uint64_t* sel = keys + key_cap;
-  const unsigned lt_mask = (1u << lane) - 1u;
-  const int64_t r0 = raw_off[s];
-  const int n = (int)(raw_off[s + 1] - r0);
-  int n_in = 0;
-  for (int i0 = 0; i0 < n; i0 += 32) {
-    const int i = i0 + lane;
-    bool keep = false;
-    uint64_t k = 0;
-    if (i < n) {
-      const float mz = raw_mz[r0 + i];
-      keep = in_range(mz, fmin, fmax);
-      if (keep) k = mass_key(mz, raw_int[r0 + i]);
-    }
-    const unsigned m = __ballot_sync(VK_FULL, keep);
-    if (keep) keys[n_in + __popc(m & lt_mask)] = k;
-    n_in += __popc(m);
-  }
-  __syncwarp();
-  bool sorted = true;
-  for (int i = 1 + lane; i < n_in; i += 32) sorted &= keys[i - 1] <= keys[i];
-  if (!__all_sync(VK_FULL, sorted)) {
-    int n_pow2 = 32;
-    while (n_pow2 < n_in) n_pow2 <<= 1;
-    for (int i = n_in + lane; i < n_pow2; i += 32) keys[i] = ~0ull;
-    __syncwarp();
-    warp_bitonic_u64(keys, n_pow2, lane);
-  }
-  const int64_t o0 = pk_off[s];
-  const int kept = (int)(pk_off[s + 1] - o0);
-  uint64_t thr = ~0ull;
-  int ties_left = 0;
-  if (n_in > kept) {
-    int n_pow2 = 32;
-    while (n_pow2 < n_in) n_pow2 <<= 1;
-    for (int i = lane; i < n_pow2; i += 32) sel[i] = i < n_in ? sel_of(keys[i]) : ~0ull;
-    __syncwarp();
-    warp_bitonic_u64(sel, n_pow2, lane);
-    thr = sel[kept - 1];
-    int above = 0;
-    for (int i = lane; i < n_in; i += 32) above += sel_of(keys[i]) < thr;
-    above = __reduce_add_sync(VK_FULL, above);
-    ties_left = kept - above;
-    __syncwarp();
-  }
-  double part = 0.0;
-  int w = 0;
-  for (int i0 = 0; i0 < n_in; i0 += 32) {
-    const int i = i0 + lane;
-    uint64_t k = i < n_in ? keys[i] : ~0ull;
-    bool take = false;
-    if (i < n_in) {
-      const uint64_t q = sel_of(k);
-      take = q < thr || n_in <= kept;
-      if (!take && q == thr) take = true;   // a tie: resolved below in order
-    }
-    const unsigned tie = __ballot_sync(VK_FULL, take && n_in > kept && sel_of(k) == thr);
-    if (take && n_in > kept && sel_of(k) == thr) take = __popc(tie & lt_mask) < ties_left;
-    ties_left -= __popc(tie);
-    if (ties_left < 0) ties_left = 0;
-    const unsigned m = __ballot_sync(VK_FULL, take);
-    if (take) {
-      const int pos = w + __popc(m & lt_mask);
-      const float mass = unord_f32((uint32_t)(k >> 32));
-      const float it = unord_f32(~(uint32_t)k);
-      pk_mass[o0 + pos] = mass;
-      pk_int[o0 + pos] = it;
-      part += (double)it;
-    }
-    w += __popc(m);
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(VK_FULL, part, o);
-  if (lane == 0) {
-    tic[s] = (float)part;
-    valid[s] = kept >= min_peaks;
-  }
-  __syncwarp();
-  }
-}
-
 __global__ void hyp_count_k(int n_spec, const uint8_t* valid, const double* pmz, const int8_t* charge, int n_z,
                             int n_iso, int64_t* n_hyp) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -398,24 +280,13 @@ int vk_k0_fill(int n_spec, const int64_t* raw_off, const float* raw_mz, const fl
   int dev = 0, n_sm = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-  if (max_raw <= 2048) {
-    int key_cap = 32;
-    while (key_cap < max_raw) key_cap <<= 1;
-    size_t shw = (size_t)K0W_WARPS * 2 * key_cap * sizeof(uint64_t);
-    e = cudaFuncSetAttribute(k0_fill_warp_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shw);
-    if (e != cudaSuccess) return vk_err(e);
-    const int grid = (int)min((int64_t)n_sm * 4, ((int64_t)n_spec + K0W_WARPS - 1) / K0W_WARPS);
-    k0_fill_warp_k<<<grid, K0W_WARPS * 32, shw, st>>>(hard_list, n_hard, raw_off, raw_mz, raw_int, fmin, fmax,
-                                                     max_peaks, min_peaks, pk_off, pk_mass, pk_int, tic, valid,
-                                                     key_cap);
-    return vk_launch_status();
-  }
-  int n_pow2 = 1;
+  // hard spectra (unsorted, NaN, or more than max_peaks in range): one CTA each, sorting in shared memory
+  int n_pow2 = 32;
   while (n_pow2 < max_raw) n_pow2 <<= 1;
   size_t sh = (size_t)n_pow2 * sizeof(uint64_t);
   e = cudaFuncSetAttribute(k0_fill_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
   if (e != cudaSuccess) return vk_err(e);
-  const int grid = (int)min((int64_t)n_sm * 2, (int64_t)n_spec);
+  const int grid = (int)min((int64_t)n_sm * 8, (int64_t)n_spec);
   k0_fill_k<<<grid, K0_THREADS, sh, st>>>(hard_list, n_hard, raw_off, raw_mz, raw_int, fmin, fmax, max_peaks,
                                           min_peaks, pk_off, pk_mass, pk_int, tic, valid);
   return vk_launch_status();

@@ -337,11 +337,13 @@ int vk_mlp_infer(int64_t n, const int64_t* n_dev, const void* feat_bf16, const v
 
 int vk_select_pruned(int n_spec, const int64_t* spec_hyp_off, const int64_t* hit_off, const int64_t* hit_hyp,
                      const int32_t* hit_row, const int64_t* hit_cnt, const float* logit, float tau, int min_keep,
-                     int max_keep, int pair_closure, const int64_t* partner, int cap, int64_t* c_hyp, int64_t* c_row,
-                     int64_t* c_cnt, int64_t* n_cand, void* stream) {
+                     int max_keep, int pair_closure, const int64_t* partner, int cap, int max_hits, int64_t* c_hyp,
+                     int64_t* c_row, int64_t* c_cnt, int64_t* n_cand, void* stream) {
   if (n_spec == 0) return 0;
   if (max_keep < 1 || min_keep < 0 || min_keep > max_keep || cap < (pair_closure ? 2 : 1) * max_keep) return VK_E_ARG;
-  const int sort_cap = 1024;
+  if (max_hits < 1 || max_hits > 4096) return VK_E_ARG;
+  int sort_cap = 32;
+  while (sort_cap < max_hits) sort_cap <<= 1;
   const int list_cap = 2 * max_keep > 32 ? 2 * max_keep : 32;
   int list_pow2 = 1;
   while (list_pow2 < list_cap) list_pow2 <<= 1;

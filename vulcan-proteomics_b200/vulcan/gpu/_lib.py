@@ -92,7 +92,7 @@ _SIGS_B200 = {
     "vk_cand_features": [I64, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P],
     "vk_mlp_infer": [I64, P, P, P, P, P, P, P, F32, P, I32, P],
     "vk_mlp_infer_tc": [I64, P, P, P, P, P, P, P, F32, P, I32, P, P],
-    "vk_select_pruned": [I32, P, P, P, P, P, P, F32, I32, I32, I32, P, I32, P, P, P, P, P],
+    "vk_select_pruned": [I32, P, P, P, P, P, P, F32, I32, I32, I32, P, I32, I32, P, P, P, P, P],
     "vk_gemm": [I32, I32, I32, P, I64, I64, P, I32, I64, I64, P, I32, I32, P, I64, I64, P],
     "vk_colsum": [I32, I32, P, P, P],
     "vk_relu_mask": [I64, P, P, P],

@@ -290,7 +290,7 @@ def _pruned_device(run: E.DeviceRun, gi: E.GpuIndex, p: SearchParams, pr: Pruner
         n_cand = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
         K.check(L.vk_select_pruned(n, K.ptr(f["dh"]["spec_off"]), K.ptr(hits["cand_off"]), K.ptr(hits["c_hyp"]),
                                    K.ptr(hits["c_row32"]), K.ptr(hits["c_cnt"]), K.ptr(logit), pr.tau, pr.min_keep,
-                                   pr.max_keep, int(p.pair_closure), K.ptr(gi.partner), cap, K.ptr(s_hyp),
+                                   pr.max_keep, int(p.pair_closure), K.ptr(gi.partner), cap, p.topk, K.ptr(s_hyp),
                                    K.ptr(s_row), K.ptr(s_cnt), K.ptr(n_cand), K.stream()), "select_pruned")
         cand = E._compact(n, cap, n_cand, s_hyp, s_row, s_cnt, f["dh"], dev)
     with phase("k2"):
