@@ -477,17 +477,19 @@ def _kernel_table(a, p, gi, run, flush, pr, dev):
     n_items = int(item_off[-1])
     cursor = torch.empty(nt, dtype=torch.int64, device=dev)
     item_hyp = torch.empty(max(n_items, 1), dtype=torch.int32, device=dev)
-    K.check(L.vk_k1_plan_fill(C.byref(gi.tix), dh["n_max"], K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(item_off),
-                              K.ptr(cursor), K.ptr(item_hyp), K.stream()), "k1_plan_fill")
     status = torch.zeros(1, dtype=torch.int32, device=dev)
+    K.check(L.vk_k1_plan_fill(C.byref(gi.tix), dh["n_max"], K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(item_off),
+                              K.ptr(cursor), K.ptr(item_hyp), item_hyp.numel(), K.ptr(status), K.stream()),
+            "k1_plan_fill")
     win_off, cnt = so["win_off"], so["cnt"]
     n_win = int(win_off[-1])
     isum = so.get("isum")
     kern = {}
     ms_k1 = timed(lambda: K.check(L.vk_k1_tiles(
         C.byref(gi.tix), C.byref(gi.fp), float(p.fragment_ppm[0]), float(p.fragment_ppm[1]), p.k1_warps,
-        K.ptr(item_off), K.ptr(item_hyp), K.ptr(dh["spec"]), K.ptr(dh["maxfz"]), K.ptr(dh["lo"]), K.ptr(dh["hi"]),
-        K.ptr(win_off), K.ptr(peaks["off"]), K.ptr(peaks["mass"]), K.ptr(cnt), K.ptr(status),
+        K.ptr(item_off), K.ptr(item_hyp), dh["n_max"], item_hyp.numel(), K.ptr(dh["spec"]), K.ptr(dh["maxfz"]),
+        K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(win_off), cnt.numel(), K.ptr(peaks["off"]), K.ptr(peaks["mass"]),
+        K.ptr(cnt), K.ptr(status),
         K.ptr(peaks["int"]) if pruned else None, K.ptr(peaks["tic"]) if pruned else None,
         K.ptr(isum) if pruned else None, K.stream()), "k1_tiles"))
     k1b = k1_algorithmic_bytes(gi, dh, peaks, win_off, item_off, item_hyp)
@@ -506,8 +508,8 @@ def _kernel_table(a, p, gi, run, flush, pr, dev):
     ss_ = torch.empty(n, dtype=torch.int64, device=dev)
     sm_ = torch.empty(n, dtype=torch.int64, device=dev)
     ms_tk = timed(lambda: K.check(L.vk_select_topk(
-        n, K.ptr(dh["spec_off"]), K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(win_off), K.ptr(cnt), K.ptr(gi.partner),
-        thr, p.topk, closure, cap, K.ptr(tk["h"]), K.ptr(tk["r"]), K.ptr(tk["c"]),
+        n, K.ptr(dh["spec_off"]), K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(win_off), K.ptr(cnt), cnt.numel(),
+        K.ptr(gi.partner), thr, p.topk, closure, cap, K.ptr(tk["h"]), K.ptr(tk["r"]), K.ptr(tk["c"]),
         K.ptr(tk_n), K.ptr(hs_), K.ptr(hm_), K.ptr(ss_), K.ptr(sm_), K.stream()), "select_topk"))
     n_hit = int(hits["cand_off"][-1])
     n_sel = int(((hits["c_cnt"][:n_hit] >= 0)).sum())

@@ -189,16 +189,20 @@ int vk_hyp_fill(int n_spec, const uint8_t* valid, const double* precursor_mz, co
  * the caller) gets VK_STATUS_WAIT_TIMEOUT if a tile copy did not complete within the bounded wait.  `warps`
  * (1..16) per CTA, one CTA per tile.  isum (may be NULL; then pk_int and tic may be NULL too): per window row the
  * summed intensity of its matches, u32 fixed point = sum of round(intensity * 2^24 / tic[s]), for the candidate
- * pruner's features.  VK_E_TOO_LARGE if a tile and the histograms do not fit one CTA's shared memory. */
+ * pruner's features.  VK_E_TOO_LARGE if a tile and the histograms do not fit one CTA's shared memory.
+ * The buffers may be sized by bounds instead of the exact totals (no host read-back between the calls):
+ * item_hyp holds item_cap entries, cnt / isum cnt_cap; items or windows that would not fit are skipped and set
+ * VK_STATUS_OVERFLOW in `status` (the caller then retries with larger buffers). */
 int vk_k1_plan_count(const vk_tindex* ix, int64_t n_hyp, const int64_t* h_lo, const int64_t* h_hi,
                      int64_t* tile_items, int64_t* win_len, void* stream);
 int vk_k1_plan_fill(const vk_tindex* ix, int64_t n_hyp, const int64_t* h_lo, const int64_t* h_hi,
-                    const int64_t* tile_item_off, int64_t* cursor, int32_t* item_hyp, void* stream);
+                    const int64_t* tile_item_off, int64_t* cursor, int32_t* item_hyp, int64_t item_cap,
+                    int32_t* status, void* stream);
 int vk_k1_tiles(const vk_tindex* ix, const vk_frag_params* fp, float tol_lo, float tol_hi, int warps,
-                const int64_t* tile_item_off, const int32_t* item_hyp, const int32_t* h_spec,
-                const int8_t* h_maxfz, const int64_t* h_lo, const int64_t* h_hi, const int64_t* win_off,
-                const int64_t* pk_off, const float* pk_mass, int32_t* cnt, int32_t* status, const float* pk_int,
-                const float* tic, uint32_t* isum, void* stream);
+                const int64_t* tile_item_off, const int32_t* item_hyp, int64_t n_hyp, int64_t item_cap,
+                const int32_t* h_spec, const int8_t* h_maxfz, const int64_t* h_lo, const int64_t* h_hi,
+                const int64_t* win_off, int64_t cnt_cap, const int64_t* pk_off, const float* pk_mass, int32_t* cnt,
+                int32_t* status, const float* pk_int, const float* tic, uint32_t* isum, void* stream);
 
 /* Top-K + pair closure (reference vulcan/gpu/engine.py:284-312) per spectrum, from the dense K1 counts.
  * Spectrum s owns hypotheses [spec_hyp_off[s], spec_hyp_off[s+1]).  Per spectrum: entries with count >= thr,
@@ -207,10 +211,10 @@ int vk_k1_tiles(const vk_tindex* ix, const vk_frag_params* fp, float tol_lo, flo
  * slots: spectrum s writes n_cand[s] candidates sorted by row at [s*cap, s*cap + n_cand[s]) of c_hyp (i64),
  * c_row (i64), c_cnt (i64); cap >= (pair_closure ? 2 : 1) * topk.  Also hyp_scored (u32, #rows with count > 0)
  * and hyp_matched (u64, sum of counts) per hypothesis, and their sums per spectrum (spec_scored, spec_matched,
- * i64; may be NULL). */
+ * i64; may be NULL).  cnt holds cnt_cap entries: a window whose slice would end past it counts as empty. */
 int vk_select_topk(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo, const int64_t* h_hi,
-                   const int64_t* win_off, const int32_t* cnt, const int64_t* partner, int thr, int topk,
-                   int pair_closure, int cap, int64_t* c_hyp, int64_t* c_row, int64_t* c_cnt, int64_t* n_cand,
+                   const int64_t* win_off, const int32_t* cnt, int64_t cnt_cap, const int64_t* partner, int thr,
+                   int topk, int pair_closure, int cap, int64_t* c_hyp, int64_t* c_row, int64_t* c_cnt, int64_t* n_cand,
                    uint32_t* hyp_scored, uint64_t* hyp_matched, int64_t* spec_scored, int64_t* spec_matched,
                    void* stream);
 

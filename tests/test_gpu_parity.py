@@ -66,7 +66,7 @@ def test_search_stages_equal_reference(mini, golden_py, golden_kernels, param_se
     P = O.make_params(STATIC, VAR, p.fragment_unit)
     peaks = {k: g[f"{name}/k0_{k}"] for k in ("off", "mass", "int")}
     win_off, cnt, sc, mt = O.k1_windows(l1, hyp, peaks, p, P)
-    assert np.array_equal(out["cnt"].cpu().numpy(), cnt)
+    assert np.array_equal(out["cnt"][:int(out["win_off"][-1])].cpu().numpy(), cnt)
     assert np.array_equal(out["hyp_scored"][:nh].cpu().numpy().astype(np.int64), golden_kernels[f"{name}/k1_scored"])
     assert np.array_equal(out["hyp_matched"][:nh].cpu().numpy().astype(np.int64),
                           golden_kernels[f"{name}/k1_matched"])
@@ -250,10 +250,60 @@ def test_k1_counts_for_every_tile_layout(mini, param_sets, torch_cuda, layout):
         pk = {k: f["peaks"][k].cpu().numpy() for k in ("off", "mass", "int")}
         P = O.make_params(STATIC, VAR, q.fragment_unit)
         win_off, cnt, _, _, isum = O.k1_windows(l1, hyp, pk, q, P, tic=f["peaks"]["tic"].cpu().numpy())
-        assert np.array_equal(f["cnt"].cpu().numpy(), cnt), name
-        assert np.array_equal(f["isum"].cpu().numpy().view(np.uint32), isum), name
+        n_win = int(f["win_off"][-1])
+        assert np.array_equal(f["cnt"][:n_win].cpu().numpy(), cnt), name
+        assert np.array_equal(f["isum"][:n_win].cpu().numpy().view(np.uint32), isum), name
         # the plain search's counts (no intensity sums) are the same
-        assert np.array_equal(E.search(sp, gi, l1, q)[2]["cnt"].cpu().numpy(), cnt), name
+        out = E.search(sp, gi, l1, q)[2]
+        assert np.array_equal(out["cnt"][:n_win].cpu().numpy(), cnt), name
+
+
+def test_k1_buffer_bounds_hold_and_overflow_is_reported(mini, param_sets, torch_cuda):
+    """K1 buffers sized by the index's window bound never overflow on real windows; buffers made too small on
+    purpose are not overrun: the kernels skip what does not fit and report VK_STATUS_OVERFLOW."""
+    import ctypes as C
+    from vulcan.gpu import _lib as K
+    from vulcan.gpu import engine as E
+    torch = torch_cuda
+    l1, sp, _ = mini
+    p = param_sets["da"]
+    gi = E.GpuIndex(l1, p, STATIC, VAR)
+    run = E.DeviceRun(sp, gi.dev)
+    peaks = E._k0_device(run, p, gi.dev)
+    dh = E._hyp_device(run, peaks, gi, p)
+    n_h = dh["n_max"]
+    win = (dh["hi"][:n_h] - dh["lo"][:n_h]).clamp(min=0)
+    assert int(win.max()) <= gi.window_bound(*p.precursor_ppm)
+    win_off, cnt, status = E._k1_dense(gi, dh, peaks, p, n_h)
+    assert int(status.item()) == 0
+    n_win = int(win_off[-1])
+    L = K.lib()
+    ix = gi.tix
+    nt = ix.n_tiles
+    tile_items = torch.empty(nt, dtype=torch.int64, device=gi.dev)
+    wl = torch.empty(n_h, dtype=torch.int64, device=gi.dev)
+    K.check(L.vk_k1_plan_count(C.byref(ix), n_h, K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(tile_items), K.ptr(wl),
+                               K.stream()), "k1_plan_count")
+    item_off = E._scan(tile_items)
+    n_items = int(item_off[-1])
+    item_cap, cnt_cap = n_items // 2, n_win // 2
+    st = torch.zeros(1, dtype=torch.int32, device=gi.dev)
+    cursor = torch.empty(nt, dtype=torch.int64, device=gi.dev)
+    item_hyp = torch.full((item_cap,), -1, dtype=torch.int32, device=gi.dev)
+    K.check(L.vk_k1_plan_fill(C.byref(ix), n_h, K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(item_off), K.ptr(cursor),
+                              K.ptr(item_hyp), item_cap, K.ptr(st), K.stream()), "k1_plan_fill")
+    small = torch.full((cnt_cap + 64,), -5, dtype=torch.int32, device=gi.dev)   # 64 guard entries past the cap
+    K.check(L.vk_k1_tiles(C.byref(ix), C.byref(gi.fp), float(p.fragment_ppm[0]), float(p.fragment_ppm[1]),
+                          p.k1_warps, K.ptr(item_off), K.ptr(item_hyp), n_h, item_cap, K.ptr(dh["spec"]),
+                          K.ptr(dh["maxfz"]), K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(win_off), cnt_cap,
+                          K.ptr(peaks["off"]), K.ptr(peaks["mass"]), K.ptr(small), K.ptr(st), None, None, None,
+                          K.stream()), "k1_tiles")
+    assert int(st.item()) & 2
+    assert bool((small[cnt_cap:] == -5).all())           # nothing written past the cap
+    # rows of the windows that fit hold their exact count, or the fill value where the tile's item was skipped
+    head = small[:cnt_cap]
+    assert bool(((head == cnt[:cnt_cap]) | (head == -5)).all())
+    assert bool((head == cnt[:cnt_cap]).any())
 
 
 def test_tiles_too_large_for_shared_memory_are_refused(mini, param_sets, torch_cuda):
@@ -366,3 +416,31 @@ def test_fused_search_equals_staged_and_reference(mini, golden_py, param_sets, i
         assert np.array_equal(cd["c_hyp"].cpu().numpy()[sel], g[f"{name}/topk_h"])
         assert np.array_equal(cd["c_row"].cpu().numpy()[sel], g[f"{name}/topk_r"])
         assert np.array_equal(t_f.column("pf_row").to_numpy(), g[f"{name}/psm_pf_row"])
+
+
+@pytest.mark.parametrize("name", SETS)
+def test_graphed_searcher_equals_search(mini, param_sets, indexes, name, torch_cuda):
+    """The graph-captured Searcher returns engine.search's PSM table, for pinned and pageable inputs, for runs of
+    the same shape replayed through the same captured pass and for a run of another shape."""
+    import dataclasses
+    from vulcan.gpu import engine as E
+    from vulcan.gpu.host import Spectra
+    l1, sp, _ = mini
+    p = dataclasses.replace(param_sets[name], search_method="staged")
+    gi = indexes[name]
+    want = E.search(sp, gi, l1, p, report=2)[0]
+    se = E.Searcher(gi, l1, p, report=2)
+    # a second run of the same shape: the peaks of every spectrum reversed in intensity order
+    inv = sp.intensity[::-1].copy()
+    sp2 = Spectra("other", sp.scan, sp.index, sp.rt, sp.precursor_mz, sp.charge, sp.mz, inv, sp.offsets)
+    want2 = E.search(sp2, gi, l1, p, report=2)[0]
+    res = se.search_many([sp, E.pin_spectra(sp2), sp, sp2])
+    assert res[0][0].equals(want) and res[2][0].equals(want)
+    assert res[1][0].equals(want2) and res[3][0].equals(want2)
+    # another shape: the first 100 spectra
+    n = 100
+    o = sp.offsets[:n + 1]
+    sp3 = Spectra("head", sp.scan[:n], sp.index[:n], sp.rt[:n], sp.precursor_mz[:n], sp.charge[:n], sp.mz[:o[-1]],
+                  sp.intensity[:o[-1]], o.copy())
+    assert se.search(sp3)[0].equals(E.search(sp3, gi, l1, p, report=2)[0])
+    assert len(se.slots) == 2

@@ -55,8 +55,9 @@ def test_k1_intensity_sums_equal_oracle(mini, param_sets, indexes, name):
     P = O.make_params(STATIC, VAR, p.fragment_unit)
     win_off, cnt, _, _, isum = O.k1_windows(l1, hyp, pk, p, P, tic=_np(f["peaks"]["tic"]))
     assert np.array_equal(_np(f["win_off"]), win_off)
-    assert np.array_equal(_np(f["cnt"]), cnt)
-    assert np.array_equal(_np(f["isum"]).view(np.uint32), isum)
+    n_win = int(f["win_off"][-1])
+    assert np.array_equal(_np(f["cnt"][:n_win]), cnt)
+    assert np.array_equal(_np(f["isum"][:n_win]).view(np.uint32), isum)
     assert isum.max() > 0
 
 
@@ -231,6 +232,24 @@ def test_pruned_search_without_pruning_is_plain(mini, param_sets, indexes, name,
     t_pr, s_pr, out = PR.search_pruned(sp, gi, l1, p, pr, report=3)
     assert t_pr.equals(t_plain)
     assert s_pr.counts["n_rescored"] == s_plain.counts["n_rescored"]
+
+
+@pytest.mark.parametrize("name", SETS)
+def test_graphed_pruned_search_equals_search_pruned(mini, param_sets, indexes, name, torch_cuda):
+    """The graph-captured Searcher with a pruner returns search_pruned's PSM table (random network, threshold at
+    the median logit so that the selection prunes)."""
+    from vulcan.gpu import engine as E
+    from vulcan.gpu import prune as PR
+    l1, sp, _ = mini
+    p = param_sets[name]
+    gi = indexes[name]
+    pr = _random_pruner(torch_cuda, gi.dev, 5)
+    pr.tau, pr.min_keep, pr.max_keep, pr.min_count = 0.0, 1, 16, 2
+    want, st, out = PR.search_pruned(sp, gi, l1, p, pr, report=2)
+    assert st.counts["n_rescored"] < st.counts["n_hits"] * 2
+    se = E.Searcher(gi, l1, p, pruner=pr, report=2)
+    for tbl, _ in se.search_many([sp, sp, sp]):
+        assert tbl.equals(want)
 
 
 # ------------------------------------------------------------------------------------------- trained pruner

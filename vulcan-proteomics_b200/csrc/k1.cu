@@ -28,27 +28,32 @@ __global__ void plan_count_k(int64_t n_hyp, int shift, const int64_t* h_lo, cons
   for (int64_t t = lo >> shift; t <= (hi - 1) >> shift; ++t) atomicAdd(&tile_items[t], 1ull);
 }
 
+// item_cap bounds item_hyp: an item past it is not written and sets VK_STATUS_OVERFLOW
 __global__ void plan_fill_k(int64_t n_hyp, int shift, const int64_t* h_lo, const int64_t* h_hi,
-                            const int64_t* tile_item_off, unsigned long long* cursor, int32_t* item_hyp) {
+                            const int64_t* tile_item_off, unsigned long long* cursor, int32_t* item_hyp,
+                            int64_t item_cap, int32_t* status) {
   int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (h >= n_hyp) return;
   int64_t lo = h_lo[h], hi = h_hi[h];
   if (hi <= lo) return;
   for (int64_t t = lo >> shift; t <= (hi - 1) >> shift; ++t) {
     unsigned long long pos = atomicAdd(&cursor[t], 1ull);
-    item_hyp[tile_item_off[t] + (int64_t)pos] = (int32_t)h;
+    const int64_t at = tile_item_off[t] + (int64_t)pos;
+    if (at < item_cap) item_hyp[at] = (int32_t)h;
+    else atomicOr(status, VK_STATUS_OVERFLOW);
   }
 }
 
 __global__ void __launch_bounds__(K1_MAX_WARPS * 32)
 k1_tiles_k(vk_tindex ix, float tol_lo, float tol_hi, int tol_da, int post_cap, const int64_t* tile_item_off,
-           const int32_t* item_hyp, const int32_t* h_spec, const int8_t* h_maxfz, const int64_t* h_lo,
-           const int64_t* h_hi, const int64_t* win_off, const int64_t* pk_off, const float* pk_mass, int32_t* cnt,
-           int32_t* status, const float* pk_int, const float* tic, uint32_t* isum_out) {
+           const int32_t* item_hyp, int64_t n_hyp, int64_t item_cap, const int32_t* h_spec, const int8_t* h_maxfz,
+           const int64_t* h_lo, const int64_t* h_hi, const int64_t* win_off, int64_t cnt_cap, const int64_t* pk_off,
+           const float* pk_mass, int32_t* cnt, int32_t* status, const float* pk_int, const float* tic,
+           uint32_t* isum_out) {
   extern __shared__ __align__(16) uint8_t k1_smem[];
   __shared__ __align__(8) uint64_t bar;
   const int64_t t = blockIdx.x;
-  const int64_t i0 = tile_item_off[t], i1 = tile_item_off[t + 1];
+  const int64_t i0 = min(tile_item_off[t], item_cap), i1 = min(tile_item_off[t + 1], item_cap);
   if (i0 == i1) return;
   const int n_warps = blockDim.x >> 5;
   const int T = 1 << ix.tile_shift;
@@ -81,7 +86,16 @@ k1_tiles_k(vk_tindex ix, float tol_lo, float tol_hi, int tol_da, int post_cap, c
   const int64_t r0 = t << ix.tile_shift;
   for (int64_t it = i0 + warp; it < i1; it += n_warps) {
     const int h = item_hyp[it];
+    // items and windows must lie inside the buffers the caller sized by bounds; anything else is skipped
+    if (h < 0 || h >= n_hyp) {
+      if (lane == 0) atomicOr(status, VK_STATUS_OVERFLOW);
+      continue;
+    }
     const int64_t lo = h_lo[h], hi = h_hi[h];
+    if (hi <= lo || win_off[h] + (hi - lo) > cnt_cap) {
+      if (lane == 0 && hi > lo) atomicOr(status, VK_STATUS_OVERFLOW);
+      continue;
+    }
     const int rlo = (int)max(lo - r0, (int64_t)0), rhi = (int)min(hi - r0, (int64_t)T);
     for (int j = rlo + lane; j < rhi; j += 32) {
       hw[j] = 0;
@@ -121,7 +135,9 @@ int vk_k1_plan_count(const vk_tindex* ix, int64_t n_hyp, const int64_t* h_lo, co
 }
 
 int vk_k1_plan_fill(const vk_tindex* ix, int64_t n_hyp, const int64_t* h_lo, const int64_t* h_hi,
-                    const int64_t* tile_item_off, int64_t* cursor, int32_t* item_hyp, void* stream) {
+                    const int64_t* tile_item_off, int64_t* cursor, int32_t* item_hyp, int64_t item_cap,
+                    int32_t* status, void* stream) {
+  if (!status || item_cap < 0) return VK_E_ARG;
   if (!ix) return VK_E_ARG;
   cudaStream_t st = (cudaStream_t)stream;
   if (ix->n_tiles > 0) {
@@ -130,15 +146,16 @@ int vk_k1_plan_fill(const vk_tindex* ix, int64_t n_hyp, const int64_t* h_lo, con
   }
   if (n_hyp == 0) return 0;
   plan_fill_k<<<(unsigned)((n_hyp + 255) / 256), 256, 0, st>>>(n_hyp, ix->tile_shift, h_lo, h_hi, tile_item_off,
-                                                                (unsigned long long*)cursor, item_hyp);
+                                                                (unsigned long long*)cursor, item_hyp, item_cap,
+                                                                status);
   return vk_launch_status();
 }
 
 int vk_k1_tiles(const vk_tindex* ix, const vk_frag_params* fp, float tol_lo, float tol_hi, int warps,
-                const int64_t* tile_item_off, const int32_t* item_hyp, const int32_t* h_spec,
-                const int8_t* h_maxfz, const int64_t* h_lo, const int64_t* h_hi, const int64_t* win_off,
-                const int64_t* pk_off, const float* pk_mass, int32_t* cnt, int32_t* status, const float* pk_int,
-                const float* tic, uint32_t* isum, void* stream) {
+                const int64_t* tile_item_off, const int32_t* item_hyp, int64_t n_hyp, int64_t item_cap,
+                const int32_t* h_spec, const int8_t* h_maxfz, const int64_t* h_lo, const int64_t* h_hi,
+                const int64_t* win_off, int64_t cnt_cap, const int64_t* pk_off, const float* pk_mass, int32_t* cnt,
+                int32_t* status, const float* pk_int, const float* tic, uint32_t* isum, void* stream) {
   if (!ix || !fp || !status) return VK_E_ARG;
   if (ix->n_tiles == 0) return 0;
   if ((ix->max_tile_postings & 3) || ix->max_tile_postings < 0 || warps < 1 || warps > K1_MAX_WARPS) return VK_E_ARG;
@@ -150,8 +167,8 @@ int vk_k1_tiles(const vk_tindex* ix, const vk_frag_params* fp, float tol_lo, flo
   cudaError_t e = cudaFuncSetAttribute(k1_tiles_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
   if (e != cudaSuccess) return vk_err(e);
   k1_tiles_k<<<(unsigned)ix->n_tiles, warps * 32, sh, (cudaStream_t)stream>>>(
-      *ix, tol_lo, tol_hi, fp->tol_da, ix->max_tile_postings, tile_item_off, item_hyp, h_spec, h_maxfz, h_lo, h_hi,
-      win_off, pk_off, pk_mass, cnt, status, pk_int, tic, isum);
+      *ix, tol_lo, tol_hi, fp->tol_da, ix->max_tile_postings, tile_item_off, item_hyp, n_hyp, item_cap, h_spec,
+      h_maxfz, h_lo, h_hi, win_off, cnt_cap, pk_off, pk_mass, cnt, status, pk_int, tic, isum);
   return vk_launch_status();
 }
 

@@ -44,9 +44,15 @@ __device__ __forceinline__ void warp_bitonic_u64(uint64_t* v, int n_pow2, int la
   }
 }
 
+// rows of a hypothesis window, or 0 when its slice would end past the count buffer (cnt_cap entries)
+__device__ __forceinline__ int64_t win_rows(int64_t w0, int64_t lo, int64_t hi, int64_t cnt_cap) {
+  const int64_t n = hi > lo ? hi - lo : 0;
+  return w0 + n <= cnt_cap ? n : 0;
+}
+
 __global__ void __launch_bounds__(TK_WARPS * 32)
 select_topk_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo, const int64_t* h_hi,
-              const int64_t* win_off, const int32_t* cnt, const int64_t* partner, int thr, int topk, int pair_closure,
+              const int64_t* win_off, const int32_t* cnt, int64_t cnt_cap, const int64_t* partner, int thr, int topk, int pair_closure,
               int cap, int list_pow2, int key_cap, int64_t* c_hyp, int64_t* c_row, int64_t* c_cnt, int64_t* n_cand,
               uint32_t* hyp_scored, uint64_t* hyp_matched, int64_t* spec_scored, int64_t* spec_matched) {
   extern __shared__ __align__(16) uint8_t tk_smem[];
@@ -67,7 +73,7 @@ select_topk_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo, cons
   // pass A: per-hypothesis statistics and the number of appended entries
   long long n_app = 0, s_sc = 0, s_mt = 0;
   for (int64_t h = hb; h < he; ++h) {
-    const int64_t w0 = win_off[h], n = h_hi[h] - h_lo[h];
+    const int64_t w0 = win_off[h], n = win_rows(w0, h_lo[h], h_hi[h], cnt_cap);
     long long sc = 0, mt = 0, ap = 0;
     for (int64_t j = lane; j < n; j += 32) {
       int c = cnt[w0 + j];
@@ -97,7 +103,7 @@ select_topk_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo, cons
     // sort path: every appended key into shared memory, bitonic sort, the topk-th largest is the threshold
     int n_k = 0;
     for (int64_t h = hb; h < he; ++h) {
-      const int64_t w0 = win_off[h], lo = h_lo[h], n = h_hi[h] - lo;
+      const int64_t w0 = win_off[h], lo = h_lo[h], n = win_rows(w0, lo, h_hi[h], cnt_cap);
       for (int64_t j0 = 0; j0 < n; j0 += 32) {
         const int64_t j = j0 + lane;
         const int c = j < n ? cnt[w0 + j] : -1;
@@ -121,7 +127,7 @@ select_topk_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo, cons
       for (int i = lane; i < 256; i += 32) W.hist[i] = 0;
       __syncwarp();
       for (int64_t h = hb; h < he; ++h) {
-        const int64_t w0 = win_off[h], lo = h_lo[h], n = h_hi[h] - lo;
+        const int64_t w0 = win_off[h], lo = h_lo[h], n = win_rows(w0, lo, h_hi[h], cnt_cap);
         for (int64_t j = lane; j < n; j += 32) {
           int c = cnt[w0 + j];
           if (c < thr) continue;
@@ -158,7 +164,7 @@ select_topk_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo, cons
   // gather the selected entries (ballot compaction, order: hypothesis, row)
   int n_sel = 0;
   for (int64_t h = hb; h < he; ++h) {
-    const int64_t w0 = win_off[h], lo = h_lo[h], n = h_hi[h] - lo;
+    const int64_t w0 = win_off[h], lo = h_lo[h], n = win_rows(w0, lo, h_hi[h], cnt_cap);
     for (int64_t j0 = 0; j0 < n; j0 += 32) {
       const int64_t j = j0 + lane;
       int c = j < n ? cnt[w0 + j] : -1;
@@ -238,7 +244,8 @@ __global__ void compact_k(int n_spec, int cap, const int64_t* n_cand, const int6
 extern "C" {
 
 int vk_select_topk(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo, const int64_t* h_hi,
-                   const int64_t* win_off, const int32_t* cnt, const int64_t* partner, int thr, int topk,
+                   const int64_t* win_off, const int32_t* cnt, int64_t cnt_cap, const int64_t* partner, int thr,
+                   int topk,
                    int pair_closure, int cap, int64_t* c_hyp, int64_t* c_row, int64_t* c_cnt, int64_t* n_cand,
                    uint32_t* hyp_scored, uint64_t* hyp_matched, int64_t* spec_scored, int64_t* spec_matched,
                    void* stream) {
@@ -253,7 +260,8 @@ int vk_select_topk(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo,
   cudaError_t e = cudaFuncSetAttribute(select_topk_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
   if (e != cudaSuccess) return vk_err(e);
   select_topk_k<<<(unsigned)((n_spec + TK_WARPS - 1) / TK_WARPS), TK_WARPS * 32, sh, (cudaStream_t)stream>>>(
-      n_spec, spec_hyp_off, h_lo, h_hi, win_off, cnt, partner, thr, topk, pair_closure, cap, list_pow2, key_cap, c_hyp,
+      n_spec, spec_hyp_off, h_lo, h_hi, win_off, cnt, cnt_cap, partner, thr, topk, pair_closure, cap, list_pow2,
+      key_cap, c_hyp,
       c_row,
       c_cnt, n_cand, hyp_scored, hyp_matched, spec_scored, spec_matched);
   return vk_launch_status();

@@ -80,9 +80,9 @@ _SIGS_B200 = {
     "vk_hyp_count": [I32, P, P, P, I32, I32, I32, I32, P, P],
     "vk_hyp_fill": [I32, P, P, P, I32, I32, I32, I32, F32, F32, I32, P, I64, P, P, P, P, P, P, P, P, P, P],
     "vk_k1_plan_count": [P, I64, P, P, P, P, P],
-    "vk_k1_plan_fill": [P, I64, P, P, P, P, P, P],
-    "vk_k1_tiles": [P, P, F32, F32, I32, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P],
-    "vk_select_topk": [I32, P, P, P, P, P, P, I32, I32, I32, I32, P, P, P, P, P, P, P, P, P],
+    "vk_k1_plan_fill": [P, I64, P, P, P, P, P, I64, P, P],
+    "vk_k1_tiles": [P, P, F32, F32, I32, P, P, I64, I64, P, P, P, P, P, I64, P, P, P, P, P, P, P, P],
+    "vk_select_topk": [I32, P, P, P, P, P, I64, P, I32, I32, I32, I32, P, P, P, P, P, P, P, P, P],
     "vk_compact_cands": [I32, I32, P, P, P, P, P, P, P, P, P, P, P, P],
     "vk_k2_spectra": [P, I32, P, P, P, P, P, P, P, P, P, P, P, F32, F32, P, P, P, P, P, P, P, P, P, P],
     "vk_psm_rank": [I32, P, P, P, P, P, I32, I32, P, P, P, P, P, P],

@@ -144,6 +144,22 @@ class GpuIndex:
     def table_ptrs(self):
         return (K.ptr(self.seq_off), K.ptr(self.length), K.ptr(self.mask), K.ptr(self.mass32), K.ptr(self.residues))
 
+    def window_bound(self, ppm_lo: float, ppm_hi: float) -> int:
+        """Most index rows one precursor window [M(1 + lo/1e6), M(1 + hi/1e6)] can hold, for any M: the largest
+        number of rows within a relative mass width of (hi - lo)/1e6 (with a margin for the f32 rounding of the
+        window edges).  Sizes the K1 buffers without reading the exact totals back from the device."""
+        key = (float(ppm_lo), float(ppm_hi))
+        cache = self.__dict__.setdefault("_window_bound", {})
+        if key not in cache:
+            m = np.asarray(self.mass32_np, np.float64)
+            w = max(0.0, (ppm_hi - ppm_lo) * 1e-6) * 1.001 + 1e-6
+            if len(m):
+                j = np.searchsorted(m, m * (1.0 + w), side="right")
+                cache[key] = int((j - np.arange(len(m))).max()) + 2
+            else:
+                cache[key] = 0
+        return cache[key]
+
     def _build_tiles(self):
         L = K.lib()
         p = self.p
@@ -365,36 +381,50 @@ def _as_dev(hyp, dev):
 def _k1_dense(gi: GpuIndex, dh, peaks, p: SearchParams, n_hyp: int, stats: Stats | None = None,
               isum: bool = False):
     """Tiled K1: dense counts of every window row.  Returns (win_off, cnt, status), plus the summed matched
-    intensity of every window row (u32, 2^24 = the spectrum's TIC) when ``isum``."""
+    intensity of every window row (u32, 2^24 = the spectrum's TIC) when ``isum``.  The buffers are sized by the
+    index's window bound (``GpuIndex.window_bound``), so nothing is read back from the device: cnt / isum hold
+    more entries than the win_off[-1] window rows, and ``status`` gets VK_STATUS_OVERFLOW should a bound not hold."""
     L = K.lib()
     dev = gi.dev
     ix = gi.tix
     nt = ix.n_tiles
+    max_win = gi.window_bound(*p.precursor_ppm)
+    T = 1 << ix.tile_shift
+    item_cap = max(1, n_hyp * ((max_win + T - 1) // T + 1))
+    cnt_cap = max(1, n_hyp * max_win)
     tile_items = torch.empty(max(nt, 1), dtype=torch.int64, device=dev)
     win_len = torch.empty(max(n_hyp, 1), dtype=torch.int64, device=dev)
     K.check(L.vk_k1_plan_count(C.byref(ix), n_hyp, K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(tile_items),
                                K.ptr(win_len), K.stream()), "k1_plan_count")
     item_off = _scan(tile_items[:nt])
     win_off = _scan(win_len[:n_hyp])
-    n_items, n_win = torch.stack([item_off[-1], win_off[-1]]).cpu().tolist()
-    cursor = torch.empty(max(nt, 1), dtype=torch.int64, device=dev)
-    item_hyp = torch.empty(max(n_items, 1), dtype=torch.int32, device=dev)
-    K.check(L.vk_k1_plan_fill(C.byref(ix), n_hyp, K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(item_off),
-                              K.ptr(cursor), K.ptr(item_hyp), K.stream()), "k1_plan_fill")
-    cnt = torch.empty(max(n_win, 1), dtype=torch.int32, device=dev)
     status = torch.zeros(1, dtype=torch.int32, device=dev)
-    isw = torch.empty(max(n_win, 1), dtype=torch.int32, device=dev) if isum else None
+    cursor = torch.empty(max(nt, 1), dtype=torch.int64, device=dev)
+    item_hyp = torch.empty(item_cap, dtype=torch.int32, device=dev)
+    K.check(L.vk_k1_plan_fill(C.byref(ix), n_hyp, K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(item_off),
+                              K.ptr(cursor), K.ptr(item_hyp), item_cap, K.ptr(status), K.stream()), "k1_plan_fill")
+    cnt = torch.empty(cnt_cap, dtype=torch.int32, device=dev)
+    isw = torch.empty(cnt_cap, dtype=torch.int32, device=dev) if isum else None
     K.check(L.vk_k1_tiles(C.byref(ix), C.byref(gi.fp), float(p.fragment_ppm[0]), float(p.fragment_ppm[1]),
-                          p.k1_warps, K.ptr(item_off), K.ptr(item_hyp), K.ptr(dh["spec"]), K.ptr(dh["maxfz"]), K.ptr(dh["lo"]),
-                          K.ptr(dh["hi"]), K.ptr(win_off), K.ptr(peaks["off"]), K.ptr(peaks["mass"]), K.ptr(cnt),
-                          K.ptr(status), K.ptr(peaks["int"]) if isum else None, K.ptr(peaks["tic"]) if isum else None,
+                          p.k1_warps, K.ptr(item_off), K.ptr(item_hyp), n_hyp, item_cap, K.ptr(dh["spec"]),
+                          K.ptr(dh["maxfz"]), K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(win_off), cnt_cap,
+                          K.ptr(peaks["off"]), K.ptr(peaks["mass"]), K.ptr(cnt), K.ptr(status),
+                          K.ptr(peaks["int"]) if isum else None, K.ptr(peaks["tic"]) if isum else None,
                           K.ptr(isw) if isum else None, K.stream()), "k1_tiles")
-    if stats is not None:
-        stats.counts["k1_work_items"] = stats.counts.get("k1_work_items", 0) + n_items
-        stats.counts["k1_window_candidates"] = stats.counts.get("k1_window_candidates", 0) + n_win
     if isum:
-        return win_off, cnt[:n_win], status, isw[:n_win]
-    return win_off, cnt[:n_win], status
+        return win_off, cnt, status, isw
+    return win_off, cnt, status
+
+
+def check_status(status: torch.Tensor, what: str = "search"):
+    """Raise on the device status bits of a pass (one host read)."""
+    v = int(status.item())
+    if v & 1:
+        raise RuntimeError(f"{what}: a bounded device wait timed out (tile copy or tensor-core MMA)")
+    if v & 2:
+        raise RuntimeError(f"{what}: a device buffer bound was exceeded")
+    if v:
+        raise RuntimeError(f"{what}: device status {v}")
 
 
 def run_k1(gi: GpuIndex, hyp, peaks, p: SearchParams, stats: Stats):
@@ -404,8 +434,8 @@ def run_k1(gi: GpuIndex, hyp, peaks, p: SearchParams, stats: Stats):
     dh = _as_dev(hyp, dev)
     n_h = len(hyp["spec"])
     win_off, cnt, status = _k1_dense(gi, dh, peaks, p, n_h, stats)
-    if int(status.item()):
-        raise RuntimeError("k1_tiles: a tile copy did not complete")
+    check_status(status, "k1")
+    cnt = cnt[:int(win_off[-1])]
     win_len = (dh["hi"] - dh["lo"]).clamp(min=0)
     hh = torch.repeat_interleave(torch.arange(n_h, device=dev), win_len)
     rr = dh["lo"][hh] + (torch.arange(len(hh), device=dev) - win_off[:-1][hh])
@@ -601,7 +631,7 @@ def _shortlist(gi: GpuIndex, p: SearchParams, n: int, dh, win_off, cnt, topk: in
     spec_scored = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
     spec_matched = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
     K.check(L.vk_select_topk(n, K.ptr(dh["spec_off"]), K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(win_off),
-                             K.ptr(cnt), K.ptr(gi.partner), p.k1_threshold if thr is None else thr, topk,
+                             K.ptr(cnt), cnt.numel(), K.ptr(gi.partner), p.k1_threshold if thr is None else thr, topk,
                              int(closure), cap,
                              K.ptr(s_hyp), K.ptr(s_row), K.ptr(s_cnt), K.ptr(n_cand), K.ptr(hyp_scored),
                              K.ptr(hyp_matched), K.ptr(spec_scored), K.ptr(spec_matched), K.stream()),
@@ -809,8 +839,7 @@ def search(sp: Spectra, gi: GpuIndex, l1, p: SearchParams, report: int | None = 
                 rec = _gather_fused(out, report, st)
         if method == "staged":
             out = _search_device(run, gi, p, report, st, timers)
-            if int(out["status"].item()):
-                raise RuntimeError("k1_tiles: a tile copy did not complete")
+            check_status(out["status"])
             rec = _gather_psms(*out["psm"], out["c_hyp"], out["c_row"], out["c_cnt"], out["k2"], out["dh"],
                                out["spec_scored"], out["spec_matched"], out["peaks"]["tic"], report, st)
         elif method != "fused":
@@ -821,8 +850,239 @@ def search(sp: Spectra, gi: GpuIndex, l1, p: SearchParams, report: int | None = 
     n_rescored = int(out["cand_off"][-1]) if "cand_off" in out else -1
     st.counts.update(n_spectra=len(sp), n_searched=int(out["peaks"]["valid_d"].sum()),
                      n_hypotheses=int(out["dh"]["spec_off"][-1]), n_rescored=n_rescored, n_psms=tbl.num_rows)
+    if "win_off" in out:
+        st.counts["k1_window_rows"] = int(out["win_off"][-1])
     st.counts["cpu_core_s"] = (ru1.ru_utime - ru0.ru_utime) + (ru1.ru_stime - ru0.ru_stime)
     return tbl, st, out
+
+
+# ------------------------------------------------------------------------------------------------ graphs
+_PSM_COLS = (("cand", None), ("spec", None), ("rank", None), ("dnext", None), ("dbest", None), ("row", None),
+             ("hyp", None), ("k1", None), ("z", None), ("iso", None), ("pm", None), ("spec_scored", None),
+             ("spec_matched", None), ("tic", None), ("hyperscore", None), ("summed_b", None), ("summed_y", None),
+             ("ppm", None), ("matched_b", None), ("matched_y", None), ("longest_b", None), ("longest_y", None))
+
+
+def _pack_psms(out: dict, report: int, n: int):
+    """Every PSM slot's columns (empty slots included, marked cand = -1) packed into one byte buffer on the
+    device, without a host read: the graph-captured pass ends with it and the host reads it in one copy.
+    Returns (buffer, layout) with layout = [(name, numpy dtype, byte offset, count)]."""
+    psm_cand, psm_rank, dnext, dbest = out["psm"]
+    slots = n * report
+    ci = psm_cand[:slots].clamp(min=0)
+    s = torch.arange(slots, device=psm_cand.device) // max(report, 1)
+    hh = out["c_hyp"][ci]
+    dh, k2, pk = out["dh"], out["k2"], out["peaks"]
+    cols = {"cand": psm_cand[:slots], "spec": s, "rank": psm_rank[:slots], "dnext": dnext[:slots],
+            "dbest": dbest[:slots], "row": out["c_row"][ci], "hyp": hh, "k1": out["c_cnt"][ci], "z": dh["z"][hh],
+            "iso": dh["iso"][hh], "pm": dh["pm"][hh], "spec_scored": out["spec_scored"][s],
+            "spec_matched": out["spec_matched"][s], "tic": pk["tic"][s]}
+    for k in ("hyperscore", "summed_b", "summed_y", "ppm", "matched_b", "matched_y", "longest_b", "longest_y"):
+        cols[k] = k2[k][ci]
+    parts, layout, off = [], [], 0
+    for name, _ in _PSM_COLS:
+        t = cols[name].contiguous()
+        b = t.view(torch.uint8)
+        pad = (-b.numel()) % 8
+        parts.append(b)
+        if pad:
+            parts.append(torch.zeros(pad, dtype=torch.uint8, device=b.device))
+        layout.append((name, np.dtype(str(t.dtype).replace("torch.", "")), off, t.numel()))
+        off += b.numel() + pad
+    return torch.cat(parts), layout
+
+
+def _unpack_psms(host: np.ndarray, layout) -> dict:
+    """Host records of the filled PSM slots from a packed buffer."""
+    cols = {name: np.frombuffer(host, dtype=dt, count=cnt, offset=off) for name, dt, off, cnt in layout}
+    ok = cols["cand"] >= 0
+    rec = {k: v[ok] for k, v in cols.items() if k != "cand"}
+    return rec
+
+
+class GraphedPass:
+    """One device pass over the fixed buffers of a resident run, captured once as a CUDA graph and replayed: the
+    whole pass (K0 ... ranking and the packed PSM gather) is one launch.  Every buffer size is known on the host
+    (bounds), so the pass reads nothing back while it runs.  ``fn()`` runs the pass and returns its outputs."""
+
+    def __init__(self, fn, dev):
+        side = torch.cuda.Stream(dev)
+        side.wait_stream(torch.cuda.current_stream(dev))
+        with torch.cuda.stream(side):
+            for _ in range(2):
+                fn()
+        torch.cuda.current_stream(dev).wait_stream(side)
+        torch.cuda.synchronize(dev)
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph, capture_error_mode="relaxed"):
+            self.out = fn()
+
+    def replay(self):
+        self.graph.replay()
+        return self.out
+
+
+def _pinned_like(a: np.ndarray) -> np.ndarray:
+    return torch.empty(a.shape, dtype=torch.from_numpy(np.ascontiguousarray(a[:0])).dtype,
+                       pin_memory=True).numpy()
+
+
+def _is_pinned(a: np.ndarray) -> bool:
+    try:
+        return bool(torch.from_numpy(a).is_pinned())
+    except (TypeError, ValueError, RuntimeError):
+        return False
+
+
+class _Slot:
+    """Device buffers of one run shape, the captured pass over them, pinned staging and the packed result."""
+
+    def __init__(self, sp: Spectra, searcher: "Searcher", cap_raw: int, max_raw: int):
+        se = searcher
+        dev = se.gi.dev
+        self.n = len(sp)
+        pad = _pad_run(sp, cap_raw, max_raw)
+        self.run = DeviceRun(pad, dev, pinned=False)
+        self.run.max_raw = max_raw
+        self.run.n_raw = cap_raw
+        report = se.report
+
+        def fn():
+            out = se.device_pass(self.run)
+            buf, layout = _pack_psms(out, report, self.n)
+            out["packed"] = buf
+            self.layout = layout
+            return out
+        self.gp = GraphedPass(fn, dev)
+        self.host_out = torch.empty(self.gp.out["packed"].numel(), dtype=torch.uint8, pin_memory=True)
+        self.stage = {}
+        self.h2d_done = torch.cuda.Event()
+        self.done = torch.cuda.Event()
+        self.busy = False
+
+
+def _pad_run(sp: Spectra, cap_raw: int, max_raw: int) -> Spectra:
+    """A copy of the run whose peak arrays have cap_raw entries (the tail unused) for sizing slot buffers."""
+    mz = np.zeros(cap_raw, np.float32)
+    it = np.zeros(cap_raw, np.float32)
+    n_raw = int(sp.offsets[-1])
+    mz[:n_raw] = sp.mz
+    it[:n_raw] = sp.intensity
+    return Spectra(sp.run, sp.scan, sp.index, sp.rt, sp.precursor_mz, sp.charge, mz, it, np.asarray(sp.offsets))
+
+
+class Searcher:
+    """Repeated searches of runs through graph-captured device passes (plain, or pruned with ``pruner``).
+
+    Runs are grouped by shape (spectra, peak capacity, largest peak count, hypothesis bound); each shape gets two
+    slots of device buffers with a captured pass, used alternately, so that the host-to-device copy of one run (on
+    a copy stream) overlaps the pass of the previous one.  ``submit(sp)`` queues a run and returns a handle,
+    ``result(handle)`` waits for it and builds its PSM table; ``search(sp)`` does both; ``search_many(runs)``
+    keeps one run in flight while the previous table is built.  Inputs already in pinned host memory
+    (``pin_spectra``) are copied straight to the device; others are staged through pinned buffers first.  Results
+    are identical to ``engine.search`` / ``prune.search_pruned``."""
+
+    def __init__(self, gi: GpuIndex, l1, p: SearchParams, pruner=None, report: int | None = None):
+        self.gi, self.l1, self.p, self.pruner = gi, l1, p, pruner
+        self.report = p.report_psms if report is None else report
+        self.slots = {}
+        self.copy_stream = torch.cuda.Stream(gi.dev)
+        self.compute_stream = torch.cuda.Stream(gi.dev)
+        self._turn = {}
+
+    def device_pass(self, run: DeviceRun):
+        if self.pruner is None:
+            return _search_device(run, self.gi, self.p, self.report, Stats())
+        from . import prune
+        return prune._pruned_device(run, self.gi, self.p, self.pruner, self.report, Stats())
+
+    def _key(self, sp: Spectra):
+        n_raw = int(np.asarray(sp.offsets)[-1]) if len(sp.offsets) else 0
+        lens = np.diff(np.asarray(sp.offsets, np.int64))
+        mr = int(lens.max()) if len(lens) else 0
+        cap = 1 << max(10, int(n_raw - 1).bit_length())
+        mr2 = 1 << max(5, int(mr - 1).bit_length())
+        z0, z1 = self.p.precursor_charge
+        i0, i1 = self.p.isotope_errors
+        n_max = int(np.where(np.asarray(sp.charge) > 0, 1, z1 - z0 + 1).sum()) * (i1 - i0 + 1)
+        return (len(sp), cap, mr2, n_max)
+
+    def submit(self, sp: Spectra):
+        key = self._key(sp)
+        with torch.cuda.device(self.gi.dev):
+            if key not in self.slots:
+                self.slots[key] = [_Slot(sp, self, key[1], key[2]) for _ in range(2)]
+                self._turn[key] = 0
+            slot = self.slots[key][self._turn[key]]
+            self._turn[key] ^= 1
+            if slot.busy:
+                raise RuntimeError("result() of the previous run in this slot was not collected")
+            slot.busy = True
+            run = slot.run
+            n_raw = int(sp.offsets[-1])
+            pairs = ((run.mz, sp.mz, n_raw), (run.intensity, sp.intensity, n_raw),
+                     (run.offsets, sp.offsets, len(sp) + 1), (run.precursor_mz, sp.precursor_mz, len(sp)),
+                     (run.charge, sp.charge, len(sp)))
+            # the previous pass over this slot must be done before its inputs are overwritten
+            self.copy_stream.wait_event(slot.done)
+            h2d = 0
+            with torch.cuda.stream(self.copy_stream):
+                for i, (dst, a, cnt) in enumerate(pairs):
+                    a = np.ascontiguousarray(a)[:cnt]
+                    if a.dtype != torch.empty(0, dtype=dst.dtype).numpy().dtype:
+                        a = a.astype(torch.empty(0, dtype=dst.dtype).numpy().dtype)
+                    if not _is_pinned(a):
+                        st = slot.stage.get(i)
+                        if st is None or len(st) < cnt:
+                            st = slot.stage[i] = _pinned_like(np.empty(max(cnt, 1), a.dtype))
+                        np.copyto(st[:cnt], a)
+                        a = st[:cnt]
+                    dst[:cnt].copy_(torch.from_numpy(a), non_blocking=True)
+                    h2d += a.nbytes
+            slot.h2d_done.record(self.copy_stream)
+            self.compute_stream.wait_event(slot.h2d_done)
+            with torch.cuda.stream(self.compute_stream):
+                out = slot.gp.replay()
+                slot.host_out.copy_(out["packed"], non_blocking=True)
+                slot.done.record(self.compute_stream)
+            return (sp, slot, h2d)
+
+    def result(self, handle):
+        sp, slot, h2d = handle
+        slot.done.synchronize()
+        check_status(slot.gp.out["status"])
+        rec = _unpack_psms(slot.host_out.numpy(), slot.layout)
+        rec = {k: v.copy() for k, v in rec.items()}
+        slot.busy = False
+        st = Stats()
+        st.h2d_bytes, st.d2h_bytes = h2d, slot.host_out.numel()
+        return _psm_columns(sp, self.l1, rec, self.p), st
+
+    def search(self, sp: Spectra):
+        return self.result(self.submit(sp))
+
+    def search_many(self, runs):
+        """PSM tables of many runs, one run queued ahead of the table being built."""
+        out, pending = [], None
+        for sp in runs:
+            h = self.submit(sp)
+            if pending is not None:
+                out.append(self.result(pending))
+            pending = h
+        if pending is not None:
+            out.append(self.result(pending))
+        return out
+
+
+def pin_spectra(sp: Spectra) -> Spectra:
+    """The run with its peak and precursor arrays in pinned host memory (copied once), for Searcher.submit."""
+    def pin(a, dt):
+        a = np.ascontiguousarray(a, dtype=dt)
+        b = _pinned_like(a)
+        np.copyto(b, a)
+        return b
+    return Spectra(sp.run, sp.scan, sp.index, sp.rt, pin(sp.precursor_mz, np.float64), pin(sp.charge, np.int8),
+                   pin(sp.mz, np.float32), pin(sp.intensity, np.float32), pin(sp.offsets, np.int64))
 
 
 # ------------------------------------------------------------------------------------------------ references

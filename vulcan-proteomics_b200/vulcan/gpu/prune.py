@@ -316,8 +316,7 @@ def search_pruned(sp: Spectra, gi: E.GpuIndex, l1, p: SearchParams, pruner: Prun
     with torch.cuda.device(gi.dev):
         run = E.DeviceRun(sp, gi.dev, st)
         out = _pruned_device(run, gi, p, pruner, report, st, timers)
-        if int(out["status"].item()):
-            raise RuntimeError("k1_tiles: a tile copy did not complete")
+        E.check_status(out["status"])
         rec = E._gather_psms(*out["psm"], out["c_hyp"], out["c_row"], out["c_cnt"], out["k2"], out["dh"],
                              out["spec_scored"], out["spec_matched"], out["peaks"]["tic"], report, st)
     tbl = E._psm_columns(sp, l1, rec, p)
