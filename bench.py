@@ -12,10 +12,12 @@ calibrated on one more run to >= 99.95% top-1 recall; the plain exhaustive path 
 K2) is then timed the same way on the same run and the pruned path's top-1 recall and PSMs at 1% q are judged
 against it (`vs_plain`).
 
-  value      spectra/s with the run's raw spectra already in HBM (device pass, CUDA events on the stream, L2
-             flushed between steps), summed over ranks (each rank searches its own run: weak scaling)
-  e2e        spectra/s through the public API (prune.search_pruned / engine.search) with host buffers: H2D of the
-             raw spectra, the device pass, D2H of the PSM rows and the host PSM table (wall clock around each call)
+  value      spectra/s with the run's raw spectra already in HBM (device pass captured once as a CUDA graph and
+             replayed, CUDA events on the stream, L2 flushed between steps), summed over ranks (each rank searches
+             its own run: weak scaling); eager_ms_per_step is the same pass launched kernel by kernel
+  e2e        spectra/s through the public API (engine.Searcher, plain or with the pruner) over the run in pinned host
+             memory: H2D of the raw spectra on a copy stream, the graph replay, one D2H of the packed PSM slots and
+             the host PSM table, runs queued one ahead (wall clock around all steps)
   roofline   the dominant kernel's algorithmic bytes per launch / its mean CUDA-event duration vs the measured
              HBM copy bandwidth; mlp_roofline: the MLP's FLOPs / duration vs the measured bf16 tensor peak
   cpu_baseline  the CPU oracle (C/OpenMP restatement of the reference kernels) on a bounded sample, all cores
@@ -331,32 +333,66 @@ def run_b200(a):
 
     def step_pruned():
         return PR._pruned_device(run, gi, p, pr, 1, st)
-    step = step_pruned if pruned else step_plain
-    for _ in range(a.warmup):
-        step()
-    torch.cuda.synchronize()
+
+    def graphed(fn):
+        """(replay function, our kernel launches per pass): the pass captured as one CUDA graph."""
+        n0 = K.LAUNCHES["n"]
+        fn()
+        per_pass = K.LAUNCHES["n"] - n0
+        gp = E.GraphedPass(fn, dev)
+        return gp.replay, per_pass
+
+    def device_timing(fn, graph: bool):
+        for _ in range(a.warmup):
+            fn()
+        step, per_pass = graphed(fn) if graph else (fn, None)
+        for _ in range(a.warmup):
+            step()
+        torch.cuda.synchronize()
+        ms, launches, out = _timed_passes(step, flush, a.steps, world, dist, K)
+        return ms, (per_pass * a.steps if per_pass is not None else launches), out
+
+    use_graph = p.search_method != "fused"
     clocks = ClockSampler(local)
-    ms_max, launches, out = _timed_passes(step, flush, a.steps, world, dist, K)
+    ms_max, launches, out = device_timing(step_pruned if pruned else step_plain, use_graph)
     clk = clocks.stop()
+    if use_graph:
+        E.check_status(out["status"])
     ms_per_step = ms_max / a.steps
     value = len(sp) * world * a.steps / (ms_max / 1e3)
+    ms_eager, _, _ = _timed_passes(step_pruned if pruned else step_plain, flush, a.steps, world, dist, K)
     if p.search_method == "fused" and not pruned:
         st_ok = int(out["status"][:len(sp)].max())
         if st_ok:
             raise RuntimeError(f"fused search status {st_ok}: spectra over the window capacity or a copy timeout")
+
+    # end to end through the public API: Searcher (graph-captured passes) over runs in pinned host memory, or
+    # engine.search for the fused method
     e2e_steps = max(3, min(a.steps, 20))
-    if pruned:
-        e2e, s2 = _timed_e2e(lambda: PR.search_pruned(sp, gi, l1, p, pr), len(sp), e2e_steps, world, dist, dev)
-    else:
-        e2e, s2 = _timed_e2e(lambda: E.search(sp, gi, l1, p), len(sp), e2e_steps, world, dist, dev)
+    pinned = E.pin_spectra(sp)
+
+    def e2e_rate(pruner):
+        if not use_graph:
+            return _timed_e2e(lambda: E.search(sp, gi, l1, p), len(sp), e2e_steps, world, dist, dev)
+        se = E.Searcher(gi, l1, p, pruner=pruner, report=1)
+        se.search_many([pinned, pinned])
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        res = se.search_many([pinned] * e2e_steps)
+        torch.cuda.synchronize()
+        t = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return len(sp) * world * e2e_steps / float(t.item()), res[-1][1]
+    e2e, s2 = e2e_rate(pr)
     h2d, d2h = s2.h2d_bytes, s2.d2h_bytes
     comparison = None
     if pruned:
         # the plain exhaustive path on the same run, same timing rules, and the pruned path's accuracy against it
-        for _ in range(a.warmup):
-            step_plain()
-        ms_plain, _, _ = _timed_passes(step_plain, flush, a.steps, world, dist, K)
-        e2e_plain, _ = _timed_e2e(lambda: E.search(sp, gi, l1, p), len(sp), e2e_steps, world, dist, dev)
+        ms_plain, _, _ = device_timing(step_plain, True)
+        e2e_plain, _ = e2e_rate(None)
         ev = PR.evaluate(sp, gi, l1, lab, p, pr)
         comparison = {"plain_value": round(len(sp) * world * a.steps / (ms_plain / 1e3), 1),
                       "plain_ms_per_step": round(ms_plain / a.steps, 4), "plain_e2e": round(e2e_plain, 1),
@@ -398,7 +434,11 @@ def run_b200(a):
                    "sample": f"first {n_s} spectra of the run through the oracle's plain path K0->hypotheses->K1->"
                              f"top-k->K2->ranking ({t_s:.1f} s)"}
         extra = {"spectra_per_step_per_gpu": len(sp), "index_rows": len(l1), "index_postings": gi.n_postings,
-                 "tile_rows": p.tile_rows, "parallelism": f"replicas x{world} (one run per GPU)"}
+                 "tile_rows": p.tile_rows, "parallelism": f"replicas x{world} (one run per GPU)",
+                 "launch": "one CUDA graph per pass (eager_ms_per_step: the same pass launched kernel by kernel)"
+                           if use_graph else "kernel by kernel",
+                 "e2e": "Searcher.search_many over the run in pinned host memory: H2D on a copy stream, graph replay, "
+                        "one D2H of the packed PSM slots, host PSM table" if use_graph else "engine.search"}
         if pruned:
             extra["path"] = ("learned-pruned search: K1 (+ intensity sums) -> top-k shortlist of hits with count >= "
                              f"{pr.min_count} -> BF16 MLP 16-256-256-1 -> logit >= calibrated tau or best "
@@ -406,7 +446,8 @@ def run_b200(a):
             extra["pruner"] = pr_info
         line = {
             "metric": METRIC, "value": round(value, 1), "unit": "spectra/s", "n_gpus": world, "steps": a.steps,
-            "warmup": a.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True, "scaling": "weak",
+            "warmup": a.warmup, "ms_per_step": round(ms_per_step, 4), "eager_ms_per_step": round(ms_eager / a.steps, 4),
+            "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 (MLP: bf16 weights, fp32 accumulate)" if pruned else "f32",
             "data": "synthetic",
             "config": _config(w, p, extra),
