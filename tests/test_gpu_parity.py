@@ -444,3 +444,29 @@ def test_graphed_searcher_equals_search(mini, param_sets, indexes, name, torch_c
                   sp.intensity[:o[-1]], o.copy())
     assert se.search(sp3)[0].equals(E.search(sp3, gi, l1, p, report=2)[0])
     assert len(se.slots) == 2
+
+
+@pytest.mark.parametrize("name", SETS)
+def test_psm_table_features_on_device_equal_host(mini, param_sets, indexes, name, torch_cuda):
+    """The PSM table columns computed on the device (packed gather) equal the host computation of the same
+    features from the gathered records: bit for bit, except the f64 Poisson term (device exp / log / pow)."""
+    import dataclasses
+    from vulcan.gpu import engine as E
+    l1, sp, _ = mini
+    p = dataclasses.replace(param_sets[name], search_method="staged")
+    gi = indexes[name]
+    st = E.Stats()
+    run = E.DeviceRun(sp, gi.dev, st)
+    out = E._search_device(run, gi, p, 3, st)
+    dev_tbl = E._read_packed(*E._pack_psms(gi, out, 3, run.n), sp)
+    rec = E._gather_psms(*out["psm"], out["c_hyp"], out["c_row"], out["c_cnt"], out["k2"], out["dh"],
+                         out["spec_scored"], out["spec_matched"], out["peaks"]["tic"], 3)
+    host_tbl = E._psm_columns(sp, l1, rec, p)
+    assert dev_tbl.num_rows == host_tbl.num_rows > 0
+    assert dev_tbl.column_names == host_tbl.column_names
+    for c in dev_tbl.column_names:
+        a, b = dev_tbl.column(c).to_numpy(), host_tbl.column(c).to_numpy()
+        if c == "poisson":
+            np.testing.assert_allclose(a, b, rtol=1e-12)
+        else:
+            assert np.array_equal(a, b, equal_nan=a.dtype.kind == "f"), c

@@ -126,6 +126,8 @@ class GpuIndex:
         self.residues = up(l1.residues.astype(np.uint8))
         self.partner = up(l1.partner.astype(np.int64))
         self.missed = up(np.asarray(l1.missed).astype(np.uint8))
+        self.n_var = up(np.asarray(l1.n_var).astype(np.uint8))
+        self.pf_id = up(np.asarray(l1.pf_id).astype(np.uint64).view(np.int64))
         if self.n >= 2 ** ROW_BITS:
             raise ValueError("index rows must be < 2^28")
         # reference layout constants (used by the compatible entry points)
@@ -139,7 +141,7 @@ class GpuIndex:
         self.build_s = time.perf_counter() - t0
         self.device_bytes = sum(t.numel() * t.element_size() for t in
                                 [self.seq_off, self.length, self.mask, self.mass32, self.residues, self.partner,
-                                 self.missed, self.tile_off, self.cbin_off, self.postings])
+                                 self.missed, self.n_var, self.pf_id, self.tile_off, self.cbin_off, self.postings])
 
     def table_ptrs(self):
         return (K.ptr(self.seq_off), K.ptr(self.length), K.ptr(self.mask), K.ptr(self.mass32), K.ptr(self.residues))
@@ -555,7 +557,7 @@ def _psm_columns(sp: Spectra, l1, rec: dict, p: SearchParams) -> pa.Table:
     plen = l1.length[rows].astype(np.int64)
     sbs = (rec["summed_b"] + rec["summed_y"]).astype(np.float32)
     cols = {
-        "run": pa.array([sp.run] * len(s)),
+        "run": pa.repeat(pa.scalar(sp.run, pa.string()), len(s)),
         "spec_idx": s.astype(np.int64), "scan": sp.scan[s], "rt": sp.rt[s],
         "rank": rec["rank"].astype(np.int32), "pf_row": rows.astype(np.int64), "pf_id": l1.pf_id[rows],
         "charge": z.astype(np.int8), "isotope_error": iso.astype(np.int8),
@@ -836,15 +838,13 @@ def search(sp: Spectra, gi: GpuIndex, l1, p: SearchParams, report: int | None = 
             if stat & 1:   # a spectrum spans more window rows than the fused kernel holds: staged path for the run
                 method = "staged"
             else:
-                rec = _gather_fused(out, report, st)
+                tbl = _read_packed(*_pack_fused(gi, out, report, run.n), sp, st)
         if method == "staged":
             out = _search_device(run, gi, p, report, st, timers)
             check_status(out["status"])
-            rec = _gather_psms(*out["psm"], out["c_hyp"], out["c_row"], out["c_cnt"], out["k2"], out["dh"],
-                               out["spec_scored"], out["spec_matched"], out["peaks"]["tic"], report, st)
+            tbl = _read_packed(*_pack_psms(gi, out, report, run.n), sp, st)
         elif method != "fused":
             raise ValueError(f"unknown search_method {method!r}")
-    tbl = _psm_columns(sp, l1, rec, p)
     ru1 = resource.getrusage(resource.RUSAGE_SELF)
     st.wall_s["total"] = time.perf_counter() - t0
     n_rescored = int(out["cand_off"][-1]) if "cand_off" in out else -1
@@ -857,47 +857,127 @@ def search(sp: Spectra, gi: GpuIndex, l1, p: SearchParams, report: int | None = 
 
 
 # ------------------------------------------------------------------------------------------------ graphs
-_PSM_COLS = (("cand", None), ("spec", None), ("rank", None), ("dnext", None), ("dbest", None), ("row", None),
-             ("hyp", None), ("k1", None), ("z", None), ("iso", None), ("pm", None), ("spec_scored", None),
-             ("spec_matched", None), ("tic", None), ("hyperscore", None), ("summed_b", None), ("summed_y", None),
-             ("ppm", None), ("matched_b", None), ("matched_y", None), ("longest_b", None), ("longest_y", None))
+_PSM_TABLE = ("spec_idx", "rank", "pf_row", "pf_id", "charge", "isotope_error", "expmass", "calcmass",
+              "delta_mass_ppm", "hyperscore", "delta_next", "delta_best", "matched_b", "matched_y", "matched_peaks",
+              "summed_intensity", "matched_intensity_pct", "average_ppm", "longest_b", "longest_y", "longest_y_pct",
+              "peptide_len", "missed_cleavages", "n_var", "k1_count", "scored_candidates", "poisson")
 
 
-def _pack_psms(out: dict, report: int, n: int):
-    """Every PSM slot's columns (empty slots included, marked cand = -1) packed into one byte buffer on the
-    device, without a host read: the graph-captured pass ends with it and the host reads it in one copy.
-    Returns (buffer, layout) with layout = [(name, numpy dtype, byte offset, count)]."""
-    psm_cand, psm_rank, dnext, dbest = out["psm"]
-    slots = n * report
-    ci = psm_cand[:slots].clamp(min=0)
-    s = torch.arange(slots, device=psm_cand.device) // max(report, 1)
-    hh = out["c_hyp"][ci]
-    dh, k2, pk = out["dh"], out["k2"], out["peaks"]
-    cols = {"cand": psm_cand[:slots], "spec": s, "rank": psm_rank[:slots], "dnext": dnext[:slots],
-            "dbest": dbest[:slots], "row": out["c_row"][ci], "hyp": hh, "k1": out["c_cnt"][ci], "z": dh["z"][hh],
-            "iso": dh["iso"][hh], "pm": dh["pm"][hh], "spec_scored": out["spec_scored"][s],
-            "spec_matched": out["spec_matched"][s], "tic": pk["tic"][s]}
-    for k in ("hyperscore", "summed_b", "summed_y", "ppm", "matched_b", "matched_y", "longest_b", "longest_y"):
-        cols[k] = k2[k][ci]
+def _lnfact_t(n: torch.Tensor) -> torch.Tensor:
+    """``lnfact`` on the device (f64; 1.0 at n = 0, as the reference's table code)."""
+    x = n.double()
+    v = x * torch.log(x) - x + 0.5 * torch.log(x) + 0.5 * torch.log(2 * math.pi * x)
+    return torch.where(x == 0, torch.ones_like(v), v)
+
+
+def _psm_device_cols(gi: GpuIndex, raw: dict) -> dict:
+    """The PSM table's columns on the device (reference engine.py:361-432, the features ``_psm_columns`` computes on
+    the host), from per-slot raw values: spec, rank, dnext, dbest, row (>= 0), k1, z, iso, pm, spec_scored,
+    spec_matched, tic and K2's outputs.  Same operations in the same precisions as the host code: f32 masses and
+    percentages, f64 Poisson term (its exp / log / pow may differ from the host's libm in the last bit)."""
+    rows = raw["row"]
+    mbk, myk = raw["matched_b"].long(), raw["matched_y"].long()
+    kk = mbk + myk
+    sc, mt = raw["spec_scored"].long(), raw["spec_matched"].long()
+    lam = mt.double() / sc.double()
+    pois = lam.pow(kk.double()) * torch.exp(-lam) / torch.exp(_lnfact_t(kk))
+    pois = torch.where(torch.isinf(pois), torch.full_like(pois, 1e-325), pois)
+    log_pois = torch.log10(pois)
+    z, iso, pm = raw["z"], raw["iso"], raw["pm"].float()
+    calc = gi.mass32[rows]
+    # Python scalars enter f32 kernels as f32 operands (NEUTRON and 2e6 are exact f32 values): f32 arithmetic
+    ie = iso.float() * float(NEUTRON)
+    dm = torch.abs(pm - calc - ie) * 2e6 / (pm - ie + calc)
+    plen = gi.length[rows].long()
+    sbs = raw["summed_b"] + raw["summed_y"]
+    return {
+        "spec_idx": raw["spec"].long(), "rank": raw["rank"].int(), "pf_row": rows.long(), "pf_id": gi.pf_id[rows],
+        "charge": z.to(torch.int8), "isotope_error": iso.to(torch.int8), "expmass": pm, "calcmass": calc,
+        "delta_mass_ppm": dm, "hyperscore": raw["hyperscore"].double(), "delta_next": raw["dnext"].double(),
+        "delta_best": raw["dbest"].double(), "matched_b": mbk.to(torch.int16), "matched_y": myk.to(torch.int16),
+        "matched_peaks": kk.to(torch.int16), "summed_intensity": sbs, "matched_intensity_pct": 100.0 * sbs / raw["tic"],
+        "average_ppm": raw["ppm"], "longest_b": raw["longest_b"], "longest_y": raw["longest_y"],
+        "longest_y_pct": (raw["longest_y"].double() / plen.double()).float(), "peptide_len": plen.to(torch.int16),
+        "missed_cleavages": gi.missed[rows], "n_var": gi.n_var[rows], "k1_count": raw["k1"].int(),
+        "scored_candidates": sc.int(), "poisson": log_pois}
+
+
+def _pack(cols: dict, valid: torch.Tensor):
+    """Device columns (plus the slot mask) in one byte buffer; returns (buffer, layout)."""
     parts, layout, off = [], [], 0
-    for name, _ in _PSM_COLS:
-        t = cols[name].contiguous()
+    for name, t in [("valid", valid.to(torch.uint8))] + list(cols.items()):
+        t = t.contiguous()
         b = t.view(torch.uint8)
         pad = (-b.numel()) % 8
         parts.append(b)
         if pad:
             parts.append(torch.zeros(pad, dtype=torch.uint8, device=b.device))
-        layout.append((name, np.dtype(str(t.dtype).replace("torch.", "")), off, t.numel()))
+        dt = np.dtype("uint64") if name == "pf_id" else np.dtype(str(t.dtype).replace("torch.", ""))
+        layout.append((name, dt, off, t.numel()))
         off += b.numel() + pad
     return torch.cat(parts), layout
+
+
+def _pack_psms(gi: GpuIndex, out: dict, report: int, n: int):
+    """Every PSM slot of a staged / pruned pass, its table columns computed on the device, packed into one byte
+    buffer without a host read (empty slots masked): the graph-captured pass ends with it and the host reads it
+    in one copy.  Returns (buffer, layout) with layout = [(name, numpy dtype, byte offset, count)]."""
+    psm_cand, psm_rank, dnext, dbest = out["psm"]
+    slots = n * report
+    cand = psm_cand[:slots]
+    ci = cand.clamp(min=0)
+    s = torch.arange(slots, device=cand.device) // max(report, 1)
+    dh, k2 = out["dh"], out["k2"]
+    # empty slots read candidate 0, which may be unset: clamp every index into its table
+    hh = out["c_hyp"][ci].clamp(0, dh["z"].numel() - 1)
+    raw = {"spec": s, "rank": psm_rank[:slots], "dnext": dnext[:slots], "dbest": dbest[:slots],
+           "row": out["c_row"][ci].clamp(0, max(gi.n - 1, 0)), "k1": out["c_cnt"][ci], "z": dh["z"][hh],
+           "iso": dh["iso"][hh],
+           "pm": dh["pm"][hh], "spec_scored": out["spec_scored"][s], "spec_matched": out["spec_matched"][s],
+           "tic": out["peaks"]["tic"][s]}
+    for k in ("hyperscore", "summed_b", "summed_y", "ppm", "matched_b", "matched_y", "longest_b", "longest_y"):
+        raw[k] = k2[k][ci]
+    return _pack(_psm_device_cols(gi, raw), cand >= 0)
+
+
+def _pack_fused(gi: GpuIndex, o: dict, report: int, n: int):
+    """The fused search's PSM slots, packed like ``_pack_psms``."""
+    psm, dh = o["psm"], o["dh"]
+    slots = n * report
+    ok = psm["row"][:slots] >= 0
+    s = torch.arange(slots, device=ok.device) // max(report, 1)
+    hh = psm["hyp"][:slots].long().clamp(0, dh["z"].numel() - 1)
+    raw = {"spec": s, "rank": psm["rank"][:slots], "dnext": psm["dnext"][:slots], "dbest": psm["dbest"][:slots],
+           "row": psm["row"][:slots].long().clamp(0, max(gi.n - 1, 0)), "k1": psm["k1"][:slots], "z": dh["z"][hh], "iso": dh["iso"][hh],
+           "pm": dh["pm"][hh], "spec_scored": o["spec_scored"][s], "spec_matched": o["spec_matched"][s],
+           "tic": o["peaks"]["tic"][s]}
+    for k, name, _ in _K2_KEYS:
+        raw[name] = psm[k][:slots]
+    return _pack(_psm_device_cols(gi, raw), ok)
 
 
 def _unpack_psms(host: np.ndarray, layout) -> dict:
     """Host records of the filled PSM slots from a packed buffer."""
     cols = {name: np.frombuffer(host, dtype=dt, count=cnt, offset=off) for name, dt, off, cnt in layout}
-    ok = cols["cand"] >= 0
-    rec = {k: v[ok] for k, v in cols.items() if k != "cand"}
-    return rec
+    ok = cols.pop("valid").astype(bool)
+    return {k: v[ok] for k, v in cols.items()}
+
+
+def _table(sp: Spectra, rec: dict) -> pa.Table:
+    """The PSM table from device-computed columns: run, scan and retention time added on the host."""
+    s = rec["spec_idx"]
+    cols = {"run": pa.repeat(pa.scalar(sp.run, pa.string()), len(s)), "spec_idx": s, "scan": sp.scan[s],
+            "rt": sp.rt[s]}
+    for k in _PSM_TABLE[1:]:
+        cols[k] = rec[k]
+    return pa.table(cols)
+
+
+def _read_packed(buf: torch.Tensor, layout, sp: Spectra, stats: Stats | None = None) -> pa.Table:
+    host = buf.cpu().numpy()
+    if stats is not None:
+        stats.d2h_bytes += host.nbytes
+    return _table(sp, _unpack_psms(host, layout))
 
 
 class GraphedPass:
@@ -949,7 +1029,7 @@ class _Slot:
 
         def fn():
             out = se.device_pass(self.run)
-            buf, layout = _pack_psms(out, report, self.n)
+            buf, layout = _pack_psms(se.gi, out, report, self.n)
             out["packed"] = buf
             self.layout = layout
             return out
@@ -1056,7 +1136,7 @@ class Searcher:
         slot.busy = False
         st = Stats()
         st.h2d_bytes, st.d2h_bytes = h2d, slot.host_out.numel()
-        return _psm_columns(sp, self.l1, rec, self.p), st
+        return _table(sp, rec), st
 
     def search(self, sp: Spectra):
         return self.result(self.submit(sp))

@@ -317,9 +317,7 @@ def search_pruned(sp: Spectra, gi: E.GpuIndex, l1, p: SearchParams, pruner: Prun
         run = E.DeviceRun(sp, gi.dev, st)
         out = _pruned_device(run, gi, p, pruner, report, st, timers)
         E.check_status(out["status"])
-        rec = E._gather_psms(*out["psm"], out["c_hyp"], out["c_row"], out["c_cnt"], out["k2"], out["dh"],
-                             out["spec_scored"], out["spec_matched"], out["peaks"]["tic"], report, st)
-    tbl = E._psm_columns(sp, l1, rec, p)
+        tbl = E._read_packed(*E._pack_psms(gi, out, report, run.n), sp, st)
     ru1 = resource.getrusage(resource.RUSAGE_SELF)
     st.wall_s["total"] = time.perf_counter() - t0
     st.counts.update(n_spectra=len(sp), n_searched=int(out["peaks"]["valid_d"].sum()),
