@@ -562,13 +562,15 @@ def _kernel_table(a, p, gi, run, flush, pr, dev):
         kern["cand_features_k"] = (ms_f, n_hit * 87)
         ms_m = timed(lambda: pr.logits(feat, n_hit))
         flops = 2 * n_hit * (16 * 256 + 256 * 256 + 256)
-        kern["mlp_infer_k"] = (ms_m, n_hit * 36 + 2 * (256 * 16 + 256 * 256) + 4 * 256 * 3)
+        mlp_name = "mlp_infer_tc_k" if pr.tensor_cores == "tcgen05" else "mlp_infer_k"
+        kern[mlp_name] = (ms_m, n_hit * 36 + 2 * (256 * 16 + 256 * 256) + 4 * 256 * 3)
         tpk, tkind = _tensor_peak()
         ach = flops / (ms_m / 1e3) / 1e12
-        mlp = {"bound": "tensor", "kernel": "mlp_infer_k", "achieved": round(ach, 1), "peak": tpk,
+        mlp = {"bound": "tensor", "kernel": mlp_name, "achieved": round(ach, 1), "peak": tpk,
                "unit": "TFLOP/s", "frac": round(ach / tpk, 4), "peak_source": tkind, "flops_per_launch": flops,
                "hits_per_launch": n_hit, "mean_launch_ms": round(ms_m, 4),
-               "instruction": "mma.sync m16n8k16 bf16 (fp32 accumulate)"}
+               "instruction": ("tcgen05.mma kind::f16 M128 N256 (bf16, fp32 accumulate in TMEM)"
+                               if pr.tensor_cores == "tcgen05" else "mma.sync m16n8k16 bf16 (fp32 accumulate)")}
     n_cand = int(so["cand_off"][-1])
     k2o = E._k2_outputs(max(n_cand, 1), dev)
     ms_k2 = timed(lambda: K.check(L.vk_k2_spectra(
