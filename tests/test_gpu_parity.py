@@ -470,3 +470,32 @@ def test_psm_table_features_on_device_equal_host(mini, param_sets, indexes, name
             np.testing.assert_allclose(a, b, rtol=1e-12)
         else:
             assert np.array_equal(a, b, equal_nan=a.dtype.kind == "f"), c
+
+
+def _slice_run(sp, a, b, name):
+    from vulcan.gpu.host import Spectra
+    o = sp.offsets[a:b + 1]
+    return Spectra(name, sp.scan[a:b], sp.index[a:b], sp.rt[a:b], sp.precursor_mz[a:b], sp.charge[a:b],
+                   sp.mz[o[0]:o[-1]], sp.intensity[o[0]:o[-1]], o - o[0])
+
+
+@pytest.mark.parametrize("name", SETS)
+def test_batched_search_equals_per_run_search(mini, param_sets, indexes, name, torch_cuda):
+    """Runs of different sizes packed into fixed-shape padded batches (one captured pass replayed per batch):
+    every run's table equals its own engine.search."""
+    import dataclasses
+    from vulcan.gpu import engine as E
+    l1, sp, _ = mini
+    p = dataclasses.replace(param_sets[name], search_method="staged")
+    gi = indexes[name]
+    cuts = [0, 7, 60, 61, 100, 160]
+    runs = [_slice_run(sp, a, b, f"run{i}") for i, (a, b) in enumerate(zip(cuts[:-1], cuts[1:]))]
+    runs.append(_slice_run(sp, 0, 0, "empty"))
+    runs.append(sp)
+    se = E.Searcher(gi, l1, p, report=2)
+    got = se.search_batch(runs, batch_spectra=64)
+    assert len(got) == len(runs)
+    for r, (tbl, _) in zip(runs, got):
+        want = E.search(r, gi, l1, p, report=2)[0]
+        assert tbl.equals(want), r.run
+    assert len(se.slots) == 1     # every batch replayed the same captured pass

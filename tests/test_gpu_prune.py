@@ -252,6 +252,26 @@ def test_graphed_pruned_search_equals_search_pruned(mini, param_sets, indexes, n
         assert tbl.equals(want)
 
 
+def test_batched_pruned_search_equals_per_run(mini, param_sets, indexes, torch_cuda):
+    """The pruned path in padded batches gives every run's own search_pruned table."""
+    from vulcan.gpu import engine as E
+    from vulcan.gpu import prune as PR
+    from vulcan.gpu.host import Spectra
+    l1, sp, _ = mini
+    p = param_sets["ppm"]
+    gi = indexes["ppm"]
+    pr = _random_pruner(torch_cuda, gi.dev, 9)
+    pr.tau, pr.min_keep, pr.max_keep, pr.min_count = 0.0, 1, 16, 2
+    runs = []
+    for i, (a, b) in enumerate(((0, 50), (50, 51), (51, 160))):
+        o = sp.offsets[a:b + 1]
+        runs.append(Spectra(f"r{i}", sp.scan[a:b], sp.index[a:b], sp.rt[a:b], sp.precursor_mz[a:b], sp.charge[a:b],
+                            sp.mz[o[0]:o[-1]], sp.intensity[o[0]:o[-1]], o - o[0]))
+    se = E.Searcher(gi, l1, p, pruner=pr, report=1)
+    for r, (tbl, _) in zip(runs, se.search_batch(runs, batch_spectra=60)):
+        assert tbl.equals(PR.search_pruned(r, gi, l1, p, pr, report=1)[0]), r.run
+
+
 # ------------------------------------------------------------------------------------------- trained pruner
 @pytest.fixture(scope="module")
 def small(tmp_path_factory, torch_cuda):

@@ -308,6 +308,8 @@ def _hyp_device(run: DeviceRun, peaks, gi: GpuIndex, p: SearchParams):
     i0, i1 = p.isotope_errors
     n_iso = i1 - i0 + 1
     n_max = int(np.where(run.charge_np > 0, 1, z1 - z0 + 1).sum()) * n_iso
+    # a run in a captured slot carries the slot's hypothesis capacity (>= what any run of that shape needs)
+    n_max = max(n_max, int(getattr(run, "n_hyp_cap", 0) or 0))
     cnt = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
     K.check(L.vk_hyp_count(n, K.ptr(peaks["valid_d"]), K.ptr(run.precursor_mz), K.ptr(run.charge), z0, z1, i0, i1,
                            K.ptr(cnt), K.stream()), "hyp_count")
@@ -1017,7 +1019,7 @@ def _is_pinned(a: np.ndarray) -> bool:
 class _Slot:
     """Device buffers of one run shape, the captured pass over them, pinned staging and the packed result."""
 
-    def __init__(self, sp: Spectra, searcher: "Searcher", cap_raw: int, max_raw: int):
+    def __init__(self, sp: Spectra, searcher: "Searcher", cap_raw: int, max_raw: int, n_hyp_cap: int):
         se = searcher
         dev = se.gi.dev
         self.n = len(sp)
@@ -1025,6 +1027,7 @@ class _Slot:
         self.run = DeviceRun(pad, dev, pinned=False)
         self.run.max_raw = max_raw
         self.run.n_raw = cap_raw
+        self.run.n_hyp_cap = n_hyp_cap
         report = se.report
 
         def fn():
@@ -1076,22 +1079,28 @@ class Searcher:
         from . import prune
         return prune._pruned_device(run, self.gi, self.p, self.pruner, self.report, Stats())
 
+    def _n_hyp(self, sp: Spectra) -> int:
+        z0, z1 = self.p.precursor_charge
+        i0, i1 = self.p.isotope_errors
+        return int(np.where(np.asarray(sp.charge) > 0, 1, z1 - z0 + 1).sum()) * (i1 - i0 + 1)
+
     def _key(self, sp: Spectra):
         n_raw = int(np.asarray(sp.offsets)[-1]) if len(sp.offsets) else 0
         lens = np.diff(np.asarray(sp.offsets, np.int64))
         mr = int(lens.max()) if len(lens) else 0
         cap = 1 << max(10, int(n_raw - 1).bit_length())
         mr2 = 1 << max(5, int(mr - 1).bit_length())
-        z0, z1 = self.p.precursor_charge
-        i0, i1 = self.p.isotope_errors
-        n_max = int(np.where(np.asarray(sp.charge) > 0, 1, z1 - z0 + 1).sum()) * (i1 - i0 + 1)
+        n_max = self._n_hyp(sp)
+        if getattr(self, "_force", None):
+            cap, mr2 = max(cap, self._force[0]), max(mr2, self._force[1])
+            n_max = max(n_max, self._force[2])
         return (len(sp), cap, mr2, n_max)
 
     def submit(self, sp: Spectra):
         key = self._key(sp)
         with torch.cuda.device(self.gi.dev):
             if key not in self.slots:
-                self.slots[key] = [_Slot(sp, self, key[1], key[2]) for _ in range(2)]
+                self.slots[key] = [_Slot(sp, self, key[1], key[2], key[3]) for _ in range(2)]
                 self._turn[key] = 0
             slot = self.slots[key][self._turn[key]]
             self._turn[key] ^= 1
@@ -1127,7 +1136,7 @@ class Searcher:
                 slot.done.record(self.compute_stream)
             return (sp, slot, h2d)
 
-    def result(self, handle):
+    def _records(self, handle):
         sp, slot, h2d = handle
         slot.done.synchronize()
         check_status(slot.gp.out["status"])
@@ -1136,10 +1145,42 @@ class Searcher:
         slot.busy = False
         st = Stats()
         st.h2d_bytes, st.d2h_bytes = h2d, slot.host_out.numel()
-        return _table(sp, rec), st
+        return rec, st
+
+    def result(self, handle):
+        rec, st = self._records(handle)
+        return _table(handle[0], rec), st
 
     def search(self, sp: Spectra):
         return self.result(self.submit(sp))
+
+    def search_batch(self, runs, batch_spectra: int = 131072):
+        """PSM tables of many runs searched in batches: whole runs packed into batches of one fixed shape (padded
+        with empty spectra to the largest batch, peak capacity of the largest batch), so that every batch replays
+        the same captured pass; batch i+1 is copied while batch i runs.  Each run's table equals its own search."""
+        groups = plan_batches(runs, batch_spectra)
+        n_b = max(sum(len(runs[i]) for i in g) for g in groups) if groups else 0
+        cats = [concat_runs([runs[i] for i in g], n_b) for g in groups]
+        raw = max((int(c.offsets[-1]) for c, _ in cats), default=0)
+        mr = max((int(np.diff(np.asarray(c.offsets)).max()) if len(c) else 0 for c, _ in cats), default=0)
+        self._force = (1 << max(10, int(raw - 1).bit_length()), 1 << max(5, int(mr - 1).bit_length()),
+                       max((self._n_hyp(c) for c, _ in cats), default=0))
+        try:
+            tables, pending = [], None
+            for (c, starts), g in zip(cats, groups):
+                h = self.submit(c)
+                if pending is not None:
+                    tables += self._split(*pending)
+                pending = (h, [runs[i] for i in g], starts)
+            if pending is not None:
+                tables += self._split(*pending)
+        finally:
+            self._force = None
+        return tables
+
+    def _split(self, handle, runs, starts):
+        rec, st = self._records(handle)
+        return [(t, st) for t in split_table(rec, runs, starts)]
 
     def search_many(self, runs):
         """PSM tables of many runs, one run queued ahead of the table being built."""
@@ -1152,6 +1193,60 @@ class Searcher:
         if pending is not None:
             out.append(self.result(pending))
         return out
+
+
+def concat_runs(runs, n_total: int | None = None) -> tuple[Spectra, list[int]]:
+    """Runs as one Spectra (spectrum order kept, run after run), padded with empty spectra (no peaks, charge 1,
+    which search to nothing) up to n_total; returns it and the first spectrum of each run (+ the end)."""
+    starts = [0]
+    for sp in runs:
+        starts.append(starts[-1] + len(sp))
+    n = starts[-1] if n_total is None else int(n_total)
+    pad = n - starts[-1]
+    if pad < 0:
+        raise ValueError("n_total is smaller than the runs' spectra")
+    offs = [np.zeros(1, np.int64)]
+    base = 0
+    for sp in runs:
+        o = np.asarray(sp.offsets, np.int64)
+        offs.append(o[1:] + base)
+        base += int(o[-1])
+    offs.append(np.full(pad, base, np.int64))
+    cat = lambda k, dt, fill: np.concatenate([np.asarray(getattr(sp, k), dt) for sp in runs] +  # noqa: E731
+                                             [np.full(pad, fill, dt)])
+    out = Spectra("batch", cat("scan", np.uint32, 0), cat("index", np.uint32, 0), cat("rt", np.float64, 0.0),
+                  cat("precursor_mz", np.float64, 0.0), cat("charge", np.int8, 1),
+                  np.concatenate([np.asarray(sp.mz, np.float32) for sp in runs] + [np.zeros(0, np.float32)]),
+                  np.concatenate([np.asarray(sp.intensity, np.float32) for sp in runs] + [np.zeros(0, np.float32)]),
+                  np.concatenate(offs))
+    return out, starts
+
+
+def split_table(rec: dict, runs, starts) -> list:
+    """Per-run PSM tables from the records of a batch (spectrum indices back to each run's own)."""
+    s = rec["spec_idx"]
+    out = []
+    for r, sp in enumerate(runs):
+        lo, hi = np.searchsorted(s, [starts[r], starts[r + 1]])
+        sub = {k: v[lo:hi] for k, v in rec.items()}
+        sub["spec_idx"] = sub["spec_idx"] - starts[r]
+        out.append(_table(sp, sub))
+    return out
+
+
+def plan_batches(runs, batch_spectra: int):
+    """Greedy packing of whole runs, in order, into batches of at most batch_spectra spectra (a longer run is a
+    batch of its own); returns lists of run indices."""
+    batches, cur, size = [], [], 0
+    for i, sp in enumerate(runs):
+        if cur and size + len(sp) > batch_spectra:
+            batches.append(cur)
+            cur, size = [], 0
+        cur.append(i)
+        size += len(sp)
+    if cur:
+        batches.append(cur)
+    return batches
 
 
 def pin_spectra(sp: Spectra) -> Spectra:
