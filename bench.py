@@ -588,6 +588,89 @@ def _kernel_table(a, p, gi, run, flush, pr, dev):
     return kern, mlp
 
 
+def run_batch(a):
+    """Configuration 2: 64 runs of 5,000-60,000 spectra (log-uniform), drawn from a pool of simulated spectra,
+    searched in fixed-shape batches, each batch one replay of a captured CUDA graph; tile rows and K1 warps chosen
+    by the autotuner on a sample; learned-pruned and plain paths, each run's table checked against its own search."""
+    import torch
+    from vulcan import synth
+    from vulcan.gpu import autotune as AT
+    from vulcan.gpu import engine as E
+    from vulcan.gpu import prune as PR
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    w, l1, lab, _, t_build = _workload_setup("human", rank)
+    p0 = _params(w, a)
+    pool = synth.simulate_run(l1, lab, w, n_spectra=120000, seed=90000 + rank, run="pool")[0]
+    runs = synth.batch_runs(pool, 64, 5000, 60000, seed=2 + rank)
+    n_total = sum(len(r) for r in runs)
+    gi0 = E.GpuIndex(l1, p0, STATIC, VAR, device=dev)
+    pr, pr_info = _pruner_setup(a, w, l1, lab, gi0, p0, rank)
+    del gi0
+    torch.cuda.empty_cache()
+    sample = synth.take_spectra(pool, np.arange(40000), "sample")
+    p, tune_report = AT.tune(l1, p0, STATIC, VAR, sample, pruner=pr, device=dev)
+    gi = E.GpuIndex(l1, p, STATIC, VAR, device=dev)
+    pinned = [E.pin_spectra(r) for r in runs]
+    reps = max(2, a.steps // 10)
+    res = {}
+    clocks = ClockSampler(local)
+    for name, prn in (("pruned", pr), ("plain", None)):
+        se = E.Searcher(gi, l1, p, pruner=prn, report=1)
+        tables = se.search_batch(pinned, batch_spectra=a.batch_spectra)     # captures the batch shape
+        torch.cuda.synchronize()
+        se.device_ms = 0.0
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            tables = se.search_batch(pinned, batch_spectra=a.batch_spectra)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        res[name] = {"tables": [t for t, _ in tables], "device_ms": se.device_ms / reps, "wall_s": wall / reps,
+                     "batches": len(E.plan_batches(runs, a.batch_spectra)), "h2d": sum(s.h2d_bytes for _, s in tables),
+                     "d2h": sum(s.d2h_bytes for _, s in tables)}
+        del se
+        torch.cuda.empty_cache()
+    clk = clocks.stop()
+    # each run's batched table equals its own search (first two runs)
+    for i in range(2):
+        assert res["plain"]["tables"][i].equals(E.search(runs[i], gi, l1, p)[0]), "batched plain table differs"
+        assert res["pruned"]["tables"][i].equals(PR.search_pruned(runs[i], gi, l1, p, pr)[0]), \
+            "batched pruned table differs"
+    rec = sum(PR.top1_recall(a_, b_) * a_.num_rows for a_, b_ in zip(res["plain"]["tables"], res["pruned"]["tables"]))
+    rec /= max(1, sum(t.num_rows for t in res["plain"]["tables"]))
+    acc_plain = sum(PR.accepted_psms(t, lab) for t in res["plain"]["tables"])
+    acc_pr = sum(PR.accepted_psms(t, lab) for t in res["pruned"]["tables"])
+    pr_ms, pl_ms = res["pruned"]["device_ms"], res["plain"]["device_ms"]
+    if rank == 0:
+        line = {
+            "metric": METRIC + " (configuration 2: 64 runs, batched, graph-captured)", "value":
+                round(n_total * world / (pr_ms / 1e3), 1), "unit": "spectra/s", "n_gpus": world, "steps": reps,
+            "warmup": 1, "ms_per_step": round(pr_ms, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (MLP: bf16 weights, fp32 accumulate)", "data": "synthetic",
+            "config": {"workload": f"64 runs of 5,000-60,000 spectra (log-uniform; {n_total} spectra) drawn from "
+                                   "120,000 simulated spectra, human-scale index",
+                       "batch_spectra": a.batch_spectra, "batches": res["pruned"]["batches"],
+                       "step": "all 64 runs once", "tile_rows": p.tile_rows, "k1_warps": p.k1_warps,
+                       "l2": "not flushed (batches of up to 131,072 spectra, working sets above L2)",
+                       "pruner": pr_info},
+            "e2e": {"value": round(n_total * world / res["pruned"]["wall_s"], 1), "unit": "spectra/s",
+                    "h2d_bytes_per_step": int(res["pruned"]["h2d"]), "d2h_bytes_per_step": int(res["pruned"]["d2h"])},
+            "vs_plain": {"plain_value": round(n_total * world / (pl_ms / 1e3), 1), "plain_ms_per_step": round(pl_ms, 3),
+                         "plain_e2e": round(n_total * world / res["plain"]["wall_s"], 1),
+                         "speedup_device": round(pl_ms / pr_ms, 3),
+                         "speedup_e2e": round(res["plain"]["wall_s"] / res["pruned"]["wall_s"], 3),
+                         "top1_recall": round(rec, 6), "accepted_at_1pct_q_plain": acc_plain,
+                         "accepted_at_1pct_q_pruned": acc_pr,
+                         "delta_accepted": round((acc_pr - acc_plain) / max(acc_plain, 1), 6),
+                         "tables_checked_against_per_run_search": 2},
+            "autotune": tune_report, "clocks": clk, "index_build_s": round(t_build, 1),
+        }
+        print(json.dumps(line), flush=True)
+
+
 def _traffic_from_profiles(kernel: str):
     """DRAM bytes per launch of `kernel` recorded from an ncu capture in profiles/<kernel>_*.md (a line
     'dram_bytes_per_launch: N'), or None."""
@@ -634,7 +717,7 @@ def run_reference(a):
     if rank != 0:
         return
     from oracle import oracle as O
-    w, l1, _, sp, _ = _workload_setup(a.workload, 0)
+    w, l1, _, sp, _ = _workload_setup("human" if a.workload == "batch64" else a.workload, 0)
     p = w.search_params()
     _ARR[id(l1)] = {k: np.ascontiguousarray(getattr(l1, k)) for k in ("seq_off", "length", "mask", "mass32",
                                                                          "residues")}
@@ -669,7 +752,9 @@ def main():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
-    ap.add_argument("--workload", choices=("human", "small"), default="human")
+    ap.add_argument("--workload", choices=("human", "small", "batch64"), default="human",
+                    help="batch64: configuration 2 (64 runs, batched graph-captured search, autotuned layout)")
+    ap.add_argument("--batch-spectra", type=int, default=131072, help="spectra per batch (batch64)")
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of CPU-baseline work (rank 0, N=1)")
     ap.add_argument("--cpu-total", type=float, default=120.0, help="seconds of the reference arm in total")
     ap.add_argument("--method", choices=("staged", "fused"), default="staged",
@@ -694,6 +779,8 @@ def main():
         ap.error("--warmup must be >= 3")
     if a.impl == "reference":
         run_reference(a)
+    elif a.workload == "batch64":
+        run_batch(a)
     elif a.mode == "profile":
         run_profile(a)
     else:

@@ -499,3 +499,24 @@ def test_batched_search_equals_per_run_search(mini, param_sets, indexes, name, t
         want = E.search(r, gi, l1, p, report=2)[0]
         assert tbl.equals(want), r.run
     assert len(se.slots) == 1     # every batch replayed the same captured pass
+
+
+def test_autotuner_picks_a_measured_layout(mini, param_sets, tmp_path, torch_cuda):
+    """The autotuner times every candidate layout on the sample, returns the fastest, reports peak-count buckets,
+    and reuses its cached choice."""
+    from vulcan.gpu import autotune as AT
+    from vulcan.gpu import engine as E
+    l1, sp, _ = mini
+    p = param_sets["da"]
+    cache = str(tmp_path / "tune.json")
+    q, rep = AT.tune(l1, p, STATIC, VAR, sp, reps=2, tile_rows=(64, 128), k1_warps=(4, 8), cache=cache)
+    ok = [c for c in rep["candidates"] if "ms" in c]
+    assert len(ok) == 4 and not rep["cached"]
+    best = min(ok, key=lambda c: c["ms"])
+    assert (q.tile_rows, q.k1_warps) == (best["tile_rows"], best["k1_warps"])
+    assert sum(b["spectra"] for b in rep["peak_buckets"]) == sum(np.diff(sp.offsets) > 0)
+    q2, rep2 = AT.tune(l1, p, STATIC, VAR, sp, cache=cache)
+    assert rep2["cached"] and (q2.tile_rows, q2.k1_warps) == (q.tile_rows, q.k1_warps)
+    # the chosen layout searches like any other
+    gi = E.GpuIndex(l1, q, STATIC, VAR)
+    assert E.search(sp, gi, l1, q)[0].num_rows > 0

@@ -1017,14 +1017,17 @@ def _is_pinned(a: np.ndarray) -> bool:
 
 
 class _Slot:
-    """Device buffers of one run shape, the captured pass over them, pinned staging and the packed result."""
+    """Device buffers of one run shape (n spectra, cap_raw peaks), the pass captured over them, pinned staging for
+    inputs that are not pinned, and the packed result in pinned host memory."""
 
-    def __init__(self, sp: Spectra, searcher: "Searcher", cap_raw: int, max_raw: int, n_hyp_cap: int):
+    def __init__(self, searcher: "Searcher", n: int, cap_raw: int, max_raw: int, n_hyp_cap: int):
         se = searcher
         dev = se.gi.dev
-        self.n = len(sp)
-        pad = _pad_run(sp, cap_raw, max_raw)
-        self.run = DeviceRun(pad, dev, pinned=False)
+        self.n, self.cap_raw = n, cap_raw
+        empty = Spectra("slot", np.zeros(n, np.uint32), np.zeros(n, np.uint32), np.zeros(n), np.zeros(n),
+                        np.ones(n, np.int8), np.zeros(cap_raw, np.float32), np.zeros(cap_raw, np.float32),
+                        np.zeros(n + 1, np.int64))
+        self.run = DeviceRun(empty, dev, pinned=False)
         self.run.max_raw = max_raw
         self.run.n_raw = cap_raw
         self.run.n_hyp_cap = n_hyp_cap
@@ -1038,20 +1041,19 @@ class _Slot:
             return out
         self.gp = GraphedPass(fn, dev)
         self.host_out = torch.empty(self.gp.out["packed"].numel(), dtype=torch.uint8, pin_memory=True)
+        self.offsets = torch.empty(n + 1, dtype=torch.int64, pin_memory=True)   # offsets staging
         self.stage = {}
         self.h2d_done = torch.cuda.Event()
         self.done = torch.cuda.Event()
         self.busy = False
 
-
-def _pad_run(sp: Spectra, cap_raw: int, max_raw: int) -> Spectra:
-    """A copy of the run whose peak arrays have cap_raw entries (the tail unused) for sizing slot buffers."""
-    mz = np.zeros(cap_raw, np.float32)
-    it = np.zeros(cap_raw, np.float32)
-    n_raw = int(sp.offsets[-1])
-    mz[:n_raw] = sp.mz
-    it[:n_raw] = sp.intensity
-    return Spectra(sp.run, sp.scan, sp.index, sp.rt, sp.precursor_mz, sp.charge, mz, it, np.asarray(sp.offsets))
+    def staged(self, key, a: np.ndarray) -> np.ndarray:
+        """A pinned copy of a (reusing this slot's staging buffer for key)."""
+        st = self.stage.get(key)
+        if st is None or len(st) < len(a) or st.dtype != a.dtype:
+            st = self.stage[key] = _pinned_like(np.empty(max(len(a), 1), a.dtype))
+        np.copyto(st[:len(a)], a)
+        return st[:len(a)]
 
 
 class Searcher:
@@ -1069,6 +1071,7 @@ class Searcher:
         self.gi, self.l1, self.p, self.pruner = gi, l1, p, pruner
         self.report = p.report_psms if report is None else report
         self.slots = {}
+        self.device_ms = 0.0          # summed CUDA-event time of the replayed passes (inputs already copied)
         self.copy_stream = torch.cuda.Stream(gi.dev)
         self.compute_stream = torch.cuda.Stream(gi.dev)
         self._turn = {}
@@ -1084,23 +1087,30 @@ class Searcher:
         i0, i1 = self.p.isotope_errors
         return int(np.where(np.asarray(sp.charge) > 0, 1, z1 - z0 + 1).sum()) * (i1 - i0 + 1)
 
-    def _key(self, sp: Spectra):
-        n_raw = int(np.asarray(sp.offsets)[-1]) if len(sp.offsets) else 0
-        lens = np.diff(np.asarray(sp.offsets, np.int64))
-        mr = int(lens.max()) if len(lens) else 0
+    def _shape(self, parts, n_total: int):
+        """(spectra, peak capacity, largest peak count, hypothesis capacity) of consecutive runs padded to n_total
+        spectra (padding: empty spectra of known charge)."""
+        n_raw = sum(int(np.asarray(sp.offsets)[-1]) for sp in parts)
+        mr = max((int(np.diff(np.asarray(sp.offsets, np.int64)).max()) for sp in parts if len(sp)), default=0)
+        z0, z1 = self.p.precursor_charge
+        i0, i1 = self.p.isotope_errors
+        n_max = sum(self._n_hyp(sp) for sp in parts) + (n_total - sum(len(sp) for sp in parts)) * (i1 - i0 + 1)
         cap = 1 << max(10, int(n_raw - 1).bit_length())
         mr2 = 1 << max(5, int(mr - 1).bit_length())
-        n_max = self._n_hyp(sp)
         if getattr(self, "_force", None):
             cap, mr2 = max(cap, self._force[0]), max(mr2, self._force[1])
             n_max = max(n_max, self._force[2])
-        return (len(sp), cap, mr2, n_max)
+        return (n_total, cap, mr2, n_max)
 
     def submit(self, sp: Spectra):
-        key = self._key(sp)
+        """Queue one run; returns a handle for ``result``."""
+        return self._submit([sp], len(sp))
+
+    def _submit(self, parts, n_total: int):
+        key = self._shape(parts, n_total)
         with torch.cuda.device(self.gi.dev):
             if key not in self.slots:
-                self.slots[key] = [_Slot(sp, self, key[1], key[2], key[3]) for _ in range(2)]
+                self.slots[key] = [_Slot(self, *key) for _ in range(2)]
                 self._turn[key] = 0
             slot = self.slots[key][self._turn[key]]
             self._turn[key] ^= 1
@@ -1108,37 +1118,57 @@ class Searcher:
                 raise RuntimeError("result() of the previous run in this slot was not collected")
             slot.busy = True
             run = slot.run
-            n_raw = int(sp.offsets[-1])
-            pairs = ((run.mz, sp.mz, n_raw), (run.intensity, sp.intensity, n_raw),
-                     (run.offsets, sp.offsets, len(sp) + 1), (run.precursor_mz, sp.precursor_mz, len(sp)),
-                     (run.charge, sp.charge, len(sp)))
+            # offsets of the concatenated runs (host, into pinned staging), the padding spectra empty
+            offs = slot.offsets.numpy()
+            base_pk = base_sp = 0
+            offs[0] = 0
+            for sp in parts:
+                o = np.asarray(sp.offsets, np.int64)
+                offs[base_sp + 1:base_sp + len(sp) + 1] = o[1:] + base_pk
+                base_pk += int(o[-1])
+                base_sp += len(sp)
+            offs[base_sp + 1:] = base_pk
             # the previous pass over this slot must be done before its inputs are overwritten
             self.copy_stream.wait_event(slot.done)
             h2d = 0
             with torch.cuda.stream(self.copy_stream):
-                for i, (dst, a, cnt) in enumerate(pairs):
-                    a = np.ascontiguousarray(a)[:cnt]
-                    if a.dtype != torch.empty(0, dtype=dst.dtype).numpy().dtype:
-                        a = a.astype(torch.empty(0, dtype=dst.dtype).numpy().dtype)
-                    if not _is_pinned(a):
-                        st = slot.stage.get(i)
-                        if st is None or len(st) < cnt:
-                            st = slot.stage[i] = _pinned_like(np.empty(max(cnt, 1), a.dtype))
-                        np.copyto(st[:cnt], a)
-                        a = st[:cnt]
-                    dst[:cnt].copy_(torch.from_numpy(a), non_blocking=True)
-                    h2d += a.nbytes
+                run.offsets.copy_(slot.offsets, non_blocking=True)
+                h2d += slot.offsets.numel() * 8
+                bp = bs = 0
+                for j, sp in enumerate(parts):
+                    nr = int(np.asarray(sp.offsets)[-1])
+                    ns = len(sp)
+                    for name, dst, a, lo, cnt in (("mz", run.mz, sp.mz, bp, nr), ("int", run.intensity, sp.intensity, bp, nr),
+                                                  ("pmz", run.precursor_mz, sp.precursor_mz, bs, ns),
+                                                  ("z", run.charge, sp.charge, bs, ns)):
+                        if cnt == 0:
+                            continue
+                        dt = torch.empty(0, dtype=dst.dtype).numpy().dtype
+                        a = np.asarray(a)[:cnt]
+                        if a.dtype != dt or not a.flags.c_contiguous or not _is_pinned(a):
+                            a = slot.staged((name, j), np.ascontiguousarray(a, dtype=dt))
+                        dst[lo:lo + cnt].copy_(torch.from_numpy(a), non_blocking=True)
+                        h2d += a.nbytes
+                    bp += nr
+                    bs += ns
+                if bs < n_total:
+                    run.precursor_mz[bs:n_total].fill_(0.0)
+                    run.charge[bs:n_total].fill_(1)
             slot.h2d_done.record(self.copy_stream)
             self.compute_stream.wait_event(slot.h2d_done)
+            ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
             with torch.cuda.stream(self.compute_stream):
+                ev[0].record(self.compute_stream)
                 out = slot.gp.replay()
+                ev[1].record(self.compute_stream)
                 slot.host_out.copy_(out["packed"], non_blocking=True)
                 slot.done.record(self.compute_stream)
-            return (sp, slot, h2d)
+            return (parts[0] if len(parts) == 1 else None, slot, h2d, ev)
 
     def _records(self, handle):
-        sp, slot, h2d = handle
+        sp, slot, h2d, ev = handle
         slot.done.synchronize()
+        self.device_ms += ev[0].elapsed_time(ev[1])
         check_status(slot.gp.out["status"])
         rec = _unpack_psms(slot.host_out.numpy(), slot.layout)
         rec = {k: v.copy() for k, v in rec.items()}
@@ -1157,21 +1187,27 @@ class Searcher:
     def search_batch(self, runs, batch_spectra: int = 131072):
         """PSM tables of many runs searched in batches: whole runs packed into batches of one fixed shape (padded
         with empty spectra to the largest batch, peak capacity of the largest batch), so that every batch replays
-        the same captured pass; batch i+1 is copied while batch i runs.  Each run's table equals its own search."""
+        the same captured pass; each run's arrays are copied straight into the batch's device buffers, and batch
+        i+1 is copied while batch i runs.  Each run's table equals its own search.  Returns [(table, stats)], the
+        stats (bytes moved) per batch on the batch's first run."""
         groups = plan_batches(runs, batch_spectra)
         n_b = max(sum(len(runs[i]) for i in g) for g in groups) if groups else 0
-        cats = [concat_runs([runs[i] for i in g], n_b) for g in groups]
-        raw = max((int(c.offsets[-1]) for c, _ in cats), default=0)
-        mr = max((int(np.diff(np.asarray(c.offsets)).max()) if len(c) else 0 for c, _ in cats), default=0)
-        self._force = (1 << max(10, int(raw - 1).bit_length()), 1 << max(5, int(mr - 1).bit_length()),
-                       max((self._n_hyp(c) for c, _ in cats), default=0))
+        raw = max((sum(int(np.asarray(runs[i].offsets)[-1]) for i in g) for g in groups), default=0)
+        mr = max((int(np.diff(np.asarray(r.offsets, np.int64)).max()) for r in runs if len(r)), default=0)
+        z0, z1 = self.p.precursor_charge
+        i0, i1 = self.p.isotope_errors
+        n_hyp = max((sum(self._n_hyp(runs[i]) for i in g) + (n_b - sum(len(runs[i]) for i in g)) * (i1 - i0 + 1)
+                     for g in groups), default=0)
+        self._force = (1 << max(10, int(raw - 1).bit_length()), 1 << max(5, int(mr - 1).bit_length()), n_hyp)
         try:
             tables, pending = [], None
-            for (c, starts), g in zip(cats, groups):
-                h = self.submit(c)
+            for g in groups:
+                parts = [runs[i] for i in g]
+                starts = np.concatenate([[0], np.cumsum([len(r) for r in parts])]).tolist()
+                h = self._submit(parts, n_b)
                 if pending is not None:
                     tables += self._split(*pending)
-                pending = (h, [runs[i] for i in g], starts)
+                pending = (h, parts, starts)
             if pending is not None:
                 tables += self._split(*pending)
         finally:
@@ -1180,7 +1216,8 @@ class Searcher:
 
     def _split(self, handle, runs, starts):
         rec, st = self._records(handle)
-        return [(t, st) for t in split_table(rec, runs, starts)]
+        empty = Stats()
+        return [(t, st if i == 0 else empty) for i, t in enumerate(split_table(rec, runs, starts))]
 
     def search_many(self, runs):
         """PSM tables of many runs, one run queued ahead of the table being built."""
@@ -1193,33 +1230,6 @@ class Searcher:
         if pending is not None:
             out.append(self.result(pending))
         return out
-
-
-def concat_runs(runs, n_total: int | None = None) -> tuple[Spectra, list[int]]:
-    """Runs as one Spectra (spectrum order kept, run after run), padded with empty spectra (no peaks, charge 1,
-    which search to nothing) up to n_total; returns it and the first spectrum of each run (+ the end)."""
-    starts = [0]
-    for sp in runs:
-        starts.append(starts[-1] + len(sp))
-    n = starts[-1] if n_total is None else int(n_total)
-    pad = n - starts[-1]
-    if pad < 0:
-        raise ValueError("n_total is smaller than the runs' spectra")
-    offs = [np.zeros(1, np.int64)]
-    base = 0
-    for sp in runs:
-        o = np.asarray(sp.offsets, np.int64)
-        offs.append(o[1:] + base)
-        base += int(o[-1])
-    offs.append(np.full(pad, base, np.int64))
-    cat = lambda k, dt, fill: np.concatenate([np.asarray(getattr(sp, k), dt) for sp in runs] +  # noqa: E731
-                                             [np.full(pad, fill, dt)])
-    out = Spectra("batch", cat("scan", np.uint32, 0), cat("index", np.uint32, 0), cat("rt", np.float64, 0.0),
-                  cat("precursor_mz", np.float64, 0.0), cat("charge", np.int8, 1),
-                  np.concatenate([np.asarray(sp.mz, np.float32) for sp in runs] + [np.zeros(0, np.float32)]),
-                  np.concatenate([np.asarray(sp.intensity, np.float32) for sp in runs] + [np.zeros(0, np.float32)]),
-                  np.concatenate(offs))
-    return out, starts
 
 
 def split_table(rec: dict, runs, starts) -> list:

@@ -175,3 +175,24 @@ def simulate_run(l1, labels, w: Workload | str, n_spectra: int | None = None, se
                  np.linspace(0.0, 120.0, n), pmz, ch, np.concatenate(mz_l) if n else np.zeros(0, np.float32),
                  np.concatenate(it_l) if n else np.zeros(0, np.float32), off)
     return sp, rows
+
+
+def take_spectra(sp: Spectra, sel: np.ndarray, run: str) -> Spectra:
+    """The spectra sel (indices, repeats allowed, in that order) of a run, as a new run."""
+    sel = np.asarray(sel, np.int64)
+    off = np.asarray(sp.offsets, np.int64)
+    lens = off[1:][sel] - off[:-1][sel]
+    new_off = np.zeros(len(sel) + 1, np.int64)
+    np.cumsum(lens, out=new_off[1:])
+    idx = np.repeat(off[:-1][sel] - new_off[:-1], lens) + np.arange(int(new_off[-1]))
+    return Spectra(run, np.arange(len(sel), dtype=np.uint32), np.arange(len(sel), dtype=np.uint32),
+                   np.asarray(sp.rt)[sel], np.asarray(sp.precursor_mz)[sel], np.asarray(sp.charge)[sel],
+                   np.asarray(sp.mz)[idx], np.asarray(sp.intensity)[idx], new_off)
+
+
+def batch_runs(pool: Spectra, n_runs: int = 64, lo: int = 5000, hi: int = 60000, seed: int = 2):
+    """Runs for the batched benchmark: sizes log-uniform in [lo, hi], spectra drawn (with replacement, seeded)
+    from a pool of simulated spectra."""
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(lo), np.log(hi), n_runs)).astype(np.int64)
+    return [take_spectra(pool, rng.integers(0, len(pool), int(n)), f"batch_run{i}") for i, n in enumerate(sizes)]
