@@ -277,10 +277,8 @@ def _timed_passes(step, flush, steps, world, dist, K):
     if world > 1:
         dist.barrier()
     ms = sum(e0.elapsed_time(e1) for e0, e1 in evs)
-    t = torch.tensor([ms], dtype=torch.float64, device=flush.device)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item()), launches, out
+    from vulcan.gpu.replicas import max_over_ranks
+    return max_over_ranks(ms, flush.device), launches, out
 
 
 def _timed_e2e(call, n_spec, steps, world, dist, dev):
@@ -295,10 +293,8 @@ def _timed_e2e(call, n_spec, steps, world, dist, dev):
     for _ in range(steps):
         st = call()[1]
     torch.cuda.synchronize()
-    e2e_s = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(e2e_s, op=dist.ReduceOp.MAX)
-    return n_spec * world * steps / float(e2e_s.item()), st
+    from vulcan.gpu.replicas import max_over_ranks
+    return n_spec * world * steps / max_over_ranks(time.perf_counter() - t0, dev), st
 
 
 def run_b200(a):
@@ -382,10 +378,8 @@ def run_b200(a):
         t0 = time.perf_counter()
         res = se.search_many([pinned] * e2e_steps)
         torch.cuda.synchronize()
-        t = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return len(sp) * world * e2e_steps / float(t.item()), res[-1][1]
+        from vulcan.gpu.replicas import max_over_ranks
+        return len(sp) * world * e2e_steps / max_over_ranks(time.perf_counter() - t0, dev), res[-1][1]
     e2e, s2 = e2e_rate(pr)
     h2d, d2h = s2.h2d_bytes, s2.d2h_bytes
     comparison = None
@@ -602,6 +596,11 @@ def run_batch(a):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    import torch.distributed as dist
+    from vulcan.gpu.replicas import max_over_ranks
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
     w, l1, lab, _, t_build = _workload_setup("human", rank)
     p0 = _params(w, a)
     pool = synth.simulate_run(l1, lab, w, n_spectra=120000, seed=90000 + rank, run="pool")[0]
@@ -622,13 +621,16 @@ def run_batch(a):
         se = E.Searcher(gi, l1, p, pruner=prn, report=1)
         tables = se.search_batch(pinned, batch_spectra=a.batch_spectra)     # captures the batch shape
         torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
         se.device_ms = 0.0
         t0 = time.perf_counter()
         for _ in range(reps):
             tables = se.search_batch(pinned, batch_spectra=a.batch_spectra)
         torch.cuda.synchronize()
-        wall = time.perf_counter() - t0
-        res[name] = {"tables": [t for t, _ in tables], "device_ms": se.device_ms / reps, "wall_s": wall / reps,
+        wall = max_over_ranks(time.perf_counter() - t0, dev)
+        res[name] = {"tables": [t for t, _ in tables], "device_ms": max_over_ranks(se.device_ms, dev) / reps,
+                     "wall_s": wall / reps,
                      "batches": len(E.plan_batches(runs, a.batch_spectra)), "h2d": sum(s.h2d_bytes for _, s in tables),
                      "d2h": sum(s.d2h_bytes for _, s in tables)}
         del se
@@ -669,6 +671,9 @@ def run_batch(a):
             "autotune": tune_report, "clocks": clk, "index_build_s": round(t_build, 1),
         }
         print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def _traffic_from_profiles(kernel: str):
