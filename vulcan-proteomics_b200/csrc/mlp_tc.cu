@@ -5,13 +5,15 @@
 //
 // Persistent CTAs of 16 warps, one per SM (the weights fill most of the shared memory).  Warp w reads TMEM lanes
 // 32*(w%4).. (hit rows; a warp may only touch its lane quarter) and columns 64*(w/4).. .  Per tile of 128 hits:
-//   1. the 128 x 16 feature tile is copied into shared memory in the UMMA canonical K-major layout;
-//   2. one thread issues D = X W1^T (M 128, N 256, K 16) into 256 TMEM columns and commits to an mbarrier;
+//   1. the 128 x 16 feature tile (loaded into registers one tile ahead) is stored into shared memory in the UMMA
+//      canonical K-major layout;
+//   2. one thread issues D = X W1^T (M 128, N 256, K 16) into the tile's 256 TMEM columns and commits to an
+//      mbarrier;
 //   3. epilogue 1: every warp reads its 32 rows x 64 columns with tcgen05.ld, adds b1, applies ReLU, rounds to
 //      BF16 and writes them into shared memory as the layer-2 A operand;
 //   4. one thread issues D = H1 W2^T (K 256: 16 UMMAs) into the same TMEM columns and commits;
-//   5. epilogue 2: ReLU(D + b2) . w3 over the warp's 64 columns, the four column quarters of a row summed in a
-//      fixed order through shared memory, + b3, written to `logit`.
+//   5. epilogue 2 (done while the next tile's layer 2 runs): ReLU(D + b2) . w3 over the warp's 64 columns, the four
+//      column quarters of a row summed in a fixed order through shared memory, + b3, written to `logit`.
 // Shared-memory operands use the no-swizzle canonical layout: 8-row x 16-byte core matrices (128 contiguous bytes),
 // the two 16-byte K chunks of one UMMA K-step 128 bytes apart (leading byte offset), 8-row groups a whole K-row of
 // core matrices apart (stride byte offset).  Every mbarrier wait is bounded: on a timeout the CTA records
@@ -95,13 +97,17 @@ __device__ __forceinline__ uint32_t pack2(float lo, float hi) {
   return *reinterpret_cast<uint32_t*>(&v);
 }
 
+// Two TMEM accumulators of 256 columns (tile i uses buffer i % 2 for both layers), so that the layer-2 UMMAs of
+// tile i run while the warps finish tile i-1 (epilogue 2), and the layer-1 UMMA of tile i+1 is issued before the
+// epilogue of tile i.  tcgen05.commit tracks every earlier MMA of the issuing thread, so the wait for tile i's
+// layer 1 also covers tile i-1's layer 2 (which reads H1 in shared memory and tile i-1's TMEM buffer).
 __global__ void __launch_bounds__(TC_THREADS, 1)
 mlp_infer_tc_k(int64_t n, const int64_t* n_dev, const __nv_bfloat16* __restrict__ feat,
                const __nv_bfloat16* __restrict__ W1, const float* __restrict__ b1,
                const __nv_bfloat16* __restrict__ W2, const float* __restrict__ b2, const float* __restrict__ w3,
                float b3, float* __restrict__ logit, int32_t* status) {
   extern __shared__ uint8_t tc_raw[];
-  __shared__ __align__(8) uint64_t bar;
+  __shared__ __align__(8) uint64_t bar1[2], bar2[2];
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_flag;
   uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(tc_raw) + 127) & ~uintptr_t(127));
@@ -128,15 +134,31 @@ mlp_infer_tc_k(int64_t n, const int64_t* n_dev, const __nv_bfloat16* __restrict_
   }
   if (tid == 0) {
     abort_flag = 0;
-    vk::mbar_init(&bar, 1);
+    for (int q = 0; q < 2; ++q) {
+      vk::mbar_init(&bar1[q], 1);
+      vk::mbar_init(&bar2[q], 1);
+    }
     vk::fence_mbar_init();
   }
   if (warp == 0) {
     const uint32_t slot = (uint32_t)__cvta_generic_to_shared(&tmem_slot);
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot),
-                 "r"(TC_TMEM_COLS));
+                 "r"(2 * TC_TMEM_COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
   }
+  const int64_t n_tiles = (n + TC_M - 1) / TC_M;
+  const int64_t G = gridDim.x;
+  // feature rows: threads < 256 each hold one 16-byte half row of the next tile
+  const int fr = tid >> 1, fk = (tid & 1) * 8;
+  auto load_feat = [&](int64_t tile) {
+    uint4 v = make_uint4(0, 0, 0, 0);
+    if (tid < 2 * TC_M && tile < n_tiles) {
+      const int64_t row = tile * TC_M + fr;
+      if (row < n) v = *reinterpret_cast<const uint4*>(feat + row * TC_IN + fk);
+    }
+    return v;
+  };
+  uint4 fv = load_feat(blockIdx.x);
   async_proxy_fence();
   tc_fence_before();
   __syncthreads();
@@ -149,35 +171,39 @@ mlp_infer_tc_k(int64_t n, const int64_t* n_dev, const __nv_bfloat16* __restrict_
   const int rq = warp & 3, cq = warp >> 2;                 // lane (row) quarter, column quarter
   const int my_row = rq * 32 + (threadIdx.x & 31);
   const int col0 = cq * TC_COLS_PER_WARP;
-  const uint32_t lane_base = tmem + ((uint32_t)(rq * 32) << 16);
+  const uint32_t lane_off = (uint32_t)(rq * 32) << 16;
   float* part = reinterpret_cast<float*>(sm + OFF_PART);
-  uint32_t phase = 0;
-  const int64_t n_tiles = (n + TC_M - 1) / TC_M;
-  for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
-    // 1. feature tile (one 16-byte half row per thread)
-    if (tid < 2 * TC_M) {
-      const int r = tid >> 1, k = (tid & 1) * 8;
-      const int64_t row = tile * TC_M + r;
-      uint4 v = make_uint4(0, 0, 0, 0);
-      if (row < n) v = *reinterpret_cast<const uint4*>(feat + row * TC_IN + k);
-      *reinterpret_cast<uint4*>(sm + OFF_X + canon_off(r, k, TC_IN)) = v;
-    }
+  uint32_t ph1 = 0u, ph2 = 0u;                   // phase bit q of bar1[q] / bar2[q] to wait for next
+  uint64_t* last_bar = nullptr;                   // the latest commit (it covers every earlier MMA) ...
+  uint32_t last_ph = 0u;                          // ... and the phase it completes
+  int64_t tile = blockIdx.x, prev = -1;
+  int k = 0;
+  // prologue: tile 0's features and its layer 1
+  if (tile < n_tiles) {
+    if (tid < 2 * TC_M) *reinterpret_cast<uint4*>(sm + OFF_X + canon_off(fr, fk, TC_IN)) = fv;
     async_proxy_fence();
     tc_fence_before();
     __syncthreads();
-    // 2. layer 1
     if (tid == 0) {
       tc_fence_after();
       umma_bf16(tmem, dX, dW1, id_l, 0u);
-      umma_commit(&bar);
+      umma_commit(&bar1[0]);
     }
-    if (!vk::mbar_wait(&bar, phase, TC_WAIT)) atomicOr(&abort_flag, 1);
-    phase ^= 1u;
+    last_bar = &bar1[0];
+    last_ph = 0u;
+    fv = load_feat(tile + G);
+  }
+  while (tile < n_tiles) {
+    const int b = k & 1;
+    const uint32_t buf = tmem + (uint32_t)b * TC_TMEM_COLS;
+    // layer 1 of this tile (and everything issued before it) is done
+    if (!vk::mbar_wait(&bar1[b], (ph1 >> b) & 1u, TC_WAIT)) atomicOr(&abort_flag, 1);
+    ph1 ^= 1u << b;
     tc_fence_after();
-    // 3. epilogue 1: H1 = bf16(relu(D + b1)) into the layer-2 operand
+    // epilogue 1: H1 = bf16(relu(D + b1)) into the layer-2 operand
     for (int c0 = col0; c0 < col0 + TC_COLS_PER_WARP; c0 += 32) {
       uint32_t v[32];
-      tmem_ld32(lane_base + (uint32_t)c0, v);
+      tmem_ld32(buf + lane_off + (uint32_t)c0, v);
       tmem_wait_ld();
       uint8_t* dst = sm + OFF_H + canon_off(my_row, c0, TC_H);
 #pragma unroll
@@ -199,25 +225,73 @@ mlp_infer_tc_k(int64_t n, const int64_t* n_dev, const __nv_bfloat16* __restrict_
     tc_fence_before();
     __syncthreads();
     if (abort_flag) break;
-    // 4. layer 2 (K = 256 in 16 steps of 16)
+    // layer 2 of this tile into the same buffer (K = 256 in 16 steps)
     if (tid == 0) {
       tc_fence_after();
 #pragma unroll 1
       for (int ks = 0; ks < TC_H / 16; ++ks) {
         const uint64_t dA = smem_desc(s_base + OFF_H + ks * 256, 128, (TC_H / 8) * 128);
         const uint64_t dB = smem_desc(s_base + OFF_W2 + ks * 256, 128, (TC_H / 8) * 128);
-        umma_bf16(tmem, dA, dB, id_l, ks > 0 ? 1u : 0u);
+        umma_bf16(buf, dA, dB, id_l, ks > 0 ? 1u : 0u);
       }
-      umma_commit(&bar);
+      umma_commit(&bar2[b]);
     }
-    if (!vk::mbar_wait(&bar, phase, TC_WAIT)) atomicOr(&abort_flag, 1);
-    phase ^= 1u;
+    last_bar = &bar2[b];
+    last_ph = (ph2 >> b) & 1u;
+    // epilogue 2 of the previous tile (its buffer), overlapping this tile's layer 2
+    if (prev >= 0) {
+      const int pb = b ^ 1;
+      if (!vk::mbar_wait(&bar2[pb], (ph2 >> pb) & 1u, TC_WAIT)) atomicOr(&abort_flag, 1);
+      ph2 ^= 1u << pb;
+      tc_fence_after();
+      const uint32_t pbuf = tmem + (uint32_t)pb * TC_TMEM_COLS;
+      float z = 0.f;
+      for (int c0 = col0; c0 < col0 + TC_COLS_PER_WARP; c0 += 32) {
+        uint32_t v[32];
+        tmem_ld32(pbuf + lane_off + (uint32_t)c0, v);
+        tmem_wait_ld();
+#pragma unroll
+        for (int j = 0; j < 32; ++j) z += fmaxf(__uint_as_float(v[j]) + sb2[c0 + j], 0.f) * sw3[c0 + j];
+      }
+      part[cq * TC_M + my_row] = z;
+    }
+    // the next tile's features (layer 1 of this tile is done with the feature buffer)
+    const int64_t nt = tile + G;
+    if (nt < n_tiles && tid < 2 * TC_M) *reinterpret_cast<uint4*>(sm + OFF_X + canon_off(fr, fk, TC_IN)) = fv;
+    async_proxy_fence();
+    tc_fence_before();
+    __syncthreads();
+    if (prev >= 0 && tid < TC_M) {
+      const int64_t row = prev * TC_M + tid;
+      if (row < n) logit[row] = ((part[tid] + part[TC_M + tid]) + (part[2 * TC_M + tid] + part[3 * TC_M + tid])) + b3;
+    }
+    if (abort_flag) break;
+    // layer 1 of the next tile into the other buffer (epilogue 2 above has finished reading it)
+    if (nt < n_tiles) {
+      if (tid == 0) {
+        tc_fence_after();
+        umma_bf16(tmem + (uint32_t)(b ^ 1) * TC_TMEM_COLS, dX, dW1, id_l, 0u);
+        umma_commit(&bar1[b ^ 1]);
+      }
+      last_bar = &bar1[b ^ 1];
+      last_ph = (ph1 >> (b ^ 1)) & 1u;
+      fv = load_feat(nt + G);
+    }
+    prev = tile;
+    tile = nt;
+    ++k;
+  }
+  // epilogue 2 of the last tile
+  if (!abort_flag && prev >= 0) {
+    const int pb = (k - 1) & 1;
+    if (!vk::mbar_wait(&bar2[pb], (ph2 >> pb) & 1u, TC_WAIT)) atomicOr(&abort_flag, 1);
+    ph2 ^= 1u << pb;
     tc_fence_after();
-    // 5. epilogue 2: partial logit of this thread's row over the warp's columns, then the row's four quarters
+    const uint32_t pbuf = tmem + (uint32_t)pb * TC_TMEM_COLS;
     float z = 0.f;
     for (int c0 = col0; c0 < col0 + TC_COLS_PER_WARP; c0 += 32) {
       uint32_t v[32];
-      tmem_ld32(lane_base + (uint32_t)c0, v);
+      tmem_ld32(pbuf + lane_off + (uint32_t)c0, v);
       tmem_wait_ld();
 #pragma unroll
       for (int j = 0; j < 32; ++j) z += fmaxf(__uint_as_float(v[j]) + sb2[c0 + j], 0.f) * sw3[c0 + j];
@@ -226,21 +300,22 @@ mlp_infer_tc_k(int64_t n, const int64_t* n_dev, const __nv_bfloat16* __restrict_
     tc_fence_before();
     __syncthreads();
     if (tid < TC_M) {
-      const int64_t row = tile * TC_M + tid;
+      const int64_t row = prev * TC_M + tid;
       if (row < n) logit[row] = ((part[tid] + part[TC_M + tid]) + (part[2 * TC_M + tid] + part[3 * TC_M + tid])) + b3;
     }
-    if (abort_flag) break;
   }
+  __syncthreads();
   if (abort_flag) {
     if (tid == 0) {
       atomicOr(status, VK_STATUS_WAIT_TIMEOUT);
-      vk::mbar_wait(&bar, phase, TC_WAIT);   // the MMAs in flight, once more, bounded
+      // the MMAs in flight, once more, bounded: the latest commit covers every earlier MMA
+      if (last_bar) vk::mbar_wait(last_bar, last_ph, TC_WAIT);
     }
     __syncthreads();
   }
   if (warp == 0) {
     tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * TC_TMEM_COLS));
   }
 }
 
