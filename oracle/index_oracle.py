@@ -75,7 +75,8 @@ def expand_pairs(fwd, dec, perms, static, var, max_var, min_mass, max_mass, id_s
                     for k in comb:
                         if k != 63:
                             per[f[k]] = per.get(f[k], 0) + 1
-                    if any(per.get(c, 0) > lim for c, lim in site_limits.items()):
+                    # a key of one or more residues caps the sites of those residues together
+                    if any(sum(per.get(c, 0) for c in key) > lim for key, lim in site_limits.items()):
                         continue
                 m = 0
                 for k in comb:

@@ -4,8 +4,9 @@
 // peptide, every set of variable-modification sites of size <= max_var is one peptidoform; the decoy side gets the
 // same modifications carried through the pair's permutation; forms whose f64 mass is outside [min_mass, max_mass]
 // are dropped; ids are xxh64(canonical string, id_seed) and masses are Sage's f32 sums.  This file restates that
-// contract in C++ (plain C ABI, called through ctypes) and adds per-residue site limits
-// (limit_res[r] = max sites of residue type r, 255 = no own limit) on top of the global max_var.
+// contract in C++ (plain C ABI, called through ctypes) and adds site limits on top of the global max_var: residue
+// type r belongs to site group group_res[r], and a form may carry at most limit_group[g] sites of group g (255 = no
+// own limit); e.g. S, T and Y in one group capped at 3 phospho sites, M in its own group capped at 1.
 //
 // xxh64 follows the published XXH64 specification (Yann Collet, xxHash); the tests compare it with the Python
 // `xxhash` package.
@@ -64,7 +65,8 @@ struct Cfg {
   float h2o32;
   double h2o64;
   int max_var;
-  const uint8_t* limit_res; // 26 per-residue site limits (255 = none)
+  const uint8_t* group_res;   // 26: site group of each residue type
+  const uint8_t* limit_group; // 26: site limit of each group (255 = none)
   char tag[26][24];         // "[+15.9949]" per residue
   char ntag[24];
 };
@@ -123,8 +125,8 @@ void forms_of(const Cfg& c, const uint8_t* s, int n, std::vector<uint64_t>& out)
         int k = sites[idx[i]];
         m |= 1ull << k;
         if (k != 63) {
-          int t = s[k] - 'A';
-          if (++per[t] > c.limit_res[t]) ok = false;
+          int g = c.group_res[s[k] - 'A'];
+          if (++per[g] > c.limit_group[g]) ok = false;
         }
       }
       if (ok) out.push_back(m);
@@ -148,13 +150,15 @@ uint64_t vc_xxh64(const uint8_t* p, int64_t n, uint64_t seed) { return xxh64(p, 
 // them (capacity = that number) and returns it again.  Negative return: bad input (index of the pair, -1 - i).
 int64_t vc_expand_pairs(int64_t n_pairs, const uint8_t* fwd, const uint8_t* dec, const int64_t* seq_off,
                         const uint8_t* perm_flat, const int64_t* perm_off, const float* mono, const double* res_f64,
-                        const double* stat, const double* var, double nterm, int max_var, const uint8_t* limit_res,
+                        const double* stat, const double* var, double nterm, int max_var, const uint8_t* group_res,
+                        const uint8_t* limit_group,
                         double min_mass, double max_mass, uint64_t id_seed, int nthreads,
                         uint32_t* o_seq, uint64_t* o_mask_f, uint64_t* o_mask_d, double* o_mass, uint8_t* o_nvar,
                         uint64_t* o_id_f, uint64_t* o_id_d, float* o_m32f, float* o_m32d) {
   Cfg c;
   c.mono = mono; c.res_f64 = res_f64; c.stat = stat; c.var = var; c.nterm = nterm;
-  c.h2o32 = 18.010565f; c.h2o64 = 18.010564684; c.max_var = max_var; c.limit_res = limit_res;
+  c.h2o32 = 18.010565f; c.h2o64 = 18.010564684; c.max_var = max_var; c.group_res = group_res;
+  c.limit_group = limit_group;
   for (int i = 0; i < 26; ++i) std::snprintf(c.tag[i], sizeof(c.tag[i]), "[%+.4f]", var[i]);
   std::snprintf(c.ntag, sizeof(c.ntag), "[%+.4f]", nterm);
 #ifdef _OPENMP

@@ -50,8 +50,9 @@ def core_lib():
     if _core is None:
         L = _load(CORE_SO, "native index core")
         L.vc_expand_pairs.restype = C.c_int64
-        L.vc_expand_pairs.argtypes = [C.c_int64] + [C.c_void_p] * 9 + [C.c_double, C.c_int, C.c_void_p, C.c_double,
-                                                                          C.c_double, C.c_uint64, C.c_int] + \
+        L.vc_expand_pairs.argtypes = [C.c_int64] + [C.c_void_p] * 9 + [C.c_double, C.c_int, C.c_void_p, C.c_void_p,
+                                                                          C.c_double, C.c_double, C.c_uint64,
+                                                                          C.c_int] + \
             [C.c_void_p] * 9
         L.vc_xxh64.restype = C.c_uint64
         L.vc_xxh64.argtypes = [C.c_char_p, C.c_int64, C.c_uint64]

@@ -201,8 +201,9 @@ def _native():
 def expand_pairs(fwd, dec, perm_flat, perm_off, static_mods, var_mods, max_var, min_mass, max_mass, id_seed,
                  site_limits: dict | None = None, nthreads: int = 0):
     """Paired peptidoforms, one row per (forward form, decoy form) pair (``lib.rs:271-399``), computed by the
-    native core (``csrc/vulcan_core.cpp``).  ``site_limits`` optionally caps the sites of one residue type
-    (e.g. ``{"S": 3, "T": 3, "Y": 3}`` shares nothing: each residue type has its own cap) under ``max_var``."""
+    native core (``csrc/vulcan_core.cpp``).  ``site_limits`` optionally caps modification sites under ``max_var``:
+    each key is one or more residue letters whose sites are capped together (``{"STY": 3, "M": 1}``: at most three
+    phospho sites on S/T/Y in total and one oxidised M)."""
     import ctypes as C
     if len(fwd) != len(dec):
         raise ValueError("fwd and dec differ in length")
@@ -220,9 +221,13 @@ def expand_pairs(fwd, dec, perm_flat, perm_off, static_mods, var_mods, max_var, 
         raise ValueError("non-standard residue in a pair")
     perm_flat = np.ascontiguousarray(perm_flat, np.uint8)
     perm_off = np.ascontiguousarray(perm_off, np.int64)
+    group = np.arange(26, dtype=np.uint8)
     lim = np.full(26, 255, np.uint8)
-    for r, k in (site_limits or {}).items():
-        lim[ord(r) - 65] = min(255, int(k))
+    for key, k in (site_limits or {}).items():
+        g = ord(key[0]) - 65
+        for r in key:
+            group[ord(r) - 65] = g
+        lim[g] = min(255, int(k))
     mono = np.ascontiguousarray(SAGE_MONO, np.float32)
     resf = np.ascontiguousarray(RESIDUE_F64, np.float64)
     st = np.ascontiguousarray(static_res, np.float64)
@@ -230,7 +235,7 @@ def expand_pairs(fwd, dec, perm_flat, perm_off, static_mods, var_mods, max_var, 
     L = _native()
     ptr = lambda a: a.ctypes.data_as(C.c_void_p)
     args = [C.c_int64(n), ptr(fres), ptr(dres), ptr(off), ptr(perm_flat), ptr(perm_off), ptr(mono), ptr(resf),
-            ptr(st), ptr(va), C.c_double(nterm), C.c_int(int(max_var)), ptr(lim), C.c_double(min_mass),
+            ptr(st), ptr(va), C.c_double(nterm), C.c_int(int(max_var)), ptr(group), ptr(lim), C.c_double(min_mass),
             C.c_double(max_mass), C.c_uint64(int(id_seed)), C.c_int(int(nthreads))]
     total = L.vc_expand_pairs(*args, *([None] * 9))
     if total < 0:
