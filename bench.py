@@ -146,10 +146,10 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_oracle_pass(l1, sp_sub, p):
+def cpu_oracle_pass(l1, sp_sub, p, var=None):
     """The oracle's search of a run (K0, hypotheses, K1, top-K + closure, K2, ranking) on the host cores."""
     from oracle import oracle as O
-    P = O.make_params(STATIC, VAR, p.fragment_unit)
+    P = O.make_params(STATIC, VAR if var is None else var, p.fragment_unit)
     pk = O.k0_view(sp_sub, p)
     hyp = O.make_hypotheses(sp_sub, pk["valid"], l1.mass32, p)
     win_off, cnt, sc, mt = O.k1_windows(l1, hyp, pk, p, P, arrays=_ARR.get(id(l1)))
@@ -170,18 +170,18 @@ def _subset(sp, n):
                    sp.mz[:o[-1]], sp.intensity[:o[-1]], o.copy())
 
 
-def cpu_rate(l1, sp, p, budget_s: float):
+def cpu_rate(l1, sp, p, budget_s: float, var=None):
     """spectra/s of the CPU oracle on a sample sized to take about budget_s."""
     from oracle import oracle as O
     _ARR[id(l1)] = {k: np.ascontiguousarray(getattr(l1, k)) for k in ("seq_off", "length", "mask", "mass32",
                                                                          "residues")}
     n = 500
     t0 = time.perf_counter()
-    cpu_oracle_pass(l1, _subset(sp, n), p)
+    cpu_oracle_pass(l1, _subset(sp, n), p, var)
     t = time.perf_counter() - t0
     n2 = int(min(len(sp), max(n, n * budget_s / max(t, 1e-3))))
     t0 = time.perf_counter()
-    cpu_oracle_pass(l1, _subset(sp, n2), p)
+    cpu_oracle_pass(l1, _subset(sp, n2), p, var)
     t2 = time.perf_counter() - t0
     return n2 / t2, n2, t2, O.n_threads()
 
@@ -313,7 +313,7 @@ def run_b200(a):
     from vulcan.gpu import prune as PR
     w, l1, lab, sp, t_build = _workload_setup(a.workload, rank)
     p = _params(w, a)
-    gi = E.GpuIndex(l1, p, STATIC, VAR, device=dev)
+    gi = E.GpuIndex(l1, p, STATIC, w.var_mods, device=dev)
     pruned = a.path == "pruned"
     pr, pr_info = _pruner_setup(a, w, l1, lab, gi, p, rank) if pruned else (None, None)
     if pruned and a.save_pruner and rank == 0:
@@ -423,7 +423,7 @@ def run_b200(a):
     if rank == 0:
         cpu = None
         if world == 1:
-            rate, n_s, t_s, cores = cpu_rate(l1, sp, p, a.cpu_budget)
+            rate, n_s, t_s, cores = cpu_rate(l1, sp, p, a.cpu_budget, w.var_mods)
             cpu = {"value": round(rate, 1), "unit": "spectra/s", "cores": cores, "kind": "port",
                    "sample": f"first {n_s} spectra of the run through the oracle's plain path K0->hypotheses->K1->"
                              f"top-k->K2->ranking ({t_s:.1f} s)"}
@@ -582,10 +582,17 @@ def _kernel_table(a, p, gi, run, flush, pr, dev):
     return kern, mlp
 
 
+BATCH_SETUPS = {   # workload -> (index workload, runs, smallest, largest run, spectra per batch, description)
+    "batch64": ("human", 64, 5000, 60000, 131072, "configuration 2: 64 runs, batched, graph-captured"),
+    "phospho": ("phospho", 32, 20000, 50000, 65536,
+                "configuration 4: phospho S/T/Y <= 3 + Met-ox <= 1 index, 32 runs, batched, graph-captured"),
+}
+
+
 def run_batch(a):
-    """Configuration 2: 64 runs of 5,000-60,000 spectra (log-uniform), drawn from a pool of simulated spectra,
-    searched in fixed-shape batches, each batch one replay of a captured CUDA graph; tile rows and K1 warps chosen
-    by the autotuner on a sample; learned-pruned and plain paths, each run's table checked against its own search."""
+    """Configurations 2 and 4: many runs (sizes log-uniform), drawn from a pool of simulated spectra, searched in
+    fixed-shape batches, each batch one replay of a captured CUDA graph; tile rows and K1 warps chosen by the
+    autotuner on a sample; learned-pruned and plain paths, each run's table checked against its own search."""
     import torch
     from vulcan import synth
     from vulcan.gpu import autotune as AT
@@ -601,37 +608,40 @@ def run_batch(a):
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
-    w, l1, lab, _, t_build = _workload_setup("human", rank)
+    wl, n_runs, lo_run, hi_run, batch_default, desc = BATCH_SETUPS[a.workload]
+    batch_spectra = a.batch_spectra or batch_default
+    w, l1, lab, _, t_build = _workload_setup(wl, rank)
+    var = w.var_mods
     p0 = _params(w, a)
     pool = synth.simulate_run(l1, lab, w, n_spectra=120000, seed=90000 + rank, run="pool")[0]
-    runs = synth.batch_runs(pool, 64, 5000, 60000, seed=2 + rank)
+    runs = synth.batch_runs(pool, n_runs, lo_run, hi_run, seed=2 + rank)
     n_total = sum(len(r) for r in runs)
-    gi0 = E.GpuIndex(l1, p0, STATIC, VAR, device=dev)
+    gi0 = E.GpuIndex(l1, p0, STATIC, var, device=dev)
     pr, pr_info = _pruner_setup(a, w, l1, lab, gi0, p0, rank)
     del gi0
     torch.cuda.empty_cache()
     sample = synth.take_spectra(pool, np.arange(40000), "sample")
-    p, tune_report = AT.tune(l1, p0, STATIC, VAR, sample, pruner=pr, device=dev)
-    gi = E.GpuIndex(l1, p, STATIC, VAR, device=dev)
+    p, tune_report = AT.tune(l1, p0, STATIC, var, sample, pruner=pr, device=dev)
+    gi = E.GpuIndex(l1, p, STATIC, var, device=dev)
     pinned = [E.pin_spectra(r) for r in runs]
     reps = max(2, a.steps // 10)
     res = {}
     clocks = ClockSampler(local)
     for name, prn in (("pruned", pr), ("plain", None)):
         se = E.Searcher(gi, l1, p, pruner=prn, report=1)
-        tables = se.search_batch(pinned, batch_spectra=a.batch_spectra)     # captures the batch shape
+        tables = se.search_batch(pinned, batch_spectra=batch_spectra)     # captures the batch shape
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
         se.device_ms = 0.0
         t0 = time.perf_counter()
         for _ in range(reps):
-            tables = se.search_batch(pinned, batch_spectra=a.batch_spectra)
+            tables = se.search_batch(pinned, batch_spectra=batch_spectra)
         torch.cuda.synchronize()
         wall = max_over_ranks(time.perf_counter() - t0, dev)
         res[name] = {"tables": [t for t, _ in tables], "device_ms": max_over_ranks(se.device_ms, dev) / reps,
                      "wall_s": wall / reps,
-                     "batches": len(E.plan_batches(runs, a.batch_spectra)), "h2d": sum(s.h2d_bytes for _, s in tables),
+                     "batches": len(E.plan_batches(runs, batch_spectra)), "h2d": sum(s.h2d_bytes for _, s in tables),
                      "d2h": sum(s.d2h_bytes for _, s in tables)}
         del se
         torch.cuda.empty_cache()
@@ -648,15 +658,18 @@ def run_batch(a):
     pr_ms, pl_ms = res["pruned"]["device_ms"], res["plain"]["device_ms"]
     if rank == 0:
         line = {
-            "metric": METRIC + " (configuration 2: 64 runs, batched, graph-captured)", "value":
+            "metric": METRIC + f" ({desc})", "value":
                 round(n_total * world / (pr_ms / 1e3), 1), "unit": "spectra/s", "n_gpus": world, "steps": reps,
             "warmup": 1, "ms_per_step": round(pr_ms, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 (MLP: bf16 weights, fp32 accumulate)", "data": "synthetic",
-            "config": {"workload": f"64 runs of 5,000-60,000 spectra (log-uniform; {n_total} spectra) drawn from "
-                                   "120,000 simulated spectra, human-scale index",
-                       "batch_spectra": a.batch_spectra, "batches": res["pruned"]["batches"],
-                       "step": "all 64 runs once", "tile_rows": p.tile_rows, "k1_warps": p.k1_warps,
-                       "l2": "not flushed (batches of up to 131,072 spectra, working sets above L2)",
+            "config": {"workload": f"{n_runs} runs of {lo_run:,}-{hi_run:,} spectra (log-uniform; {n_total} spectra) "
+                                   f"drawn from 120,000 simulated spectra, {wl} index ({len(l1)} peptidoforms)"
+                                   + (f", {int(100 * w.phospho_frac)}% of spectra from phosphopeptides"
+                                      if w.phospho_frac else ""),
+                       "topk": p.topk,
+                       "batch_spectra": batch_spectra, "batches": res["pruned"]["batches"],
+                       "step": f"all {n_runs} runs once", "tile_rows": p.tile_rows, "k1_warps": p.k1_warps,
+                       "l2": f"not flushed (batches of up to {batch_spectra:,} spectra, working sets above L2)",
                        "pruner": pr_info},
             "e2e": {"value": round(n_total * world / res["pruned"]["wall_s"], 1), "unit": "spectra/s",
                     "h2d_bytes_per_step": int(res["pruned"]["h2d"]), "d2h_bytes_per_step": int(res["pruned"]["d2h"])},
@@ -699,7 +712,7 @@ def run_profile(a):
     dev = torch.device("cuda", 0)
     w, l1, _, sp, _ = _workload_setup(a.workload, 0)
     p = _params(w, a)
-    gi = E.GpuIndex(l1, p, STATIC, VAR, device=dev)
+    gi = E.GpuIndex(l1, p, STATIC, w.var_mods, device=dev)
     run = E.DeviceRun(sp, dev)
     st = E.Stats()
     pr = None
@@ -722,20 +735,20 @@ def run_reference(a):
     if rank != 0:
         return
     from oracle import oracle as O
-    w, l1, _, sp, _ = _workload_setup("human" if a.workload == "batch64" else a.workload, 0)
+    w, l1, _, sp, _ = _workload_setup(BATCH_SETUPS[a.workload][0] if a.workload in BATCH_SETUPS else a.workload, 0)
     p = w.search_params()
     _ARR[id(l1)] = {k: np.ascontiguousarray(getattr(l1, k)) for k in ("seq_off", "length", "mask", "mass32",
                                                                          "residues")}
     # per-step sample sized so warmup + steps take about a.cpu_total seconds
     t0 = time.perf_counter()
-    cpu_oracle_pass(l1, _subset(sp, 300), p)
+    cpu_oracle_pass(l1, _subset(sp, 300), p, w.var_mods)
     per_spec = (time.perf_counter() - t0) / 300
     n_step = int(max(100, min(len(sp), a.cpu_total / max(1, a.steps + a.warmup) / max(per_spec, 1e-6))))
     for i in range(a.warmup):
-        cpu_oracle_pass(l1, _subset(sp, n_step), p)
+        cpu_oracle_pass(l1, _subset(sp, n_step), p, w.var_mods)
     t0 = time.perf_counter()
     for i in range(a.steps):
-        cpu_oracle_pass(l1, _subset(sp, n_step), p)
+        cpu_oracle_pass(l1, _subset(sp, n_step), p, w.var_mods)
     t = time.perf_counter() - t0
     value = n_step * a.steps / t
     cores = O.n_threads()
@@ -757,9 +770,10 @@ def main():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
-    ap.add_argument("--workload", choices=("human", "small", "batch64"), default="human",
-                    help="batch64: configuration 2 (64 runs, batched graph-captured search, autotuned layout)")
-    ap.add_argument("--batch-spectra", type=int, default=131072, help="spectra per batch (batch64)")
+    ap.add_argument("--workload", choices=("human", "small", "batch64", "phospho"), default="human",
+                    help="batch64: configuration 2 (64 runs, batched graph-captured search, autotuned layout); "
+                         "phospho: configuration 4 (phospho var-mod index, 32 runs, batched)")
+    ap.add_argument("--batch-spectra", type=int, default=None, help="spectra per batch (batch workloads)")
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of CPU-baseline work (rank 0, N=1)")
     ap.add_argument("--cpu-total", type=float, default=120.0, help="seconds of the reference arm in total")
     ap.add_argument("--method", choices=("staged", "fused"), default="staged",
@@ -784,7 +798,7 @@ def main():
         ap.error("--warmup must be >= 3")
     if a.impl == "reference":
         run_reference(a)
-    elif a.workload == "batch64":
+    elif a.workload in BATCH_SETUPS:
         run_batch(a)
     elif a.mode == "profile":
         run_profile(a)

@@ -520,3 +520,35 @@ def test_autotuner_picks_a_measured_layout(mini, param_sets, tmp_path, torch_cud
     # the chosen layout searches like any other
     gi = E.GpuIndex(l1, q, STATIC, VAR)
     assert E.search(sp, gi, l1, q)[0].num_rows > 0
+
+
+def test_phospho_index_search_equals_oracle(tmp_path, torch_cuda):
+    """A small phospho index (S/T/Y at most 3 sites together, Met-ox at most 1; three variable residues) searched
+    on the device equals the oracle's search: K1 counts, candidates, K2 and the top PSMs."""
+    import dataclasses
+    from oracle import oracle as O
+    from vulcan import synth
+    from vulcan.gpu import engine as E
+    from vulcan.index.build import L1Index, read_labels
+    w = dataclasses.replace(synth.WORKLOADS["phospho"], name="phospho_mini", n_proteins=60, n_spectra=300)
+    d = synth.build_index(w, str(tmp_path))
+    l1, lab = L1Index(d), read_labels(d)
+    sp = synth.simulate_run(l1, lab, w)[0]
+    p = w.search_params(topk=20)
+    static, var = {"C": 57.021464}, w.var_mods
+    gi = E.GpuIndex(l1, p, static, var)
+    tbl, st, out = E.search(sp, gi, l1, p, report=2)
+    P = O.make_params(static, var, p.fragment_unit)
+    pk = O.k0_view(sp, p)
+    hyp = O.make_hypotheses(sp, pk["valid"], l1.mass32, p)
+    win_off, cnt, sc, mt = O.k1_windows(l1, hyp, pk, p, P)
+    assert np.array_equal(out["cnt"][:int(out["win_off"][-1])].cpu().numpy(), cnt)
+    oh, orr, oc = O.k1_appended(hyp, win_off, cnt, p.k1_threshold)
+    h, r, c = O.select_topk(oh, orr, oc, hyp["spec"], l1.partner, p.topk)
+    nc = int(out["cand_off"][-1])
+    assert np.array_equal(out["c_row"][:nc].cpu().numpy(), r)
+    k2 = O.k2(l1, hyp, pk, h, r, p, P)
+    np.testing.assert_allclose(out["k2"]["hyperscore"][:nc].cpu().numpy(), k2["hyperscore"], rtol=1e-12)
+    rk = O.psm_rank(k2, r, p.min_matched_peaks, 2)
+    assert np.array_equal(tbl.column("pf_row").to_numpy(), r[rk["cand"]])
+    assert tbl.num_rows > 0 and sum(synth.phospho_rows(l1)[tbl.column("pf_row").to_numpy()]) > 0

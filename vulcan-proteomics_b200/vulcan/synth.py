@@ -54,13 +54,18 @@ class Workload:
     proteome_seed: int
     spectra_seed: int
     iso_frac: tuple = (0.85, 0.12, 0.03)   # fraction of precursors picked at isotope 0 / +1 / +2
+    site_limits: dict | None = None         # site caps per residue group, e.g. {"STY": 3, "M": 1}
+    phospho_frac: float | None = None       # fraction of spectra simulated from phosphopeptides (S/T/Y sites)
 
     def index_params(self) -> dict:
-        return {"enzyme": {"cleave_at": "KR", "restrict": "P", "c_terminal": True,
-                           "missed_cleavages": self.missed_cleavages, "min_len": self.min_len,
-                           "max_len": self.max_len},
-                "static_mods": {"C": 57.021464}, "variable_mods": dict(self.var_mods),
-                "max_variable_mods": self.max_var}
+        d = {"enzyme": {"cleave_at": "KR", "restrict": "P", "c_terminal": True,
+                        "missed_cleavages": self.missed_cleavages, "min_len": self.min_len,
+                        "max_len": self.max_len},
+             "static_mods": {"C": 57.021464}, "variable_mods": dict(self.var_mods),
+             "max_variable_mods": self.max_var}
+        if self.site_limits:
+            d["site_limits"] = dict(self.site_limits)
+        return d
 
     def search_params(self, **kw) -> SearchParams:
         d = dict(precursor_ppm=(-10.0, 10.0), fragment_ppm=(-0.02, 0.02), fragment_unit="da",
@@ -74,7 +79,28 @@ WORKLOADS = {
                       50, 150, 20241, 7),
     "human": Workload("human", 20400, 2, 7, 30, {"M": 15.9949}, 1, 40000, (2, 4), 0.6, None, 150.0, 0.5,
                       (20, 600), 100, 512, 20400, 11),
+    # configuration 4: the human proteome with phospho on S/T/Y (at most 3 sites) and Met-ox (at most 1);
+    # runs of 20,000-50,000 spectra, 40% from phosphopeptides, top-k 200
+    "phospho": Workload("phospho", 20400, 2, 7, 30, {"M": 15.9949, "S": 79.966331, "T": 79.966331,
+                                                   "Y": 79.966331}, 4, 40000, (2, 4), 0.6, None, 150.0, 0.5,
+                        (20, 600), 200, 512, 20400, 13, site_limits={"STY": 3, "M": 1}, phospho_frac=0.4),
 }
+
+
+def phospho_rows(l1) -> np.ndarray:
+    """Whether each row carries a modification on S, T or Y."""
+    mask = np.asarray(l1.mask, np.uint64)
+    off = np.asarray(l1.seq_off, np.int64)
+    ln = np.asarray(l1.length, np.int64)
+    res = np.asarray(l1.residues)
+    sty = np.zeros(256, bool)
+    sty[[ord("S"), ord("T"), ord("Y")]] = True
+    out = np.zeros(len(mask), bool)
+    for k in range(int(ln.max()) if len(ln) else 0):
+        on = ((mask >> np.uint64(k)) & np.uint64(1)).astype(bool) & (ln > k)
+        idx = np.flatnonzero(on)
+        out[idx] |= sty[res[off[idx] + k]]
+    return out
 
 
 def random_proteome_fasta(n_proteins: int, seed: int, median_len: float = 400.0, sigma: float = 0.6) -> str:
@@ -96,6 +122,8 @@ def random_proteome_fasta(n_proteins: int, seed: int, median_len: float = 400.0,
 def _cache_key(w: Workload) -> str:
     d = {"n": w.n_proteins, "mc": w.missed_cleavages, "len": [w.min_len, w.max_len], "var": w.var_mods,
          "mv": w.max_var, "seed": w.proteome_seed, "v": 2}
+    if w.site_limits:
+        d["lim"] = w.site_limits
     return hashlib.sha256(json.dumps(d, sort_keys=True).encode()).hexdigest()[:12]
 
 
@@ -139,7 +167,15 @@ def simulate_run(l1, labels, w: Workload | str, n_spectra: int | None = None, se
     rng = np.random.default_rng(w.spectra_seed if seed is None else seed)
     is_dec = np.asarray(labels.column("is_decoy").to_numpy(zero_copy_only=False), bool)
     tgt = np.flatnonzero(~is_dec)
-    rows = rng.choice(tgt, n, replace=len(tgt) < n)
+    if w.phospho_frac:
+        ph = phospho_rows(l1)[tgt]
+        n_ph = int(round(n * w.phospho_frac))
+        a, b = tgt[ph], tgt[~ph]
+        rows = np.concatenate([rng.choice(a, n_ph, replace=len(a) < n_ph),
+                               rng.choice(b, n - n_ph, replace=len(b) < n - n_ph)])
+        rows = rows[rng.permutation(n)]
+    else:
+        rows = rng.choice(tgt, n, replace=len(tgt) < n)
     static = {"C": 57.021464}
     mz_l, it_l = [], []
     off = np.zeros(n + 1, np.int64)
