@@ -91,7 +91,8 @@ def _config(w, p, extra=None):
            "method": ("fused persistent kernel (K1+top-k+K2+ranking per spectrum)" if p.search_method == "fused"
                       else "staged kernels"),
            "precursor_ppm": list(p.precursor_ppm), "fragment_tol": f"+-{p.fragment_ppm[1]} {p.fragment_unit}",
-           "topk": p.topk, "max_peaks": p.max_peaks, "k1": f"per-peak search, {p.k1_warps} warps per tile CTA",
+           "topk": p.topk, "max_peaks": p.max_peaks,
+           "k1": f"bitmap-filtered per-peak search, {p.k1_warps} warps per tile CTA",
            "l2": "flushed between steps (256 MiB write)"}
     if extra:
         cfg.update(extra)
@@ -187,15 +188,19 @@ def cpu_rate(l1, sp, p, budget_s: float, var=None):
 
 
 def k1_algorithmic_bytes(gi, dh, peaks, win_off, item_off, item_hyp):
-    """Bytes K1 must move per launch: each tile with work is read once (postings + coarse-bin CSR); per work item
-    the spectrum's peak masses (4 B each) and the hypothesis record (spec 4, maxfz 1, lo/hi 16, peak offsets 16,
-    item id 4); per window row one 4-byte count written."""
+    """Bytes K1 must move per launch: each tile with work is read once (postings, coarse-bin CSR and presence
+    bitmap); per work item the spectrum's peak filter words (one u32 per peak and fragment charge, from
+    vk_k1_peak_keys) and the hypothesis record (spec 4, maxfz 1, lo/hi 16, peak offsets 16, item id 4); per window
+    row one 4-byte count written.  The window keys read for the few windows that pass the bitmap are not counted."""
     nt = gi.tix.n_tiles
-    stride = ((1 << gi.tix.cbin_bits) + 1 + 7) & ~7
+    nb = 1 << gi.tix.cbin_bits
+    stride = (nb + 1 + 7) & ~7
     busy = (item_off[1:] - item_off[:-1]) > 0
-    tile_bytes = ((gi.tile_off[1:nt + 1] - gi.tile_off[:nt]) * 4 + stride * 2)[busy].sum()
-    s = dh["spec"][item_hyp.long()].long()
-    item_bytes = ((peaks["off"][s + 1] - peaks["off"][s]) * 4 + 41).sum()
+    tile_bytes = ((gi.tile_off[1:nt + 1] - gi.tile_off[:nt]) * 4 + stride * 2 + nb * 16)[busy].sum()
+    it = item_hyp.long()
+    s = dh["spec"][it].long()
+    nz = (dh["maxfz"][it].long() - 1).clamp(min=0)
+    item_bytes = ((peaks["off"][s + 1] - peaks["off"][s]) * 4 * nz + 41).sum()
     return int((tile_bytes + item_bytes + win_off[-1] * 4).item())
 
 
@@ -520,13 +525,17 @@ def _kernel_table(a, p, gi, run, flush, pr, dev):
     n_win = int(win_off[-1])
     isum = so.get("isum")
     kern = {}
+    keys, filt, n_kz, kstride = E.peak_keys(gi, peaks, p)
+    n_pk = int(peaks["off"][-1])
+    ms_keys = timed(lambda: E.peak_keys(gi, peaks, p))
+    kern["peak_keys_k"] = (ms_keys, n_pk * (4 + 12 * n_kz))
     ms_k1 = timed(lambda: K.check(L.vk_k1_tiles(
         C.byref(gi.tix), C.byref(gi.fp), float(p.fragment_ppm[0]), float(p.fragment_ppm[1]), p.k1_warps,
         K.ptr(item_off), K.ptr(item_hyp), dh["n_max"], item_hyp.numel(), K.ptr(dh["spec"]), K.ptr(dh["maxfz"]),
         K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(win_off), cnt.numel(), K.ptr(peaks["off"]), K.ptr(peaks["mass"]),
         K.ptr(cnt), K.ptr(status),
         K.ptr(peaks["int"]) if pruned else None, K.ptr(peaks["tic"]) if pruned else None,
-        K.ptr(isum) if pruned else None, K.stream()), "k1_tiles"))
+        K.ptr(isum) if pruned else None, K.ptr(keys), K.ptr(filt), n_kz, kstride, K.stream()), "k1_tiles"))
     k1b = k1_algorithmic_bytes(gi, dh, peaks, win_off, item_off, item_hyp)
     if pruned:   # peak intensities per item and the window-row intensity sums
         s_it = dh["spec"][item_hyp.long()].long()

@@ -96,7 +96,10 @@ typedef struct {
  * bins.  The bin being implicit in the position, a posting is one u32 holding the rest of the key and the local
  * row: (key mod 2^(mass_bits - cbin_bits)) << row_bits | (row - tile*tile_rows), row_bits = 32 - mass_bits +
  * cbin_bits.  tile_off[n_tiles+1] (i64) locates each tile's postings (16-byte aligned, padding 0xffffffff after
- * the last bin). */
+ * the last bin).  bitmap[tile * 2^cbin_bits * 4 + ...] (u32, 16-byte aligned; vk_tindex_bitmap): the tile's presence
+ * bitmap, 128 bits per coarse bin, bit s of bin b set when a posting of bin b has (low key bits) >> (low_bits - 7)
+ * == s (low_bits = mass_bits - cbin_bits; with low_bits < 7 the low key itself); K1 drops the tolerance windows
+ * whose bits are all clear. */
 typedef struct {
   int64_t n_rows;
   int64_t n_tiles;
@@ -112,6 +115,7 @@ typedef struct {
   const int64_t* tile_off;
   const uint16_t* cbin_off;
   const uint32_t* postings;
+  const uint32_t* bitmap;
 } vk_tindex;
 
 /* Layout of a tiled index for tile_rows/fmin/fmax: fills tile_shift, row_bits, mass_bits, cbin_bits, fmin_bits,
@@ -128,6 +132,9 @@ int vk_tindex_count(const vk_tindex* ix, const vk_frag_params* fp, const int64_t
 int vk_tindex_emit(const vk_tindex* ix, const vk_frag_params* fp, const int64_t* seq_off, const uint8_t* len,
                    const uint64_t* mask, const float* mass32, const uint8_t* res, uint32_t* postings,
                    uint16_t* cbin_off, void* stream);
+/* Presence bitmaps of every tile (ix->tile_off, cbin_off and postings in place): bitmap[n_tiles * 2^cbin_bits * 4]
+ * (u32, 16-byte aligned), see vk_tindex. */
+int vk_tindex_bitmap(const vk_tindex* ix, uint32_t* bitmap, void* stream);
 
 /* Exclusive scan of n int64 values: out[0] = 0, out[i+1] = sum(in[0..i]) (out has n+1 entries; in == out+1
  * is allowed).  Uses `tmp` of vk_scan_tmp_bytes(n) bytes. */
@@ -186,13 +193,24 @@ int vk_hyp_fill(int n_spec, const uint8_t* valid, const double* precursor_mz, co
  *   vk_k1_tiles:      dense counts cnt[win_off[h] + row - lo[h]] (i32) for every window row of every hypothesis.
  * Counts equal the reference's brute force (kernels.cu:195-232): #(peak p, fragment charge z < maxfz, index
  * fragment f) with tol_bound(p*z, tol_lo) <= f <= tol_bound(p*z, tol_hi) in f32.  `status` (device i32, zeroed by
- * the caller) gets VK_STATUS_WAIT_TIMEOUT if a tile copy did not complete within the bounded wait.  `warps`
- * (1..16) per CTA, one CTA per tile.  isum (may be NULL; then pk_int and tic may be NULL too): per window row the
- * summed intensity of its matches, u32 fixed point = sum of round(intensity * 2^24 / tic[s]), for the candidate
- * pruner's features.  VK_E_TOO_LARGE if a tile and the histograms do not fit one CTA's shared memory.
+ * the caller) gets VK_STATUS_WAIT_TIMEOUT if a tile copy did not complete within the bounded wait.  `warps` (1..16)
+ * per CTA, one CTA per tile with work.  isum (may be
+ * NULL; then pk_int and tic may be NULL too): per window row the summed intensity of its matches, u32 fixed point
+ * = sum of round(intensity * 2^24 / tic[s]), for the candidate pruner's features.  VK_E_TOO_LARGE if a tile and
+ * the histograms do not fit one CTA's shared memory.
  * The buffers may be sized by bounds instead of the exact totals (no host read-back between the calls):
  * item_hyp holds item_cap entries, cnt / isum cnt_cap; items or windows that would not fit are skipped and set
- * VK_STATUS_OVERFLOW in `status` (the caller then retries with larger buffers). */
+ * VK_STATUS_OVERFLOW in `status` (the caller then retries with larger buffers).
+ * The index's tile bitmaps (ix->bitmap) are required.  pk_keys / pk_filt (may be NULL with n_kz = 0): the window
+ * keys and filter words of vk_k1_peak_keys for fragment charges 1..n_kz, plane stride kstride (pk_keys 8-byte
+ * aligned); higher charges are computed inside the kernel.  The result does not depend on them: they only save
+ * recomputing a peak's window for every tile its hypotheses cover.
+ *   vk_k1_peak_keys:  keys[(z-1)*kstride + p] = (ka, kb), two u32 per kept peak p < min(*n_peaks, kstride)
+ *                     (n_peaks: device i64, e.g. pk_off + n_spec) and charge z = 1..n_kz: the tolerance window of
+ *                     mass pk_mass[p]*z as an inclusive key range of the tiled index (key = f32bits - fmin bits),
+ *                     clamped to the fragment range; ka > kb when the window misses it.  filt[(z-1)*kstride + p]
+ *                     (u32): the window's bitmap position ga (bits 0..19) and span min(gb - ga, 4095) (bits
+ *                     20..31), 0xffffffff when the window misses the range. */
 int vk_k1_plan_count(const vk_tindex* ix, int64_t n_hyp, const int64_t* h_lo, const int64_t* h_hi,
                      int64_t* tile_items, int64_t* win_len, void* stream);
 int vk_k1_plan_fill(const vk_tindex* ix, int64_t n_hyp, const int64_t* h_lo, const int64_t* h_hi,
@@ -202,7 +220,10 @@ int vk_k1_tiles(const vk_tindex* ix, const vk_frag_params* fp, float tol_lo, flo
                 const int64_t* tile_item_off, const int32_t* item_hyp, int64_t n_hyp, int64_t item_cap,
                 const int32_t* h_spec, const int8_t* h_maxfz, const int64_t* h_lo, const int64_t* h_hi,
                 const int64_t* win_off, int64_t cnt_cap, const int64_t* pk_off, const float* pk_mass, int32_t* cnt,
-                int32_t* status, const float* pk_int, const float* tic, uint32_t* isum, void* stream);
+                int32_t* status, const float* pk_int, const float* tic, uint32_t* isum, const uint32_t* pk_keys,
+                const uint32_t* pk_filt, int n_kz, int64_t kstride, void* stream);
+int vk_k1_peak_keys(const vk_tindex* ix, const vk_frag_params* fp, float tol_lo, float tol_hi, const int64_t* n_peaks,
+                    const float* pk_mass, int n_kz, int64_t kstride, uint32_t* keys, uint32_t* filt, void* stream);
 
 /* Top-K + pair closure (reference vulcan/gpu/engine.py:284-312) per spectrum, from the dense K1 counts.
  * Spectrum s owns hypotheses [spec_hyp_off[s], spec_hyp_off[s+1]).  Per spectrum: entries with count >= thr,

@@ -258,6 +258,86 @@ def test_k1_counts_for_every_tile_layout(mini, param_sets, torch_cuda, layout):
         assert np.array_equal(out["cnt"][:n_win].cpu().numpy(), cnt), name
 
 
+@pytest.mark.parametrize("name", SETS)
+def test_k1_window_keys_precomputed_or_inline(mini, param_sets, indexes, name, torch_cuda, monkeypatch):
+    """vk_k1_peak_keys equals an f32 numpy restatement of the tolerance window (Sage bounds, clamped to the
+    fragment range), and K1's counts and intensity sums are the same whether every fragment charge's keys are
+    precomputed, some, or none (computed inside the kernel)."""
+    from vulcan.gpu import engine as E
+    l1, sp, _ = mini
+    p, gi = param_sets[name], indexes[name]
+    run = E.DeviceRun(sp, gi.dev)
+    peaks = E._k0_device(run, p, gi.dev)
+    dh = E._hyp_device(run, peaks, gi, p)
+    n_h = dh["n_max"]
+    keys, filt, n_kz, kstride = E.peak_keys(gi, peaks, p)
+    n_pk = int(peaks["off"][-1])
+    m = peaks["mass"][:n_pk].cpu().numpy().astype(np.float32)
+    kk = keys.cpu().numpy().view(np.uint32).reshape(-1, 2)
+    fb, xb = np.uint32(gi.tix.fmin_bits), np.uint32(gi.tix.fmax_bits)
+    fmin, fmax = fb.view(np.float32), xb.view(np.float32)
+    lo_t, hi_t = np.float32(p.fragment_ppm[0]), np.float32(p.fragment_ppm[1])
+    for z in range(1, n_kz + 1):
+        mz = m * np.float32(z)
+        if p.fragment_unit == "da":
+            a, bd = mz + lo_t, mz + hi_t
+        else:
+            a = mz + (mz * lo_t) / np.float32(1e6)
+            bd = mz + (mz * hi_t) / np.float32(1e6)
+        ok = (bd >= fmin) & (a <= fmax)
+        ka = np.where(a <= fmin, np.uint32(0), a.view(np.uint32) - fb)
+        kb = np.where(bd >= fmax, xb - fb, bd.view(np.uint32) - fb)
+        ka[~ok], kb[~ok] = 1, 0
+        got = kk[(z - 1) * kstride:(z - 1) * kstride + n_pk]
+        assert np.array_equal(got[:, 0], ka) and np.array_equal(got[:, 1], kb), (name, z)
+        # filter words: bitmap positions of ka and kb (span capped at 4095), 0xffffffff for a missed window
+        ix = gi.tix
+        low = ix.mass_bits - ix.cbin_bits
+        bits = min(7, low)
+        pos = lambda k: ((k >> low) << 7) | ((k & ((1 << low) - 1)) >> (low - bits))
+        ga, gb = pos(ka.astype(np.int64)), pos(kb.astype(np.int64))
+        want = (ga | (np.minimum(gb - ga, 4095) << 20)).astype(np.uint32)
+        want[~ok] = 0xffffffff
+        fw = filt.cpu().numpy().view(np.uint32)[(z - 1) * kstride:(z - 1) * kstride + n_pk]
+        assert np.array_equal(fw, want), (name, z)
+    ref = E._k1_dense(gi, dh, peaks, p, n_h, isum=True)
+    n_win = int(ref[0][-1])
+    assert n_win > 0
+    for nk in (0, 1, 3):
+        monkeypatch.setattr(E, "key_charges", lambda q, nk=nk: nk)
+        win_off, cnt, status, isum = E._k1_dense(gi, dh, peaks, p, n_h, isum=True)
+        assert int(status.item()) == 0
+        assert torch_cuda.equal(cnt[:n_win], ref[1][:n_win]), (name, nk)
+        assert torch_cuda.equal(isum[:n_win], ref[3][:n_win]), (name, nk)
+
+
+@pytest.mark.parametrize("layout", [(64, 8), (128, 9), (128, 1), (512, 11)])
+def test_tile_bitmaps_equal_numpy(mini, param_sets, torch_cuda, layout):
+    """vk_tindex_bitmap: bit (bin * 128 + posting >> (32 - bits)) of each tile is set exactly for the postings of the
+    tile (bits = min(7, low key bits)), recomputed here from the postings and the coarse-bin CSR."""
+    import dataclasses
+    from vulcan.gpu import engine as E
+    l1, _, _ = mini
+    tile_rows, cbin = layout
+    p = dataclasses.replace(param_sets["ppm"], tile_rows=tile_rows, cbin_bits=cbin)
+    gi = E.GpuIndex(l1, p, STATIC, VAR)
+    ix = gi.tix
+    nb = 1 << ix.cbin_bits
+    stride = (nb + 1 + 7) & ~7
+    bits = min(7, ix.mass_bits - ix.cbin_bits)
+    post = gi.postings.cpu().numpy().view(np.uint32)
+    toff = gi.tile_off.cpu().numpy()
+    cb = gi.cbin_off.cpu().numpy().view(np.uint16).astype(np.int64)
+    bm = gi.bitmap.cpu().numpy().view(np.uint32)
+    for t in range(ix.n_tiles):
+        c = cb[t * stride:t * stride + nb + 1]
+        pt = post[toff[t]:toff[t] + c[-1]].astype(np.int64)
+        pos = np.repeat(np.arange(nb), np.diff(c)) * 128 + (pt >> (32 - bits))
+        want = np.zeros(nb * 4, np.uint32)
+        np.bitwise_or.at(want, pos >> 5, (np.uint32(1) << (pos & 31).astype(np.uint32)))
+        assert np.array_equal(bm[t * nb * 4:(t + 1) * nb * 4], want), t
+
+
 def test_k1_buffer_bounds_hold_and_overflow_is_reported(mini, param_sets, torch_cuda):
     """K1 buffers sized by the index's window bound never overflow on real windows; buffers made too small on
     purpose are not overrun: the kernels skip what does not fit and report VK_STATUS_OVERFLOW."""
@@ -297,7 +377,7 @@ def test_k1_buffer_bounds_hold_and_overflow_is_reported(mini, param_sets, torch_
                           p.k1_warps, K.ptr(item_off), K.ptr(item_hyp), n_h, item_cap, K.ptr(dh["spec"]),
                           K.ptr(dh["maxfz"]), K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(win_off), cnt_cap,
                           K.ptr(peaks["off"]), K.ptr(peaks["mass"]), K.ptr(small), K.ptr(st), None, None, None,
-                          K.stream()), "k1_tiles")
+                          None, None, 0, 0, K.stream()), "k1_tiles")
     assert int(st.item()) & 2
     assert bool((small[cnt_cap:] == -5).all())           # nothing written past the cap
     # rows of the windows that fit hold their exact count, or the fill value where the tile's item was skipped

@@ -12,6 +12,7 @@
 #include <mutex>
 
 #include "common.cuh"
+#include "k1_impl.cuh"
 
 namespace {
 
@@ -158,6 +159,15 @@ tindex_emit_k(vk_tindex ix, vk_frag_params fpv, const int64_t* seq_off, const ui
     }
     cbin_off[t * stride + b] = (uint16_t)pos;
   }
+}
+
+// One CTA per tile: the tile's presence bitmap (128 bits per coarse bin) from its postings and coarse-bin CSR.
+__global__ void __launch_bounds__(256) tindex_bitmap_k(vk_tindex ix, uint4* bitmap) {
+  const int64_t t = blockIdx.x;
+  const int nb = 1 << ix.cbin_bits;
+  const int stride = (nb + 1 + 7) & ~7;
+  vk::k1_build_bitmap(ix.postings + ix.tile_off[t], ix.cbin_off + t * stride, nb, vk::k1_bm_bits(ix),
+                      bitmap + t * nb);
 }
 
 // ------------------------------------------------------------------------------------------ exclusive scan
@@ -316,6 +326,13 @@ int vk_tindex_emit(const vk_tindex* ix, const vk_frag_params* fp, const int64_t*
   if (e != cudaSuccess) return vk_err(e);
   tindex_emit_k<<<(unsigned)ix->n_tiles, 512, sh, (cudaStream_t)stream>>>(*ix, *fp, seq_off, len, mask, mass32, res,
                                                                           postings, cbin_off, n_pow2);
+  return vk_launch_status();
+}
+
+int vk_tindex_bitmap(const vk_tindex* ix, uint32_t* bitmap, void* stream) {
+  if (!ix || !ix->tile_off || !ix->cbin_off || !ix->postings || !bitmap || ((uintptr_t)bitmap & 15)) return VK_E_ARG;
+  if (ix->n_tiles == 0) return 0;
+  tindex_bitmap_k<<<(unsigned)ix->n_tiles, 256, 0, (cudaStream_t)stream>>>(*ix, reinterpret_cast<uint4*>(bitmap));
   return vk_launch_status();
 }
 

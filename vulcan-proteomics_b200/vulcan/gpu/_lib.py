@@ -30,7 +30,7 @@ class TIndex(C.Structure):
                 ("tile_shift", C.c_int32), ("row_bits", C.c_int32), ("mass_bits", C.c_int32),
                 ("cbin_bits", C.c_int32), ("fmin_bits", C.c_uint32), ("fmax_bits", C.c_uint32),
                 ("min_ion_index", C.c_int32), ("max_tile_postings", C.c_int32),
-                ("tile_off", P), ("cbin_off", P), ("postings", P)]
+                ("tile_off", P), ("cbin_off", P), ("postings", P), ("bitmap", P)]
 
 
 class FusedIn(C.Structure):
@@ -81,7 +81,9 @@ _SIGS_B200 = {
     "vk_hyp_fill": [I32, P, P, P, I32, I32, I32, I32, F32, F32, I32, P, I64, P, P, P, P, P, P, P, P, P, P],
     "vk_k1_plan_count": [P, I64, P, P, P, P, P],
     "vk_k1_plan_fill": [P, I64, P, P, P, P, P, I64, P, P],
-    "vk_k1_tiles": [P, P, F32, F32, I32, P, P, I64, I64, P, P, P, P, P, I64, P, P, P, P, P, P, P, P],
+    "vk_k1_tiles": [P, P, F32, F32, I32, P, P, I64, I64, P, P, P, P, P, I64, P, P, P, P, P, P, P, P, P, I32, I64, P],
+    "vk_k1_peak_keys": [P, P, F32, F32, P, P, I32, I64, P, P, P],
+    "vk_tindex_bitmap": [P, P, P],
     "vk_select_topk": [I32, P, P, P, P, P, I64, P, I32, I32, I32, I32, P, P, P, P, P, P, P, P, P],
     "vk_compact_cands": [I32, I32, P, P, P, P, P, P, P, P, P, P, P, P],
     "vk_k2_spectra": [P, I32, P, P, P, P, P, P, P, P, P, P, P, F32, F32, P, P, P, P, P, P, P, P, P, P],

@@ -21,7 +21,7 @@ from . import engine as E
 from .host import SearchParams, Spectra
 
 TILE_ROWS = (64, 128, 256)
-K1_WARPS = (4, 8, 16)
+K1_WARPS = (3, 4, 6, 8)
 PEAK_BUCKETS = (64, 128, 256, 512, 1 << 30)
 
 

@@ -141,7 +141,8 @@ class GpuIndex:
         self.build_s = time.perf_counter() - t0
         self.device_bytes = sum(t.numel() * t.element_size() for t in
                                 [self.seq_off, self.length, self.mask, self.mass32, self.residues, self.partner,
-                                 self.missed, self.n_var, self.pf_id, self.tile_off, self.cbin_off, self.postings])
+                                 self.missed, self.n_var, self.pf_id, self.tile_off, self.cbin_off, self.postings,
+                                 self.bitmap])
 
     def table_ptrs(self):
         return (K.ptr(self.seq_off), K.ptr(self.length), K.ptr(self.mask), K.ptr(self.mass32), K.ptr(self.residues))
@@ -186,6 +187,9 @@ class GpuIndex:
                                  K.ptr(self.cbin_off), K.stream()), "tindex_emit")
         ix.cbin_off = K.ptr(self.cbin_off)
         ix.postings = K.ptr(self.postings)
+        self.bitmap = torch.empty(max(nt * (1 << ix.cbin_bits) * 4, 4), dtype=torch.int32, device=d)
+        K.check(L.vk_tindex_bitmap(C.byref(ix), K.ptr(self.bitmap), K.stream()), "tindex_bitmap")
+        ix.bitmap = K.ptr(self.bitmap)
         self.tix = ix
         self.n_postings = ix.n_postings
 
@@ -382,6 +386,26 @@ def _as_dev(hyp, dev):
     return out
 
 
+def key_charges(p: SearchParams) -> int:
+    """Fragment charges whose window keys are precomputed per pass: all of them when max_fragment_charge bounds
+    them, else 1 and 2 (K1 computes higher charges itself)."""
+    mfc = p.max_fragment_charge or 0
+    return mfc if mfc > 0 else 2
+
+
+def peak_keys(gi: GpuIndex, peaks, p: SearchParams):
+    """Window keys and filter words of every kept peak (vk_k1_peak_keys): (keys, filt, n_kz, kstride), computed once
+    per pass for all the (tile, hypothesis) items of K1."""
+    n_kz = key_charges(p)
+    kstride = int(peaks["mass"].numel())
+    keys = torch.empty(max(n_kz * kstride * 2, 2), dtype=torch.int32, device=gi.dev)
+    filt = torch.empty(max(n_kz * kstride, 1), dtype=torch.int32, device=gi.dev)
+    K.check(K.lib().vk_k1_peak_keys(C.byref(gi.tix), C.byref(gi.fp), float(p.fragment_ppm[0]),
+                                    float(p.fragment_ppm[1]), K.ptr(peaks["off"][-1:]), K.ptr(peaks["mass"]), n_kz,
+                                    kstride, K.ptr(keys), K.ptr(filt), K.stream()), "k1_peak_keys")
+    return keys, filt, n_kz, kstride
+
+
 def _k1_dense(gi: GpuIndex, dh, peaks, p: SearchParams, n_hyp: int, stats: Stats | None = None,
               isum: bool = False):
     """Tiled K1: dense counts of every window row.  Returns (win_off, cnt, status), plus the summed matched
@@ -409,12 +433,14 @@ def _k1_dense(gi: GpuIndex, dh, peaks, p: SearchParams, n_hyp: int, stats: Stats
                               K.ptr(cursor), K.ptr(item_hyp), item_cap, K.ptr(status), K.stream()), "k1_plan_fill")
     cnt = torch.empty(cnt_cap, dtype=torch.int32, device=dev)
     isw = torch.empty(cnt_cap, dtype=torch.int32, device=dev) if isum else None
+    keys, filt, n_kz, kstride = peak_keys(gi, peaks, p)
     K.check(L.vk_k1_tiles(C.byref(ix), C.byref(gi.fp), float(p.fragment_ppm[0]), float(p.fragment_ppm[1]),
                           p.k1_warps, K.ptr(item_off), K.ptr(item_hyp), n_hyp, item_cap, K.ptr(dh["spec"]),
                           K.ptr(dh["maxfz"]), K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(win_off), cnt_cap,
                           K.ptr(peaks["off"]), K.ptr(peaks["mass"]), K.ptr(cnt), K.ptr(status),
                           K.ptr(peaks["int"]) if isum else None, K.ptr(peaks["tic"]) if isum else None,
-                          K.ptr(isw) if isum else None, K.stream()), "k1_tiles")
+                          K.ptr(isw) if isum else None, K.ptr(keys), K.ptr(filt), n_kz, kstride, K.stream()),
+            "k1_tiles")
     if isum:
         return win_off, cnt, status, isw
     return win_off, cnt, status

@@ -47,7 +47,7 @@ class SearchParams:
     # CTA's shared memory), coarse m/z bins per tile (0 = 2^8 per 64 rows), warps per K1 CTA
     tile_rows: int = 128
     cbin_bits: int = 0
-    k1_warps: int = 8
+    k1_warps: int = 4
     search_method: str = "staged"           # "staged" (a kernel per stage) or "fused" (one persistent kernel)
     fused_warps: int = 4                    # warps of a fused-search CTA (one spectrum at a time)
     fused_cnt_cap: int = 4096               # window rows a spectrum may span in the fused search
