@@ -211,6 +211,34 @@ def test_topk_radix_selection_path(mini, param_sets, torch_cuda):
         assert np.array_equal(out["c_cnt"][:nc].cpu().numpy(), Cc)
 
 
+@pytest.mark.parametrize("topk", (3, 60))
+def test_topk_over_shared_memory_capacity(mini, param_sets, torch_cuda, topk):
+    """Precursor windows of +-2% make some spectra append more entries than a warp keeps in shared memory (512
+    keys): their threshold comes from the radix select over the dense counts in global memory.  Candidates ==
+    oracle select_topk, with and without pair closure."""
+    from oracle import oracle as O
+    from vulcan.gpu import engine as E
+    import dataclasses
+    l1, sp, _ = mini
+    for closure in (True, False):
+        p = dataclasses.replace(param_sets["ppm"], topk=topk, precursor_ppm=(-20000.0, 20000.0),
+                                pair_closure=closure, search_method="staged")
+        gi = E.GpuIndex(l1, p, STATIC, VAR)
+        tbl, st, out = E.search(sp, gi, l1, p)
+        pk = O.k0_view(sp, p)
+        hyp = O.make_hypotheses(sp, pk["valid"], l1.mass32, p)
+        P = O.make_params(STATIC, VAR, p.fragment_unit)
+        win_off, cnt, sc, mt = O.k1_windows(l1, hyp, pk, p, P)
+        oh, orr, oc = O.k1_appended(hyp, win_off, cnt, p.k1_threshold)
+        n_app = np.bincount(np.asarray(hyp["spec"])[oh], minlength=len(sp.charge))
+        assert n_app.max() > 512 and (n_app > topk).any()
+        H, R, Cc = O.select_topk(oh, orr, oc, hyp["spec"], l1.partner, p.topk, closure)
+        nc = int(out["cand_off"][-1])
+        assert np.array_equal(out["c_hyp"][:nc].cpu().numpy(), H)
+        assert np.array_equal(out["c_row"][:nc].cpu().numpy(), R)
+        assert np.array_equal(out["c_cnt"][:nc].cpu().numpy(), Cc)
+
+
 def test_search_finds_planted_truth(mini, param_sets, indexes):
     from vulcan.gpu import engine as E
     l1, sp, fx = mini

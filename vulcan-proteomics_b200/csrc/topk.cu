@@ -3,12 +3,14 @@
 // The reference sorts every appended (hyp, row, count) of the run by a packed key
 // (spectrum, 32767 - min(count, 32767), 2^28 - 1 - row) and keeps rank < topk per spectrum, then adds partner rows
 // and merges duplicates of (spectrum, row) to the lowest hypothesis and highest count.  Here a warp reads its
-// spectrum's dense K1 counts, computes the per-hypothesis scored/matched statistics, and
-//   - if at most topk entries pass the threshold, takes them all (ballot compaction);
-//   - otherwise finds the topk-th largest 63-bit key (min(count,32767), row, -hypothesis) -- by a warp bitonic sort
-//     of the appended keys when at most 512 pass, else by an 8-bit radix select -- and keeps the keys at or above
-//     it (keys are unique, so exactly topk);
-// then appends the partners, sorts by (row, hypothesis) with a warp bitonic sort and merges duplicates.
+// spectrum's dense K1 counts once (loads unrolled), computing the per-hypothesis scored/matched statistics and
+// collecting the appended entries as unique 63-bit keys (min(count,32767), row, -hypothesis) in shared memory;
+//   - if at most topk entries pass the threshold, takes them all;
+//   - otherwise finds the topk-th largest key by an 8-bit radix select over the collected keys and keeps the keys
+//     at or above it (keys are unique, so exactly topk);
+// a spectrum with more appended entries than shared memory holds (key_cap) takes the same radix select over its
+// counts in global memory and a second read to gather.  Then it appends the partners, sorts by (row, hypothesis)
+// with a warp bitonic sort and merges duplicates.
 #include "common.cuh"
 
 namespace {
@@ -44,6 +46,51 @@ __device__ __forceinline__ void warp_bitonic_u64(uint64_t* v, int n_pow2, int la
   }
 }
 
+// Digit selection of a radix select: with hist[256] the counts of the candidates' current digit, the digit d such
+// that the candidates with a larger digit number < need <= those with digit >= d; need becomes the number still to
+// take among the candidates with digit d.
+__device__ __forceinline__ int radix_digit(const uint32_t* hist, long long& need, int lane) {
+  long long above = 0;
+  for (int d0 = 255; d0 >= 0; d0 -= 32) {
+    const int d = d0 - lane;
+    const long long v = hist[d];
+    // inclusive scan from the top digit downwards across the lanes of this group of 32 digits
+    const long long inc = vk::warp_incl_scan(v);
+    const unsigned hit = __ballot_sync(VK_FULL, above + inc >= need);
+    if (hit) {
+      const int l = __ffs(hit) - 1;
+      const long long inc_l = __shfl_sync(VK_FULL, inc, l);
+      const long long v_l = __shfl_sync(VK_FULL, v, l);
+      need -= above + inc_l - v_l;
+      return d0 - l;
+    }
+    above += __shfl_sync(VK_FULL, inc, 31);
+  }
+  return 0;
+}
+
+// The k-th largest of n unique keys in shared memory (1 <= k <= n): an 8-bit radix select, most significant
+// digit first, counting only the keys that match the digits chosen so far.
+__device__ __forceinline__ uint64_t smem_kth_largest(const uint64_t* key, int n, int k, uint32_t* hist, int lane) {
+  uint64_t prefix = 0, pmask = 0;
+  long long need = k;
+  for (int shift = 56; shift >= 0; shift -= 8) {
+    for (int i = lane; i < 256; i += 32) hist[i] = 0;
+    __syncwarp();
+    for (int i = lane; i < n; i += 32) {
+      const uint64_t v = key[i];
+      if ((v & pmask) == prefix) atomicAdd(&hist[(v >> shift) & 255], 1u);
+    }
+    __syncwarp();
+    prefix |= (uint64_t)radix_digit(hist, need, lane) << shift;
+    pmask |= 255ull << shift;
+    __syncwarp();
+  }
+  return prefix;
+}
+
+constexpr int TK_UNROLL = 4;   // count loads in flight per lane
+
 // rows of a hypothesis window, or 0 when its slice would end past the count buffer (cnt_cap entries)
 __device__ __forceinline__ int64_t win_rows(int64_t w0, int64_t lo, int64_t hi, int64_t cnt_cap) {
   const int64_t n = hi > lo ? hi - lo : 0;
@@ -70,25 +117,38 @@ select_topk_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo, cons
   const unsigned lt_mask = (1u << lane) - 1u;
 
   const int64_t hb = spec_hyp_off[s], he = spec_hyp_off[s + 1];
-  // pass A: per-hypothesis statistics and the number of appended entries
+  // one read of the counts: per-hypothesis statistics, and the appended keys into shared memory (as many as fit)
   long long n_app = 0, s_sc = 0, s_mt = 0;
   for (int64_t h = hb; h < he; ++h) {
-    const int64_t w0 = win_off[h], n = win_rows(w0, h_lo[h], h_hi[h], cnt_cap);
-    long long sc = 0, mt = 0, ap = 0;
-    for (int64_t j = lane; j < n; j += 32) {
-      int c = cnt[w0 + j];
-      sc += c > 0;
-      mt += c;
-      ap += c >= thr;
+    const int64_t w0 = win_off[h], lo = h_lo[h], n = win_rows(w0, lo, h_hi[h], cnt_cap);
+    long long sc = 0, mt = 0;
+    for (int64_t j0 = 0; j0 < n; j0 += 32 * TK_UNROLL) {
+      int c[TK_UNROLL];
+#pragma unroll
+      for (int u = 0; u < TK_UNROLL; ++u) {
+        const int64_t j = j0 + 32 * u + lane;
+        c[u] = j < n ? cnt[w0 + j] : -1;
+      }
+#pragma unroll
+      for (int u = 0; u < TK_UNROLL; ++u) {
+        const int64_t j = j0 + 32 * u + lane;
+        if (c[u] >= 0) {
+          sc += c[u] > 0;
+          mt += c[u];
+        }
+        const bool take = c[u] >= thr && j < n;
+        const unsigned m = __ballot_sync(VK_FULL, take);
+        const long long at = n_app + __popc(m & lt_mask);
+        if (take && at < key_cap) W.key[at] = sel_key(c[u], lo + j, (int)(h - hb));
+        n_app += __popc(m);
+      }
     }
     sc = vk::warp_sum(sc);
     mt = vk::warp_sum(mt);
-    ap = vk::warp_sum(ap);
     if (lane == 0) {
       hyp_scored[h] = (uint32_t)sc;
       hyp_matched[h] = (uint64_t)mt;
     }
-    n_app += ap;
     s_sc += sc;
     s_mt += mt;
   }
@@ -96,87 +156,70 @@ select_topk_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo, cons
     spec_scored[s] = s_sc;
     spec_matched[s] = s_mt;
   }
-  // threshold key: every entry with key >= kth is selected
-  uint64_t kth = 0;
+  __syncwarp();
   const bool limit = n_app > topk;
-  if (limit && n_app <= key_cap) {
-    // sort path: every appended key into shared memory, bitonic sort, the topk-th largest is the threshold
-    int n_k = 0;
-    for (int64_t h = hb; h < he; ++h) {
-      const int64_t w0 = win_off[h], lo = h_lo[h], n = win_rows(w0, lo, h_hi[h], cnt_cap);
-      for (int64_t j0 = 0; j0 < n; j0 += 32) {
-        const int64_t j = j0 + lane;
-        const int c = j < n ? cnt[w0 + j] : -1;
-        const bool take = j < n && c >= thr;
-        const unsigned m = __ballot_sync(VK_FULL, take);
-        if (take) W.key[n_k + __popc(m & lt_mask)] = sel_key(c, lo + j, (int)(h - hb));
-        n_k += __popc(m);
+  int n_sel = 0;
+  if (n_app <= key_cap) {
+    // every appended key is in shared memory: threshold (if needed) and gather from there, in collection order
+    const int n_k = (int)n_app;
+    const uint64_t kth = limit ? smem_kth_largest(W.key, n_k, topk, W.hist, lane) : 0ull;
+    for (int i0 = 0; i0 < n_k; i0 += 32) {
+      const int i = i0 + lane;
+      const uint64_t k = i < n_k ? W.key[i] : 0ull;
+      const bool take = i < n_k && (!limit || k >= kth);
+      const unsigned m = __ballot_sync(VK_FULL, take);
+      if (take) {
+        const int pos = n_sel + __popc(m & lt_mask);
+        const int hl = (1 << 18) - 1 - (int)(k & 0x3ffff);
+        const int64_t row = (int64_t)((k >> 18) & 0x3fffffffull);
+        int c = (int)(k >> 48);
+        if (c >= 32767) {   // the key holds min(count, 32767): the exact count from the dense slice
+          const int64_t h = hb + hl;
+          c = cnt[win_off[h] + (row - h_lo[h])];
+        }
+        W.row[pos] = (int32_t)row;
+        W.hl[pos] = hl;
+        W.cnt[pos] = c;
       }
+      n_sel += __popc(m);
     }
-    int n_pow2 = 32;
-    while (n_pow2 < n_k) n_pow2 <<= 1;
-    for (int i = n_k + lane; i < n_pow2; i += 32) W.key[i] = 0ull;   // smaller than every real key
-    __syncwarp();
-    warp_bitonic_u64(W.key, n_pow2, lane);
-    kth = W.key[n_pow2 - topk];
-    __syncwarp();
-  } else if (limit) {
+  } else {
+    // more appended entries than shared memory holds: radix select over the dense counts, then a second read
     uint64_t prefix = 0, pmask = 0;
-    long long need = topk;   // how many still to take from the entries matching prefix
+    long long need = topk;
     for (int shift = 56; shift >= 0; shift -= 8) {
       for (int i = lane; i < 256; i += 32) W.hist[i] = 0;
       __syncwarp();
       for (int64_t h = hb; h < he; ++h) {
         const int64_t w0 = win_off[h], lo = h_lo[h], n = win_rows(w0, lo, h_hi[h], cnt_cap);
         for (int64_t j = lane; j < n; j += 32) {
-          int c = cnt[w0 + j];
+          const int c = cnt[w0 + j];
           if (c < thr) continue;
-          uint64_t k = sel_key(c, lo + j, (int)(h - hb));
+          const uint64_t k = sel_key(c, lo + j, (int)(h - hb));
           if ((k & pmask) == prefix) atomicAdd(&W.hist[(k >> shift) & 255], 1u);
         }
       }
       __syncwarp();
-      // digit d from the top such that the entries with digit > d number < need <= those with digit >= d
-      long long above = 0;
-      int dsel = 0;
-      for (int d0 = 255; d0 >= 0; d0 -= 32) {
-        int d = d0 - lane;
-        long long v = W.hist[d];
-        // inclusive scan from the top digit downwards across the lanes of this group of 32 digits
-        long long inc = vk::warp_incl_scan(v);
-        unsigned hit = __ballot_sync(VK_FULL, above + inc >= need);
-        if (hit) {
-          int l = __ffs(hit) - 1;
-          long long inc_l = __shfl_sync(VK_FULL, inc, l);
-          long long v_l = __shfl_sync(VK_FULL, v, l);
-          dsel = d0 - l;
-          need -= above + inc_l - v_l;
-          break;
-        }
-        above += __shfl_sync(VK_FULL, inc, 31);
-      }
-      prefix |= (uint64_t)dsel << shift;
+      prefix |= (uint64_t)radix_digit(W.hist, need, lane) << shift;
       pmask |= 255ull << shift;
       __syncwarp();
     }
-    kth = prefix;
-  }
-  // gather the selected entries (ballot compaction, order: hypothesis, row)
-  int n_sel = 0;
-  for (int64_t h = hb; h < he; ++h) {
-    const int64_t w0 = win_off[h], lo = h_lo[h], n = win_rows(w0, lo, h_hi[h], cnt_cap);
-    for (int64_t j0 = 0; j0 < n; j0 += 32) {
-      const int64_t j = j0 + lane;
-      int c = j < n ? cnt[w0 + j] : -1;
-      bool take = j < n && c >= thr && (!limit || sel_key(c, lo + j, (int)(h - hb)) >= kth);
-      unsigned m = __ballot_sync(VK_FULL, take);
-      if (take) {
-        int pos = n_sel + __popc(m & lt_mask);
-        W.row[pos] = (int32_t)(lo + j);
-        W.hl[pos] = (int32_t)(h - hb);
-        W.cnt[pos] = c;
+    const uint64_t kth = prefix;
+    for (int64_t h = hb; h < he; ++h) {
+      const int64_t w0 = win_off[h], lo = h_lo[h], n = win_rows(w0, lo, h_hi[h], cnt_cap);
+      for (int64_t j0 = 0; j0 < n; j0 += 32) {
+        const int64_t j = j0 + lane;
+        const int c = j < n ? cnt[w0 + j] : -1;
+        const bool take = j < n && c >= thr && sel_key(c, lo + j, (int)(h - hb)) >= kth;
+        const unsigned m = __ballot_sync(VK_FULL, take);
+        if (take) {
+          const int pos = n_sel + __popc(m & lt_mask);
+          W.row[pos] = (int32_t)(lo + j);
+          W.hl[pos] = (int32_t)(h - hb);
+          W.cnt[pos] = c;
+        }
+        n_sel += __popc(m);
       }
-      n_sel += __popc(m);
     }
   }
   __syncwarp();
