@@ -576,14 +576,21 @@ def _kernel_table(a, p, gi, run, flush, pr, dev):
                                if pr.tensor_cores == "tcgen05" else "mma.sync m16n8k16 bf16 (fp32 accumulate)")}
     n_cand = int(so["cand_off"][-1])
     k2o = E._k2_outputs(max(n_cand, 1), dev)
-    ms_k2 = timed(lambda: K.check(L.vk_k2_spectra(
-        C.byref(gi.fp), n, K.ptr(so["cand_off"]), K.ptr(so["c_row32"]), K.ptr(so["c_maxfz"]), K.ptr(peaks["off"]),
-        K.ptr(peaks["mass"]), K.ptr(peaks["int"]), *gi.table_ptrs(), float(p.fragment_ppm[0]),
-        float(p.fragment_ppm[1]), None, *E._k2_ptrs(k2o), K.stream()), "k2_spectra"))
+    k2_args = (C.byref(gi.fp), n, K.ptr(so["cand_off"]), K.ptr(so["c_row32"]), K.ptr(so["c_maxfz"]),
+               K.ptr(peaks["off"]), K.ptr(peaks["mass"]), K.ptr(peaks["int"]), *gi.table_ptrs(),
+               float(p.fragment_ppm[0]), float(p.fragment_ppm[1]))
     rows = so["c_row"][:n_cand]
     npk = (peaks["off"][1:n + 1] - peaks["off"][:n]).clamp(max=512)
     k2_bytes = int(((21 + gi.length[rows].long() + 5 + 28).sum() + npk.sum() * 8 + n * 16).item())
-    kern["k2_spectra_k"] = (ms_k2, k2_bytes)
+    # the path's K2 (thread per candidate after the pruner, warp per spectrum otherwise) and the other for reference
+    ms_sp = timed(lambda: K.check(L.vk_k2_spectra(*k2_args, None, *E._k2_ptrs(k2o), K.stream()), "k2_spectra"))
+    ms_cd = timed(lambda: K.check(L.vk_k2_cands(*k2_args, *E._k2_ptrs(k2o), K.stream()), "k2_cands"))
+    if pruned:
+        kern["k2_cands_k"] = (ms_cd, k2_bytes)
+        kern["k2_spectra_k (not used on this path)"] = (ms_sp, k2_bytes)
+    else:
+        kern["k2_spectra_k"] = (ms_sp, k2_bytes)
+        kern["k2_cands_k (not used on this path)"] = (ms_cd, k2_bytes)
     if p.search_method == "fused" and not pruned:
         kern = {"fused_search_k": (timed(lambda: E._fused_device(gi, p, 1, peaks, dh, run.n)),
                                    fused_algorithmic_bytes(gi, dh, peaks, E._fused_device(gi, p, 1, peaks, dh, run.n,

@@ -254,6 +254,15 @@ int vk_k2_spectra(const vk_frag_params* fp, int n_spec, const int64_t* cand_off,
                   const uint8_t* res, float tol_lo, float tol_hi, const float* c_shift, double* o_hs, float* o_sb,
                   float* o_sy, float* o_ppm, int16_t* o_mb, int16_t* o_my, int16_t* o_lb, int16_t* o_ly,
                   void* stream);
+/* vk_k2_spectra without the shift, one thread per candidate (grid-stride over cand_off[n_spec] candidates, the
+ * spectrum found by binary search of cand_off) with the peaks read in global memory: for sparse candidate lists (a
+ * few per spectrum, e.g. after the learned pruner), where a warp per spectrum would leave most lanes idle.  Same
+ * outputs, bit for bit. */
+int vk_k2_cands(const vk_frag_params* fp, int n_spec, const int64_t* cand_off, const int32_t* c_row,
+                const int8_t* c_maxfz, const int64_t* pk_off, const float* pk_mass, const float* pk_int,
+                const int64_t* seq_off, const uint8_t* len, const uint64_t* mask, const float* mass32,
+                const uint8_t* res, float tol_lo, float tol_hi, double* o_hs, float* o_sb, float* o_sy, float* o_ppm,
+                int16_t* o_mb, int16_t* o_my, int16_t* o_lb, int16_t* o_ly, void* stream);
 
 /* PSM ranking (reference vulcan/gpu/engine.py:366-392): per spectrum, candidates with matched_b + matched_y >=
  * min_matched ranked by (hyperscore desc, row asc); the first `report` go to slots [s*report, ...): psm_cand (i64,

@@ -211,6 +211,28 @@ def test_topk_radix_selection_path(mini, param_sets, torch_cuda):
         assert np.array_equal(out["c_cnt"][:nc].cpu().numpy(), Cc)
 
 
+@pytest.mark.parametrize("name", SETS)
+def test_k2_candidate_parallel_equals_warp_per_spectrum(mini, param_sets, indexes, name, torch_cuda):
+    """vk_k2_cands (a thread per candidate, peaks read in global memory) == vk_k2_spectra (a warp per spectrum,
+    staged peaks, bucket table) bit for bit on the exhaustive path's candidate lists."""
+    import dataclasses
+    from vulcan.gpu import engine as E
+    l1, sp, _ = mini
+    p = dataclasses.replace(param_sets[name], search_method="staged")
+    gi = indexes[name]
+    st = E.Stats()
+    out = E._search_device(E.DeviceRun(sp, gi.dev, st), gi, p, 3, st)
+    E.check_status(out["status"])
+    cand = {k: out[k] for k in ("cand_off", "c_row32", "c_maxfz", "cap")}
+    k2 = E._k2_cands(gi, p, len(sp.charge), cand, out["peaks"], sparse=True)
+    nc = int(out["cand_off"][-1])
+    assert nc > 0
+    for key in out["k2"]:
+        a, b = out["k2"][key][:nc], k2[key][:nc]
+        assert torch_cuda.equal(a, b) or (a.is_floating_point() and torch_cuda.equal(a.isnan(), b.isnan()) and
+                                          torch_cuda.equal(a[~a.isnan()], b[~b.isnan()])), (name, key)
+
+
 @pytest.mark.parametrize("topk", (3, 60))
 def test_topk_over_shared_memory_capacity(mini, param_sets, torch_cuda, topk):
     """Precursor windows of +-2% make some spectra append more entries than a warp keeps in shared memory (512

@@ -95,8 +95,25 @@ __device__ __forceinline__ PeakTable build_table(const float* sm, const float* s
   return t;
 }
 
-template <bool SHIFT>
-__device__ __forceinline__ void k2_score(const SmemFrag& fp, const PeakTable& pt, int r,
+// A spectrum's mass-sorted peaks read where they lie (global memory); first_ge is the lower bound by binary search,
+// the index the bucket table also finds.  For candidate-parallel scoring of sparse candidate lists.
+struct GlobalPeaks {
+  const float* sm;
+  const float* si;
+  int np;
+
+  __device__ __forceinline__ int first_ge(float a) const {
+    int lo = 0, hi = np;
+    while (lo < hi) {
+      const int m = (lo + hi) >> 1;
+      if (__ldg(sm + m) < a) lo = m + 1; else hi = m;
+    }
+    return lo;
+  }
+};
+
+template <bool SHIFT, class PT>
+__device__ __forceinline__ void k2_score(const SmemFrag& fp, const PT& pt, int r,
                                          int maxfz, const int64_t* seq_off, const uint8_t* len,
                                          const uint64_t* mask, const float* mass32, const uint8_t* res,
                                          float tol_lo, float tol_hi, float shift, const K2Out& out, int64_t c) {
@@ -134,7 +151,7 @@ __device__ __forceinline__ void k2_score(const SmemFrag& fp, const PeakTable& pt
           int best_a = -1;
           float mx_a = 0.f;
           float base = alt == 0 ? cum : __fadd_rn(cum, shift);
-          float mz = __fdiv_rn(base, (float)z);
+          float mz = z == 1 ? base : __fdiv_rn(base, (float)z);   // x / 1 == x exactly
           float a = tol_bound(mz, tol_lo, da), bd = tol_bound(mz, tol_hi, da);
           for (int j = pt.first_ge(a); j < np && sm[j] <= bd; ++j) {
             float it = si[j];
@@ -220,7 +237,8 @@ __device__ __forceinline__ void k2_body(const SmemFrag& fp, int n_spec, const in
     int64_t c1 = cand_off[bs + 1];
     for (int64_t c = cand_off[bs] + lane; c < c1; c += 32) {
       float shift = SHIFT ? c_shift[c] : 0.f;
-      k2_score<SHIFT>(fp, pt, c_row[c], c_maxfz[c], seq_off, len, mask, mass32, res, tol_lo, tol_hi, shift, out, c);
+      k2_score<SHIFT, PeakTable>(fp, pt, c_row[c], c_maxfz[c], seq_off, len, mask, mass32, res, tol_lo, tol_hi,
+                                 shift, out, c);
     }
   }
 }

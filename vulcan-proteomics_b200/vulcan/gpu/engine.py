@@ -688,15 +688,20 @@ def _compact(n: int, cap: int, n_cand, s_hyp, s_row, s_cnt, dh, dev):
             "c_maxfz": c_maxfz, "cap": cap, "n_cand": n_cand}
 
 
-def _k2_cands(gi: GpuIndex, p: SearchParams, n: int, cand, peaks):
-    """K2 (``vk_k2_spectra``) over compacted candidate lists; one output row per candidate."""
+def _k2_cands(gi: GpuIndex, p: SearchParams, n: int, cand, peaks, sparse: bool = False):
+    """K2 over compacted candidate lists; one output row per candidate.  Dense lists (the exhaustive path's top-k
+    per spectrum): ``vk_k2_spectra``, a warp per spectrum over its staged peaks; sparse lists (a few candidates per
+    spectrum after the pruner): ``vk_k2_cands``, a thread per candidate.  Same outputs."""
     L = K.lib()
     dev = gi.dev
     k2 = _k2_outputs(max(n * cand["cap"], 1), dev)
-    K.check(L.vk_k2_spectra(C.byref(gi.fp), n, K.ptr(cand["cand_off"]), K.ptr(cand["c_row32"]),
-                            K.ptr(cand["c_maxfz"]), K.ptr(peaks["off"]), K.ptr(peaks["mass"]), K.ptr(peaks["int"]),
-                            *gi.table_ptrs(), float(p.fragment_ppm[0]), float(p.fragment_ppm[1]), None,
-                            *_k2_ptrs(k2), K.stream()), "k2_spectra")
+    common = (C.byref(gi.fp), n, K.ptr(cand["cand_off"]), K.ptr(cand["c_row32"]), K.ptr(cand["c_maxfz"]),
+              K.ptr(peaks["off"]), K.ptr(peaks["mass"]), K.ptr(peaks["int"]), *gi.table_ptrs(),
+              float(p.fragment_ppm[0]), float(p.fragment_ppm[1]))
+    if sparse:
+        K.check(L.vk_k2_cands(*common, *_k2_ptrs(k2), K.stream()), "k2_cands")
+    else:
+        K.check(L.vk_k2_spectra(*common, None, *_k2_ptrs(k2), K.stream()), "k2_spectra")
     return k2
 
 

@@ -294,7 +294,7 @@ def _pruned_device(run: E.DeviceRun, gi: E.GpuIndex, p: SearchParams, pr: Pruner
                                    K.ptr(s_row), K.ptr(s_cnt), K.ptr(n_cand), K.stream()), "select_pruned")
         cand = E._compact(n, cap, n_cand, s_hyp, s_row, s_cnt, f["dh"], dev)
     with phase("k2"):
-        k2 = E._k2_cands(gi, p, n, cand, f["peaks"])
+        k2 = E._k2_cands(gi, p, n, cand, f["peaks"], sparse=True)
     with phase("rank"):
         psm = E._rank_device(n, cand["cand_off"], cand["c_row"], k2, p, report, dev)
     return {**f, **cand, "logit": logit, "feat": feat, "k2": k2, "psm": psm}
