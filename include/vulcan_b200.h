@@ -96,10 +96,11 @@ typedef struct {
  * bins.  The bin being implicit in the position, a posting is one u32 holding the rest of the key and the local
  * row: (key mod 2^(mass_bits - cbin_bits)) << row_bits | (row - tile*tile_rows), row_bits = 32 - mass_bits +
  * cbin_bits.  tile_off[n_tiles+1] (i64) locates each tile's postings (16-byte aligned, padding 0xffffffff after
- * the last bin).  bitmap[tile * 2^cbin_bits * 4 + ...] (u32, 16-byte aligned; vk_tindex_bitmap): the tile's presence
- * bitmap, 128 bits per coarse bin, bit s of bin b set when a posting of bin b has (low key bits) >> (low_bits - 7)
- * == s (low_bits = mass_bits - cbin_bits; with low_bits < 7 the low key itself); K1 drops the tolerance windows
- * whose bits are all clear. */
+ * the last bin).  bitmap (u32, 16-byte aligned; vk_tindex_bitmap, vk_tindex_bitmap_bytes): each tile's presence
+ * bitmap, 2^B bits per coarse bin (B = 6 in this build), the words of tile t's bin b at (t * 2^cbin_bits + b) *
+ * 2^B / 32; bit s of bin b is set when a posting of bin b has (low key bits) >> (low_bits - B) == s (low_bits =
+ * mass_bits - cbin_bits; with low_bits < B the low key itself); K1 drops the tolerance windows whose bits are all
+ * clear. */
 typedef struct {
   int64_t n_rows;
   int64_t n_tiles;
@@ -132,9 +133,10 @@ int vk_tindex_count(const vk_tindex* ix, const vk_frag_params* fp, const int64_t
 int vk_tindex_emit(const vk_tindex* ix, const vk_frag_params* fp, const int64_t* seq_off, const uint8_t* len,
                    const uint64_t* mask, const float* mass32, const uint8_t* res, uint32_t* postings,
                    uint16_t* cbin_off, void* stream);
-/* Presence bitmaps of every tile (ix->tile_off, cbin_off and postings in place): bitmap[n_tiles * 2^cbin_bits * 4]
- * (u32, 16-byte aligned), see vk_tindex. */
+/* Presence bitmaps of every tile (ix->tile_off, cbin_off and postings in place) into bitmap (u32, 16-byte aligned,
+ * vk_tindex_bitmap_bytes(ix) bytes), see vk_tindex. */
 int vk_tindex_bitmap(const vk_tindex* ix, uint32_t* bitmap, void* stream);
+int64_t vk_tindex_bitmap_bytes(const vk_tindex* ix);
 
 /* Exclusive scan of n int64 values: out[0] = 0, out[i+1] = sum(in[0..i]) (out has n+1 entries; in == out+1
  * is allowed).  Uses `tmp` of vk_scan_tmp_bytes(n) bytes. */

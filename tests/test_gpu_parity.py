@@ -343,8 +343,9 @@ def test_k1_window_keys_precomputed_or_inline(mini, param_sets, indexes, name, t
         # filter words: bitmap positions of ka and kb (span capped at 4095), 0xffffffff for a missed window
         ix = gi.tix
         low = ix.mass_bits - ix.cbin_bits
-        bits = min(7, low)
-        pos = lambda k: ((k >> low) << 7) | ((k & ((1 << low) - 1)) >> (low - bits))
+        blog = _bitmap_log(gi)
+        bits = min(blog, low)
+        pos = lambda k: ((k >> low) << blog) | ((k & ((1 << low) - 1)) >> (low - bits))
         ga, gb = pos(ka.astype(np.int64)), pos(kb.astype(np.int64))
         want = (ga | (np.minimum(gb - ga, 4095) << 20)).astype(np.uint32)
         want[~ok] = 0xffffffff
@@ -361,10 +362,21 @@ def test_k1_window_keys_precomputed_or_inline(mini, param_sets, indexes, name, t
         assert torch_cuda.equal(isum[:n_win], ref[3][:n_win]), (name, nk)
 
 
+def _bitmap_log(gi):
+    """log2 of the presence-bitmap bits per coarse bin of the library build."""
+    import ctypes as C
+    from vulcan.gpu import _lib as K
+    total = int(K.lib().vk_tindex_bitmap_bytes(C.byref(gi.tix)))
+    per_bin = total * 8 // (gi.tix.n_tiles << gi.tix.cbin_bits)
+    assert per_bin in (64, 128)
+    return per_bin.bit_length() - 1
+
+
 @pytest.mark.parametrize("layout", [(64, 8), (128, 9), (128, 1), (512, 11)])
 def test_tile_bitmaps_equal_numpy(mini, param_sets, torch_cuda, layout):
-    """vk_tindex_bitmap: bit (bin * 128 + posting >> (32 - bits)) of each tile is set exactly for the postings of the
-    tile (bits = min(7, low key bits)), recomputed here from the postings and the coarse-bin CSR."""
+    """vk_tindex_bitmap: bit (bin * 2^B + posting >> (32 - bits)) of each tile is set exactly for the postings of the
+    tile (B = the build's bits-per-bin log, bits = min(B, low key bits)), recomputed here from the postings and the
+    coarse-bin CSR."""
     import dataclasses
     from vulcan.gpu import engine as E
     l1, _, _ = mini
@@ -374,7 +386,9 @@ def test_tile_bitmaps_equal_numpy(mini, param_sets, torch_cuda, layout):
     ix = gi.tix
     nb = 1 << ix.cbin_bits
     stride = (nb + 1 + 7) & ~7
-    bits = min(7, ix.mass_bits - ix.cbin_bits)
+    blog = _bitmap_log(gi)
+    words = (1 << blog) // 32
+    bits = min(blog, ix.mass_bits - ix.cbin_bits)
     post = gi.postings.cpu().numpy().view(np.uint32)
     toff = gi.tile_off.cpu().numpy()
     cb = gi.cbin_off.cpu().numpy().view(np.uint16).astype(np.int64)
@@ -382,10 +396,10 @@ def test_tile_bitmaps_equal_numpy(mini, param_sets, torch_cuda, layout):
     for t in range(ix.n_tiles):
         c = cb[t * stride:t * stride + nb + 1]
         pt = post[toff[t]:toff[t] + c[-1]].astype(np.int64)
-        pos = np.repeat(np.arange(nb), np.diff(c)) * 128 + (pt >> (32 - bits))
-        want = np.zeros(nb * 4, np.uint32)
+        pos = (np.repeat(np.arange(nb), np.diff(c)) << blog) + (pt >> (32 - bits))
+        want = np.zeros(nb * words, np.uint32)
         np.bitwise_or.at(want, pos >> 5, (np.uint32(1) << (pos & 31).astype(np.uint32)))
-        assert np.array_equal(bm[t * nb * 4:(t + 1) * nb * 4], want), t
+        assert np.array_equal(bm[t * nb * words:(t + 1) * nb * words], want), t
 
 
 def test_k1_buffer_bounds_hold_and_overflow_is_reported(mini, param_sets, torch_cuda):

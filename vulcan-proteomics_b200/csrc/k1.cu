@@ -1,7 +1,7 @@
 // K1 shared-peak counting on the tiled fragment index.
 //
 // Work items are (tile, hypothesis) pairs grouped by tile.  One CTA owns one tile: thread 0 stages the tile's
-// postings, its coarse-bin CSR and its presence bitmap (128 bits per coarse bin) into shared memory with three bulk
+// postings, its coarse-bin CSR and its presence bitmap (a few bits per coarse bin) into shared memory with three bulk
 // (TMA) copies completing on one mbarrier; then each warp takes the tile's hypotheses in turn (k1_impl.cuh,
 // k1_item_filtered): lanes stride over the spectrum's peaks x fragment charges, read each tolerance window's filter
 // word (computed once per pass by vk_k1_peak_keys), drop the windows whose bitmap bits are clear, and search the rest
@@ -109,21 +109,21 @@ k1_tiles_k(vk_tindex ix, float tol_lo, float tol_hi, int tol_da, int post_cap, c
   const int stride = (nb + 1 + 7) & ~7;
   uint32_t* post = reinterpret_cast<uint32_t*>(k1_smem);
   uint16_t* cb = reinterpret_cast<uint16_t*>(k1_smem + (size_t)post_cap * 4);
-  uint4* bm = reinterpret_cast<uint4*>(k1_smem + (size_t)post_cap * 4 + (size_t)stride * 2);
-  uint32_t* hist = reinterpret_cast<uint32_t*>(bm + nb);
+  uint32_t* bm = reinterpret_cast<uint32_t*>(k1_smem + (size_t)post_cap * 4 + (size_t)stride * 2);
+  uint32_t* hist = bm + nb * vk::K1_BM_WORDS;
   uint32_t* queue = hist + n_warps * T;   // per warp K1_QUEUE entries
   uint32_t* ihist = queue + n_warps * vk::K1_QUEUE;   // per warp T intensity sums (pruner features only)
   const int64_t po = ix.tile_off[t];
   const uint32_t post_bytes = (uint32_t)((ix.tile_off[t + 1] - po) * 4);
   const uint32_t cb_bytes = (uint32_t)stride * 2;
-  const uint32_t bm_bytes = (uint32_t)nb * 16;
+  const uint32_t bm_bytes = (uint32_t)nb * vk::K1_BM_WORDS * 4;
   if (threadIdx.x == 0) {
     vk::mbar_init(&bar, 1);
     vk::fence_mbar_init();
     vk::mbar_expect_tx(&bar, post_bytes + cb_bytes + bm_bytes);
     if (post_bytes) vk::bulk_g2s(post, ix.postings + po, post_bytes, &bar);
     vk::bulk_g2s(cb, ix.cbin_off + t * stride, cb_bytes, &bar);
-    vk::bulk_g2s(bm, ix.bitmap + t * nb * 4, bm_bytes, &bar);
+    vk::bulk_g2s(bm, ix.bitmap + t * nb * vk::K1_BM_WORDS, bm_bytes, &bar);
   }
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint32_t* qw = queue + warp * vk::K1_QUEUE;
@@ -156,7 +156,7 @@ k1_tiles_k(vk_tindex ix, float tol_lo, float tol_hi, int tol_da, int post_cap, c
         if (iw) iw[q] = 0;
       }
       __syncwarp();
-      vk::k1_item_filtered(post, cb, reinterpret_cast<const uint32_t*>(bm), hw, iw, rlo, rhi, r.p0, r.p0 + r.n,
+      vk::k1_item_filtered(post, cb, bm, hw, iw, rlo, rhi, r.p0, r.p0 + r.n,
                            r.mfz, pk_keys, pk_filt, n_kz, kstride, pk_mass, tol_lo, tol_hi, tol_da, ix, lane, qw,
                            pk_int, r.ws);
       __syncwarp();
@@ -234,7 +234,7 @@ int vk_k1_tiles(const vk_tindex* ix, const vk_frag_params* fp, float tol_lo, flo
   const int nb = 1 << ix->cbin_bits;
   const int stride = (nb + 1 + 7) & ~7;
   if (isum && (!pk_int || !tic)) return VK_E_ARG;
-  const size_t sh = (size_t)ix->max_tile_postings * 4 + (size_t)stride * 2 + (size_t)nb * 16 +
+  const size_t sh = (size_t)ix->max_tile_postings * 4 + (size_t)stride * 2 + (size_t)nb * vk::K1_BM_WORDS * 4 +
                     (size_t)warps * (T * 4 * (isum ? 2 : 1) + vk::K1_QUEUE * 4);
   if (sh > 200 * 1024) return VK_E_TOO_LARGE;
   cudaError_t e = cudaFuncSetAttribute(k1_tiles_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);

@@ -11,7 +11,14 @@
 #pragma once
 #include "common.cuh"
 
+#ifndef K1_BM_LOG
+#define K1_BM_LOG 6            // log2 of the presence-bitmap bits per coarse bin (6 or 7)
+#endif
+static_assert(K1_BM_LOG == 6 || K1_BM_LOG == 7, "64 or 128 bitmap bits per coarse bin");
+
 namespace vk {
+
+constexpr int K1_BM_WORDS = (1 << K1_BM_LOG) / 32;   // u32 words of a coarse bin's bitmap
 
 // cnt[hoff + l] is the count of tile row l (rows rlo <= l < rhi only).  With isum != nullptr, every match also adds
 // the peak's weight round(intensity * wscale) (u32, wscale = 2^24 / TIC of the spectrum) to isum[hoff + l]: the
@@ -67,8 +74,8 @@ __device__ __forceinline__ void k1_item_per_peak(const uint32_t* post, const uin
 // The tolerance window of a peak does not depend on the tile, so its key range is computed once per pass
 // (k1_window_keys, by vk_k1_peak_keys) instead of once per (tile, hypothesis) item, together with a 32-bit filter
 // word (k1_filter_word).  Every tile has a presence bitmap, built with the index (vk_tindex_bitmap) and staged with
-// the tile: 128 bits per coarse bin, bit s of bin b set when a posting of the bin has (low key) >> (low_bits - 7)
-// == s.  A window whose bits are all clear holds no posting and is dropped after one shared-memory word; the
+// the tile: 2^K1_BM_LOG bits per coarse bin, bit s of bin b set when a posting of the bin has (low key) >>
+// (low_bits - K1_BM_LOG) == s.  A window whose bits are all clear holds no posting and is dropped after one shared-memory word; the
 // windows that may match are compacted into a per-warp queue (ballot) and searched exactly, one per lane, so the
 // bin lookup and binary search run with every lane busy and only for them.  The counts are those of
 // k1_item_per_peak: the bitmap only skips windows that hold no posting.
@@ -86,20 +93,22 @@ __device__ __forceinline__ uint2 k1_window_keys(float pm, int z, float tol_lo, f
   return make_uint2(ka, kb);
 }
 
-// Bits per coarse bin actually used: 2^min(7, low_bits); a posting's bit is its top bits (row_bits + low_bits = 32).
+// Bits per coarse bin actually used: 2^min(K1_BM_LOG, low_bits); a posting's bit is its top bits (row_bits +
+// low_bits = 32).
 __device__ __forceinline__ int k1_bm_bits(const vk_tindex& ix) {
   const int low_bits = ix.mass_bits - ix.cbin_bits;
-  return low_bits < 7 ? low_bits : 7;
+  return low_bits < K1_BM_LOG ? low_bits : K1_BM_LOG;
 }
 
-// Bitmap position of key k: bin * 128 + (low key >> (low_bits - bits)); monotone in k, below 2^(cbin_bits + 7).
+// Bitmap position of key k: bin * 2^K1_BM_LOG + (low key >> (low_bits - bits)); monotone in k, below
+// 2^(cbin_bits + K1_BM_LOG).
 __device__ __forceinline__ uint32_t k1_bm_pos(uint32_t k, int low_bits, int bshift) {
-  return ((k >> low_bits) << 7) | ((k & ((1u << low_bits) - 1u)) >> bshift);
+  return ((k >> low_bits) << K1_BM_LOG) | ((k & ((1u << low_bits) - 1u)) >> bshift);
 }
 
-// One thread per coarse bin builds the bin's four words in registers (the index build calls this per tile).
+// One thread per coarse bin builds the bin's K1_BM_WORDS words in registers (the index build calls this per tile).
 __device__ __forceinline__ void k1_build_bitmap(const uint32_t* post, const uint16_t* cb, int nb, int bits,
-                                                uint4* bm) {
+                                                uint32_t* bm) {
   const int top = 32 - bits;
   for (int b = threadIdx.x; b < nb; b += blockDim.x) {
     unsigned long long lo = 0ull, hi = 0ull;
@@ -108,7 +117,13 @@ __device__ __forceinline__ void k1_build_bitmap(const uint32_t* post, const uint
       const uint32_t s = post[e] >> top;
       if (s < 64u) lo |= 1ull << s; else hi |= 1ull << (s - 64u);
     }
-    bm[b] = make_uint4((uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)hi, (uint32_t)(hi >> 32));
+    uint32_t* w = bm + (size_t)b * K1_BM_WORDS;
+    w[0] = (uint32_t)lo;
+    w[1] = (uint32_t)(lo >> 32);
+    if (K1_BM_WORDS == 4) {
+      w[2] = (uint32_t)hi;
+      w[3] = (uint32_t)(hi >> 32);
+    }
   }
 }
 

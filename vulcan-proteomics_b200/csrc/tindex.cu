@@ -161,13 +161,14 @@ tindex_emit_k(vk_tindex ix, vk_frag_params fpv, const int64_t* seq_off, const ui
   }
 }
 
-// One CTA per tile: the tile's presence bitmap (128 bits per coarse bin) from its postings and coarse-bin CSR.
-__global__ void __launch_bounds__(256) tindex_bitmap_k(vk_tindex ix, uint4* bitmap) {
+// One CTA per tile: the tile's presence bitmap (2^K1_BM_LOG bits per coarse bin) from its postings and coarse-bin
+// CSR.
+__global__ void __launch_bounds__(256) tindex_bitmap_k(vk_tindex ix, uint32_t* bitmap) {
   const int64_t t = blockIdx.x;
   const int nb = 1 << ix.cbin_bits;
   const int stride = (nb + 1 + 7) & ~7;
   vk::k1_build_bitmap(ix.postings + ix.tile_off[t], ix.cbin_off + t * stride, nb, vk::k1_bm_bits(ix),
-                      bitmap + t * nb);
+                      bitmap + t * nb * vk::K1_BM_WORDS);
 }
 
 // ------------------------------------------------------------------------------------------ exclusive scan
@@ -332,8 +333,13 @@ int vk_tindex_emit(const vk_tindex* ix, const vk_frag_params* fp, const int64_t*
 int vk_tindex_bitmap(const vk_tindex* ix, uint32_t* bitmap, void* stream) {
   if (!ix || !ix->tile_off || !ix->cbin_off || !ix->postings || !bitmap || ((uintptr_t)bitmap & 15)) return VK_E_ARG;
   if (ix->n_tiles == 0) return 0;
-  tindex_bitmap_k<<<(unsigned)ix->n_tiles, 256, 0, (cudaStream_t)stream>>>(*ix, reinterpret_cast<uint4*>(bitmap));
+  tindex_bitmap_k<<<(unsigned)ix->n_tiles, 256, 0, (cudaStream_t)stream>>>(*ix, bitmap);
   return vk_launch_status();
+}
+
+int64_t vk_tindex_bitmap_bytes(const vk_tindex* ix) {
+  if (!ix) return -1;
+  return ix->n_tiles * ((int64_t)1 << ix->cbin_bits) * vk::K1_BM_WORDS * 4;
 }
 
 int64_t vk_scan_noalloc_max_n(void) { return NOALLOC_SCAN_BLOCKS * SCAN_TILE; }

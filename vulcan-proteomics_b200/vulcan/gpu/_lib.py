@@ -124,6 +124,8 @@ def lib():
     L.vk_scan_noalloc_max_n.restype = I64
     L.vk_mlp_infer_smem.argtypes = []
     L.vk_mlp_infer_smem.restype = I64
+    L.vk_tindex_bitmap_bytes.argtypes = [P]
+    L.vk_tindex_bitmap_bytes.restype = I64
     L.vk_mlp_infer_tc_smem.argtypes = []
     L.vk_mlp_infer_tc_smem.restype = I64
     _lib = L

@@ -187,7 +187,8 @@ class GpuIndex:
                                  K.ptr(self.cbin_off), K.stream()), "tindex_emit")
         ix.cbin_off = K.ptr(self.cbin_off)
         ix.postings = K.ptr(self.postings)
-        self.bitmap = torch.empty(max(nt * (1 << ix.cbin_bits) * 4, 4), dtype=torch.int32, device=d)
+        self.bitmap = torch.empty(max(int(L.vk_tindex_bitmap_bytes(C.byref(ix))) // 4, 4), dtype=torch.int32,
+                                  device=d)
         K.check(L.vk_tindex_bitmap(C.byref(ix), K.ptr(self.bitmap), K.stream()), "tindex_bitmap")
         ix.bitmap = K.ptr(self.bitmap)
         self.tix = ix
