@@ -991,10 +991,11 @@ def _pack_fused(gi: GpuIndex, o: dict, report: int, n: int):
 
 
 def _unpack_psms(host: np.ndarray, layout) -> dict:
-    """Host records of the filled PSM slots from a packed buffer."""
+    """Host records of the filled PSM slots from a packed buffer: new arrays (np.take), so the buffer may be reused
+    as soon as this returns."""
     cols = {name: np.frombuffer(host, dtype=dt, count=cnt, offset=off) for name, dt, off, cnt in layout}
-    ok = cols.pop("valid").astype(bool)
-    return {k: v[ok] for k, v in cols.items()}
+    idx = np.flatnonzero(cols.pop("valid"))
+    return {k: np.take(v, idx) for k, v in cols.items()}
 
 
 def _table(sp: Spectra, rec: dict) -> pa.Table:
@@ -1203,7 +1204,6 @@ class Searcher:
         self.device_ms += ev[0].elapsed_time(ev[1])
         check_status(slot.gp.out["status"])
         rec = _unpack_psms(slot.host_out.numpy(), slot.layout)
-        rec = {k: v.copy() for k, v in rec.items()}
         slot.busy = False
         st = Stats()
         st.h2d_bytes, st.d2h_bytes = h2d, slot.host_out.numel()
