@@ -273,6 +273,50 @@ int vk_psm_rank(int n_spec, const int64_t* cand_off, const int64_t* c_row, const
                 const int16_t* my, int min_matched, int report, int64_t* psm_cand, int32_t* psm_rank,
                 double* psm_dnext, double* psm_dbest, int32_t* n_psm, void* stream);
 
+/* PSM table columns of every ranked slot (the features of the reference's psm_table, vulcan/gpu/engine.py:361-432,
+ * computed on the device), packed into one byte buffer for a single device-to-host copy.  Slot j (0 <= j < slots,
+ * spectrum j / report) takes candidate psm_cand[j] (-1: empty slot, its row is written with valid = 0 and
+ * arbitrary values; every index it reads is clamped into its table).  Column c (VK_PSM_COLS of them, in this
+ * order: valid u8, spec_idx i64, rank i32, pf_row i64, pf_id u64, charge i8, isotope_error i8, expmass f32,
+ * calcmass f32, delta_mass_ppm f32, hyperscore f64, delta_next f64, delta_best f64, matched_b i16, matched_y i16,
+ * matched_peaks i16, summed_intensity f32, matched_intensity_pct f32, average_ppm f32, longest_b i16, longest_y
+ * i16, longest_y_pct f32, peptide_len i16, missed_cleavages u8, n_var u8, k1_count i32, scored_candidates i32,
+ * poisson f64) holds `slots` elements starting at byte col_off[c] (host array; multiples of 8) of `packed`.
+ * Arithmetic: f32 masses and percentages, f64 Poisson term, one rounding per operation in the reference's order. */
+#define VK_PSM_COLS 28
+typedef struct {
+  const int64_t* psm_cand;
+  const int32_t* psm_rank;
+  const double* dnext;
+  const double* dbest;
+  const int64_t* c_hyp;
+  const int64_t* c_row;
+  const int64_t* c_cnt;
+  const int8_t* h_z;
+  const int8_t* h_iso;
+  const float* h_pm;
+  int64_t n_hyp;            /* entries of the hypothesis columns */
+  const int64_t* spec_scored;
+  const int64_t* spec_matched;
+  const float* tic;
+  const double* hs;
+  const float* sb;
+  const float* sy;
+  const float* ppm;
+  const int16_t* mb;
+  const int16_t* my;
+  const int16_t* lb;
+  const int16_t* ly;
+  const float* mass32;
+  const uint8_t* length;
+  const int64_t* pf_id;
+  const uint8_t* missed;
+  const uint8_t* n_var;
+  int64_t n_rows;           /* index rows */
+} vk_psm_pack_in;
+int vk_pack_psms(const vk_psm_pack_in* in, int64_t slots, int report, const int64_t* col_off, uint8_t* packed,
+                 void* stream);
+
 /* ============================================================ Part 3: fused persistent search */
 
 /* Inputs of the fused search.  Spectra are the batch's (global ids 0..n_spec-1, peaks and hypotheses grouped by

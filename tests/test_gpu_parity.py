@@ -233,6 +233,29 @@ def test_k2_candidate_parallel_equals_warp_per_spectrum(mini, param_sets, indexe
                                           torch_cuda.equal(a[~a.isnan()], b[~b.isnan()])), (name, key)
 
 
+@pytest.mark.parametrize("name", SETS)
+def test_psm_pack_kernel_equals_torch_columns(mini, param_sets, indexes, name, torch_cuda):
+    """vk_pack_psms (one kernel) writes the same packed PSM rows as the torch formulation of the table columns,
+    bit for bit, with 1 and 3 PSMs reported per spectrum."""
+    import dataclasses
+    from vulcan.gpu import engine as E
+    l1, sp, _ = mini
+    p = dataclasses.replace(param_sets[name], search_method="staged")
+    gi = indexes[name]
+    n = len(sp.charge)
+    for report in (1, 3):
+        st = E.Stats()
+        out = E._search_device(E.DeviceRun(sp, gi.dev, st), gi, p, report, st)
+        a_buf, a_lay = E._pack_psms(gi, out, report, n)
+        b_buf, b_lay = E._pack_psms_torch(gi, out, report, n)
+        assert a_lay == b_lay
+        a = E._unpack_psms(a_buf.cpu().numpy(), a_lay)
+        b = E._unpack_psms(b_buf.cpu().numpy(), b_lay)
+        assert len(a["spec_idx"]) > 0
+        for k in b:
+            assert np.array_equal(a[k], b[k], equal_nan=a[k].dtype.kind == "f"), (name, report, k)
+
+
 @pytest.mark.parametrize("topk", (3, 60))
 def test_topk_over_shared_memory_capacity(mini, param_sets, torch_cuda, topk):
     """Precursor windows of +-2% make some spectra append more entries than a warp keeps in shared memory (512

@@ -69,6 +69,75 @@ psm_rank_k(int n_spec, const int64_t* cand_off, const int64_t* c_row, const doub
   }
 }
 
+// Column offsets of the packed PSM table, passed by value.
+struct PackLayout {
+  int64_t off[VK_PSM_COLS];
+};
+
+template <class T>
+__device__ __forceinline__ void put(uint8_t* packed, const PackLayout& L, int c, int64_t j, T v) {
+  reinterpret_cast<T*>(packed + L.off[c])[j] = v;
+}
+
+// One thread per PSM slot: the reference psm_table features (lnfact(0) = 1, Poisson term with +-inf -> 1e-325,
+// which is 0 in f64), each operation rounded once (the library is built with -fmad=false).
+__global__ void __launch_bounds__(256) pack_psms_k(vk_psm_pack_in in, int64_t slots, int report, PackLayout L,
+                                                   uint8_t* packed) {
+  const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (j >= slots) return;
+  const int64_t cand = in.psm_cand[j];
+  const int64_t ci = cand < 0 ? 0 : cand;
+  const int64_t s = j / report;
+  const int64_t hh = min(max(in.c_hyp[ci], (int64_t)0), in.n_hyp - 1);
+  const int64_t row = min(max(in.c_row[ci], (int64_t)0), in.n_rows - 1);
+  const int64_t mbk = in.mb[ci], myk = in.my[ci], kk = mbk + myk;
+  const int64_t sc = in.spec_scored[s], mt = in.spec_matched[s];
+  // Poisson term of the matched-peak count: lam^k e^-lam / e^lnfact(k), log10
+  const double lam = (double)mt / (double)sc;
+  const double x = (double)kk;
+  const double lx = log(x);
+  const double lnf = x == 0.0 ? 1.0 : ((x * lx - x) + 0.5 * lx) + 0.5 * log(6.283185307179586 * x);
+  double pois = pow(lam, x) * exp(-lam) / exp(lnf);
+  if (isinf(pois)) pois = 0.0;   // the reference's 1e-325, which is 0 in f64
+  const int iso = in.h_iso[hh];
+  const float pm = in.h_pm[hh];
+  const float calc = in.mass32[row];
+  const float ie = __fmul_rn((float)iso, 1.00335f);   // NEUTRON (an f32 value)
+  const float dm = __fdiv_rn(__fmul_rn(fabsf(__fsub_rn(__fsub_rn(pm, calc), ie)), 2.0e6f),
+                             __fadd_rn(__fsub_rn(pm, ie), calc));
+  const float sbs = __fadd_rn(in.sb[ci], in.sy[ci]);
+  const int plen = in.length[row];
+  const int16_t ly = in.ly[ci];
+  put<uint8_t>(packed, L, 0, j, cand >= 0 ? 1 : 0);
+  put<int64_t>(packed, L, 1, j, s);
+  put<int32_t>(packed, L, 2, j, in.psm_rank[j]);
+  put<int64_t>(packed, L, 3, j, row);
+  put<int64_t>(packed, L, 4, j, in.pf_id[row]);
+  put<int8_t>(packed, L, 5, j, in.h_z[hh]);
+  put<int8_t>(packed, L, 6, j, (int8_t)iso);
+  put<float>(packed, L, 7, j, pm);
+  put<float>(packed, L, 8, j, calc);
+  put<float>(packed, L, 9, j, dm);
+  put<double>(packed, L, 10, j, in.hs[ci]);
+  put<double>(packed, L, 11, j, in.dnext[j]);
+  put<double>(packed, L, 12, j, in.dbest[j]);
+  put<int16_t>(packed, L, 13, j, (int16_t)mbk);
+  put<int16_t>(packed, L, 14, j, (int16_t)myk);
+  put<int16_t>(packed, L, 15, j, (int16_t)kk);
+  put<float>(packed, L, 16, j, sbs);
+  put<float>(packed, L, 17, j, __fdiv_rn(__fmul_rn(100.0f, sbs), in.tic[s]));
+  put<float>(packed, L, 18, j, in.ppm[ci]);
+  put<int16_t>(packed, L, 19, j, in.lb[ci]);
+  put<int16_t>(packed, L, 20, j, ly);
+  put<float>(packed, L, 21, j, (float)((double)ly / (double)plen));
+  put<int16_t>(packed, L, 22, j, (int16_t)plen);
+  put<uint8_t>(packed, L, 23, j, in.missed[row]);
+  put<uint8_t>(packed, L, 24, j, in.n_var[row]);
+  put<int32_t>(packed, L, 25, j, (int32_t)in.c_cnt[ci]);
+  put<int32_t>(packed, L, 26, j, (int32_t)sc);
+  put<double>(packed, L, 27, j, log10(pois));
+}
+
 }  // namespace
 
 extern "C" int vk_psm_rank(int n_spec, const int64_t* cand_off, const int64_t* c_row, const double* hs,
@@ -78,5 +147,18 @@ extern "C" int vk_psm_rank(int n_spec, const int64_t* cand_off, const int64_t* c
   if (report < 1) return VK_E_ARG;
   psm_rank_k<<<(unsigned)((n_spec + RK_WARPS - 1) / RK_WARPS), RK_WARPS * 32, 0, (cudaStream_t)stream>>>(
       n_spec, cand_off, c_row, hs, mb, my, min_matched, report, psm_cand, psm_rank, psm_dnext, psm_dbest, n_psm);
+  return vk_launch_status();
+}
+
+extern "C" int vk_pack_psms(const vk_psm_pack_in* in, int64_t slots, int report, const int64_t* col_off,
+                            uint8_t* packed, void* stream) {
+  if (!in || !col_off || !packed || report < 1 || in->n_hyp < 1 || in->n_rows < 1) return VK_E_ARG;
+  if (slots <= 0) return 0;
+  PackLayout L;
+  for (int c = 0; c < VK_PSM_COLS; ++c) {
+    if (col_off[c] < 0 || (col_off[c] & 7)) return VK_E_ARG;
+    L.off[c] = col_off[c];
+  }
+  pack_psms_k<<<(unsigned)((slots + 255) / 256), 256, 0, (cudaStream_t)stream>>>(*in, slots, report, L, packed);
   return vk_launch_status();
 }

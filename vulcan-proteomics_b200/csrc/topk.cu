@@ -266,20 +266,26 @@ select_topk_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo, cons
   if (lane == 0) n_cand[s] = n_out;
 }
 
-__global__ void compact_k(int n_spec, int cap, const int64_t* n_cand, const int64_t* cand_off, const int64_t* s_hyp,
-                          const int64_t* s_row, const int64_t* s_cnt, const int8_t* h_maxfz, int64_t* c_hyp,
-                          int64_t* c_row, int64_t* c_cnt, int32_t* c_row32, int8_t* c_maxfz) {
-  int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  int64_t s = g / cap;
-  int j = (int)(g % cap);
-  if (s >= n_spec || j >= n_cand[s]) return;
-  int64_t src = s * cap + j, dst = cand_off[s] + j;
-  int64_t h = s_hyp[src];
-  c_hyp[dst] = h;
-  c_row[dst] = s_row[src];
-  c_cnt[dst] = s_cnt[src];
-  c_row32[dst] = (int32_t)s_row[src];
-  c_maxfz[dst] = h_maxfz[h];
+// One warp per spectrum: its n_cand[s] (<= cap) slots to [cand_off[s], ...).  A thread per slot of n_spec x cap
+// would launch mostly idle threads (cap is a bound; a few slots per spectrum are filled after the pruner).
+constexpr int CP_WARPS = 8;
+
+__global__ void __launch_bounds__(CP_WARPS * 32)
+compact_k(int n_spec, int cap, const int64_t* n_cand, const int64_t* cand_off, const int64_t* s_hyp,
+          const int64_t* s_row, const int64_t* s_cnt, const int8_t* h_maxfz, int64_t* c_hyp, int64_t* c_row,
+          int64_t* c_cnt, int32_t* c_row32, int8_t* c_maxfz) {
+  const int s = blockIdx.x * CP_WARPS + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (s >= n_spec) return;
+  const int64_t m = min(n_cand[s], (int64_t)cap), dst0 = cand_off[s], src0 = (int64_t)s * cap;
+  for (int64_t j = lane; j < m; j += 32) {
+    const int64_t src = src0 + j, dst = dst0 + j;
+    const int64_t h = s_hyp[src];
+    c_hyp[dst] = h;
+    c_row[dst] = s_row[src];
+    c_cnt[dst] = s_cnt[src];
+    c_row32[dst] = (int32_t)s_row[src];
+    c_maxfz[dst] = h_maxfz[h];
+  }
 }
 
 }  // namespace
@@ -314,10 +320,8 @@ int vk_compact_cands(int n_spec, int cap, const int64_t* n_cand, const int64_t* 
                      const int64_t* s_row, const int64_t* s_cnt, const int8_t* h_maxfz, int64_t* c_hyp,
                      int64_t* c_row, int64_t* c_cnt, int32_t* c_row32, int8_t* c_maxfz, void* stream) {
   if (n_spec == 0) return 0;
-  int64_t n = (int64_t)n_spec * cap;
-  compact_k<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(n_spec, cap, n_cand, cand_off, s_hyp,
-                                                                           s_row, s_cnt, h_maxfz, c_hyp, c_row, c_cnt,
-                                                                           c_row32, c_maxfz);
+  compact_k<<<(unsigned)((n_spec + CP_WARPS - 1) / CP_WARPS), CP_WARPS * 32, 0, (cudaStream_t)stream>>>(
+      n_spec, cap, n_cand, cand_off, s_hyp, s_row, s_cnt, h_maxfz, c_hyp, c_row, c_cnt, c_row32, c_maxfz);
   return vk_launch_status();
 }
 

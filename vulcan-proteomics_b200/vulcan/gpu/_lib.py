@@ -33,6 +33,15 @@ class TIndex(C.Structure):
                 ("tile_off", P), ("cbin_off", P), ("postings", P), ("bitmap", P)]
 
 
+class PsmPackIn(C.Structure):
+    """vk_psm_pack_in"""
+    _fields_ = [("psm_cand", P), ("psm_rank", P), ("dnext", P), ("dbest", P), ("c_hyp", P), ("c_row", P),
+                ("c_cnt", P), ("h_z", P), ("h_iso", P), ("h_pm", P), ("n_hyp", C.c_int64), ("spec_scored", P),
+                ("spec_matched", P), ("tic", P), ("hs", P), ("sb", P), ("sy", P), ("ppm", P), ("mb", P), ("my", P),
+                ("lb", P), ("ly", P), ("mass32", P), ("length", P), ("pf_id", P), ("missed", P), ("n_var", P),
+                ("n_rows", C.c_int64)]
+
+
 class FusedIn(C.Structure):
     """vk_fused_in"""
     _fields_ = [("n_spec", C.c_int), ("n_work", C.c_int), ("spec_ids", P), ("pk_off", P), ("pk_mass", P),
@@ -88,6 +97,7 @@ _SIGS_B200 = {
     "vk_compact_cands": [I32, I32, P, P, P, P, P, P, P, P, P, P, P, P],
     "vk_k2_spectra": [P, I32, P, P, P, P, P, P, P, P, P, P, P, F32, F32, P, P, P, P, P, P, P, P, P, P],
     "vk_k2_cands": [P, I32, P, P, P, P, P, P, P, P, P, P, P, F32, F32, P, P, P, P, P, P, P, P, P],
+    "vk_pack_psms": [P, I64, I32, P, P, P],
     "vk_psm_rank": [I32, P, P, P, P, P, I32, I32, P, P, P, P, P, P],
     "vk_search_fused": [P, P, P, I32, I32, I32, P, P, P, P, P, P, P, P, P, P],
     "vk_search_fused_smem": [P, I32, I32, I32, I32, P],

@@ -952,10 +952,57 @@ def _pack(cols: dict, valid: torch.Tensor):
     return torch.cat(parts), layout
 
 
+# columns of the packed PSM slots (vk_pack_psms), in buffer order
+_PACK_COLS = (("valid", np.uint8), ("spec_idx", np.int64), ("rank", np.int32), ("pf_row", np.int64),
+              ("pf_id", np.uint64), ("charge", np.int8), ("isotope_error", np.int8), ("expmass", np.float32),
+              ("calcmass", np.float32), ("delta_mass_ppm", np.float32), ("hyperscore", np.float64),
+              ("delta_next", np.float64), ("delta_best", np.float64), ("matched_b", np.int16),
+              ("matched_y", np.int16), ("matched_peaks", np.int16), ("summed_intensity", np.float32),
+              ("matched_intensity_pct", np.float32), ("average_ppm", np.float32), ("longest_b", np.int16),
+              ("longest_y", np.int16), ("longest_y_pct", np.float32), ("peptide_len", np.int16),
+              ("missed_cleavages", np.uint8), ("n_var", np.uint8), ("k1_count", np.int32),
+              ("scored_candidates", np.int32), ("poisson", np.float64))
+_PACK_LAYOUTS = {}
+
+
+def _pack_layout(slots: int):
+    """[(name, numpy dtype, byte offset, count)] of the packed buffer of `slots` PSM slots, its size, and the byte
+    offsets as an int64 array for vk_pack_psms (each column padded to 8 bytes)."""
+    if slots not in _PACK_LAYOUTS:
+        layout, off = [], 0
+        for name, dt in _PACK_COLS:
+            dt = np.dtype(dt)
+            layout.append((name, dt, off, slots))
+            off += (slots * dt.itemsize + 7) & ~7
+        _PACK_LAYOUTS[slots] = (layout, off, np.array([o for _, _, o, _ in layout], np.int64))
+    return _PACK_LAYOUTS[slots]
+
+
 def _pack_psms(gi: GpuIndex, out: dict, report: int, n: int):
-    """Every PSM slot of a staged / pruned pass, its table columns computed on the device, packed into one byte
-    buffer without a host read (empty slots masked): the graph-captured pass ends with it and the host reads it
-    in one copy.  Returns (buffer, layout) with layout = [(name, numpy dtype, byte offset, count)]."""
+    """Every PSM slot of a staged / pruned pass, its table columns computed on the device by one kernel
+    (``vk_pack_psms``) straight into one byte buffer without a host read (empty slots masked): the graph-captured
+    pass ends with it and the host reads it in one copy.  Returns (buffer, layout) with layout = [(name, numpy
+    dtype, byte offset, count)]; the same buffer as ``_pack_psms_torch``."""
+    psm_cand, psm_rank, dnext, dbest = out["psm"]
+    slots = n * report
+    layout, size, col_off = _pack_layout(slots)
+    buf = torch.empty(max(size, 8), dtype=torch.uint8, device=psm_cand.device)
+    dh, k2 = out["dh"], out["k2"]
+    pin = K.PsmPackIn(K.ptr(psm_cand), K.ptr(psm_rank), K.ptr(dnext), K.ptr(dbest), K.ptr(out["c_hyp"]),
+                      K.ptr(out["c_row"]), K.ptr(out["c_cnt"]), K.ptr(dh["z"]), K.ptr(dh["iso"]), K.ptr(dh["pm"]),
+                      dh["z"].numel(), K.ptr(out["spec_scored"]), K.ptr(out["spec_matched"]),
+                      K.ptr(out["peaks"]["tic"]), K.ptr(k2["hyperscore"]), K.ptr(k2["summed_b"]),
+                      K.ptr(k2["summed_y"]), K.ptr(k2["ppm"]), K.ptr(k2["matched_b"]), K.ptr(k2["matched_y"]),
+                      K.ptr(k2["longest_b"]), K.ptr(k2["longest_y"]), K.ptr(gi.mass32), K.ptr(gi.length),
+                      K.ptr(gi.pf_id), K.ptr(gi.missed), K.ptr(gi.n_var), gi.n)
+    K.check(K.lib().vk_pack_psms(C.byref(pin), slots, report, col_off.ctypes.data, K.ptr(buf), K.stream()),
+            "pack_psms")
+    return buf, layout
+
+
+def _pack_psms_torch(gi: GpuIndex, out: dict, report: int, n: int):
+    """The same packed buffer as ``_pack_psms`` built from torch operations (``_psm_device_cols``): the
+    formulation the fused search's packing shares, and the check of the kernel."""
     psm_cand, psm_rank, dnext, dbest = out["psm"]
     slots = n * report
     cand = psm_cand[:slots]
