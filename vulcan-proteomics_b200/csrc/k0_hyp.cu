@@ -28,6 +28,8 @@ __device__ __forceinline__ bool in_range(float mz, float fmin, float fmax) {
   return mz >= fmin && mz <= fmax;   // false for NaN
 }
 
+constexpr int K0_UNROLL = 4;   // raw-peak chunks of 32 loaded ahead per warp
+
 // mass-order key of a peak: ascending = mass ascending, then intensity descending
 __device__ __forceinline__ uint64_t mass_key(float mz, float it) {
   return ((uint64_t)ord_f32(__fsub_rn(mz, VK_PROTON)) << 32) | (uint64_t)(~ord_f32(it));
@@ -45,19 +47,28 @@ __global__ void k0_count_k(int n_spec, const int64_t* raw_off, const float* raw_
   long long c = 0;
   bool sorted = true;
   uint64_t carry = 0;   // key of the previous chunk's last peak
-  for (int64_t i0 = r0; i0 < r1; i0 += 32) {
-    const int64_t i = i0 + lane;
-    uint64_t k = 0;
-    if (i < r1) {
-      const float mz = raw_mz[i];
-      c += in_range(mz, fmin, fmax);
-      sorted &= !isnan(mz);
-      k = mass_key(mz, raw_int[i]);
+  for (int64_t b0 = r0; b0 < r1; b0 += 32 * K0_UNROLL) {
+    float mzv[K0_UNROLL], itv[K0_UNROLL];
+#pragma unroll
+    for (int u = 0; u < K0_UNROLL; ++u) {   // the loads first: K0_UNROLL chunks in flight per lane
+      const int64_t i = b0 + 32 * u + lane;
+      mzv[u] = i < r1 ? raw_mz[i] : 0.f;
+      itv[u] = i < r1 ? raw_int[i] : 0.f;
     }
-    uint64_t prev = __shfl_up_sync(VK_FULL, k, 1);
-    if (lane == 0) prev = carry;
-    if (i < r1 && i > r0) sorted &= prev <= k;
-    carry = __shfl_sync(VK_FULL, k, 31);
+#pragma unroll
+    for (int u = 0; u < K0_UNROLL; ++u) {
+      const int64_t i = b0 + 32 * u + lane;
+      uint64_t k = 0;
+      if (i < r1) {
+        c += in_range(mzv[u], fmin, fmax);
+        sorted &= !isnan(mzv[u]);
+        k = mass_key(mzv[u], itv[u]);
+      }
+      uint64_t prev = __shfl_up_sync(VK_FULL, k, 1);
+      if (lane == 0) prev = carry;
+      if (i < r1 && i > r0) sorted &= prev <= k;
+      carry = __shfl_sync(VK_FULL, k, 31);
+    }
   }
   c = vk::warp_sum(c);
   sorted = __all_sync(VK_FULL, sorted);
@@ -81,23 +92,27 @@ __global__ void k0_easy_k(int n_spec, const int64_t* raw_off, const float* raw_m
   const int64_t o0 = pk_off[s];
   double part = 0.0;
   int w = 0;
-  for (int64_t i0 = r0; i0 < r1; i0 += 32) {
-    const int64_t i = i0 + lane;
-    float mz = 0.f, it = 0.f;
-    bool take = false;
-    if (i < r1) {
-      mz = raw_mz[i];
-      take = in_range(mz, fmin, fmax);
-      if (take) it = raw_int[i];
+  for (int64_t b0 = r0; b0 < r1; b0 += 32 * K0_UNROLL) {
+    float mzv[K0_UNROLL], itv[K0_UNROLL];
+#pragma unroll
+    for (int u = 0; u < K0_UNROLL; ++u) {   // the loads first: K0_UNROLL chunks in flight per lane
+      const int64_t i = b0 + 32 * u + lane;
+      mzv[u] = i < r1 ? raw_mz[i] : 0.f;
+      itv[u] = i < r1 ? raw_int[i] : 0.f;
     }
-    const unsigned m = __ballot_sync(VK_FULL, take);
-    if (take) {
-      const int pos = w + __popc(m & lt_mask);
-      pk_mass[o0 + pos] = __fsub_rn(mz, VK_PROTON);
-      pk_int[o0 + pos] = it;
-      part += (double)it;
+#pragma unroll
+    for (int u = 0; u < K0_UNROLL; ++u) {
+      const int64_t i = b0 + 32 * u + lane;
+      const bool take = i < r1 && in_range(mzv[u], fmin, fmax);
+      const unsigned m = __ballot_sync(VK_FULL, take);
+      if (take) {
+        const int pos = w + __popc(m & lt_mask);
+        pk_mass[o0 + pos] = __fsub_rn(mzv[u], VK_PROTON);
+        pk_int[o0 + pos] = itv[u];
+        part += (double)itv[u];
+      }
+      w += __popc(m);
     }
-    w += __popc(m);
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(VK_FULL, part, o);
@@ -215,36 +230,46 @@ __device__ __forceinline__ int64_t upper_bound_g(const float* a, int64_t n, floa
   return lo;
 }
 
-__global__ void hyp_fill_k(int n_spec, const uint8_t* valid, const double* pmz, const int8_t* charge, int z_lo,
-                           int z_hi, int iso_lo, int iso_hi, float ppm_lo, float ppm_hi, int mfc,
-                           const float* idx_mass32, int64_t n_rows, const int64_t* hyp_off, int32_t* h_spec,
-                           int8_t* h_z, int8_t* h_iso, float* h_pm, float* h_M, int64_t* h_lo, int64_t* h_hi,
-                           int8_t* h_maxfz) {
-  int s = blockIdx.x * blockDim.x + threadIdx.x;
+// Warp per spectrum: its hypotheses (charges x isotope errors) and their two window bounds are 2 x n_hyp
+// independent binary searches over the index masses, one per lane (the per-thread version ran them one after
+// another: up to six dependent chains of ~23 global loads).  Lane t takes hypothesis t / 2, bound t % 2.
+constexpr int HF_WARPS = 4;
+
+__global__ void __launch_bounds__(HF_WARPS * 32)
+hyp_fill_k(int n_spec, const uint8_t* valid, const double* pmz, const int8_t* charge, int z_lo, int z_hi, int iso_lo,
+           int iso_hi, float ppm_lo, float ppm_hi, int mfc, const float* idx_mass32, int64_t n_rows,
+           const int64_t* hyp_off, int32_t* h_spec, int8_t* h_z, int8_t* h_iso, float* h_pm, float* h_M,
+           int64_t* h_lo, int64_t* h_hi, int8_t* h_maxfz) {
+  const int s = blockIdx.x * HF_WARPS + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (s >= n_spec) return;
   if (!(valid[s] && isfinite(pmz[s]))) return;
-  int64_t o = hyp_off[s];
+  const int64_t o = hyp_off[s];
   const int zk = charge[s];
   const int za = zk > 0 ? zk : z_lo, zb = zk > 0 ? zk : z_hi;
+  const int n_iso = iso_hi - iso_lo + 1;
+  const int n_task = 2 * (zb - za + 1) * n_iso;
   const float mz = __fsub_rn(__double2float_rn(pmz[s]), VK_PROTON);
-  for (int z = za; z <= zb; ++z) {
+  for (int t = lane; t < n_task; t += 32) {
+    const int q = t >> 1, upper = t & 1;
+    const int z = za + q / n_iso, iso = iso_lo + q % n_iso;
     const float pm = __fmul_rn(mz, (float)z);
-    int mf = z;
-    if (mfc > 0) mf = min(z, mfc + 1);
-    mf = max(mf, 2);
-    for (int iso = iso_lo; iso <= iso_hi; ++iso) {
-      const float M = __fsub_rn(pm, __fmul_rn((float)iso, VK_NEUTRON));
-      const float lo = __fadd_rn(M, __fdiv_rn(__fmul_rn(M, ppm_lo), 1000000.0f));
+    const float M = __fsub_rn(pm, __fmul_rn((float)iso, VK_NEUTRON));
+    const int64_t h = o + q;
+    if (upper) {
       const float hi = __fadd_rn(M, __fdiv_rn(__fmul_rn(M, ppm_hi), 1000000.0f));
-      h_spec[o] = s;
-      h_z[o] = (int8_t)z;
-      h_iso[o] = (int8_t)iso;
-      h_pm[o] = pm;
-      h_M[o] = M;
-      h_lo[o] = lower_bound_g(idx_mass32, n_rows, lo);
-      h_hi[o] = upper_bound_g(idx_mass32, n_rows, hi);
-      h_maxfz[o] = (int8_t)mf;
-      ++o;
+      h_hi[h] = upper_bound_g(idx_mass32, n_rows, hi);
+    } else {
+      const float lo = __fadd_rn(M, __fdiv_rn(__fmul_rn(M, ppm_lo), 1000000.0f));
+      int mf = z;
+      if (mfc > 0) mf = min(z, mfc + 1);
+      mf = max(mf, 2);
+      h_spec[h] = s;
+      h_z[h] = (int8_t)z;
+      h_iso[h] = (int8_t)iso;
+      h_pm[h] = pm;
+      h_M[h] = M;
+      h_maxfz[h] = (int8_t)mf;
+      h_lo[h] = lower_bound_g(idx_mass32, n_rows, lo);
     }
   }
 }
@@ -308,7 +333,7 @@ int vk_hyp_fill(int n_spec, const uint8_t* valid, const double* precursor_mz, co
                 void* stream) {
   if (n_spec == 0) return 0;
   if (z_hi < z_lo || iso_hi < iso_lo) return VK_E_ARG;
-  hyp_fill_k<<<(unsigned)((n_spec + 127) / 128), 128, 0, (cudaStream_t)stream>>>(
+  hyp_fill_k<<<(unsigned)((n_spec + HF_WARPS - 1) / HF_WARPS), HF_WARPS * 32, 0, (cudaStream_t)stream>>>(
       n_spec, valid, precursor_mz, charge, z_lo, z_hi, iso_lo, iso_hi, ppm_lo, ppm_hi, max_fragment_charge,
       idx_mass32, n_rows, hyp_off, h_spec, h_z, h_iso, h_pm, h_M, h_lo, h_hi, h_maxfz);
   return vk_launch_status();

@@ -212,7 +212,31 @@ select_pruned_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* hit_off,
   // (hypothesis, row) ascending, so among equal (logit, count) the later index = higher row wins on "desc"; the
   // hypothesis tie (same row in two hypotheses) is resolved by the lower index first through the complement below
   int n_keep = 0;
-  if (n > 0) {
+  // the usual case needs no ranking: when every hit with logit >= tau is kept (their number is within
+  // [min(min_keep, n), max_keep]) the selection is exactly those hits, since they rank above all others (keys are
+  // ordered by logit first); NaN logits rank highest, so the shortcut is taken only when there is none
+  int n_pass = 0;
+  bool any_nan = false;
+  for (int i0 = 0; i0 < n; i0 += 32) {
+    const int i = i0 + lane;
+    const float lg = i < n ? logit[a + i] : 0.f;
+    n_pass += __popc(__ballot_sync(VK_FULL, i < n && lg >= tau));
+    any_nan |= __any_sync(VK_FULL, i < n && isnan(lg));
+  }
+  const bool direct = n > 0 && !any_nan && n_pass <= max_keep && n_pass >= min(min_keep, n);
+  if (direct) {
+    for (int i0 = 0; i0 < n; i0 += 32) {
+      const int i = i0 + lane;
+      const bool take = i < n && logit[a + i] >= tau;
+      const unsigned m = __ballot_sync(VK_FULL, take);
+      if (take) {
+        const int pos = n_keep + __popc(m & lt);
+        lst[pos] = ((uint64_t)hit_row[a + i] << 34) | ((uint64_t)(hit_hyp[a + i] - h0) << 16) | (uint64_t)pos;
+        lcnt[pos] = (int32_t)hit_cnt[a + i];
+      }
+      n_keep += __popc(m);
+    }
+  } else if (n > 0) {
     if (n > sort_cap) {
       // more hits than the sort buffer: keep those with logit >= tau by hit order, up to max_keep (rare)
       for (int i0 = 0; i0 < n && n_keep < max_keep; i0 += 32) {
