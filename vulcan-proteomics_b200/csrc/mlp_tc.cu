@@ -210,14 +210,16 @@ mlp_infer_tc_k(int64_t n, const int64_t* n_dev, const __nv_bfloat16* __restrict_
       for (int q = 0; q < 4; ++q) {
         uint4 w;
         const int c = c0 + 8 * q;
-        w.x = pack2(fmaxf(__uint_as_float(v[8 * q + 0]) + sb1[c + 0], 0.f),
-                    fmaxf(__uint_as_float(v[8 * q + 1]) + sb1[c + 1], 0.f));
-        w.y = pack2(fmaxf(__uint_as_float(v[8 * q + 2]) + sb1[c + 2], 0.f),
-                    fmaxf(__uint_as_float(v[8 * q + 3]) + sb1[c + 3], 0.f));
-        w.z = pack2(fmaxf(__uint_as_float(v[8 * q + 4]) + sb1[c + 4], 0.f),
-                    fmaxf(__uint_as_float(v[8 * q + 5]) + sb1[c + 5], 0.f));
-        w.w = pack2(fmaxf(__uint_as_float(v[8 * q + 6]) + sb1[c + 6], 0.f),
-                    fmaxf(__uint_as_float(v[8 * q + 7]) + sb1[c + 7], 0.f));
+        const float4 ba = *reinterpret_cast<const float4*>(sb1 + c);       // 16-byte aligned (c % 8 == 0)
+        const float4 bb = *reinterpret_cast<const float4*>(sb1 + c + 4);
+        w.x = pack2(fmaxf(__uint_as_float(v[8 * q + 0]) + ba.x, 0.f),
+                    fmaxf(__uint_as_float(v[8 * q + 1]) + ba.y, 0.f));
+        w.y = pack2(fmaxf(__uint_as_float(v[8 * q + 2]) + ba.z, 0.f),
+                    fmaxf(__uint_as_float(v[8 * q + 3]) + ba.w, 0.f));
+        w.z = pack2(fmaxf(__uint_as_float(v[8 * q + 4]) + bb.x, 0.f),
+                    fmaxf(__uint_as_float(v[8 * q + 5]) + bb.y, 0.f));
+        w.w = pack2(fmaxf(__uint_as_float(v[8 * q + 6]) + bb.z, 0.f),
+                    fmaxf(__uint_as_float(v[8 * q + 7]) + bb.w, 0.f));
         *reinterpret_cast<uint4*>(dst + q * 128) = w;    // k chunks 128 bytes apart
       }
     }
@@ -251,7 +253,14 @@ mlp_infer_tc_k(int64_t n, const int64_t* n_dev, const __nv_bfloat16* __restrict_
         tmem_ld32(pbuf + lane_off + (uint32_t)c0, v);
         tmem_wait_ld();
 #pragma unroll
-        for (int j = 0; j < 32; ++j) z += fmaxf(__uint_as_float(v[j]) + sb2[c0 + j], 0.f) * sw3[c0 + j];
+        for (int j = 0; j < 32; j += 4) {   // b2 and w3 four at a time; relu(D + b2) . w3 with fused multiply-adds
+          const float4 b = *reinterpret_cast<const float4*>(sb2 + c0 + j);
+          const float4 w = *reinterpret_cast<const float4*>(sw3 + c0 + j);
+          z = __fmaf_rn(fmaxf(__uint_as_float(v[j + 0]) + b.x, 0.f), w.x, z);
+          z = __fmaf_rn(fmaxf(__uint_as_float(v[j + 1]) + b.y, 0.f), w.y, z);
+          z = __fmaf_rn(fmaxf(__uint_as_float(v[j + 2]) + b.z, 0.f), w.z, z);
+          z = __fmaf_rn(fmaxf(__uint_as_float(v[j + 3]) + b.w, 0.f), w.w, z);
+        }
       }
       part[cq * TC_M + my_row] = z;
     }
@@ -294,7 +303,14 @@ mlp_infer_tc_k(int64_t n, const int64_t* n_dev, const __nv_bfloat16* __restrict_
       tmem_ld32(pbuf + lane_off + (uint32_t)c0, v);
       tmem_wait_ld();
 #pragma unroll
-      for (int j = 0; j < 32; ++j) z += fmaxf(__uint_as_float(v[j]) + sb2[c0 + j], 0.f) * sw3[c0 + j];
+      for (int j = 0; j < 32; j += 4) {   // b2 and w3 four at a time; relu(D + b2) . w3 with fused multiply-adds
+        const float4 b = *reinterpret_cast<const float4*>(sb2 + c0 + j);
+        const float4 w = *reinterpret_cast<const float4*>(sw3 + c0 + j);
+        z = __fmaf_rn(fmaxf(__uint_as_float(v[j + 0]) + b.x, 0.f), w.x, z);
+        z = __fmaf_rn(fmaxf(__uint_as_float(v[j + 1]) + b.y, 0.f), w.y, z);
+        z = __fmaf_rn(fmaxf(__uint_as_float(v[j + 2]) + b.z, 0.f), w.z, z);
+        z = __fmaf_rn(fmaxf(__uint_as_float(v[j + 3]) + b.w, 0.f), w.w, z);
+      }
     }
     part[cq * TC_M + my_row] = z;
     tc_fence_before();
