@@ -282,7 +282,11 @@ int vk_psm_rank(int n_spec, const int64_t* cand_off, const int64_t* c_row, const
  * matched_peaks i16, summed_intensity f32, matched_intensity_pct f32, average_ppm f32, longest_b i16, longest_y
  * i16, longest_y_pct f32, peptide_len i16, missed_cleavages u8, n_var u8, k1_count i32, scored_candidates i32,
  * poisson f64) holds `slots` elements starting at byte col_off[c] (host array; multiples of 8) of `packed`.
- * Arithmetic: f32 masses and percentages, f64 Poisson term, one rounding per operation in the reference's order. */
+ * Arithmetic: f32 masses and percentages, f64 Poisson term, one rounding per operation in the reference's order.
+ * row_pos (may be NULL): the exclusive prefix count of filled slots (slots + 1 entries, e.g. a scan of
+ * psm_cand >= 0); with it the filled slots are written contiguously in slot order (slot j to row row_pos[j]),
+ * empty slots not at all, and column 0 holds their number row_pos[slots] as one i64 instead of the valid bytes
+ * (0 when slots = 0; column 0 then needs 8 bytes), so the host reads plain slices. */
 #define VK_PSM_COLS 28
 typedef struct {
   const int64_t* psm_cand;
@@ -314,8 +318,8 @@ typedef struct {
   const uint8_t* n_var;
   int64_t n_rows;           /* index rows */
 } vk_psm_pack_in;
-int vk_pack_psms(const vk_psm_pack_in* in, int64_t slots, int report, const int64_t* col_off, uint8_t* packed,
-                 void* stream);
+int vk_pack_psms(const vk_psm_pack_in* in, int64_t slots, int report, const int64_t* col_off,
+                 const int64_t* row_pos, uint8_t* packed, void* stream);
 
 /* ============================================================ Part 3: fused persistent search */
 

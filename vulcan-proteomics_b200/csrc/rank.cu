@@ -82,12 +82,15 @@ __device__ __forceinline__ void put(uint8_t* packed, const PackLayout& L, int c,
 // One thread per PSM slot: the reference psm_table features (lnfact(0) = 1, Poisson term with +-inf -> 1e-325,
 // which is 0 in f64), each operation rounded once (the library is built with -fmad=false).
 __global__ void __launch_bounds__(256) pack_psms_k(vk_psm_pack_in in, int64_t slots, int report, PackLayout L,
-                                                   uint8_t* packed) {
-  const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (j >= slots) return;
-  const int64_t cand = in.psm_cand[j];
+                                                   const int64_t* row_pos, uint8_t* packed) {
+  const int64_t slot = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (slot >= slots) return;
+  if (row_pos && slot == 0) reinterpret_cast<int64_t*>(packed + L.off[0])[0] = row_pos[slots];
+  const int64_t cand = in.psm_cand[slot];
+  if (row_pos && cand < 0) return;   // compacted: filled slots only
+  const int64_t j = row_pos ? row_pos[slot] : slot;   // output row
   const int64_t ci = cand < 0 ? 0 : cand;
-  const int64_t s = j / report;
+  const int64_t s = slot / report;
   const int64_t hh = min(max(in.c_hyp[ci], (int64_t)0), in.n_hyp - 1);
   const int64_t row = min(max(in.c_row[ci], (int64_t)0), in.n_rows - 1);
   const int64_t mbk = in.mb[ci], myk = in.my[ci], kk = mbk + myk;
@@ -108,9 +111,9 @@ __global__ void __launch_bounds__(256) pack_psms_k(vk_psm_pack_in in, int64_t sl
   const float sbs = __fadd_rn(in.sb[ci], in.sy[ci]);
   const int plen = in.length[row];
   const int16_t ly = in.ly[ci];
-  put<uint8_t>(packed, L, 0, j, cand >= 0 ? 1 : 0);
+  if (!row_pos) put<uint8_t>(packed, L, 0, j, cand >= 0 ? 1 : 0);
   put<int64_t>(packed, L, 1, j, s);
-  put<int32_t>(packed, L, 2, j, in.psm_rank[j]);
+  put<int32_t>(packed, L, 2, j, in.psm_rank[slot]);
   put<int64_t>(packed, L, 3, j, row);
   put<int64_t>(packed, L, 4, j, in.pf_id[row]);
   put<int8_t>(packed, L, 5, j, in.h_z[hh]);
@@ -119,8 +122,8 @@ __global__ void __launch_bounds__(256) pack_psms_k(vk_psm_pack_in in, int64_t sl
   put<float>(packed, L, 8, j, calc);
   put<float>(packed, L, 9, j, dm);
   put<double>(packed, L, 10, j, in.hs[ci]);
-  put<double>(packed, L, 11, j, in.dnext[j]);
-  put<double>(packed, L, 12, j, in.dbest[j]);
+  put<double>(packed, L, 11, j, in.dnext[slot]);
+  put<double>(packed, L, 12, j, in.dbest[slot]);
   put<int16_t>(packed, L, 13, j, (int16_t)mbk);
   put<int16_t>(packed, L, 14, j, (int16_t)myk);
   put<int16_t>(packed, L, 15, j, (int16_t)kk);
@@ -151,14 +154,19 @@ extern "C" int vk_psm_rank(int n_spec, const int64_t* cand_off, const int64_t* c
 }
 
 extern "C" int vk_pack_psms(const vk_psm_pack_in* in, int64_t slots, int report, const int64_t* col_off,
-                            uint8_t* packed, void* stream) {
-  if (!in || !col_off || !packed || report < 1 || in->n_hyp < 1 || in->n_rows < 1) return VK_E_ARG;
-  if (slots <= 0) return 0;
+                            const int64_t* row_pos, uint8_t* packed, void* stream) {
+  if (!in || !col_off || !packed || report < 1 || in->n_hyp < 1 || in->n_rows < 1 || slots < 0) return VK_E_ARG;
   PackLayout L;
   for (int c = 0; c < VK_PSM_COLS; ++c) {
     if (col_off[c] < 0 || (col_off[c] & 7)) return VK_E_ARG;
     L.off[c] = col_off[c];
   }
-  pack_psms_k<<<(unsigned)((slots + 255) / 256), 256, 0, (cudaStream_t)stream>>>(*in, slots, report, L, packed);
+  if (slots == 0) {   // no slots: a compacted buffer still states its (zero) rows
+    if (!row_pos) return 0;
+    const cudaError_t e = cudaMemsetAsync(packed + L.off[0], 0, sizeof(int64_t), (cudaStream_t)stream);
+    return e == cudaSuccess ? 0 : vk_err(e);
+  }
+  pack_psms_k<<<(unsigned)((slots + 255) / 256), 256, 0, (cudaStream_t)stream>>>(*in, slots, report, L, row_pos,
+                                                                                   packed);
   return vk_launch_status();
 }

@@ -987,6 +987,8 @@ def _pack_psms(gi: GpuIndex, out: dict, report: int, n: int):
     slots = n * report
     layout, size, col_off = _pack_layout(slots)
     buf = torch.empty(max(size, 8), dtype=torch.uint8, device=psm_cand.device)
+    # filled slots written contiguously in slot order: their rows from a scan of the fill flags
+    row_pos = _scan((psm_cand[:slots] >= 0).to(torch.int64))
     dh, k2 = out["dh"], out["k2"]
     pin = K.PsmPackIn(K.ptr(psm_cand), K.ptr(psm_rank), K.ptr(dnext), K.ptr(dbest), K.ptr(out["c_hyp"]),
                       K.ptr(out["c_row"]), K.ptr(out["c_cnt"]), K.ptr(dh["z"]), K.ptr(dh["iso"]), K.ptr(dh["pm"]),
@@ -995,9 +997,9 @@ def _pack_psms(gi: GpuIndex, out: dict, report: int, n: int):
                       K.ptr(k2["summed_y"]), K.ptr(k2["ppm"]), K.ptr(k2["matched_b"]), K.ptr(k2["matched_y"]),
                       K.ptr(k2["longest_b"]), K.ptr(k2["longest_y"]), K.ptr(gi.mass32), K.ptr(gi.length),
                       K.ptr(gi.pf_id), K.ptr(gi.missed), K.ptr(gi.n_var), gi.n)
-    K.check(K.lib().vk_pack_psms(C.byref(pin), slots, report, col_off.ctypes.data, K.ptr(buf), K.stream()),
-            "pack_psms")
-    return buf, layout
+    K.check(K.lib().vk_pack_psms(C.byref(pin), slots, report, col_off.ctypes.data, K.ptr(row_pos), K.ptr(buf),
+                                 K.stream()), "pack_psms")
+    return buf, [("n_rows", np.dtype(np.int64), int(col_off[0]), 1)] + layout[1:]
 
 
 def _pack_psms_torch(gi: GpuIndex, out: dict, report: int, n: int):
@@ -1038,8 +1040,12 @@ def _pack_fused(gi: GpuIndex, o: dict, report: int, n: int):
 
 
 def _unpack_psms(host: np.ndarray, layout) -> dict:
-    """Host records of the filled PSM slots from a packed buffer: new arrays (np.take), so the buffer may be reused
-    as soon as this returns."""
+    """Host records of the filled PSM slots from a packed buffer: new arrays, so the buffer may be reused as soon
+    as this returns.  A compacted buffer (layout starting with "n_rows": the filled slots first, in slot order) is
+    read as slices; otherwise the "valid" column selects the rows."""
+    if layout and layout[0][0] == "n_rows":
+        n = int(np.frombuffer(host, dtype=np.int64, count=1, offset=layout[0][2])[0])
+        return {name: np.frombuffer(host, dtype=dt, count=n, offset=off).copy() for name, dt, off, cnt in layout[1:]}
     cols = {name: np.frombuffer(host, dtype=dt, count=cnt, offset=off) for name, dt, off, cnt in layout}
     idx = np.flatnonzero(cols.pop("valid"))
     return {k: np.take(v, idx) for k, v in cols.items()}
