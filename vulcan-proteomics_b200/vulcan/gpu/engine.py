@@ -10,6 +10,7 @@ arithmetic; candidate order and tie rules of ``engine.py:284-312`` and ``:366-39
 """
 from __future__ import annotations
 
+import collections
 import ctypes as C
 import math
 import resource
@@ -1285,35 +1286,43 @@ class Searcher:
                      for g in groups), default=0)
         self._force = (1 << max(10, int(raw - 1).bit_length()), 1 << max(5, int(mr - 1).bit_length()), n_hyp)
         try:
-            tables, pending = [], None
-            for g in groups:
-                parts = [runs[i] for i in g]
+            tables, inflight, k = [], collections.deque(), 0
+
+            def submit_next():
+                nonlocal k
+                parts = [runs[i] for i in groups[k]]
                 starts = np.concatenate([[0], np.cumsum([len(r) for r in parts])]).tolist()
-                h = self._submit(parts, n_b)
-                if pending is not None:
-                    tables += self._split(*pending)
-                pending = (h, parts, starts)
-            if pending is not None:
-                tables += self._split(*pending)
+                inflight.append((self._submit(parts, n_b), parts, starts))
+                k += 1
+            while k < len(groups) and len(inflight) < 2:
+                submit_next()
+            while inflight:
+                h, parts, starts = inflight.popleft()
+                rec, st = self._records(h)          # frees the batch's slot ...
+                if k < len(groups):
+                    submit_next()                   # ... for the batch after next, copied while the tables build
+                empty = Stats()
+                tables += [(t, st if i == 0 else empty) for i, t in enumerate(split_table(rec, parts, starts))]
         finally:
             self._force = None
         return tables
 
-    def _split(self, handle, runs, starts):
-        rec, st = self._records(handle)
-        empty = Stats()
-        return [(t, st if i == 0 else empty) for i, t in enumerate(split_table(rec, runs, starts))]
-
     def search_many(self, runs):
-        """PSM tables of many runs, one run queued ahead of the table being built."""
-        out, pending = [], None
-        for sp in runs:
-            h = self.submit(sp)
-            if pending is not None:
-                out.append(self.result(pending))
-            pending = h
-        if pending is not None:
-            out.append(self.result(pending))
+        """PSM tables of many runs, two runs in flight: as soon as a run's PSM slots are read back (which frees its
+        slot), the run after next is submitted, so its host-to-device copy overlaps the device pass of the next run
+        while the host builds the table."""
+        runs = list(runs)
+        out, inflight, k = [], collections.deque(), 0
+        while k < len(runs) and len(inflight) < 2:
+            inflight.append(self.submit(runs[k]))
+            k += 1
+        while inflight:
+            h = inflight.popleft()
+            rec, st = self._records(h)
+            if k < len(runs):
+                inflight.append(self.submit(runs[k]))
+                k += 1
+            out.append((_table(h[0], rec), st))
         return out
 
 
