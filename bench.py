@@ -316,6 +316,11 @@ def run_b200(a):
     from vulcan.gpu import _lib as K
     from vulcan.gpu import engine as E
     from vulcan.gpu import prune as PR
+    if world > 1:   # one rank builds the cached index; the others load it after the barrier
+        if rank == 0:
+            from vulcan import synth
+            synth.build_index(a.workload, CACHE)
+        dist.barrier()
     w, l1, lab, sp, t_build = _workload_setup(a.workload, rank)
     p = _params(w, a)
     gi = E.GpuIndex(l1, p, STATIC, w.var_mods, device=dev)

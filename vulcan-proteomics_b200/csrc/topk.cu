@@ -89,7 +89,9 @@ __device__ __forceinline__ uint64_t smem_kth_largest(const uint64_t* key, int n,
   return prefix;
 }
 
-constexpr int TK_UNROLL = 4;   // count loads in flight per lane
+#ifndef TK_UNROLL
+#define TK_UNROLL 8            // count loads in flight per lane
+#endif
 
 // rows of a hypothesis window, or 0 when its slice would end past the count buffer (cnt_cap entries)
 __device__ __forceinline__ int64_t win_rows(int64_t w0, int64_t lo, int64_t hi, int64_t cnt_cap) {

@@ -19,6 +19,7 @@ import dataclasses
 import hashlib
 import json
 import os
+import shutil
 
 import numpy as np
 
@@ -134,11 +135,22 @@ def build_index(w: Workload | str, root: str):
     d = os.path.join(root, f"{w.name}_{_cache_key(w)}")
     if os.path.exists(os.path.join(d, "meta.json")):
         return d
-    os.makedirs(d, exist_ok=True)
-    fa = os.path.join(d, "proteome.fasta")
+    # built in a directory of this process and renamed into place, so that processes building the same index at
+    # the same time (one per GPU) never see each other's partial files; the first rename wins
+    os.makedirs(root, exist_ok=True)
+    tmp = f"{d}.tmp{os.getpid()}"
+    shutil.rmtree(tmp, ignore_errors=True)
+    os.makedirs(tmp)
+    fa = os.path.join(tmp, "proteome.fasta")
     with open(fa, "w") as fh:
         fh.write(random_proteome_fasta(w.n_proteins, w.proteome_seed))
-    build([fa], d, w.index_params())
+    build([fa], tmp, w.index_params())
+    try:
+        os.rename(tmp, d)
+    except OSError:   # another process renamed its copy first
+        shutil.rmtree(tmp, ignore_errors=True)
+        if not os.path.exists(os.path.join(d, "meta.json")):
+            raise
     return d
 
 
