@@ -137,7 +137,7 @@ __device__ __forceinline__ void block_bitonic_u64(uint64_t* v, int n_pow2) {
     }
 }
 
-constexpr int K0_THREADS = 256;
+constexpr int K0_THREADS = 512;
 
 __global__ void __launch_bounds__(K0_THREADS)
 k0_fill_k(const int32_t* hard_list, const int32_t* n_hard, const int64_t* raw_off, const float* raw_mz,
