@@ -177,7 +177,8 @@ int vk_k0_fill(int n_spec, const int64_t* raw_off, const float* raw_mz, const fl
 
 /* Hypotheses (reference vulcan/gpu/host.py:64-91), two calls like K0: vk_hyp_count writes n_hyp[n_spec] (i64);
  * vk_hyp_fill writes, at hyp_off[s], the spectrum's hypotheses in (charge, isotope) order with f32 Sage
- * arithmetic and the row window [lo, hi) by binary search of the mass-sorted index masses. */
+ * arithmetic and the row window [lo, hi) by binary search of the mass-sorted index masses (hyp_off: the scan of
+ * n_hyp, n_spec + 1 entries; the searches of all hyp_off[n_spec] hypotheses run in parallel, a thread per bound). */
 int vk_hyp_count(int n_spec, const uint8_t* valid, const double* precursor_mz, const int8_t* charge, int z_lo,
                  int z_hi, int iso_lo, int iso_hi, int64_t* n_hyp, void* stream);
 int vk_hyp_fill(int n_spec, const uint8_t* valid, const double* precursor_mz, const int8_t* charge, int z_lo,

@@ -230,45 +230,47 @@ __device__ __forceinline__ int64_t upper_bound_g(const float* a, int64_t n, floa
   return lo;
 }
 
-// Warp per spectrum: its hypotheses (charges x isotope errors) and their two window bounds are 2 x n_hyp
-// independent binary searches over the index masses, one per lane (the per-thread version ran them one after
-// another: up to six dependent chains of ~23 global loads).  Lane t takes hypothesis t / 2, bound t % 2.
-constexpr int HF_WARPS = 4;
-
-__global__ void __launch_bounds__(HF_WARPS * 32)
-hyp_fill_k(int n_spec, const uint8_t* valid, const double* pmz, const int8_t* charge, int z_lo, int z_hi, int iso_lo,
-           int iso_hi, float ppm_lo, float ppm_hi, int mfc, const float* idx_mass32, int64_t n_rows,
-           const int64_t* hyp_off, int32_t* h_spec, int8_t* h_z, int8_t* h_iso, float* h_pm, float* h_M,
-           int64_t* h_lo, int64_t* h_hi, int8_t* h_maxfz) {
-  const int s = blockIdx.x * HF_WARPS + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+// Hypotheses of a spectrum (thread per spectrum): every column but the row window, in (charge, isotope) order.
+__global__ void hyp_fill_k(int n_spec, const uint8_t* valid, const double* pmz, const int8_t* charge, int z_lo,
+                           int z_hi, int iso_lo, int iso_hi, int mfc, const int64_t* hyp_off, int32_t* h_spec,
+                           int8_t* h_z, int8_t* h_iso, float* h_pm, float* h_M, int8_t* h_maxfz) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n_spec) return;
   if (!(valid[s] && isfinite(pmz[s]))) return;
-  const int64_t o = hyp_off[s];
+  int64_t o = hyp_off[s];
   const int zk = charge[s];
   const int za = zk > 0 ? zk : z_lo, zb = zk > 0 ? zk : z_hi;
-  const int n_iso = iso_hi - iso_lo + 1;
-  const int n_task = 2 * (zb - za + 1) * n_iso;
   const float mz = __fsub_rn(__double2float_rn(pmz[s]), VK_PROTON);
-  for (int t = lane; t < n_task; t += 32) {
-    const int q = t >> 1, upper = t & 1;
-    const int z = za + q / n_iso, iso = iso_lo + q % n_iso;
+  for (int z = za; z <= zb; ++z) {
     const float pm = __fmul_rn(mz, (float)z);
-    const float M = __fsub_rn(pm, __fmul_rn((float)iso, VK_NEUTRON));
-    const int64_t h = o + q;
-    if (upper) {
+    int mf = z;
+    if (mfc > 0) mf = min(z, mfc + 1);
+    mf = max(mf, 2);
+    for (int iso = iso_lo; iso <= iso_hi; ++iso) {
+      h_spec[o] = s;
+      h_z[o] = (int8_t)z;
+      h_iso[o] = (int8_t)iso;
+      h_pm[o] = pm;
+      h_M[o] = __fsub_rn(pm, __fmul_rn((float)iso, VK_NEUTRON));
+      h_maxfz[o] = (int8_t)mf;
+      ++o;
+    }
+  }
+}
+
+// Row windows: one thread per (hypothesis, bound) over the *n_hyp hypotheses, each an independent binary search
+// of the index masses (all of them in flight at once instead of one after another per spectrum).
+__global__ void hyp_window_k(const int64_t* n_hyp, const float* h_M, float ppm_lo, float ppm_hi,
+                             const float* idx_mass32, int64_t n_rows, int64_t* h_lo, int64_t* h_hi) {
+  const int64_t n2 = 2 * *n_hyp;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n2; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t h = t >> 1;
+    const float M = h_M[h];
+    if (t & 1) {
       const float hi = __fadd_rn(M, __fdiv_rn(__fmul_rn(M, ppm_hi), 1000000.0f));
       h_hi[h] = upper_bound_g(idx_mass32, n_rows, hi);
     } else {
       const float lo = __fadd_rn(M, __fdiv_rn(__fmul_rn(M, ppm_lo), 1000000.0f));
-      int mf = z;
-      if (mfc > 0) mf = min(z, mfc + 1);
-      mf = max(mf, 2);
-      h_spec[h] = s;
-      h_z[h] = (int8_t)z;
-      h_iso[h] = (int8_t)iso;
-      h_pm[h] = pm;
-      h_M[h] = M;
-      h_maxfz[h] = (int8_t)mf;
       h_lo[h] = lower_bound_g(idx_mass32, n_rows, lo);
     }
   }
@@ -333,9 +335,17 @@ int vk_hyp_fill(int n_spec, const uint8_t* valid, const double* precursor_mz, co
                 void* stream) {
   if (n_spec == 0) return 0;
   if (z_hi < z_lo || iso_hi < iso_lo) return VK_E_ARG;
-  hyp_fill_k<<<(unsigned)((n_spec + HF_WARPS - 1) / HF_WARPS), HF_WARPS * 32, 0, (cudaStream_t)stream>>>(
-      n_spec, valid, precursor_mz, charge, z_lo, z_hi, iso_lo, iso_hi, ppm_lo, ppm_hi, max_fragment_charge,
-      idx_mass32, n_rows, hyp_off, h_spec, h_z, h_iso, h_pm, h_M, h_lo, h_hi, h_maxfz);
+  cudaStream_t st = (cudaStream_t)stream;
+  hyp_fill_k<<<(unsigned)((n_spec + 255) / 256), 256, 0, st>>>(n_spec, valid, precursor_mz, charge, z_lo, z_hi, iso_lo,
+                                                                iso_hi, max_fragment_charge, hyp_off, h_spec, h_z,
+                                                                h_iso, h_pm, h_M, h_maxfz);
+  const int rc = vk_launch_status();
+  if (rc != 0) return rc;
+  int dev = 0, n_sm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+  hyp_window_k<<<(unsigned)(n_sm * 8), 256, 0, st>>>(hyp_off + n_spec, h_M, ppm_lo, ppm_hi, idx_mass32, n_rows, h_lo,
+                                                      h_hi);
   return vk_launch_status();
 }
 
