@@ -273,6 +273,11 @@ int vk_k2_cands(const vk_frag_params* fp, int n_spec, const int64_t* cand_off, c
 int vk_psm_rank(int n_spec, const int64_t* cand_off, const int64_t* c_row, const double* hs, const int16_t* mb,
                 const int16_t* my, int min_matched, int report, int64_t* psm_cand, int32_t* psm_rank,
                 double* psm_dnext, double* psm_dbest, int32_t* n_psm, void* stream);
+/* vk_psm_rank with one thread per spectrum scanning its candidates in order (a warp per spectrum above): for sparse
+ * candidate lists (a few per spectrum after the learned pruner), where most of a warp would idle.  Same outputs. */
+int vk_psm_rank_sparse(int n_spec, const int64_t* cand_off, const int64_t* c_row, const double* hs, const int16_t* mb,
+                       const int16_t* my, int min_matched, int report, int64_t* psm_cand, int32_t* psm_rank,
+                       double* psm_dnext, double* psm_dbest, int32_t* n_psm, void* stream);
 
 /* PSM table columns of every ranked slot (the features of the reference's psm_table, vulcan/gpu/engine.py:361-432,
  * computed on the device), packed into one byte buffer for a single device-to-host copy.  Slot j (0 <= j < slots,

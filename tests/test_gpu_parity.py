@@ -234,6 +234,28 @@ def test_k2_candidate_parallel_equals_warp_per_spectrum(mini, param_sets, indexe
 
 
 @pytest.mark.parametrize("name", SETS)
+def test_psm_rank_sparse_equals_warp_ranking(mini, param_sets, indexes, name, torch_cuda):
+    """vk_psm_rank_sparse (a thread per spectrum) ranks exactly like vk_psm_rank (a warp per spectrum): the same
+    slots, ranks and deltas, with 1 and 3 PSMs per spectrum."""
+    import dataclasses
+    from vulcan.gpu import engine as E
+    l1, sp, _ = mini
+    p = dataclasses.replace(param_sets[name], search_method="staged")
+    gi = indexes[name]
+    st = E.Stats()
+    out = E._search_device(E.DeviceRun(sp, gi.dev, st), gi, p, 1, st)
+    n = len(sp.charge)
+    for report in (1, 3):
+        a = E._rank_device(n, out["cand_off"], out["c_row"], out["k2"], p, report, gi.dev)
+        b = E._rank_device(n, out["cand_off"], out["c_row"], out["k2"], p, report, gi.dev, sparse=True)
+        filled = a[0] >= 0
+        assert int(filled.sum()) > 0
+        assert torch_cuda.equal(a[0], b[0]), (name, report)
+        for x, y in zip(a[1:], b[1:]):   # rank and deltas of the filled slots (empty slots leave them unwritten)
+            assert torch_cuda.equal(x[filled], y[filled]), (name, report)
+
+
+@pytest.mark.parametrize("name", SETS)
 def test_psm_pack_kernel_equals_torch_columns(mini, param_sets, indexes, name, torch_cuda):
     """vk_pack_psms (one kernel, filled slots compacted in slot order) writes the same PSM rows as the torch
     formulation of the table columns (all slots, a valid mask), bit for bit, with 1 and 3 PSMs per spectrum."""

@@ -15,35 +15,38 @@ __device__ __forceinline__ bool before(double ha, int64_t ra, double hb, int64_t
   return ha > hb || (ha == hb && ra < rb);
 }
 
-__global__ void __launch_bounds__(RK_WARPS * 32)
-psm_rank_k(int n_spec, const int64_t* cand_off, const int64_t* c_row, const double* hs, const int16_t* mb,
-           const int16_t* my, int min_matched, int report, int64_t* psm_cand, int32_t* psm_rank, double* psm_dnext,
-           double* psm_dbest, int32_t* n_psm) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int s = blockIdx.x * RK_WARPS + warp;
-  if (s >= n_spec) return;
+// Spectrum s's ranking: pass k selects the k-th element of the order (k = 0..report) among the candidates with
+// enough matched peaks, element k-1 is then written with its delta_next.  WARP: the 32 lanes of a warp scan the
+// candidates and reduce (dense lists); otherwise one thread scans them in order (sparse lists).  Candidate rows are
+// unique within a spectrum, so both find the same element.
+template <bool WARP>
+__device__ __forceinline__ void rank_spectrum(int s, int lane, const int64_t* cand_off, const int64_t* c_row,
+                                              const double* hs, const int16_t* mb, const int16_t* my,
+                                              int min_matched, int report, int64_t* psm_cand, int32_t* psm_rank,
+                                              double* psm_dnext, double* psm_dbest, int32_t* n_psm) {
   const int64_t c0 = cand_off[s], c1 = cand_off[s + 1];
   double prev_h = 0.0, best_h = 0.0, cur_h = 0.0;
   int64_t prev_r = -1, cur_c = -1;
   bool have_prev = false;
   int n = 0;
-  // pass k selects the k-th element of the order (k = 0..report); element k-1 is then written with its delta_next
   for (int k = 0; k <= report; ++k) {
     double bh = 0.0;
     int64_t br = -1, bc = -1;
-    for (int64_t c = c0 + lane; c < c1; c += 32) {
+    for (int64_t c = c0 + (WARP ? lane : 0); c < c1; c += (WARP ? 32 : 1)) {
       if ((int)mb[c] + (int)my[c] < min_matched) continue;
       double h = hs[c];
       int64_t r = c_row[c];
       if (have_prev && !before(prev_h, prev_r, h, r)) continue;
       if (bc < 0 || before(h, r, bh, br)) { bh = h; br = r; bc = c; }
     }
+    if (WARP) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      double oh = __shfl_xor_sync(VK_FULL, bh, o);
-      int64_t orr = __shfl_xor_sync(VK_FULL, br, o);
-      int64_t oc = __shfl_xor_sync(VK_FULL, bc, o);
-      if (oc >= 0 && (bc < 0 || before(oh, orr, bh, br))) { bh = oh; br = orr; bc = oc; }
+      for (int o = 16; o > 0; o >>= 1) {
+        double oh = __shfl_xor_sync(VK_FULL, bh, o);
+        int64_t orr = __shfl_xor_sync(VK_FULL, br, o);
+        int64_t oc = __shfl_xor_sync(VK_FULL, bc, o);
+        if (oc >= 0 && (bc < 0 || before(oh, orr, bh, br))) { bh = oh; br = orr; bc = oc; }
+      }
     }
     if (k > 0) {
       if (lane == 0) {
@@ -67,6 +70,26 @@ psm_rank_k(int n_spec, const int64_t* cand_off, const int64_t* c_row, const doub
     for (int k = n; k < report; ++k) psm_cand[(int64_t)s * report + k] = -1;
     n_psm[s] = n;
   }
+}
+
+__global__ void __launch_bounds__(RK_WARPS * 32)
+psm_rank_k(int n_spec, const int64_t* cand_off, const int64_t* c_row, const double* hs, const int16_t* mb,
+           const int16_t* my, int min_matched, int report, int64_t* psm_cand, int32_t* psm_rank, double* psm_dnext,
+           double* psm_dbest, int32_t* n_psm) {
+  const int s = blockIdx.x * RK_WARPS + (threadIdx.x >> 5);
+  if (s >= n_spec) return;
+  rank_spectrum<true>(s, threadIdx.x & 31, cand_off, c_row, hs, mb, my, min_matched, report, psm_cand, psm_rank,
+                      psm_dnext, psm_dbest, n_psm);
+}
+
+__global__ void __launch_bounds__(256)
+psm_rank_seq_k(int n_spec, const int64_t* cand_off, const int64_t* c_row, const double* hs, const int16_t* mb,
+               const int16_t* my, int min_matched, int report, int64_t* psm_cand, int32_t* psm_rank,
+               double* psm_dnext, double* psm_dbest, int32_t* n_psm) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n_spec) return;
+  rank_spectrum<false>(s, 0, cand_off, c_row, hs, mb, my, min_matched, report, psm_cand, psm_rank, psm_dnext,
+                       psm_dbest, n_psm);
 }
 
 // Column offsets of the packed PSM table, passed by value.
@@ -149,6 +172,17 @@ extern "C" int vk_psm_rank(int n_spec, const int64_t* cand_off, const int64_t* c
   if (n_spec == 0) return 0;
   if (report < 1) return VK_E_ARG;
   psm_rank_k<<<(unsigned)((n_spec + RK_WARPS - 1) / RK_WARPS), RK_WARPS * 32, 0, (cudaStream_t)stream>>>(
+      n_spec, cand_off, c_row, hs, mb, my, min_matched, report, psm_cand, psm_rank, psm_dnext, psm_dbest, n_psm);
+  return vk_launch_status();
+}
+
+extern "C" int vk_psm_rank_sparse(int n_spec, const int64_t* cand_off, const int64_t* c_row, const double* hs,
+                                  const int16_t* mb, const int16_t* my, int min_matched, int report,
+                                  int64_t* psm_cand, int32_t* psm_rank, double* psm_dnext, double* psm_dbest,
+                                  int32_t* n_psm, void* stream) {
+  if (n_spec == 0) return 0;
+  if (report < 1) return VK_E_ARG;
+  psm_rank_seq_k<<<(unsigned)((n_spec + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
       n_spec, cand_off, c_row, hs, mb, my, min_matched, report, psm_cand, psm_rank, psm_dnext, psm_dbest, n_psm);
   return vk_launch_status();
 }

@@ -99,6 +99,7 @@ _SIGS_B200 = {
     "vk_k2_cands": [P, I32, P, P, P, P, P, P, P, P, P, P, P, F32, F32, P, P, P, P, P, P, P, P, P],
     "vk_pack_psms": [P, I64, I32, P, P, P, P],
     "vk_psm_rank": [I32, P, P, P, P, P, I32, I32, P, P, P, P, P, P],
+    "vk_psm_rank_sparse": [I32, P, P, P, P, P, I32, I32, P, P, P, P, P, P],
     "vk_search_fused": [P, P, P, I32, I32, I32, P, P, P, P, P, P, P, P, P, P],
     "vk_search_fused_smem": [P, I32, I32, I32, I32, P],
     "vk_search_fused_grid": [P, I32, I32, I32, I32, P],

@@ -552,7 +552,9 @@ def lnfact(n):
     return np.where(n == 0, 1.0, v)
 
 
-def _rank_device(n_spec, cand_off, rows, k2, p: SearchParams, report: int, dev):
+def _rank_device(n_spec, cand_off, rows, k2, p: SearchParams, report: int, dev, sparse: bool = False):
+    """PSM ranking per spectrum (``vk_psm_rank``; ``vk_psm_rank_sparse``, a thread per spectrum, for the few
+    candidates per spectrum the pruner leaves).  Same outputs."""
     L = K.lib()
     slots = max(n_spec * report, 1)
     psm_cand = torch.empty(slots, dtype=torch.int64, device=dev)
@@ -560,9 +562,10 @@ def _rank_device(n_spec, cand_off, rows, k2, p: SearchParams, report: int, dev):
     dnext = torch.empty(slots, dtype=torch.float64, device=dev)
     dbest = torch.empty(slots, dtype=torch.float64, device=dev)
     n_psm = torch.empty(max(n_spec, 1), dtype=torch.int32, device=dev)
-    K.check(L.vk_psm_rank(n_spec, K.ptr(cand_off), K.ptr(rows), K.ptr(k2["hyperscore"]), K.ptr(k2["matched_b"]),
-                          K.ptr(k2["matched_y"]), p.min_matched_peaks, report, K.ptr(psm_cand), K.ptr(psm_rank),
-                          K.ptr(dnext), K.ptr(dbest), K.ptr(n_psm), K.stream()), "psm_rank")
+    fn = L.vk_psm_rank_sparse if sparse else L.vk_psm_rank
+    K.check(fn(n_spec, K.ptr(cand_off), K.ptr(rows), K.ptr(k2["hyperscore"]), K.ptr(k2["matched_b"]),
+               K.ptr(k2["matched_y"]), p.min_matched_peaks, report, K.ptr(psm_cand), K.ptr(psm_rank), K.ptr(dnext),
+               K.ptr(dbest), K.ptr(n_psm), K.stream()), "psm_rank")
     return psm_cand[:n_spec * report], psm_rank[:n_spec * report], dnext[:n_spec * report], dbest[:n_spec * report]
 
 

@@ -296,7 +296,7 @@ def _pruned_device(run: E.DeviceRun, gi: E.GpuIndex, p: SearchParams, pr: Pruner
     with phase("k2"):
         k2 = E._k2_cands(gi, p, n, cand, f["peaks"], sparse=True)
     with phase("rank"):
-        psm = E._rank_device(n, cand["cand_off"], cand["c_row"], k2, p, report, dev)
+        psm = E._rank_device(n, cand["cand_off"], cand["c_row"], k2, p, report, dev, sparse=True)
     return {**f, **cand, "logit": logit, "feat": feat, "k2": k2, "psm": psm}
 
 
