@@ -507,8 +507,9 @@ def test_tiles_too_large_for_shared_memory_are_refused(mini, param_sets, torch_c
 
 @pytest.mark.parametrize("name", ("da", "ppm"))
 def test_k0_easy_and_hard_spectra(mini, param_sets, name, torch_cuda):
-    """Sorted spectra take the stream-copy path; shuffled ones, ones with a NaN m/z and ones with more in-range
-    peaks than max_peaks take the sorting path: every spectrum equals the oracle's peak view."""
+    """Sorted spectra take the stream-copy path, sorted ones with more in-range peaks than max_peaks the selection
+    path (threshold ties included: every peak twice), shuffled ones and ones with a NaN m/z the sorting path: every
+    spectrum equals the oracle's peak view."""
     from oracle import oracle as O
     from vulcan.gpu import engine as E
     from vulcan.gpu.host import Spectra
@@ -532,6 +533,9 @@ def test_k0_easy_and_hard_spectra(mini, param_sets, name, torch_cuda):
         off.append(off[-1] + len(m))
     sp2 = Spectra("mixed", sp.scan, sp.index, sp.rt, sp.precursor_mz, sp.charge, np.concatenate(mz).astype(np.float32),
                   np.concatenate(it).astype(np.float32), np.array(off, np.int64))
+    in_order_over = sum(1 for m in mz if len(m) and np.all(np.diff(m) >= 0) and
+                        int(((m >= p.fragment_min_mz) & (m <= p.fragment_max_mz)).sum()) > p.max_peaks)
+    assert in_order_over > 0   # the selection path is reached
     pk = E.k0_preprocess(sp2, p, torch_cuda.device("cuda"), E.Stats())
     ref = O.k0_view(sp2, p)
     assert np.array_equal(pk["off"].cpu().numpy(), ref["off"])

@@ -75,7 +75,7 @@ __global__ void k0_count_k(int n_spec, const int64_t* raw_off, const float* raw_
   if (lane == 0) {
     kept[warp] = min(c, (long long)max_peaks);
     const bool e = sorted && c <= max_peaks;
-    easy[warp] = e;
+    easy[warp] = e ? 1 : (sorted ? 2 : 0);   // 2: in order, more than max_peaks in range (selection, no sort)
     if (!e) hard_list[atomicAdd(n_hard, 1)] = warp;
   }
 }
@@ -86,7 +86,7 @@ __global__ void k0_easy_k(int n_spec, const int64_t* raw_off, const float* raw_m
                           float fmax, int min_peaks, const int64_t* pk_off, float* pk_mass, float* pk_int, float* tic,
                           uint8_t* valid, const uint8_t* easy) {
   const int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (s >= n_spec || !easy[s]) return;
+  if (s >= n_spec || easy[s] != 1) return;
   const unsigned lt_mask = (1u << lane) - 1u;
   const int64_t r0 = raw_off[s], r1 = raw_off[s + 1];
   const int64_t o0 = pk_off[s];
@@ -139,17 +139,134 @@ __device__ __forceinline__ void block_bitonic_u64(uint64_t* v, int n_pow2) {
 
 constexpr int K0_THREADS = 512;
 
+// Exclusive scan of one int per thread over the CTA (K0_THREADS threads); wsum: K0_THREADS / 32 ints of scratch.
+__device__ __forceinline__ int k0_block_excl_scan(int v, int* wsum) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int inc = (int)vk::warp_incl_scan(v);
+  if (lane == 31) wsum[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    const int w = lane < K0_THREADS / 32 ? wsum[lane] : 0;
+    const int wi = (int)vk::warp_incl_scan(w);
+    if (lane < K0_THREADS / 32) wsum[lane] = wi - w;
+  }
+  __syncthreads();
+  const int r = wsum[warp] + inc - v;
+  __syncthreads();
+  return r;
+}
+
+// A spectrum whose raw peaks are in (mass asc, intensity desc) order but with more than max_peaks in range: the
+// kept peaks are the `kept` smallest selection keys (~ord(intensity), ~ord(mass)), found by an 8-bit radix select in
+// shared memory, and their output order is the input order, so a compaction replaces both sorts.  Keys equal to
+// the threshold are taken in input order (equal keys are equal peaks).  Writes pk_mass / pk_int[o0, o0 + kept).
+__device__ __forceinline__ void k0_select(uint64_t* keys, int n, int kept, const float* mz, const float* it,
+                                          float fmin, float fmax, float* pk_mass, float* pk_int, int64_t o0,
+                                          uint32_t* hist, int* wsum, int* bcast) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (kept <= 0) return;   // nothing kept (max_peaks 0): no selection (uniform over the CTA)
+  for (int i = tid; i < n; i += K0_THREADS) {
+    const float m = mz[i];
+    keys[i] = in_range(m, fmin, fmax)
+                  ? ((uint64_t)(~ord_f32(it[i])) << 32) | (uint64_t)(~ord_f32(__fsub_rn(m, VK_PROTON)))
+                  : ~0ull;
+  }
+  uint64_t prefix = 0ull, pmask = 0ull;
+  int need = kept;   // the need-th smallest key among those matching the digits chosen so far
+  for (int shift = 56; shift >= 0; shift -= 8) {
+    for (int i = tid; i < 256; i += K0_THREADS) hist[i] = 0u;
+    __syncthreads();
+    for (int i = tid; i < n; i += K0_THREADS) {
+      const uint64_t k = keys[i];
+      if ((k & pmask) == prefix) atomicAdd(&hist[(k >> shift) & 255], 1u);
+    }
+    __syncthreads();
+    if (warp == 0) {
+      uint32_t c[8], tot = 0u;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        c[q] = hist[lane * 8 + q];
+        tot += c[q];
+      }
+      const int inc = (int)vk::warp_incl_scan((long long)tot);
+      const int exc = inc - (int)tot;
+      if (exc < need && need <= inc) {   // the lane whose digits hold the need-th key
+        int cum = exc, d = lane * 8 + 7;
+        for (int q = 0; q < 8; ++q) {
+          if (cum + (int)c[q] >= need) {
+            d = lane * 8 + q;
+            break;
+          }
+          cum += (int)c[q];
+        }
+        bcast[0] = d;
+        bcast[1] = need - cum;
+      }
+    }
+    __syncthreads();
+    prefix |= (uint64_t)bcast[0] << shift;
+    pmask |= 255ull << shift;
+    need = bcast[1];
+    __syncthreads();
+  }
+  // compaction in input order: contiguous chunks per thread, keys below the threshold and the first `need` equal
+  const int per = (n + K0_THREADS - 1) / K0_THREADS;
+  const int a = min(n, tid * per), b = min(n, a + per);
+  int eq = 0;
+  for (int i = a; i < b; ++i) eq += keys[i] == prefix;
+  const int eq_base = k0_block_excl_scan(eq, wsum);
+  int cnt = 0, er = eq_base;
+  for (int i = a; i < b; ++i) {
+    const uint64_t k = keys[i];
+    if (k < prefix) ++cnt;
+    else if (k == prefix) cnt += er++ < need;
+  }
+  int pos = k0_block_excl_scan(cnt, wsum);
+  er = eq_base;
+  for (int i = a; i < b; ++i) {
+    const uint64_t k = keys[i];
+    const bool take = k < prefix || (k == prefix && er++ < need);
+    if (take) {
+      pk_int[o0 + pos] = unord_f32(~(uint32_t)(k >> 32));
+      pk_mass[o0 + pos] = unord_f32(~(uint32_t)k);
+      ++pos;
+    }
+  }
+}
+
 __global__ void __launch_bounds__(K0_THREADS)
 k0_fill_k(const int32_t* hard_list, const int32_t* n_hard, const int64_t* raw_off, const float* raw_mz,
           const float* raw_int, float fmin, float fmax, int max_peaks, int min_peaks, const int64_t* pk_off,
-          float* pk_mass, float* pk_int, float* tic, uint8_t* valid) {
+          float* pk_mass, float* pk_int, float* tic, uint8_t* valid, const uint8_t* easy) {
   extern __shared__ uint64_t k0_keys[];
   __shared__ double red[K0_THREADS / 32];
+  __shared__ uint32_t hist[256];
+  __shared__ int wsum[K0_THREADS / 32], bcast[2];
   const int n_work = *n_hard;
   for (int j = blockIdx.x; j < n_work; j += gridDim.x) {
   const int s = hard_list[j];
   const int64_t r0 = raw_off[s];
   const int n = (int)(raw_off[s + 1] - r0);
+  if (easy[s] == 2) {   // in order, too many peaks in range: selection and compaction
+    const int64_t o0 = pk_off[s];
+    const int kept = (int)(pk_off[s + 1] - o0);
+    k0_select(k0_keys, n, kept, raw_mz + r0, raw_int + r0, fmin, fmax, pk_mass, pk_int, o0, hist, wsum, bcast);
+    __syncthreads();   // the block's writes are visible to the TIC sum below
+    double part = 0.0;
+    for (int i = threadIdx.x; i < kept; i += blockDim.x) part += (double)pk_int[o0 + i];   // the sort path's order
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(VK_FULL, part, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = part;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < K0_THREADS / 32; ++w) t += red[w];
+      tic[s] = (float)t;
+      valid[s] = kept >= min_peaks;
+    }
+    __syncthreads();
+    continue;
+  }
   int n_pow2 = 1;
   while (n_pow2 < n) n_pow2 <<= 1;
   for (int i = threadIdx.x; i < n_pow2; i += blockDim.x) {
@@ -315,7 +432,7 @@ int vk_k0_fill(int n_spec, const int64_t* raw_off, const float* raw_mz, const fl
   if (e != cudaSuccess) return vk_err(e);
   const int grid = (int)min((int64_t)n_sm * 8, (int64_t)n_spec);
   k0_fill_k<<<grid, K0_THREADS, sh, st>>>(hard_list, n_hard, raw_off, raw_mz, raw_int, fmin, fmax, max_peaks,
-                                          min_peaks, pk_off, pk_mass, pk_int, tic, valid);
+                                          min_peaks, pk_off, pk_mass, pk_int, tic, valid, easy);
   return vk_launch_status();
 }
 
