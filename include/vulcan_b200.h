@@ -161,13 +161,14 @@ int vk_scan_i64_noalloc(const int64_t* in, int64_t n, int64_t* out, void* stream
 
 /* K0 peak view (reference vulcan/gpu/engine.py:171-210), two calls: vk_k0_count writes kept[n_spec] (i64) =
  * min(#peaks with fmin <= mz <= fmax and not NaN, max_peaks), easy[n_spec] (u8: 1 = the raw peaks are already in
- * (mass asc, intensity desc) order, no NaN, at most max_peaks in range; 2 = in that order with more in range; 0 =
- * otherwise) and the other spectra's indices into
- * hard_list[n_spec] (i32, any order) with their number in *n_hard (device i32, zeroed by the call); after the
- * caller's scan of kept into pk_off[n_spec+1], vk_k0_fill writes mass-sorted peaks (mass = mz - PROTON) of the top
- * max_peaks by (intensity desc, mass desc), tic[n_spec] (f32 of the f64 sum) and valid[n_spec] (u8, kept >=
- * min_peaks): easy spectra by a stream copy, in-order spectra with too many peaks by a radix selection and a
- * compaction in shared memory, the others by shared-memory sorts.  max_raw (host) = the largest
+ * (mass asc, intensity desc) order, no NaN, at most max_peaks in range; 2 = in that order with more in range and
+ * at most 512 raw peaks; 3 = the same with more raw peaks; 0 = otherwise) and the indices of the code 0 and 3
+ * spectra into hard_list[n_spec] (i32, any order) with their number in *n_hard (device i32, zeroed by the call);
+ * after the caller's scan of kept into pk_off[n_spec+1], vk_k0_fill writes mass-sorted peaks (mass = mz - PROTON)
+ * of the top max_peaks by (intensity desc, mass desc), tic[n_spec] (f32 of the f64 sum) and valid[n_spec] (u8,
+ * kept >= min_peaks): code 1 by a stream copy, code 2 by a warp each and code 3 by a CTA each (radix selection of
+ * the kept peaks, compaction in input order), code 0 (unsorted or NaN m/z) by shared-memory sorts.  max_raw
+ * (host) = the largest
  * raw peak count of a spectrum, at most 16384 (one CTA sorts a spectrum in shared memory). */
 int vk_k0_count(int n_spec, const int64_t* raw_off, const float* raw_mz, const float* raw_int, float fmin,
                 float fmax, int max_peaks, int64_t* kept, uint8_t* easy, int32_t* hard_list, int32_t* n_hard,

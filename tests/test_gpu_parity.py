@@ -508,8 +508,8 @@ def test_tiles_too_large_for_shared_memory_are_refused(mini, param_sets, torch_c
 @pytest.mark.parametrize("name", ("da", "ppm"))
 def test_k0_easy_and_hard_spectra(mini, param_sets, name, torch_cuda):
     """Sorted spectra take the stream-copy path, sorted ones with more in-range peaks than max_peaks the selection
-    path (threshold ties included: every peak twice), shuffled ones and ones with a NaN m/z the sorting path: every
-    spectrum equals the oracle's peak view."""
+    paths (a warp up to 512 raw peaks, a CTA above; threshold ties included: every peak twice), shuffled ones and
+    ones with a NaN m/z the sorting path: every spectrum equals the oracle's peak view."""
     from oracle import oracle as O
     from vulcan.gpu import engine as E
     from vulcan.gpu.host import Spectra
@@ -528,14 +528,19 @@ def test_k0_easy_and_hard_spectra(mini, param_sets, name, torch_cuda):
             m[len(m) // 2] = np.nan
         elif kind == 3 and len(m) > 2:    # every peak twice (ties in mass and intensity), still sorted
             m, i = np.repeat(m, 2), np.repeat(i, 2)
+        if s in (0, 4):                   # sorted, 400 and 900 raw peaks: both selection paths
+            n_raw = 400 if s == 0 else 900
+            m = np.sort(rng.uniform(150, 1900, n_raw)).astype(np.float32)
+            i = rng.lognormal(7, 1, n_raw).astype(np.float32)
         mz.append(m)
         it.append(i)
         off.append(off[-1] + len(m))
     sp2 = Spectra("mixed", sp.scan, sp.index, sp.rt, sp.precursor_mz, sp.charge, np.concatenate(mz).astype(np.float32),
                   np.concatenate(it).astype(np.float32), np.array(off, np.int64))
-    in_order_over = sum(1 for m in mz if len(m) and np.all(np.diff(m) >= 0) and
-                        int(((m >= p.fragment_min_mz) & (m <= p.fragment_max_mz)).sum()) > p.max_peaks)
-    assert in_order_over > 0   # the selection path is reached
+    in_order_over = [len(m) for m in mz if len(m) and np.all(np.diff(m) >= 0) and
+                     int(((m >= p.fragment_min_mz) & (m <= p.fragment_max_mz)).sum()) > p.max_peaks]
+    assert any(n <= 512 for n in in_order_over)   # the warp selection path is reached
+    assert any(n > 512 for n in in_order_over)    # the CTA selection path is reached
     pk = E.k0_preprocess(sp2, p, torch_cuda.device("cuda"), E.Stats())
     ref = O.k0_view(sp2, p)
     assert np.array_equal(pk["off"].cpu().numpy(), ref["off"])

@@ -29,6 +29,7 @@ __device__ __forceinline__ bool in_range(float mz, float fmin, float fmax) {
 }
 
 constexpr int K0_UNROLL = 4;   // raw-peak chunks of 32 loaded ahead per warp
+constexpr int K0_WARP_SELECT = 512;   // in-order spectra up to this many raw peaks are selected by one warp
 
 // mass-order key of a peak: ascending = mass ascending, then intensity descending
 __device__ __forceinline__ uint64_t mass_key(float mz, float it) {
@@ -74,22 +75,115 @@ __global__ void k0_count_k(int n_spec, const int64_t* raw_off, const float* raw_
   sorted = __all_sync(VK_FULL, sorted);
   if (lane == 0) {
     kept[warp] = min(c, (long long)max_peaks);
-    const bool e = sorted && c <= max_peaks;
-    easy[warp] = e ? 1 : (sorted ? 2 : 0);   // 2: in order, more than max_peaks in range (selection, no sort)
-    if (!e) hard_list[atomicAdd(n_hard, 1)] = warp;
+    // 1: in order, at most max_peaks in range (copy); 2: in order, more in range, at most K0_WARP_SELECT raw
+    // peaks (warp selection); 3: the same with more raw peaks (CTA selection); 0: sort
+    const int code = sorted ? (c <= max_peaks ? 1 : (r1 - r0 <= K0_WARP_SELECT ? 2 : 3)) : 0;
+    easy[warp] = (uint8_t)code;
+    if (code == 0 || code == 3) hard_list[atomicAdd(n_hard, 1)] = warp;
   }
 }
 
-// Easy spectra: the in-range peaks in input order (ballot compaction), TIC as the f64 sum of lane partials
-// (lane order, then a butterfly), the same order as the sorting kernels use for sorted input.
-__global__ void k0_easy_k(int n_spec, const int64_t* raw_off, const float* raw_mz, const float* raw_int, float fmin,
-                          float fmax, int min_peaks, const int64_t* pk_off, float* pk_mass, float* pk_int, float* tic,
-                          uint8_t* valid, const uint8_t* easy) {
+// Warp per in-order spectrum of code 1 or 2 (codes 0 and 3 are the CTA kernel's).  Code 1 (at most max_peaks in range): the in-range peaks in input order (ballot
+// compaction).  Code 2 (more in range): the kept peaks are the `kept` smallest selection keys (~ord(intensity),
+// ~ord(mass)) -- an 8-bit radix select over the spectrum's peaks (re-read each pass, a warp-private histogram) --
+// taken in input order, which is the output order; keys equal to the threshold (equal peaks) in input order.  TIC
+// as the f64 sum of lane partials (lane order, then a butterfly).
+constexpr int KE_WARPS = 8;
+
+__device__ __forceinline__ uint64_t k0_sel_key(float mz, float it) {
+  return ((uint64_t)(~ord_f32(it)) << 32) | (uint64_t)(~ord_f32(__fsub_rn(mz, VK_PROTON)));
+}
+
+__global__ void __launch_bounds__(KE_WARPS * 32)
+k0_easy_k(int n_spec, const int64_t* raw_off, const float* raw_mz, const float* raw_int, float fmin, float fmax,
+          int min_peaks, const int64_t* pk_off, float* pk_mass, float* pk_int, float* tic, uint8_t* valid,
+          const uint8_t* easy) {
+  __shared__ uint32_t whist[KE_WARPS][256];
   const int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (s >= n_spec || easy[s] != 1) return;
+  if (s >= n_spec) return;
+  const int code = easy[s];
+  if (code != 1 && code != 2) return;   // 0 and 3: the CTA kernel
+  if (code == 2) {
+    const unsigned lt = (1u << lane) - 1u;
+    const int64_t r0 = raw_off[s], r1 = raw_off[s + 1], o0 = pk_off[s];
+    const int kept = (int)(pk_off[s + 1] - o0);
+    uint32_t* hist = whist[threadIdx.x >> 5];
+    uint64_t prefix = 0ull, pmask = 0ull;
+    int need = kept;   // the need-th smallest key among those matching the digits chosen so far
+    for (int shift = 56; shift >= 0 && kept > 0; shift -= 8) {
+      for (int q = lane; q < 256; q += 32) hist[q] = 0u;
+      __syncwarp();
+      for (int64_t i = r0 + lane; i < r1; i += 32) {
+        const float m = raw_mz[i];
+        const uint64_t k = in_range(m, fmin, fmax) ? k0_sel_key(m, raw_int[i]) : ~0ull;
+        if ((k & pmask) == prefix) atomicAdd(&hist[(k >> shift) & 255], 1u);
+      }
+      __syncwarp();
+      uint32_t c[8], tot = 0u;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        c[q] = hist[lane * 8 + q];
+        tot += c[q];
+      }
+      const int inc = (int)vk::warp_incl_scan((long long)tot), exc = inc - (int)tot;
+      const bool mine = exc < need && need <= inc;   // the lane whose digits hold the need-th key
+      int d = 0, rem = 0;
+      if (mine) {
+        int cum = exc;
+        d = lane * 8 + 7;
+        for (int q = 0; q < 8; ++q) {
+          if (cum + (int)c[q] >= need) {
+            d = lane * 8 + q;
+            break;
+          }
+          cum += (int)c[q];
+        }
+        rem = need - cum;
+      }
+      const unsigned who = __ballot_sync(VK_FULL, mine);
+      const int src = who ? __ffs(who) - 1 : 0;
+      d = __shfl_sync(VK_FULL, d, src);
+      need = __shfl_sync(VK_FULL, rem, src);
+      prefix |= (uint64_t)d << shift;
+      pmask |= 255ull << shift;
+      __syncwarp();
+    }
+    double part = 0.0;
+    int w = 0, eq_seen = 0;
+    for (int64_t i0 = r0; i0 < r1 && kept > 0; i0 += 32) {
+      const int64_t i = i0 + lane;
+      float m = 0.f, it = 0.f;
+      uint64_t k = ~0ull;
+      if (i < r1) {
+        m = raw_mz[i];
+        it = raw_int[i];
+        if (in_range(m, fmin, fmax)) k = k0_sel_key(m, it);
+      }
+      const bool eq = i < r1 && k == prefix;
+      const unsigned eqb = __ballot_sync(VK_FULL, eq);
+      const bool take = i < r1 && (k < prefix || (eq && eq_seen + __popc(eqb & lt) < need));
+      const unsigned tb = __ballot_sync(VK_FULL, take);
+      const int pos = w + __popc(tb & lt);
+      if (take && pos < kept) {
+        pk_mass[o0 + pos] = __fsub_rn(m, VK_PROTON);
+        pk_int[o0 + pos] = it;
+        part += (double)it;
+      }
+      w += __popc(tb);
+      eq_seen += __popc(eqb);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(VK_FULL, part, o);
+    if (lane == 0) {
+      tic[s] = (float)part;
+      valid[s] = kept >= min_peaks;
+    }
+    return;
+  }
   const unsigned lt_mask = (1u << lane) - 1u;
   const int64_t r0 = raw_off[s], r1 = raw_off[s + 1];
   const int64_t o0 = pk_off[s];
+  const int n_out = (int)(pk_off[s + 1] - o0);   // the in-range count: every write stays in the slot
   double part = 0.0;
   int w = 0;
   for (int64_t b0 = r0; b0 < r1; b0 += 32 * K0_UNROLL) {
@@ -105,8 +199,8 @@ __global__ void k0_easy_k(int n_spec, const int64_t* raw_off, const float* raw_m
       const int64_t i = b0 + 32 * u + lane;
       const bool take = i < r1 && in_range(mzv[u], fmin, fmax);
       const unsigned m = __ballot_sync(VK_FULL, take);
-      if (take) {
-        const int pos = w + __popc(m & lt_mask);
+      const int pos = w + __popc(m & lt_mask);
+      if (take && pos < n_out) {
         pk_mass[o0 + pos] = __fsub_rn(mzv[u], VK_PROTON);
         pk_int[o0 + pos] = itv[u];
         part += (double)itv[u];
@@ -118,7 +212,7 @@ __global__ void k0_easy_k(int n_spec, const int64_t* raw_off, const float* raw_m
   for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(VK_FULL, part, o);
   if (lane == 0) {
     tic[s] = (float)part;
-    valid[s] = (int)(pk_off[s + 1] - o0) >= min_peaks;
+    valid[s] = n_out >= min_peaks;
   }
 }
 
@@ -247,7 +341,7 @@ k0_fill_k(const int32_t* hard_list, const int32_t* n_hard, const int64_t* raw_of
   const int s = hard_list[j];
   const int64_t r0 = raw_off[s];
   const int n = (int)(raw_off[s + 1] - r0);
-  if (easy[s] == 2) {   // in order, too many peaks in range: selection and compaction
+  if (easy[s] == 3) {   // in order, too many peaks in range, a large spectrum: CTA selection
     const int64_t o0 = pk_off[s];
     const int kept = (int)(pk_off[s + 1] - o0);
     k0_select(k0_keys, n, kept, raw_mz + r0, raw_int + r0, fmin, fmax, pk_mass, pk_int, o0, hist, wsum, bcast);
@@ -417,14 +511,15 @@ int vk_k0_fill(int n_spec, const int64_t* raw_off, const float* raw_mz, const fl
   if (max_raw < 0 || max_raw > 16384) return VK_E_ARG;
   cudaStream_t st = (cudaStream_t)stream;
   int64_t threads = (int64_t)n_spec * 32;
-  k0_easy_k<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(n_spec, raw_off, raw_mz, raw_int, fmin, fmax,
-                                                                min_peaks, pk_off, pk_mass, pk_int, tic, valid, easy);
+  k0_easy_k<<<(unsigned)((threads + KE_WARPS * 32 - 1) / (KE_WARPS * 32)), KE_WARPS * 32, 0, st>>>(
+      n_spec, raw_off, raw_mz, raw_int, fmin, fmax, min_peaks, pk_off, pk_mass, pk_int, tic, valid, easy);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return vk_err(e);
   int dev = 0, n_sm = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-  // hard spectra (unsorted, NaN, or more than max_peaks in range): one CTA each, sorting in shared memory
+  // hard spectra (unsorted or NaN: sorted; in order with more than max_peaks in range and more than
+  // K0_WARP_SELECT raw peaks: selected): one CTA each, keys in shared memory
   int n_pow2 = 32;
   while (n_pow2 < max_raw) n_pow2 <<= 1;
   size_t sh = (size_t)n_pow2 * sizeof(uint64_t);
