@@ -178,6 +178,22 @@ int vk_k0_fill(int n_spec, const int64_t* raw_off, const float* raw_mz, const fl
                float* tic, uint8_t* valid, int max_raw, const uint8_t* easy, const int32_t* hard_list,
                const int32_t* n_hard, void* stream);
 
+/* K0 peak view in the window peak mode (reference vulcan/gpu/engine.py:182-183, peak_mode "window"), the same two
+ * calls and buffers: the top window_k peaks (intensity desc, mass desc) of every window w = floor(mz * (1.0f /
+ * window_th)) (f32, the reference's division of an f32 CUDA tensor by a Python float) of the in-range peaks, then
+ * mass ascending (equal masses: window ascending, then intensity descending); no cap on the total.  kept[s] =
+ * sum over windows of min(count, window_k); easy[s]: 1 = already in that order with no window over window_k (a
+ * copy), 2 = in that order, some window over window_k, none over 128 peaks (a warp), 0 = otherwise (hard_list, a
+ * CTA sort).  VK_E_ARG unless window_th > 0 and 0 <= floor(fmin / window_th), floor(fmax / window_th) <= 999 (the
+ * reference's group id spectrum * 1000 + window lets windows of neighbouring spectra merge beyond that). */
+int vk_k0w_count(int n_spec, const int64_t* raw_off, const float* raw_mz, const float* raw_int, float fmin,
+                 float fmax, float window_th, int window_k, int64_t* kept, uint8_t* easy, int32_t* hard_list,
+                 int32_t* n_hard, void* stream);
+int vk_k0w_fill(int n_spec, const int64_t* raw_off, const float* raw_mz, const float* raw_int, float fmin,
+                float fmax, float window_th, int window_k, int min_peaks, const int64_t* pk_off, float* pk_mass,
+                float* pk_int, float* tic, uint8_t* valid, int max_raw, const uint8_t* easy,
+                const int32_t* hard_list, const int32_t* n_hard, void* stream);
+
 /* Hypotheses (reference vulcan/gpu/host.py:64-91), two calls like K0: vk_hyp_count writes n_hyp[n_spec] (i64);
  * vk_hyp_fill writes, at hyp_off[s], the spectrum's hypotheses in (charge, isotope) order with f32 Sage
  * arithmetic and the row window [lo, hi) by binary search of the mass-sorted index masses (hyp_off: the scan of

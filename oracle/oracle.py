@@ -88,7 +88,12 @@ def n_threads() -> int:
 def k0_view(sp, p):
     """engine.py:171-210 on the CPU: keep fragment_min_mz <= mz <= fragment_max_mz (not NaN), mass = mz - PROTON,
     top max_peaks per spectrum by (intensity desc, mass desc, input order), then mass ascending (ties keep
-    that order).  TIC = f64 sum of the kept intensities.  valid = kept >= min_peaks."""
+    that order).  TIC = f64 sum of the kept intensities.  valid = kept >= min_peaks.
+
+    Window peak mode (any peak_mode but "global", engine.py:182-183): the groups are spectrum * 1000 +
+    floor(mz / window_th) and window_k peaks are kept per group.  The reference evaluates the division on an f32
+    CUDA tensor with a Python float divisor, which the device computes as mz * (1.0f / f32(window_th)) in f32; this
+    restatement does the same."""
     n = len(sp.offsets) - 1
     mz = np.asarray(sp.mz, np.float32)
     it = np.asarray(sp.intensity, np.float32)
@@ -96,13 +101,19 @@ def k0_view(sp, p):
     seg = np.repeat(np.arange(n), lens)
     keep = (mz >= np.float32(p.fragment_min_mz)) & (mz <= np.float32(p.fragment_max_mz)) & ~np.isnan(mz)
     mass = (mz - PROTON).astype(np.float32)
-    seg, mass, it = seg[keep], mass[keep], it[keep]
+    seg, mass, it, mzk = seg[keep], mass[keep], it[keep], mz[keep]
+    if p.peak_mode == "global":
+        grp, kk = seg, p.max_peaks
+    else:
+        inv = np.float32(1.0) / np.float32(p.window_th)
+        grp = seg * 1000 + np.floor((mzk * inv).astype(np.float32)).astype(np.int64)
+        kk = p.window_k
     idx = np.arange(len(seg))
-    o = np.lexsort((idx, -mass.astype(np.float64), -it.astype(np.float64), seg))
-    g = seg[o]
+    o = np.lexsort((idx, -mass.astype(np.float64), -it.astype(np.float64), grp))
+    g = grp[o]
     first = np.searchsorted(g, g, side="left")
     rank = np.arange(len(g)) - first
-    o = o[rank < p.max_peaks]
+    o = o[rank < kk]
     pos = np.empty(len(o), np.int64)
     pos[:] = np.arange(len(o))
     o2 = np.lexsort((pos, mass[o], seg[o]))

@@ -182,3 +182,22 @@ def test_k2_hyperscore_within_fp64_oracle(mini, golden_py, param_sets, name):
     assert same.mean() > 0.999
     rel = np.abs(a["hyperscore"][same] - b["hyperscore"][same]) / np.abs(b["hyperscore"][same])
     assert rel.max() <= 1e-5
+
+
+@pytest.mark.parametrize("name", ("win100", "win64", "win12"))
+def test_k0_window_view_equals_reference(name):
+    """The window peak mode (engine.py:182-183) against the reference's own K0 on the fixture spectra and the
+    window edge cases of golden_window.npz."""
+    import os
+    from tests.golden.make_golden_window import WINDOW_SETS
+    from vulcan.gpu.host import SearchParams, Spectra
+    g = dict(np.load(os.path.join(os.path.dirname(__file__), "golden", "golden_window.npz")))
+    sp = Spectra("window", g["w_scan"], g["w_index"], g["w_rt"], g["w_precursor_mz"], g["w_charge"], g["w_mz"],
+                 g["w_intensity"], g["w_offsets"])
+    pk = O.k0_view(sp, SearchParams(**WINDOW_SETS[name]))
+    assert np.array_equal(pk["off"], g[f"{name}/k0_off"])
+    assert np.array_equal(pk["mass"], g[f"{name}/k0_mass"])
+    assert np.array_equal(pk["int"], g[f"{name}/k0_int"])
+    assert np.array_equal(pk["valid"], g[f"{name}/k0_valid"])
+    np.testing.assert_allclose(pk["tic"], g[f"{name}/k0_tic"], rtol=1e-7)
+    assert (np.diff(pk["off"]) > 15).any()   # some spectra keep more than a window's worth

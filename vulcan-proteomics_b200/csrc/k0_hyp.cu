@@ -12,21 +12,9 @@
 // Hypotheses (reference vulcan/gpu/host.py:64-91): per valid spectrum with a finite precursor m/z, charges (the
 // known one, else the configured range) x isotope errors in (charge, isotope) order, Sage f32 arithmetic, row
 // window [lower_bound(lo), upper_bound(hi)) over the mass-sorted index masses.
-#include "common.cuh"
+#include "k0_impl.cuh"
 
 namespace {
-
-__device__ __forceinline__ uint32_t ord_f32(float x) {
-  uint32_t u = __float_as_uint(x);
-  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
-}
-__device__ __forceinline__ float unord_f32(uint32_t o) {
-  uint32_t u = (o & 0x80000000u) ? (o & 0x7fffffffu) : ~o;
-  return __uint_as_float(u);
-}
-__device__ __forceinline__ bool in_range(float mz, float fmin, float fmax) {
-  return mz >= fmin && mz <= fmax;   // false for NaN
-}
 
 constexpr int K0_UNROLL = 4;   // raw-peak chunks of 32 loaded ahead per warp
 constexpr int K0_WARP_SELECT = 512;   // in-order spectra up to this many raw peaks are selected by one warp
@@ -83,11 +71,11 @@ __global__ void k0_count_k(int n_spec, const int64_t* raw_off, const float* raw_
   }
 }
 
-// Warp per in-order spectrum of code 1 or 2 (codes 0 and 3 are the CTA kernel's).  Code 1 (at most max_peaks in range): the in-range peaks in input order (ballot
-// compaction).  Code 2 (more in range): the kept peaks are the `kept` smallest selection keys (~ord(intensity),
-// ~ord(mass)) -- an 8-bit radix select over the spectrum's peaks (re-read each pass, a warp-private histogram) --
-// taken in input order, which is the output order; keys equal to the threshold (equal peaks) in input order.  TIC
-// as the f64 sum of lane partials (lane order, then a butterfly).
+// Warp per in-order spectrum of code 1 or 2 (codes 0 and 3 are the CTA kernel's).  Code 1 (at most max_peaks in
+// range): the in-range peaks in input order (ballot compaction).  Code 2 (more in range): the kept peaks are the
+// `kept` smallest selection keys (~ord(intensity), ~ord(mass)) -- an 8-bit radix select over the spectrum's peaks
+// (re-read each pass, a warp-private histogram) -- taken in input order, which is the output order; keys equal to
+// the threshold (equal peaks) in input order.  TIC as the f64 sum of lane partials (lane order, then a butterfly).
 constexpr int KE_WARPS = 8;
 
 __device__ __forceinline__ uint64_t k0_sel_key(float mz, float it) {
@@ -214,40 +202,6 @@ k0_easy_k(int n_spec, const int64_t* raw_off, const float* raw_mz, const float* 
     tic[s] = (float)part;
     valid[s] = n_out >= min_peaks;
   }
-}
-
-__device__ __forceinline__ void block_bitonic_u64(uint64_t* v, int n_pow2) {
-  for (int k = 2; k <= n_pow2; k <<= 1)
-    for (int j = k >> 1; j > 0; j >>= 1) {
-      for (int i = threadIdx.x; i < n_pow2; i += blockDim.x) {
-        int p = i ^ j;
-        if (p > i) {
-          uint64_t a = v[i], b = v[p];
-          bool up = (i & k) == 0;
-          if ((a > b) == up) { v[i] = b; v[p] = a; }
-        }
-      }
-      __syncthreads();
-    }
-}
-
-constexpr int K0_THREADS = 512;
-
-// Exclusive scan of one int per thread over the CTA (K0_THREADS threads); wsum: K0_THREADS / 32 ints of scratch.
-__device__ __forceinline__ int k0_block_excl_scan(int v, int* wsum) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int inc = (int)vk::warp_incl_scan(v);
-  if (lane == 31) wsum[warp] = inc;
-  __syncthreads();
-  if (warp == 0) {
-    const int w = lane < K0_THREADS / 32 ? wsum[lane] : 0;
-    const int wi = (int)vk::warp_incl_scan(w);
-    if (lane < K0_THREADS / 32) wsum[lane] = wi - w;
-  }
-  __syncthreads();
-  const int r = wsum[warp] + inc - v;
-  __syncthreads();
-  return r;
 }
 
 // A spectrum whose raw peaks are in (mass asc, intensity desc) order but with more than max_peaks in range: the

@@ -276,26 +276,36 @@ def _k0_device(run: DeviceRun, p: SearchParams, dev):
     easy = torch.empty(max(n, 1), dtype=torch.uint8, device=dev)
     hard = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
     n_hard = torch.empty(1, dtype=torch.int32, device=dev)
-    K.check(L.vk_k0_count(n, K.ptr(run.offsets), K.ptr(run.mz), K.ptr(run.intensity), p.fragment_min_mz,
-                          p.fragment_max_mz, p.max_peaks, K.ptr(kept), K.ptr(easy), K.ptr(hard), K.ptr(n_hard),
-                          K.stream()), "k0_count")
+    window = p.peak_mode != "global"   # the reference groups by window for any other value (engine.py:182)
+    if window:
+        K.check(L.vk_k0w_count(n, K.ptr(run.offsets), K.ptr(run.mz), K.ptr(run.intensity), p.fragment_min_mz,
+                               p.fragment_max_mz, p.window_th, p.window_k, K.ptr(kept), K.ptr(easy), K.ptr(hard),
+                               K.ptr(n_hard), K.stream()), "k0w_count")
+    else:
+        K.check(L.vk_k0_count(n, K.ptr(run.offsets), K.ptr(run.mz), K.ptr(run.intensity), p.fragment_min_mz,
+                              p.fragment_max_mz, p.max_peaks, K.ptr(kept), K.ptr(easy), K.ptr(hard), K.ptr(n_hard),
+                              K.stream()), "k0_count")
     off = _scan(kept[:n])
     cap = max(run.n_raw, 1)
     mass = torch.empty(cap, dtype=torch.float32, device=dev)
     inten = torch.empty(cap, dtype=torch.float32, device=dev)
     tic = torch.empty(max(n, 1), dtype=torch.float32, device=dev)
     valid = torch.empty(max(n, 1), dtype=torch.uint8, device=dev)
-    K.check(L.vk_k0_fill(n, K.ptr(run.offsets), K.ptr(run.mz), K.ptr(run.intensity), p.fragment_min_mz,
-                         p.fragment_max_mz, p.max_peaks, p.min_peaks, K.ptr(off), K.ptr(mass), K.ptr(inten),
-                         K.ptr(tic), K.ptr(valid), run.max_raw, K.ptr(easy), K.ptr(hard), K.ptr(n_hard),
-                         K.stream()), "k0_fill")
+    if window:
+        K.check(L.vk_k0w_fill(n, K.ptr(run.offsets), K.ptr(run.mz), K.ptr(run.intensity), p.fragment_min_mz,
+                              p.fragment_max_mz, p.window_th, p.window_k, p.min_peaks, K.ptr(off), K.ptr(mass),
+                              K.ptr(inten), K.ptr(tic), K.ptr(valid), run.max_raw, K.ptr(easy), K.ptr(hard),
+                              K.ptr(n_hard), K.stream()), "k0w_fill")
+    else:
+        K.check(L.vk_k0_fill(n, K.ptr(run.offsets), K.ptr(run.mz), K.ptr(run.intensity), p.fragment_min_mz,
+                             p.fragment_max_mz, p.max_peaks, p.min_peaks, K.ptr(off), K.ptr(mass), K.ptr(inten),
+                             K.ptr(tic), K.ptr(valid), run.max_raw, K.ptr(easy), K.ptr(hard), K.ptr(n_hard),
+                             K.stream()), "k0_fill")
     return {"off": off, "mass": mass, "int": inten, "tic": tic[:n], "valid_d": valid[:n]}
 
 
 def k0_preprocess(sp: Spectra, p: SearchParams, dev, stats: Stats):
     """K0 on the GPU (reference engine.py:171-210): device peaks + host validity mask."""
-    if p.peak_mode != "global":
-        raise NotImplementedError("only the global peak view (Sage) is implemented")
     run = DeviceRun(sp, torch.device(dev), stats)
     pk = _k0_device(run, p, torch.device(dev))
     n_kept = int(pk["off"][-1])

@@ -34,7 +34,7 @@ class SearchParams:
     k1_threshold: int = 1
     pair_closure: bool = True
     report_psms: int = 1
-    peak_mode: str = "global"               # only "global" (Sage) is searched here
+    peak_mode: str = "global"               # "global" (Sage) | "window" (top window_k per window_th Th window)
     window_th: float = 100.0
     window_k: int = 15
     # reference K1 layout knobs (the compatible entry points use them)
