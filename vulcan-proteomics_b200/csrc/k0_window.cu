@@ -99,6 +99,49 @@ k0w_count_k(int n_spec, const int64_t* raw_off, const float* raw_mz, const float
   }
 }
 
+// One over-full window of c (wk < c <= 32 * R) in-order peaks at mz / it: every lane ranks its R peaks against all
+// of the window's selection keys (broadcast by shuffles; ties by position), and the peaks ranked below wk are
+// written in input order from out_pos.  Returns the lane's sum of the written intensities.
+template <int R>
+__device__ __forceinline__ double rank_window(const float* mz, const float* it, int c, int wk, int out_pos, int n_out,
+                                              float* pk_mass, float* pk_int) {
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  uint64_t key[R];
+  int rank[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int t = lane + 32 * r;
+    key[r] = t < c ? win_sel_key(__fsub_rn(mz[t], VK_PROTON), it[t]) : ~0ull;
+    rank[r] = 0;
+  }
+#pragma unroll
+  for (int r2 = 0; r2 < R; ++r2) {
+    if (32 * r2 >= c) break;
+    for (int src = 0; src < 32; ++src) {
+      const uint64_t kj = __shfl_sync(VK_FULL, key[r2], src);
+      const int j = src + 32 * r2;
+#pragma unroll
+      for (int r = 0; r < R; ++r) rank[r] += kj < key[r] || (kj == key[r] && j < lane + 32 * r);
+    }
+  }
+  double part = 0.0;
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const bool take = lane + 32 * r < c && rank[r] < wk;
+    const unsigned m = __ballot_sync(VK_FULL, take);
+    const int pos = out_pos + __popc(m & lt);
+    if (take && pos < n_out) {
+      const float v = unord_f32(~(uint32_t)(key[r] >> 32));
+      pk_mass[pos] = unord_f32(~(uint32_t)key[r]);
+      pk_int[pos] = v;
+      part += (double)v;
+    }
+    out_pos += __popc(m);
+  }
+  return part;
+}
+
 // Warp per spectrum of code 1 or 2.  Shared memory per warp: P[n_bins + 1] (in-range peaks before each window) and
 // Q[n_bins + 1] (kept peaks before each window).
 __global__ void __launch_bounds__(KW_WARPS * 32)
@@ -182,43 +225,11 @@ k0w_warp_k(int n_spec, const int64_t* raw_off, const float* raw_mz, const float*
     for (int b = 0; b < n_bins; ++b) {
       const int pb = (int)P[b], c = (int)P[b + 1] - pb;
       if (c <= wk) continue;
-      const int64_t a = r_in + pb;
-      const int n_chunk = (c + 31) >> 5;
-      uint64_t key[KW_SEL / 32];
-      int rank[KW_SEL / 32];
-#pragma unroll
-      for (int r = 0; r < KW_SEL / 32; ++r) {
-        const int t = lane + 32 * r;
-        key[r] = t < c ? win_sel_key(__fsub_rn(raw_mz[a + t], VK_PROTON), raw_int[a + t]) : ~0ull;
-        rank[r] = 0;
-      }
-      for (int r2 = 0; r2 < n_chunk; ++r2) {
-        uint64_t kr2 = 0ull;
-#pragma unroll
-        for (int r = 0; r < KW_SEL / 32; ++r)
-          if (r == r2) kr2 = key[r];
-        for (int src = 0; src < 32; ++src) {
-          const uint64_t kj = __shfl_sync(VK_FULL, kr2, src);
-          const int j = src + 32 * r2;
-#pragma unroll
-          for (int r = 0; r < KW_SEL / 32; ++r) rank[r] += kj < key[r] || (kj == key[r] && j < lane + 32 * r);
-        }
-      }
-      int base = (int)Q[b];
-#pragma unroll
-      for (int r = 0; r < KW_SEL / 32; ++r) {
-        if (r >= n_chunk) break;
-        const bool take = lane + 32 * r < c && rank[r] < wk;
-        const unsigned m = __ballot_sync(VK_FULL, take);
-        const int pos = base + __popc(m & lt);
-        if (take && pos < n_out) {
-          const float it = unord_f32(~(uint32_t)(key[r] >> 32));
-          pk_mass[o0 + pos] = unord_f32(~(uint32_t)key[r]);
-          pk_int[o0 + pos] = it;
-          part += (double)it;
-        }
-        base += __popc(m);
-      }
+      const float *wm = raw_mz + r_in + pb, *wi = raw_int + r_in + pb;
+      float *om = pk_mass + o0, *oi = pk_int + o0;
+      if (c <= 32) part += rank_window<1>(wm, wi, c, wk, (int)Q[b], n_out, om, oi);
+      else if (c <= 64) part += rank_window<2>(wm, wi, c, wk, (int)Q[b], n_out, om, oi);
+      else part += rank_window<4>(wm, wi, c, wk, (int)Q[b], n_out, om, oi);
     }
   }
 #pragma unroll
