@@ -157,10 +157,9 @@ def stream():
 
 
 _TRACE = os.environ.get("VK_TRACE") == "1"
-# kernels launched by one successful call of an entry point (default 1); `LAUNCHES` counts them
-# kernels launched by one call of an entry point (counted by `check`; the default is 1)
+# kernels launched by one call of an entry point (counted by `check` into `LAUNCHES`; the default is 1)
 _KERNELS_PER_CALL = {"scan": 3, "set_params": 0, "set_nterm": 0, "set_tol_da": 0, "tindex_layout": 0,
-                     "fused_grid": 0, "k0_fill": 2, "hyp_fill": 2}
+                     "fused_grid": 0, "k0_fill": 2, "k0w_fill": 2, "hyp_fill": 2}
 LAUNCHES = {"n": 0}
 
 
