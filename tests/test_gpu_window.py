@@ -144,3 +144,29 @@ def test_window_mode_search_equals_oracle(mini, param_sets, name, torch_cuda):
     np.testing.assert_allclose(out["k2"]["hyperscore"][:nc].cpu().numpy(), k2["hyperscore"], rtol=1e-12)
     rk = O.psm_rank(k2, r, p.min_matched_peaks, 2)
     assert tbl.num_rows > 0 and np.array_equal(tbl.column("pf_row").to_numpy(), r[rk["cand"]])
+
+
+def _window_params(param_sets, name):
+    return dataclasses.replace(param_sets[name], peak_mode="window", window_th=100.0, window_k=8, min_peaks=8)
+
+
+@pytest.mark.parametrize("name", ("da", "ppm"))
+def test_window_mode_through_every_entry_point(mini, param_sets, name, torch_cuda):
+    """With the window peak view: the pruned search without pruning is the plain search, and the graph-captured
+    Searcher, plain and with a pruner that prunes, returns the per-run searches' tables."""
+    import math
+    from vulcan.gpu import engine as E
+    from vulcan.gpu import prune as PR
+    l1, sp, _ = mini
+    p = _window_params(param_sets, name)
+    gi = E.GpuIndex(l1, p, STATIC, VAR)
+    plain = E.search(sp, gi, l1, p, report=2)[0]
+    keep_all = PR.Pruner(gi.dev, seed=3, tau=-math.inf, min_keep=0, max_keep=16)
+    assert PR.search_pruned(sp, gi, l1, p, keep_all, report=2)[0].equals(plain)
+    for tbl, _ in E.Searcher(gi, l1, p, report=2).search_many([sp, sp]):
+        assert tbl.equals(plain)
+    pr = PR.Pruner(gi.dev, seed=5)
+    pr.tau, pr.min_keep, pr.max_keep, pr.min_count = 0.0, 1, 16, 2
+    want = PR.search_pruned(sp, gi, l1, p, pr, report=2)[0]
+    for tbl, _ in E.Searcher(gi, l1, p, pruner=pr, report=2).search_many([sp, sp]):
+        assert tbl.equals(want)
