@@ -78,3 +78,21 @@ def test_missing_library_fails_loudly(tmp_path):
     from vulcan import _native
     with pytest.raises(RuntimeError, match="not built"):
         _native._load(str(tmp_path / "nope.so"), "CUDA kernel library")
+
+
+def test_window_peak_mode_arguments_are_checked_before_any_device_call():
+    """vk_k0w_count / vk_k0w_fill refuse a window width that is not positive and finite, and a fragment range past
+    999 windows (where the reference's group ids spectrum * 1000 + window would merge spectra), before they touch
+    the device: callable here without a GPU."""
+    from vulcan import _native
+    L = _native._load(_native.GPU_SO, "CUDA kernel library")
+    P, I32, F32 = C.c_void_p, C.c_int, C.c_float
+    L.vk_k0w_count.argtypes = [I32, P, P, P, F32, F32, F32, I32, P, P, P, P, P]
+    L.vk_k0w_fill.argtypes = [I32, P, P, P, F32, F32, F32, I32, I32, P, P, P, P, P, I32, P, P, P, P]
+    vk_e_arg = int(re.search(r"#define VK_E_ARG\s+\((-?\d+)\)", open(HEADER).read()).group(1))
+    for th, fmin, fmax in ((0.0, 150.0, 2000.0), (-5.0, 150.0, 2000.0), (float("nan"), 150.0, 2000.0),
+                           (float("inf"), 150.0, 2000.0), (1.0, 150.0, 2000.0), (2.0, 150.0, 2000.0),
+                           (100.0, -150.0, 2000.0)):
+        assert L.vk_k0w_count(1, None, None, None, fmin, fmax, th, 15, None, None, None, None, None) == vk_e_arg
+        assert L.vk_k0w_fill(1, None, None, None, fmin, fmax, th, 15, 1, None, None, None, None, None, 0, None, None,
+                             None, None) == vk_e_arg

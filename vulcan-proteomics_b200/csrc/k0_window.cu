@@ -190,7 +190,8 @@ k0w_warp_k(int n_spec, const int64_t* raw_off, const float* raw_mz, const float*
     for (int b0 = 0; b0 < n_bins; b0 += 32) {
       const int b = b0 + lane;
       const uint32_t c = b < n_bins ? P[b] : 0u, ck = min(c, (uint32_t)wk);
-      const uint32_t ip = (uint32_t)vk::warp_incl_scan((long long)c), iq = (uint32_t)vk::warp_incl_scan((long long)ck);
+      const uint32_t ip = (uint32_t)vk::warp_incl_scan((long long)c);
+      const uint32_t iq = (uint32_t)vk::warp_incl_scan((long long)ck);
       if (b < n_bins) {
         P[b] = cp + ip - c;
         Q[b] = cq + iq - ck;
