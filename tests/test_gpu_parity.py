@@ -699,6 +699,34 @@ def test_batched_search_equals_per_run_search(mini, param_sets, indexes, name, t
     assert len(se.slots) == 1     # every batch replayed the same captured pass
 
 
+@pytest.mark.parametrize("depth", (1, 2, 3))
+def test_searcher_pipeline_depth(mini, param_sets, indexes, depth, torch_cuda):
+    """With 1, 2 or 3 runs in flight (slots per shape), search_many and search_batch return every run's own
+    table; a submit into a slot whose result was not collected is refused."""
+    import dataclasses
+    from vulcan.gpu import engine as E
+    from vulcan.gpu.host import Spectra
+    l1, sp, _ = mini
+    p = dataclasses.replace(param_sets["ppm"], search_method="staged")
+    gi = indexes["ppm"]
+    inv = sp.intensity[::-1].copy()
+    sp2 = Spectra("other", sp.scan, sp.index, sp.rt, sp.precursor_mz, sp.charge, sp.mz, inv, sp.offsets)
+    runs = [sp, sp2, E.pin_spectra(sp), sp2, sp]
+    want = [E.search(r, gi, l1, p, report=2)[0] for r in runs]
+    se = E.Searcher(gi, l1, p, report=2, depth=depth)
+    for (tbl, _), w in zip(se.search_many(runs), want):
+        assert tbl.equals(w)
+    assert len(se.slots[next(iter(se.slots))]) == depth
+    parts = [_slice_run(sp, a, b, f"r{i}") for i, (a, b) in enumerate(((0, 50), (50, 90), (90, 160)))]
+    for (tbl, _), r in zip(se.search_batch(parts, batch_spectra=60), parts):
+        assert tbl.equals(E.search(r, gi, l1, p, report=2)[0])
+    handles = [se.submit(sp) for _ in range(depth)]
+    with pytest.raises(RuntimeError):
+        se.submit(sp)
+    for h in handles:
+        se.result(h)
+
+
 def test_autotuner_picks_a_measured_layout(mini, param_sets, tmp_path, torch_cuda):
     """The autotuner times every candidate layout on the sample, returns the fastest, reports peak-count buckets,
     and reuses its cached choice."""

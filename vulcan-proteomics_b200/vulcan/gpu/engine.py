@@ -1159,21 +1159,26 @@ class _Slot:
 class Searcher:
     """Repeated searches of runs through graph-captured device passes (plain, or pruned with ``pruner``).
 
-    Runs are grouped by shape (spectra, peak capacity, largest peak count, hypothesis bound); each shape gets two
-    slots of device buffers with a captured pass, used alternately, so that the host-to-device copy of one run (on
-    a copy stream) overlaps the pass of the previous one.  ``submit(sp)`` queues a run and returns a handle,
-    ``result(handle)`` waits for it and builds its PSM table; ``search(sp)`` does both; ``search_many(runs)``
-    keeps one run in flight while the previous table is built.  Inputs already in pinned host memory
+    Runs are grouped by shape (spectra, peak capacity, largest peak count, hypothesis bound); each shape gets
+    ``depth`` slots of device buffers with a captured pass, used in turn: the host-to-device copies of the next runs
+    (on a copy stream) overlap the passes of the earlier ones (on a compute stream), and each pass's packed PSMs go
+    back on a third stream, so that the next pass does not wait for them.  ``submit(sp)`` queues a run and returns
+    a handle, ``result(handle)`` waits for it and builds its PSM table; ``search(sp)`` does both;
+    ``search_many(runs)`` keeps ``depth`` runs in flight while the tables are built.  Inputs already in pinned host memory
     (``pin_spectra``) are copied straight to the device; others are staged through pinned buffers first.  Results
     are identical to ``engine.search`` / ``prune.search_pruned``."""
 
-    def __init__(self, gi: GpuIndex, l1, p: SearchParams, pruner=None, report: int | None = None):
+    def __init__(self, gi: GpuIndex, l1, p: SearchParams, pruner=None, report: int | None = None, depth: int = 3):
+        if depth < 1:
+            raise ValueError("depth: at least one run in flight")
         self.gi, self.l1, self.p, self.pruner = gi, l1, p, pruner
         self.report = p.report_psms if report is None else report
+        self.depth = depth
         self.slots = {}
         self.device_ms = 0.0          # summed CUDA-event time of the replayed passes (inputs already copied)
         self.copy_stream = torch.cuda.Stream(gi.dev)
         self.compute_stream = torch.cuda.Stream(gi.dev)
+        self.d2h_stream = torch.cuda.Stream(gi.dev)
         self._turn = {}
 
     def device_pass(self, run: DeviceRun):
@@ -1210,10 +1215,10 @@ class Searcher:
         key = self._shape(parts, n_total)
         with torch.cuda.device(self.gi.dev):
             if key not in self.slots:
-                self.slots[key] = [_Slot(self, *key) for _ in range(2)]
+                self.slots[key] = [_Slot(self, *key) for _ in range(self.depth)]
                 self._turn[key] = 0
             slot = self.slots[key][self._turn[key]]
-            self._turn[key] ^= 1
+            self._turn[key] = (self._turn[key] + 1) % self.depth
             if slot.busy:
                 raise RuntimeError("result() of the previous run in this slot was not collected")
             slot.busy = True
@@ -1228,7 +1233,7 @@ class Searcher:
                 base_pk += int(o[-1])
                 base_sp += len(sp)
             offs[base_sp + 1:] = base_pk
-            # the previous pass over this slot must be done before its inputs are overwritten
+            # the previous pass over this slot and its read-back must be done before its buffers are reused
             self.copy_stream.wait_event(slot.done)
             h2d = 0
             with torch.cuda.stream(self.copy_stream):
@@ -1261,8 +1266,10 @@ class Searcher:
                 ev[0].record(self.compute_stream)
                 out = slot.gp.replay()
                 ev[1].record(self.compute_stream)
+            self.d2h_stream.wait_event(ev[1])
+            with torch.cuda.stream(self.d2h_stream):
                 slot.host_out.copy_(out["packed"], non_blocking=True)
-                slot.done.record(self.compute_stream)
+                slot.done.record(self.d2h_stream)
             return (parts[0] if len(parts) == 1 else None, slot, h2d, ev)
 
     def _records(self, handle):
@@ -1307,13 +1314,13 @@ class Searcher:
                 starts = np.concatenate([[0], np.cumsum([len(r) for r in parts])]).tolist()
                 inflight.append((self._submit(parts, n_b), parts, starts))
                 k += 1
-            while k < len(groups) and len(inflight) < 2:
+            while k < len(groups) and len(inflight) < self.depth:
                 submit_next()
             while inflight:
                 h, parts, starts = inflight.popleft()
                 rec, st = self._records(h)          # frees the batch's slot ...
                 if k < len(groups):
-                    submit_next()                   # ... for the batch after next, copied while the tables build
+                    submit_next()                   # ... for a later batch, copied while the tables build
                 empty = Stats()
                 tables += [(t, st if i == 0 else empty) for i, t in enumerate(split_table(rec, parts, starts))]
         finally:
@@ -1321,12 +1328,12 @@ class Searcher:
         return tables
 
     def search_many(self, runs):
-        """PSM tables of many runs, two runs in flight: as soon as a run's PSM slots are read back (which frees its
-        slot), the run after next is submitted, so its host-to-device copy overlaps the device pass of the next run
-        while the host builds the table."""
+        """PSM tables of many runs, ``depth`` runs in flight: as soon as a run's PSM slots are read back (which
+        frees its slot), the next run is submitted into it, so the host-to-device copies stay ahead of the device
+        passes while the host builds the tables."""
         runs = list(runs)
         out, inflight, k = [], collections.deque(), 0
-        while k < len(runs) and len(inflight) < 2:
+        while k < len(runs) and len(inflight) < self.depth:
             inflight.append(self.submit(runs[k]))
             k += 1
         while inflight:
