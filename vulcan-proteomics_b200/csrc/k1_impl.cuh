@@ -75,10 +75,10 @@ __device__ __forceinline__ void k1_item_per_peak(const uint32_t* post, const uin
 // (k1_window_keys, by vk_k1_peak_keys) instead of once per (tile, hypothesis) item, together with a 32-bit filter
 // word (k1_filter_word).  Every tile has a presence bitmap, built with the index (vk_tindex_bitmap) and staged with
 // the tile: 2^K1_BM_LOG bits per coarse bin, bit s of bin b set when a posting of the bin has (low key) >>
-// (low_bits - K1_BM_LOG) == s.  A window whose bits are all clear holds no posting and is dropped after one shared-memory word; the
-// windows that may match are compacted into a per-warp queue (ballot) and searched exactly, one per lane, so the
-// bin lookup and binary search run with every lane busy and only for them.  The counts are those of
-// k1_item_per_peak: the bitmap only skips windows that hold no posting.
+// (low_bits - K1_BM_LOG) == s.  A window whose bits are all clear holds no posting and is dropped after one
+// shared-memory word; the windows that may match are compacted into a per-warp queue (ballot) and searched
+// exactly, one per lane, so the bin lookup and binary search run with every lane busy and only for them.  The
+// counts are those of k1_item_per_peak: the bitmap only skips windows that hold no posting.
 
 // Key range [ka, kb] of the tolerance window of fragment mass pm * z (Sage f32 bounds, both edges included), clamped
 // to the index's fragment range; ka > kb when the window misses the range.

@@ -30,10 +30,10 @@ constexpr int INF_WARPS = 8;
 
 // ------------------------------------------------------------------------------------------------ features
 // One thread per candidate hit (hypothesis, row, count): its window position is win_off[h] + row - lo[h].
-__global__ void cand_features_k(int64_t n, const int64_t* n_dev, const int64_t* c_hyp, const int64_t* c_row, const int64_t* c_cnt,
-                                const int64_t* win_off, const int64_t* h_lo, const uint32_t* isum, const float* h_M,
-                                const int8_t* h_z, const float* mass32, const uint8_t* len, const uint8_t* missed,
-                                const float* mu, const float* sd, __nv_bfloat16* feat) {
+__global__ void cand_features_k(int64_t n, const int64_t* n_dev, const int64_t* c_hyp, const int64_t* c_row,
+                                const int64_t* c_cnt, const int64_t* win_off, const int64_t* h_lo, const uint32_t* isum,
+                                const float* h_M, const int8_t* h_z, const float* mass32, const uint8_t* len,
+                                const uint8_t* missed, const float* mu, const float* sd, __nv_bfloat16* feat) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (n_dev) n = min(n, *n_dev);
   if (i >= n) return;
@@ -71,9 +71,9 @@ __device__ __forceinline__ void mma_bf16(float* c, const uint32_t* a, uint32_t b
 }
 
 __global__ void __launch_bounds__(INF_WARPS * 32)
-mlp_infer_k(int64_t n, const int64_t* n_dev, const __nv_bfloat16* __restrict__ feat, const __nv_bfloat16* __restrict__ W1,
-            const float* __restrict__ b1, const __nv_bfloat16* __restrict__ W2, const float* __restrict__ b2,
-            const float* __restrict__ w3, float b3, float* __restrict__ logit) {
+mlp_infer_k(int64_t n, const int64_t* n_dev, const __nv_bfloat16* __restrict__ feat,
+            const __nv_bfloat16* __restrict__ W1, const float* __restrict__ b1, const __nv_bfloat16* __restrict__ W2,
+            const float* __restrict__ b2, const float* __restrict__ w3, float b3, float* __restrict__ logit) {
   extern __shared__ __align__(16) uint8_t mlp_smem[];
   __nv_bfloat16* sW2 = reinterpret_cast<__nv_bfloat16*>(mlp_smem);
   __nv_bfloat16* sW1 = sW2 + MLP_H * W2_STRIDE;
@@ -346,8 +346,9 @@ int64_t vk_mlp_infer_smem(void) {
   return (int64_t)MLP_H * W2_STRIDE * 2 + (int64_t)MLP_H * W1_STRIDE * 2 + 3 * MLP_H * 4;
 }
 
-int vk_mlp_infer(int64_t n, const int64_t* n_dev, const void* feat_bf16, const void* W1_bf16, const float* b1, const void* W2_bf16,
-                 const float* b2, const float* w3, float b3, float* logit, int grid, void* stream) {
+int vk_mlp_infer(int64_t n, const int64_t* n_dev, const void* feat_bf16, const void* W1_bf16, const float* b1,
+                 const void* W2_bf16, const float* b2, const float* w3, float b3, float* logit, int grid,
+                 void* stream) {
   if (n <= 0) return 0;
   if (grid < 1) return VK_E_ARG;
   size_t sh = (size_t)vk_mlp_infer_smem();

@@ -100,9 +100,9 @@ __device__ __forceinline__ int64_t win_rows(int64_t w0, int64_t lo, int64_t hi, 
 }
 
 __global__ void __launch_bounds__(TK_WARPS * 32)
-select_topk_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo, const int64_t* h_hi,
-              const int64_t* win_off, const int32_t* cnt, int64_t cnt_cap, const int64_t* partner, int thr, int topk, int pair_closure,
-              int cap, int list_pow2, int key_cap, int64_t* c_hyp, int64_t* c_row, int64_t* c_cnt, int64_t* n_cand,
+select_topk_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo, const int64_t* h_hi, const int64_t* win_off,
+              const int32_t* cnt, int64_t cnt_cap, const int64_t* partner, int thr, int topk, int pair_closure, int cap,
+              int list_pow2, int key_cap, int64_t* c_hyp, int64_t* c_row, int64_t* c_cnt, int64_t* n_cand,
               uint32_t* hyp_scored, uint64_t* hyp_matched, int64_t* spec_scored, int64_t* spec_matched) {
   extern __shared__ __align__(16) uint8_t tk_smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
