@@ -86,7 +86,8 @@ def expand_pairs(fwd, dec, perms, static, var, max_var, min_mass, max_mass, id_s
                     continue
                 md = m & NTERM_BIT
                 for j in range(n):
-                    if (m >> perm[j]) & 1 and perm[j] != 63:
+                    pj = int(perm[j])   # a Python int: m may carry bit 63 (N-terminal), beyond a numpy int64
+                    if (m >> pj) & 1 and pj != 63:
                         md |= 1 << j
                 idf = xxhash.xxh64_intdigest(canonical(f, m, resvar, nterm), id_seed)
                 idd = xxhash.xxh64_intdigest(canonical(d, md, resvar, nterm), id_seed)

@@ -29,12 +29,16 @@ def _pairs(rng, n):
     return fwd, dec, perms, np.array(flat, np.uint8), np.array(off, np.int64)
 
 
+@pytest.mark.parametrize("nterm", [False, True])
 @pytest.mark.parametrize("max_var,limits", [(2, None), (3, {"M": 1}), (4, {"STY": 3, "M": 1}), (3, {"S": 1, "TY": 1})])
-def test_native_expansion_equals_oracle(max_var, limits):
+def test_native_expansion_equals_oracle(max_var, limits, nterm):
+    """nterm: a variable peptide N-terminal modification ("^", acetyl) as well, mask bit 63."""
     rng = np.random.default_rng(max_var * 7 + (len(limits) if limits else 0))
     fwd, dec, perms, flat, off = _pairs(rng, 60)
     static = {"C": 57.021464}
     var = {"M": 15.9949, "S": 79.966331, "T": 79.966331, "Y": 79.966331}
+    if nterm:
+        var["^"] = 42.010565
     got = _core.expand_pairs(fwd, dec, flat, off, list(static.items()), list(var.items()), max_var, 500.0, 5000.0, 11,
                              site_limits=limits,
                              nthreads=2)
@@ -43,6 +47,8 @@ def test_native_expansion_equals_oracle(max_var, limits):
             for i, mf, md, m, a, b, x, y in zip(got["seq"], got["mask_f"], got["mask_d"], got["mass"], got["id_f"],
                                                  got["id_d"], got["mass32_f"], got["mass32_d"])}
     assert len(have) == len(got["seq"]) and have == want
+    if nterm:
+        assert any(int(m) >> 63 for m in got["mask_f"])
     if limits and "STY" in limits:     # the group cap binds: some peptide has 4+ S/T/Y sites
         assert any(sum(c in "STY" for c in f) > 3 for f in fwd)
         sty = [sum(((int(m) >> k) & 1) and fwd[int(i)][k] in "STY" for k in range(len(fwd[int(i)])))

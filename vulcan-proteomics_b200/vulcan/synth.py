@@ -196,7 +196,7 @@ def simulate_run(l1, labels, w: Workload | str, n_spectra: int | None = None, se
     iso = rng.choice(3, n, p=np.array(w.iso_frac) / np.sum(w.iso_frac))
     for i, r in enumerate(rows.tolist()):
         seq = l1.residues[l1.seq_off[r]:l1.seq_off[r] + l1.length[r]].tobytes()
-        b, y = fragment_ladders(seq, int(l1.mask[r]), static, w.var_mods)
+        b, y = fragment_ladders(seq, int(l1.mask[r]), static, w.var_mods, nterm=w.var_mods.get("^", 0.0))
         ions = np.concatenate([b, y]) + float(PROTON)
         ions = ions[(ions > 50.0)]
         sig = ions[rng.random(len(ions)) < w.presence]
