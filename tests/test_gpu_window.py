@@ -152,15 +152,17 @@ def _window_params(param_sets, name):
 
 @pytest.mark.parametrize("name", ("da", "ppm"))
 def test_window_mode_through_every_entry_point(mini, param_sets, name, torch_cuda):
-    """With the window peak view: the pruned search without pruning is the plain search, and the graph-captured
-    Searcher, plain and with a pruner that prunes, returns the per-run searches' tables."""
+    """With the window peak view: the fused search kernel gives the staged search's table, the pruned search
+    without pruning is the plain search, and the graph-captured Searcher, plain and with a pruner that prunes,
+    returns the per-run searches' tables."""
     import math
     from vulcan.gpu import engine as E
     from vulcan.gpu import prune as PR
     l1, sp, _ = mini
-    p = _window_params(param_sets, name)
+    p = dataclasses.replace(_window_params(param_sets, name), tile_rows=64, search_method="staged")
     gi = E.GpuIndex(l1, p, STATIC, VAR)
     plain = E.search(sp, gi, l1, p, report=2)[0]
+    assert E.search(sp, gi, l1, dataclasses.replace(p, search_method="fused"), report=2)[0].equals(plain)
     keep_all = PR.Pruner(gi.dev, seed=3, tau=-math.inf, min_keep=0, max_keep=16)
     assert PR.search_pruned(sp, gi, l1, p, keep_all, report=2)[0].equals(plain)
     for tbl, _ in E.Searcher(gi, l1, p, report=2).search_many([sp, sp]):
