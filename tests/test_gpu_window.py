@@ -172,3 +172,33 @@ def test_window_mode_through_every_entry_point(mini, param_sets, name, torch_cud
     want = PR.search_pruned(sp, gi, l1, p, pr, report=2)[0]
     for tbl, _ in E.Searcher(gi, l1, p, pruner=pr, report=2).search_many([sp, sp]):
         assert tbl.equals(want)
+
+
+@pytest.mark.parametrize("mode", ("global150", "global512", "window15", "window4"))
+def test_k0_at_run_scale_equals_oracle(mode, torch_cuda):
+    """K0 on a run of the bench's size (40,000 spectra, 20-600 peaks log-normal around 150, 6M peaks; three in four
+    in m/z order, the rest shuffled, some with duplicated peaks) equals the oracle bit for bit, in both peak modes."""
+    from oracle import oracle as O
+    from vulcan.gpu import engine as E
+    from vulcan.gpu.host import SearchParams, Spectra
+    rng = np.random.default_rng(17)
+    n = 40000
+    lens = np.clip(np.round(rng.lognormal(np.log(150), 0.55, n)), 20, 600).astype(np.int64)
+    off = np.zeros(n + 1, np.int64)
+    np.cumsum(lens, out=off[1:])
+    mz = rng.uniform(100.0, 2100.0, int(off[-1])).astype(np.float32)
+    it = rng.lognormal(7.0, 1.2, int(off[-1])).astype(np.float32)
+    for s in range(n):
+        a, b = off[s], off[s + 1]
+        if s % 4 != 3:
+            mz[a:b] = np.sort(mz[a:b])
+        if s % 16 == 5 and b - a > 4:       # duplicated peaks: equal keys around the selection threshold
+            mz[a + 1:b:2] = mz[a:b - 1:2]
+            it[a + 1:b:2] = it[a:b - 1:2]
+    sp = Spectra("scale", np.arange(n, dtype=np.uint32), np.arange(n, dtype=np.uint32), np.zeros(n),
+                 rng.uniform(400, 1200, n), np.full(n, 2, np.int8), mz, it, off)
+    kw = {"global150": dict(max_peaks=150), "global512": dict(max_peaks=512),
+          "window15": dict(peak_mode="window", window_k=15), "window4": dict(peak_mode="window", window_k=4)}[mode]
+    p = SearchParams(**kw)
+    pk = E.k0_preprocess(sp, p, torch_cuda.device("cuda"), E.Stats())
+    _assert_view(pk, O.k0_view(sp, p))
