@@ -4,7 +4,8 @@ Imported only by tests/, ``__graft_entry__.smoke()`` and ``bench.py`` (its CPU b
 the checker or the timed CPU baseline.  The product package never imports it.
 
 Pieces (each cites the reference lines it restates):
-  k0_view            vulcan/gpu/engine.py:171-210   peak view (range filter, top max_peaks, mass sort, TIC)
+  k0_view            vulcan/gpu/engine.py:171-210   peak view (range filter, top max_peaks or top window_k per
+                                                    window_th window, mass sort, TIC)
   make_hypotheses    vulcan/gpu/host.py:64-91       precursor hypotheses + row windows (f32 Sage arithmetic)
   window_candidates  vulcan/gpu/engine.py:468-480   exhaustive (hyp, row) set sorted by (spectrum, row)
   k1_windows         vulcan/gpu/kernels.cu:195-232  K1 counts of every window row (C, vk_oracle.c)
