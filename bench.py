@@ -441,8 +441,9 @@ def run_b200(a):
                  "tile_rows": p.tile_rows, "parallelism": f"replicas x{world} (one run per GPU)",
                  "launch": "one CUDA graph per pass (eager_ms_per_step: the same pass launched kernel by kernel)"
                            if use_graph else "kernel by kernel",
-                 "e2e": "Searcher.search_many over the run in pinned host memory: H2D on a copy stream, graph replay, "
-                        "one D2H of the packed PSM slots, host PSM table" if use_graph else "engine.search"}
+                 "e2e": "Searcher.search_many over the run in pinned host memory, three runs in flight: H2D on a "
+                        "copy stream, graph replay on a compute stream, one D2H of the packed PSM slots on a third "
+                        "stream, host PSM table" if use_graph else "engine.search"}
         if pruned:
             extra["path"] = ("learned-pruned search: K1 (+ intensity sums) -> top-k shortlist of hits with count >= "
                              f"{pr.min_count} -> BF16 MLP 16-256-256-1 -> logit >= calibrated tau or best "
