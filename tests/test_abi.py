@@ -96,3 +96,26 @@ def test_window_peak_mode_arguments_are_checked_before_any_device_call():
         assert L.vk_k0w_count(1, None, None, None, fmin, fmax, th, 15, None, None, None, None, None) == vk_e_arg
         assert L.vk_k0w_fill(1, None, None, None, fmin, fmax, th, 15, 1, None, None, None, None, None, 0, None, None,
                              None, None) == vk_e_arg
+
+
+def test_header_compiles_as_c_and_links(tmp_path):
+    """A C binding (cgo, JNI, N-API) includes the header as C99 and links the library: a program that takes the
+    address of every declared entry point compiles, links and loads (it calls none of them)."""
+    import shutil
+    import subprocess
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("no C compiler")
+    from vulcan import _native
+    names = [n for _, n, _ in _decls()]
+    src = tmp_path / "bind.c"
+    src.write_text('#include "vulcan_b200.h"\n#include <stdio.h>\nint main(void) {\n  const void* fns[] = {'
+                   + ", ".join(f"(const void*)&{n}" for n in names)
+                   + '};\n  printf("%d\\n", (int)(sizeof fns / sizeof fns[0]));\n  return 0;\n}\n')
+    lib = _native.GPU_SO
+    r = subprocess.run([gcc, "-std=c99", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), str(src),
+                        "-o", str(tmp_path / "bind"), lib, f"-Wl,-rpath,{os.path.dirname(lib)}"],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    run = subprocess.run([str(tmp_path / "bind")], capture_output=True, text=True, timeout=60)   # no device calls
+    assert run.returncode == 0 and int(run.stdout) == len(names)
