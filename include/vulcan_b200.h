@@ -151,8 +151,10 @@ int vk_scan_i64(const int64_t* in, int64_t n, int64_t* out, void* tmp, void* str
  *   - Scratch: the block partial sums live in one fixed device array inside the library (64 KiB on every device
  *     that loads it, held until the process exits).  n may be at most vk_scan_noalloc_max_n() = 33,554,432;
  *     larger n returns VK_E_TOO_LARGE and launches nothing.
- *   - Set-up: the first call on a device looks up the array's device address (cudaGetSymbolAddress) with that
- *     device current and keeps it; make that first call before any stream capture.
+ *   - Set-up: the first call with n > 0 on a device looks up the array's device address (cudaGetSymbolAddress)
+ *     with that device current and keeps it for the life of the process; make that first call before any stream
+ *     capture (n == 0 looks nothing up).  The kept address does not survive a cudaDeviceReset of that device in
+ *     the same process: after a reset, do not call this entry point on that device again.
  *   - Sharing: every call on a device uses the same array.  Calls whose kernels may overlap on the GPU (other
  *     streams, other host threads) race on it and give wrong sums; order them (one stream, or events).
  *     Nothing in the array has to start at zero; each call overwrites what it reads. */
@@ -246,6 +248,21 @@ int vk_k1_tiles(const vk_tindex* ix, const vk_frag_params* fp, float tol_lo, flo
                 const uint32_t* pk_filt, int n_kz, int64_t kstride, void* stream);
 int vk_k1_peak_keys(const vk_tindex* ix, const vk_frag_params* fp, float tol_lo, float tol_hi, const int64_t* n_peaks,
                     const float* pk_mass, int n_kz, int64_t kstride, uint32_t* keys, uint32_t* filt, void* stream);
+/* K1 in hit-list form (the learned-pruned search): the same counting as vk_k1_tiles, but instead of a dense count
+ * per window row, the rows with count >= thr (>= 1) of hypothesis h are appended to its region [win_off[h],
+ * win_off[h] + hyp_hits[h]) of hit_rc (u64: count << 32 | row) and, with pk_int/tic, of hit_isum (the summed
+ * matched intensity of vk_k1_tiles' isum); plus per hypothesis hyp_scored (u32, rows with count > 0) and
+ * hyp_matched (u64, sum of counts).  hyp_hits, hyp_scored and hyp_matched are accumulated with atomics: the caller
+ * zeroes them.  The order of the hits inside a region is unspecified; vk_select_hits orders them.  cnt_cap bounds
+ * hit_rc / hit_isum like vk_k1_tiles' cnt.  Reference semantics: kernels.cu:170-189 (threshold append, scored,
+ * matched). */
+int vk_k1_hits(const vk_tindex* ix, const vk_frag_params* fp, float tol_lo, float tol_hi, int warps,
+               const int64_t* tile_item_off, const int32_t* item_hyp, int64_t n_hyp, int64_t item_cap,
+               const int32_t* h_spec, const int8_t* h_maxfz, const int64_t* h_lo, const int64_t* h_hi,
+               const int64_t* win_off, int64_t cnt_cap, const int64_t* pk_off, const float* pk_mass, int thr,
+               uint64_t* hit_rc, uint32_t* hit_isum, uint32_t* hyp_hits, uint32_t* hyp_scored,
+               uint64_t* hyp_matched, int32_t* status, const float* pk_int, const float* tic,
+               const uint32_t* pk_keys, const uint32_t* pk_filt, int n_kz, int64_t kstride, void* stream);
 
 /* Top-K + pair closure (reference vulcan/gpu/engine.py:284-312) per spectrum, from the dense K1 counts.
  * Spectrum s owns hypotheses [spec_hyp_off[s], spec_hyp_off[s+1]).  Per spectrum: entries with count >= thr,
@@ -261,11 +278,27 @@ int vk_select_topk(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo,
                    uint32_t* hyp_scored, uint64_t* hyp_matched, int64_t* spec_scored, int64_t* spec_matched,
                    void* stream);
 
+/* Top-k shortlist from the hit lists of vk_k1_hits (reference vulcan/gpu/engine.py:284-301 without the pair
+ * closure): per spectrum its hypotheses' hits ranked by (count desc, row desc, hypothesis asc), the first topk kept
+ * (all when fewer), sorted by row, duplicate rows merged to the lowest hypothesis and highest count; the slots of
+ * vk_select_topk with pair_closure = 0 (cap >= topk) plus c_isum (u32, the kept hit's intensity sum; NULL when
+ * hit_isum is NULL), and spec_scored / spec_matched (i64, may be NULL) summed from K1's per-hypothesis totals.
+ * The same candidates as vk_select_topk over vk_k1_tiles' dense counts with thr = vk_k1_hits' thr. */
+int vk_select_hits(int n_spec, const int64_t* spec_hyp_off, const int64_t* win_off, const uint32_t* hyp_hits,
+                   const uint64_t* hit_rc, const uint32_t* hit_isum, const uint32_t* hyp_scored,
+                   const uint64_t* hyp_matched, int topk, int cap, int64_t* c_hyp, int64_t* c_row, int64_t* c_cnt,
+                   uint32_t* c_isum, int64_t* n_cand, int64_t* spec_scored, int64_t* spec_matched, void* stream);
+
 /* Compaction of per-spectrum slots into a flat candidate list: with cand_off = scan(n_cand), copies slot s to
- * [cand_off[s], cand_off[s+1]) and writes c_maxfz from h_maxfz[c_hyp]. */
+ * [cand_off[s], cand_off[s+1]) and writes c_maxfz from h_maxfz[c_hyp].  vk_compact_hits also carries the
+ * intensity sums (s_isum -> c_isum). */
 int vk_compact_cands(int n_spec, int cap, const int64_t* n_cand, const int64_t* cand_off, const int64_t* s_hyp,
                      const int64_t* s_row, const int64_t* s_cnt, const int8_t* h_maxfz, int64_t* c_hyp,
                      int64_t* c_row, int64_t* c_cnt, int32_t* c_row32, int8_t* c_maxfz, void* stream);
+int vk_compact_hits(int n_spec, int cap, const int64_t* n_cand, const int64_t* cand_off, const int64_t* s_hyp,
+                    const int64_t* s_row, const int64_t* s_cnt, const uint32_t* s_isum, const int8_t* h_maxfz,
+                    int64_t* c_hyp, int64_t* c_row, int64_t* c_cnt, int32_t* c_row32, int8_t* c_maxfz,
+                    uint32_t* c_isum, void* stream);
 
 /* K2 exact rescoring (reference kernels.cu:263-376, closed mode), B200 launch: one warp per spectrum, lanes over
  * candidates, the spectrum's (first 512) peaks in shared memory.  Candidates of spectrum s are
@@ -425,7 +458,8 @@ int vk_search_fused_grid(const vk_tindex* ix, int warps, int topk, int pair_clos
 
 /* Features of n candidate hits (hypothesis, row, K1 count; e.g. the top-K shortlist of vk_select_topk with
  * pair_closure = 0, compacted): 16 BF16 per hit = the standardised (x - mu) / sd of K1 count, summed matched
- * intensity (isum of vk_k1_tiles / 2^24, a fraction of the TIC), precursor error in ppm
+ * intensity (isum of vk_k1_tiles / 2^24, a fraction of the TIC; isum[win_off[h] + row - lo[h]], or isum[i] for
+ * candidate i when win_off is NULL, e.g. vk_select_hits' c_isum compacted), precursor error in ppm
  * ((M_hyp - mass32[row]) / mass32[row] * 1e6), charge, peptide length, missed cleavages; zero padded.
  * n bounds the buffers; when n_dev is given the device count *n_dev (<= n) is used instead (no host sync). */
 int vk_cand_features(int64_t n, const int64_t* n_dev, const int64_t* c_hyp, const int64_t* c_row,

@@ -1,7 +1,7 @@
 """Golden vectors of the reference's target-decoy statistics (``vulcan/stats/tdc.py``, ``vulcan/stats/_util.py``),
 used to pin ``vulcan.stats`` (the restatement that counts PSMs accepted at a q-value threshold).
 
-Run in a checkout next to the reference:  python tests/golden/make_golden_tdc.py [reference_dir]
+Run with the reference checkout as the argument:  python tests/golden/make_golden_tdc.py <reference_dir>
 Writes tests/golden/golden_tdc.npz: random scored PSM sets with ties (seeded), their q-values, double-competition
 winners and q-values, and hash tie-break keys."""
 import os
@@ -9,7 +9,9 @@ import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: make_golden_tdc.py <reference_dir>")
+REF = sys.argv[1]
 sys.path.insert(0, REF)
 from vulcan.stats import _util as RU  # noqa: E402
 from vulcan.stats import tdc as R  # noqa: E402

@@ -150,6 +150,7 @@ __global__ void __launch_bounds__(FS_MAX_WARPS * 32) fused_search_k(FusedParams 
   vk::fence_mbar_init();
   __syncthreads();
   uint32_t phase = 0;
+  bool stalled = false;   // this warp's tile barrier gave up twice: it issues no more copies for the whole launch
   const vk::K2Out kout{khs, ksb, ksy, kppm, kmb, kmy, klb, kly};
 
   for (;;) {
@@ -213,6 +214,10 @@ __global__ void __launch_bounds__(FS_MAX_WARPS * 32) fused_search_k(FusedParams 
       while (h + 1 < nh && h_tile[h + 1] <= it) ++h;
       const int64_t lo = h_lo_s[h], hi = h_hi_s[h];
       const int64_t t = (lo >> ix.tile_shift) + (it - h_tile[h]);
+      if (stalled) {   // copies of this warp may still be in flight: its buffers and barrier are not reused
+        if (lane == 0) atomicOr(&P.status[s], VK_STATUS_WAIT_TIMEOUT << 1);
+        continue;
+      }
       const int64_t po = ix.tile_off[t];
       const uint32_t post_bytes = (uint32_t)((ix.tile_off[t + 1] - po) * 4);
       if (lane == 0) {
@@ -221,9 +226,13 @@ __global__ void __launch_bounds__(FS_MAX_WARPS * 32) fused_search_k(FusedParams 
         vk::bulk_g2s(cb, ix.cbin_off + t * cb_stride, (uint32_t)cb_stride * 2, &bars[warp]);
       }
       __syncwarp();
-      if (!vk::mbar_wait(&bars[warp], phase, FS_WAIT_LIMIT)) {
+      // warp-uniform decisions: every lane waits, and the warp gives up only if a lane did
+      if (!__all_sync(0xffffffffu, vk::mbar_wait(&bars[warp], phase, FS_WAIT_LIMIT))) {
         if (lane == 0) atomicOr(&P.status[s], VK_STATUS_WAIT_TIMEOUT << 1);
-        vk::mbar_wait(&bars[warp], phase, FS_WAIT_LIMIT);
+        if (!__all_sync(0xffffffffu, vk::mbar_wait(&bars[warp], phase, FS_WAIT_LIMIT))) {
+          stalled = true;   // the staged tile is not read and no later copy targets these buffers
+          continue;
+        }
       }
       phase ^= 1u;
       const int64_t r0 = t << ix.tile_shift;

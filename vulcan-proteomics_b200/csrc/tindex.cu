@@ -21,15 +21,8 @@ constexpr int TI_COUNT_WARPS = 4;
 template <class F>
 __device__ __forceinline__ int row_frag_count(const F& fp, const uint8_t* s, int L, uint64_t mk, float mass,
                                               int min_ion, float fmin, float fmax) {
-  float b = vk::nterm_of(fp, mk), y = __fsub_rn(mass, vk::nterm_of(fp, mk));
   int c = 0;
-  for (int k = 0; k + 1 < L; ++k) {
-    float rm = vk::resmass(fp, s[k], k, mk);
-    b = __fadd_rn(b, rm);
-    y = __fsub_rn(y, rm);
-    c += (k + 1 > min_ion && b >= fmin && b <= fmax);
-    c += (L - 1 - k > min_ion && y >= fmin && y <= fmax);
-  }
+  vk::row_ladder(fp, s, L, mk, mass, min_ion, fmin, fmax, [&](float) { ++c; });
   return c;
 }
 
@@ -111,20 +104,10 @@ tindex_emit_k(vk_tindex ix, vk_frag_params fpv, const int64_t* seq_off, const ui
   // emit keys
   for (int r = threadIdx.x; r < nr; r += blockDim.x) {
     int64_t g = r0 + r;
-    const uint8_t* s = res + seq_off[g];
-    int L = len[g];
-    uint64_t mk = mask[g];
-    float b = vk::nterm_of(fp, mk), y = __fsub_rn(mass32[g], vk::nterm_of(fp, mk));
     uint64_t* o = ti_smem + row_off[r];
-    for (int k = 0; k + 1 < L; ++k) {
-      float rm = vk::resmass(fp, s[k], k, mk);
-      b = __fadd_rn(b, rm);
-      y = __fsub_rn(y, rm);
-      if (k + 1 > ix.min_ion_index && b >= fmin && b <= fmax)
-        *o++ = ((uint64_t)(__float_as_uint(b) - ix.fmin_bits) << 16) | (uint64_t)r;
-      if (L - 1 - k > ix.min_ion_index && y >= fmin && y <= fmax)
-        *o++ = ((uint64_t)(__float_as_uint(y) - ix.fmin_bits) << 16) | (uint64_t)r;
-    }
+    vk::row_ladder(fp, res + seq_off[g], len[g], mask[g], mass32[g], ix.min_ion_index, fmin, fmax, [&](float f) {
+      *o++ = ((uint64_t)(__float_as_uint(f) - ix.fmin_bits) << 16) | (uint64_t)r;
+    });
   }
   for (int i = n_post + threadIdx.x; i < n_pow2; i += blockDim.x) ti_smem[i] = ~0ull;
   __syncthreads();
@@ -250,7 +233,8 @@ constexpr int64_t NOALLOC_SCAN_BLOCKS = 8192;
 static __device__ __align__(256) int64_t g_scan_scratch[NOALLOC_SCAN_BLOCKS];
 
 // Device address of g_scan_scratch per device.  In host code the array's name is only a stand-in; the address a
-// kernel may use comes from cudaGetSymbolAddress, taken once per device with that device current.
+// kernel may use comes from cudaGetSymbolAddress, taken once per device with that device current.  The cached
+// address is never refreshed, so it goes stale after a cudaDeviceReset of that device (documented in the header).
 constexpr int NOALLOC_MAX_DEVICES = 64;
 int64_t* g_scan_scratch_dev[NOALLOC_MAX_DEVICES] = {};
 std::mutex g_scan_scratch_mu;
@@ -348,10 +332,11 @@ int vk_scan_i64_noalloc(const int64_t* in, int64_t n, int64_t* out, void* stream
   cudaStream_t st = (cudaStream_t)stream;
   if (n < 0) return VK_E_ARG;
   if (n > NOALLOC_SCAN_BLOCKS * SCAN_TILE) return VK_E_TOO_LARGE;
+  // an empty input needs no scratch: no address lookup, so this case works inside a stream capture too
+  if (n == 0) return vk_err(cudaMemsetAsync(out, 0, sizeof(int64_t), st));
   int64_t* bs = nullptr;
   int rc = scan_scratch_address(&bs);
   if (rc != 0) return rc;
-  if (n == 0) return vk_err(cudaMemsetAsync(out, 0, sizeof(int64_t), st));
   // every block sum is written by scan_reduce_k before it is read: nothing in the scratch has to start at zero
   int64_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;
   scan_reduce_k<<<(unsigned)nb, SCAN_THREADS, 0, st>>>(in, n, bs);
