@@ -1,8 +1,9 @@
-"""L1 proteome index builder (mirror of the reference's ``vulcan/index/build.py``).
+"""L1 proteome index builder (same entry points as the reference's ``vulcan/index/build.py``).
 
     python -m vulcan.index.build --fasta a.fasta [b.fasta ...] --out DIR
 
-Same entry points (``default_params``, ``build``, ``L1Index``, ``read_labels``), same files, same columns:
+Entry points ``default_params``, ``content_hash``, ``build``, ``L1Index``, ``read_labels``; the files and columns
+are the reference's (``build.py:13-21``), because the reference's consumers read them:
 
   peptidoforms.arrow  pf_id u64, mass32 f32 (Sage f32), seq_off i64, length u8, mask u64, n_var u8, missed u8,
                       partner i64 (row of the target/decoy pair partner; partner[partner[i]] == i)
@@ -11,12 +12,23 @@ Same entry points (``default_params``, ``build``, ``L1Index``, ``read_labels``),
   proteins.arrow      target peptide -> protein CSR
   meta.json           params, counts, timings
 
-Rows are sorted by (Sage f32 mass, pf_id) (``build.py:168``), so the storage order is content-defined and a
-row window of a precursor tolerance is one contiguous range.  The search kernels only read the index side.
+Output contract (what the search and the statistics rely on):
+  * rows are ordered by (Sage f32 mass, pf_id), so storage order depends on content only, and the rows of a
+    precursor window are one contiguous range (``build.py:168``);
+  * every expanded form gives two rows, one per side of its target/decoy pair, and ``partner`` links them;
+  * the index side (peptidoforms + residues) does not depend on the pair order or on which side is called the
+    target: a build with the pair list shuffled and the roles swapped is bit-identical (``build.py:78-82``);
+  * the labels follow each row's own sequence.
+
+How it is computed here: the pair list is a table of per-pair attributes (side sequences, permutation, true
+forward, family, entrapment seed, target, missed cleavages); the native expansion returns forms (pair index,
+per-side mask / mass / id); every row is (form, side), so each output column is one gather of a per-form or
+per-pair attribute through the row's (form, side) coordinates, taken directly in the sorted row order.
 """
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import hashlib
 import json
 import os
@@ -58,193 +70,223 @@ def default_params() -> dict:
 
 
 def content_hash(fasta_paths, params) -> str:
+    """Hash of the inputs that define an index: FASTA bytes, parameters, index version, Sage revision."""
     h = hashlib.sha256()
-    for p in fasta_paths:
-        with open(p, "rb") as fh:
-            for b in iter(lambda: fh.read(1 << 22), b""):
-                h.update(b)
-    h.update(json.dumps(params, sort_keys=True).encode())
-    h.update(INDEX_VERSION.encode())
+    for path in fasta_paths:
+        with open(path, "rb") as fh:
+            while True:
+                block = fh.read(1 << 22)
+                if not block:
+                    break
+                h.update(block)
+    for part in (json.dumps(params, sort_keys=True), INDEX_VERSION, core.SAGE_COMMIT):
+        h.update(part.encode())
     return h.hexdigest()[:16]
 
 
-def _pair_perm(fwd: str, perm) -> np.ndarray:
-    """Explicit permutation array of a pair (the pseudo-reverse one when perm is None)."""
-    if perm is not None:
-        return np.asarray(perm, np.uint8)
-    n = len(fwd)
-    return np.array([n - 2 - j for j in range(n - 1)] + [n - 1], np.uint8)
+# ------------------------------------------------------------------------------------------------ string tables
+class _Strings:
+    """A list of ASCII strings as one byte buffer plus offsets (the form every column below is gathered from)."""
+
+    def __init__(self, strs):
+        strs = list(strs)
+        self.n = len(strs)
+        self.data = np.frombuffer("".join(strs).encode(), np.uint8)
+        self.lens = np.fromiter(map(len, strs), np.int64, self.n)
+        self.off = np.concatenate([[0], np.cumsum(self.lens)]).astype(np.int64)
+
+    def gather_bytes(self, idx: np.ndarray):
+        """(bytes of strings idx concatenated, their offsets)."""
+        ln = self.lens[idx]
+        off = np.concatenate([[0], np.cumsum(ln)]).astype(np.int64)
+        src = np.repeat(self.off[:-1][idx] - off[:-1], ln) + np.arange(off[-1], dtype=np.int64)
+        return self.data[src], off
+
+    def arrow(self, idx: np.ndarray) -> pa.Array:
+        body, off = self.gather_bytes(idx)
+        return pa.Array.from_buffers(pa.large_string(), len(idx), [None, pa.py_buffer(off), pa.py_buffer(body)])
 
 
-def _string_column(strs: list[str], order: np.ndarray) -> pa.Array:
-    """Arrow string column of strs[order] built from one byte buffer and an offsets buffer."""
-    data = np.frombuffer("".join(strs).encode(), np.uint8)
-    ln = np.fromiter((len(q) for q in strs), np.int64, len(strs))
-    off = np.zeros(len(strs) + 1, np.int64)
-    np.cumsum(ln, out=off[1:])
-    ln_s = ln[order]
-    off_s = np.zeros(len(order) + 1, np.int64)
-    np.cumsum(ln_s, out=off_s[1:])
-    gather = np.repeat(off[:-1][order] - off_s[:-1], ln_s) + np.arange(off_s[-1])
-    body = data[gather]
-    return pa.Array.from_buffers(pa.large_string(), len(order), [None, pa.py_buffer(off_s), pa.py_buffer(body)])
+# ------------------------------------------------------------------------------------------------ pair table
+@dataclasses.dataclass
+class _PairTable:
+    """The target/decoy pairs in the order handed to the expansion.
+
+    Side A is expanded as the expansion's "forward" member and side B through the pair's permutation.  ``a_decoy``:
+    side A holds the decoys (the role-swapped build)."""
+    side_a: list
+    side_b: list
+    perm_flat: np.ndarray
+    perm_off: np.ndarray
+    forward: list         # the true forward sequence of each pair
+    family: np.ndarray    # u8 family code of the forward sequence ("T" or "E")
+    seed: np.ndarray      # i32 entrapment seed (0 for targets)
+    target: list          # the target sequence the forward was derived from
+    missed: np.ndarray    # u8 missed cleavages of that target in the digest
+    a_decoy: bool
+
+
+def _forward_families(targets: list, p: dict):
+    """{forward sequence: (family, seed, target)}: the targets themselves and, per entrapment seed, the paired
+    entrapment peptides (``build.py:96-110``); plus the entrapment statistics."""
+    fam = {t: ("T", 0, t) for t in targets}
+    taken = set(targets)
+    stats = {}
+    for seed in p["entrap_seeds"]:
+        made, n_redraw, n_drop = D.make_entrapment(targets, seed, taken)
+        stats[str(seed)] = {"n": len(made), "redrawn": n_redraw, "dropped_unpairable": n_drop}
+        fam.update({ent: ("E", seed, t) for t, (ent, _) in made.items()})
+    return fam, stats
+
+
+def _pair_table(families: dict, decoys: dict, missed_of: dict, shuffle_seed, swap: bool) -> _PairTable:
+    """Pairs of every forward peptide that has a decoy, in sorted forward order, then permuted by the G0
+    ``shuffle_seed``; ``swap`` exchanges the sides (each explicit permutation inverted; the pseudo-reverse is its
+    own inverse)."""
+    fwd = sorted(f for f in families if f in decoys)
+    order = np.arange(len(fwd)) if shuffle_seed is None else np.random.default_rng(shuffle_seed).permutation(len(fwd))
+    fwd = [fwd[i] for i in order.tolist()]
+    dec = [decoys[f][0] for f in fwd]
+    perms = [decoys[f][1] for f in fwd]
+    if swap:
+        perms = [None if q is None else np.argsort(q).astype(np.uint8) for q in perms]
+    sizes = np.fromiter((0 if q is None else len(q) for q in perms), np.int64, len(perms))
+    explicit = [q for q in perms if q is not None]
+    info = [families[f] for f in fwd]
+    return _PairTable(
+        side_a=dec if swap else fwd, side_b=fwd if swap else dec,
+        perm_flat=np.concatenate(explicit).astype(np.uint8) if explicit else np.zeros(0, np.uint8),
+        perm_off=np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64),
+        forward=fwd,
+        family=np.fromiter((FAMILY[x[0]] for x in info), np.uint8, len(info)),
+        seed=np.fromiter((x[1] for x in info), np.int32, len(info)),
+        target=[x[2] for x in info],
+        missed=np.fromiter((missed_of[x[2]] for x in info), np.uint8, len(info)),
+        a_decoy=swap)
+
+
+def _target_key(seq: str) -> int:
+    return int.from_bytes(hashlib.blake2b(seq.encode(), digest_size=8).digest(), "little")
+
+
+# ------------------------------------------------------------------------------------------------ rows
+def _row_coordinates(forms: dict):
+    """Rows as (form, side) coordinates in the canonical (mass32, pf_id) order.  Returns (form, side, order)
+    where row r of the output is form[r] on side[r] (0 = side A) and order is the permutation of the unsorted
+    side-major row list (side A rows of all forms, then side B)."""
+    n = len(forms["seq"])
+    mass = np.stack([forms["mass32_f"], forms["mass32_d"]]).ravel()
+    ids = np.stack([forms["id_f"], forms["id_d"]]).ravel()
+    if np.unique(ids).size != ids.size:
+        raise RuntimeError("peptidoform id collision")
+    order = np.lexsort((ids, mass))
+    return order % n, order // n, order
 
 
 def build(fasta_paths, out_dir: str, params: dict | None = None, workers: int | None = None,
           shuffle_rows_seed: int | None = None, swap_labels: bool = False) -> dict:
-    """Build the index (``build.py:78-248``).  ``shuffle_rows_seed`` / ``swap_labels`` permute the pair list and
-    swap the forward/decoy roles of every pair; the index side must come out bit-identical (G0 invariance)."""
+    """Build the index (the reference's ``build.py:78-248`` contract).  ``shuffle_rows_seed`` / ``swap_labels``
+    permute the pair list and swap the target/decoy sides of every pair; the index side comes out bit-identical
+    (G0 invariance), only the labels may differ.  ``workers`` is accepted for signature compatibility."""
     p = default_params()
     p.update(params or {})
-    t0 = time.perf_counter()
+    clock = {"t": time.perf_counter()}
+    t_start = clock["t"]
     timing = {}
-    text = "".join(open(f).read() for f in fasta_paths)
+
+    def lap(name):
+        now = time.perf_counter()
+        timing[name] = now - clock["t"]
+        clock["t"] = now
+
     e = p["enzyme"]
+    text = "".join(open(f).read() for f in fasta_paths)
     dg = core.digest_fasta(text, e["missed_cleavages"], e["min_len"], e["max_len"], e["cleave_at"],
                            e["restrict"], e["c_terminal"])
     targets = list(dg["keys"])
-    timing["digest_s"] = time.perf_counter() - t0
+    missed_of = dict(zip(targets, np.asarray(dg["missed"]).tolist()))
+    lap("digest_s")
 
-    t1 = time.perf_counter()
-    taken = set(targets)
-    fwd_fam = {t: ("T", 0, t) for t in targets}
-    ent_stats = {}
-    for s in p["entrap_seeds"]:
-        m, nr, nd = D.make_entrapment(targets, s, taken)
-        ent_stats[str(s)] = {"n": len(m), "redrawn": nr, "dropped_unpairable": nd}
-        for t, (ent, _) in m.items():
-            fwd_fam[ent] = ("E", s, t)
-    forward = sorted(fwd_fam)
-    dec, n_dec_shuffled = D.make_decoys(forward, p["decoy_seed"])
-    forward = [f for f in forward if f in dec]
-    timing["families_s"] = time.perf_counter() - t1
+    families, ent_stats = _forward_families(targets, p)
+    decoys, n_dec_shuffled = D.make_decoys(sorted(families), p["decoy_seed"])
+    lap("families_s")
 
-    t2 = time.perf_counter()
-    fw = forward
-    dc = [dec[f][0] for f in fw]
-    order = np.arange(len(fw))
-    if shuffle_rows_seed is not None:
-        order = np.random.default_rng(shuffle_rows_seed).permutation(len(fw))
-    a_seq = [fw[i] for i in order]
-    b_seq = [dc[i] for i in order]
-    # explicit permutations only for shuffled decoys; an empty slice is the pseudo-reverse
-    perm_lists = [dec[fw[i]][1] for i in order]
-    if swap_labels:
-        a_seq, b_seq = b_seq, a_seq
-        perm_lists = [np.argsort(_pair_perm(b_seq[j], q)).astype(np.uint8) if q is not None else None
-                      for j, q in enumerate(perm_lists)]
-        # the inverse of the pseudo-reverse permutation is itself, so None stays None
-    plens = np.fromiter((0 if q is None else len(q) for q in perm_lists), np.int64, len(perm_lists))
-    poff = np.zeros(len(perm_lists) + 1, np.int64)
-    np.cumsum(plens, out=poff[1:])
-    explicit = [q for q in perm_lists if q is not None]
-    pflat = np.concatenate(explicit).astype(np.uint8) if explicit else np.zeros(0, np.uint8)
-    smods = sorted(p["static_mods"].items())
-    vmods = sorted(p["variable_mods"].items())
-    r = core.expand_pairs(a_seq, b_seq, pflat, poff, smods, vmods, p["max_variable_mods"],
-                          p["peptide_min_mass"], p["peptide_max_mass"], p["id_seed"],
-                          site_limits=p.get("site_limits"))
-    timing["expand_s"] = time.perf_counter() - t2
+    pt = _pair_table(families, decoys, missed_of, shuffle_rows_seed, swap_labels)
+    forms = core.expand_pairs(pt.side_a, pt.side_b, pt.perm_flat, pt.perm_off, sorted(p["static_mods"].items()),
+                              sorted(p["variable_mods"].items()), p["max_variable_mods"], p["peptide_min_mass"],
+                              p["peptide_max_mass"], p["id_seed"], site_limits=p.get("site_limits"))
+    lap("expand_s")
 
-    t3 = time.perf_counter()
-    n_pairs = len(r["seq"])
-    seq_i = r["seq"].astype(np.int64)
-    a_bytes = np.frombuffer("".join(a_seq).encode(), np.uint8)
-    b_bytes = np.frombuffer("".join(b_seq).encode(), np.uint8)
-    lens = np.fromiter((len(q) for q in a_seq), np.int64, len(a_seq))
-    a_off = np.zeros(len(a_seq) + 1, np.int64)
-    np.cumsum(lens, out=a_off[1:])
-    residues = np.concatenate([a_bytes, b_bytes])
-    pf_id = np.concatenate([r["id_f"], r["id_d"]])
-    mass32 = np.concatenate([r["mass32_f"], r["mass32_d"]])
-    seq_off = np.concatenate([a_off[seq_i], a_off[-1] + a_off[seq_i]])
-    length = np.concatenate([lens[seq_i], lens[seq_i]]).astype(np.uint8)
-    mask = np.concatenate([r["mask_f"], r["mask_d"]])
-    n_var = np.concatenate([r["n_var"], r["n_var"]])
-    # missed cleavages: the forward target's digest count, a pair attribute
-    fw_arr = np.asarray(fw, dtype=object)
-    tgt_of_fw = np.asarray([fwd_fam[f][2] for f in fw], dtype=object) if ent_stats else fw_arr
-    tgt_index = {t: i for i, t in enumerate(targets)}
-    missed_fw = dg["missed"][np.fromiter((tgt_index[t] for t in tgt_of_fw), np.int64, len(fw))]
-    missed_seq = missed_fw[order]
-    missed = np.concatenate([missed_seq[seq_i], missed_seq[seq_i]])
-    side_b = np.concatenate([np.zeros(n_pairs, bool), np.ones(n_pairs, bool)])
-    if len(np.unique(pf_id)) != len(pf_id):
-        raise RuntimeError("peptidoform id collision")
-    srt = np.lexsort((pf_id, mass32))
-    inv = np.empty_like(srt)
-    inv[srt] = np.arange(len(srt))
-    partner_unsorted = np.concatenate([np.arange(n_pairs) + n_pairs, np.arange(n_pairs)])
-    partner = inv[partner_unsorted][srt]
-    lens_s = length[srt].astype(np.int64)
-    new_off = np.zeros(len(srt) + 1, np.int64)
-    np.cumsum(lens_s, out=new_off[1:])
-    gather = np.repeat(seq_off[srt] - new_off[:-1], lens_s) + np.arange(new_off[-1])
-    residues_s = residues[gather]
+    # ---- index side: every column gathered through (form, side) in sorted order
+    n_forms = len(forms["seq"])
+    form, side, order = _row_coordinates(forms)
+    pair = forms["seq"].astype(np.int64)[form]
+    rank = np.empty_like(order)
+    rank[order] = np.arange(order.size)
+    partner = rank[np.where(order < n_forms, order + n_forms, order - n_forms)]
+    a_str, b_str = _Strings(pt.side_a), _Strings(pt.side_b)
+    both = _Strings([])                 # side A sequences then side B sequences, one string table
+    both.data = np.concatenate([a_str.data, b_str.data])
+    both.lens = np.concatenate([a_str.lens, b_str.lens])
+    both.off = np.concatenate([a_str.off[:-1], a_str.off[-1] + b_str.off]).astype(np.int64)
+    residues, seq_off = both.gather_bytes(pair + side * len(pt.side_a))
+    per_side = lambda f, d: np.where(side == 0, forms[f][form], forms[d][form])
+    pf_id = per_side("id_f", "id_d")
     idx_tbl = pa.table({
-        "pf_id": pa.array(pf_id[srt], pa.uint64()),
-        "mass32": pa.array(mass32[srt], pa.float32()),
-        "seq_off": pa.array(new_off[:-1], pa.int64()),
-        "length": pa.array(length[srt], pa.uint8()),
-        "mask": pa.array(mask[srt], pa.uint64()),
-        "n_var": pa.array(n_var[srt], pa.uint8()),
-        "missed": pa.array(missed[srt], pa.uint8()),
+        "pf_id": pa.array(pf_id, pa.uint64()),
+        "mass32": pa.array(per_side("mass32_f", "mass32_d"), pa.float32()),
+        "seq_off": pa.array(seq_off[:-1], pa.int64()),
+        "length": pa.array(a_str.lens[pair].astype(np.uint8), pa.uint8()),
+        "mask": pa.array(per_side("mask_f", "mask_d"), pa.uint64()),
+        "n_var": pa.array(forms["n_var"][form], pa.uint8()),
+        "missed": pa.array(pt.missed[pair], pa.uint8()),
         "partner": pa.array(partner, pa.int64()),
     })
-    timing["arrays_s"] = time.perf_counter() - t3
+    lap("arrays_s")
 
-    fam_fw = np.fromiter((FAMILY[fwd_fam[f][0]] for f in fw), np.uint8, len(fw)) if ent_stats else \
-        np.zeros(len(fw), np.uint8)
-    seed_fw = np.fromiter((fwd_fam[f][1] for f in fw), np.int32, len(fw)) if ent_stats else np.zeros(len(fw), np.int32)
-    fam_fwd, seed_fwd = fam_fw[order], seed_fw[order]
-    is_dec = side_b if not swap_labels else ~side_b
-    fam_side = np.concatenate([fam_fwd[seq_i], fam_fwd[seq_i]])
-    fam = np.where(is_dec, fam_side + 2, fam_side)
-    fwd_member_id = np.where(is_dec, pf_id[partner_unsorted], pf_id)
-    tgt_pairs = [tgt_of_fw[i] for i in order.tolist()]
-    ep = np.fromiter((int.from_bytes(hashlib.blake2b(t.encode(), digest_size=8).digest(), "little")
-                      for t in tgt_pairs), np.uint64, len(tgt_pairs))
-    ep = np.concatenate([ep[seq_i], ep[seq_i]])
-    # string columns straight from byte buffers: the forward (true-label) sequence and its target of every row
-    fwd_strs = [x if not swap_labels else y for x, y in zip(a_seq, b_seq)]
-    fwd_col = _string_column([fwd_strs[i] for i in seq_i.tolist()] * 2, srt)
-    tgt_col = _string_column([tgt_pairs[i] for i in seq_i.tolist()] * 2, srt)
+    # ---- labels: a row is a decoy when it sits on the decoy side of its pair
+    is_decoy = (side == 0) if pt.a_decoy else (side == 1)
+    family = pt.family[pair] + np.where(is_decoy, 2, 0).astype(np.uint8)
+    fwd_str = _Strings(pt.forward)
+    tgt_str = _Strings(pt.target)
+    tgt_key = np.fromiter(map(_target_key, pt.target), np.uint64, len(pt.target))
     lab = pa.table({
-        "pf_id": pa.array(pf_id[srt], pa.uint64()),
-        "family": pa.array(fam[srt].astype(np.uint8)),
-        "entrap_seed": pa.array(np.concatenate([seed_fwd[seq_i], seed_fwd[seq_i]])[srt], pa.int32()),
-        "is_decoy": pa.array(is_dec[srt]),
-        "is_entrapment": pa.array((fam[srt] % 2) == 1),
-        "tdc_pair": pa.array(fwd_member_id[srt], pa.uint64()),
-        "entrap_pair": pa.array(ep[srt], pa.uint64()),
-        "fwd_seq": fwd_col,
-        "target_seq": tgt_col,
+        "pf_id": pa.array(pf_id, pa.uint64()),
+        "family": pa.array(family.astype(np.uint8)),
+        "entrap_seed": pa.array(pt.seed[pair], pa.int32()),
+        "is_decoy": pa.array(is_decoy),
+        "is_entrapment": pa.array((family % 2) == 1),
+        "tdc_pair": pa.array(np.where(is_decoy, pf_id[partner], pf_id), pa.uint64()),
+        "entrap_pair": pa.array(tgt_key[pair], pa.uint64()),
+        "fwd_seq": fwd_str.arrow(pair),
+        "target_seq": tgt_str.arrow(pair),
     })
+    prot_off = np.asarray(dg["prot_off"])
     prot = pa.table({
         "peptide": pa.array(targets, pa.string()),
-        "prot_off": pa.array(dg["prot_off"][:-1], pa.int64()),
-        "prot_len": pa.array(np.diff(dg["prot_off"]), pa.int64()),
+        "prot_off": pa.array(prot_off[:-1], pa.int64()),
+        "prot_len": pa.array(np.diff(prot_off), pa.int64()),
     })
     os.makedirs(out_dir, exist_ok=True)
     _write(idx_tbl, os.path.join(out_dir, "peptidoforms.arrow"))
-    np.save(os.path.join(out_dir, "residues.npy"), residues_s)
+    np.save(os.path.join(out_dir, "residues.npy"), residues)
     _write(lab, os.path.join(out_dir, "labels.arrow"))
     _write(prot, os.path.join(out_dir, "proteins.arrow"))
     np.save(os.path.join(out_dir, "protein_idx.npy"), dg["prot_idx"])
     with open(os.path.join(out_dir, "accessions.txt"), "w") as fh:
         fh.write("\n".join(dg["accessions"]) + "\n")
-    timing["total_s"] = time.perf_counter() - t0
-    fams = np.bincount(fam.astype(np.int64), minlength=4)
+    timing["total_s"] = time.perf_counter() - t_start
+    by_family = np.bincount(family.astype(np.int64), minlength=4)
     meta = {
         "index_version": INDEX_VERSION, "sage_commit": core.SAGE_COMMIT, "params": p,
         "fasta": [os.path.abspath(f) for f in fasta_paths],
         "content_hash": content_hash(fasta_paths, p),
         "n_targets": len(targets), "n_nonstandard_dropped": int(dg["n_nonstandard"]),
-        "n_forward_peptides": len(fw), "n_decoy_shuffled": n_dec_shuffled,
-        "n_forward_without_decoy": len(fwd_fam) - len(fw),
+        "n_forward_peptides": len(pt.forward), "n_decoy_shuffled": n_dec_shuffled,
+        "n_forward_without_decoy": len(families) - len(pt.forward),
         "entrapment": ent_stats,
-        "n_peptidoforms": int(len(pf_id)),
-        "n_peptidoforms_by_family": {k: int(fams[v]) for k, v in FAMILY.items()},
+        "n_peptidoforms": int(order.size),
+        "n_peptidoforms_by_family": {k: int(by_family[v]) for k, v in FAMILY.items()},
         "timing_s": timing,
         "g0_test_knobs": {"shuffle_rows_seed": shuffle_rows_seed, "swap_labels": swap_labels},
     }
@@ -259,14 +301,8 @@ class L1Index:
     def __init__(self, path: str):
         self.path = path
         t = _read(os.path.join(path, "peptidoforms.arrow"))
-        self.pf_id = t.column("pf_id").to_numpy()
-        self.mass32 = t.column("mass32").to_numpy()
-        self.seq_off = t.column("seq_off").to_numpy()
-        self.length = t.column("length").to_numpy()
-        self.mask = t.column("mask").to_numpy()
-        self.n_var = t.column("n_var").to_numpy()
-        self.missed = t.column("missed").to_numpy()
-        self.partner = t.column("partner").to_numpy()
+        for name in ("pf_id", "mass32", "seq_off", "length", "mask", "n_var", "missed", "partner"):
+            setattr(self, name, t.column(name).to_numpy())
         self.partners = [self.partner] + [t.column(f"partner_{j}").to_numpy()
                                           for j in range(1, 64) if f"partner_{j}" in t.column_names]
         self.residues = np.load(os.path.join(path, "residues.npy"))
