@@ -61,6 +61,24 @@ __device__ __forceinline__ float nterm_of(const F& fp, uint64_t mask) {
   return (mask & VK_NTERM_BIT) ? fp.nterm : 0.f;
 }
 
+// Fragment ladder of one peptidoform row in Sage f32 arithmetic (reference kernels.cu:53-71): for k = 0 .. L-2,
+// the b ion after residue k (a running sum from the N-terminal modification) and the y ion (the row's mass minus
+// that sum); visit(mass) is called for each ion whose ion index exceeds min_ion and whose mass lies in
+// [fmin, fmax], b before y at every k.  Shared by the tiled index build and the reference-layout CSR build.
+template <class F, class V>
+__device__ __forceinline__ void row_ladder(const F& fp, const uint8_t* s, int L, uint64_t mk, float mass,
+                                           int min_ion, float fmin, float fmax, V&& visit) {
+  const float nt = nterm_of(fp, mk);
+  float b = nt, y = __fsub_rn(mass, nt);
+  for (int k = 0; k + 1 < L; ++k) {
+    const float rm = resmass(fp, s[k], k, mk);
+    b = __fadd_rn(b, rm);
+    y = __fsub_rn(y, rm);
+    if (k + 1 > min_ion && b >= fmin && b <= fmax) visit(b);
+    if (L - 1 - k > min_ion && y >= fmin && y <= fmax) visit(y);
+  }
+}
+
 __device__ __forceinline__ double lnfact(int n) {
   // Stirling's approximation of ln n!, with lnfact(0) = 1 as in Sage (kernels.cu:246-250)
   if (n == 0) return 1.0;
