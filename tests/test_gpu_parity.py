@@ -340,7 +340,7 @@ def test_k1_counts_for_every_tile_layout(mini, param_sets, torch_cuda, layout):
         q = dataclasses.replace(p, tile_rows=tile_rows, cbin_bits=cbin, k1_warps=warps, search_method="staged")
         gi = E.GpuIndex(l1, q, STATIC, VAR)
         st = E.Stats()
-        f = PR._front(E.DeviceRun(sp, gi.dev, st), gi, q, st, False)
+        f = PR._front(E.DeviceRun(sp, gi.dev, st), gi, q, st, False, dense=True)
         hyp = {k: f["dh"][k].cpu().numpy() for k in ("spec", "maxfz", "lo", "hi")}
         pk = {k: f["peaks"][k].cpu().numpy() for k in ("off", "mass", "int")}
         P = O.make_params(STATIC, VAR, q.fragment_unit)
@@ -351,6 +351,29 @@ def test_k1_counts_for_every_tile_layout(mini, param_sets, torch_cuda, layout):
         # the plain search's counts (no intensity sums) are the same
         out = E.search(sp, gi, l1, q)[2]
         assert np.array_equal(out["cnt"][:n_win].cpu().numpy(), cnt), name
+        # the hit-list form gives the shortlist of the dense form, with the same intensity sums and statistics
+        for thr in (1, 2):
+            fh = PR._front(E.DeviceRun(sp, gi.dev, st), gi, q, st, False, min_count=thr)
+            fd = PR._front(E.DeviceRun(sp, gi.dev, st), gi, q, st, False, min_count=thr, dense=True)
+            _assert_same_shortlist(fh, fd, sp, (name, layout, thr))
+
+
+def _assert_same_shortlist(fh, fd, sp, what):
+    n = len(sp)
+    nc = int(fd["hits"]["cand_off"][n])
+    assert int(fh["hits"]["cand_off"][n]) == nc, what
+    for k in ("c_hyp", "c_row", "c_cnt"):
+        assert np.array_equal(fh["hits"][k][:nc].cpu().numpy(), fd["hits"][k][:nc].cpu().numpy()), (what, k)
+    dh, hits = fd["dh"], fd["hits"]
+    h = hits["c_hyp"][:nc]
+    dense_isum = fd["isum"][fd["win_off"][h] + hits["c_row"][:nc] - dh["lo"][h]]
+    assert np.array_equal(fh["hits"]["c_isum"][:nc].cpu().numpy(), dense_isum.cpu().numpy()), what
+    nh = int(dh["spec_off"][n])
+    for k in ("hyp_scored", "hyp_matched"):
+        assert np.array_equal(fh[k][:nh].cpu().numpy().astype(np.int64),
+                              fd[k][:nh].cpu().numpy().astype(np.int64)), (what, k)
+    for k in ("spec_scored", "spec_matched"):
+        assert np.array_equal(fh[k][:n].cpu().numpy(), fd[k][:n].cpu().numpy()), (what, k)
 
 
 @pytest.mark.parametrize("name", SETS)

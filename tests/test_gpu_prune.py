@@ -31,12 +31,14 @@ def indexes(mini, param_sets, torch_cuda):
     return {name: E.GpuIndex(l1, p, STATIC, VAR) for name, p in param_sets.items()}
 
 
-def _front(sp, gi, p):
+def _front(sp, gi, p, dense=True):
+    """The pruned search's front end; dense: with K1's dense per-row counts and intensity sums (the hit-list form
+    keeps only the shortlist's)."""
     from vulcan.gpu import engine as E
     from vulcan.gpu import prune as PR
     st = E.Stats()
     run = E.DeviceRun(sp, gi.dev, st)
-    return PR._front(run, gi, p, st, False)
+    return PR._front(run, gi, p, st, False, dense=dense)
 
 
 def _np(t):
@@ -87,6 +89,11 @@ def test_features_equal_oracle(mini, param_sets, indexes, name, torch_cuda):
     n_dev = hits["cand_off"][-1:]
     feat2 = pr.features(gi, f["dh"], f["win_off"], f["isum"], hits, n + 37, n_dev=n_dev)
     assert torch.equal(feat2[:n], feat)
+    # the hit-list front end (intensity sums carried with the shortlist) gives the same features
+    fh = _front(sp, gi, p, dense=False)
+    assert int(fh["hits"]["cand_off"][-1]) == n
+    feat3 = pr.features(gi, fh["dh"], fh["win_off"], None, fh["hits"], n)[:n]
+    assert torch.equal(feat3, feat)
 
 
 def _random_pruner(torch, dev, seed):

@@ -54,6 +54,19 @@ struct K1Rec {
   int32_t n, rows;    // peaks; local rows rlo | rhi << 16
   int32_t mfz;        // fragment charges + 1 (0: item skipped)
   float ws;           // intensity weight scale 2^24 / TIC
+  int32_t h;          // hypothesis (the hit-list output appends to its region)
+};
+
+// Outputs of the hit-list form of K1 (vk_k1_hits): instead of a dense count per window row, the rows with count >=
+// thr of hypothesis h are appended to its region [win_off[h], win_off[h] + hyp_hits[h]) of rc (count << 32 | row)
+// and isum; per hypothesis the number of rows with a nonzero count and the sum of the counts.
+struct K1Hits {
+  int thr;
+  uint64_t* rc;
+  uint32_t* isum;
+  uint32_t* hyp_hits;
+  uint32_t* hyp_scored;
+  unsigned long long* hyp_matched;
 };
 
 // Loads the record of item `it` of the tile whose first row is r0; items and windows must lie inside the buffers the
@@ -76,6 +89,7 @@ __device__ __forceinline__ K1Rec k1_record(int64_t it, int64_t r0, int T, const 
     return r;
   }
   const int s = h_spec[h];
+  r.h = h;
   r.p0 = pk_off[s];
   r.n = (int32_t)(pk_off[s + 1] - r.p0);
   r.base = win_off[h] + (r0 - lo);
@@ -91,12 +105,15 @@ __device__ __forceinline__ K1Rec k1_record(int64_t it, int64_t r0, int T, const 
 // item's chain of dependent loads (item -> hypothesis -> spectrum) overlaps the copy and the other items'.  Warp w
 // then runs the filtered per-item search of items w, w + warps, ... (measured faster than items taken one at a time
 // through a shared-memory counter).
+// HITS: the hit-list form (K1Hits) instead of the dense counts.
+template <bool HITS>
 __global__ void __launch_bounds__(K1_MAX_WARPS * 32, 1)
 k1_tiles_k(vk_tindex ix, float tol_lo, float tol_hi, int tol_da, int post_cap, const int64_t* tile_item_off,
            const int32_t* item_hyp, int64_t n_hyp, int64_t item_cap, const int32_t* h_spec, const int8_t* h_maxfz,
            const int64_t* h_lo, const int64_t* h_hi, const int64_t* win_off, int64_t cnt_cap, const int64_t* pk_off,
            const float* pk_mass, int32_t* cnt, int32_t* status, const float* pk_int, const float* tic,
-           uint32_t* isum_out, const uint2* pk_keys, const uint32_t* pk_filt, int n_kz, int64_t kstride) {
+           uint32_t* isum_out, const uint2* pk_keys, const uint32_t* pk_filt, int n_kz, int64_t kstride,
+           K1Hits hits) {
   extern __shared__ __align__(16) uint8_t k1_smem[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ K1Rec rec[K1_ITEMS];
@@ -160,9 +177,39 @@ k1_tiles_k(vk_tindex ix, float tol_lo, float tol_hi, int tol_da, int post_cap, c
                            r.mfz, pk_keys, pk_filt, n_kz, kstride, pk_mass, tol_lo, tol_hi, tol_da, ix, lane, qw,
                            pk_int, r.ws);
       __syncwarp();
-      for (int q = rlo + lane; q < rhi; q += 32) {
-        cnt[r.base + q] = (int32_t)hw[q];
-        if (iw) isum_out[r.base + q] = iw[q];
+      if (HITS) {
+        // rows with count >= thr appended to the hypothesis' region, one atomic per 32 rows; the statistics of
+        // the item's rows added to the hypothesis' totals (integer sums: the result does not depend on order)
+        const int64_t region = win_off[r.h];
+        long long sc = 0, mt = 0;
+        for (int q0 = rlo; q0 < rhi; q0 += 32) {
+          const int q = q0 + lane;
+          const uint32_t c = q < rhi ? hw[q] : 0u;
+          sc += c > 0u;
+          mt += c;
+          const bool keep = q < rhi && (int)c >= hits.thr;
+          const unsigned bal = __ballot_sync(VK_FULL, keep);
+          if (!bal) continue;
+          uint32_t at0 = 0;
+          if (lane == 0) at0 = atomicAdd(&hits.hyp_hits[r.h], (uint32_t)__popc(bal));
+          at0 = __shfl_sync(VK_FULL, at0, 0);
+          if (keep) {
+            const int64_t at = region + at0 + __popc(bal & ((1u << lane) - 1u));
+            hits.rc[at] = ((uint64_t)c << 32) | (uint64_t)(r0 + q);
+            if (iw) hits.isum[at] = iw[q];
+          }
+        }
+        sc = vk::warp_sum(sc);
+        mt = vk::warp_sum(mt);
+        if (lane == 0) {
+          if (sc) atomicAdd(&hits.hyp_scored[r.h], (uint32_t)sc);
+          if (mt) atomicAdd(&hits.hyp_matched[r.h], (unsigned long long)mt);
+        }
+      } else {
+        for (int q = rlo + lane; q < rhi; q += 32) {
+          cnt[r.base + q] = (int32_t)hw[q];
+          if (iw) isum_out[r.base + q] = iw[q];
+        }
       }
       __syncwarp();
     }
@@ -219,12 +266,18 @@ int vk_k1_plan_fill(const vk_tindex* ix, int64_t n_hyp, const int64_t* h_lo, con
   return vk_launch_status();
 }
 
-int vk_k1_tiles(const vk_tindex* ix, const vk_frag_params* fp, float tol_lo, float tol_hi, int warps,
-                const int64_t* tile_item_off, const int32_t* item_hyp, int64_t n_hyp, int64_t item_cap,
-                const int32_t* h_spec, const int8_t* h_maxfz, const int64_t* h_lo, const int64_t* h_hi,
-                const int64_t* win_off, int64_t cnt_cap, const int64_t* pk_off, const float* pk_mass, int32_t* cnt,
-                int32_t* status, const float* pk_int, const float* tic, uint32_t* isum, const uint32_t* pk_keys,
-                const uint32_t* pk_filt, int n_kz, int64_t kstride, void* stream) {
+}  // extern "C"
+
+namespace {
+
+template <bool HITS>
+int k1_tiles_launch(const vk_tindex* ix, const vk_frag_params* fp, float tol_lo, float tol_hi, int warps,
+                    const int64_t* tile_item_off, const int32_t* item_hyp, int64_t n_hyp, int64_t item_cap,
+                    const int32_t* h_spec, const int8_t* h_maxfz, const int64_t* h_lo, const int64_t* h_hi,
+                    const int64_t* win_off, int64_t cnt_cap, const int64_t* pk_off, const float* pk_mass,
+                    int32_t* cnt, int32_t* status, const float* pk_int, const float* tic, uint32_t* isum,
+                    const uint32_t* pk_keys, const uint32_t* pk_filt, int n_kz, int64_t kstride, K1Hits hits,
+                    void* stream) {
   if (!ix || !fp || !status) return VK_E_ARG;
   if (ix->n_tiles == 0) return 0;
   if ((ix->max_tile_postings & 3) || ix->max_tile_postings < 0 || warps < 1 || warps > K1_MAX_WARPS) return VK_E_ARG;
@@ -237,13 +290,44 @@ int vk_k1_tiles(const vk_tindex* ix, const vk_frag_params* fp, float tol_lo, flo
   const size_t sh = (size_t)ix->max_tile_postings * 4 + (size_t)stride * 2 + (size_t)nb * vk::K1_BM_WORDS * 4 +
                     (size_t)warps * (T * 4 * (isum ? 2 : 1) + vk::K1_QUEUE * 4);
   if (sh > 200 * 1024) return VK_E_TOO_LARGE;
-  cudaError_t e = cudaFuncSetAttribute(k1_tiles_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  cudaError_t e = cudaFuncSetAttribute(k1_tiles_k<HITS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
   if (e != cudaSuccess) return vk_err(e);
-  k1_tiles_k<<<(unsigned)ix->n_tiles, warps * 32, sh, (cudaStream_t)stream>>>(
+  k1_tiles_k<HITS><<<(unsigned)ix->n_tiles, warps * 32, sh, (cudaStream_t)stream>>>(
       *ix, tol_lo, tol_hi, fp->tol_da, ix->max_tile_postings, tile_item_off, item_hyp, n_hyp, item_cap, h_spec,
       h_maxfz, h_lo, h_hi, win_off, cnt_cap, pk_off, pk_mass, cnt, status, pk_int, tic, isum,
-      reinterpret_cast<const uint2*>(pk_keys), pk_filt, n_kz > 0 ? n_kz : 0, kstride);
+      reinterpret_cast<const uint2*>(pk_keys), pk_filt, n_kz > 0 ? n_kz : 0, kstride, hits);
   return vk_launch_status();
+}
+
+}  // namespace
+
+extern "C" {
+
+int vk_k1_tiles(const vk_tindex* ix, const vk_frag_params* fp, float tol_lo, float tol_hi, int warps,
+                const int64_t* tile_item_off, const int32_t* item_hyp, int64_t n_hyp, int64_t item_cap,
+                const int32_t* h_spec, const int8_t* h_maxfz, const int64_t* h_lo, const int64_t* h_hi,
+                const int64_t* win_off, int64_t cnt_cap, const int64_t* pk_off, const float* pk_mass, int32_t* cnt,
+                int32_t* status, const float* pk_int, const float* tic, uint32_t* isum, const uint32_t* pk_keys,
+                const uint32_t* pk_filt, int n_kz, int64_t kstride, void* stream) {
+  if (!cnt) return VK_E_ARG;
+  return k1_tiles_launch<false>(ix, fp, tol_lo, tol_hi, warps, tile_item_off, item_hyp, n_hyp, item_cap, h_spec,
+                                h_maxfz, h_lo, h_hi, win_off, cnt_cap, pk_off, pk_mass, cnt, status, pk_int, tic, isum,
+                                pk_keys, pk_filt, n_kz, kstride, K1Hits{}, stream);
+}
+
+int vk_k1_hits(const vk_tindex* ix, const vk_frag_params* fp, float tol_lo, float tol_hi, int warps,
+               const int64_t* tile_item_off, const int32_t* item_hyp, int64_t n_hyp, int64_t item_cap,
+               const int32_t* h_spec, const int8_t* h_maxfz, const int64_t* h_lo, const int64_t* h_hi,
+               const int64_t* win_off, int64_t cnt_cap, const int64_t* pk_off, const float* pk_mass, int thr,
+               uint64_t* hit_rc, uint32_t* hit_isum, uint32_t* hyp_hits, uint32_t* hyp_scored,
+               uint64_t* hyp_matched, int32_t* status, const float* pk_int, const float* tic,
+               const uint32_t* pk_keys, const uint32_t* pk_filt, int n_kz, int64_t kstride, void* stream) {
+  if (!hit_rc || !hyp_hits || !hyp_scored || !hyp_matched || thr < 1) return VK_E_ARG;
+  if ((hit_isum != nullptr) != (pk_int != nullptr)) return VK_E_ARG;
+  K1Hits hits{thr, hit_rc, hit_isum, hyp_hits, hyp_scored, reinterpret_cast<unsigned long long*>(hyp_matched)};
+  return k1_tiles_launch<true>(ix, fp, tol_lo, tol_hi, warps, tile_item_off, item_hyp, n_hyp, item_cap, h_spec,
+                               h_maxfz, h_lo, h_hi, win_off, cnt_cap, pk_off, pk_mass, nullptr, status, pk_int, tic,
+                               hit_isum, pk_keys, pk_filt, n_kz, kstride, hits, stream);
 }
 
 int vk_k1_peak_keys(const vk_tindex* ix, const vk_frag_params* fp, float tol_lo, float tol_hi, const int64_t* n_peaks,

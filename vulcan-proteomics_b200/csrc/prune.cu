@@ -41,7 +41,8 @@ __global__ void cand_features_k(int64_t n, const int64_t* n_dev, const int64_t* 
   const float mr = mass32[r];
   float raw[6];
   raw[0] = (float)c_cnt[i];
-  raw[1] = (float)isum[win_off[h] + (r - h_lo[h])] * (1.0f / 16777216.0f);
+  // the intensity sum from the dense K1 sums, or (win_off NULL) one per candidate, from the hit-list shortlist
+  raw[1] = (float)(win_off ? isum[win_off[h] + (r - h_lo[h])] : isum[i]) * (1.0f / 16777216.0f);
   raw[2] = (h_M[h] - mr) / mr * 1.0e6f;
   raw[3] = (float)h_z[h];
   raw[4] = (float)len[r];

@@ -268,6 +268,158 @@ select_topk_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo, cons
   if (lane == 0) n_cand[s] = n_out;
 }
 
+// Shortlist from the hit lists of vk_k1_hits, one warp per spectrum: the hits of the spectrum's hypotheses (region
+// of hypothesis h: [win_off[h], win_off[h] + hyp_hits[h]) of rc = count << 32 | row, and of isum) ranked by (count
+// desc, row desc, hypothesis asc) with the keys of select_topk_k, the first topk kept (all when fewer), sorted by
+// (row, hypothesis), duplicate rows merged to the lowest hypothesis (its intensity sum) and the highest count: the
+// slots select_topk_k writes without pair closure, plus c_isum.  The positions of the hits inside a region depend
+// on the order in which K1's items appended them, the selection and the output do not.  Spectra with more hits
+// than shared memory holds take the radix select over the hit lists in global memory and a second read.
+__global__ void __launch_bounds__(TK_WARPS * 32)
+select_hits_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* win_off, const uint32_t* hyp_hits,
+              const uint64_t* rc, const uint32_t* hit_isum, const uint32_t* hyp_scored, const uint64_t* hyp_matched,
+              int topk, int cap, int list_pow2, int key_cap, int64_t* c_hyp, int64_t* c_row, int64_t* c_cnt,
+              uint32_t* c_isum, int64_t* n_cand, int64_t* spec_scored, int64_t* spec_matched) {
+  extern __shared__ __align__(16) uint8_t tk_smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int s = blockIdx.x * TK_WARPS + warp;
+  if (s >= n_spec) return;
+  const size_t per_warp = (size_t)key_cap * 12 + (size_t)list_pow2 * 16 + 256 * 4;
+  uint8_t* base = tk_smem + per_warp * warp;
+  uint64_t* key = reinterpret_cast<uint64_t*>(base);
+  uint32_t* src = reinterpret_cast<uint32_t*>(base + (size_t)key_cap * 8);   // hit position - win_off[hb]
+  int32_t* row = reinterpret_cast<int32_t*>(src + key_cap);
+  int32_t* hl = row + list_pow2;
+  int32_t* cnt = hl + list_pow2;
+  uint32_t* isum = reinterpret_cast<uint32_t*>(cnt + list_pow2);
+  uint32_t* hist = isum + list_pow2;
+  const unsigned lt_mask = (1u << lane) - 1u;
+  const int64_t hb = spec_hyp_off[s], he = spec_hyp_off[s + 1];
+  const int64_t w_base = he > hb ? win_off[hb] : 0;
+  // per-spectrum statistics from K1's per-hypothesis totals
+  long long sc = 0, mt = 0;
+  for (int64_t h = hb + lane; h < he; h += 32) {
+    sc += hyp_scored[h];
+    mt += (long long)hyp_matched[h];
+  }
+  sc = vk::warp_sum(sc);
+  mt = vk::warp_sum(mt);
+  if (lane == 0 && spec_scored) {
+    spec_scored[s] = sc;
+    spec_matched[s] = mt;
+  }
+  auto n_hits = [&](int64_t h) -> int64_t {   // a region never holds more than its window
+    return min((int64_t)hyp_hits[h], win_off[h + 1] - win_off[h]);
+  };
+  // the hits as selection keys in shared memory (as many as fit)
+  long long n_app = 0;
+  for (int64_t h = hb; h < he; ++h) {
+    const int64_t r0 = win_off[h], n = n_hits(h);
+    for (int64_t j0 = 0; j0 < n; j0 += 32) {
+      const int64_t j = j0 + lane;
+      const bool ok = j < n;
+      const unsigned m = __ballot_sync(VK_FULL, ok);
+      if (ok) {
+        const long long at = n_app + __popc(m & lt_mask);
+        if (at < key_cap) {
+          const uint64_t v = rc[r0 + j];
+          key[at] = sel_key((int)min(v >> 32, (uint64_t)INT32_MAX), (int64_t)(uint32_t)v, (int)(h - hb));
+          src[at] = (uint32_t)(r0 + j - w_base);
+        }
+      }
+      n_app += __popc(m);
+    }
+  }
+  __syncwarp();
+  const bool limit = n_app > topk;
+  int n_sel = 0;
+  auto take_hit = [&](bool take, int64_t pos_g, int h_local) {
+    const unsigned m = __ballot_sync(VK_FULL, take);
+    if (take) {
+      const int at = n_sel + __popc(m & lt_mask);
+      const uint64_t v = rc[pos_g];
+      row[at] = (int32_t)(uint32_t)v;
+      hl[at] = h_local;
+      cnt[at] = (int32_t)min(v >> 32, (uint64_t)INT32_MAX);
+      isum[at] = hit_isum ? hit_isum[pos_g] : 0u;
+    }
+    n_sel += __popc(m);
+  };
+  if (n_app <= key_cap) {
+    const int n_k = (int)n_app;
+    const uint64_t kth = limit ? smem_kth_largest(key, n_k, topk, hist, lane) : 0ull;
+    for (int i0 = 0; i0 < n_k; i0 += 32) {
+      const int i = i0 + lane;
+      const uint64_t k = i < n_k ? key[i] : 0ull;
+      const bool take = i < n_k && (!limit || k >= kth);
+      take_hit(take, take ? w_base + src[i] : 0, (1 << 18) - 1 - (int)(k & 0x3ffff));
+    }
+  } else {
+    uint64_t prefix = 0, pmask = 0;
+    long long need = topk;
+    for (int shift = 56; shift >= 0; shift -= 8) {
+      for (int i = lane; i < 256; i += 32) hist[i] = 0;
+      __syncwarp();
+      for (int64_t h = hb; h < he; ++h) {
+        const int64_t r0 = win_off[h], n = n_hits(h);
+        for (int64_t j = lane; j < n; j += 32) {
+          const uint64_t v = rc[r0 + j];
+          const uint64_t k = sel_key((int)min(v >> 32, (uint64_t)INT32_MAX), (int64_t)(uint32_t)v, (int)(h - hb));
+          if ((k & pmask) == prefix) atomicAdd(&hist[(k >> shift) & 255], 1u);
+        }
+      }
+      __syncwarp();
+      prefix |= (uint64_t)radix_digit(hist, need, lane) << shift;
+      pmask |= 255ull << shift;
+      __syncwarp();
+    }
+    for (int64_t h = hb; h < he; ++h) {
+      const int64_t r0 = win_off[h], n = n_hits(h);
+      for (int64_t j0 = 0; j0 < n; j0 += 32) {
+        const int64_t j = j0 + lane;
+        bool take = false;
+        if (j < n) {
+          const uint64_t v = rc[r0 + j];
+          take = sel_key((int)min(v >> 32, (uint64_t)INT32_MAX), (int64_t)(uint32_t)v, (int)(h - hb)) >= prefix;
+        }
+        take_hit(take, r0 + j, (int)(h - hb));
+      }
+    }
+  }
+  __syncwarp();
+  // sort by (row, hypothesis); the low 16 bits carry the list index
+  int n_pow2 = 1;
+  while (n_pow2 < n_sel) n_pow2 <<= 1;
+  for (int i = lane; i < n_pow2; i += 32)
+    key[i] = i < n_sel ? (((uint64_t)row[i] << 34) | ((uint64_t)hl[i] << 16) | (uint64_t)i) : ~0ull;
+  __syncwarp();
+  warp_bitonic_u64(key, n_pow2, lane);
+  int n_out = 0;
+  const int64_t slot = (int64_t)s * cap;
+  for (int i0 = 0; i0 < n_sel; i0 += 32) {
+    const int i = i0 + lane;
+    bool head = false;
+    int64_t r = 0;
+    if (i < n_sel) {
+      r = (int64_t)(key[i] >> 34);
+      head = i == 0 || (int64_t)(key[i - 1] >> 34) != r;
+    }
+    const unsigned m = __ballot_sync(VK_FULL, head);
+    if (head) {
+      const int idx = (int)(key[i] & 0xffff);
+      int best = cnt[idx];
+      for (int k = i + 1; k < n_sel && (int64_t)(key[k] >> 34) == r; ++k) best = max(best, cnt[key[k] & 0xffff]);
+      const int pos = n_out + __popc(m & lt_mask);
+      c_hyp[slot + pos] = hb + (int)((key[i] >> 16) & 0x3ffff);
+      c_row[slot + pos] = r;
+      c_cnt[slot + pos] = best;
+      if (c_isum) c_isum[slot + pos] = isum[idx];
+    }
+    n_out += __popc(m);
+  }
+  if (lane == 0) n_cand[s] = n_out;
+}
+
 // One warp per spectrum: its n_cand[s] (<= cap) slots to [cand_off[s], ...).  A thread per slot of n_spec x cap
 // would launch mostly idle threads (cap is a bound; a few slots per spectrum are filled after the pruner).
 constexpr int CP_WARPS = 8;
@@ -275,7 +427,7 @@ constexpr int CP_WARPS = 8;
 __global__ void __launch_bounds__(CP_WARPS * 32)
 compact_k(int n_spec, int cap, const int64_t* n_cand, const int64_t* cand_off, const int64_t* s_hyp,
           const int64_t* s_row, const int64_t* s_cnt, const int8_t* h_maxfz, int64_t* c_hyp, int64_t* c_row,
-          int64_t* c_cnt, int32_t* c_row32, int8_t* c_maxfz) {
+          int64_t* c_cnt, int32_t* c_row32, int8_t* c_maxfz, const uint32_t* s_isum, uint32_t* c_isum) {
   const int s = blockIdx.x * CP_WARPS + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (s >= n_spec) return;
   const int64_t m = min(n_cand[s], (int64_t)cap), dst0 = cand_off[s], src0 = (int64_t)s * cap;
@@ -287,6 +439,7 @@ compact_k(int n_spec, int cap, const int64_t* n_cand, const int64_t* cand_off, c
     c_cnt[dst] = s_cnt[src];
     c_row32[dst] = (int32_t)s_row[src];
     c_maxfz[dst] = h_maxfz[h];
+    if (c_isum) c_isum[dst] = s_isum[src];
   }
 }
 
@@ -323,7 +476,41 @@ int vk_compact_cands(int n_spec, int cap, const int64_t* n_cand, const int64_t* 
                      int64_t* c_row, int64_t* c_cnt, int32_t* c_row32, int8_t* c_maxfz, void* stream) {
   if (n_spec == 0) return 0;
   compact_k<<<(unsigned)((n_spec + CP_WARPS - 1) / CP_WARPS), CP_WARPS * 32, 0, (cudaStream_t)stream>>>(
-      n_spec, cap, n_cand, cand_off, s_hyp, s_row, s_cnt, h_maxfz, c_hyp, c_row, c_cnt, c_row32, c_maxfz);
+      n_spec, cap, n_cand, cand_off, s_hyp, s_row, s_cnt, h_maxfz, c_hyp, c_row, c_cnt, c_row32, c_maxfz, nullptr,
+      nullptr);
+  return vk_launch_status();
+}
+
+int vk_compact_hits(int n_spec, int cap, const int64_t* n_cand, const int64_t* cand_off, const int64_t* s_hyp,
+                    const int64_t* s_row, const int64_t* s_cnt, const uint32_t* s_isum, const int8_t* h_maxfz,
+                    int64_t* c_hyp, int64_t* c_row, int64_t* c_cnt, int32_t* c_row32, int8_t* c_maxfz,
+                    uint32_t* c_isum, void* stream) {
+  if (n_spec == 0) return 0;
+  if ((s_isum != nullptr) != (c_isum != nullptr)) return VK_E_ARG;
+  compact_k<<<(unsigned)((n_spec + CP_WARPS - 1) / CP_WARPS), CP_WARPS * 32, 0, (cudaStream_t)stream>>>(
+      n_spec, cap, n_cand, cand_off, s_hyp, s_row, s_cnt, h_maxfz, c_hyp, c_row, c_cnt, c_row32, c_maxfz, s_isum,
+      c_isum);
+  return vk_launch_status();
+}
+
+int vk_select_hits(int n_spec, const int64_t* spec_hyp_off, const int64_t* win_off, const uint32_t* hyp_hits,
+                   const uint64_t* hit_rc, const uint32_t* hit_isum, const uint32_t* hyp_scored,
+                   const uint64_t* hyp_matched, int topk, int cap, int64_t* c_hyp, int64_t* c_row, int64_t* c_cnt,
+                   uint32_t* c_isum, int64_t* n_cand, int64_t* spec_scored, int64_t* spec_matched, void* stream) {
+  if (n_spec == 0) return 0;
+  if (topk < 1 || topk > 8192 || cap < topk) return VK_E_ARG;
+  if (!c_isum != !hit_isum) return VK_E_ARG;
+  int list_pow2 = 32;
+  while (list_pow2 < topk) list_pow2 <<= 1;
+  const int key_cap = list_pow2 > 512 ? list_pow2 : 512;
+  const size_t per_warp = (size_t)key_cap * 12 + (size_t)list_pow2 * 16 + 1024;
+  const size_t sh = per_warp * TK_WARPS;
+  if (sh > 220 * 1024) return VK_E_ARG;
+  cudaError_t e = cudaFuncSetAttribute(select_hits_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  if (e != cudaSuccess) return vk_err(e);
+  select_hits_k<<<(unsigned)((n_spec + TK_WARPS - 1) / TK_WARPS), TK_WARPS * 32, sh, (cudaStream_t)stream>>>(
+      n_spec, spec_hyp_off, win_off, hyp_hits, hit_rc, hit_isum, hyp_scored, hyp_matched, topk, cap, list_pow2,
+      key_cap, c_hyp, c_row, c_cnt, c_isum, n_cand, spec_scored, spec_matched);
   return vk_launch_status();
 }
 

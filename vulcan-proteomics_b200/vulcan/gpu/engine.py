@@ -426,6 +426,28 @@ def _k1_dense(gi: GpuIndex, dh, peaks, p: SearchParams, n_hyp: int, stats: Stats
     more entries than the win_off[-1] window rows, and ``status`` gets VK_STATUS_OVERFLOW should a bound not hold."""
     L = K.lib()
     dev = gi.dev
+    pl = _k1_plan(gi, dh, p, n_hyp)
+    cnt = torch.empty(pl["cnt_cap"], dtype=torch.int32, device=dev)
+    isw = torch.empty(pl["cnt_cap"], dtype=torch.int32, device=dev) if isum else None
+    keys, filt, n_kz, kstride = peak_keys(gi, peaks, p)
+    K.check(L.vk_k1_tiles(C.byref(gi.tix), C.byref(gi.fp), float(p.fragment_ppm[0]), float(p.fragment_ppm[1]),
+                          p.k1_warps, K.ptr(pl["item_off"]), K.ptr(pl["item_hyp"]), n_hyp, pl["item_cap"],
+                          K.ptr(dh["spec"]), K.ptr(dh["maxfz"]), K.ptr(dh["lo"]), K.ptr(dh["hi"]),
+                          K.ptr(pl["win_off"]), pl["cnt_cap"], K.ptr(peaks["off"]), K.ptr(peaks["mass"]), K.ptr(cnt),
+                          K.ptr(pl["status"]), K.ptr(peaks["int"]) if isum else None,
+                          K.ptr(peaks["tic"]) if isum else None, K.ptr(isw) if isum else None, K.ptr(keys),
+                          K.ptr(filt), n_kz, kstride, K.stream()), "k1_tiles")
+    if isum:
+        return pl["win_off"], cnt, pl["status"], isw
+    return pl["win_off"], cnt, pl["status"]
+
+
+def _k1_plan(gi: GpuIndex, dh, p: SearchParams, n_hyp: int) -> dict:
+    """The (tile, hypothesis) work items of K1 grouped by tile, and the window offsets, in buffers sized by the
+    index's window bound (nothing read back).  ``status`` (device i32) is zeroed here and collects the pass's
+    overflow / timeout bits."""
+    L = K.lib()
+    dev = gi.dev
     ix = gi.tix
     nt = ix.n_tiles
     max_win = gi.window_bound(*p.precursor_ppm)
@@ -443,19 +465,75 @@ def _k1_dense(gi: GpuIndex, dh, peaks, p: SearchParams, n_hyp: int, stats: Stats
     item_hyp = torch.empty(item_cap, dtype=torch.int32, device=dev)
     K.check(L.vk_k1_plan_fill(C.byref(ix), n_hyp, K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(item_off),
                               K.ptr(cursor), K.ptr(item_hyp), item_cap, K.ptr(status), K.stream()), "k1_plan_fill")
-    cnt = torch.empty(cnt_cap, dtype=torch.int32, device=dev)
-    isw = torch.empty(cnt_cap, dtype=torch.int32, device=dev) if isum else None
+    return {"item_off": item_off, "item_hyp": item_hyp, "item_cap": item_cap, "win_off": win_off,
+            "cnt_cap": cnt_cap, "status": status}
+
+
+def _k1_hits(gi: GpuIndex, dh, peaks, p: SearchParams, n_hyp: int, thr: int, isum: bool = True):
+    """K1 in hit-list form (``vk_k1_hits``): per hypothesis the rows with count >= thr (count << 32 | row, and the
+    summed matched intensity) in its window's region, their number, and the per-hypothesis scored / matched
+    totals.  No dense per-row output."""
+    L = K.lib()
+    dev = gi.dev
+    pl = _k1_plan(gi, dh, p, n_hyp)
+    cap = pl["cnt_cap"]
+    rc = torch.empty(cap, dtype=torch.int64, device=dev)
+    hisum = torch.empty(cap, dtype=torch.int32, device=dev) if isum else None
+    # hyp_hits (u32), hyp_scored (u32), hyp_matched (u64): one zeroed allocation
+    nh = max(n_hyp, 1)
+    z = torch.zeros(nh * 2, dtype=torch.int64, device=dev)
+    counters = z[:nh].view(torch.int32)
+    hyp_hits, hyp_scored = counters[:nh], counters[nh:]
+    hyp_matched = z[nh:]
     keys, filt, n_kz, kstride = peak_keys(gi, peaks, p)
-    K.check(L.vk_k1_tiles(C.byref(ix), C.byref(gi.fp), float(p.fragment_ppm[0]), float(p.fragment_ppm[1]),
-                          p.k1_warps, K.ptr(item_off), K.ptr(item_hyp), n_hyp, item_cap, K.ptr(dh["spec"]),
-                          K.ptr(dh["maxfz"]), K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(win_off), cnt_cap,
-                          K.ptr(peaks["off"]), K.ptr(peaks["mass"]), K.ptr(cnt), K.ptr(status),
-                          K.ptr(peaks["int"]) if isum else None, K.ptr(peaks["tic"]) if isum else None,
-                          K.ptr(isw) if isum else None, K.ptr(keys), K.ptr(filt), n_kz, kstride, K.stream()),
-            "k1_tiles")
-    if isum:
-        return win_off, cnt, status, isw
-    return win_off, cnt, status
+    K.check(L.vk_k1_hits(C.byref(gi.tix), C.byref(gi.fp), float(p.fragment_ppm[0]), float(p.fragment_ppm[1]),
+                         p.k1_warps, K.ptr(pl["item_off"]), K.ptr(pl["item_hyp"]), n_hyp, pl["item_cap"],
+                         K.ptr(dh["spec"]), K.ptr(dh["maxfz"]), K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(pl["win_off"]),
+                         cap, K.ptr(peaks["off"]), K.ptr(peaks["mass"]), int(thr), K.ptr(rc),
+                         K.ptr(hisum) if isum else None, K.ptr(hyp_hits), K.ptr(hyp_scored), K.ptr(hyp_matched),
+                         K.ptr(pl["status"]), K.ptr(peaks["int"]) if isum else None,
+                         K.ptr(peaks["tic"]) if isum else None, K.ptr(keys), K.ptr(filt), n_kz, kstride,
+                         K.stream()), "k1_hits")
+    return {"win_off": pl["win_off"], "status": pl["status"], "rc": rc, "isum": hisum, "hyp_hits": hyp_hits,
+            "hyp_scored": hyp_scored, "hyp_matched": hyp_matched}
+
+
+def _shortlist_hits(gi: GpuIndex, p: SearchParams, n: int, dh, k1h: dict, topk: int):
+    """Top-k of every spectrum by K1 count among its hit lists (``vk_select_hits``), compacted to spectrum-ordered
+    candidate lists with their intensity sums (``c_isum``); the same candidates as ``_shortlist`` without pair
+    closure over the dense counts.  Returns the candidate dict and the per-hypothesis / per-spectrum K1 sums."""
+    L = K.lib()
+    dev = gi.dev
+    cap = topk
+    s_hyp = torch.empty(max(n * cap, 1), dtype=torch.int64, device=dev)
+    s_row = torch.empty_like(s_hyp)
+    s_cnt = torch.empty_like(s_hyp)
+    isum = k1h["isum"] is not None
+    s_isum = torch.empty(max(n * cap, 1), dtype=torch.int32, device=dev) if isum else None
+    n_cand = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
+    spec_scored = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
+    spec_matched = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
+    K.check(L.vk_select_hits(n, K.ptr(dh["spec_off"]), K.ptr(k1h["win_off"]), K.ptr(k1h["hyp_hits"]),
+                             K.ptr(k1h["rc"]), K.ptr(k1h["isum"]) if isum else None, K.ptr(k1h["hyp_scored"]),
+                             K.ptr(k1h["hyp_matched"]), topk, cap, K.ptr(s_hyp), K.ptr(s_row), K.ptr(s_cnt),
+                             K.ptr(s_isum) if isum else None, K.ptr(n_cand), K.ptr(spec_scored),
+                             K.ptr(spec_matched), K.stream()), "select_hits")
+    cand_off = _scan(n_cand[:n])
+    c_hyp = torch.empty_like(s_hyp)
+    c_row = torch.empty_like(s_hyp)
+    c_cnt = torch.empty_like(s_hyp)
+    c_row32 = torch.empty(max(n * cap, 1), dtype=torch.int32, device=dev)
+    c_maxfz = torch.empty(max(n * cap, 1), dtype=torch.int8, device=dev)
+    c_isum = torch.empty(max(n * cap, 1), dtype=torch.int32, device=dev) if isum else None
+    K.check(L.vk_compact_hits(n, cap, K.ptr(n_cand), K.ptr(cand_off), K.ptr(s_hyp), K.ptr(s_row), K.ptr(s_cnt),
+                              K.ptr(s_isum) if isum else None, K.ptr(dh["maxfz"]), K.ptr(c_hyp), K.ptr(c_row),
+                              K.ptr(c_cnt), K.ptr(c_row32), K.ptr(c_maxfz), K.ptr(c_isum) if isum else None,
+                              K.stream()), "compact_hits")
+    cand = {"cand_off": cand_off, "c_hyp": c_hyp, "c_row": c_row, "c_cnt": c_cnt, "c_row32": c_row32,
+            "c_maxfz": c_maxfz, "cap": cap, "n_cand": n_cand, "c_isum": c_isum}
+    sums = {"hyp_scored": k1h["hyp_scored"], "hyp_matched": k1h["hyp_matched"], "spec_scored": spec_scored,
+            "spec_matched": spec_matched}
+    return cand, sums
 
 
 def check_status(status: torch.Tensor, what: str = "search"):
@@ -1344,6 +1422,15 @@ class Searcher:
                 k += 1
             out.append((_table(h[0], rec), st))
         return out
+
+
+    def search_sharded(self, runs, gather: bool = False):
+        """Runs spread over the GPUs of the process group (one process per GPU, each with its own ``Searcher`` on
+        its index replica): this rank searches its shard (``replicas.shard_runs``, whole runs balanced by size)
+        with ``search_many``.  Returns [(run index, table, stats)] of this rank's runs, or every run's on every rank
+        with ``gather``.  No collective touches the search itself."""
+        from . import replicas
+        return replicas.search_runs(list(runs), self.search_many, gather=gather)
 
 
 def split_table(rec: dict, runs, starts) -> list:

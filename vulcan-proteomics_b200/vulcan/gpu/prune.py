@@ -102,10 +102,14 @@ class Pruner:
 
     # ------------------------------------------------------------------ features and inference
     def features(self, gi: E.GpuIndex, dh, win_off, isum, cand, n_hits: int, n_dev=None, raw: bool = False):
-        """Standardised BF16 features [n_hits, 16] of the compacted hits ``cand`` (raw values when ``raw``)."""
+        """Standardised BF16 features [n_hits, 16] of the compacted hits ``cand`` (raw values when ``raw``).  The
+        intensity sums come from ``cand["c_isum"]`` (hit-list shortlist) when present, else from the dense K1 sums
+        ``isum`` at ``win_off``."""
         mu = torch.zeros(N_IN, device=self.dev) if raw else self.mu
         sd = torch.ones(N_IN, device=self.dev) if raw else self.sd
         feat = torch.empty(max(n_hits, 1), N_IN, dtype=torch.bfloat16, device=self.dev)
+        if cand.get("c_isum") is not None:
+            win_off, isum = None, cand["c_isum"]
         K.check(K.lib().vk_cand_features(n_hits, K.ptr(n_dev) if n_dev is not None else None,
                                          K.ptr(cand["c_hyp"]), K.ptr(cand["c_row"]), K.ptr(cand["c_cnt"]),
                                          K.ptr(win_off), K.ptr(dh["lo"]), K.ptr(isum), K.ptr(dh["M"]),
@@ -246,11 +250,15 @@ class CountRanker(Pruner):
 
 
 # ---------------------------------------------------------------------------------------------- search
-def _front(run: E.DeviceRun, gi: E.GpuIndex, p: SearchParams, st: E.Stats, timers: bool, min_count: int = 1):
+def _front(run: E.DeviceRun, gi: E.GpuIndex, p: SearchParams, st: E.Stats, timers: bool, min_count: int = 1,
+           dense: bool = False):
     """K0, hypotheses, K1 with intensity sums, and the top-k shortlist (hits with count >= min_count) without pair
-    closure."""
+    closure.  K1 writes hit lists (``vk_k1_hits``: only the rows with count >= the floor) and the shortlist reads
+    them; ``dense``: K1's dense per-row counts and sums and the shortlist over those instead (same shortlist; the
+    dense arrays are returned as "cnt" / "isum")."""
     dev = gi.dev
     n = run.n
+    thr = max(p.k1_threshold, min_count)
 
     def phase(name):
         return E.Timer(st, name) if timers else E._NoTimer()
@@ -258,11 +266,18 @@ def _front(run: E.DeviceRun, gi: E.GpuIndex, p: SearchParams, st: E.Stats, timer
         peaks = E._k0_device(run, p, dev)
     with phase("hyp"):
         dh = E._hyp_device(run, peaks, gi, p)
+    if dense:
+        with phase("k1"):
+            win_off, cnt, status, isum = E._k1_dense(gi, dh, peaks, p, dh["n_max"], st, isum=True)
+        with phase("topk"):
+            hits, sums = E._shortlist(gi, p, n, dh, win_off, cnt, p.topk, False, thr)
+        return {"peaks": peaks, "dh": dh, "win_off": win_off, "cnt": cnt, "status": status, "isum": isum,
+                "hits": hits, **sums}
     with phase("k1"):
-        win_off, cnt, status, isum = E._k1_dense(gi, dh, peaks, p, dh["n_max"], st, isum=True)
+        k1h = E._k1_hits(gi, dh, peaks, p, dh["n_max"], thr, isum=True)
     with phase("topk"):
-        hits, sums = E._shortlist(gi, p, n, dh, win_off, cnt, p.topk, False, max(p.k1_threshold, min_count))
-    return {"peaks": peaks, "dh": dh, "win_off": win_off, "cnt": cnt, "status": status, "isum": isum,
+        hits, sums = E._shortlist_hits(gi, p, n, dh, k1h, p.topk)
+    return {"peaks": peaks, "dh": dh, "win_off": k1h["win_off"], "status": k1h["status"], "k1_hits": k1h,
             "hits": hits, **sums}
 
 
@@ -281,7 +296,7 @@ def _pruned_device(run: E.DeviceRun, gi: E.GpuIndex, p: SearchParams, pr: Pruner
     def phase(name):
         return E.Timer(st, name) if timers else E._NoTimer()
     with phase("prune"):
-        feat = pr.features(gi, f["dh"], f["win_off"], f["isum"], hits, n_bound, n_dev=n_dev)
+        feat = pr.features(gi, f["dh"], f["win_off"], f.get("isum"), hits, n_bound, n_dev=n_dev)
         logit = pr.score(feat, hits, n_bound, n_dev=n_dev, status=f["status"])
         cap = (2 if p.pair_closure else 1) * pr.max_keep
         s_hyp = torch.empty(max(n * cap, 1), dtype=torch.int64, device=dev)
@@ -373,9 +388,9 @@ def collect(sp: Spectra, gi: E.GpuIndex, p: SearchParams, pr: Pruner, raw: bool 
         hits = f["hits"]
         n_hits = int(hits["cand_off"][-1])
         d = {"n": n, "hits": {k: (v[:n_hits].clone() if k.startswith("c_") else v) for k, v in hits.items()}}
-        d["feat"] = pr.features(gi, f["dh"], f["win_off"], f["isum"], hits, n_hits)[:n_hits]
+        d["feat"] = pr.features(gi, f["dh"], f["win_off"], f.get("isum"), hits, n_hits)[:n_hits]
         if raw:
-            d["raw"] = pr.features(gi, f["dh"], f["win_off"], f["isum"], hits, n_hits, raw=True)[:n_hits]
+            d["raw"] = pr.features(gi, f["dh"], f["win_off"], f.get("isum"), hits, n_hits, raw=True)[:n_hits]
         if labels:
             top = exhaustive_top(gi, p, f["peaks"], f["dh"], f["win_off"], n)
             d["y"] = hit_labels(gi, hits, top, n)
