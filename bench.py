@@ -148,16 +148,12 @@ class ClockSampler:
 
 
 def cpu_oracle_pass(l1, sp_sub, p, var=None):
-    """The oracle's search of a run (K0, hypotheses, K1, top-K + closure, K2, ranking) on the host cores."""
+    """The oracle's search of a run (K0, hypotheses, K1, top-K + closure, K2, ranking) on the host cores; returns
+    every intermediate (``oracle.parity.oracle_plain``), so that the device pass can be checked against it."""
     from oracle import oracle as O
+    from oracle import parity
     P = O.make_params(STATIC, VAR if var is None else var, p.fragment_unit)
-    pk = O.k0_view(sp_sub, p)
-    hyp = O.make_hypotheses(sp_sub, pk["valid"], l1.mass32, p)
-    win_off, cnt, sc, mt = O.k1_windows(l1, hyp, pk, p, P, arrays=_ARR.get(id(l1)))
-    oh, orr, oc = O.k1_appended(hyp, win_off, cnt, p.k1_threshold)
-    h, r, c = O.select_topk(oh, orr, oc, hyp["spec"], l1.partner, p.topk, p.pair_closure)
-    k2 = O.k2(l1, hyp, pk, h, r, p, P)
-    return O.psm_rank(k2, r, p.min_matched_peaks, p.report_psms)
+    return parity.oracle_plain(l1, sp_sub, p, P, arrays=_ARR.get(id(l1)), f64=False)
 
 
 _ARR = {}
@@ -182,26 +178,45 @@ def cpu_rate(l1, sp, p, budget_s: float, var=None):
     t = time.perf_counter() - t0
     n2 = int(min(len(sp), max(n, n * budget_s / max(t, 1e-3))))
     t0 = time.perf_counter()
-    cpu_oracle_pass(l1, _subset(sp, n2), p, var)
+    ref = cpu_oracle_pass(l1, _subset(sp, n2), p, var)
     t2 = time.perf_counter() - t0
-    return n2 / t2, n2, t2, O.n_threads()
+    return n2 / t2, n2, t2, O.n_threads(), ref
 
 
-def k1_algorithmic_bytes(gi, dh, peaks, win_off, item_off, item_hyp):
-    """Bytes K1 must move per launch: each tile with work is read once (postings, coarse-bin CSR and presence
-    bitmap); per work item the spectrum's peak filter words (one u32 per peak and fragment charge, from
-    vk_k1_peak_keys) and the hypothesis record (spec 4, maxfz 1, lo/hi 16, peak offsets 16, item id 4); per window
-    row one 4-byte count written.  The window keys read for the few windows that pass the bitmap are not counted."""
+def parity_check(l1, sp, p, var, out, n, ref):
+    """The timed plain device pass ``out`` against the oracle on the first n spectra of the run (the CPU baseline's
+    own sample and results): K0, hypotheses, K1 counts and statistics, top-K lists, K2, top-1 PSMs bit for bit, and
+    the largest hyperscore error against the FP64 oracle (computed here, untimed)."""
+    from oracle import oracle as O
+    from oracle import parity
+    P = O.make_params(STATIC, VAR if var is None else var, p.fragment_unit)
+    ref["k2_f64"] = O.k2_f64(l1, ref["hyp"], ref["pk"], ref["h"], ref["r"], p, P)
+    res = parity.check_plain(l1, sp, p, P, out, n, ref=ref)
+    res["hs_rtol_fp64"] = 1e-5
+    res["all_equal"] = bool(all(res[k] for k in ("k0_equal", "hyp_equal", "k1_equal", "topk_equal", "k2_equal",
+                                                 "top1_equal")) and res["hs_max_rel_err_fp64"] <= 1e-5)
+    return res
+
+
+def k1_algorithmic_bytes(gi, dh, peaks, item_off, n_hyp: int, intensities: bool, out_bytes: int):
+    """Bytes K1 must move per launch, each piece counted once: every tile with work (postings 4 B each, coarse-bin
+    CSR 2 B per bin, presence bitmap 8 B per bin); every hypothesis's spectrum peaks as K1 reads them (one 4-byte
+    filter word per kept peak and fragment charge, from vk_k1_peak_keys, plus the 4-byte intensity per kept peak
+    with the pruner's sums) and its record (spec 4, maxfz 1, lo/hi 16, peak offsets 16); plus ``out_bytes`` written
+    (dense counts / sums per window row, or the hit lists and per-hypothesis totals).  The kernel reads a spectrum's
+    filter words once per (tile, hypothesis) item; the re-reads beyond the first are not algorithmic (they mostly hit
+    L2), nor are the window keys of the windows that pass the bitmap."""
     nt = gi.tix.n_tiles
     nb = 1 << gi.tix.cbin_bits
     stride = (nb + 1 + 7) & ~7
     busy = (item_off[1:] - item_off[:-1]) > 0
-    tile_bytes = ((gi.tile_off[1:nt + 1] - gi.tile_off[:nt]) * 4 + stride * 2 + nb * 16)[busy].sum()
-    it = item_hyp.long()
-    s = dh["spec"][it].long()
-    nz = (dh["maxfz"][it].long() - 1).clamp(min=0)
-    item_bytes = ((peaks["off"][s + 1] - peaks["off"][s]) * 4 * nz + 41).sum()
-    return int((tile_bytes + item_bytes + win_off[-1] * 4).item())
+    tile_bytes = ((gi.tile_off[1:nt + 1] - gi.tile_off[:nt]) * 4 + stride * 2 + nb * 8)[busy].sum()
+    s = dh["spec"][:n_hyp].long()
+    nz = (dh["maxfz"][:n_hyp].long() - 1).clamp(min=0)
+    npk = peaks["off"][s + 1] - peaks["off"][s]
+    live = dh["hi"][:n_hyp] > dh["lo"][:n_hyp]
+    hyp_bytes = ((npk * (4 * nz + (4 if intensities else 0)) + 37) * live).sum()
+    return int((tile_bytes + hyp_bytes).item()) + int(out_bytes)
 
 
 def fused_algorithmic_bytes(gi, dh, peaks, oc, n_spec):
@@ -331,6 +346,14 @@ def run_b200(a):
     run = E.DeviceRun(sp, dev)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device=dev)   # 256 MiB > 126 MB L2
     st = E.Stats()
+    # the CPU baseline (rank 0 of a 1-GPU run): the oracle timed on a sample of the run; its results are kept as the
+    # checker of the timed plain device pass below
+    cpu, cpu_ref, n_cpu = None, None, 0
+    if rank == 0 and world == 1:
+        rate, n_cpu, t_s, cores, cpu_ref = cpu_rate(l1, sp, p, a.cpu_budget, w.var_mods)
+        cpu = {"value": round(rate, 1), "unit": "spectra/s", "cores": cores, "kind": "port",
+               "sample": f"first {n_cpu} spectra of the run through the oracle's plain path K0->hypotheses->K1->"
+                         f"top-k->K2->ranking ({t_s:.1f} s)"}
 
     def step_plain():
         if p.search_method == "fused":
@@ -371,6 +394,9 @@ def run_b200(a):
         st_ok = int(out["status"][:len(sp)].max())
         if st_ok:
             raise RuntimeError(f"fused search status {st_ok}: spectra over the window capacity or a copy timeout")
+    parity = None
+    if cpu_ref is not None and not pruned and use_graph:   # the timed plain pass itself, against the oracle
+        parity = parity_check(l1, sp, p, w.var_mods, out, n_cpu, cpu_ref)
 
     # end to end through the public API: Searcher (graph-captured passes) over runs in pinned host memory, or
     # engine.search for the fused method
@@ -395,7 +421,11 @@ def run_b200(a):
     comparison = None
     if pruned:
         # the plain exhaustive path on the same run, same timing rules, and the pruned path's accuracy against it
-        ms_plain, _, _ = device_timing(step_plain, True)
+        ms_plain, _, out_plain = device_timing(step_plain, True)
+        E.check_status(out_plain["status"])
+        if cpu_ref is not None:   # the timed plain pass itself, against the oracle
+            parity = parity_check(l1, sp, p, w.var_mods, out_plain, n_cpu, cpu_ref)
+        del out_plain
         e2e_plain, _ = e2e_rate(None)
         ev = PR.evaluate(sp, gi, l1, lab, p, pr)
         comparison = {"plain_value": round(len(sp) * world * a.steps / (ms_plain / 1e3), 1),
@@ -426,17 +456,13 @@ def run_b200(a):
     dom = max(kern, key=lambda k: kern[k][0])
     k_mean, algo = kern[dom]
     achieved = algo / (k_mean / 1e3) / 1e9
-    traffic = _traffic_from_profiles(dom[:-2] if dom.endswith("_k") else dom)
+    # DRAM bytes per launch from the committed ncu summary of the same kernel form (profiles/<name>_*.md)
+    traffic = _traffic_from_profiles({"k1_tiles_k (hit lists)": "k1_tiles_hits", "k1_tiles_k": "k1_tiles_dense"}.get(
+        dom, dom[:-2] if dom.endswith("_k") else dom))
     kernels = {k: {"mean_launch_ms": round(v[0], 4), "algorithmic_bytes": v[1],
                    "algorithmic_gbs": round(v[1] / (v[0] / 1e3) / 1e9, 1)} for k, v in kern.items()}
 
     if rank == 0:
-        cpu = None
-        if world == 1:
-            rate, n_s, t_s, cores = cpu_rate(l1, sp, p, a.cpu_budget, w.var_mods)
-            cpu = {"value": round(rate, 1), "unit": "spectra/s", "cores": cores, "kind": "port",
-                   "sample": f"first {n_s} spectra of the run through the oracle's plain path K0->hypotheses->K1->"
-                             f"top-k->K2->ranking ({t_s:.1f} s)"}
         extra = {"spectra_per_step_per_gpu": len(sp), "index_rows": len(l1), "index_postings": gi.n_postings,
                  "tile_rows": p.tile_rows, "parallelism": f"replicas x{world} (one run per GPU)",
                  "launch": "one CUDA graph per pass (eager_ms_per_step: the same pass launched kernel by kernel)"
@@ -462,7 +488,9 @@ def run_b200(a):
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1),
                          "peak": peak_gbs, "unit": "GB/s", "frac": round(achieved / peak_gbs, 4),
                          "peak_source": peak_kind, "traffic": traffic, "algorithmic_bytes": algo,
-                         "mean_launch_ms": round(k_mean, 4)},
+                         "mean_launch_ms": round(k_mean, 4),
+                         # the same launch time against the DRAM bytes ncu measured per launch
+                         "dram_frac": round(traffic / (k_mean / 1e3) / 1e9 / peak_gbs, 4) if traffic else None},
             "kernels": kernels,
             "cpu_baseline": cpu,
             "clocks": clk,
@@ -473,6 +501,8 @@ def run_b200(a):
             line["mlp_roofline"] = mlp
         if comparison:
             line["vs_plain"] = comparison
+        if parity is not None:
+            line["parity"] = parity
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
@@ -514,60 +544,79 @@ def _kernel_table(a, p, gi, run, flush, pr, dev):
             torch.cuda.synchronize()
             ts.append(e0.elapsed_time(e1))
         return sum(ts[2:]) / len(ts[2:])
-    nt = gi.tix.n_tiles
-    tile_items = torch.empty(nt, dtype=torch.int64, device=dev)
-    win_len = torch.empty(dh["n_max"], dtype=torch.int64, device=dev)
-    K.check(L.vk_k1_plan_count(C.byref(gi.tix), dh["n_max"], K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(tile_items),
-                               K.ptr(win_len), K.stream()), "k1_plan_count")
-    item_off = E._scan(tile_items)
-    n_items = int(item_off[-1])
-    cursor = torch.empty(nt, dtype=torch.int64, device=dev)
-    item_hyp = torch.empty(max(n_items, 1), dtype=torch.int32, device=dev)
-    status = torch.zeros(1, dtype=torch.int32, device=dev)
-    K.check(L.vk_k1_plan_fill(C.byref(gi.tix), dh["n_max"], K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(item_off),
-                              K.ptr(cursor), K.ptr(item_hyp), item_hyp.numel(), K.ptr(status), K.stream()),
-            "k1_plan_fill")
-    win_off, cnt = so["win_off"], so["cnt"]
+    nh = int(dh["spec_off"][-1])
+    pl = E._k1_plan(gi, dh, p, dh["n_max"])
+    item_off, item_hyp = pl["item_off"], pl["item_hyp"]
+    win_off = pl["win_off"]
     n_win = int(win_off[-1])
-    isum = so.get("isum")
     kern = {}
     keys, filt, n_kz, kstride = E.peak_keys(gi, peaks, p)
     n_pk = int(peaks["off"][-1])
     ms_keys = timed(lambda: E.peak_keys(gi, peaks, p))
     kern["peak_keys_k"] = (ms_keys, n_pk * (4 + 12 * n_kz))
-    ms_k1 = timed(lambda: K.check(L.vk_k1_tiles(
-        C.byref(gi.tix), C.byref(gi.fp), float(p.fragment_ppm[0]), float(p.fragment_ppm[1]), p.k1_warps,
-        K.ptr(item_off), K.ptr(item_hyp), dh["n_max"], item_hyp.numel(), K.ptr(dh["spec"]), K.ptr(dh["maxfz"]),
-        K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(win_off), cnt.numel(), K.ptr(peaks["off"]), K.ptr(peaks["mass"]),
-        K.ptr(cnt), K.ptr(status),
-        K.ptr(peaks["int"]) if pruned else None, K.ptr(peaks["tic"]) if pruned else None,
-        K.ptr(isum) if pruned else None, K.ptr(keys), K.ptr(filt), n_kz, kstride, K.stream()), "k1_tiles"))
-    k1b = k1_algorithmic_bytes(gi, dh, peaks, win_off, item_off, item_hyp)
-    if pruned:   # peak intensities per item and the window-row intensity sums
-        s_it = dh["spec"][item_hyp.long()].long()
-        k1b += int(((peaks["off"][s_it + 1] - peaks["off"][s_it]) * 4).sum().item()) + n_win * 4
-    kern["k1_tiles_k"] = (ms_k1, k1b)
     hits = so["hits"] if pruned else so
-    thr = max(p.k1_threshold, pr.min_count) if pruned else p.k1_threshold
-    closure = 0 if pruned else int(p.pair_closure)
-    cap = hits["cap"]
-    tk = {k: torch.empty(max(n * cap, 1), dtype=torch.int64, device=dev) for k in ("h", "r", "c")}
-    tk_n = torch.empty(n, dtype=torch.int64, device=dev)
-    hs_ = torch.empty(dh["n_max"], dtype=torch.int32, device=dev)
-    hm_ = torch.empty(dh["n_max"], dtype=torch.int64, device=dev)
-    ss_ = torch.empty(n, dtype=torch.int64, device=dev)
-    sm_ = torch.empty(n, dtype=torch.int64, device=dev)
-    ms_tk = timed(lambda: K.check(L.vk_select_topk(
-        n, K.ptr(dh["spec_off"]), K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(win_off), K.ptr(cnt), cnt.numel(),
-        K.ptr(gi.partner), thr, p.topk, closure, cap, K.ptr(tk["h"]), K.ptr(tk["r"]), K.ptr(tk["c"]),
-        K.ptr(tk_n), K.ptr(hs_), K.ptr(hm_), K.ptr(ss_), K.ptr(sm_), K.stream()), "select_topk"))
     n_hit = int(hits["cand_off"][-1])
-    n_sel = int(((hits["c_cnt"][:n_hit] >= 0)).sum())
-    kern["select_topk_k"] = (ms_tk, n_win * 4 + n_sel * 8 + n_hit * 24 + dh["n_max"] * 12 + n * 16)
+    cap = hits["cap"]
+    if pruned:
+        # K1 in hit-list form (rows with count >= the floor appended per hypothesis), then the shortlist over the
+        # hit lists: the kernels of the pruned path
+        thr = max(p.k1_threshold, pr.min_count)
+        k1h = so["k1_hits"]
+        z = torch.zeros(dh["n_max"] * 2, dtype=torch.int64, device=dev)
+
+        def run_k1():
+            z.zero_()
+            K.check(L.vk_k1_hits(
+                C.byref(gi.tix), C.byref(gi.fp), float(p.fragment_ppm[0]), float(p.fragment_ppm[1]), p.k1_warps,
+                K.ptr(item_off), K.ptr(item_hyp), dh["n_max"], pl["item_cap"], K.ptr(dh["spec"]), K.ptr(dh["maxfz"]),
+                K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(win_off), pl["cnt_cap"], K.ptr(peaks["off"]),
+                K.ptr(peaks["mass"]), thr, K.ptr(k1h["rc"]), K.ptr(k1h["isum"]),
+                K.ptr(z[:dh["n_max"]].view(torch.int32)[:dh["n_max"]]),
+                K.ptr(z[:dh["n_max"]].view(torch.int32)[dh["n_max"]:]), K.ptr(z[dh["n_max"]:]), K.ptr(pl["status"]),
+                K.ptr(peaks["int"]), K.ptr(peaks["tic"]), K.ptr(keys), K.ptr(filt), n_kz, kstride, K.stream()),
+                "k1_hits")
+        ms_k1 = timed(run_k1)
+        n_k1_hits = int(k1h["hyp_hits"][:nh].long().sum())
+        kern["k1_tiles_k (hit lists)"] = (ms_k1, k1_algorithmic_bytes(gi, dh, peaks, item_off, nh, True,
+                                                                       n_k1_hits * 12 + nh * 16))
+        tk = {k: torch.empty(max(n * cap, 1), dtype=torch.int64, device=dev) for k in ("h", "r", "c")}
+        ti = torch.empty(max(n * cap, 1), dtype=torch.int32, device=dev)
+        tk_n = torch.empty(n, dtype=torch.int64, device=dev)
+        ss_ = torch.empty(n, dtype=torch.int64, device=dev)
+        sm_ = torch.empty(n, dtype=torch.int64, device=dev)
+        ms_tk = timed(lambda: K.check(L.vk_select_hits(
+            n, K.ptr(dh["spec_off"]), K.ptr(win_off), K.ptr(k1h["hyp_hits"]), K.ptr(k1h["rc"]), K.ptr(k1h["isum"]),
+            K.ptr(k1h["hyp_scored"]), K.ptr(k1h["hyp_matched"]), p.topk, cap, K.ptr(tk["h"]), K.ptr(tk["r"]),
+            K.ptr(tk["c"]), K.ptr(ti), K.ptr(tk_n), K.ptr(ss_), K.ptr(sm_), K.stream()), "select_hits"))
+        # hits read (12 B), per-hypothesis totals (16 B), per spectrum its hypothesis range and outputs; the
+        # shortlist written (28 B per kept hit)
+        kern["select_hits_k"] = (ms_tk, n_k1_hits * 12 + nh * 24 + n * 32 + n_hit * 28)
+    else:
+        cnt = so["cnt"]
+        status = torch.zeros(1, dtype=torch.int32, device=dev)
+        ms_k1 = timed(lambda: K.check(L.vk_k1_tiles(
+            C.byref(gi.tix), C.byref(gi.fp), float(p.fragment_ppm[0]), float(p.fragment_ppm[1]), p.k1_warps,
+            K.ptr(item_off), K.ptr(item_hyp), dh["n_max"], pl["item_cap"], K.ptr(dh["spec"]), K.ptr(dh["maxfz"]),
+            K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(win_off), cnt.numel(), K.ptr(peaks["off"]),
+            K.ptr(peaks["mass"]), K.ptr(cnt), K.ptr(status), None, None, None, K.ptr(keys), K.ptr(filt), n_kz,
+            kstride, K.stream()), "k1_tiles"))
+        kern["k1_tiles_k"] = (ms_k1, k1_algorithmic_bytes(gi, dh, peaks, item_off, nh, False, n_win * 4))
+        tk = {k: torch.empty(max(n * cap, 1), dtype=torch.int64, device=dev) for k in ("h", "r", "c")}
+        tk_n = torch.empty(n, dtype=torch.int64, device=dev)
+        hs_ = torch.empty(dh["n_max"], dtype=torch.int32, device=dev)
+        hm_ = torch.empty(dh["n_max"], dtype=torch.int64, device=dev)
+        ss_ = torch.empty(n, dtype=torch.int64, device=dev)
+        sm_ = torch.empty(n, dtype=torch.int64, device=dev)
+        ms_tk = timed(lambda: K.check(L.vk_select_topk(
+            n, K.ptr(dh["spec_off"]), K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(win_off), K.ptr(cnt), cnt.numel(),
+            K.ptr(gi.partner), p.k1_threshold, p.topk, int(p.pair_closure), cap, K.ptr(tk["h"]), K.ptr(tk["r"]),
+            K.ptr(tk["c"]), K.ptr(tk_n), K.ptr(hs_), K.ptr(hm_), K.ptr(ss_), K.ptr(sm_), K.stream()), "select_topk"))
+        n_sel = int(((hits["c_cnt"][:n_hit] >= 0)).sum())
+        kern["select_topk_k"] = (ms_tk, n_win * 4 + n_sel * 8 + n_hit * 24 + nh * 12 + n * 16)
     mlp = None
     if pruned:
         feat = so["feat"]
-        ms_f = timed(lambda: pr.features(gi, dh, win_off, isum, hits, n_hit))
+        ms_f = timed(lambda: pr.features(gi, dh, win_off, None, hits, n_hit))
         kern["cand_features_k"] = (ms_f, n_hit * 87)
         ms_m = timed(lambda: pr.logits(feat, n_hit))
         flops = 2 * n_hit * (16 * 256 + 256 * 256 + 256)
@@ -786,6 +835,19 @@ def run_reference(a):
     print(json.dumps(line), flush=True)
 
 
+def _launch_ranks(n: int) -> int:
+    """Run this command as n ranks on this node (torch.distributed.run, rendezvous on 127.0.0.1, a free port),
+    bounded by a timeout well above the process group's own; returns the launcher's exit status."""
+    import socket
+    with socket.socket() as sock:
+        sock.bind(("127.0.0.1", 0))
+        port = sock.getsockname()[1]
+    cmd = ["timeout", "-k", "60", "3600", sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={n}", "--master-addr", "127.0.0.1", "--master-port", str(port),
+           os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -818,6 +880,13 @@ def main():
     a = ap.parse_args()
     if a.warmup < 3:
         ap.error("--warmup must be >= 3")
+    if a.gpus < 1:
+        ap.error("--gpus must be >= 1")
+    if a.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # one process per GPU: relaunch this command under torch.distributed.run with N ranks (rank 0 prints)
+        sys.exit(_launch_ranks(a.gpus))
+    if int(os.environ.get("WORLD_SIZE", "1")) != a.gpus:
+        ap.error(f"--gpus {a.gpus} but WORLD_SIZE={os.environ.get('WORLD_SIZE')}")
     if a.impl == "reference":
         run_reference(a)
     elif a.workload in BATCH_SETUPS:
