@@ -248,8 +248,9 @@ int vk_k1_tiles(const vk_tindex* ix, const vk_frag_params* fp, float tol_lo, flo
                 const uint32_t* pk_filt, int n_kz, int64_t kstride, void* stream);
 int vk_k1_peak_keys(const vk_tindex* ix, const vk_frag_params* fp, float tol_lo, float tol_hi, const int64_t* n_peaks,
                     const float* pk_mass, int n_kz, int64_t kstride, uint32_t* keys, uint32_t* filt, void* stream);
-/* K1 in hit-list form (the learned-pruned search): the same counting as vk_k1_tiles, but instead of a dense count
- * per window row, the rows with count >= thr (>= 1) of hypothesis h are appended to its region [win_off[h],
+/* K1 in hit-list form (the learned-pruned search, the open / mass-offset modes): the same counting as vk_k1_tiles,
+ * but instead of a dense count per window row, the rows with count >= thr (>= 1; h_thr[h] instead when h_thr is
+ * given, i32 per hypothesis, a threshold < 1 appending every window row) of hypothesis h are appended to its region [win_off[h],
  * win_off[h] + hyp_hits[h]) of hit_rc (u64: count << 32 | row) and, with pk_int/tic, of hit_isum (the summed
  * matched intensity of vk_k1_tiles' isum); plus per hypothesis hyp_scored (u32, rows with count > 0) and
  * hyp_matched (u64, sum of counts).  hyp_hits, hyp_scored and hyp_matched are accumulated with atomics: the caller
@@ -260,7 +261,7 @@ int vk_k1_hits(const vk_tindex* ix, const vk_frag_params* fp, float tol_lo, floa
                const int64_t* tile_item_off, const int32_t* item_hyp, int64_t n_hyp, int64_t item_cap,
                const int32_t* h_spec, const int8_t* h_maxfz, const int64_t* h_lo, const int64_t* h_hi,
                const int64_t* win_off, int64_t cnt_cap, const int64_t* pk_off, const float* pk_mass, int thr,
-               uint64_t* hit_rc, uint32_t* hit_isum, uint32_t* hyp_hits, uint32_t* hyp_scored,
+               const int32_t* h_thr, uint64_t* hit_rc, uint32_t* hit_isum, uint32_t* hyp_hits, uint32_t* hyp_scored,
                uint64_t* hyp_matched, int32_t* status, const float* pk_int, const float* tic,
                const uint32_t* pk_keys, const uint32_t* pk_filt, int n_kz, int64_t kstride, void* stream);
 
@@ -278,16 +279,18 @@ int vk_select_topk(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo,
                    uint32_t* hyp_scored, uint64_t* hyp_matched, int64_t* spec_scored, int64_t* spec_matched,
                    void* stream);
 
-/* Top-k shortlist from the hit lists of vk_k1_hits (reference vulcan/gpu/engine.py:284-301 without the pair
- * closure): per spectrum its hypotheses' hits ranked by (count desc, row desc, hypothesis asc), the first topk kept
- * (all when fewer), sorted by row, duplicate rows merged to the lowest hypothesis and highest count; the slots of
- * vk_select_topk with pair_closure = 0 (cap >= topk) plus c_isum (u32, the kept hit's intensity sum; NULL when
- * hit_isum is NULL), and spec_scored / spec_matched (i64, may be NULL) summed from K1's per-hypothesis totals.
- * The same candidates as vk_select_topk over vk_k1_tiles' dense counts with thr = vk_k1_hits' thr. */
+/* Top-K + pair closure from the hit lists of vk_k1_hits (reference vulcan/gpu/engine.py:284-312): per spectrum
+ * its hypotheses' hits ranked by (count desc, row desc, hypothesis asc), the first topk kept (all when fewer);
+ * with pair_closure the partner rows added with count -1; sorted by row, duplicate rows merged to the lowest
+ * hypothesis and highest count: the slots of vk_select_topk (cap >= (pair_closure ? 2 : 1) * topk) plus c_isum
+ * (u32, the kept hit's intensity sum, 0 for a partner-only row; NULL when hit_isum is NULL), and spec_scored /
+ * spec_matched (i64, may be NULL) summed from K1's per-hypothesis totals.  The same candidates as vk_select_topk
+ * over vk_k1_tiles' dense counts with thr = vk_k1_hits' thr. */
 int vk_select_hits(int n_spec, const int64_t* spec_hyp_off, const int64_t* win_off, const uint32_t* hyp_hits,
                    const uint64_t* hit_rc, const uint32_t* hit_isum, const uint32_t* hyp_scored,
-                   const uint64_t* hyp_matched, int topk, int cap, int64_t* c_hyp, int64_t* c_row, int64_t* c_cnt,
-                   uint32_t* c_isum, int64_t* n_cand, int64_t* spec_scored, int64_t* spec_matched, void* stream);
+                   const uint64_t* hyp_matched, int topk, int pair_closure, const int64_t* partner, int cap,
+                   int64_t* c_hyp, int64_t* c_row, int64_t* c_cnt, uint32_t* c_isum, int64_t* n_cand,
+                   int64_t* spec_scored, int64_t* spec_matched, void* stream);
 
 /* Compaction of per-spectrum slots into a flat candidate list: with cand_off = scan(n_cand), copies slot s to
  * [cand_off[s], cand_off[s+1]) and writes c_maxfz from h_maxfz[c_hyp].  vk_compact_hits also carries the
@@ -300,9 +303,11 @@ int vk_compact_hits(int n_spec, int cap, const int64_t* n_cand, const int64_t* c
                     int64_t* c_hyp, int64_t* c_row, int64_t* c_cnt, int32_t* c_row32, int8_t* c_maxfz,
                     uint32_t* c_isum, void* stream);
 
-/* K2 exact rescoring (reference kernels.cu:263-376, closed mode), B200 launch: one warp per spectrum, lanes over
- * candidates, the spectrum's (first 512) peaks in shared memory.  Candidates of spectrum s are
- * [cand_off[s], cand_off[s+1]) (cand_off has n_spec+1 entries, spectrum ids are 0..n_spec-1). */
+/* K2 exact rescoring (reference kernels.cu:263-376), B200 launch: one warp per spectrum, lanes over candidates,
+ * the spectrum's (first 512) peaks in shared memory.  Candidates of spectrum s are [cand_off[s], cand_off[s+1])
+ * (cand_off has n_spec+1 entries, spectrum ids are 0..n_spec-1).  c_shift NULL: the closed mode; else the
+ * per-candidate precursor shift (Da, f32) of the open / mass-offset modes: shifted and unshifted ions scored as
+ * the reference's shift mode (kernels.cu:294-363). */
 int vk_k2_spectra(const vk_frag_params* fp, int n_spec, const int64_t* cand_off, const int32_t* c_row,
                   const int8_t* c_maxfz, const int64_t* pk_off, const float* pk_mass, const float* pk_int,
                   const int64_t* seq_off, const uint8_t* len, const uint64_t* mask, const float* mass32,

@@ -62,6 +62,7 @@ struct K1Rec {
 // and isum; per hypothesis the number of rows with a nonzero count and the sum of the counts.
 struct K1Hits {
   int thr;
+  const int32_t* h_thr;   // per-hypothesis thresholds (NULL: thr for all)
   uint64_t* rc;
   uint32_t* isum;
   uint32_t* hyp_hits;
@@ -181,13 +182,14 @@ k1_tiles_k(vk_tindex ix, float tol_lo, float tol_hi, int tol_da, int post_cap, c
         // rows with count >= thr appended to the hypothesis' region, one atomic per 32 rows; the statistics of
         // the item's rows added to the hypothesis' totals (integer sums: the result does not depend on order)
         const int64_t region = win_off[r.h];
+        const int thr_h = hits.h_thr ? hits.h_thr[r.h] : hits.thr;
         long long sc = 0, mt = 0;
         for (int q0 = rlo; q0 < rhi; q0 += 32) {
           const int q = q0 + lane;
           const uint32_t c = q < rhi ? hw[q] : 0u;
           sc += c > 0u;
           mt += c;
-          const bool keep = q < rhi && (int)c >= hits.thr;
+          const bool keep = q < rhi && (int)c >= thr_h;
           const unsigned bal = __ballot_sync(VK_FULL, keep);
           if (!bal) continue;
           uint32_t at0 = 0;
@@ -319,12 +321,13 @@ int vk_k1_hits(const vk_tindex* ix, const vk_frag_params* fp, float tol_lo, floa
                const int64_t* tile_item_off, const int32_t* item_hyp, int64_t n_hyp, int64_t item_cap,
                const int32_t* h_spec, const int8_t* h_maxfz, const int64_t* h_lo, const int64_t* h_hi,
                const int64_t* win_off, int64_t cnt_cap, const int64_t* pk_off, const float* pk_mass, int thr,
-               uint64_t* hit_rc, uint32_t* hit_isum, uint32_t* hyp_hits, uint32_t* hyp_scored,
+               const int32_t* h_thr, uint64_t* hit_rc, uint32_t* hit_isum, uint32_t* hyp_hits, uint32_t* hyp_scored,
                uint64_t* hyp_matched, int32_t* status, const float* pk_int, const float* tic,
                const uint32_t* pk_keys, const uint32_t* pk_filt, int n_kz, int64_t kstride, void* stream) {
-  if (!hit_rc || !hyp_hits || !hyp_scored || !hyp_matched || thr < 1) return VK_E_ARG;
+  if (!hit_rc || !hyp_hits || !hyp_scored || !hyp_matched || (!h_thr && thr < 1)) return VK_E_ARG;
   if ((hit_isum != nullptr) != (pk_int != nullptr)) return VK_E_ARG;
-  K1Hits hits{thr, hit_rc, hit_isum, hyp_hits, hyp_scored, reinterpret_cast<unsigned long long*>(hyp_matched)};
+  K1Hits hits{thr, h_thr, hit_rc, hit_isum, hyp_hits, hyp_scored,
+              reinterpret_cast<unsigned long long*>(hyp_matched)};
   return k1_tiles_launch<true>(ix, fp, tol_lo, tol_hi, warps, tile_item_off, item_hyp, n_hyp, item_cap, h_spec,
                                h_maxfz, h_lo, h_hi, win_off, cnt_cap, pk_off, pk_mass, nullptr, status, pk_int, tic,
                                hit_isum, pk_keys, pk_filt, n_kz, kstride, hits, stream);

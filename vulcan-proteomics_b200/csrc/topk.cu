@@ -278,8 +278,9 @@ select_topk_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo, cons
 __global__ void __launch_bounds__(TK_WARPS * 32)
 select_hits_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* win_off, const uint32_t* hyp_hits,
               const uint64_t* rc, const uint32_t* hit_isum, const uint32_t* hyp_scored, const uint64_t* hyp_matched,
-              int topk, int cap, int list_pow2, int key_cap, int64_t* c_hyp, int64_t* c_row, int64_t* c_cnt,
-              uint32_t* c_isum, int64_t* n_cand, int64_t* spec_scored, int64_t* spec_matched) {
+              int topk, int pair_closure, const int64_t* partner, int cap, int list_pow2, int key_cap,
+              int64_t* c_hyp, int64_t* c_row, int64_t* c_cnt, uint32_t* c_isum, int64_t* n_cand,
+              int64_t* spec_scored, int64_t* spec_matched) {
   extern __shared__ __align__(16) uint8_t tk_smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int s = blockIdx.x * TK_WARPS + warp;
@@ -387,20 +388,32 @@ select_hits_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* win_off, c
     }
   }
   __syncwarp();
+  // pair closure: the partner row of every kept hit, same hypothesis, count -1 (no intensity sum)
+  int n_list = n_sel;
+  if (pair_closure) {
+    for (int i = lane; i < n_sel; i += 32) {
+      row[n_sel + i] = (int32_t)partner[row[i]];
+      hl[n_sel + i] = hl[i];
+      cnt[n_sel + i] = -1;
+      isum[n_sel + i] = 0u;
+    }
+    n_list = 2 * n_sel;
+  }
+  __syncwarp();
   // sort by (row, hypothesis); the low 16 bits carry the list index
   int n_pow2 = 1;
-  while (n_pow2 < n_sel) n_pow2 <<= 1;
+  while (n_pow2 < n_list) n_pow2 <<= 1;
   for (int i = lane; i < n_pow2; i += 32)
-    key[i] = i < n_sel ? (((uint64_t)row[i] << 34) | ((uint64_t)hl[i] << 16) | (uint64_t)i) : ~0ull;
+    key[i] = i < n_list ? (((uint64_t)row[i] << 34) | ((uint64_t)hl[i] << 16) | (uint64_t)i) : ~0ull;
   __syncwarp();
   warp_bitonic_u64(key, n_pow2, lane);
   int n_out = 0;
   const int64_t slot = (int64_t)s * cap;
-  for (int i0 = 0; i0 < n_sel; i0 += 32) {
+  for (int i0 = 0; i0 < n_list; i0 += 32) {
     const int i = i0 + lane;
     bool head = false;
     int64_t r = 0;
-    if (i < n_sel) {
+    if (i < n_list) {
       r = (int64_t)(key[i] >> 34);
       head = i == 0 || (int64_t)(key[i - 1] >> 34) != r;
     }
@@ -408,7 +421,7 @@ select_hits_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* win_off, c
     if (head) {
       const int idx = (int)(key[i] & 0xffff);
       int best = cnt[idx];
-      for (int k = i + 1; k < n_sel && (int64_t)(key[k] >> 34) == r; ++k) best = max(best, cnt[key[k] & 0xffff]);
+      for (int k = i + 1; k < n_list && (int64_t)(key[k] >> 34) == r; ++k) best = max(best, cnt[key[k] & 0xffff]);
       const int pos = n_out + __popc(m & lt_mask);
       c_hyp[slot + pos] = hb + (int)((key[i] >> 16) & 0x3ffff);
       c_row[slot + pos] = r;
@@ -495,13 +508,14 @@ int vk_compact_hits(int n_spec, int cap, const int64_t* n_cand, const int64_t* c
 
 int vk_select_hits(int n_spec, const int64_t* spec_hyp_off, const int64_t* win_off, const uint32_t* hyp_hits,
                    const uint64_t* hit_rc, const uint32_t* hit_isum, const uint32_t* hyp_scored,
-                   const uint64_t* hyp_matched, int topk, int cap, int64_t* c_hyp, int64_t* c_row, int64_t* c_cnt,
-                   uint32_t* c_isum, int64_t* n_cand, int64_t* spec_scored, int64_t* spec_matched, void* stream) {
+                   const uint64_t* hyp_matched, int topk, int pair_closure, const int64_t* partner, int cap,
+                   int64_t* c_hyp, int64_t* c_row, int64_t* c_cnt, uint32_t* c_isum, int64_t* n_cand,
+                   int64_t* spec_scored, int64_t* spec_matched, void* stream) {
   if (n_spec == 0) return 0;
-  if (topk < 1 || topk > 8192 || cap < topk) return VK_E_ARG;
-  if (!c_isum != !hit_isum) return VK_E_ARG;
+  if (topk < 1 || topk > 8192 || cap < (pair_closure ? 2 : 1) * topk) return VK_E_ARG;
+  if (!c_isum != !hit_isum || (pair_closure && !partner)) return VK_E_ARG;
   int list_pow2 = 32;
-  while (list_pow2 < topk) list_pow2 <<= 1;
+  while (list_pow2 < (pair_closure ? 2 : 1) * topk) list_pow2 <<= 1;
   const int key_cap = list_pow2 > 512 ? list_pow2 : 512;
   const size_t per_warp = (size_t)key_cap * 12 + (size_t)list_pow2 * 16 + 1024;
   const size_t sh = per_warp * TK_WARPS;
@@ -509,8 +523,8 @@ int vk_select_hits(int n_spec, const int64_t* spec_hyp_off, const int64_t* win_o
   cudaError_t e = cudaFuncSetAttribute(select_hits_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
   if (e != cudaSuccess) return vk_err(e);
   select_hits_k<<<(unsigned)((n_spec + TK_WARPS - 1) / TK_WARPS), TK_WARPS * 32, sh, (cudaStream_t)stream>>>(
-      n_spec, spec_hyp_off, win_off, hyp_hits, hit_rc, hit_isum, hyp_scored, hyp_matched, topk, cap, list_pow2,
-      key_cap, c_hyp, c_row, c_cnt, c_isum, n_cand, spec_scored, spec_matched);
+      n_spec, spec_hyp_off, win_off, hyp_hits, hit_rc, hit_isum, hyp_scored, hyp_matched, topk, pair_closure,
+      partner, cap, list_pow2, key_cap, c_hyp, c_row, c_cnt, c_isum, n_cand, spec_scored, spec_matched);
   return vk_launch_status();
 }
 

@@ -244,6 +244,71 @@ class GpuIndex:
 
 
 # ------------------------------------------------------------------------------------------------ spectra
+_STORE_COLUMNS = ("ms_level", "scan", "index", "rt_min", "precursor_mz", "precursor_charge", "mz", "intensity")
+
+
+def load_store(path: str, pinned: bool = False) -> Spectra:
+    """The MS2 spectra of one run from its spectral store (reference engine.py:157-168): an Arrow IPC file with one
+    row per spectrum (scalar columns and list<float32> ``mz`` / ``intensity``), the run's metadata as JSON under the
+    schema's ``vulcan`` key and in a ``.json`` sidecar (reference ``vulcan/io/store.py``).  The file is
+    memory-mapped and only the columns the search reads are touched; the MS2 rows' peaks are gathered from the
+    Arrow value buffers straight into one flat array each -- in pinned host memory with ``pinned``, so that
+    ``Searcher`` copies them to the device without staging.  Unknown charges (null) become 0, a missing precursor
+    m/z NaN; the run name is the metadata's ``run_name`` (else the path)."""
+    import json
+    import os
+    reader = pa.ipc.open_file(pa.memory_map(path, "r"))
+    meta = {}
+    md = reader.schema.metadata or {}
+    if b"vulcan" in md:
+        meta.update(json.loads(md[b"vulcan"]))
+    if os.path.exists(path + ".json"):
+        with open(path + ".json") as fh:
+            meta.update(json.load(fh))
+    batches = [reader.get_batch(i).select(list(_STORE_COLUMNS)) for i in range(reader.num_record_batches)]
+    # per batch: the MS2 rows and their peak ranges in the batch's list value buffers
+    sel, plans = [], []
+    n_spec = n_peaks = 0
+    for b in batches:
+        ms2 = np.flatnonzero(b.column("ms_level").to_numpy(zero_copy_only=False) == 2)
+        mzc, itc = b.column("mz"), b.column("intensity")
+        off = mzc.offsets.to_numpy().astype(np.int64)
+        if not np.array_equal(off, itc.offsets.to_numpy()):
+            raise ValueError(f"{path}: mz and intensity lists differ in length")
+        lens = off[1:][ms2] - off[:-1][ms2]
+        sel.append(ms2)
+        plans.append((off[:-1][ms2], lens, mzc.values, itc.values))
+        n_spec += len(ms2)
+        n_peaks += int(lens.sum())
+    alloc = _pinned_like if pinned else (lambda a: np.empty_like(a))
+    mz = alloc(np.empty(n_peaks, np.float32))
+    inten = alloc(np.empty(n_peaks, np.float32))
+    offsets = alloc(np.empty(n_spec + 1, np.int64))
+    offsets[0] = 0
+    pos = spec = 0
+    for (starts, lens, mzv, itv) in plans:
+        tot = int(lens.sum())
+        np.cumsum(lens, out=offsets[spec + 1:spec + 1 + len(lens)])
+        offsets[spec + 1:spec + 1 + len(lens)] += pos
+        if tot:
+            src = np.repeat(starts - (offsets[spec:spec + len(lens)] - pos), lens) + np.arange(tot, dtype=np.int64)
+            np.take(mzv.to_numpy(zero_copy_only=False), src, out=mz[pos:pos + tot])
+            np.take(itv.to_numpy(zero_copy_only=False), src, out=inten[pos:pos + tot])
+        pos += tot
+        spec += len(lens)
+
+    def col(name, dt=None):
+        parts = [b.column(name).to_numpy(zero_copy_only=False)[m] for b, m in zip(batches, sel)]
+        v = np.concatenate(parts) if parts else np.zeros(0, dt or np.float64)
+        return v if dt is None else np.asarray(v, dt)
+    pmz = alloc(np.empty(n_spec, np.float64))
+    pmz[:] = col("precursor_mz", np.float64)
+    charge = alloc(np.empty(n_spec, np.int8))
+    charge[:] = np.nan_to_num(col("precursor_charge", np.float64), nan=0).astype(np.int8)
+    return Spectra(meta.get("run_name", path), col("scan", np.uint32), col("index", np.uint32),
+                   col("rt_min", np.float64), pmz, charge, mz, inten, offsets)
+
+
 class DeviceRun:
     """One run's raw spectra on the device (the inputs of K0 and of the hypotheses)."""
 
@@ -442,18 +507,21 @@ def _k1_dense(gi: GpuIndex, dh, peaks, p: SearchParams, n_hyp: int, stats: Stats
     return pl["win_off"], cnt, pl["status"]
 
 
-def _k1_plan(gi: GpuIndex, dh, p: SearchParams, n_hyp: int) -> dict:
+def _k1_plan(gi: GpuIndex, dh, p: SearchParams, n_hyp: int, caps: tuple | None = None) -> dict:
     """The (tile, hypothesis) work items of K1 grouped by tile, and the window offsets, in buffers sized by the
-    index's window bound (nothing read back).  ``status`` (device i32) is zeroed here and collects the pass's
-    overflow / timeout bits."""
+    index's window bound, or by ``caps`` = (items, window rows) (nothing read back).  ``status`` (device i32) is
+    zeroed here and collects the pass's overflow / timeout bits."""
     L = K.lib()
     dev = gi.dev
     ix = gi.tix
     nt = ix.n_tiles
-    max_win = gi.window_bound(*p.precursor_ppm)
-    T = 1 << ix.tile_shift
-    item_cap = max(1, n_hyp * ((max_win + T - 1) // T + 1))
-    cnt_cap = max(1, n_hyp * max_win)
+    if caps is None:
+        max_win = gi.window_bound(*p.precursor_ppm)
+        T = 1 << ix.tile_shift
+        item_cap = max(1, n_hyp * ((max_win + T - 1) // T + 1))
+        cnt_cap = max(1, n_hyp * max_win)
+    else:
+        item_cap, cnt_cap = max(1, int(caps[0])), max(1, int(caps[1]))
     tile_items = torch.empty(max(nt, 1), dtype=torch.int64, device=dev)
     win_len = torch.empty(max(n_hyp, 1), dtype=torch.int64, device=dev)
     K.check(L.vk_k1_plan_count(C.byref(ix), n_hyp, K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(tile_items),
@@ -469,13 +537,15 @@ def _k1_plan(gi: GpuIndex, dh, p: SearchParams, n_hyp: int) -> dict:
             "cnt_cap": cnt_cap, "status": status}
 
 
-def _k1_hits(gi: GpuIndex, dh, peaks, p: SearchParams, n_hyp: int, thr: int, isum: bool = True):
-    """K1 in hit-list form (``vk_k1_hits``): per hypothesis the rows with count >= thr (count << 32 | row, and the
-    summed matched intensity) in its window's region, their number, and the per-hypothesis scored / matched
-    totals.  No dense per-row output."""
+def _k1_hits(gi: GpuIndex, dh, peaks, p: SearchParams, n_hyp: int, thr: int, isum: bool = True,
+             h_thr: torch.Tensor | None = None, caps: tuple | None = None):
+    """K1 in hit-list form (``vk_k1_hits``): per hypothesis the rows with count >= thr (``h_thr``: a device i32
+    threshold per hypothesis instead) -- count << 32 | row, and the summed matched intensity -- in its window's
+    region, their number, and the per-hypothesis scored / matched totals.  No dense per-row output.  ``caps``:
+    (item capacity, window-row capacity) when the caller knows them (else the index's window bound)."""
     L = K.lib()
     dev = gi.dev
-    pl = _k1_plan(gi, dh, p, n_hyp)
+    pl = _k1_plan(gi, dh, p, n_hyp, caps)
     cap = pl["cnt_cap"]
     rc = torch.empty(cap, dtype=torch.int64, device=dev)
     hisum = torch.empty(cap, dtype=torch.int32, device=dev) if isum else None
@@ -489,7 +559,8 @@ def _k1_hits(gi: GpuIndex, dh, peaks, p: SearchParams, n_hyp: int, thr: int, isu
     K.check(L.vk_k1_hits(C.byref(gi.tix), C.byref(gi.fp), float(p.fragment_ppm[0]), float(p.fragment_ppm[1]),
                          p.k1_warps, K.ptr(pl["item_off"]), K.ptr(pl["item_hyp"]), n_hyp, pl["item_cap"],
                          K.ptr(dh["spec"]), K.ptr(dh["maxfz"]), K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(pl["win_off"]),
-                         cap, K.ptr(peaks["off"]), K.ptr(peaks["mass"]), int(thr), K.ptr(rc),
+                         cap, K.ptr(peaks["off"]), K.ptr(peaks["mass"]), int(thr) if h_thr is None else 0,
+                         K.ptr(h_thr), K.ptr(rc),
                          K.ptr(hisum) if isum else None, K.ptr(hyp_hits), K.ptr(hyp_scored), K.ptr(hyp_matched),
                          K.ptr(pl["status"]), K.ptr(peaks["int"]) if isum else None,
                          K.ptr(peaks["tic"]) if isum else None, K.ptr(keys), K.ptr(filt), n_kz, kstride,
@@ -498,13 +569,14 @@ def _k1_hits(gi: GpuIndex, dh, peaks, p: SearchParams, n_hyp: int, thr: int, isu
             "hyp_scored": hyp_scored, "hyp_matched": hyp_matched}
 
 
-def _shortlist_hits(gi: GpuIndex, p: SearchParams, n: int, dh, k1h: dict, topk: int):
-    """Top-k of every spectrum by K1 count among its hit lists (``vk_select_hits``), compacted to spectrum-ordered
-    candidate lists with their intensity sums (``c_isum``); the same candidates as ``_shortlist`` without pair
-    closure over the dense counts.  Returns the candidate dict and the per-hypothesis / per-spectrum K1 sums."""
+def _shortlist_hits(gi: GpuIndex, p: SearchParams, n: int, dh, k1h: dict, topk: int, closure: bool = False):
+    """Top-k of every spectrum by K1 count among its hit lists (``vk_select_hits``), optionally with pair closure,
+    compacted to spectrum-ordered candidate lists with their intensity sums (``c_isum``); the same candidates as
+    ``_shortlist`` over the dense counts.  Returns the candidate dict and the per-hypothesis / per-spectrum K1
+    sums."""
     L = K.lib()
     dev = gi.dev
-    cap = topk
+    cap = (2 if closure else 1) * topk
     s_hyp = torch.empty(max(n * cap, 1), dtype=torch.int64, device=dev)
     s_row = torch.empty_like(s_hyp)
     s_cnt = torch.empty_like(s_hyp)
@@ -515,7 +587,8 @@ def _shortlist_hits(gi: GpuIndex, p: SearchParams, n: int, dh, k1h: dict, topk: 
     spec_matched = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
     K.check(L.vk_select_hits(n, K.ptr(dh["spec_off"]), K.ptr(k1h["win_off"]), K.ptr(k1h["hyp_hits"]),
                              K.ptr(k1h["rc"]), K.ptr(k1h["isum"]) if isum else None, K.ptr(k1h["hyp_scored"]),
-                             K.ptr(k1h["hyp_matched"]), topk, cap, K.ptr(s_hyp), K.ptr(s_row), K.ptr(s_cnt),
+                             K.ptr(k1h["hyp_matched"]), topk, int(closure), K.ptr(gi.partner), cap, K.ptr(s_hyp),
+                             K.ptr(s_row), K.ptr(s_cnt),
                              K.ptr(s_isum) if isum else None, K.ptr(n_cand), K.ptr(spec_scored),
                              K.ptr(spec_matched), K.stream()), "select_hits")
     cand_off = _scan(n_cand[:n])
