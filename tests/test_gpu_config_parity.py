@@ -118,3 +118,39 @@ def test_small_search_exhaustive_equals_oracle(small):
     assert np.array_equal(tbl.column("pf_row").to_numpy(), r[rk["cand"]])
     np.testing.assert_allclose(tbl.column("hyperscore").to_numpy(), rk["hyperscore"], rtol=1e-12)
     assert len(h) > 200_000
+
+
+def test_small_k1_shapes_per_peak_bucket_give_the_same_search(small):
+    """K1 shapes routed by peak-count bucket (each bucket's spectra on its own tiling and warps, as the autotuner
+    chooses them) give the single-shape pass's counts, statistics, candidates and K2 outputs, and the pruned
+    front end's shortlist."""
+    import dataclasses
+    from vulcan.gpu import engine as E
+    from vulcan.gpu import prune as PR
+    w, l1, sp, p, gi, P = small
+    npk = np.diff(sp.offsets)
+    q = dataclasses.replace(p, k1_shapes=((int(np.percentile(npk, 30)), 64, 3), (int(np.percentile(npk, 70)), 256, 8)))
+    gq = E.GpuIndex(l1, q, STATIC, w.var_mods)
+    assert set(gq.tilings) == {64, 128, 256}
+    a = E._search_device(E.DeviceRun(sp, gi.dev), gi, p, 1, E.Stats())
+    b = E._search_device(E.DeviceRun(sp, gq.dev), gq, q, 1, E.Stats())
+    E.check_status(b["status"])
+    nw = int(a["win_off"][-1])
+    assert torch_equal(a["win_off"], b["win_off"]) and torch_equal(a["cnt"][:nw], b["cnt"][:nw])
+    nc = int(a["cand_off"][-1])
+    for k in ("c_hyp", "c_row", "c_cnt"):
+        assert torch_equal(a[k][:nc], b[k][:nc]), k
+    for k in ("hyperscore", "matched_b", "matched_y", "summed_b", "summed_y"):
+        assert torch_equal(a["k2"][k][:nc], b["k2"][k][:nc]), k
+    fa = PR._front(E.DeviceRun(sp, gi.dev), gi, p, E.Stats(), False, min_count=2)
+    fb = PR._front(E.DeviceRun(sp, gq.dev), gq, q, E.Stats(), False, min_count=2)
+    n = len(sp)
+    nc = int(fa["hits"]["cand_off"][n])
+    assert int(fb["hits"]["cand_off"][n]) == nc
+    for k in ("c_hyp", "c_row", "c_cnt", "c_isum"):
+        assert torch_equal(fa["hits"][k][:nc], fb["hits"][k][:nc]), k
+
+
+def torch_equal(x, y):
+    import torch
+    return bool(torch.equal(x, y))

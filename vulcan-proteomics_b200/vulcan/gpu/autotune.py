@@ -1,11 +1,13 @@
-"""Autotuner of the search's launch shapes: fragment-index tile rows and K1 warps per CTA.
+"""Autotuner of the search's launch shapes: fragment-index tile rows and K1 warps per CTA, per peak-count bucket.
 
 The best shapes depend on the index (peptidoform density, fragments per row), the spectra (peak counts, charges)
 and the GPU, so they are measured, not guessed: for every candidate layout the index is tiled once, and a full
 device pass (plain, or pruned with a pruner) over a sample of the workload is timed with CUDA events (median of
-``reps`` after warm-up, L2 flushed before each).  Spectra are grouped into peak-count buckets for the report (the
-per-bucket pass time of the chosen layout), so that a workload whose peak counts shift can be re-tuned.  Results
-are cached in a JSON file keyed by index size, GPU name and tolerances.
+``reps`` after warm-up, L2 flushed before each).  Then, per peak-count bucket (kept peaks 1-64, 65-128, 129-256,
+257-512, 513+), K1 alone over that bucket's spectra of the sample is timed for every (tile rows, warps) and the
+fastest is kept; the buckets' shapes go into ``SearchParams.k1_shapes`` (each bucket's spectra then run K1 on
+their own tiling and warps inside the same pass), and the routed pass is kept if it beats the single layout.
+Results are cached in a JSON file keyed by index size, GPU name and tolerances.
 """
 from __future__ import annotations
 
@@ -72,7 +74,9 @@ def tune(l1, p: SearchParams, static: dict, var: dict, sample: Spectra, pruner=N
             known = json.load(fh)
         if key in known:
             r = known[key]
-            return dataclasses.replace(p, tile_rows=r["tile_rows"], k1_warps=r["k1_warps"]), dict(r, cached=True)
+            return (dataclasses.replace(p, tile_rows=r["tile_rows"], k1_warps=r["k1_warps"],
+                                        k1_shapes=tuple(tuple(x) for x in r.get("k1_shapes", ()))),
+                    dict(r, cached=True))
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device=dev)
     table = []
     best = None
@@ -100,7 +104,11 @@ def tune(l1, p: SearchParams, static: dict, var: dict, sample: Spectra, pruner=N
     if best is None:
         raise RuntimeError("autotune: no layout ran")
     ms, tr, w = best
-    chosen = dataclasses.replace(p, tile_rows=tr, k1_warps=w)
+    chosen = dataclasses.replace(p, tile_rows=tr, k1_warps=w, k1_shapes=())
+    routed, route_report = _tune_buckets(l1, chosen, static, var, sample, pruner, reps, flush, tile_rows, k1_warps,
+                                         ms, log)
+    if routed is not None:
+        chosen = routed
     # per peak-count bucket: the chosen layout's pass time over the spectra of that bucket
     lens = np.diff(np.asarray(sample.offsets, np.int64))
     buckets = []
@@ -114,7 +122,8 @@ def tune(l1, p: SearchParams, static: dict, var: dict, sample: Spectra, pruner=N
                             "ms": round(t, 4), "us_per_spectrum": round(1e3 * t / len(sel), 4)})
         lo = hi
     report = {"tile_rows": tr, "k1_warps": w, "ms": round(ms, 4), "sample_spectra": len(sample),
-              "candidates": table, "peak_buckets": buckets, "cached": False}
+              "candidates": table, "peak_buckets": buckets, "k1_shapes": [list(x) for x in chosen.k1_shapes],
+              "per_bucket": route_report, "cached": False}
     if cache:
         known = {}
         if os.path.exists(cache):
@@ -124,3 +133,86 @@ def tune(l1, p: SearchParams, static: dict, var: dict, sample: Spectra, pruner=N
         with open(cache, "w") as fh:
             json.dump(known, fh, indent=1)
     return chosen, report
+
+
+def _time_k1(gi, p, sp: Spectra, pruner, reps: int, flush) -> float:
+    """CUDA-event time of K1 alone (planning, window keys, counting; the pruned path's hit-list form with a
+    pruner) over a resident run whose K0 and hypotheses are done."""
+    run = E.DeviceRun(sp, gi.dev)
+    peaks = E._k0_device(run, p, gi.dev)
+    dh = E._hyp_device(run, peaks, gi, p)
+    thr = max(p.k1_threshold, pruner.min_count) if pruner is not None else p.k1_threshold
+
+    def step():
+        if pruner is not None:
+            return E._k1_hits(gi, dh, peaks, p, dh["n_max"], thr, isum=True)["status"]
+        return E._k1_dense(gi, dh, peaks, p, dh["n_max"])[2]
+    for _ in range(2):
+        step()
+    ts = []
+    for _ in range(reps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        status = step()
+        e1.record()
+        torch.cuda.synchronize(gi.dev)
+        ts.append(e0.elapsed_time(e1))
+    E.check_status(status)
+    return float(np.median(ts))
+
+
+def _tune_buckets(l1, p: SearchParams, static, var, sample: Spectra, pruner, reps, flush, tile_rows, k1_warps,
+                  single_ms: float, log=None):
+    """Per peak-count bucket the fastest (tile rows, warps) of K1 over the bucket's spectra; returns (params with
+    ``k1_shapes``, report), params None when routing the buckets does not beat the single layout."""
+    gi = E.GpuIndex(l1, p, static, var, device=flush.device)
+    for tr in tile_rows:
+        try:
+            gi.tiling(tr)
+        except RuntimeError:
+            continue
+    from ..synth import take_spectra
+    lens = np.diff(np.asarray(sample.offsets, np.int64))
+    kept = np.minimum(lens, p.max_peaks)           # an upper bound of the kept peaks, the bucket key
+    rows, lower = [], 0
+    for upper in PEAK_BUCKETS:
+        sel = np.flatnonzero((kept > lower) & (kept <= upper))
+        if len(sel) >= 64:
+            sub = take_spectra(sample, sel, sample.run)
+            best = None
+            for tr in tile_rows:
+                if tr not in gi.tilings:
+                    continue
+                for w in k1_warps:
+                    q = dataclasses.replace(p, k1_shapes=((1 << 30, tr, w),))
+                    try:
+                        t = _time_k1(gi, q, sub, pruner, reps, flush)
+                    except RuntimeError:
+                        continue
+                    if best is None or t < best[0]:
+                        best = (t, tr, w)
+            base = _time_k1(gi, p, sub, pruner, reps, flush)
+            rows.append({"peaks": f"{lower + 1}-{upper if upper < 1 << 30 else 'max'}", "spectra": int(len(sel)),
+                         "tile_rows": best[1], "k1_warps": best[2], "k1_ms": round(best[0], 4),
+                         "k1_ms_single_layout": round(base, 4)})
+            if log:
+                log(f"bucket {rows[-1]['peaks']}: {best[1]} rows x {best[2]} warps {best[0]:.3f} ms "
+                    f"(single layout {base:.3f})")
+        lower = upper
+    shapes = tuple((int(r["peaks"].split("-")[1]) if r["peaks"].split("-")[1] != "max" else 1 << 30,
+                    r["tile_rows"], r["k1_warps"]) for r in rows)
+    shapes = tuple(x for x in shapes if (x[1], x[2]) != (p.tile_rows, p.k1_warps) or x[0] < (1 << 30))
+    report = {"buckets": rows}
+    if not shapes or all((x[1], x[2]) == (p.tile_rows, p.k1_warps) for x in shapes):
+        report["routed"] = False
+        return None, report
+    routed = dataclasses.replace(p, k1_shapes=tuple(x for x in shapes if x[0] < (1 << 30)),
+                                 tile_rows=shapes[-1][1] if shapes[-1][0] >= (1 << 30) else p.tile_rows,
+                                 k1_warps=shapes[-1][2] if shapes[-1][0] >= (1 << 30) else p.k1_warps)
+    gi_r = E.GpuIndex(l1, routed, static, var, device=flush.device)
+    ms_r = _time_pass(gi_r, routed, sample, pruner, reps, flush)
+    report.update(routed_ms=round(ms_r, 4), single_ms=round(single_ms, 4), routed=ms_r < single_ms)
+    del gi_r, gi
+    torch.cuda.empty_cache()
+    return (routed if ms_r < single_ms else None), report

@@ -136,14 +136,17 @@ class GpuIndex:
         self.n_bins = int(math.floor(math.log(params.fragment_max_mz / params.fragment_min_mz) * self.inv_logw)) + 2
         self.n_chunks = (self.n + params.chunk_size - 1) // params.chunk_size
         self._slices = None
+        self.tilings = {}
         with torch.cuda.device(d):
             self._build_tiles()
+            for _, rows, _ in getattr(params, "k1_shapes", ()):   # the other tilings K1's shapes name
+                self.tiling(int(rows))
         torch.cuda.synchronize(d)
         self.build_s = time.perf_counter() - t0
         self.device_bytes = sum(t.numel() * t.element_size() for t in
                                 [self.seq_off, self.length, self.mask, self.mass32, self.residues, self.partner,
-                                 self.missed, self.n_var, self.pf_id, self.tile_off, self.cbin_off, self.postings,
-                                 self.bitmap])
+                                 self.missed, self.n_var, self.pf_id]) + \
+            sum(sum(x.numel() * x.element_size() for x in tl["tensors"]) for tl in self.tilings.values())
 
     def table_ptrs(self):
         return (K.ptr(self.seq_off), K.ptr(self.length), K.ptr(self.mask), K.ptr(self.mass32), K.ptr(self.residues))
@@ -164,9 +167,18 @@ class GpuIndex:
                 cache[key] = 0
         return cache[key]
 
-    def _build_tiles(self):
+    def tiling(self, tile_rows: int) -> dict:
+        """The tiled fragment index with ``tile_rows`` rows per tile ({"tix": vk_tindex, "tensors": [...]}), built
+        on first use (outside any stream capture).  The search's own tiling is ``p.tile_rows``."""
+        if tile_rows not in self.tilings:
+            with torch.cuda.device(self.dev):
+                self._build_tiles(tile_rows)
+        return self.tilings[tile_rows]
+
+    def _build_tiles(self, tile_rows: int | None = None):
         L = K.lib()
-        p = self.p
+        main = tile_rows is None or tile_rows == self.p.tile_rows
+        p = self.p if main else _replace(self.p, tile_rows=int(tile_rows), cbin_bits=0)
         ix = K.TIndex()
         K.check(L.vk_tindex_layout(self.n, p.tile_rows, p.fragment_min_mz, p.fragment_max_mz, p.min_ion_index,
                                    cbin_bits(p), C.byref(ix)), "tindex_layout")
@@ -175,25 +187,27 @@ class GpuIndex:
         tile_count = torch.empty(max(nt, 1), dtype=torch.int64, device=d)
         K.check(L.vk_tindex_count(C.byref(ix), C.byref(self.fp), *self.table_ptrs(), K.ptr(tile_count), K.stream()),
                 "tindex_count")
-        self.tile_off = _scan(tile_count[:nt])
+        tile_off = _scan(tile_count[:nt])
         stats = torch.stack([tile_count[:nt].max() if nt else torch.zeros((), dtype=torch.int64, device=d),
-                             self.tile_off[-1]]).cpu().tolist()
+                             tile_off[-1]]).cpu().tolist()
         ix.max_tile_postings = int(stats[0])
         ix.n_postings = int(stats[1])
         stride = ((1 << ix.cbin_bits) + 1 + 7) & ~7
-        self.postings = torch.empty(max(ix.n_postings, 4), dtype=torch.int32, device=d)
-        self.cbin_off = torch.empty(max(nt * stride, 8), dtype=torch.int16, device=d)
-        ix.tile_off = K.ptr(self.tile_off)
-        K.check(L.vk_tindex_emit(C.byref(ix), C.byref(self.fp), *self.table_ptrs(), K.ptr(self.postings),
-                                 K.ptr(self.cbin_off), K.stream()), "tindex_emit")
-        ix.cbin_off = K.ptr(self.cbin_off)
-        ix.postings = K.ptr(self.postings)
-        self.bitmap = torch.empty(max(int(L.vk_tindex_bitmap_bytes(C.byref(ix))) // 4, 4), dtype=torch.int32,
-                                  device=d)
-        K.check(L.vk_tindex_bitmap(C.byref(ix), K.ptr(self.bitmap), K.stream()), "tindex_bitmap")
-        ix.bitmap = K.ptr(self.bitmap)
-        self.tix = ix
-        self.n_postings = ix.n_postings
+        postings = torch.empty(max(ix.n_postings, 4), dtype=torch.int32, device=d)
+        cbin_off = torch.empty(max(nt * stride, 8), dtype=torch.int16, device=d)
+        ix.tile_off = K.ptr(tile_off)
+        K.check(L.vk_tindex_emit(C.byref(ix), C.byref(self.fp), *self.table_ptrs(), K.ptr(postings),
+                                 K.ptr(cbin_off), K.stream()), "tindex_emit")
+        ix.cbin_off = K.ptr(cbin_off)
+        ix.postings = K.ptr(postings)
+        bitmap = torch.empty(max(int(L.vk_tindex_bitmap_bytes(C.byref(ix))) // 4, 4), dtype=torch.int32, device=d)
+        K.check(L.vk_tindex_bitmap(C.byref(ix), K.ptr(bitmap), K.stream()), "tindex_bitmap")
+        ix.bitmap = K.ptr(bitmap)
+        self.tilings[p.tile_rows] = {"tix": ix, "tensors": [tile_off, cbin_off, postings, bitmap]}
+        if main:
+            self.tile_off, self.cbin_off, self.postings, self.bitmap = tile_off, cbin_off, postings, bitmap
+            self.tix = ix
+            self.n_postings = ix.n_postings
 
     # ------------------------------------------------------------------ reference-layout CSR (compatible vk_k1)
     @property
@@ -470,17 +484,55 @@ def key_charges(p: SearchParams) -> int:
     return mfc if mfc > 0 else 2
 
 
-def peak_keys(gi: GpuIndex, peaks, p: SearchParams):
+def peak_keys(gi: GpuIndex, peaks, p: SearchParams, tix=None):
     """Window keys and filter words of every kept peak (vk_k1_peak_keys): (keys, filt, n_kz, kstride), computed once
-    per pass for all the (tile, hypothesis) items of K1."""
+    per pass for all the (tile, hypothesis) items of K1; the filter words are bitmap positions of the tiling
+    ``tix`` (default: the index's own)."""
     n_kz = key_charges(p)
     kstride = int(peaks["mass"].numel())
     keys = torch.empty(max(n_kz * kstride * 2, 2), dtype=torch.int32, device=gi.dev)
     filt = torch.empty(max(n_kz * kstride, 1), dtype=torch.int32, device=gi.dev)
-    K.check(K.lib().vk_k1_peak_keys(C.byref(gi.tix), C.byref(gi.fp), float(p.fragment_ppm[0]),
+    K.check(K.lib().vk_k1_peak_keys(C.byref(tix or gi.tix), C.byref(gi.fp), float(p.fragment_ppm[0]),
                                     float(p.fragment_ppm[1]), K.ptr(peaks["off"][-1:]), K.ptr(peaks["mass"]), n_kz,
                                     kstride, K.ptr(keys), K.ptr(filt), K.stream()), "k1_peak_keys")
     return keys, filt, n_kz, kstride
+
+
+def k1_shape_list(gi: GpuIndex, p: SearchParams) -> list:
+    """K1's launch shapes: [(tiling, k1 warps, lower, upper)] -- the spectra whose kept peaks n satisfy
+    lower < n <= upper take that shape (``p.k1_shapes``; one shape for all without it)."""
+    out, lower = [], 0
+    for upper, rows, warps in sorted(tuple(x) for x in getattr(p, "k1_shapes", ())):
+        out.append((gi.tiling(int(rows)), int(warps), lower, int(upper)))
+        lower = int(upper)
+    out.append((gi.tiling(p.tile_rows), int(p.k1_warps), lower, 1 << 62))
+    return out
+
+
+def _k1_passes(gi: GpuIndex, dh, peaks, p: SearchParams, n_hyp: int, caps: tuple | None = None):
+    """The K1 launches of a pass: per shape (``k1_shape_list``) its work items -- the hypotheses of the spectra in
+    the shape's peak-count bucket, planned on the shape's tiling -- with the window keys of that tiling.  Yields
+    (tix, warps, plan, keys, filt, n_kz, kstride); every plan shares one ``win_off`` (the windows of all the
+    hypotheses) and one ``status``."""
+    shapes = k1_shape_list(gi, p)
+    if len(shapes) == 1:
+        tl, warps, _, _ = shapes[0]
+        pl = _k1_plan(gi, dh, p, n_hyp, caps, tiling=tl)
+        yield (tl["tix"], warps, pl) + peak_keys(gi, peaks, p, tl["tix"])
+        return
+    lo, hi = dh["lo"][:n_hyp], dh["hi"][:n_hyp]
+    win_off = _scan((hi - lo).clamp(min=0))
+    status = torch.zeros(1, dtype=torch.int32, device=gi.dev)
+    npk = (peaks["off"][1:] - peaks["off"][:-1])[dh["spec"][:n_hyp].long()]
+    keys_of = {}
+    for tl, warps, lower, upper in shapes:
+        mine = (npk > lower) & (npk <= upper)
+        pl = _k1_plan(gi, dh, p, n_hyp, caps, tiling=tl, hi=torch.where(mine, hi, lo), win_off=win_off,
+                      status=status)
+        key = id(tl)
+        if key not in keys_of:
+            keys_of[key] = peak_keys(gi, peaks, p, tl["tix"])
+        yield (tl["tix"], warps, pl) + keys_of[key]
 
 
 def _k1_dense(gi: GpuIndex, dh, peaks, p: SearchParams, n_hyp: int, stats: Stats | None = None,
@@ -488,32 +540,37 @@ def _k1_dense(gi: GpuIndex, dh, peaks, p: SearchParams, n_hyp: int, stats: Stats
     """Tiled K1: dense counts of every window row.  Returns (win_off, cnt, status), plus the summed matched
     intensity of every window row (u32, 2^24 = the spectrum's TIC) when ``isum``.  The buffers are sized by the
     index's window bound (``GpuIndex.window_bound``), so nothing is read back from the device: cnt / isum hold
-    more entries than the win_off[-1] window rows, and ``status`` gets VK_STATUS_OVERFLOW should a bound not hold."""
+    more entries than the win_off[-1] window rows, and ``status`` gets VK_STATUS_OVERFLOW should a bound not hold.
+    With ``p.k1_shapes`` each peak-count bucket's hypotheses run with their own tiling and warps (same counts)."""
     L = K.lib()
     dev = gi.dev
-    pl = _k1_plan(gi, dh, p, n_hyp)
-    cnt = torch.empty(pl["cnt_cap"], dtype=torch.int32, device=dev)
-    isw = torch.empty(pl["cnt_cap"], dtype=torch.int32, device=dev) if isum else None
-    keys, filt, n_kz, kstride = peak_keys(gi, peaks, p)
-    K.check(L.vk_k1_tiles(C.byref(gi.tix), C.byref(gi.fp), float(p.fragment_ppm[0]), float(p.fragment_ppm[1]),
-                          p.k1_warps, K.ptr(pl["item_off"]), K.ptr(pl["item_hyp"]), n_hyp, pl["item_cap"],
-                          K.ptr(dh["spec"]), K.ptr(dh["maxfz"]), K.ptr(dh["lo"]), K.ptr(dh["hi"]),
-                          K.ptr(pl["win_off"]), pl["cnt_cap"], K.ptr(peaks["off"]), K.ptr(peaks["mass"]), K.ptr(cnt),
-                          K.ptr(pl["status"]), K.ptr(peaks["int"]) if isum else None,
-                          K.ptr(peaks["tic"]) if isum else None, K.ptr(isw) if isum else None, K.ptr(keys),
-                          K.ptr(filt), n_kz, kstride, K.stream()), "k1_tiles")
+    cnt = isw = pl = None
+    for tix, warps, pl, keys, filt, n_kz, kstride in _k1_passes(gi, dh, peaks, p, n_hyp):
+        if cnt is None:
+            cnt = torch.empty(pl["cnt_cap"], dtype=torch.int32, device=dev)
+            isw = torch.empty(pl["cnt_cap"], dtype=torch.int32, device=dev) if isum else None
+        K.check(L.vk_k1_tiles(C.byref(tix), C.byref(gi.fp), float(p.fragment_ppm[0]), float(p.fragment_ppm[1]),
+                              warps, K.ptr(pl["item_off"]), K.ptr(pl["item_hyp"]), n_hyp, pl["item_cap"],
+                              K.ptr(dh["spec"]), K.ptr(dh["maxfz"]), K.ptr(dh["lo"]), K.ptr(dh["hi"]),
+                              K.ptr(pl["win_off"]), pl["cnt_cap"], K.ptr(peaks["off"]), K.ptr(peaks["mass"]),
+                              K.ptr(cnt), K.ptr(pl["status"]), K.ptr(peaks["int"]) if isum else None,
+                              K.ptr(peaks["tic"]) if isum else None, K.ptr(isw) if isum else None, K.ptr(keys),
+                              K.ptr(filt), n_kz, kstride, K.stream()), "k1_tiles")
     if isum:
         return pl["win_off"], cnt, pl["status"], isw
     return pl["win_off"], cnt, pl["status"]
 
 
-def _k1_plan(gi: GpuIndex, dh, p: SearchParams, n_hyp: int, caps: tuple | None = None) -> dict:
+def _k1_plan(gi: GpuIndex, dh, p: SearchParams, n_hyp: int, caps: tuple | None = None, tiling: dict | None = None,
+             hi=None, win_off=None, status=None) -> dict:
     """The (tile, hypothesis) work items of K1 grouped by tile, and the window offsets, in buffers sized by the
-    index's window bound, or by ``caps`` = (items, window rows) (nothing read back).  ``status`` (device i32) is
-    zeroed here and collects the pass's overflow / timeout bits."""
+    index's window bound, or by ``caps`` = (items, window rows) (nothing read back).  ``tiling``: plan on that
+    tiling of the index (default its own); ``hi``: the window ends to plan items for (default the hypotheses' own;
+    an empty window gets no item), with ``win_off`` of the full windows given.  ``status`` (device i32) is zeroed
+    here unless given, and collects the pass's overflow / timeout bits."""
     L = K.lib()
     dev = gi.dev
-    ix = gi.tix
+    ix = tiling["tix"] if tiling is not None else gi.tix
     nt = ix.n_tiles
     if caps is None:
         max_win = gi.window_bound(*p.precursor_ppm)
@@ -522,16 +579,19 @@ def _k1_plan(gi: GpuIndex, dh, p: SearchParams, n_hyp: int, caps: tuple | None =
         cnt_cap = max(1, n_hyp * max_win)
     else:
         item_cap, cnt_cap = max(1, int(caps[0])), max(1, int(caps[1]))
+    h_hi = dh["hi"] if hi is None else hi
     tile_items = torch.empty(max(nt, 1), dtype=torch.int64, device=dev)
     win_len = torch.empty(max(n_hyp, 1), dtype=torch.int64, device=dev)
-    K.check(L.vk_k1_plan_count(C.byref(ix), n_hyp, K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(tile_items),
+    K.check(L.vk_k1_plan_count(C.byref(ix), n_hyp, K.ptr(dh["lo"]), K.ptr(h_hi), K.ptr(tile_items),
                                K.ptr(win_len), K.stream()), "k1_plan_count")
     item_off = _scan(tile_items[:nt])
-    win_off = _scan(win_len[:n_hyp])
-    status = torch.zeros(1, dtype=torch.int32, device=dev)
+    if win_off is None:
+        win_off = _scan(win_len[:n_hyp])
+    if status is None:
+        status = torch.zeros(1, dtype=torch.int32, device=dev)
     cursor = torch.empty(max(nt, 1), dtype=torch.int64, device=dev)
     item_hyp = torch.empty(item_cap, dtype=torch.int32, device=dev)
-    K.check(L.vk_k1_plan_fill(C.byref(ix), n_hyp, K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(item_off),
+    K.check(L.vk_k1_plan_fill(C.byref(ix), n_hyp, K.ptr(dh["lo"]), K.ptr(h_hi), K.ptr(item_off),
                               K.ptr(cursor), K.ptr(item_hyp), item_cap, K.ptr(status), K.stream()), "k1_plan_fill")
     return {"item_off": item_off, "item_hyp": item_hyp, "item_cap": item_cap, "win_off": win_off,
             "cnt_cap": cnt_cap, "status": status}
@@ -545,26 +605,27 @@ def _k1_hits(gi: GpuIndex, dh, peaks, p: SearchParams, n_hyp: int, thr: int, isu
     (item capacity, window-row capacity) when the caller knows them (else the index's window bound)."""
     L = K.lib()
     dev = gi.dev
-    pl = _k1_plan(gi, dh, p, n_hyp, caps)
-    cap = pl["cnt_cap"]
-    rc = torch.empty(cap, dtype=torch.int64, device=dev)
-    hisum = torch.empty(cap, dtype=torch.int32, device=dev) if isum else None
-    # hyp_hits (u32), hyp_scored (u32), hyp_matched (u64): one zeroed allocation
     nh = max(n_hyp, 1)
+    # hyp_hits (u32), hyp_scored (u32), hyp_matched (u64): one zeroed allocation
     z = torch.zeros(nh * 2, dtype=torch.int64, device=dev)
     counters = z[:nh].view(torch.int32)
     hyp_hits, hyp_scored = counters[:nh], counters[nh:]
     hyp_matched = z[nh:]
-    keys, filt, n_kz, kstride = peak_keys(gi, peaks, p)
-    K.check(L.vk_k1_hits(C.byref(gi.tix), C.byref(gi.fp), float(p.fragment_ppm[0]), float(p.fragment_ppm[1]),
-                         p.k1_warps, K.ptr(pl["item_off"]), K.ptr(pl["item_hyp"]), n_hyp, pl["item_cap"],
-                         K.ptr(dh["spec"]), K.ptr(dh["maxfz"]), K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(pl["win_off"]),
-                         cap, K.ptr(peaks["off"]), K.ptr(peaks["mass"]), int(thr) if h_thr is None else 0,
-                         K.ptr(h_thr), K.ptr(rc),
-                         K.ptr(hisum) if isum else None, K.ptr(hyp_hits), K.ptr(hyp_scored), K.ptr(hyp_matched),
-                         K.ptr(pl["status"]), K.ptr(peaks["int"]) if isum else None,
-                         K.ptr(peaks["tic"]) if isum else None, K.ptr(keys), K.ptr(filt), n_kz, kstride,
-                         K.stream()), "k1_hits")
+    rc = hisum = pl = None
+    for tix, warps, pl, keys, filt, n_kz, kstride in _k1_passes(gi, dh, peaks, p, n_hyp, caps):
+        cap = pl["cnt_cap"]
+        if rc is None:
+            rc = torch.empty(cap, dtype=torch.int64, device=dev)
+            hisum = torch.empty(cap, dtype=torch.int32, device=dev) if isum else None
+        K.check(L.vk_k1_hits(C.byref(tix), C.byref(gi.fp), float(p.fragment_ppm[0]), float(p.fragment_ppm[1]),
+                             warps, K.ptr(pl["item_off"]), K.ptr(pl["item_hyp"]), n_hyp, pl["item_cap"],
+                             K.ptr(dh["spec"]), K.ptr(dh["maxfz"]), K.ptr(dh["lo"]), K.ptr(dh["hi"]),
+                             K.ptr(pl["win_off"]), cap, K.ptr(peaks["off"]), K.ptr(peaks["mass"]),
+                             int(thr) if h_thr is None else 0, K.ptr(h_thr), K.ptr(rc),
+                             K.ptr(hisum) if isum else None, K.ptr(hyp_hits), K.ptr(hyp_scored), K.ptr(hyp_matched),
+                             K.ptr(pl["status"]), K.ptr(peaks["int"]) if isum else None,
+                             K.ptr(peaks["tic"]) if isum else None, K.ptr(keys), K.ptr(filt), n_kz, kstride,
+                             K.stream()), "k1_hits")
     return {"win_off": pl["win_off"], "status": pl["status"], "rc": rc, "isum": hisum, "hyp_hits": hyp_hits,
             "hyp_scored": hyp_scored, "hyp_matched": hyp_matched}
 

@@ -48,6 +48,10 @@ class SearchParams:
     tile_rows: int = 128
     cbin_bits: int = 0
     k1_warps: int = 4
+    # K1 shapes per peak-count bucket (chosen by the autotuner): ((most kept peaks, tile_rows, k1_warps), ...) in
+    # ascending peak bounds; a spectrum takes the first bucket its kept peaks fit, spectra above the last bound
+    # take (tile_rows, k1_warps).  Empty: one shape for every spectrum.  The counts do not depend on the shapes.
+    k1_shapes: tuple = ()
     search_method: str = "staged"           # "staged" (a kernel per stage) or "fused" (one persistent kernel)
     fused_warps: int = 4                    # warps of a fused-search CTA (one spectrum at a time)
     fused_cnt_cap: int = 4096               # window rows a spectrum may span in the fused search
