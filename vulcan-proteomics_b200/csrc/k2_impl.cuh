@@ -128,14 +128,15 @@ __device__ __forceinline__ void k2_score(const SmemFrag& fp, const PT& pt, int r
   RunLen rb = {0, 0, 0, 0}, ry = {0, 0, 0, 0};
   const int da = fp.tol_da;
   int n_alt = 1;
-  float iu[2][SHIFT ? VK_K2_MAXLEN : 1], is_[2][SHIFT ? VK_K2_MAXLEN : 1];
-  unsigned char nu[2][SHIFT ? VK_K2_MAXLEN : 1], ns[2][SHIFT ? VK_K2_MAXLEN : 1];
+  // per ion kind and index: matched intensity and match count of the unshifted / shifted fragment
+  float hit_u[2][SHIFT ? VK_K2_MAXLEN : 1], hit_s[2][SHIFT ? VK_K2_MAXLEN : 1];
+  unsigned char cnt_u[2][SHIFT ? VK_K2_MAXLEN : 1], cnt_s[2][SHIFT ? VK_K2_MAXLEN : 1];
   if (SHIFT) {
     n_alt = shift != 0.f ? 2 : 1;
     if (n_alt == 2) {
       for (int k = 0; k < (SHIFT ? VK_K2_MAXLEN : 1); ++k) {
-        iu[0][k] = iu[1][k] = is_[0][k] = is_[1][k] = 0.f;
-        nu[0][k] = nu[1][k] = ns[0][k] = ns[1][k] = 0;
+        hit_u[0][k] = hit_u[1][k] = hit_s[0][k] = hit_s[1][k] = 0.f;
+        cnt_u[0][k] = cnt_u[1][k] = cnt_s[0][k] = cnt_s[1][k] = 0;
       }
     }
   }
@@ -159,8 +160,8 @@ __device__ __forceinline__ void k2_score(const SmemFrag& fp, const PT& pt, int r
             if (SHIFT && it >= mx_a) { mx_a = it; best_a = j; }
           }
           if (SHIFT && n_alt == 2 && best_a >= 0 && k < VK_K2_MAXLEN) {
-            if (alt == 0) { iu[kind][k] = __fadd_rn(iu[kind][k], si[best_a]); nu[kind][k] += 1; }
-            else { is_[kind][k] = __fadd_rn(is_[kind][k], si[best_a]); ns[kind][k] += 1; }
+            if (alt == 0) { hit_u[kind][k] = __fadd_rn(hit_u[kind][k], si[best_a]); cnt_u[kind][k] += 1; }
+            else { hit_s[kind][k] = __fadd_rn(hit_s[kind][k], si[best_a]); cnt_s[kind][k] += 1; }
           }
         }
         if (best >= 0) {
@@ -176,21 +177,23 @@ __device__ __forceinline__ void k2_score(const SmemFrag& fp, const PT& pt, int r
   if (SHIFT && n_alt == 2) {
     // best site of the delta (kernels.cu:343-363): b_k shifted iff k >= site, y_k iff k < site
     int Lk = min(L - 1, VK_K2_MAXLEN);
-    float b_u = 0.f, y_s = 0.f, b_s = 0.f, y_u = 0.f;
-    int nb_u = 0, ny_s = 0, nb_s = 0, ny_u = 0;
+    float sum_bu = 0.f, sum_ys = 0.f, sum_bs = 0.f, sum_yu = 0.f;
+    int n_bu = 0, n_ys = 0, n_bs = 0, n_yu = 0;
     for (int k = 0; k < Lk; ++k) {
-      b_s = __fadd_rn(b_s, is_[0][k]); nb_s += ns[0][k];
-      y_u = __fadd_rn(y_u, iu[1][k]); ny_u += nu[1][k];
+      sum_bs = __fadd_rn(sum_bs, hit_s[0][k]); n_bs += cnt_s[0][k];
+      sum_yu = __fadd_rn(sum_yu, hit_u[1][k]); n_yu += cnt_u[1][k];
     }
     double best_hs = -1e300;
-    for (int st = 0; st < L; ++st) {
-      if (st > 0 && st - 1 < Lk) {
-        int k = st - 1;
-        b_u = __fadd_rn(b_u, iu[0][k]); nb_u += nu[0][k]; b_s = __fsub_rn(b_s, is_[0][k]); nb_s -= ns[0][k];
-        y_s = __fadd_rn(y_s, is_[1][k]); ny_s += ns[1][k]; y_u = __fsub_rn(y_u, iu[1][k]); ny_u -= nu[1][k];
+    for (int site = 0; site < L; ++site) {
+      if (site > 0 && site - 1 < Lk) {
+        int k = site - 1;
+        sum_bu = __fadd_rn(sum_bu, hit_u[0][k]); n_bu += cnt_u[0][k];
+        sum_bs = __fsub_rn(sum_bs, hit_s[0][k]); n_bs -= cnt_s[0][k];
+        sum_ys = __fadd_rn(sum_ys, hit_s[1][k]); n_ys += cnt_s[1][k];
+        sum_yu = __fsub_rn(sum_yu, hit_u[1][k]); n_yu -= cnt_u[1][k];
       }
-      float sb2 = __fadd_rn(b_u, b_s), sy2 = __fadd_rn(y_u, y_s);
-      int mb2 = nb_u + nb_s, my2 = ny_u + ny_s;
+      float sb2 = __fadd_rn(sum_bu, sum_bs), sy2 = __fadd_rn(sum_yu, sum_ys);
+      int mb2 = n_bu + n_bs, my2 = n_yu + n_ys;
       double h2 = log((double)__fadd_rn(fmaxf(sb2, 0.f), 1.0f) * (double)__fadd_rn(fmaxf(sy2, 0.f), 1.0f)) +
                   lnfact(mb2) + lnfact(my2);
       if (h2 > best_hs) { best_hs = h2; mb = mb2; my = my2; sb = fmaxf(sb2, 0.f); sy = fmaxf(sy2, 0.f); }
