@@ -586,35 +586,39 @@ def _kernel_table(a, p, gi, run, flush, pr, dev):
         # hit lists: the kernels of the pruned path
         thr = max(p.k1_threshold, pr.min_count)
         k1h = so["k1_hits"]
-        z = torch.zeros(dh["n_max"] * 2, dtype=torch.int64, device=dev)
+        nm = dh["n_max"]
+        z = torch.zeros(nm * 3, dtype=torch.int64, device=dev)
 
         def run_k1():
             z.zero_()
             K.check(L.vk_k1_hits(
                 C.byref(gi.tix), C.byref(gi.fp), float(p.fragment_ppm[0]), float(p.fragment_ppm[1]), p.k1_warps,
-                K.ptr(item_off), K.ptr(item_hyp), dh["n_max"], pl["item_cap"], K.ptr(dh["spec"]), K.ptr(dh["maxfz"]),
+                K.ptr(item_off), K.ptr(item_hyp), nm, pl["item_cap"], K.ptr(dh["spec"]), K.ptr(dh["maxfz"]),
                 K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(win_off), pl["cnt_cap"], K.ptr(peaks["off"]),
                 K.ptr(peaks["mass"]), thr, None, K.ptr(k1h["rc"]), K.ptr(k1h["isum"]),
-                K.ptr(z[:dh["n_max"]].view(torch.int32)[:dh["n_max"]]),
-                K.ptr(z[:dh["n_max"]].view(torch.int32)[dh["n_max"]:]), K.ptr(z[dh["n_max"]:]), K.ptr(pl["status"]),
-                K.ptr(peaks["int"]), K.ptr(peaks["tic"]), K.ptr(keys), K.ptr(filt), n_kz, kstride, K.stream()),
-                "k1_hits")
+                K.ptr(z[2 * nm:].view(torch.int8)[:nm]), K.ptr(z[:nm].view(torch.int32)[:nm]), K.ptr(z[nm:2 * nm]),
+                K.ptr(pl["status"]), K.ptr(peaks["int"]), K.ptr(peaks["tic"]), K.ptr(keys), K.ptr(filt), n_kz,
+                kstride, K.stream()), "k1_hits")
         ms_k1 = timed(run_k1)
-        n_k1_hits = int(k1h["hyp_hits"][:nh].long().sum())
+        # the hits K1 keeps: the dense counts of the same windows over the floor
+        cnt_d = E._k1_dense(gi, dh, peaks, p, nm)[1]
+        n_k1_hits = int((cnt_d[:n_win] >= thr).sum())
+        del cnt_d
         kern["k1_tiles_k (hit lists)"] = (ms_k1, k1_algorithmic_bytes(gi, dh, peaks, item_off, nh, True,
-                                                                       n_k1_hits * 12 + nh * 16))
+                                                                       n_k1_hits * 12 + nh * 13))
         tk = {k: torch.empty(max(n * cap, 1), dtype=torch.int64, device=dev) for k in ("h", "r", "c")}
         ti = torch.empty(max(n * cap, 1), dtype=torch.int32, device=dev)
         tk_n = torch.empty(n, dtype=torch.int64, device=dev)
         ss_ = torch.empty(n, dtype=torch.int64, device=dev)
         sm_ = torch.empty(n, dtype=torch.int64, device=dev)
         ms_tk = timed(lambda: K.check(L.vk_select_hits(
-            n, K.ptr(dh["spec_off"]), K.ptr(win_off), K.ptr(k1h["hyp_hits"]), K.ptr(k1h["rc"]), K.ptr(k1h["isum"]),
-            K.ptr(k1h["hyp_scored"]), K.ptr(k1h["hyp_matched"]), p.topk, 0, None, cap, K.ptr(tk["h"]), K.ptr(tk["r"]),
+            n, K.ptr(dh["spec_off"]), K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(win_off), K.ptr(k1h["hyp_shift"]),
+            K.ptr(k1h["rc"]), K.ptr(k1h["isum"]), K.ptr(k1h["hyp_scored"]), K.ptr(k1h["hyp_matched"]), p.topk, 0,
+            None, cap, K.ptr(tk["h"]), K.ptr(tk["r"]),
             K.ptr(tk["c"]), K.ptr(ti), K.ptr(tk_n), K.ptr(ss_), K.ptr(sm_), K.stream()), "select_hits"))
-        # hits read (12 B), per-hypothesis totals (16 B), per spectrum its hypothesis range and outputs; the
-        # shortlist written (28 B per kept hit)
-        kern["select_hits_k"] = (ms_tk, n_k1_hits * 12 + nh * 24 + n * 32 + n_hit * 28)
+        # hits read (12 B), per-hypothesis windows, totals and tile shift (33 B), per spectrum its hypothesis range
+        # and outputs; the shortlist written (28 B per kept hit)
+        kern["select_hits_k"] = (ms_tk, n_k1_hits * 12 + nh * 41 + n * 32 + n_hit * 28)
     else:
         cnt = so["cnt"]
         status = torch.zeros(1, dtype=torch.int32, device=dev)

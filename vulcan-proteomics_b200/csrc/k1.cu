@@ -57,15 +57,18 @@ struct K1Rec {
   int32_t h;          // hypothesis (the hit-list output appends to its region)
 };
 
-// Outputs of the hit-list form of K1 (vk_k1_hits): instead of a dense count per window row, the rows with count >=
-// thr of hypothesis h are appended to its region [win_off[h], win_off[h] + hyp_hits[h]) of rc (count << 32 | row)
-// and isum; per hypothesis the number of rows with a nonzero count and the sum of the counts.
+// Outputs of the hit-list form of K1 (vk_k1_hits): instead of a dense count per window row, each (tile, hypothesis)
+// item writes the rows of its tile with count >= thr, in row order, to the start of its own segment of the
+// hypothesis' region -- the slots of the window rows it covers -- as count << 32 | row (rc) and isum, followed by
+// the end mark VK_HIT_END when fewer than the segment's slots are used; hyp_shift[h] gets the tiling's tile shift (the
+// segment boundaries); per hypothesis the number of rows with a nonzero count and the sum of the counts (integer
+// atomics).  No atomic decides a position, so the layout does not depend on scheduling.
 struct K1Hits {
   int thr;
   const int32_t* h_thr;   // per-hypothesis thresholds (NULL: thr for all)
   uint64_t* rc;
   uint32_t* isum;
-  uint32_t* hyp_hits;
+  int8_t* hyp_shift;
   uint32_t* hyp_scored;
   unsigned long long* hyp_matched;
 };
@@ -179,11 +182,12 @@ k1_tiles_k(vk_tindex ix, float tol_lo, float tol_hi, int tol_da, int post_cap, c
                            pk_int, r.ws);
       __syncwarp();
       if (HITS) {
-        // rows with count >= thr appended to the hypothesis' region, one atomic per 32 rows; the statistics of
-        // the item's rows added to the hypothesis' totals (integer sums: the result does not depend on order)
-        const int64_t region = win_off[r.h];
+        // the item's segment: the slots of the window rows rlo..rhi of this tile (r.base is the region index of
+        // the tile's row 0); kept rows compacted to its start in row order, then the end mark
+        const int64_t seg = r.base + rlo;
         const int thr_h = hits.h_thr ? hits.h_thr[r.h] : hits.thr;
         long long sc = 0, mt = 0;
+        int n_kept = 0;
         for (int q0 = rlo; q0 < rhi; q0 += 32) {
           const int q = q0 + lane;
           const uint32_t c = q < rhi ? hw[q] : 0u;
@@ -191,19 +195,18 @@ k1_tiles_k(vk_tindex ix, float tol_lo, float tol_hi, int tol_da, int post_cap, c
           mt += c;
           const bool keep = q < rhi && (int)c >= thr_h;
           const unsigned bal = __ballot_sync(VK_FULL, keep);
-          if (!bal) continue;
-          uint32_t at0 = 0;
-          if (lane == 0) at0 = atomicAdd(&hits.hyp_hits[r.h], (uint32_t)__popc(bal));
-          at0 = __shfl_sync(VK_FULL, at0, 0);
           if (keep) {
-            const int64_t at = region + at0 + __popc(bal & ((1u << lane) - 1u));
+            const int64_t at = seg + n_kept + __popc(bal & ((1u << lane) - 1u));
             hits.rc[at] = ((uint64_t)c << 32) | (uint64_t)(r0 + q);
             if (iw) hits.isum[at] = iw[q];
           }
+          n_kept += __popc(bal);
         }
         sc = vk::warp_sum(sc);
         mt = vk::warp_sum(mt);
         if (lane == 0) {
+          if (n_kept < rhi - rlo) hits.rc[seg + n_kept] = VK_HIT_END;
+          hits.hyp_shift[r.h] = (int8_t)ix.tile_shift;   // every item of h writes the same value
           if (sc) atomicAdd(&hits.hyp_scored[r.h], (uint32_t)sc);
           if (mt) atomicAdd(&hits.hyp_matched[r.h], (unsigned long long)mt);
         }
@@ -321,12 +324,12 @@ int vk_k1_hits(const vk_tindex* ix, const vk_frag_params* fp, float tol_lo, floa
                const int64_t* tile_item_off, const int32_t* item_hyp, int64_t n_hyp, int64_t item_cap,
                const int32_t* h_spec, const int8_t* h_maxfz, const int64_t* h_lo, const int64_t* h_hi,
                const int64_t* win_off, int64_t cnt_cap, const int64_t* pk_off, const float* pk_mass, int thr,
-               const int32_t* h_thr, uint64_t* hit_rc, uint32_t* hit_isum, uint32_t* hyp_hits, uint32_t* hyp_scored,
+               const int32_t* h_thr, uint64_t* hit_rc, uint32_t* hit_isum, int8_t* hyp_shift, uint32_t* hyp_scored,
                uint64_t* hyp_matched, int32_t* status, const float* pk_int, const float* tic,
                const uint32_t* pk_keys, const uint32_t* pk_filt, int n_kz, int64_t kstride, void* stream) {
-  if (!hit_rc || !hyp_hits || !hyp_scored || !hyp_matched || (!h_thr && thr < 1)) return VK_E_ARG;
+  if (!hit_rc || !hyp_shift || !hyp_scored || !hyp_matched || (!h_thr && thr < 1)) return VK_E_ARG;
   if ((hit_isum != nullptr) != (pk_int != nullptr)) return VK_E_ARG;
-  K1Hits hits{thr, h_thr, hit_rc, hit_isum, hyp_hits, hyp_scored,
+  K1Hits hits{thr, h_thr, hit_rc, hit_isum, hyp_shift, hyp_scored,
               reinterpret_cast<unsigned long long*>(hyp_matched)};
   return k1_tiles_launch<true>(ix, fp, tol_lo, tol_hi, warps, tile_item_off, item_hyp, n_hyp, item_cap, h_spec,
                                h_maxfz, h_lo, h_hi, win_off, cnt_cap, pk_off, pk_mass, nullptr, status, pk_int, tic,

@@ -268,19 +268,46 @@ select_topk_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo, cons
   if (lane == 0) n_cand[s] = n_out;
 }
 
-// Shortlist from the hit lists of vk_k1_hits, one warp per spectrum: the hits of the spectrum's hypotheses (region
-// of hypothesis h: [win_off[h], win_off[h] + hyp_hits[h]) of rc = count << 32 | row, and of isum) ranked by (count
-// desc, row desc, hypothesis asc) with the keys of select_topk_k, the first topk kept (all when fewer), sorted by
-// (row, hypothesis), duplicate rows merged to the lowest hypothesis (its intensity sum) and the highest count: the
-// slots select_topk_k writes without pair closure, plus c_isum.  The positions of the hits inside a region depend
-// on the order in which K1's items appended them, the selection and the output do not.  Spectra with more hits
-// than shared memory holds take the radix select over the hit lists in global memory and a second read.
+// Visits the hits vk_k1_hits wrote for one hypothesis (window [lo, hi), region start `region`, tile shift `shift`;
+// shift 0: no item of the hypothesis ran, nothing to visit), in row order: segment by segment (one per tile the
+// window covers), 32 slots at a time up to the segment's end mark.  f(ok, slot, value) is called by the whole warp;
+// lanes with ok hold a hit.
+template <class F>
+__device__ __forceinline__ void for_hyp_hits(int64_t lo, int64_t hi, int shift, int64_t region, const uint64_t* rc,
+                                             int lane, F&& f) {
+  if (hi <= lo || shift <= 0) return;
+  for (int64_t t = lo >> shift; t <= (hi - 1) >> shift; ++t) {
+    const int64_t a = max(lo, t << shift), b = min(hi, (t + 1) << shift);
+    const int64_t seg = region + (a - lo), len = b - a;
+    for (int64_t j0 = 0; j0 < len; j0 += 32) {
+      const int64_t j = j0 + lane;
+      const uint64_t v = j < len ? rc[seg + j] : VK_HIT_END;
+      const unsigned end = __ballot_sync(VK_FULL, v == VK_HIT_END);
+      const int n_ok = end ? __ffs(end) - 1 : 32;
+      f(lane < n_ok, seg + j, v);
+      if (end) break;
+    }
+  }
+}
+
+__device__ __forceinline__ int hit_count(uint64_t v) { return (int)min(v >> 32, (uint64_t)INT32_MAX); }
+__device__ __forceinline__ int64_t hit_row(uint64_t v) { return (int64_t)(uint32_t)v; }
+
+// Shortlist from the hit lists of vk_k1_hits, one warp per spectrum: the hits of the spectrum's hypotheses ranked by
+// (count desc, row desc, hypothesis asc) with the keys of select_topk_k, the first topk kept (all when fewer),
+// optionally with pair closure, sorted by (row, hypothesis), duplicate rows merged to the lowest hypothesis (its
+// intensity sum) and the highest count: the slots select_topk_k writes, plus c_isum.
+//   Fast path (no closure, at most 32 hypotheses, their windows pairwise disjoint -- the usual case): the hypotheses
+//   are visited in window order and each one's hits come in row order, so the collected hits are already sorted by
+//   row with no duplicates; selection keeps that order and no sort is needed.
+//   Otherwise: collect, select, add partners, bitonic sort and merge.  Spectra with more hits than shared memory
+//   holds run the radix select over the hit lists in global memory and a second read.
 __global__ void __launch_bounds__(TK_WARPS * 32)
-select_hits_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* win_off, const uint32_t* hyp_hits,
-              const uint64_t* rc, const uint32_t* hit_isum, const uint32_t* hyp_scored, const uint64_t* hyp_matched,
-              int topk, int pair_closure, const int64_t* partner, int cap, int list_pow2, int key_cap,
-              int64_t* c_hyp, int64_t* c_row, int64_t* c_cnt, uint32_t* c_isum, int64_t* n_cand,
-              int64_t* spec_scored, int64_t* spec_matched) {
+select_hits_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo, const int64_t* h_hi,
+              const int64_t* win_off, const int8_t* hyp_shift, const uint64_t* rc, const uint32_t* hit_isum,
+              const uint32_t* hyp_scored, const uint64_t* hyp_matched, int topk, int pair_closure,
+              const int64_t* partner, int cap, int list_pow2, int key_cap, int64_t* c_hyp, int64_t* c_row,
+              int64_t* c_cnt, uint32_t* c_isum, int64_t* n_cand, int64_t* spec_scored, int64_t* spec_matched) {
   extern __shared__ __align__(16) uint8_t tk_smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int s = blockIdx.x * TK_WARPS + warp;
@@ -288,7 +315,7 @@ select_hits_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* win_off, c
   const size_t per_warp = (size_t)key_cap * 12 + (size_t)list_pow2 * 16 + 256 * 4;
   uint8_t* base = tk_smem + per_warp * warp;
   uint64_t* key = reinterpret_cast<uint64_t*>(base);
-  uint32_t* src = reinterpret_cast<uint32_t*>(base + (size_t)key_cap * 8);   // hit position - win_off[hb]
+  uint32_t* src = reinterpret_cast<uint32_t*>(base + (size_t)key_cap * 8);   // hit slot - win_off[hb]
   int32_t* row = reinterpret_cast<int32_t*>(src + key_cap);
   int32_t* hl = row + list_pow2;
   int32_t* cnt = hl + list_pow2;
@@ -296,7 +323,9 @@ select_hits_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* win_off, c
   uint32_t* hist = isum + list_pow2;
   const unsigned lt_mask = (1u << lane) - 1u;
   const int64_t hb = spec_hyp_off[s], he = spec_hyp_off[s + 1];
+  const int nhs = (int)(he - hb);
   const int64_t w_base = he > hb ? win_off[hb] : 0;
+  const int64_t slot = (int64_t)s * cap;
   // per-spectrum statistics from K1's per-hypothesis totals
   long long sc = 0, mt = 0;
   for (int64_t h = hb + lane; h < he; h += 32) {
@@ -309,27 +338,83 @@ select_hits_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* win_off, c
     spec_scored[s] = sc;
     spec_matched[s] = mt;
   }
-  auto n_hits = [&](int64_t h) -> int64_t {   // a region never holds more than its window
-    return min((int64_t)hyp_hits[h], win_off[h + 1] - win_off[h]);
+  auto visit = [&](int64_t h, auto&& f) {
+    for_hyp_hits(h_lo[h], h_hi[h], hyp_shift[h], win_off[h], rc, lane, f);
   };
-  // the hits as selection keys in shared memory (as many as fit)
+
+  // ---------------------------------------------------------------- fast path
+  bool fast = !pair_closure && nhs <= 32;
+  int my_rank = 0;
+  if (fast) {
+    const bool mine = lane < nhs;
+    const int64_t my_lo = mine ? h_lo[hb + lane] : 0, my_hi = mine ? h_hi[hb + lane] : 0;
+    const bool live = mine && my_hi > my_lo;
+    bool overlap = false;
+    for (int j = 0; j < nhs; ++j) {
+      const int64_t lo_j = __shfl_sync(VK_FULL, my_lo, j), hi_j = __shfl_sync(VK_FULL, my_hi, j);
+      const bool live_j = hi_j > lo_j;
+      if (live && live_j && j != lane) {
+        if (lo_j < my_lo || (lo_j == my_lo && j < lane)) ++my_rank;
+        overlap |= lo_j < my_hi && my_lo < hi_j;
+      }
+      if (mine && !live && live_j) ++my_rank;   // empty windows after every live one
+      if (mine && !live && !live_j && j < lane) ++my_rank;
+    }
+    fast = !__any_sync(VK_FULL, overlap);
+  }
+  if (fast) {
+    long long n_app = 0;
+    for (int r = 0; r < nhs; ++r) {
+      const int j = __ffs(__ballot_sync(VK_FULL, lane < nhs && my_rank == r)) - 1;
+      visit(hb + j, [&](bool ok, int64_t pos, uint64_t v) {
+        const unsigned m = __ballot_sync(VK_FULL, ok);
+        const long long at = n_app + __popc(m & lt_mask);
+        if (ok && at < key_cap) {
+          key[at] = sel_key(hit_count(v), hit_row(v), j);
+          src[at] = (uint32_t)(pos - w_base);
+        }
+        n_app += __popc(m);
+      });
+    }
+    __syncwarp();
+    if (n_app <= key_cap) {
+      const int n_k = (int)n_app;
+      const bool limit = n_k > topk;
+      const uint64_t kth = limit ? smem_kth_largest(key, n_k, topk, hist, lane) : 0ull;
+      int n_out = 0;
+      for (int i0 = 0; i0 < n_k; i0 += 32) {
+        const int i = i0 + lane;
+        const uint64_t k = i < n_k ? key[i] : 0ull;
+        const bool take = i < n_k && (!limit || k >= kth);
+        const unsigned m = __ballot_sync(VK_FULL, take);
+        if (take) {
+          const int64_t pos = w_base + src[i];
+          const uint64_t v = rc[pos];
+          const int64_t at = slot + n_out + __popc(m & lt_mask);
+          c_hyp[at] = hb + ((1 << 18) - 1 - (int)(k & 0x3ffff));
+          c_row[at] = hit_row(v);
+          c_cnt[at] = hit_count(v);
+          if (c_isum) c_isum[at] = hit_isum[pos];
+        }
+        n_out += __popc(m);
+      }
+      if (lane == 0) n_cand[s] = n_out;
+      return;
+    }
+  }
+
+  // ---------------------------------------------------------------- general path
   long long n_app = 0;
   for (int64_t h = hb; h < he; ++h) {
-    const int64_t r0 = win_off[h], n = n_hits(h);
-    for (int64_t j0 = 0; j0 < n; j0 += 32) {
-      const int64_t j = j0 + lane;
-      const bool ok = j < n;
+    visit(h, [&](bool ok, int64_t pos, uint64_t v) {
       const unsigned m = __ballot_sync(VK_FULL, ok);
-      if (ok) {
-        const long long at = n_app + __popc(m & lt_mask);
-        if (at < key_cap) {
-          const uint64_t v = rc[r0 + j];
-          key[at] = sel_key((int)min(v >> 32, (uint64_t)INT32_MAX), (int64_t)(uint32_t)v, (int)(h - hb));
-          src[at] = (uint32_t)(r0 + j - w_base);
-        }
+      const long long at = n_app + __popc(m & lt_mask);
+      if (ok && at < key_cap) {
+        key[at] = sel_key(hit_count(v), hit_row(v), (int)(h - hb));
+        src[at] = (uint32_t)(pos - w_base);
       }
       n_app += __popc(m);
-    }
+    });
   }
   __syncwarp();
   const bool limit = n_app > topk;
@@ -339,9 +424,9 @@ select_hits_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* win_off, c
     if (take) {
       const int at = n_sel + __popc(m & lt_mask);
       const uint64_t v = rc[pos_g];
-      row[at] = (int32_t)(uint32_t)v;
+      row[at] = (int32_t)hit_row(v);
       hl[at] = h_local;
-      cnt[at] = (int32_t)min(v >> 32, (uint64_t)INT32_MAX);
+      cnt[at] = hit_count(v);
       isum[at] = hit_isum ? hit_isum[pos_g] : 0u;
     }
     n_sel += __popc(m);
@@ -362,12 +447,11 @@ select_hits_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* win_off, c
       for (int i = lane; i < 256; i += 32) hist[i] = 0;
       __syncwarp();
       for (int64_t h = hb; h < he; ++h) {
-        const int64_t r0 = win_off[h], n = n_hits(h);
-        for (int64_t j = lane; j < n; j += 32) {
-          const uint64_t v = rc[r0 + j];
-          const uint64_t k = sel_key((int)min(v >> 32, (uint64_t)INT32_MAX), (int64_t)(uint32_t)v, (int)(h - hb));
+        visit(h, [&](bool ok, int64_t, uint64_t v) {
+          if (!ok) return;
+          const uint64_t k = sel_key(hit_count(v), hit_row(v), (int)(h - hb));
           if ((k & pmask) == prefix) atomicAdd(&hist[(k >> shift) & 255], 1u);
-        }
+        });
       }
       __syncwarp();
       prefix |= (uint64_t)radix_digit(hist, need, lane) << shift;
@@ -375,16 +459,10 @@ select_hits_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* win_off, c
       __syncwarp();
     }
     for (int64_t h = hb; h < he; ++h) {
-      const int64_t r0 = win_off[h], n = n_hits(h);
-      for (int64_t j0 = 0; j0 < n; j0 += 32) {
-        const int64_t j = j0 + lane;
-        bool take = false;
-        if (j < n) {
-          const uint64_t v = rc[r0 + j];
-          take = sel_key((int)min(v >> 32, (uint64_t)INT32_MAX), (int64_t)(uint32_t)v, (int)(h - hb)) >= prefix;
-        }
-        take_hit(take, r0 + j, (int)(h - hb));
-      }
+      visit(h, [&](bool ok, int64_t pos, uint64_t v) {
+        const bool take = ok && sel_key(hit_count(v), hit_row(v), (int)(h - hb)) >= prefix;
+        take_hit(take, pos, (int)(h - hb));
+      });
     }
   }
   __syncwarp();
@@ -408,7 +486,6 @@ select_hits_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* win_off, c
   __syncwarp();
   warp_bitonic_u64(key, n_pow2, lane);
   int n_out = 0;
-  const int64_t slot = (int64_t)s * cap;
   for (int i0 = 0; i0 < n_list; i0 += 32) {
     const int i = i0 + lane;
     bool head = false;
@@ -506,14 +583,14 @@ int vk_compact_hits(int n_spec, int cap, const int64_t* n_cand, const int64_t* c
   return vk_launch_status();
 }
 
-int vk_select_hits(int n_spec, const int64_t* spec_hyp_off, const int64_t* win_off, const uint32_t* hyp_hits,
-                   const uint64_t* hit_rc, const uint32_t* hit_isum, const uint32_t* hyp_scored,
-                   const uint64_t* hyp_matched, int topk, int pair_closure, const int64_t* partner, int cap,
-                   int64_t* c_hyp, int64_t* c_row, int64_t* c_cnt, uint32_t* c_isum, int64_t* n_cand,
-                   int64_t* spec_scored, int64_t* spec_matched, void* stream) {
+int vk_select_hits(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo, const int64_t* h_hi,
+                   const int64_t* win_off, const int8_t* hyp_shift, const uint64_t* hit_rc, const uint32_t* hit_isum,
+                   const uint32_t* hyp_scored, const uint64_t* hyp_matched, int topk, int pair_closure,
+                   const int64_t* partner, int cap, int64_t* c_hyp, int64_t* c_row, int64_t* c_cnt, uint32_t* c_isum,
+                   int64_t* n_cand, int64_t* spec_scored, int64_t* spec_matched, void* stream) {
   if (n_spec == 0) return 0;
   if (topk < 1 || topk > 8192 || cap < (pair_closure ? 2 : 1) * topk) return VK_E_ARG;
-  if (!c_isum != !hit_isum || (pair_closure && !partner)) return VK_E_ARG;
+  if (!c_isum != !hit_isum || (pair_closure && !partner) || !h_lo || !h_hi || !hyp_shift) return VK_E_ARG;
   int list_pow2 = 32;
   while (list_pow2 < (pair_closure ? 2 : 1) * topk) list_pow2 <<= 1;
   const int key_cap = list_pow2 > 512 ? list_pow2 : 512;
@@ -523,8 +600,9 @@ int vk_select_hits(int n_spec, const int64_t* spec_hyp_off, const int64_t* win_o
   cudaError_t e = cudaFuncSetAttribute(select_hits_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
   if (e != cudaSuccess) return vk_err(e);
   select_hits_k<<<(unsigned)((n_spec + TK_WARPS - 1) / TK_WARPS), TK_WARPS * 32, sh, (cudaStream_t)stream>>>(
-      n_spec, spec_hyp_off, win_off, hyp_hits, hit_rc, hit_isum, hyp_scored, hyp_matched, topk, pair_closure,
-      partner, cap, list_pow2, key_cap, c_hyp, c_row, c_cnt, c_isum, n_cand, spec_scored, spec_matched);
+      n_spec, spec_hyp_off, h_lo, h_hi, win_off, hyp_shift, hit_rc, hit_isum, hyp_scored, hyp_matched, topk,
+      pair_closure, partner, cap, list_pow2, key_cap, c_hyp, c_row, c_cnt, c_isum, n_cand, spec_scored,
+      spec_matched);
   return vk_launch_status();
 }
 

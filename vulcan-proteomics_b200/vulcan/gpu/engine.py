@@ -606,11 +606,11 @@ def _k1_hits(gi: GpuIndex, dh, peaks, p: SearchParams, n_hyp: int, thr: int, isu
     L = K.lib()
     dev = gi.dev
     nh = max(n_hyp, 1)
-    # hyp_hits (u32), hyp_scored (u32), hyp_matched (u64): one zeroed allocation
-    z = torch.zeros(nh * 2, dtype=torch.int64, device=dev)
-    counters = z[:nh].view(torch.int32)
-    hyp_hits, hyp_scored = counters[:nh], counters[nh:]
-    hyp_matched = z[nh:]
+    # hyp_scored (u32), hyp_matched (u64), hyp_shift (i8): one zeroed allocation
+    z = torch.zeros(nh * 3, dtype=torch.int64, device=dev)
+    hyp_scored = z[:nh].view(torch.int32)[:nh]
+    hyp_matched = z[nh:2 * nh]
+    hyp_shift = z[2 * nh:].view(torch.int8)[:nh]
     rc = hisum = pl = None
     for tix, warps, pl, keys, filt, n_kz, kstride in _k1_passes(gi, dh, peaks, p, n_hyp, caps):
         cap = pl["cnt_cap"]
@@ -622,11 +622,11 @@ def _k1_hits(gi: GpuIndex, dh, peaks, p: SearchParams, n_hyp: int, thr: int, isu
                              K.ptr(dh["spec"]), K.ptr(dh["maxfz"]), K.ptr(dh["lo"]), K.ptr(dh["hi"]),
                              K.ptr(pl["win_off"]), cap, K.ptr(peaks["off"]), K.ptr(peaks["mass"]),
                              int(thr) if h_thr is None else 0, K.ptr(h_thr), K.ptr(rc),
-                             K.ptr(hisum) if isum else None, K.ptr(hyp_hits), K.ptr(hyp_scored), K.ptr(hyp_matched),
+                             K.ptr(hisum) if isum else None, K.ptr(hyp_shift), K.ptr(hyp_scored), K.ptr(hyp_matched),
                              K.ptr(pl["status"]), K.ptr(peaks["int"]) if isum else None,
                              K.ptr(peaks["tic"]) if isum else None, K.ptr(keys), K.ptr(filt), n_kz, kstride,
                              K.stream()), "k1_hits")
-    return {"win_off": pl["win_off"], "status": pl["status"], "rc": rc, "isum": hisum, "hyp_hits": hyp_hits,
+    return {"win_off": pl["win_off"], "status": pl["status"], "rc": rc, "isum": hisum, "hyp_shift": hyp_shift,
             "hyp_scored": hyp_scored, "hyp_matched": hyp_matched}
 
 
@@ -646,8 +646,9 @@ def _shortlist_hits(gi: GpuIndex, p: SearchParams, n: int, dh, k1h: dict, topk: 
     n_cand = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
     spec_scored = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
     spec_matched = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
-    K.check(L.vk_select_hits(n, K.ptr(dh["spec_off"]), K.ptr(k1h["win_off"]), K.ptr(k1h["hyp_hits"]),
-                             K.ptr(k1h["rc"]), K.ptr(k1h["isum"]) if isum else None, K.ptr(k1h["hyp_scored"]),
+    K.check(L.vk_select_hits(n, K.ptr(dh["spec_off"]), K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(k1h["win_off"]),
+                             K.ptr(k1h["hyp_shift"]), K.ptr(k1h["rc"]), K.ptr(k1h["isum"]) if isum else None,
+                             K.ptr(k1h["hyp_scored"]),
                              K.ptr(k1h["hyp_matched"]), topk, int(closure), K.ptr(gi.partner), cap, K.ptr(s_hyp),
                              K.ptr(s_row), K.ptr(s_cnt),
                              K.ptr(s_isum) if isum else None, K.ptr(n_cand), K.ptr(spec_scored),
