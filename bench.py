@@ -434,11 +434,16 @@ def run_b200(a):
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
+        se.host_s = {k: 0.0 for k in se.host_s}
         t0 = time.perf_counter()
         res = se.search_many([pinned] * e2e_steps)
         torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        e2e_parts.append({"wall_ms_per_run": round(1e3 * wall / e2e_steps, 4),
+                          **{f"host_{k}_ms_per_run": round(1e3 * v / e2e_steps, 4) for k, v in se.host_s.items()}})
         from vulcan.gpu.replicas import max_over_ranks
-        return len(sp) * world * e2e_steps / max_over_ranks(time.perf_counter() - t0, dev), res[-1][1]
+        return len(sp) * world * e2e_steps / max_over_ranks(wall, dev), res[-1][1]
+    e2e_parts = []
     e2e, s2 = e2e_rate(pr)
     h2d, d2h = s2.h2d_bytes, s2.d2h_bytes
     h2d_copy = _h2d_rate(pinned, run, dev)
@@ -507,7 +512,8 @@ def run_b200(a):
             "data": "synthetic",
             "config": _config(w, p, extra),
             "e2e": {"value": round(e2e, 1), "unit": "spectra/s", "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h), "h2d_copy_alone": h2d_copy},
+                    "d2h_bytes_per_step": int(d2h), "h2d_copy_alone": h2d_copy,
+                    "per_run": e2e_parts[0] if e2e_parts else None},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1),
                          "peak": peak_gbs, "unit": "GB/s", "frac": round(achieved / peak_gbs, 4),
@@ -595,7 +601,7 @@ def _kernel_table(a, p, gi, run, flush, pr, dev):
                 C.byref(gi.tix), C.byref(gi.fp), float(p.fragment_ppm[0]), float(p.fragment_ppm[1]), p.k1_warps,
                 K.ptr(item_off), K.ptr(item_hyp), nm, pl["item_cap"], K.ptr(dh["spec"]), K.ptr(dh["maxfz"]),
                 K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(win_off), pl["cnt_cap"], K.ptr(peaks["off"]),
-                K.ptr(peaks["mass"]), thr, None, K.ptr(k1h["rc"]), K.ptr(k1h["isum"]),
+                K.ptr(peaks["mass"]), thr, None, K.ptr(k1h["rc"]), K.ptr(k1h["isum"]), K.ptr(k1h["seg_cnt"]),
                 K.ptr(z[2 * nm:].view(torch.int8)[:nm]), K.ptr(z[:nm].view(torch.int32)[:nm]), K.ptr(z[nm:2 * nm]),
                 K.ptr(pl["status"]), K.ptr(peaks["int"]), K.ptr(peaks["tic"]), K.ptr(keys), K.ptr(filt), n_kz,
                 kstride, K.stream()), "k1_hits")
@@ -605,7 +611,8 @@ def _kernel_table(a, p, gi, run, flush, pr, dev):
         n_k1_hits = int((cnt_d[:n_win] >= thr).sum())
         del cnt_d
         kern["k1_tiles_k (hit lists)"] = (ms_k1, k1_algorithmic_bytes(gi, dh, peaks, item_off, nh, True,
-                                                                       n_k1_hits * 12 + nh * 13))
+                                                                       n_k1_hits * 12 + int(item_off[-1]) * 4 +
+                                                                       nh * 13))
         tk = {k: torch.empty(max(n * cap, 1), dtype=torch.int64, device=dev) for k in ("h", "r", "c")}
         ti = torch.empty(max(n * cap, 1), dtype=torch.int32, device=dev)
         tk_n = torch.empty(n, dtype=torch.int64, device=dev)
@@ -613,12 +620,12 @@ def _kernel_table(a, p, gi, run, flush, pr, dev):
         sm_ = torch.empty(n, dtype=torch.int64, device=dev)
         ms_tk = timed(lambda: K.check(L.vk_select_hits(
             n, K.ptr(dh["spec_off"]), K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(win_off), K.ptr(k1h["hyp_shift"]),
-            K.ptr(k1h["rc"]), K.ptr(k1h["isum"]), K.ptr(k1h["hyp_scored"]), K.ptr(k1h["hyp_matched"]), p.topk, 0,
+            K.ptr(k1h["seg_cnt"]), K.ptr(k1h["rc"]), K.ptr(k1h["isum"]), K.ptr(k1h["hyp_scored"]), K.ptr(k1h["hyp_matched"]), p.topk, 0,
             None, cap, K.ptr(tk["h"]), K.ptr(tk["r"]),
             K.ptr(tk["c"]), K.ptr(ti), K.ptr(tk_n), K.ptr(ss_), K.ptr(sm_), K.stream()), "select_hits"))
         # hits read (12 B), per-hypothesis windows, totals and tile shift (33 B), per spectrum its hypothesis range
         # and outputs; the shortlist written (28 B per kept hit)
-        kern["select_hits_k"] = (ms_tk, n_k1_hits * 12 + nh * 41 + n * 32 + n_hit * 28)
+        kern["select_hits_k"] = (ms_tk, n_k1_hits * 12 + int(item_off[-1]) * 4 + nh * 41 + n * 32 + n_hit * 28)
     else:
         cnt = so["cnt"]
         status = torch.zeros(1, dtype=torch.int32, device=dev)

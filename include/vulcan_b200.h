@@ -252,8 +252,8 @@ int vk_k1_peak_keys(const vk_tindex* ix, const vk_frag_params* fp, float tol_lo,
  * but instead of a dense count per window row, each (tile, hypothesis) item writes the rows of its tile with count >=
  * thr (>= 1; h_thr[h] instead when h_thr is given, i32 per hypothesis) in row order to the start of its segment of
  * the hypothesis' region -- the slots win_off[h] + (row - lo[h]) of the window rows the tile holds -- as hit_rc
- * (u64: count << 32 | row) and, with pk_int/tic, hit_isum (the summed matched intensity of vk_k1_tiles' isum), then
- * the end mark VK_HIT_END (all ones) when the segment has slots left; hyp_shift[h] (i8, zeroed by the caller) gets
+ * (u64: count << 32 | row) and, with pk_int/tic, hit_isum (the summed matched intensity of vk_k1_tiles' isum), and
+ * their number to seg_cnt (u32, same slots) at the segment's first slot; hyp_shift[h] (i8, zeroed by the caller) gets
  * the tiling's tile_shift, which fixes the segment boundaries; hyp_scored (u32, rows with count > 0) and hyp_matched
  * (u64, sum of counts) are accumulated with atomics (zeroed by the caller).  No atomic decides a position: the
  * layout does not depend on scheduling.  cnt_cap bounds hit_rc / hit_isum like vk_k1_tiles' cnt.  Reference
@@ -262,8 +262,8 @@ int vk_k1_hits(const vk_tindex* ix, const vk_frag_params* fp, float tol_lo, floa
                const int64_t* tile_item_off, const int32_t* item_hyp, int64_t n_hyp, int64_t item_cap,
                const int32_t* h_spec, const int8_t* h_maxfz, const int64_t* h_lo, const int64_t* h_hi,
                const int64_t* win_off, int64_t cnt_cap, const int64_t* pk_off, const float* pk_mass, int thr,
-               const int32_t* h_thr, uint64_t* hit_rc, uint32_t* hit_isum, int8_t* hyp_shift, uint32_t* hyp_scored,
-               uint64_t* hyp_matched, int32_t* status, const float* pk_int, const float* tic,
+               const int32_t* h_thr, uint64_t* hit_rc, uint32_t* hit_isum, uint32_t* seg_cnt, int8_t* hyp_shift,
+               uint32_t* hyp_scored, uint64_t* hyp_matched, int32_t* status, const float* pk_int, const float* tic,
                const uint32_t* pk_keys, const uint32_t* pk_filt, int n_kz, int64_t kstride, void* stream);
 
 /* Top-K + pair closure (reference vulcan/gpu/engine.py:284-312) per spectrum, from the dense K1 counts.
@@ -285,12 +285,14 @@ int vk_select_topk(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo,
  * with pair_closure the partner rows added with count -1; sorted by row, duplicate rows merged to the lowest
  * hypothesis and highest count: the slots of vk_select_topk (cap >= (pair_closure ? 2 : 1) * topk) plus c_isum
  * (u32, the kept hit's intensity sum, 0 for a partner-only row; NULL when hit_isum is NULL), and spec_scored /
- * spec_matched (i64, may be NULL) summed from K1's per-hypothesis totals; h_lo / h_hi / win_off / hyp_shift
- * locate each hypothesis' hit segments.  The same candidates as vk_select_topk over vk_k1_tiles' dense counts with
+ * spec_matched (i64, may be NULL) summed from K1's per-hypothesis totals; h_lo / h_hi / win_off / hyp_shift /
+ * seg_cnt locate each hypothesis' hit segments (per 32 segments, one parallel read of their counts, then one of
+ * their hits).  The same candidates as vk_select_topk over vk_k1_tiles' dense counts with
  * thr = vk_k1_hits' thr.  Without closure, when a spectrum's windows are pairwise disjoint (the usual case), the
  * hits are collected in row order and kept in that order, with no sort. */
 int vk_select_hits(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo, const int64_t* h_hi,
-                   const int64_t* win_off, const int8_t* hyp_shift, const uint64_t* hit_rc, const uint32_t* hit_isum,
+                   const int64_t* win_off, const int8_t* hyp_shift, const uint32_t* seg_cnt, const uint64_t* hit_rc,
+                   const uint32_t* hit_isum,
                    const uint32_t* hyp_scored, const uint64_t* hyp_matched, int topk, int pair_closure,
                    const int64_t* partner, int cap, int64_t* c_hyp, int64_t* c_row, int64_t* c_cnt, uint32_t* c_isum,
                    int64_t* n_cand, int64_t* spec_scored, int64_t* spec_matched, void* stream);

@@ -20,9 +20,6 @@
 #define VK_STATUS_WAIT_TIMEOUT 1
 #define VK_STATUS_OVERFLOW 2
 
-// End mark of a K1 hit-list segment (a hit is count << 32 | row with count >= 1, so never all ones).
-#define VK_HIT_END 0xffffffffffffffffull
-
 namespace vk {
 
 // Fragment constants copied into shared memory by kernels that index them per lane.

@@ -59,15 +59,16 @@ struct K1Rec {
 
 // Outputs of the hit-list form of K1 (vk_k1_hits): instead of a dense count per window row, each (tile, hypothesis)
 // item writes the rows of its tile with count >= thr, in row order, to the start of its own segment of the
-// hypothesis' region -- the slots of the window rows it covers -- as count << 32 | row (rc) and isum, followed by
-// the end mark VK_HIT_END when fewer than the segment's slots are used; hyp_shift[h] gets the tiling's tile shift (the
-// segment boundaries); per hypothesis the number of rows with a nonzero count and the sum of the counts (integer
-// atomics).  No atomic decides a position, so the layout does not depend on scheduling.
+// hypothesis' region -- the slots of the window rows it covers -- as count << 32 | row (rc) and isum, and the number
+// of those rows to seg_cnt at the segment's first slot; hyp_shift[h] gets the tiling's tile shift (the segment
+// boundaries); per hypothesis the number of rows with a nonzero count and the sum of the counts (integer atomics).
+// No atomic decides a position, so the layout does not depend on scheduling.
 struct K1Hits {
   int thr;
   const int32_t* h_thr;   // per-hypothesis thresholds (NULL: thr for all)
   uint64_t* rc;
   uint32_t* isum;
+  uint32_t* seg_cnt;
   int8_t* hyp_shift;
   uint32_t* hyp_scored;
   unsigned long long* hyp_matched;
@@ -183,7 +184,7 @@ k1_tiles_k(vk_tindex ix, float tol_lo, float tol_hi, int tol_da, int post_cap, c
       __syncwarp();
       if (HITS) {
         // the item's segment: the slots of the window rows rlo..rhi of this tile (r.base is the region index of
-        // the tile's row 0); kept rows compacted to its start in row order, then the end mark
+        // the tile's row 0); kept rows compacted to its start in row order, their number at its first slot
         const int64_t seg = r.base + rlo;
         const int thr_h = hits.h_thr ? hits.h_thr[r.h] : hits.thr;
         long long sc = 0, mt = 0;
@@ -205,7 +206,7 @@ k1_tiles_k(vk_tindex ix, float tol_lo, float tol_hi, int tol_da, int post_cap, c
         sc = vk::warp_sum(sc);
         mt = vk::warp_sum(mt);
         if (lane == 0) {
-          if (n_kept < rhi - rlo) hits.rc[seg + n_kept] = VK_HIT_END;
+          hits.seg_cnt[seg] = (uint32_t)n_kept;
           hits.hyp_shift[r.h] = (int8_t)ix.tile_shift;   // every item of h writes the same value
           if (sc) atomicAdd(&hits.hyp_scored[r.h], (uint32_t)sc);
           if (mt) atomicAdd(&hits.hyp_matched[r.h], (unsigned long long)mt);
@@ -324,12 +325,12 @@ int vk_k1_hits(const vk_tindex* ix, const vk_frag_params* fp, float tol_lo, floa
                const int64_t* tile_item_off, const int32_t* item_hyp, int64_t n_hyp, int64_t item_cap,
                const int32_t* h_spec, const int8_t* h_maxfz, const int64_t* h_lo, const int64_t* h_hi,
                const int64_t* win_off, int64_t cnt_cap, const int64_t* pk_off, const float* pk_mass, int thr,
-               const int32_t* h_thr, uint64_t* hit_rc, uint32_t* hit_isum, int8_t* hyp_shift, uint32_t* hyp_scored,
-               uint64_t* hyp_matched, int32_t* status, const float* pk_int, const float* tic,
+               const int32_t* h_thr, uint64_t* hit_rc, uint32_t* hit_isum, uint32_t* seg_cnt, int8_t* hyp_shift,
+               uint32_t* hyp_scored, uint64_t* hyp_matched, int32_t* status, const float* pk_int, const float* tic,
                const uint32_t* pk_keys, const uint32_t* pk_filt, int n_kz, int64_t kstride, void* stream) {
-  if (!hit_rc || !hyp_shift || !hyp_scored || !hyp_matched || (!h_thr && thr < 1)) return VK_E_ARG;
+  if (!hit_rc || !seg_cnt || !hyp_shift || !hyp_scored || !hyp_matched || (!h_thr && thr < 1)) return VK_E_ARG;
   if ((hit_isum != nullptr) != (pk_int != nullptr)) return VK_E_ARG;
-  K1Hits hits{thr, h_thr, hit_rc, hit_isum, hyp_shift, hyp_scored,
+  K1Hits hits{thr, h_thr, hit_rc, hit_isum, seg_cnt, hyp_shift, hyp_scored,
               reinterpret_cast<unsigned long long*>(hyp_matched)};
   return k1_tiles_launch<true>(ix, fp, tol_lo, tol_hi, warps, tile_item_off, item_hyp, n_hyp, item_cap, h_spec,
                                h_maxfz, h_lo, h_hi, win_off, cnt_cap, pk_off, pk_mass, nullptr, status, pk_int, tic,

@@ -268,25 +268,86 @@ select_topk_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo, cons
   if (lane == 0) n_cand[s] = n_out;
 }
 
-// Visits the hits vk_k1_hits wrote for one hypothesis (window [lo, hi), region start `region`, tile shift `shift`;
-// shift 0: no item of the hypothesis ran, nothing to visit), in row order: segment by segment (one per tile the
-// window covers), 32 slots at a time up to the segment's end mark.  f(ok, slot, value) is called by the whole warp;
-// lanes with ok hold a hit.
+// Per-warp scratch of the hit reader: up to 32 hypotheses in visiting order and one chunk of 32 segments.
+struct HitScratch {
+  int64_t lo[32], region[32], t0[32];
+  int32_t shift[32], hyp[32], seg_base[32];
+  int64_t slot[32];
+  int32_t pos[32], who[32];
+};
+
+// Visits the hits vk_k1_hits wrote for the hypotheses hb + S.hyp[0 .. nv) (nv <= 32, in that order): their segments
+// (one per tile a window covers; a hypothesis with tile shift 0 ran no item and has none) in hypothesis order, tile
+// order, and each segment's hits in row order.  Two parallel rounds per 32 segments: their hit counts (seg_cnt at
+// the segment's first slot), then the hits themselves spread over the lanes.  f(ok, slot, value, local hypothesis)
+// is called by the whole warp; lanes with ok hold a hit.
 template <class F>
-__device__ __forceinline__ void for_hyp_hits(int64_t lo, int64_t hi, int shift, int64_t region, const uint64_t* rc,
-                                             int lane, F&& f) {
-  if (hi <= lo || shift <= 0) return;
-  for (int64_t t = lo >> shift; t <= (hi - 1) >> shift; ++t) {
-    const int64_t a = max(lo, t << shift), b = min(hi, (t + 1) << shift);
-    const int64_t seg = region + (a - lo), len = b - a;
-    for (int64_t j0 = 0; j0 < len; j0 += 32) {
-      const int64_t j = j0 + lane;
-      const uint64_t v = j < len ? rc[seg + j] : VK_HIT_END;
-      const unsigned end = __ballot_sync(VK_FULL, v == VK_HIT_END);
-      const int n_ok = end ? __ffs(end) - 1 : 32;
-      f(lane < n_ok, seg + j, v);
-      if (end) break;
+__device__ __forceinline__ void gather_hits(HitScratch& S, int nv, int64_t hb, const int64_t* h_lo, const int64_t* h_hi,
+                                            const int64_t* win_off, const int8_t* hyp_shift, const uint32_t* seg_cnt,
+                                            const uint64_t* rc, int lane, F&& f) {
+  int nt = 0;
+  if (lane < nv) {
+    const int64_t h = hb + S.hyp[lane];
+    const int64_t lo = h_lo[h], hi = h_hi[h];
+    const int sh = hyp_shift[h];
+    int64_t t0 = 0;
+    if (hi > lo && sh > 0) {
+      t0 = lo >> sh;
+      nt = (int)(((hi - 1) >> sh) - t0 + 1);
     }
+    S.lo[lane] = lo;
+    S.region[lane] = win_off[h];
+    S.t0[lane] = t0;
+    S.shift[lane] = sh;
+  }
+  const int incl = (int)vk::warp_incl_scan(nt);
+  S.seg_base[lane] = incl - nt;
+  const int total = __shfl_sync(VK_FULL, incl, 31);
+  __syncwarp();
+  for (int k0 = 0; k0 < total; k0 += 32) {
+    const int k = k0 + lane;
+    uint32_t c = 0;
+    int64_t slot = 0;
+    int who = 0;
+    if (k < total) {
+      int a = 0, b = nv;            // the last hypothesis whose first segment is at or before k
+      while (b - a > 1) {
+        const int m = (a + b) >> 1;
+        if (S.seg_base[m] <= k) a = m; else b = m;
+      }
+      who = a;
+      const int sh = S.shift[who];
+      const int64_t t = S.t0[who] + (k - S.seg_base[who]);
+      const int64_t lo = S.lo[who];
+      slot = S.region[who] + (max(lo, t << sh) - lo);
+      c = seg_cnt[slot];
+    }
+    const int pincl = (int)vk::warp_incl_scan((long long)c);
+    const int n_hits = __shfl_sync(VK_FULL, pincl, 31);
+    __syncwarp();
+    S.slot[lane] = slot;
+    S.pos[lane] = pincl - (int)c;
+    S.who[lane] = who;
+    __syncwarp();
+    for (int u0 = 0; u0 < n_hits; u0 += 32) {
+      const int u = u0 + lane;
+      const bool ok = u < n_hits;
+      int64_t at = 0;
+      uint64_t v = 0;
+      int hl = 0;
+      if (ok) {
+        int a = 0, b = 32;          // the segment holding hit u
+        while (b - a > 1) {
+          const int m = (a + b) >> 1;
+          if (S.pos[m] <= u) a = m; else b = m;
+        }
+        at = S.slot[a] + (u - S.pos[a]);
+        v = rc[at];
+        hl = S.hyp[S.who[a]];
+      }
+      f(ok, at, v, hl);
+    }
+    __syncwarp();
   }
 }
 
@@ -304,7 +365,8 @@ __device__ __forceinline__ int64_t hit_row(uint64_t v) { return (int64_t)(uint32
 //   holds run the radix select over the hit lists in global memory and a second read.
 __global__ void __launch_bounds__(TK_WARPS * 32)
 select_hits_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo, const int64_t* h_hi,
-              const int64_t* win_off, const int8_t* hyp_shift, const uint64_t* rc, const uint32_t* hit_isum,
+              const int64_t* win_off, const int8_t* hyp_shift, const uint32_t* seg_cnt, const uint64_t* rc,
+              const uint32_t* hit_isum,
               const uint32_t* hyp_scored, const uint64_t* hyp_matched, int topk, int pair_closure,
               const int64_t* partner, int cap, int list_pow2, int key_cap, int64_t* c_hyp, int64_t* c_row,
               int64_t* c_cnt, uint32_t* c_isum, int64_t* n_cand, int64_t* spec_scored, int64_t* spec_matched) {
@@ -312,8 +374,9 @@ select_hits_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo, cons
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int s = blockIdx.x * TK_WARPS + warp;
   if (s >= n_spec) return;
-  const size_t per_warp = (size_t)key_cap * 12 + (size_t)list_pow2 * 16 + 256 * 4;
+  const size_t per_warp = (size_t)key_cap * 12 + (size_t)list_pow2 * 16 + 256 * 4 + sizeof(HitScratch);
   uint8_t* base = tk_smem + per_warp * warp;
+  HitScratch& S = *reinterpret_cast<HitScratch*>(base + per_warp - sizeof(HitScratch));
   uint64_t* key = reinterpret_cast<uint64_t*>(base);
   uint32_t* src = reinterpret_cast<uint32_t*>(base + (size_t)key_cap * 8);   // hit slot - win_off[hb]
   int32_t* row = reinterpret_cast<int32_t*>(src + key_cap);
@@ -338,8 +401,14 @@ select_hits_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo, cons
     spec_scored[s] = sc;
     spec_matched[s] = mt;
   }
-  auto visit = [&](int64_t h, auto&& f) {
-    for_hyp_hits(h_lo[h], h_hi[h], hyp_shift[h], win_off[h], rc, lane, f);
+  // every hit of the spectrum's hypotheses in index order, 32 hypotheses at a time
+  auto visit_all = [&](auto&& f) {
+    for (int g0 = 0; g0 < nhs; g0 += 32) {
+      __syncwarp();
+      if (lane < min(32, nhs - g0)) S.hyp[lane] = g0 + lane;
+      __syncwarp();
+      gather_hits(S, min(32, nhs - g0), hb, h_lo, h_hi, win_off, hyp_shift, seg_cnt, rc, lane, f);
+    }
   };
 
   // ---------------------------------------------------------------- fast path
@@ -364,18 +433,19 @@ select_hits_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo, cons
   }
   if (fast) {
     long long n_app = 0;
-    for (int r = 0; r < nhs; ++r) {
-      const int j = __ffs(__ballot_sync(VK_FULL, lane < nhs && my_rank == r)) - 1;
-      visit(hb + j, [&](bool ok, int64_t pos, uint64_t v) {
-        const unsigned m = __ballot_sync(VK_FULL, ok);
-        const long long at = n_app + __popc(m & lt_mask);
-        if (ok && at < key_cap) {
-          key[at] = sel_key(hit_count(v), hit_row(v), j);
-          src[at] = (uint32_t)(pos - w_base);
-        }
-        n_app += __popc(m);
-      });
-    }
+    __syncwarp();
+    if (lane < nhs) S.hyp[my_rank] = lane;     // the hypotheses in window order
+    __syncwarp();
+    gather_hits(S, nhs, hb, h_lo, h_hi, win_off, hyp_shift, seg_cnt, rc, lane,
+                [&](bool ok, int64_t pos, uint64_t v, int hl_) {
+      const unsigned m = __ballot_sync(VK_FULL, ok);
+      const long long at = n_app + __popc(m & lt_mask);
+      if (ok && at < key_cap) {
+        key[at] = sel_key(hit_count(v), hit_row(v), hl_);
+        src[at] = (uint32_t)(pos - w_base);
+      }
+      n_app += __popc(m);
+    });
     __syncwarp();
     if (n_app <= key_cap) {
       const int n_k = (int)n_app;
@@ -405,17 +475,15 @@ select_hits_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo, cons
 
   // ---------------------------------------------------------------- general path
   long long n_app = 0;
-  for (int64_t h = hb; h < he; ++h) {
-    visit(h, [&](bool ok, int64_t pos, uint64_t v) {
-      const unsigned m = __ballot_sync(VK_FULL, ok);
-      const long long at = n_app + __popc(m & lt_mask);
-      if (ok && at < key_cap) {
-        key[at] = sel_key(hit_count(v), hit_row(v), (int)(h - hb));
-        src[at] = (uint32_t)(pos - w_base);
-      }
-      n_app += __popc(m);
-    });
-  }
+  visit_all([&](bool ok, int64_t pos, uint64_t v, int hl_) {
+    const unsigned m = __ballot_sync(VK_FULL, ok);
+    const long long at = n_app + __popc(m & lt_mask);
+    if (ok && at < key_cap) {
+      key[at] = sel_key(hit_count(v), hit_row(v), hl_);
+      src[at] = (uint32_t)(pos - w_base);
+    }
+    n_app += __popc(m);
+  });
   __syncwarp();
   const bool limit = n_app > topk;
   int n_sel = 0;
@@ -446,24 +514,20 @@ select_hits_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo, cons
     for (int shift = 56; shift >= 0; shift -= 8) {
       for (int i = lane; i < 256; i += 32) hist[i] = 0;
       __syncwarp();
-      for (int64_t h = hb; h < he; ++h) {
-        visit(h, [&](bool ok, int64_t, uint64_t v) {
-          if (!ok) return;
-          const uint64_t k = sel_key(hit_count(v), hit_row(v), (int)(h - hb));
-          if ((k & pmask) == prefix) atomicAdd(&hist[(k >> shift) & 255], 1u);
-        });
-      }
+      visit_all([&](bool ok, int64_t, uint64_t v, int hl_) {
+        if (!ok) return;
+        const uint64_t k = sel_key(hit_count(v), hit_row(v), hl_);
+        if ((k & pmask) == prefix) atomicAdd(&hist[(k >> shift) & 255], 1u);
+      });
       __syncwarp();
       prefix |= (uint64_t)radix_digit(hist, need, lane) << shift;
       pmask |= 255ull << shift;
       __syncwarp();
     }
-    for (int64_t h = hb; h < he; ++h) {
-      visit(h, [&](bool ok, int64_t pos, uint64_t v) {
-        const bool take = ok && sel_key(hit_count(v), hit_row(v), (int)(h - hb)) >= prefix;
-        take_hit(take, pos, (int)(h - hb));
-      });
-    }
+    visit_all([&](bool ok, int64_t pos, uint64_t v, int hl_) {
+      const bool take = ok && sel_key(hit_count(v), hit_row(v), hl_) >= prefix;
+      take_hit(take, pos, hl_);
+    });
   }
   __syncwarp();
   // pair closure: the partner row of every kept hit, same hypothesis, count -1 (no intensity sum)
@@ -584,23 +648,24 @@ int vk_compact_hits(int n_spec, int cap, const int64_t* n_cand, const int64_t* c
 }
 
 int vk_select_hits(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo, const int64_t* h_hi,
-                   const int64_t* win_off, const int8_t* hyp_shift, const uint64_t* hit_rc, const uint32_t* hit_isum,
+                   const int64_t* win_off, const int8_t* hyp_shift, const uint32_t* seg_cnt, const uint64_t* hit_rc,
+                   const uint32_t* hit_isum,
                    const uint32_t* hyp_scored, const uint64_t* hyp_matched, int topk, int pair_closure,
                    const int64_t* partner, int cap, int64_t* c_hyp, int64_t* c_row, int64_t* c_cnt, uint32_t* c_isum,
                    int64_t* n_cand, int64_t* spec_scored, int64_t* spec_matched, void* stream) {
   if (n_spec == 0) return 0;
   if (topk < 1 || topk > 8192 || cap < (pair_closure ? 2 : 1) * topk) return VK_E_ARG;
-  if (!c_isum != !hit_isum || (pair_closure && !partner) || !h_lo || !h_hi || !hyp_shift) return VK_E_ARG;
+  if (!c_isum != !hit_isum || (pair_closure && !partner) || !h_lo || !h_hi || !hyp_shift || !seg_cnt) return VK_E_ARG;
   int list_pow2 = 32;
   while (list_pow2 < (pair_closure ? 2 : 1) * topk) list_pow2 <<= 1;
   const int key_cap = list_pow2 > 512 ? list_pow2 : 512;
-  const size_t per_warp = (size_t)key_cap * 12 + (size_t)list_pow2 * 16 + 1024;
+  const size_t per_warp = (size_t)key_cap * 12 + (size_t)list_pow2 * 16 + 1024 + sizeof(HitScratch);
   const size_t sh = per_warp * TK_WARPS;
   if (sh > 220 * 1024) return VK_E_ARG;
   cudaError_t e = cudaFuncSetAttribute(select_hits_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
   if (e != cudaSuccess) return vk_err(e);
   select_hits_k<<<(unsigned)((n_spec + TK_WARPS - 1) / TK_WARPS), TK_WARPS * 32, sh, (cudaStream_t)stream>>>(
-      n_spec, spec_hyp_off, h_lo, h_hi, win_off, hyp_shift, hit_rc, hit_isum, hyp_scored, hyp_matched, topk,
+      n_spec, spec_hyp_off, h_lo, h_hi, win_off, hyp_shift, seg_cnt, hit_rc, hit_isum, hyp_scored, hyp_matched, topk,
       pair_closure, partner, cap, list_pow2, key_cap, c_hyp, c_row, c_cnt, c_isum, n_cand, spec_scored,
       spec_matched);
   return vk_launch_status();

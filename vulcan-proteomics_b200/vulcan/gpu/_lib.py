@@ -95,8 +95,8 @@ _SIGS_B200 = {
     "vk_k1_tiles": [P, P, F32, F32, I32, P, P, I64, I64, P, P, P, P, P, I64, P, P, P, P, P, P, P, P, P, I32, I64, P],
     "vk_k1_peak_keys": [P, P, F32, F32, P, P, I32, I64, P, P, P],
     "vk_k1_hits": [P, P, F32, F32, I32, P, P, I64, I64, P, P, P, P, P, I64, P, P, I32, P, P, P, P, P, P, P, P, P, P,
-                   P, I32, I64, P],
-    "vk_select_hits": [I32, P, P, P, P, P, P, P, P, P, I32, I32, P, I32, P, P, P, P, P, P, P, P],
+                   P, P, I32, I64, P],
+    "vk_select_hits": [I32, P, P, P, P, P, P, P, P, P, P, I32, I32, P, I32, P, P, P, P, P, P, P, P],
     "vk_compact_hits": [I32, I32, P, P, P, P, P, P, P, P, P, P, P, P, P, P],
     "vk_tindex_bitmap": [P, P, P],
     "vk_select_topk": [I32, P, P, P, P, P, I64, P, I32, I32, I32, I32, P, P, P, P, P, P, P, P, P],

@@ -616,17 +616,20 @@ def _k1_hits(gi: GpuIndex, dh, peaks, p: SearchParams, n_hyp: int, thr: int, isu
         cap = pl["cnt_cap"]
         if rc is None:
             rc = torch.empty(cap, dtype=torch.int64, device=dev)
+            seg_cnt = torch.empty(cap, dtype=torch.int32, device=dev)
             hisum = torch.empty(cap, dtype=torch.int32, device=dev) if isum else None
         K.check(L.vk_k1_hits(C.byref(tix), C.byref(gi.fp), float(p.fragment_ppm[0]), float(p.fragment_ppm[1]),
                              warps, K.ptr(pl["item_off"]), K.ptr(pl["item_hyp"]), n_hyp, pl["item_cap"],
                              K.ptr(dh["spec"]), K.ptr(dh["maxfz"]), K.ptr(dh["lo"]), K.ptr(dh["hi"]),
                              K.ptr(pl["win_off"]), cap, K.ptr(peaks["off"]), K.ptr(peaks["mass"]),
                              int(thr) if h_thr is None else 0, K.ptr(h_thr), K.ptr(rc),
-                             K.ptr(hisum) if isum else None, K.ptr(hyp_shift), K.ptr(hyp_scored), K.ptr(hyp_matched),
+                             K.ptr(hisum) if isum else None, K.ptr(seg_cnt), K.ptr(hyp_shift), K.ptr(hyp_scored),
+                             K.ptr(hyp_matched),
                              K.ptr(pl["status"]), K.ptr(peaks["int"]) if isum else None,
                              K.ptr(peaks["tic"]) if isum else None, K.ptr(keys), K.ptr(filt), n_kz, kstride,
                              K.stream()), "k1_hits")
-    return {"win_off": pl["win_off"], "status": pl["status"], "rc": rc, "isum": hisum, "hyp_shift": hyp_shift,
+    return {"win_off": pl["win_off"], "status": pl["status"], "rc": rc, "isum": hisum, "seg_cnt": seg_cnt,
+            "hyp_shift": hyp_shift,
             "hyp_scored": hyp_scored, "hyp_matched": hyp_matched}
 
 
@@ -647,7 +650,8 @@ def _shortlist_hits(gi: GpuIndex, p: SearchParams, n: int, dh, k1h: dict, topk: 
     spec_scored = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
     spec_matched = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
     K.check(L.vk_select_hits(n, K.ptr(dh["spec_off"]), K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(k1h["win_off"]),
-                             K.ptr(k1h["hyp_shift"]), K.ptr(k1h["rc"]), K.ptr(k1h["isum"]) if isum else None,
+                             K.ptr(k1h["hyp_shift"]), K.ptr(k1h["seg_cnt"]), K.ptr(k1h["rc"]),
+                             K.ptr(k1h["isum"]) if isum else None,
                              K.ptr(k1h["hyp_scored"]),
                              K.ptr(k1h["hyp_matched"]), topk, int(closure), K.ptr(gi.partner), cap, K.ptr(s_hyp),
                              K.ptr(s_row), K.ptr(s_cnt),
@@ -1389,6 +1393,8 @@ class Searcher:
         self.depth = depth
         self.slots = {}
         self.device_ms = 0.0          # summed CUDA-event time of the replayed passes (inputs already copied)
+        # host seconds: waiting for results, unpacking them, building tables, submitting runs
+        self.host_s = {"wait": 0.0, "unpack": 0.0, "table": 0.0, "submit": 0.0}
         self.copy_stream = torch.cuda.Stream(gi.dev)
         self.compute_stream = torch.cuda.Stream(gi.dev)
         self.d2h_stream = torch.cuda.Stream(gi.dev)
@@ -1487,10 +1493,14 @@ class Searcher:
 
     def _records(self, handle):
         sp, slot, h2d, ev = handle
+        t0 = time.perf_counter()
         slot.done.synchronize()
+        t1 = time.perf_counter()
         self.device_ms += ev[0].elapsed_time(ev[1])
         check_status(slot.gp.out["status"])
         rec = _unpack_psms(slot.host_out.numpy(), slot.layout)
+        self.host_s["wait"] += t1 - t0
+        self.host_s["unpack"] += time.perf_counter() - t1
         slot.busy = False
         st = Stats()
         st.h2d_bytes, st.d2h_bytes = h2d, slot.host_out.numel()
@@ -1552,10 +1562,14 @@ class Searcher:
         while inflight:
             h = inflight.popleft()
             rec, st = self._records(h)
+            t0 = time.perf_counter()
             if k < len(runs):
                 inflight.append(self.submit(runs[k]))
                 k += 1
+            t1 = time.perf_counter()
             out.append((_table(h[0], rec), st))
+            self.host_s["submit"] += t1 - t0
+            self.host_s["table"] += time.perf_counter() - t1
         return out
 
 
