@@ -750,6 +750,30 @@ def test_searcher_pipeline_depth(mini, param_sets, indexes, depth, torch_cuda):
         se.result(h)
 
 
+def test_searcher_tables_own_their_result_buffers(mini, param_sets, indexes, torch_cuda):
+    """Tables kept across many more runs than slots stay intact (each holds its own pinned result buffer); the
+    held bytes go back to zero when they are dropped; over ``hold_bytes`` the tables get copied columns."""
+    import dataclasses
+    import gc
+    from vulcan.gpu import engine as E
+    l1, sp, _ = mini
+    p = dataclasses.replace(param_sets["ppm"], search_method="staged")
+    gi = indexes["ppm"]
+    want = E.search(sp, gi, l1, p, report=2)[0]
+    se = E.Searcher(gi, l1, p, report=2, depth=2)
+    got = se.search_many([sp] * 7)
+    assert se._held[0] > 0
+    for tbl, _ in got:
+        assert tbl.equals(want)
+    del got, tbl
+    gc.collect()
+    assert se._held[0] == 0
+    se0 = E.Searcher(gi, l1, p, report=2, depth=2, hold_bytes=0)
+    for tbl, _ in se0.search_many([sp] * 4):
+        assert tbl.equals(want)
+    assert se0._held[0] == 0
+
+
 def test_autotuner_picks_a_measured_layout(mini, param_sets, tmp_path, torch_cuda):
     """The autotuner times every candidate layout on the sample, returns the fastest, reports peak-count buckets,
     and reuses its cached choice."""

@@ -65,6 +65,18 @@ def test_compacted_pack_unpacks_by_row_count():
         assert np.array_equal(rec[k], v[:n_rows]), k
     host[:] = 0      # the records own their memory: the pinned buffer may be reused at once
     assert np.array_equal(rec["hyperscore"], cols["hyperscore"][:n_rows])
+    host[layout[0][2]:layout[0][2] + 8] = np.array([n_rows], np.int64).view(np.uint8)
+    views = E._unpack_psms(host, lay, copy=False)   # views: the buffer belongs to the records
+    assert all(v.base is not None and len(v) == n_rows for v in views.values())
+    host[layout[1][2]:layout[1][2] + 8] = 7
+    assert views[layout[1][0]].view(np.uint8)[0] == 7
+
+
+def test_run_column_is_a_cached_slice():
+    a = E._run_column("runA", 10)
+    b = E._run_column("runA", 70_000)
+    assert a.to_pylist() == ["runA"] * 10 and len(b) == 70_000 and b[69_999].as_py() == "runA"
+    assert E._run_column("runB", 3).to_pylist() == ["runB"] * 3
 
 
 def _run(name, n, n_peaks=3):

@@ -15,6 +15,7 @@ import ctypes as C
 import math
 import resource
 import time
+import weakref
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -1270,23 +1271,37 @@ def _pack_fused(gi: GpuIndex, o: dict, report: int, n: int):
     return _pack(_psm_device_cols(gi, raw), ok)
 
 
-def _unpack_psms(host: np.ndarray, layout) -> dict:
-    """Host records of the filled PSM slots from a packed buffer: new arrays, so the buffer may be reused as soon
-    as this returns.  A compacted buffer (layout starting with "n_rows": the filled slots first, in slot order) is
-    read as slices; otherwise the "valid" column selects the rows."""
+def _unpack_psms(host: np.ndarray, layout, copy: bool = True) -> dict:
+    """Host records of the filled PSM slots from a packed buffer.  A compacted buffer (layout starting with
+    "n_rows": the filled slots first, in slot order) is read as slices: new arrays with ``copy`` (the buffer may be
+    reused as soon as this returns), else views of the buffer, which then belongs to the records.  Otherwise the
+    "valid" column selects the rows (new arrays)."""
     if layout and layout[0][0] == "n_rows":
         n = int(np.frombuffer(host, dtype=np.int64, count=1, offset=layout[0][2])[0])
-        return {name: np.frombuffer(host, dtype=dt, count=n, offset=off).copy() for name, dt, off, cnt in layout[1:]}
+        cols = {name: np.frombuffer(host, dtype=dt, count=n, offset=off) for name, dt, off, cnt in layout[1:]}
+        return {k: v.copy() for k, v in cols.items()} if copy else cols
     cols = {name: np.frombuffer(host, dtype=dt, count=cnt, offset=off) for name, dt, off, cnt in layout}
     idx = np.flatnonzero(cols.pop("valid"))
     return {k: np.take(v, idx) for k, v in cols.items()}
 
 
+_RUN_COLUMNS: dict = {}
+
+
+def _run_column(run: str, n: int) -> pa.Array:
+    """The "run" column of n rows: a slice of a cached repeated-string array (the last few run names kept)."""
+    col = _RUN_COLUMNS.get(run)
+    if col is None or len(col) < n:
+        if len(_RUN_COLUMNS) >= 8:
+            _RUN_COLUMNS.pop(next(iter(_RUN_COLUMNS)))
+        col = _RUN_COLUMNS[run] = pa.repeat(pa.scalar(run, pa.string()), max(n, 1 << 16))
+    return col.slice(0, n)
+
+
 def _table(sp: Spectra, rec: dict) -> pa.Table:
     """The PSM table from device-computed columns: run, scan and retention time added on the host."""
     s = rec["spec_idx"]
-    cols = {"run": pa.repeat(pa.scalar(sp.run, pa.string()), len(s)), "spec_idx": s, "scan": sp.scan[s],
-            "rt": sp.rt[s]}
+    cols = {"run": _run_column(sp.run, len(s)), "spec_idx": s, "scan": sp.scan[s], "rt": sp.rt[s]}
     for k in _PSM_TABLE[1:]:
         cols[k] = rec[k]
     return pa.table(cols)
@@ -1333,9 +1348,13 @@ def _is_pinned(a: np.ndarray) -> bool:
         return False
 
 
+def _release_held(held: list, nbytes: int):
+    held[0] -= nbytes
+
+
 class _Slot:
-    """Device buffers of one run shape (n spectra, cap_raw peaks), the pass captured over them, pinned staging for
-    inputs that are not pinned, and the packed result in pinned host memory."""
+    """Device buffers of one run shape (n spectra, cap_raw peaks), the pass captured over them and pinned staging
+    for inputs that are not pinned."""
 
     def __init__(self, searcher: "Searcher", n: int, cap_raw: int, max_raw: int, n_hyp_cap: int):
         se = searcher
@@ -1357,7 +1376,7 @@ class _Slot:
             self.layout = layout
             return out
         self.gp = GraphedPass(fn, dev)
-        self.host_out = torch.empty(self.gp.out["packed"].numel(), dtype=torch.uint8, pin_memory=True)
+        self.out_bytes = self.gp.out["packed"].numel()
         self.offsets = torch.empty(n + 1, dtype=torch.int64, pin_memory=True)   # offsets staging
         self.stage = {}
         self.h2d_done = torch.cuda.Event()
@@ -1383,14 +1402,22 @@ class Searcher:
     a handle, ``result(handle)`` waits for it and builds its PSM table; ``search(sp)`` does both;
     ``search_many(runs)`` keeps ``depth`` runs in flight while the tables are built.  Inputs already in pinned host memory
     (``pin_spectra``) are copied straight to the device; others are staged through pinned buffers first.  Results
-    are identical to ``engine.search`` / ``prune.search_pruned``."""
+    are identical to ``engine.search`` / ``prune.search_pruned``.
 
-    def __init__(self, gi: GpuIndex, l1, p: SearchParams, pruner=None, report: int | None = None, depth: int = 3):
+    Each run's packed PSMs come back into a pinned buffer of its own (torch's caching host allocator), and the
+    run's table columns are views of it: the table owns the buffer, which goes back to the allocator's cache when
+    the table is dropped.  Once the buffers held by live tables reach ``hold_bytes``, further tables get copied
+    columns instead and their buffers are recycled at once."""
+
+    def __init__(self, gi: GpuIndex, l1, p: SearchParams, pruner=None, report: int | None = None, depth: int = 3,
+                 hold_bytes: int = 1 << 30):
         if depth < 1:
             raise ValueError("depth: at least one run in flight")
         self.gi, self.l1, self.p, self.pruner = gi, l1, p, pruner
         self.report = p.report_psms if report is None else report
         self.depth = depth
+        self.hold_bytes = hold_bytes
+        self._held = [0]              # bytes of result buffers owned by live tables
         self.slots = {}
         self.device_ms = 0.0          # summed CUDA-event time of the replayed passes (inputs already copied)
         # host seconds: waiting for results, unpacking them, building tables, submitting runs
@@ -1486,24 +1513,30 @@ class Searcher:
                 out = slot.gp.replay()
                 ev[1].record(self.compute_stream)
             self.d2h_stream.wait_event(ev[1])
+            host_out = torch.empty(slot.out_bytes, dtype=torch.uint8, pin_memory=True)
             with torch.cuda.stream(self.d2h_stream):
-                slot.host_out.copy_(out["packed"], non_blocking=True)
+                host_out.copy_(out["packed"], non_blocking=True)
                 slot.done.record(self.d2h_stream)
-            return (parts[0] if len(parts) == 1 else None, slot, h2d, ev)
+            return (parts[0] if len(parts) == 1 else None, slot, h2d, ev, host_out)
 
     def _records(self, handle):
-        sp, slot, h2d, ev = handle
+        sp, slot, h2d, ev, host_out = handle
         t0 = time.perf_counter()
         slot.done.synchronize()
         t1 = time.perf_counter()
         self.device_ms += ev[0].elapsed_time(ev[1])
         check_status(slot.gp.out["status"])
-        rec = _unpack_psms(slot.host_out.numpy(), slot.layout)
+        nb = host_out.numel()
+        keep = self._held[0] + nb <= self.hold_bytes
+        rec = _unpack_psms(host_out.numpy(), slot.layout, copy=not keep)
+        if keep:   # the records are views of host_out: count it as held until they are all gone
+            self._held[0] += nb
+            weakref.finalize(host_out, _release_held, self._held, nb)
         self.host_s["wait"] += t1 - t0
         self.host_s["unpack"] += time.perf_counter() - t1
         slot.busy = False
         st = Stats()
-        st.h2d_bytes, st.d2h_bytes = h2d, slot.host_out.numel()
+        st.h2d_bytes, st.d2h_bytes = h2d, nb
         return rec, st
 
     def result(self, handle):
