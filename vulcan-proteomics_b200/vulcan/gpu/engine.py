@@ -1528,10 +1528,11 @@ class Searcher:
         check_status(slot.gp.out["status"])
         nb = host_out.numel()
         keep = self._held[0] + nb <= self.hold_bytes
-        rec = _unpack_psms(host_out.numpy(), slot.layout, copy=not keep)
-        if keep:   # the records are views of host_out: count it as held until they are all gone
+        host = host_out.numpy()
+        rec = _unpack_psms(host, slot.layout, copy=not keep)
+        if keep:   # the records are views of `host` (and through it of the pinned block): held until they are gone
             self._held[0] += nb
-            weakref.finalize(host_out, _release_held, self._held, nb)
+            weakref.finalize(host, _release_held, self._held, nb)
         self.host_s["wait"] += t1 - t0
         self.host_s["unpack"] += time.perf_counter() - t1
         slot.busy = False
