@@ -187,7 +187,8 @@ k1_tiles_k(vk_tindex ix, float tol_lo, float tol_hi, int tol_da, int post_cap, c
         // the tile's row 0); kept rows compacted to its start in row order, their number at its first slot
         const int64_t seg = r.base + rlo;
         const int thr_h = hits.h_thr ? hits.h_thr[r.h] : hits.thr;
-        long long sc = 0, mt = 0;
+        // per item at most T rows of at most (peaks x charges) counts each: 32-bit sums, one warp reduction each
+        uint32_t sc = 0, mt = 0;
         int n_kept = 0;
         for (int q0 = rlo; q0 < rhi; q0 += 32) {
           const int q = q0 + lane;
@@ -203,12 +204,12 @@ k1_tiles_k(vk_tindex ix, float tol_lo, float tol_hi, int tol_da, int post_cap, c
           }
           n_kept += __popc(bal);
         }
-        sc = vk::warp_sum(sc);
-        mt = vk::warp_sum(mt);
+        sc = __reduce_add_sync(VK_FULL, sc);
+        mt = __reduce_add_sync(VK_FULL, mt);
         if (lane == 0) {
           hits.seg_cnt[seg] = (uint32_t)n_kept;
           hits.hyp_shift[r.h] = (int8_t)ix.tile_shift;   // every item of h writes the same value
-          if (sc) atomicAdd(&hits.hyp_scored[r.h], (uint32_t)sc);
+          if (sc) atomicAdd(&hits.hyp_scored[r.h], sc);
           if (mt) atomicAdd(&hits.hyp_matched[r.h], (unsigned long long)mt);
         }
       } else {

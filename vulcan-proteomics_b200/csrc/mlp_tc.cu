@@ -9,11 +9,13 @@
 //      canonical K-major layout;
 //   2. one thread issues D = X W1^T (M 128, N 256, K 16) into the tile's 256 TMEM columns and commits to an
 //      mbarrier;
-//   3. epilogue 1: every warp reads its 32 rows x 64 columns with tcgen05.ld, adds b1, applies ReLU, rounds to
-//      BF16 and writes them into shared memory as the layer-2 A operand;
+//   3. epilogue 1: every warp reads its 32 rows x 64 columns with tcgen05.ld, adds b1 (packed f32x2 adds),
+//      applies ReLU and rounds to BF16 in one cvt per pair, and writes them into shared memory as the layer-2 A
+//      operand;
 //   4. one thread issues D = H1 W2^T (K 256: 16 UMMAs) into the same TMEM columns and commits;
-//   5. epilogue 2 (done while the next tile's layer 2 runs): ReLU(D + b2) . w3 over the warp's 64 columns, the four
-//      column quarters of a row summed in a fixed order through shared memory, + b3, written to `logit`.
+//   5. epilogue 2 (done while the next tile's layer 2 runs): ReLU(D + b2) . w3 over the warp's 64 columns (packed
+//      f32x2 adds and fused multiply-adds into four partial sums), the four column quarters of a row summed in a
+//      fixed order through shared memory, + b3, written to `logit`.
 // Shared-memory operands use the no-swizzle canonical layout: 8-row x 16-byte core matrices (128 contiguous bytes),
 // the two 16-byte K chunks of one UMMA K-step 128 bytes apart (leading byte offset), 8-row groups a whole K-row of
 // core matrices apart (stride byte offset).  Every mbarrier wait is bounded: on a timeout the CTA records
@@ -92,9 +94,77 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t* v) {
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-__device__ __forceinline__ uint32_t pack2(float lo, float hi) {
-  __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
-  return *reinterpret_cast<uint32_t*>(&v);
+// Pairs of f32 in one 64-bit register (element 2j in the low half), added / fused-multiply-added with the
+// packed-f32x2 instructions: two IEEE round-to-nearest operations each, half the instruction count.
+__device__ __forceinline__ uint64_t f2(uint32_t lo, uint32_t hi) {
+  uint64_t d;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(d) : "r"(lo), "r"(hi));
+  return d;
+}
+__device__ __forceinline__ uint64_t add_f2(uint64_t a, uint64_t b) {
+  uint64_t d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ uint64_t fma_f2(uint64_t a, uint64_t b, uint64_t c) {
+  uint64_t d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+__device__ __forceinline__ float lo_f(uint64_t a) { return __uint_as_float((uint32_t)a); }
+__device__ __forceinline__ float hi_f(uint64_t a) { return __uint_as_float((uint32_t)(a >> 32)); }
+__device__ __forceinline__ uint64_t relu_f2(uint64_t a) {
+  return f2(__float_as_uint(fmaxf(lo_f(a), 0.f)), __float_as_uint(fmaxf(hi_f(a), 0.f)));
+}
+// BF16 pair of relu(lo), relu(hi) rounded to nearest (lo in the low half): rounding keeps the sign, so this is
+// the rounding of the ReLU output
+__device__ __forceinline__ uint32_t relu_bf16x2(uint64_t a) {
+  uint32_t d;
+  asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi_f(a)), "f"(lo_f(a)));
+  return d;
+}
+
+// Epilogue 1 of 32 accumulator columns c0.. of this thread's row: BF16(relu(D + b1)) into the layer-2 operand
+// (four 16-byte K chunks, 128 bytes apart).
+__device__ __forceinline__ void epi1_cols(const uint32_t* v, const float* sb1, int c0, uint8_t* dst) {
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const ulonglong2 ba = *reinterpret_cast<const ulonglong2*>(sb1 + c0 + 8 * q);       // 16-byte aligned
+    const ulonglong2 bb = *reinterpret_cast<const ulonglong2*>(sb1 + c0 + 8 * q + 4);
+    uint4 w;
+    w.x = relu_bf16x2(add_f2(f2(v[8 * q + 0], v[8 * q + 1]), ba.x));
+    w.y = relu_bf16x2(add_f2(f2(v[8 * q + 2], v[8 * q + 3]), ba.y));
+    w.z = relu_bf16x2(add_f2(f2(v[8 * q + 4], v[8 * q + 5]), bb.x));
+    w.w = relu_bf16x2(add_f2(f2(v[8 * q + 6], v[8 * q + 7]), bb.y));
+    *reinterpret_cast<uint4*>(dst + q * 128) = w;
+  }
+}
+
+// Epilogue 2 of 32 accumulator columns c0..: relu(D + b2) . w3 accumulated into two f32 pairs (four partial
+// sums: columns c = 0, 1, 2, 3 mod 4).
+__device__ __forceinline__ void epi2_cols(const uint32_t* v, const float* sb2, const float* sw3, int c0,
+                                          uint64_t& za, uint64_t& zb) {
+#pragma unroll
+  for (int j = 0; j < 32; j += 4) {
+    const ulonglong2 b = *reinterpret_cast<const ulonglong2*>(sb2 + c0 + j);
+    const ulonglong2 w = *reinterpret_cast<const ulonglong2*>(sw3 + c0 + j);
+    za = fma_f2(relu_f2(add_f2(f2(v[j + 0], v[j + 1]), b.x)), w.x, za);
+    zb = fma_f2(relu_f2(add_f2(f2(v[j + 2], v[j + 3]), b.y)), w.y, zb);
+  }
+}
+
+// This thread's share of a row's logit from the 64 columns col0.. of TMEM buffer pbuf (layer-2 accumulators).
+__device__ __forceinline__ float epi2_share(uint32_t pbuf, uint32_t lane_off, int col0, const float* sb2,
+                                            const float* sw3) {
+  uint64_t za = 0ull, zb = 0ull;   // +0.0f pairs
+#pragma unroll 1
+  for (int c0 = col0; c0 < col0 + TC_COLS_PER_WARP; c0 += 32) {
+    uint32_t v[32];
+    tmem_ld32(pbuf + lane_off + (uint32_t)c0, v);
+    tmem_wait_ld();
+    epi2_cols(v, sb2, sw3, c0, za, zb);
+  }
+  return (lo_f(za) + hi_f(za)) + (lo_f(zb) + hi_f(zb));
 }
 
 // Two TMEM accumulators of 256 columns (tile i uses buffer i % 2 for both layers), so that the layer-2 UMMAs of
@@ -201,27 +271,12 @@ mlp_infer_tc_k(int64_t n, const int64_t* n_dev, const __nv_bfloat16* __restrict_
     ph1 ^= 1u << b;
     tc_fence_after();
     // epilogue 1: H1 = bf16(relu(D + b1)) into the layer-2 operand
+#pragma unroll 1
     for (int c0 = col0; c0 < col0 + TC_COLS_PER_WARP; c0 += 32) {
       uint32_t v[32];
       tmem_ld32(buf + lane_off + (uint32_t)c0, v);
       tmem_wait_ld();
-      uint8_t* dst = sm + OFF_H + canon_off(my_row, c0, TC_H);
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        uint4 w;
-        const int c = c0 + 8 * q;
-        const float4 ba = *reinterpret_cast<const float4*>(sb1 + c);       // 16-byte aligned (c % 8 == 0)
-        const float4 bb = *reinterpret_cast<const float4*>(sb1 + c + 4);
-        w.x = pack2(fmaxf(__uint_as_float(v[8 * q + 0]) + ba.x, 0.f),
-                    fmaxf(__uint_as_float(v[8 * q + 1]) + ba.y, 0.f));
-        w.y = pack2(fmaxf(__uint_as_float(v[8 * q + 2]) + ba.z, 0.f),
-                    fmaxf(__uint_as_float(v[8 * q + 3]) + ba.w, 0.f));
-        w.z = pack2(fmaxf(__uint_as_float(v[8 * q + 4]) + bb.x, 0.f),
-                    fmaxf(__uint_as_float(v[8 * q + 5]) + bb.y, 0.f));
-        w.w = pack2(fmaxf(__uint_as_float(v[8 * q + 6]) + bb.z, 0.f),
-                    fmaxf(__uint_as_float(v[8 * q + 7]) + bb.w, 0.f));
-        *reinterpret_cast<uint4*>(dst + q * 128) = w;    // k chunks 128 bytes apart
-      }
+      epi1_cols(v, sb1, c0, sm + OFF_H + canon_off(my_row, c0, TC_H));
     }
     async_proxy_fence();
     tc_fence_before();
@@ -246,23 +301,7 @@ mlp_infer_tc_k(int64_t n, const int64_t* n_dev, const __nv_bfloat16* __restrict_
       if (!vk::mbar_wait(&bar2[pb], (ph2 >> pb) & 1u, TC_WAIT)) atomicOr(&abort_flag, 1);
       ph2 ^= 1u << pb;
       tc_fence_after();
-      const uint32_t pbuf = tmem + (uint32_t)pb * TC_TMEM_COLS;
-      float z = 0.f;
-      for (int c0 = col0; c0 < col0 + TC_COLS_PER_WARP; c0 += 32) {
-        uint32_t v[32];
-        tmem_ld32(pbuf + lane_off + (uint32_t)c0, v);
-        tmem_wait_ld();
-#pragma unroll
-        for (int j = 0; j < 32; j += 4) {   // b2 and w3 four at a time; relu(D + b2) . w3 with fused multiply-adds
-          const float4 b = *reinterpret_cast<const float4*>(sb2 + c0 + j);
-          const float4 w = *reinterpret_cast<const float4*>(sw3 + c0 + j);
-          z = __fmaf_rn(fmaxf(__uint_as_float(v[j + 0]) + b.x, 0.f), w.x, z);
-          z = __fmaf_rn(fmaxf(__uint_as_float(v[j + 1]) + b.y, 0.f), w.y, z);
-          z = __fmaf_rn(fmaxf(__uint_as_float(v[j + 2]) + b.z, 0.f), w.z, z);
-          z = __fmaf_rn(fmaxf(__uint_as_float(v[j + 3]) + b.w, 0.f), w.w, z);
-        }
-      }
-      part[cq * TC_M + my_row] = z;
+      part[cq * TC_M + my_row] = epi2_share(tmem + (uint32_t)pb * TC_TMEM_COLS, lane_off, col0, sb2, sw3);
     }
     // the next tile's features (layer 1 of this tile is done with the feature buffer)
     const int64_t nt = tile + G;
@@ -296,23 +335,7 @@ mlp_infer_tc_k(int64_t n, const int64_t* n_dev, const __nv_bfloat16* __restrict_
     if (!vk::mbar_wait(&bar2[pb], (ph2 >> pb) & 1u, TC_WAIT)) atomicOr(&abort_flag, 1);
     ph2 ^= 1u << pb;
     tc_fence_after();
-    const uint32_t pbuf = tmem + (uint32_t)pb * TC_TMEM_COLS;
-    float z = 0.f;
-    for (int c0 = col0; c0 < col0 + TC_COLS_PER_WARP; c0 += 32) {
-      uint32_t v[32];
-      tmem_ld32(pbuf + lane_off + (uint32_t)c0, v);
-      tmem_wait_ld();
-#pragma unroll
-      for (int j = 0; j < 32; j += 4) {   // b2 and w3 four at a time; relu(D + b2) . w3 with fused multiply-adds
-        const float4 b = *reinterpret_cast<const float4*>(sb2 + c0 + j);
-        const float4 w = *reinterpret_cast<const float4*>(sw3 + c0 + j);
-        z = __fmaf_rn(fmaxf(__uint_as_float(v[j + 0]) + b.x, 0.f), w.x, z);
-        z = __fmaf_rn(fmaxf(__uint_as_float(v[j + 1]) + b.y, 0.f), w.y, z);
-        z = __fmaf_rn(fmaxf(__uint_as_float(v[j + 2]) + b.z, 0.f), w.z, z);
-        z = __fmaf_rn(fmaxf(__uint_as_float(v[j + 3]) + b.w, 0.f), w.w, z);
-      }
-    }
-    part[cq * TC_M + my_row] = z;
+    part[cq * TC_M + my_row] = epi2_share(tmem + (uint32_t)pb * TC_TMEM_COLS, lane_off, col0, sb2, sw3);
     tc_fence_before();
     __syncthreads();
     if (tid < TC_M) {
