@@ -756,6 +756,9 @@ def run_batch(a):
         se.device_ms = 0.0
         t0 = time.perf_counter()
         for _ in range(reps):
+            # a step's tables are written out and dropped before the next step: their pinned result buffers go
+            # back to the Searcher's pool (a caller keeping every table gets copies once the pool is lent out)
+            tables = None
             tables = se.search_batch(pinned, batch_spectra=batch_spectra)
         torch.cuda.synchronize()
         wall = max_over_ranks(time.perf_counter() - t0, dev)

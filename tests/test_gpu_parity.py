@@ -751,8 +751,9 @@ def test_searcher_pipeline_depth(mini, param_sets, indexes, depth, torch_cuda):
 
 
 def test_searcher_tables_own_their_result_buffers(mini, param_sets, indexes, torch_cuda):
-    """Tables kept across many more runs than slots stay intact (each holds its own pinned result buffer); the
-    held bytes go back to zero when they are dropped; over ``hold_bytes`` the tables get copied columns."""
+    """Tables kept across many more runs than slots stay intact (each views its own pinned result buffer from the
+    Searcher's pool); the buffers return to the pool when the tables are dropped and are reused; with no pool
+    (``hold_bytes`` 0) or the pool exhausted the tables get copied columns."""
     import dataclasses
     import gc
     from vulcan.gpu import engine as E
@@ -762,16 +763,24 @@ def test_searcher_tables_own_their_result_buffers(mini, param_sets, indexes, tor
     want = E.search(sp, gi, l1, p, report=2)[0]
     se = E.Searcher(gi, l1, p, report=2, depth=2)
     got = se.search_many([sp] * 7)
-    assert se._held[0] > 0
+    assert se.held_bytes() > 0
     for tbl, _ in got:
         assert tbl.equals(want)
+    n_buf = sum(pl.n for pl in se.pools.values())
     del got, tbl
     gc.collect()
-    assert se._held[0] == 0
+    assert se.held_bytes() == 0
+    for tbl, _ in se.search_many([sp] * 7):   # the returned buffers are reused: no new ones
+        assert tbl.equals(want)
+    assert sum(pl.n for pl in se.pools.values()) == n_buf
     se0 = E.Searcher(gi, l1, p, report=2, depth=2, hold_bytes=0)
     for tbl, _ in se0.search_many([sp] * 4):
         assert tbl.equals(want)
-    assert se0._held[0] == 0
+    assert se0.held_bytes() == 0
+    pool = next(iter(se.pools.values()))
+    se2 = E.Searcher(gi, l1, p, report=2, depth=2, hold_bytes=2 * pool.nbytes)   # two buffers, then copies
+    kept = se2.search_many([sp] * 5)
+    assert all(t.equals(want) for t, _ in kept) and se2.held_bytes() == 2 * pool.nbytes
 
 
 def test_autotuner_picks_a_measured_layout(mini, param_sets, tmp_path, torch_cuda):

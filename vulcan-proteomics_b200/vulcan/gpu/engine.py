@@ -1348,8 +1348,25 @@ def _is_pinned(a: np.ndarray) -> bool:
         return False
 
 
-def _release_held(held: list, nbytes: int):
-    held[0] -= nbytes
+class _ResultPool:
+    """Pinned result buffers of one size (a run shape's packed PSMs), lent to the tables that view them and
+    returned to ``free`` when those tables are dropped; at most ``cap`` exist."""
+
+    def __init__(self, nbytes: int, cap: int):
+        self.nbytes, self.cap = nbytes, cap
+        self.free, self.n = [], 0
+
+    def take(self):
+        """A free buffer, a new one while fewer than ``cap`` exist, else None."""
+        if self.free:
+            return self.free.pop()
+        if self.n < self.cap:
+            self.n += 1
+            return torch.empty(self.nbytes, dtype=torch.uint8, pin_memory=True)
+        return None
+
+    def lent_bytes(self) -> int:
+        return (self.n - len(self.free)) * self.nbytes
 
 
 class _Slot:
@@ -1377,6 +1394,8 @@ class _Slot:
             return out
         self.gp = GraphedPass(fn, dev)
         self.out_bytes = self.gp.out["packed"].numel()
+        # the packed PSMs' landing buffer when the shape's result pool has none free: read into copies at once
+        self.host_out = torch.empty(self.out_bytes, dtype=torch.uint8, pin_memory=True)
         self.offsets = torch.empty(n + 1, dtype=torch.int64, pin_memory=True)   # offsets staging
         self.stage = {}
         self.h2d_done = torch.cuda.Event()
@@ -1404,10 +1423,11 @@ class Searcher:
     (``pin_spectra``) are copied straight to the device; others are staged through pinned buffers first.  Results
     are identical to ``engine.search`` / ``prune.search_pruned``.
 
-    Each run's packed PSMs come back into a pinned buffer of its own (torch's caching host allocator), and the
-    run's table columns are views of it: the table owns the buffer, which goes back to the allocator's cache when
-    the table is dropped.  Once the buffers held by live tables reach ``hold_bytes``, further tables get copied
-    columns instead and their buffers are recycled at once."""
+    Each run's packed PSMs come back into a pinned buffer lent from the shape's pool, and the run's table columns
+    are views of it (no host copy); the buffer returns to the pool when the table is dropped, so a caller that
+    drops (or writes out) its tables reuses the same few buffers.  The pool of a shape holds at most ``hold_bytes``
+    of buffers: while all of them are lent to live tables, further runs land in the slot's own pinned buffer and
+    their tables get copied columns."""
 
     def __init__(self, gi: GpuIndex, l1, p: SearchParams, pruner=None, report: int | None = None, depth: int = 3,
                  hold_bytes: int = 1 << 30):
@@ -1417,7 +1437,7 @@ class Searcher:
         self.report = p.report_psms if report is None else report
         self.depth = depth
         self.hold_bytes = hold_bytes
-        self._held = [0]              # bytes of result buffers owned by live tables
+        self.pools = {}               # packed-buffer size -> _ResultPool
         self.slots = {}
         self.device_ms = 0.0          # summed CUDA-event time of the replayed passes (inputs already copied)
         # host seconds: waiting for results, unpacking them, building tables, submitting runs
@@ -1513,26 +1533,34 @@ class Searcher:
                 out = slot.gp.replay()
                 ev[1].record(self.compute_stream)
             self.d2h_stream.wait_event(ev[1])
-            host_out = torch.empty(slot.out_bytes, dtype=torch.uint8, pin_memory=True)
+            pool = self.pools.get(slot.out_bytes)
+            if pool is None:
+                pool = self.pools[slot.out_bytes] = _ResultPool(slot.out_bytes, self.hold_bytes // slot.out_bytes)
+            host_out = pool.take()
+            lent = host_out is not None
+            if not lent:
+                host_out = slot.host_out
             with torch.cuda.stream(self.d2h_stream):
                 host_out.copy_(out["packed"], non_blocking=True)
                 slot.done.record(self.d2h_stream)
-            return (parts[0] if len(parts) == 1 else None, slot, h2d, ev, host_out)
+            return (parts[0] if len(parts) == 1 else None, slot, h2d, ev, host_out, pool if lent else None)
+
+    def held_bytes(self) -> int:
+        """Bytes of pinned result buffers lent to live tables."""
+        return sum(pl.lent_bytes() for pl in self.pools.values())
 
     def _records(self, handle):
-        sp, slot, h2d, ev, host_out = handle
+        sp, slot, h2d, ev, host_out, pool = handle
         t0 = time.perf_counter()
         slot.done.synchronize()
         t1 = time.perf_counter()
         self.device_ms += ev[0].elapsed_time(ev[1])
         check_status(slot.gp.out["status"])
         nb = host_out.numel()
-        keep = self._held[0] + nb <= self.hold_bytes
         host = host_out.numpy()
-        rec = _unpack_psms(host, slot.layout, copy=not keep)
-        if keep:   # the records are views of `host` (and through it of the pinned block): held until they are gone
-            self._held[0] += nb
-            weakref.finalize(host, _release_held, self._held, nb)
+        rec = _unpack_psms(host, slot.layout, copy=pool is None)
+        if pool is not None:   # the records are views of `host`: the buffer goes back to the pool with them
+            weakref.finalize(host, pool.free.append, host_out)
         self.host_s["wait"] += t1 - t0
         self.host_s["unpack"] += time.perf_counter() - t1
         slot.busy = False
