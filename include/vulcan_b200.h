@@ -507,7 +507,20 @@ int vk_select_pruned(int n_spec, const int64_t* spec_hyp_off, const int64_t* hit
 int vk_gemm(int M, int N, int K, const float* A, int64_t sam, int64_t sak, const void* B, int b_bf16, int64_t sbk,
             int64_t sbn, const float* bias, int relu, int round_bf16, float* C, int64_t scm, int64_t scn,
             void* stream);
-int vk_colsum(int n, int o, const float* dY, float* db, void* stream);                 /* db[j] = sum_i dY[i, j] */
+/* The same product on the tcgen05 tensor cores: A and B rounded to BF16 as they are staged, FP32 accumulation in
+ * TMEM (the tensor core's summation order, not vk_gemm's).  N a multiple of 16.  When the output tiles are few the K
+ * range is split over CTAs: ws (device FP32, ws_floats >= vk_tc_gemm_ws_floats(M, N, K), may be NULL when that is
+ * 0) takes the partial tiles, summed in split order by a second kernel.  status (device i32, not zeroed) gets
+ * VK_STATUS_WAIT_TIMEOUT if an MMA did not complete within the bounded wait (the output is then not to be used). */
+int64_t vk_tc_gemm_ws_floats(int M, int N, int K);
+int vk_tc_gemm(int M, int N, int K, const float* A, int64_t sam, int64_t sak, const void* B, int b_bf16, int64_t sbk,
+               int64_t sbn, const float* bias, int relu, int round_bf16, float* C, int64_t scm, int64_t scn,
+               float* ws, int64_t ws_floats, int32_t* status, void* stream);
+/* db[j] = sum_i dY[i, j], or sum_i v[i] dY[i, j] when v (device, n floats) is given: rows in chunks of 64 summed
+ * sequentially, the chunk sums added in chunk order; ws (device, ws_floats >= vk_colsum_ws_floats(n, o)) holds the
+ * chunk sums */
+int64_t vk_colsum_ws_floats(int n, int o);
+int vk_colsum(int n, int o, const float* dY, const float* v, float* ws, int64_t ws_floats, float* db, void* stream);
 int vk_relu_mask(int64_t n, const float* Y, float* dY, void* stream);                  /* dY *= (Y > 0) */
 /* weighted BCE with logits: dz = w (sigmoid(z) - y) inv_wsum; loss_part[ceil(n/256)] block partial sums */
 int vk_bce(int n, const float* z, const float* y, const float* w, float inv_wsum, float* dz, float* loss_part,

@@ -6,10 +6,11 @@ rescoring, ``vulcan/gpu/engine.py:315-351``), so this oracle pins the arithmetic
 
 * ``raw_features`` / ``standardise``: the per-hit features of ``vk_cand_features`` in the same f32 operations and
   the same round-to-nearest-even BF16 conversion (bit-exact);
-* ``forward_train`` / ``backward``: the training pass of ``mlp_train.cu`` -- every matrix product summed
-  sequentially over k in f32 with separately rounded products (the kernels compile without FMA contraction), ReLU,
-  BF16 rounding of the layer-1 activations, column sums in row order -- so given the same loss gradient ``dz`` every
-  weight gradient is bit-identical;
+* ``forward_train`` / ``backward``: the training pass of ``mlp_train.cu`` with its FP32 SIMT GEMMs -- every
+  matrix product summed sequentially over k in f32 with separately rounded products (the kernels compile without
+  FMA contraction), ReLU, BF16 rounding of the layer-1 activations, the bias and layer-3 gradients as column sums in
+  vk_colsum's chunked order -- so given the same loss gradient ``dz`` every weight gradient is bit-identical (the
+  tensor-core GEMMs of ``mlp_train_tc.cu`` are checked against it within a tolerance);
 * ``bce`` / ``adam``: the loss gradient and the optimiser step (within a few f32 ulps: ``expf`` / ``powf`` of the
   device and of numpy may differ in the last bit);
 * ``logits``: the inference network in float64 with the layer-1 activations rounded to BF16, the reference value
@@ -99,17 +100,26 @@ def bce(z, y, w, inv_wsum):
     return dz.astype(np.float32), float(np.sum(loss, dtype=np.float64))
 
 
-def _colsum(D):
-    s = np.zeros(D.shape[1], np.float32)
-    for i in range(D.shape[0]):
-        s = s + D[i]
-    return s
+CS_ROWS = 64   # rows per chunk of the device column sums (csrc/mlp_train.cu, vk_colsum)
+
+
+def _colsum(D, v=None):
+    """Column sums in vk_colsum's order: rows in chunks of CS_ROWS summed sequentially (each term v[i] * D[i] as
+    one rounded product when a row weight v is given), the chunk sums added in chunk order."""
+    D = np.asarray(D, np.float32)
+    tot = np.zeros(D.shape[1], np.float32)
+    for c0 in range(0, D.shape[0], CS_ROWS):
+        s = np.zeros(D.shape[1], np.float32)
+        for i in range(c0, min(D.shape[0], c0 + CS_ROWS)):
+            s = s + (D[i] if v is None else (D[i] * np.float32(v[i])).astype(np.float32))
+        tot = tot + s
+    return tot
 
 
 def backward(X, H1, H2, dz, W2b, w3):
     """Gradients {W1, b1, W2, b2, w3, b3} from the loss gradient dz, in the kernels' summation order."""
     dz = np.asarray(dz, np.float32)
-    g = {"w3": _seq_matmul(H2.T, dz[:, None])[:, 0], "b3": _colsum(dz[:, None])}
+    g = {"w3": _colsum(H2, dz), "b3": _colsum(dz[:, None])}
     dH2 = (dz[:, None] * np.asarray(w3, np.float32)[None, :]).astype(np.float32)
     dH2 = np.where(H2 > 0, dH2, np.float32(0))
     g["W2"] = _seq_matmul(dH2.T, H1)

@@ -153,11 +153,12 @@ def test_mlp_inference_matches_oracle(torch_cuda, n, kernel):
 
 @pytest.mark.parametrize("B", [200, 4096])
 def test_training_pass_equals_oracle(torch_cuda, B):
-    """Forward activations and every weight gradient bit-identical to the oracle's f32 pass (given the device's
-    loss gradient); the loss gradient and the Adam step within f32 ulps."""
+    """With the SIMT GEMMs: forward activations and every weight gradient bit-identical to the oracle's f32 pass
+    (given the device's loss gradient); the loss gradient and the Adam step within f32 ulps."""
     torch = torch_cuda
     dev = torch.device("cuda")
     pr = _random_pruner(torch, dev, 11)
+    pr.train_gemm = "simt"
     g = torch.Generator(device="cpu").manual_seed(B)
     X = torch.zeros(B, 16)
     X[:, :6] = torch.randn(B, 6, generator=g)
@@ -188,6 +189,44 @@ def test_training_pass_equals_oracle(torch_cuda, B):
                           1e-8, 1, 1e-4)
         np.testing.assert_allclose(_np(pr.w[k]), pw, rtol=1e-6, atol=1e-9)
     np.testing.assert_array_equal(_np(pr.bf["W2"].float()), M.bf16_round(_np(pr.w["W2"])))
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(np.asarray(a, np.float64) - np.asarray(b, np.float64)) /
+                 max(np.linalg.norm(np.asarray(b, np.float64)), 1e-30))
+
+
+@pytest.mark.parametrize("B", [200, 4096, 8192])
+def test_training_pass_on_tensor_cores_close_to_oracle(torch_cuda, B):
+    """With the tcgen05 GEMMs (BF16 operands, FP32 accumulation, K split over the batch for the weight gradients):
+    forward activations within BF16 rounding of the oracle's f32 pass, every weight gradient within 1% (relative
+    norm) of the oracle's gradients of the same activations, and the f64 gradient of the loss within 2%."""
+    torch = torch_cuda
+    dev = torch.device("cuda")
+    pr = _random_pruner(torch, dev, 11)
+    assert pr.train_gemm == "tcgen05"
+    g = torch.Generator(device="cpu").manual_seed(B + 1)
+    X = torch.zeros(B, 16)
+    X[:, :6] = torch.randn(B, 6, generator=g)
+    X = X.to(torch.bfloat16).float().to(dev).contiguous()
+    y = (torch.rand(B, generator=g) < 0.2).float().to(dev)
+    w = (0.5 + torch.rand(B, generator=g)).to(dev)
+    z = pr.forward_train(X, B)
+    loss, grads = pr.backward(X, y, w, B, 1.0 / float(w.sum()))
+    W1b, b1, W2b, b2, w3, b3 = _weights_np(pr, torch)
+    Xn = _np(X)
+    H1o, H2o, zo = M.forward_train(Xn, W1b, b1, W2b, b2, w3, b3)
+    H1, H2 = _np(pr._buf["H1"][:B]), _np(pr._buf["H2"][:B])
+    assert _rel(H1, H1o) < 4e-3 and _rel(H2, H2o) < 1e-2 and _rel(_np(z), zo) < 1e-2
+    dz = _np(pr._buf["dz"][:B])
+    go = M.backward(Xn, H1, H2, dz, W2b, w3)
+    for k in ("W1", "b1", "W2", "b2", "w3", "b3"):
+        assert _rel(_np(grads[k]).reshape(go[k].shape), go[k]) < 1e-2, k
+    params = {"W1": W1b.astype(np.float64), "b1": b1, "W2": W2b.astype(np.float64), "b2": b2, "w3": w3, "b3": b3}
+    g64 = M.grad_f64(params, Xn, _np(y), _np(w))
+    for k in ("W1", "W2", "w3"):
+        assert _rel(_np(grads[k]).reshape(g64[k].shape), g64[k]) < 2e-2, k
+    assert int(pr._buf["status"].item()) == 0
 
 
 @pytest.mark.parametrize("name", SETS)

@@ -81,12 +81,29 @@ gemm_k(int M, int N, int K, const float* __restrict__ A, int64_t sam, int64_t sa
   }
 }
 
-// Column sums db[j] = sum_i dY[i, j] (fixed order per column).
-__global__ void colsum_k(int n, int o, const float* dY, float* db) {
+// Column sums db[j] = sum_i dY[i, j] (v[i] dY[i, j] when v is given: the weighted sum of layer 3's weight
+// gradient), in a fixed order: rows in chunks of CS_ROWS, each chunk summed sequentially (colsum_chunk_k, one thread
+// per (chunk, column)), the chunk sums added in chunk order (colsum_total_k).
+constexpr int CS_ROWS = 64;
+
+__global__ void colsum_chunk_k(int n, int o, const float* dY, const float* v, float* part) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = blockIdx.y;
+  if (j >= o) return;
+  const int i1 = min(n, (c + 1) * CS_ROWS);
+  float s = 0.f;
+  for (int i = c * CS_ROWS; i < i1; ++i) {
+    const float x = dY[(int64_t)i * o + j];
+    s = __fadd_rn(s, v ? __fmul_rn(x, v[i]) : x);
+  }
+  part[(int64_t)c * o + j] = s;
+}
+
+__global__ void colsum_total_k(int chunks, int o, const float* part, float* db) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= o) return;
   float s = 0.f;
-  for (int i = 0; i < n; ++i) s = __fadd_rn(s, dY[(int64_t)i * o + j]);
+  for (int c = 0; c < chunks; ++c) s = __fadd_rn(s, part[(int64_t)c * o + j]);
   db[j] = s;
 }
 
@@ -162,9 +179,22 @@ int vk_gemm(int M, int N, int K, const float* A, int64_t sam, int64_t sak, const
   return vk_launch_status();
 }
 
-int vk_colsum(int n, int o, const float* dY, float* db, void* stream) {
+int64_t vk_colsum_ws_floats(int n, int o) {
+  return n > 0 && o > 0 ? (int64_t)((n + CS_ROWS - 1) / CS_ROWS) * o : 0;
+}
+
+int vk_colsum(int n, int o, const float* dY, const float* v, float* ws, int64_t ws_floats, float* db, void* stream) {
   if (o <= 0) return 0;
-  colsum_k<<<(unsigned)((o + 255) / 256), 256, 0, (cudaStream_t)stream>>>(n, o, dY, db);
+  cudaStream_t st = (cudaStream_t)stream;
+  const int chunks = n > 0 ? (n + CS_ROWS - 1) / CS_ROWS : 0;
+  if (chunks > 0 && (!ws || ws_floats < vk_colsum_ws_floats(n, o))) return VK_E_ARG;
+  if (chunks > 0) {
+    dim3 grid((unsigned)((o + 127) / 128), (unsigned)chunks);
+    colsum_chunk_k<<<grid, 128, 0, st>>>(n, o, dY, v, ws);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return vk_err(e);
+  }
+  colsum_total_k<<<(unsigned)((o + 255) / 256), 256, 0, st>>>(chunks, o, ws, db);
   return vk_launch_status();
 }
 

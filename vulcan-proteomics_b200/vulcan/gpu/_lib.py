@@ -114,7 +114,8 @@ _SIGS_B200 = {
     "vk_mlp_infer_tc": [I64, P, P, P, P, P, P, P, F32, P, I32, P, P],
     "vk_select_pruned": [I32, P, P, P, P, P, P, F32, I32, I32, I32, P, I32, I32, P, P, P, P, P],
     "vk_gemm": [I32, I32, I32, P, I64, I64, P, I32, I64, I64, P, I32, I32, P, I64, I64, P],
-    "vk_colsum": [I32, I32, P, P, P],
+    "vk_tc_gemm": [I32, I32, I32, P, I64, I64, P, I32, I64, I64, P, I32, I32, P, I64, I64, P, I64, P, P],
+    "vk_colsum": [I32, I32, P, P, P, I64, P, P],
     "vk_relu_mask": [I64, P, P, P],
     "vk_bce": [I32, P, P, P, F32, P, P, P],
     "vk_adam": [I64, P, P, P, P, F32, F32, F32, F32, I32, F32, P, P],
@@ -145,6 +146,10 @@ def lib():
     L.vk_tindex_bitmap_bytes.restype = I64
     L.vk_mlp_infer_tc_smem.argtypes = []
     L.vk_mlp_infer_tc_smem.restype = I64
+    L.vk_tc_gemm_ws_floats.argtypes = [I32, I32, I32]
+    L.vk_tc_gemm_ws_floats.restype = I64
+    L.vk_colsum_ws_floats.argtypes = [I32, I32]
+    L.vk_colsum_ws_floats.restype = I64
     _lib = L
     return L
 

@@ -11,8 +11,12 @@ label-free and pair closure runs after the pruning, so targets and decoys are tr
 Features per hit (``vk_cand_features``): K1 shared-peak count, summed matched intensity (fraction of the spectrum's
 TIC, K1's fixed-point sums), precursor error in ppm, precursor charge, peptide length, missed cleavages.
 Network: 16 -> 256 (ReLU) -> 256 (ReLU) -> 1, BF16 weights and layer-1 activations, FP32 accumulation; inference
-on the tcgen05 tensor cores (``vk_mlp_infer_tc``; ``vk_mlp_infer`` is the mma.sync variant), training by the deterministic kernels of ``mlp_train.cu`` (forward, backward,
-weighted BCE, Adam) on the GPU.  Training target: the hit, itself or through its pair-closure partner, lands in the
+on the tcgen05 tensor cores (``vk_mlp_infer_tc``; ``vk_mlp_infer`` is the mma.sync variant).  Training on the GPU
+by the project's own kernels: the forward and backward GEMMs of the 256-wide layers on the tcgen05 tensor cores
+(``vk_tc_gemm``: BF16 operands, FP32 accumulation, K split over the batch for the weight gradients), the rest --
+the 1-wide layer, weighted BCE, ReLU masks, bias sums, Adam -- by the kernels of ``mlp_train.cu``;
+``train_gemm="simt"`` runs every GEMM on its FP32 SIMT kernel instead, in a fixed summation order (the pass the
+oracle reproduces bit for bit).  Training target: the hit, itself or through its pair-closure partner, lands in the
 top 5 of the exhaustive rescoring of its spectrum (K2 over every row of the precursor windows).
 """
 from __future__ import annotations
@@ -45,7 +49,8 @@ class Pruner:
     selection parameters (``tau``, ``min_keep``, ``max_keep``)."""
 
     def __init__(self, device="cuda", seed: int = 0, tau: float = -math.inf, min_keep: int = 1,
-                 max_keep: int = 128, min_count: int = 1, tensor_cores: str = "tcgen05"):
+                 max_keep: int = 128, min_count: int = 1, tensor_cores: str = "tcgen05",
+                 train_gemm: str = "tcgen05"):
         self.dev = torch.device(device)
         g = torch.Generator().manual_seed(seed)
         W1 = torch.zeros(HIDDEN, N_IN)
@@ -61,6 +66,9 @@ class Pruner:
         if tensor_cores not in ("tcgen05", "mma.sync"):
             raise ValueError("tensor_cores must be 'tcgen05' or 'mma.sync'")
         self.tensor_cores = tensor_cores    # inference kernel: vk_mlp_infer_tc or vk_mlp_infer
+        if train_gemm not in ("tcgen05", "simt"):
+            raise ValueError("train_gemm must be 'tcgen05' or 'simt'")
+        self.train_gemm = train_gemm        # training GEMMs: vk_tc_gemm or the FP32 SIMT vk_gemm
         self.step = 0
         self._adam = None
         self._sync_bf16()
@@ -144,22 +152,48 @@ class Pruner:
             f = lambda *s: torch.empty(*s, dtype=torch.float32, device=self.dev)  # noqa: E731
             self._buf = {"H1": f(B, HIDDEN), "H2": f(B, HIDDEN), "z": f(B), "dz": f(B), "dH2": f(B, HIDDEN),
                          "dH1": f(B, HIDDEN), "loss": f((B + 255) // 256)}
+            L = K.lib()
+            ws = max(L.vk_tc_gemm_ws_floats(m, n, k) for m, n, k in ((B, HIDDEN, N_IN), (B, HIDDEN, HIDDEN),
+                                                                   (HIDDEN, HIDDEN, B), (HIDDEN, N_IN, B)))
+            self._buf["ws"] = f(max(ws, 1))
+            self._buf["ws_cs"] = f(max(L.vk_colsum_ws_floats(B, HIDDEN), 1))
+            self._buf["status"] = torch.zeros(1, dtype=torch.int32, device=self.dev)
             self._grad = {k: torch.zeros_like(v) for k, v in self.w.items()}
             self._buf_B = B
         if self._adam is None:
             self._adam = {k: (torch.zeros_like(v), torch.zeros_like(v)) for k, v in self.w.items()}
         return self._buf, self._grad
 
+    def _gemm(self, M, N, Kd, A, sam, sak, Bm, b_bf16, sbk, sbn, bias, relu, rnd, Cm, scm, scn, what):
+        """C[M, N] = A[M, K] B[K, N] (+ bias) (ReLU) (BF16 rounding), A FP32 and B BF16 / FP32 given by strides:
+        on the tensor cores (``vk_tc_gemm``) when N is a multiple of 16 and ``train_gemm`` is "tcgen05", else on
+        the FP32 SIMT kernel (``vk_gemm``)."""
+        L = K.lib()
+        if self.train_gemm == "tcgen05" and N % 16 == 0:
+            bf = self._buf
+            K.check(L.vk_tc_gemm(M, N, Kd, K.ptr(A), sam, sak, K.ptr(Bm), b_bf16, sbk, sbn, K.ptr(bias), relu, rnd,
+                                 K.ptr(Cm), scm, scn, K.ptr(bf["ws"]), bf["ws"].numel(), K.ptr(bf["status"]),
+                                 K.stream()), what)
+        else:
+            K.check(L.vk_gemm(M, N, Kd, K.ptr(A), sam, sak, K.ptr(Bm), b_bf16, sbk, sbn, K.ptr(bias), relu, rnd,
+                              K.ptr(Cm), scm, scn, K.stream()), what)
+
+    def _colsum(self, n, o, D, v, out, what):
+        """out[j] = sum_i D[i, j] (v[i] D[i, j] with a row weight v), in ``vk_colsum``'s fixed chunked order."""
+        ws = self._buf["ws_cs"]
+        K.check(K.lib().vk_colsum(n, o, K.ptr(D), K.ptr(v), K.ptr(ws), ws.numel(), K.ptr(out), K.stream()), what)
+
     def forward_train(self, X: torch.Tensor, B: int):
         """Training forward of B rows of FP32 features X [B, 16] (BF16 values): H1 (ReLU, rounded to BF16), H2
-        (ReLU), logits z -- the arithmetic of the inference kernel in a fixed summation order."""
+        (ReLU), logits z -- the arithmetic of the inference kernel (in a fixed summation order with
+        ``train_gemm="simt"``)."""
         L = K.lib()
         bf, g = self._buffers(B)
         w, st = self.w, K.stream()
-        K.check(L.vk_gemm(B, HIDDEN, N_IN, K.ptr(X), N_IN, 1, K.ptr(self.bf["W1"]), 1, 1, N_IN, K.ptr(w["b1"]), 1,
-                          1, K.ptr(bf["H1"]), HIDDEN, 1, st), "gemm_l1")
-        K.check(L.vk_gemm(B, HIDDEN, HIDDEN, K.ptr(bf["H1"]), HIDDEN, 1, K.ptr(self.bf["W2"]), 1, 1, HIDDEN,
-                          K.ptr(w["b2"]), 1, 0, K.ptr(bf["H2"]), HIDDEN, 1, st), "gemm_l2")
+        self._gemm(B, HIDDEN, N_IN, X, N_IN, 1, self.bf["W1"], 1, 1, N_IN, w["b1"], 1, 1, bf["H1"], HIDDEN, 1,
+                   "gemm_l1")
+        self._gemm(B, HIDDEN, HIDDEN, bf["H1"], HIDDEN, 1, self.bf["W2"], 1, 1, HIDDEN, w["b2"], 1, 0, bf["H2"],
+                   HIDDEN, 1, "gemm_l2")
         K.check(L.vk_gemm(B, 1, HIDDEN, K.ptr(bf["H2"]), HIDDEN, 1, K.ptr(w["w3"]), 0, 1, 0, K.ptr(w["b3"]), 0, 0,
                           K.ptr(bf["z"]), 1, 0, st), "gemm_l3")
         return bf["z"][:B]
@@ -171,24 +205,23 @@ class Pruner:
         w, st = self.w, K.stream()
         K.check(L.vk_bce(B, K.ptr(bf["z"]), K.ptr(y), K.ptr(wt), inv_wsum, K.ptr(bf["dz"]), K.ptr(bf["loss"]), st),
                 "bce")
-        # layer 3: gw3[j] = sum_b H2[b, j] dz[b]; gb3 = sum_b dz[b]; dH2[b, j] = dz[b] w3[j] (H2 > 0)
-        K.check(L.vk_gemm(HIDDEN, 1, B, K.ptr(bf["H2"]), 1, HIDDEN, K.ptr(bf["dz"]), 0, 1, 0, None, 0, 0,
-                          K.ptr(g["w3"]), 1, 0, st), "gemm_gw3")
-        K.check(L.vk_colsum(B, 1, K.ptr(bf["dz"]), K.ptr(g["b3"]), st), "colsum_b3")
+        # layer 3: gw3[j] = sum_b H2[b, j] dz[b]; gb3 = sum_b dz[b] (chunked column sums); dH2[b, j] = dz[b] w3[j]
+        # (H2 > 0)
+        self._colsum(B, HIDDEN, bf["H2"], bf["dz"], g["w3"], "colsum_w3")
+        self._colsum(B, 1, bf["dz"], None, g["b3"], "colsum_b3")
         K.check(L.vk_gemm(B, HIDDEN, 1, K.ptr(bf["dz"]), 1, 0, K.ptr(w["w3"]), 0, 0, 1, None, 0, 0,
                           K.ptr(bf["dH2"]), HIDDEN, 1, st), "gemm_dh2")
         K.check(L.vk_relu_mask(B * HIDDEN, K.ptr(bf["H2"]), K.ptr(bf["dH2"]), st), "relu_mask2")
         # layer 2: gW2[o, i] = sum_b dH2[b, o] H1[b, i]; gb2; dH1[b, i] = sum_o dH2[b, o] W2[o, i] (H1 > 0)
-        K.check(L.vk_gemm(HIDDEN, HIDDEN, B, K.ptr(bf["dH2"]), 1, HIDDEN, K.ptr(bf["H1"]), 0, HIDDEN, 1, None, 0, 0,
-                          K.ptr(g["W2"]), HIDDEN, 1, st), "gemm_gw2")
-        K.check(L.vk_colsum(B, HIDDEN, K.ptr(bf["dH2"]), K.ptr(g["b2"]), st), "colsum_b2")
-        K.check(L.vk_gemm(B, HIDDEN, HIDDEN, K.ptr(bf["dH2"]), HIDDEN, 1, K.ptr(self.bf["W2"]), 1, HIDDEN, 1, None,
-                          0, 0, K.ptr(bf["dH1"]), HIDDEN, 1, st), "gemm_dh1")
+        self._gemm(HIDDEN, HIDDEN, B, bf["dH2"], 1, HIDDEN, bf["H1"], 0, HIDDEN, 1, None, 0, 0, g["W2"], HIDDEN, 1,
+                   "gemm_gw2")
+        self._colsum(B, HIDDEN, bf["dH2"], None, g["b2"], "colsum_b2")
+        self._gemm(B, HIDDEN, HIDDEN, bf["dH2"], HIDDEN, 1, self.bf["W2"], 1, HIDDEN, 1, None, 0, 0, bf["dH1"],
+                   HIDDEN, 1, "gemm_dh1")
         K.check(L.vk_relu_mask(B * HIDDEN, K.ptr(bf["H1"]), K.ptr(bf["dH1"]), st), "relu_mask1")
         # layer 1: gW1[o, i] = sum_b dH1[b, o] X[b, i]; gb1
-        K.check(L.vk_gemm(HIDDEN, N_IN, B, K.ptr(bf["dH1"]), 1, HIDDEN, K.ptr(X), 0, N_IN, 1, None, 0, 0,
-                          K.ptr(g["W1"]), N_IN, 1, st), "gemm_gw1")
-        K.check(L.vk_colsum(B, HIDDEN, K.ptr(bf["dH1"]), K.ptr(g["b1"]), st), "colsum_b1")
+        self._gemm(HIDDEN, N_IN, B, bf["dH1"], 1, HIDDEN, X, 0, N_IN, 1, None, 0, 0, g["W1"], N_IN, 1, "gemm_gw1")
+        self._colsum(B, HIDDEN, bf["dH1"], None, g["b1"], "colsum_b1")
         return bf["loss"][:(B + 255) // 256], g
 
     def adam_step(self, lr: float, b1: float = 0.9, b2: float = 0.999, eps: float = 1e-8, wd: float = 0.0):
@@ -235,6 +268,7 @@ class Pruner:
                 self.adam_step(lr * 0.5 * (1.0 + math.cos(math.pi * frac)), wd=wd)
                 tot += loss.sum()
             losses.append(float(tot) / max(n_batch, 1))
+            E.check_status(self._buf["status"], "training GEMM")
             if log:
                 log(f"epoch {ep}: loss {losses[-1]:.5f} ({time.perf_counter() - t0:.1f} s)")
         self._b3 = float(self.w["b3"].item())
