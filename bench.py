@@ -653,8 +653,20 @@ def _kernel_table(a, p, gi, run, flush, pr, dev):
     mlp = None
     if pruned:
         feat = so["feat"]
-        ms_f = timed(lambda: pr.features(gi, dh, win_off, None, hits, n_hit))
-        kern["cand_features_k"] = (ms_f, n_hit * 87)
+        # the shortlist's compaction with the features written on the way (the pass's form), on select_hits' slots
+        c_off = E._scan(tk_n[:n])
+        cc = {k: torch.empty(max(n * cap, 1), dtype=torch.int64, device=dev) for k in ("h", "r", "c")}
+        c32 = torch.empty(max(n * cap, 1), dtype=torch.int32, device=dev)
+        cmf = torch.empty(max(n * cap, 1), dtype=torch.int8, device=dev)
+        cis = torch.empty(max(n * cap, 1), dtype=torch.int32, device=dev)
+        fe = torch.empty(max(n * cap, 1), 16, dtype=torch.bfloat16, device=dev)
+        ms_f = timed(lambda: K.check(L.vk_compact_hits_features(
+            n, cap, K.ptr(tk_n), K.ptr(c_off), K.ptr(tk["h"]), K.ptr(tk["r"]), K.ptr(tk["c"]), K.ptr(ti),
+            K.ptr(dh["maxfz"]), K.ptr(cc["h"]), K.ptr(cc["r"]), K.ptr(cc["c"]), K.ptr(c32), K.ptr(cmf), K.ptr(cis),
+            K.ptr(dh["M"]), K.ptr(dh["z"]), K.ptr(gi.mass32), K.ptr(gi.length), K.ptr(gi.missed), K.ptr(pr.mu),
+            K.ptr(pr.sd), K.ptr(fe), K.stream()), "compact_hits_features"))
+        # per hit: its slot read (28 B), hypothesis / row gathers (12 B), compacted columns (33 B), features (32 B)
+        kern["compact_hits_features_k"] = (ms_f, n_hit * 105)
         ms_m = timed(lambda: pr.logits(feat, n_hit))
         flops = 2 * n_hit * (16 * 256 + 256 * 256 + 256)
         mlp_name = "mlp_infer_tc_k" if pr.tensor_cores == "tcgen05" else "mlp_infer_k"

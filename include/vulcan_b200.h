@@ -471,11 +471,22 @@ int vk_search_fused_grid(const vk_tindex* ix, int warps, int topk, int pair_clos
  * intensity (isum of vk_k1_tiles / 2^24, a fraction of the TIC; isum[win_off[h] + row - lo[h]], or isum[i] for
  * candidate i when win_off is NULL, e.g. vk_select_hits' c_isum compacted), precursor error in ppm
  * ((M_hyp - mass32[row]) / mass32[row] * 1e6), charge, peptide length, missed cleavages; zero padded.
- * n bounds the buffers; when n_dev is given the device count *n_dev (<= n) is used instead (no host sync). */
+ * n bounds the buffers; when n_dev is given the device count *n_dev (<= n) is used instead (no host sync).  feat
+ * 16-byte aligned (two 16-byte stores per hit). */
 int vk_cand_features(int64_t n, const int64_t* n_dev, const int64_t* c_hyp, const int64_t* c_row,
                      const int64_t* c_cnt, const int64_t* win_off, const int64_t* h_lo, const uint32_t* isum,
                      const float* h_M, const int8_t* h_z, const float* mass32, const uint8_t* len,
                      const uint8_t* missed, const float* mu, const float* sd, void* feat_bf16, void* stream);
+/* vk_compact_hits with the features on the way: the compacted hits as vk_compact_hits writes them (s_isum / c_isum
+ * required) and, for every hit, the 16 standardised BF16 features vk_cand_features gives it, into feat (device,
+ * 16-byte aligned, 16 BF16 per hit at the hit's compacted position; h_M, h_z the hypotheses' columns, mass32 /
+ * length / missed the index rows'). */
+int vk_compact_hits_features(int n_spec, int cap, const int64_t* n_cand, const int64_t* cand_off,
+                             const int64_t* s_hyp, const int64_t* s_row, const int64_t* s_cnt, const uint32_t* s_isum,
+                             const int8_t* h_maxfz, int64_t* c_hyp, int64_t* c_row, int64_t* c_cnt, int32_t* c_row32,
+                             int8_t* c_maxfz, uint32_t* c_isum, const float* h_M, const int8_t* h_z,
+                             const float* mass32, const uint8_t* len, const uint8_t* missed, const float* mu,
+                             const float* sd, void* feat_bf16, void* stream);
 /* MLP logits of n feature rows (16 BF16 each; n_dev as above): W1 [256 x 16] and W2 [256 x 256] BF16 row-major,
  * b1, b2, w3 (256) FP32, scalar b3; tensor cores (mma.sync BF16, FP32 accumulate); `grid` persistent CTAs of 256
  * threads, each holding the weights in vk_mlp_infer_smem() bytes of shared memory. */

@@ -154,3 +154,33 @@ def test_small_k1_shapes_per_peak_bucket_give_the_same_search(small):
 def torch_equal(x, y):
     import torch
     return bool(torch.equal(x, y))
+
+
+@pytest.mark.parametrize("min_count", (1, 2))
+def test_human_hit_lists_give_the_dense_shortlist(human, min_count):
+    """On the whole human run, the pruned path's front end over K1 hit lists (``vk_k1_hits`` + ``vk_select_hits``)
+    gives the shortlist, intensity sums and statistics of the dense form (``vk_k1_tiles`` + ``vk_select_topk``).
+    With a count floor of 1 most spectra hold more hits than ``vk_select_hits`` keeps in shared memory, so its
+    global-memory selection is compared too."""
+    from vulcan.gpu import engine as E
+    from vulcan.gpu import prune as PR
+    w, l1, sp, p, gi, P = human
+    st = E.Stats()
+    fh = PR._front(E.DeviceRun(sp, gi.dev, st), gi, p, st, False, min_count=min_count)
+    fd = PR._front(E.DeviceRun(sp, gi.dev, st), gi, p, st, False, min_count=min_count, dense=True)
+    E.check_status(fh["status"])
+    E.check_status(fd["status"])
+    n = len(sp)
+    nc = int(fd["hits"]["cand_off"][n])
+    assert int(fh["hits"]["cand_off"][n]) == nc and nc > 100_000
+    for k in ("c_hyp", "c_row", "c_cnt"):
+        assert torch_equal(fh["hits"][k][:nc], fd["hits"][k][:nc]), k
+    dh, hits = fd["dh"], fd["hits"]
+    h = hits["c_hyp"][:nc]
+    dense_isum = fd["isum"][fd["win_off"][h] + hits["c_row"][:nc] - dh["lo"][h]]
+    assert torch_equal(fh["hits"]["c_isum"][:nc], dense_isum)
+    for k in ("spec_scored", "spec_matched"):
+        assert torch_equal(fh[k][:n], fd[k][:n]), k
+    if min_count == 1:   # spectra whose hits outnumber the top-k: the selection ran (over global memory for most)
+        per_spec = fh["hits"]["cand_off"][1:n + 1] - fh["hits"]["cand_off"][:n]
+        assert int((per_spec == p.topk).sum()) > 1000

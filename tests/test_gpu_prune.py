@@ -191,6 +191,29 @@ def test_training_pass_equals_oracle(torch_cuda, B):
     np.testing.assert_array_equal(_np(pr.bf["W2"].float()), M.bf16_round(_np(pr.w["W2"])))
 
 
+def test_compacted_features_equal_the_features_kernel(mini, param_sets, indexes, torch_cuda):
+    """The pruned front end's compaction writes every shortlist hit's features (``vk_compact_hits_features``):
+    the rows ``vk_cand_features`` computes from the compacted hits, bit for bit."""
+    torch = torch_cuda
+    from vulcan.gpu import engine as E
+    from vulcan.gpu import prune as PR
+    l1, sp, _ = mini
+    for name in SETS:
+        p = param_sets[name]
+        gi = indexes[name]
+        pr = PR.Pruner(gi.dev, seed=3)
+        g = torch.Generator(device="cpu").manual_seed(4)
+        pr.mu[:6] = (torch.randn(6, generator=g) * 2).to(gi.dev)
+        pr.sd[:6] = (0.5 + torch.rand(6, generator=g)).to(gi.dev)
+        st = E.Stats()
+        f = PR._front(E.DeviceRun(sp, gi.dev, st), gi, p, st, False, min_count=1, pr=pr)
+        hits = f["hits"]
+        nc = int(hits["cand_off"][len(sp)])
+        assert nc > 100 and "feat" in hits
+        want = pr.features(gi, f["dh"], f["win_off"], None, hits, nc)
+        assert torch.equal(hits["feat"][:nc], want[:nc]), name
+
+
 def _rel(a, b):
     return float(np.linalg.norm(np.asarray(a, np.float64) - np.asarray(b, np.float64)) /
                  max(np.linalg.norm(np.asarray(b, np.float64)), 1e-30))

@@ -29,6 +29,33 @@ constexpr int W2_STRIDE = MLP_H + 8;    // bf16 elements per W2 row in shared me
 constexpr int INF_WARPS = 8;
 
 // ------------------------------------------------------------------------------------------------ features
+// The 16 standardised BF16 features of one hit (hypothesis h, row r, K1 count, fixed-point intensity sum) into
+// feat_row (32 bytes, 16-byte aligned): the six used ones first, the rest zero.
+__device__ __forceinline__ void hit_features(int64_t h, int64_t r, int64_t cnt, uint32_t isum_fx, const float* h_M,
+                                             const int8_t* h_z, const float* mass32, const uint8_t* len,
+                                             const uint8_t* missed, const float* mu, const float* sd,
+                                             __nv_bfloat16* feat_row) {
+  const float mr = mass32[r];
+  float raw[6];
+  raw[0] = (float)cnt;
+  raw[1] = (float)isum_fx * (1.0f / 16777216.0f);
+  raw[2] = (h_M[h] - mr) / mr * 1.0e6f;
+  raw[3] = (float)h_z[h];
+  raw[4] = (float)len[r];
+  raw[5] = (float)missed[r];
+  __nv_bfloat162 v0 = __floats2bfloat162_rn((raw[0] - mu[0]) / sd[0], (raw[1] - mu[1]) / sd[1]);
+  __nv_bfloat162 v1 = __floats2bfloat162_rn((raw[2] - mu[2]) / sd[2], (raw[3] - mu[3]) / sd[3]);
+  __nv_bfloat162 v2 = __floats2bfloat162_rn((raw[4] - mu[4]) / sd[4], (raw[5] - mu[5]) / sd[5]);
+  uint4 a;
+  a.x = *reinterpret_cast<uint32_t*>(&v0);
+  a.y = *reinterpret_cast<uint32_t*>(&v1);
+  a.z = *reinterpret_cast<uint32_t*>(&v2);
+  a.w = 0u;
+  uint4* f = reinterpret_cast<uint4*>(feat_row);
+  f[0] = a;
+  f[1] = make_uint4(0u, 0u, 0u, 0u);
+}
+
 // One thread per candidate hit (hypothesis, row, count): its window position is win_off[h] + row - lo[h].
 __global__ void cand_features_k(int64_t n, const int64_t* n_dev, const int64_t* c_hyp, const int64_t* c_row,
                                 const int64_t* c_cnt, const int64_t* win_off, const int64_t* h_lo, const uint32_t* isum,
@@ -38,23 +65,36 @@ __global__ void cand_features_k(int64_t n, const int64_t* n_dev, const int64_t* 
   if (n_dev) n = min(n, *n_dev);
   if (i >= n) return;
   const int64_t h = c_hyp[i], r = c_row[i];
-  const float mr = mass32[r];
-  float raw[6];
-  raw[0] = (float)c_cnt[i];
   // the intensity sum from the dense K1 sums, or (win_off NULL) one per candidate, from the hit-list shortlist
-  raw[1] = (float)(win_off ? isum[win_off[h] + (r - h_lo[h])] : isum[i]) * (1.0f / 16777216.0f);
-  raw[2] = (h_M[h] - mr) / mr * 1.0e6f;
-  raw[3] = (float)h_z[h];
-  raw[4] = (float)len[r];
-  raw[5] = (float)missed[r];
-  uint32_t* f = reinterpret_cast<uint32_t*>(feat + i * MLP_IN);
-  __nv_bfloat162 v0 = __floats2bfloat162_rn((raw[0] - mu[0]) / sd[0], (raw[1] - mu[1]) / sd[1]);
-  __nv_bfloat162 v1 = __floats2bfloat162_rn((raw[2] - mu[2]) / sd[2], (raw[3] - mu[3]) / sd[3]);
-  __nv_bfloat162 v2 = __floats2bfloat162_rn((raw[4] - mu[4]) / sd[4], (raw[5] - mu[5]) / sd[5]);
-  f[0] = *reinterpret_cast<uint32_t*>(&v0);
-  f[1] = *reinterpret_cast<uint32_t*>(&v1);
-  f[2] = *reinterpret_cast<uint32_t*>(&v2);
-  for (int k = 3; k < MLP_IN / 2; ++k) f[k] = 0u;
+  const uint32_t is = win_off ? isum[win_off[h] + (r - h_lo[h])] : isum[i];
+  hit_features(h, r, c_cnt[i], is, h_M, h_z, mass32, len, missed, mu, sd, feat + i * MLP_IN);
+}
+
+// The hit-list shortlist's per-spectrum slots compacted (as vk_compact_hits does) and every hit's features written
+// on the way, one warp per spectrum: the features kernel's second read of the compacted hits is saved.
+constexpr int CF_WARPS = 8;
+
+__global__ void __launch_bounds__(CF_WARPS * 32)
+compact_features_k(int n_spec, int cap, const int64_t* n_cand, const int64_t* cand_off, const int64_t* s_hyp,
+                   const int64_t* s_row, const int64_t* s_cnt, const uint32_t* s_isum, const int8_t* h_maxfz,
+                   int64_t* c_hyp, int64_t* c_row, int64_t* c_cnt, int32_t* c_row32, int8_t* c_maxfz,
+                   uint32_t* c_isum, const float* h_M, const int8_t* h_z, const float* mass32, const uint8_t* len,
+                   const uint8_t* missed, const float* mu, const float* sd, __nv_bfloat16* feat) {
+  const int s = blockIdx.x * CF_WARPS + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (s >= n_spec) return;
+  const int64_t m = min(n_cand[s], (int64_t)cap), dst0 = cand_off[s], src0 = (int64_t)s * cap;
+  for (int64_t j = lane; j < m; j += 32) {
+    const int64_t src = src0 + j, dst = dst0 + j;
+    const int64_t h = s_hyp[src], r = s_row[src], c = s_cnt[src];
+    const uint32_t is = s_isum[src];
+    c_hyp[dst] = h;
+    c_row[dst] = r;
+    c_cnt[dst] = c;
+    c_row32[dst] = (int32_t)r;
+    c_maxfz[dst] = h_maxfz[h];
+    c_isum[dst] = is;
+    hit_features(h, r, c, is, h_M, h_z, mass32, len, missed, mu, sd, feat + dst * MLP_IN);
+  }
 }
 
 // ------------------------------------------------------------------------------------------------ MLP inference
@@ -337,9 +377,24 @@ int vk_cand_features(int64_t n, const int64_t* n_dev, const int64_t* c_hyp, cons
                      const float* h_M, const int8_t* h_z, const float* mass32, const uint8_t* len,
                      const uint8_t* missed, const float* mu, const float* sd, void* feat_bf16, void* stream) {
   if (n <= 0) return 0;
+  if (!feat_bf16 || ((uintptr_t)feat_bf16 & 15)) return VK_E_ARG;
   cand_features_k<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
       n, n_dev, c_hyp, c_row, c_cnt, win_off, h_lo, isum, h_M, h_z, mass32, len, missed, mu, sd,
       reinterpret_cast<__nv_bfloat16*>(feat_bf16));
+  return vk_launch_status();
+}
+
+int vk_compact_hits_features(int n_spec, int cap, const int64_t* n_cand, const int64_t* cand_off,
+                             const int64_t* s_hyp, const int64_t* s_row, const int64_t* s_cnt, const uint32_t* s_isum,
+                             const int8_t* h_maxfz, int64_t* c_hyp, int64_t* c_row, int64_t* c_cnt, int32_t* c_row32,
+                             int8_t* c_maxfz, uint32_t* c_isum, const float* h_M, const int8_t* h_z,
+                             const float* mass32, const uint8_t* len, const uint8_t* missed, const float* mu,
+                             const float* sd, void* feat_bf16, void* stream) {
+  if (n_spec == 0) return 0;
+  if (!s_isum || !c_isum || !mu || !sd || !feat_bf16 || ((uintptr_t)feat_bf16 & 15)) return VK_E_ARG;
+  compact_features_k<<<(unsigned)((n_spec + CF_WARPS - 1) / CF_WARPS), CF_WARPS * 32, 0, (cudaStream_t)stream>>>(
+      n_spec, cap, n_cand, cand_off, s_hyp, s_row, s_cnt, s_isum, h_maxfz, c_hyp, c_row, c_cnt, c_row32, c_maxfz,
+      c_isum, h_M, h_z, mass32, len, missed, mu, sd, reinterpret_cast<__nv_bfloat16*>(feat_bf16));
   return vk_launch_status();
 }
 

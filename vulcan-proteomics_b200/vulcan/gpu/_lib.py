@@ -98,6 +98,7 @@ _SIGS_B200 = {
                    P, P, I32, I64, P],
     "vk_select_hits": [I32, P, P, P, P, P, P, P, P, P, P, I32, I32, P, I32, P, P, P, P, P, P, P, P],
     "vk_compact_hits": [I32, I32, P, P, P, P, P, P, P, P, P, P, P, P, P, P],
+    "vk_compact_hits_features": [I32, I32, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P],
     "vk_tindex_bitmap": [P, P, P],
     "vk_select_topk": [I32, P, P, P, P, P, I64, P, I32, I32, I32, I32, P, P, P, P, P, P, P, P, P],
     "vk_compact_cands": [I32, I32, P, P, P, P, P, P, P, P, P, P, P, P],

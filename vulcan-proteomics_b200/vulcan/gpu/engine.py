@@ -634,11 +634,13 @@ def _k1_hits(gi: GpuIndex, dh, peaks, p: SearchParams, n_hyp: int, thr: int, isu
             "hyp_scored": hyp_scored, "hyp_matched": hyp_matched}
 
 
-def _shortlist_hits(gi: GpuIndex, p: SearchParams, n: int, dh, k1h: dict, topk: int, closure: bool = False):
+def _shortlist_hits(gi: GpuIndex, p: SearchParams, n: int, dh, k1h: dict, topk: int, closure: bool = False,
+                    features=None):
     """Top-k of every spectrum by K1 count among its hit lists (``vk_select_hits``), optionally with pair closure,
     compacted to spectrum-ordered candidate lists with their intensity sums (``c_isum``); the same candidates as
-    ``_shortlist`` over the dense counts.  Returns the candidate dict and the per-hypothesis / per-spectrum K1
-    sums."""
+    ``_shortlist`` over the dense counts.  ``features`` = (index, mu, sd): the compaction also writes every hit's
+    standardised BF16 features (``vk_compact_hits_features``, the rows ``vk_cand_features`` gives) as "feat".
+    Returns the candidate dict and the per-hypothesis / per-spectrum K1 sums."""
     L = K.lib()
     dev = gi.dev
     cap = (2 if closure else 1) * topk
@@ -665,12 +667,25 @@ def _shortlist_hits(gi: GpuIndex, p: SearchParams, n: int, dh, k1h: dict, topk: 
     c_row32 = torch.empty(max(n * cap, 1), dtype=torch.int32, device=dev)
     c_maxfz = torch.empty(max(n * cap, 1), dtype=torch.int8, device=dev)
     c_isum = torch.empty(max(n * cap, 1), dtype=torch.int32, device=dev) if isum else None
-    K.check(L.vk_compact_hits(n, cap, K.ptr(n_cand), K.ptr(cand_off), K.ptr(s_hyp), K.ptr(s_row), K.ptr(s_cnt),
-                              K.ptr(s_isum) if isum else None, K.ptr(dh["maxfz"]), K.ptr(c_hyp), K.ptr(c_row),
-                              K.ptr(c_cnt), K.ptr(c_row32), K.ptr(c_maxfz), K.ptr(c_isum) if isum else None,
-                              K.stream()), "compact_hits")
+    feat = None
+    if features is not None and isum:
+        fi, mu, sd = features
+        feat = torch.empty(max(n * cap, 1), 16, dtype=torch.bfloat16, device=dev)
+        K.check(L.vk_compact_hits_features(n, cap, K.ptr(n_cand), K.ptr(cand_off), K.ptr(s_hyp), K.ptr(s_row),
+                                           K.ptr(s_cnt), K.ptr(s_isum), K.ptr(dh["maxfz"]), K.ptr(c_hyp),
+                                           K.ptr(c_row), K.ptr(c_cnt), K.ptr(c_row32), K.ptr(c_maxfz), K.ptr(c_isum),
+                                           K.ptr(dh["M"]), K.ptr(dh["z"]), K.ptr(fi.mass32), K.ptr(fi.length),
+                                           K.ptr(fi.missed), K.ptr(mu), K.ptr(sd), K.ptr(feat), K.stream()),
+                "compact_hits_features")
+    else:
+        K.check(L.vk_compact_hits(n, cap, K.ptr(n_cand), K.ptr(cand_off), K.ptr(s_hyp), K.ptr(s_row), K.ptr(s_cnt),
+                                  K.ptr(s_isum) if isum else None, K.ptr(dh["maxfz"]), K.ptr(c_hyp), K.ptr(c_row),
+                                  K.ptr(c_cnt), K.ptr(c_row32), K.ptr(c_maxfz), K.ptr(c_isum) if isum else None,
+                                  K.stream()), "compact_hits")
     cand = {"cand_off": cand_off, "c_hyp": c_hyp, "c_row": c_row, "c_cnt": c_cnt, "c_row32": c_row32,
             "c_maxfz": c_maxfz, "cap": cap, "n_cand": n_cand, "c_isum": c_isum}
+    if feat is not None:
+        cand["feat"] = feat
     sums = {"hyp_scored": k1h["hyp_scored"], "hyp_matched": k1h["hyp_matched"], "spec_scored": spec_scored,
             "spec_matched": spec_matched}
     return cand, sums

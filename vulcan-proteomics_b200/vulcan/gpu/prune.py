@@ -285,11 +285,12 @@ class CountRanker(Pruner):
 
 # ---------------------------------------------------------------------------------------------- search
 def _front(run: E.DeviceRun, gi: E.GpuIndex, p: SearchParams, st: E.Stats, timers: bool, min_count: int = 1,
-           dense: bool = False):
+           dense: bool = False, pr: "Pruner | None" = None):
     """K0, hypotheses, K1 with intensity sums, and the top-k shortlist (hits with count >= min_count) without pair
     closure.  K1 writes hit lists (``vk_k1_hits``: only the rows with count >= the floor) and the shortlist reads
     them; ``dense``: K1's dense per-row counts and sums and the shortlist over those instead (same shortlist; the
-    dense arrays are returned as "cnt" / "isum")."""
+    dense arrays are returned as "cnt" / "isum").  With a pruner ``pr`` (hit lists) the compaction of the shortlist
+    also writes its standardised features, as ``hits["feat"]``."""
     dev = gi.dev
     n = run.n
     thr = max(p.k1_threshold, min_count)
@@ -310,7 +311,8 @@ def _front(run: E.DeviceRun, gi: E.GpuIndex, p: SearchParams, st: E.Stats, timer
     with phase("k1"):
         k1h = E._k1_hits(gi, dh, peaks, p, dh["n_max"], thr, isum=True)
     with phase("topk"):
-        hits, sums = E._shortlist_hits(gi, p, n, dh, k1h, p.topk)
+        hits, sums = E._shortlist_hits(gi, p, n, dh, k1h, p.topk,
+                                       features=(gi, pr.mu, pr.sd) if pr is not None else None)
     return {"peaks": peaks, "dh": dh, "win_off": k1h["win_off"], "status": k1h["status"], "k1_hits": k1h,
             "hits": hits, **sums}
 
@@ -322,7 +324,7 @@ def _pruned_device(run: E.DeviceRun, gi: E.GpuIndex, p: SearchParams, pr: Pruner
     L = K.lib()
     dev = gi.dev
     n = run.n
-    f = _front(run, gi, p, st, timers, pr.min_count)
+    f = _front(run, gi, p, st, timers, pr.min_count, pr=pr)
     hits = f["hits"]
     n_bound = n * hits["cap"]
     n_dev = hits["cand_off"][n:]
@@ -330,7 +332,8 @@ def _pruned_device(run: E.DeviceRun, gi: E.GpuIndex, p: SearchParams, pr: Pruner
     def phase(name):
         return E.Timer(st, name) if timers else E._NoTimer()
     with phase("prune"):
-        feat = pr.features(gi, f["dh"], f["win_off"], f.get("isum"), hits, n_bound, n_dev=n_dev)
+        feat = hits["feat"] if "feat" in hits else pr.features(gi, f["dh"], f["win_off"], f.get("isum"), hits,
+                                                                 n_bound, n_dev=n_dev)
         logit = pr.score(feat, hits, n_bound, n_dev=n_dev, status=f["status"])
         cap = (2 if p.pair_closure else 1) * pr.max_keep
         s_hyp = torch.empty(max(n * cap, 1), dtype=torch.int64, device=dev)
