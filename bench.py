@@ -259,7 +259,8 @@ def _pruner_setup(a, w, l1, lab, gi, p, rank):
     from vulcan.gpu import prune as PR
     if a.pruner != "train":
         pr = PR.Pruner.load(a.pruner, gi.dev)
-        return pr, {"source": os.path.basename(a.pruner), "tau": pr.tau, "min_count": pr.min_count}
+        return pr, {"source": os.path.basename(a.pruner), "tau": pr.tau, "min_count": pr.min_count,
+                    "shortlist_k": pr.shortlist_k}
     t0 = time.perf_counter()
     n_left, runs, i = a.train_spectra, [], 0
     while n_left > 0:
@@ -271,6 +272,7 @@ def _pruner_setup(a, w, l1, lab, gi, p, rank):
     t_sim = time.perf_counter() - t0
     pr, info = PR.train(gi, p, runs, calib, seed=rank, epochs=a.epochs, batch=8192, target=a.target)
     info.update(source="trained in this run", simulate_s=round(t_sim, 1), min_count=pr.min_count,
+                shortlist_k=pr.shortlist_k,
                 min_keep=pr.min_keep, max_keep=pr.max_keep, target=a.target,
                 losses=[round(x, 5) for x in info["losses"]])
     return pr, info
@@ -502,7 +504,8 @@ def run_b200(a):
                         "copy stream, graph replay on a compute stream, one D2H of the packed PSM slots on a third "
                         "stream, host PSM table" if use_graph else "engine.search"}
         if pruned:
-            extra["path"] = ("learned-pruned search: K1 (+ intensity sums) -> top-k shortlist of hits with count >= "
+            extra["path"] = ("learned-pruned search: K1 (+ intensity sums) -> shortlist of the top "
+                             f"{pr.shortlist_k or p.topk} hits by count with count >= "
                              f"{pr.min_count} -> BF16 MLP 16-256-256-1 -> logit >= calibrated tau or best "
                              f"{pr.min_keep} -> pair closure -> K2 -> ranking")
             extra["pruner"] = pr_info
@@ -622,7 +625,7 @@ def _kernel_table(a, p, gi, run, flush, pr, dev):
         sm_ = torch.empty(n, dtype=torch.int64, device=dev)
         ms_tk = timed(lambda: K.check(L.vk_select_hits(
             n, K.ptr(dh["spec_off"]), K.ptr(dh["lo"]), K.ptr(dh["hi"]), K.ptr(win_off), K.ptr(k1h["hyp_shift"]),
-            K.ptr(k1h["seg_cnt"]), K.ptr(k1h["rc"]), K.ptr(k1h["isum"]), K.ptr(k1h["hyp_scored"]), K.ptr(k1h["hyp_matched"]), p.topk, 0,
+            K.ptr(k1h["seg_cnt"]), K.ptr(k1h["rc"]), K.ptr(k1h["isum"]), K.ptr(k1h["hyp_scored"]), K.ptr(k1h["hyp_matched"]), cap, 0,
             None, cap, K.ptr(tk["h"]), K.ptr(tk["r"]),
             K.ptr(tk["c"]), K.ptr(ti), K.ptr(tk_n), K.ptr(ss_), K.ptr(sm_), K.stream()), "select_hits"))
         # hits read (12 B), per-hypothesis windows, totals and tile shift (33 B), per spectrum its hypothesis range

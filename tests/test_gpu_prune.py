@@ -363,6 +363,9 @@ def test_trained_pruner_small_workload(small):
     l1, lab, p, gi, runs = small
     pr, info = PR.train(gi, p, runs[:2], runs[2:3], epochs=3, batch=2048, target=0.9995)
     assert info["losses"][-1] < info["losses"][0]
+    assert pr.shortlist_k == 0 or pr.shortlist_k in PR.SHORTLIST_KS
+    back = PR.Pruner(gi.dev).load_state_dict(pr.state_dict())
+    assert (back.shortlist_k, back.min_count, back.tau) == (pr.shortlist_k, pr.min_count, pr.tau)
     ev = PR.evaluate(runs[3], gi, l1, lab, p, pr)
     assert ev["recall"] >= 0.998, ev
     assert ev["rescored_pruned"] < ev["rescored_plain"], ev

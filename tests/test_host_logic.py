@@ -128,3 +128,15 @@ def test_split_table_gives_each_run_its_own_rows():
 def test_searcher_refuses_an_empty_pipeline():
     with pytest.raises(ValueError):
         E.Searcher(None, None, None, depth=0)
+
+
+def test_shortlist_count_rank_follows_the_selection_keys():
+    """The calibration's count rank of a shortlist hit: its place in its spectrum by count descending, then row
+    descending, then hypothesis ascending -- the order of vk_select_hits' selection keys."""
+    from vulcan.gpu import prune as PR
+    spec = torch.tensor([0, 0, 0, 0, 1, 1, 1])
+    cnt = torch.tensor([3, 5, 3, 3, 2, 2, 9])
+    row = torch.tensor([10, 4, 12, 12, 7, 8, 1])
+    hyp = torch.tensor([0, 0, 2, 1, 3, 3, 4])
+    d = {"spec": spec, "cnt": cnt, "row": row, "hits": {"c_hyp": hyp}}
+    assert PR._count_rank(d).tolist() == [3, 0, 2, 1, 2, 1, 0]

@@ -63,6 +63,7 @@ class Pruner:
         self.sd = torch.ones(N_IN, device=self.dev)
         self.tau, self.min_keep, self.max_keep = float(tau), int(min_keep), int(max_keep)
         self.min_count = int(min_count)     # shortlist only hits with K1 count >= min_count (calibrated)
+        self.shortlist_k = 0                # shortlist the top shortlist_k hits by K1 count (calibrated; 0: top-k)
         if tensor_cores not in ("tcgen05", "mma.sync"):
             raise ValueError("tensor_cores must be 'tcgen05' or 'mma.sync'")
         self.tensor_cores = tensor_cores    # inference kernel: vk_mlp_infer_tc or vk_mlp_infer
@@ -86,7 +87,8 @@ class Pruner:
     def state_dict(self) -> dict:
         d = {k: v.detach().cpu().numpy() for k, v in self.w.items()}
         d.update(mu=self.mu.cpu().numpy(), sd=self.sd.cpu().numpy(),
-                 sel=np.array([self.tau, self.min_keep, self.max_keep, self.min_count], np.float64))
+                 sel=np.array([self.tau, self.min_keep, self.max_keep, self.min_count, self.shortlist_k],
+                              np.float64))
         return d
 
     def load_state_dict(self, d: dict):
@@ -94,9 +96,10 @@ class Pruner:
             self.w[k] = torch.from_numpy(np.asarray(d[k], np.float32)).to(self.dev).contiguous()
         self.mu = torch.from_numpy(np.asarray(d["mu"], np.float32)).to(self.dev)
         self.sd = torch.from_numpy(np.asarray(d["sd"], np.float32)).to(self.dev)
-        sel = [float(x) for x in d["sel"]] + [1.0]
+        sel = [float(x) for x in d["sel"]] + [1.0, 0.0]
         self.tau = sel[0]
         self.min_keep, self.max_keep, self.min_count = int(sel[1]), int(sel[2]), int(sel[3])
+        self.shortlist_k = int(sel[4]) if len(d["sel"]) > 4 else 0
         self._adam = None
         self._sync_bf16()
         return self
@@ -289,8 +292,9 @@ def _front(run: E.DeviceRun, gi: E.GpuIndex, p: SearchParams, st: E.Stats, timer
     """K0, hypotheses, K1 with intensity sums, and the top-k shortlist (hits with count >= min_count) without pair
     closure.  K1 writes hit lists (``vk_k1_hits``: only the rows with count >= the floor) and the shortlist reads
     them; ``dense``: K1's dense per-row counts and sums and the shortlist over those instead (same shortlist; the
-    dense arrays are returned as "cnt" / "isum").  With a pruner ``pr`` (hit lists) the compaction of the shortlist
-    also writes its standardised features, as ``hits["feat"]``."""
+    dense arrays are returned as "cnt" / "isum").  With a pruner ``pr`` (hit lists) the shortlist holds the top
+    ``pr.shortlist_k`` hits by count (when set) and its compaction also writes their standardised features, as
+    ``hits["feat"]``."""
     dev = gi.dev
     n = run.n
     thr = max(p.k1_threshold, min_count)
@@ -310,9 +314,9 @@ def _front(run: E.DeviceRun, gi: E.GpuIndex, p: SearchParams, st: E.Stats, timer
                 "hits": hits, **sums}
     with phase("k1"):
         k1h = E._k1_hits(gi, dh, peaks, p, dh["n_max"], thr, isum=True)
+    k = p.topk if pr is None or pr.shortlist_k <= 0 else min(p.topk, pr.shortlist_k)
     with phase("topk"):
-        hits, sums = E._shortlist_hits(gi, p, n, dh, k1h, p.topk,
-                                       features=(gi, pr.mu, pr.sd) if pr is not None else None)
+        hits, sums = E._shortlist_hits(gi, p, n, dh, k1h, k, features=(gi, pr.mu, pr.sd) if pr is not None else None)
     return {"peaks": peaks, "dh": dh, "win_off": k1h["win_off"], "status": k1h["status"], "k1_hits": k1h,
             "hits": hits, **sums}
 
@@ -442,13 +446,33 @@ def collect(sp: Spectra, gi: E.GpuIndex, p: SearchParams, pr: Pruner, raw: bool 
         return d
 
 
+SHORTLIST_KS = (8, 10, 12, 16, 20, 24, 32, 48, 64)
+
+
+def _count_rank(d) -> torch.Tensor:
+    """Rank of every shortlist hit inside its spectrum in the shortlist's own order: count descending, then row
+    descending, then hypothesis ascending (``vk_select_hits``' keys)."""
+    spec, cnt, row, hyp = d["spec"], d["cnt"], d["row"], d["hits"]["c_hyp"]
+    idx = torch.arange(len(spec), device=spec.device)
+    o = torch.argsort(hyp, stable=True)
+    o = o[torch.argsort(row[o], descending=True, stable=True)]
+    o = o[torch.argsort(cnt[o], descending=True, stable=True)]
+    o = o[torch.argsort(spec[o], stable=True)]
+    ss = spec[o]
+    first = torch.searchsorted(ss, ss, side="left")
+    rank = torch.empty_like(idx)
+    rank[o] = idx - first
+    return rank
+
+
 def calibrate(pr: Pruner, gi: E.GpuIndex, data: list[dict], target: float = 0.9995, count_share: float = 0.25,
-              max_count: int = 16) -> float:
+              max_count: int = 16, cap_share: float = 0.25) -> float:
     """Selection parameters from calibration runs (``collect`` data): the spectra with a plain-path top-1 PSM
     must keep a hit that brings that row (the row itself or its pair-closure partner) for at least ``target`` of
     them.  First ``min_count``: the largest shortlist count floor that loses at most ``count_share`` of the
-    allowed misses; then ``tau``: the largest threshold that loses no more than the rest, given ``min_keep`` and
-    ``max_keep``.  Sets both on the pruner and returns tau."""
+    allowed misses; then ``shortlist_k``: the smallest cap on the shortlist (its top hits by count) that loses at
+    most ``cap_share`` more; then ``tau``: the largest threshold that loses no more than the rest, given
+    ``min_keep`` and ``max_keep``.  Sets them on the pruner and returns tau."""
     dev = gi.dev
     per = []
     n_top = 0
@@ -469,20 +493,37 @@ def calibrate(pr: Pruner, gi: E.GpuIndex, data: list[dict], target: float = 0.99
             c0 = c
             break
     lost_c0 = sum(int((has & (bc < c0)).sum()) for _, _, _, bc, has in per)
-    need = []
+    # the best count rank of a hit bringing the top-1 row (count >= c0): a cap k loses the spectra where it is >= k
+    crank, br = [], []
     for d, z, good, bc, has in per:
-        f = d["cnt"] >= c0
+        cr = _count_rank(d)
+        g = good & (d["cnt"] >= c0)
+        crank.append(cr)
+        br.append(torch.full((d["n"],), 1 << 30, dtype=torch.int64, device=dev).scatter_reduce(
+            0, d["spec"][g], cr[g], reduce="amin"))
+    k_cap = 0
+    for k in SHORTLIST_KS:
+        lost = sum(int((has & (bc >= c0) & (b >= k)).sum()) for (_, _, _, bc, has), b in zip(per, br))
+        if lost <= int(math.floor(cap_share * allowed)):
+            k_cap = k
+            break
+    lost_k = lost_c0 + (sum(int((has & (bc >= c0) & (b >= k_cap)).sum()) for (_, _, _, bc, has), b in zip(per, br))
+                        if k_cap else 0)
+    need = []
+    for (d, z, good, bc, has), cr, b in zip(per, crank, br):
+        f = (d["cnt"] >= c0) & ((cr < k_cap) if k_cap else True)
         zf, sf, gf = z[f], d["spec"][f], good[f]
         rank = _rank_in_spectrum(zf, d["cnt"][f], sf, d["n"])
         ok = gf & (rank < pr.max_keep)
         best = torch.full((d["n"],), -math.inf, device=dev).scatter_reduce(0, sf[ok], zf[ok], reduce="amax")
         brank = torch.full((d["n"],), 1 << 30, dtype=torch.int64, device=dev).scatter_reduce(
             0, sf[ok], rank[ok], reduce="amin")
-        alive = has & (bc >= c0)
+        alive = has & (bc >= c0) & ((b < k_cap) if k_cap else True)
         need.append(best[alive & (brank >= pr.min_keep)])
     v = torch.sort(torch.cat(need)).values
-    rest = allowed - lost_c0
+    rest = allowed - lost_k
     pr.min_count = c0
+    pr.shortlist_k = k_cap
     pr.tau = float(v[rest]) if rest < len(v) else math.inf
     return pr.tau
 
