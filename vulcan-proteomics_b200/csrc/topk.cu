@@ -70,8 +70,37 @@ __device__ __forceinline__ int radix_digit(const uint32_t* hist, long long& need
 }
 
 // The k-th largest of n unique keys in shared memory (1 <= k <= n): an 8-bit radix select, most significant
-// digit first, counting only the keys that match the digits chosen so far.
+// digit first, counting only the keys that match the digits chosen so far.  Up to KTH_SMALL keys (a short
+// shortlist over few hits) are ranked by counting instead: each lane counts, for its keys, how many keys are
+// larger (broadcast reads), and the key with k - 1 larger ones is the answer -- n reads per key against the radix
+// select's eight histogram passes.
+constexpr int KTH_SMALL = 64;
+
+__device__ __forceinline__ uint64_t smem_kth_largest_radix(const uint64_t* key, int n, int k, uint32_t* hist,
+                                                           int lane);
+
 __device__ __forceinline__ uint64_t smem_kth_largest(const uint64_t* key, int n, int k, uint32_t* hist, int lane) {
+  if (n <= KTH_SMALL) {
+    uint64_t found = 0ull;
+    bool have = false;
+    for (int i = lane; i < n; i += 32) {
+      const uint64_t v = key[i];
+      int larger = 0;
+      for (int j = 0; j < n; ++j) larger += key[j] > v;
+      if (larger == k - 1) {
+        found = v;
+        have = true;
+      }
+    }
+    const unsigned b = __ballot_sync(VK_FULL, have);
+    if (b) return __shfl_sync(VK_FULL, found, __ffs(b) - 1);
+    // unreachable for unique keys; the radix select below is the fallback
+  }
+  return smem_kth_largest_radix(key, n, k, hist, lane);
+}
+
+__device__ __forceinline__ uint64_t smem_kth_largest_radix(const uint64_t* key, int n, int k, uint32_t* hist,
+                                                           int lane) {
   uint64_t prefix = 0, pmask = 0;
   long long need = k;
   for (int shift = 56; shift >= 0; shift -= 8) {
