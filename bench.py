@@ -883,7 +883,11 @@ def run_profile(a):
     pr = None
     if a.path == "pruned":   # kernel shapes only: a saved pruner, or an untrained one with a typical count floor
         from vulcan.gpu import prune as PR
-        pr = PR.Pruner.load(a.pruner, dev) if a.pruner != "train" else PR.Pruner(dev, tau=0.0, min_count=2)
+        if a.pruner != "train":
+            pr = PR.Pruner.load(a.pruner, dev)
+        else:   # the count floor and shortlist cap the calibration picks on the human run
+            pr = PR.Pruner(dev, tau=0.0, min_count=2)
+            pr.shortlist_k = 8
     for _ in range(2):
         if pr is not None:
             PR._pruned_device(run, gi, p, pr, 1, st)
