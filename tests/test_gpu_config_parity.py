@@ -184,3 +184,25 @@ def test_human_hit_lists_give_the_dense_shortlist(human, min_count):
     if min_count == 1:   # spectra whose hits outnumber the top-k: the selection ran (over global memory for most)
         per_spec = fh["hits"]["cand_off"][1:n + 1] - fh["hits"]["cand_off"][:n]
         assert int((per_spec == p.topk).sum()) > 1000
+
+
+@pytest.mark.parametrize("topk", (8, 32))
+def test_human_short_hit_lists_give_the_dense_shortlist(human, topk):
+    """Short lists (top 8 and 32, no closure: ``vk_select_hits`` keeps them in registers as the hits stream by) give
+    the dense form's shortlist of the same size on the whole human run."""
+    import dataclasses
+    from vulcan.gpu import engine as E
+    from vulcan.gpu import prune as PR
+    w, l1, sp, p, gi, P = human
+    q = dataclasses.replace(p, topk=topk)
+    st = E.Stats()
+    fh = PR._front(E.DeviceRun(sp, gi.dev, st), gi, q, st, False, min_count=2)
+    fd = PR._front(E.DeviceRun(sp, gi.dev, st), gi, q, st, False, min_count=2, dense=True)
+    n = len(sp)
+    nc = int(fd["hits"]["cand_off"][n])
+    assert int(fh["hits"]["cand_off"][n]) == nc and nc > 100_000
+    for k in ("c_hyp", "c_row", "c_cnt"):
+        assert torch_equal(fh["hits"][k][:nc], fd["hits"][k][:nc]), k
+    dh, hits = fd["dh"], fd["hits"]
+    h = hits["c_hyp"][:nc]
+    assert torch_equal(fh["hits"]["c_isum"][:nc], fd["isum"][fd["win_off"][h] + hits["c_row"][:nc] - dh["lo"][h]])

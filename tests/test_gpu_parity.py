@@ -834,3 +834,27 @@ def test_phospho_index_search_equals_oracle(tmp_path, torch_cuda):
     rk = O.psm_rank(k2, r, p.min_matched_peaks, 2)
     assert np.array_equal(tbl.column("pf_row").to_numpy(), r[rk["cand"]])
     assert tbl.num_rows > 0 and sum(synth.phospho_rows(l1)[tbl.column("pf_row").to_numpy()]) > 0
+
+
+@pytest.mark.parametrize("topk", (3, 8, 32))
+def test_short_hit_lists_with_overlapping_windows(mini, param_sets, torch_cuda, topk):
+    """Precursor windows of +-1500 ppm make a spectrum's isotope hypotheses overlap, so rows are reached by several
+    hypotheses: the short-list selection over hit lists merges them as the dense top-K does (lowest hypothesis, its
+    intensity sum, highest count)."""
+    import dataclasses
+    from vulcan.gpu import engine as E
+    from vulcan.gpu import prune as PR
+    l1, sp, _ = mini
+    for name in ("da", "ppm"):
+        q = dataclasses.replace(param_sets[name], precursor_ppm=(-1500.0, 1500.0), topk=topk,
+                                search_method="staged")
+        gi = E.GpuIndex(l1, q, STATIC, VAR)
+        st = E.Stats()
+        fh = PR._front(E.DeviceRun(sp, gi.dev, st), gi, q, st, False, min_count=1)
+        fd = PR._front(E.DeviceRun(sp, gi.dev, st), gi, q, st, False, min_count=1, dense=True)
+        dh = fd["dh"]
+        lo, hi, so = dh["lo"].cpu().numpy(), dh["hi"].cpu().numpy(), dh["spec_off"].cpu().numpy()
+        overlap = any(max(lo[a], lo[b]) < min(hi[a], hi[b]) for s in range(len(sp))
+                      for a in range(so[s], so[s + 1]) for b in range(a + 1, so[s + 1]))
+        assert overlap, name
+        _assert_same_shortlist(fh, fd, sp, (name, topk))

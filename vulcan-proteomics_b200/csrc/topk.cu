@@ -603,6 +603,111 @@ select_hits_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo, cons
   if (lane == 0) n_cand[s] = n_out;
 }
 
+// select_hits_k for a short list without pair closure (topk <= 32), one warp per spectrum, with no per-warp key
+// buffer: the running top topk (by the same 63-bit keys) is held in the registers of lanes 0 .. topk-1 and merged
+// with every batch of 32 hits as they are read -- each key's rank among the batch and the running list is counted
+// with shuffles, and lane r takes the key of rank r.  The kept hits are then ordered by (row, hypothesis) and rows
+// reached by several hypotheses merged (lowest hypothesis and its intensity sum, highest count): the outputs of
+// select_hits_k, bit for bit, from shared memory for the hit reader alone (more warps per SM).
+__global__ void __launch_bounds__(TK_WARPS * 32)
+select_hits_small_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo, const int64_t* h_hi,
+                    const int64_t* win_off, const int8_t* hyp_shift, const uint32_t* seg_cnt, const uint64_t* rc,
+                    const uint32_t* hit_isum, const uint32_t* hyp_scored, const uint64_t* hyp_matched, int topk,
+                    int cap, int64_t* c_hyp, int64_t* c_row, int64_t* c_cnt, uint32_t* c_isum, int64_t* n_cand,
+                    int64_t* spec_scored, int64_t* spec_matched) {
+  __shared__ HitScratch scratch[TK_WARPS];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int s = blockIdx.x * TK_WARPS + warp;
+  if (s >= n_spec) return;
+  HitScratch& S = scratch[warp];
+  const int64_t hb = spec_hyp_off[s], he = spec_hyp_off[s + 1];
+  const int nhs = (int)(he - hb);
+  long long sc = 0, mt = 0;
+  for (int64_t h = hb + lane; h < he; h += 32) {
+    sc += hyp_scored[h];
+    mt += (long long)hyp_matched[h];
+  }
+  sc = vk::warp_sum(sc);
+  mt = vk::warp_sum(mt);
+  if (lane == 0 && spec_scored) {
+    spec_scored[s] = sc;
+    spec_matched[s] = mt;
+  }
+  // running list: lane r < topk holds the key of rank r (0 = empty: a hit's key has its count >= 1 in the top bits)
+  uint64_t tk = 0ull;
+  int64_t tp = 0;
+  for (int g0 = 0; g0 < nhs; g0 += 32) {
+    __syncwarp();
+    if (lane < min(32, nhs - g0)) S.hyp[lane] = g0 + lane;
+    __syncwarp();
+    gather_hits(S, min(32, nhs - g0), hb, h_lo, h_hi, win_off, hyp_shift, seg_cnt, rc, lane,
+                [&](bool ok, int64_t pos, uint64_t v, int hl_) {
+      const uint64_t nk = ok ? sel_key(hit_count(v), hit_row(v), hl_) : 0ull;
+      int rn = 0, rt = 0;   // ranks of this lane's new key and of its running key among all 32 + topk keys
+#pragma unroll 4
+      for (int j = 0; j < 32; ++j) {
+        const uint64_t x = __shfl_sync(VK_FULL, nk, j);
+        rn += x > nk;
+        rt += x > tk;
+      }
+      for (int j = 0; j < topk; ++j) {
+        const uint64_t x = __shfl_sync(VK_FULL, tk, j);
+        rn += x > nk;
+        rt += x > tk;
+      }
+      uint64_t nt = 0ull;
+      int64_t np = 0;
+      for (int r = 0; r < topk; ++r) {   // lane r takes the key of rank r, from the batch or the running list
+        const unsigned bn = __ballot_sync(VK_FULL, nk != 0ull && rn == r);
+        const unsigned bt = __ballot_sync(VK_FULL, lane < topk && tk != 0ull && rt == r);
+        const int src = bn ? __ffs(bn) - 1 : (bt ? __ffs(bt) - 1 : 0);
+        const uint64_t kx = __shfl_sync(VK_FULL, bn ? nk : tk, src);
+        const int64_t px = __shfl_sync(VK_FULL, bn ? pos : tp, src);
+        if (lane == r && (bn | bt)) {
+          nt = kx;
+          np = px;
+        }
+      }
+      tk = nt;
+      tp = np;
+    });
+  }
+  // the kept hits ordered by (row, hypothesis); a row reached by several hypotheses keeps its lowest one
+  const bool have = tk != 0ull;
+  const int hl = have ? (1 << 18) - 1 - (int)(tk & 0x3ffff) : 0;
+  const uint64_t v = have ? rc[tp] : 0ull;
+  const int64_t row = hit_row(v);
+  const int cnt = hit_count(v);
+  int best = cnt;
+  bool head = have;
+  for (int j = 0; j < topk; ++j) {   // the whole warp shuffles: same row -> highest count, lowest hypothesis
+    const bool hj = __shfl_sync(VK_FULL, have, j);
+    const int64_t rj = __shfl_sync(VK_FULL, row, j);
+    const int lj = __shfl_sync(VK_FULL, hl, j);
+    const int cj = __shfl_sync(VK_FULL, cnt, j);
+    if (have && hj && rj == row) {
+      best = max(best, cj);
+      if (lj < hl) head = false;
+    }
+  }
+  int before = 0;   // the output position: the kept rows below this one, each counted once (at its head)
+  for (int j = 0; j < topk; ++j) {
+    const bool hj = __shfl_sync(VK_FULL, head, j);
+    const int64_t rj = __shfl_sync(VK_FULL, row, j);
+    if (head && hj && rj < row) ++before;
+  }
+  const int64_t slot = (int64_t)s * cap;
+  if (head) {
+    const int64_t at = slot + before;
+    c_hyp[at] = hb + hl;
+    c_row[at] = row;
+    c_cnt[at] = best;
+    if (c_isum) c_isum[at] = hit_isum[tp];
+  }
+  const unsigned heads = __ballot_sync(VK_FULL, head);
+  if (lane == 0) n_cand[s] = __popc(heads);
+}
+
 // One warp per spectrum: its n_cand[s] (<= cap) slots to [cand_off[s], ...).  A thread per slot of n_spec x cap
 // would launch mostly idle threads (cap is a bound; a few slots per spectrum are filled after the pruner).
 constexpr int CP_WARPS = 8;
@@ -685,6 +790,13 @@ int vk_select_hits(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo,
   if (n_spec == 0) return 0;
   if (topk < 1 || topk > 8192 || cap < (pair_closure ? 2 : 1) * topk) return VK_E_ARG;
   if (!c_isum != !hit_isum || (pair_closure && !partner) || !h_lo || !h_hi || !hyp_shift || !seg_cnt) return VK_E_ARG;
+  if (!pair_closure && topk <= 32) {   // a short list: kept in registers while the hits stream by
+    select_hits_small_k<<<(unsigned)((n_spec + TK_WARPS - 1) / TK_WARPS), TK_WARPS * 32, 0,
+                          (cudaStream_t)stream>>>(n_spec, spec_hyp_off, h_lo, h_hi, win_off, hyp_shift, seg_cnt,
+                                                  hit_rc, hit_isum, hyp_scored, hyp_matched, topk, cap, c_hyp, c_row,
+                                                  c_cnt, c_isum, n_cand, spec_scored, spec_matched);
+    return vk_launch_status();
+  }
   int list_pow2 = 32;
   while (list_pow2 < (pair_closure ? 2 : 1) * topk) list_pow2 <<= 1;
   const int key_cap = list_pow2 > 512 ? list_pow2 : 512;
