@@ -589,6 +589,18 @@ def _kernel_table(a, p, gi, run, flush, pr, dev):
     n_pk = int(peaks["off"][-1])
     ms_keys = timed(lambda: E.peak_keys(gi, peaks, p))
     kern["peak_keys_k"] = (ms_keys, n_pk * (4 + 12 * n_kz))
+    # the small stages before K1, each captured as a CUDA graph of its launches and replayed (as in the pass): K0
+    # (count, scan of the kept counts, the copy or selection of every spectrum's peaks), the hypotheses (count,
+    # scan, fill, row windows), K1's planning (items per tile, scans, fill); bytes: raw peaks read twice and the
+    # view written / spectra and hypotheses / items
+    n_raw = int(run.offsets[-1])
+    ms_k0 = timed(E.GraphedPass(lambda: E._k0_device(run, p, dev), dev).replay)
+    kern["k0 stage (graph of its launches)"] = (ms_k0, n_raw * 16 + n_pk * 8 + n * 40)
+    ms_hy = timed(E.GraphedPass(lambda: E._hyp_device(run, peaks, gi, p), dev).replay)
+    kern["hypotheses stage (graph of its launches)"] = (ms_hy, n * 16 + nh * 40)
+    ms_pl = timed(E.GraphedPass(lambda: E._k1_plan(gi, dh, p, dh["n_max"]), dev).replay)
+    kern["K1 planning stage (graph of its launches)"] = (ms_pl, nh * 40 + int(item_off[-1]) * 8 +
+                                                         gi.tix.n_tiles * 32)
     hits = so["hits"] if pruned else so
     n_hit = int(hits["cand_off"][-1])
     cap = hits["cap"]
