@@ -339,6 +339,13 @@ def test_batched_pruned_search_equals_per_run(mini, param_sets, indexes, torch_c
     se = E.Searcher(gi, l1, p, pruner=pr, report=1)
     for r, (tbl, _) in zip(runs, se.search_batch(runs, batch_spectra=60)):
         assert tbl.equals(PR.search_pruned(r, gi, l1, p, pr, report=1)[0]), r.run
+    # with a shortlist cap: the MLP sees the top 3 hits by count of every spectrum, in batches too
+    pr.shortlist_k = 3
+    se = E.Searcher(gi, l1, p, pruner=pr, report=1)
+    for r, (tbl, _) in zip(runs, se.search_batch(runs, batch_spectra=60)):
+        assert tbl.equals(PR.search_pruned(r, gi, l1, p, pr, report=1)[0]), r.run
+    st = PR.search_pruned(sp, gi, l1, p, pr, report=1)[1]
+    assert 0 < st.counts["n_hits"] <= 3 * len(sp)
 
 
 # ------------------------------------------------------------------------------------------- trained pruner
