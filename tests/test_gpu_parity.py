@@ -213,7 +213,7 @@ def test_topk_radix_selection_path(mini, param_sets, torch_cuda):
 
 @pytest.mark.parametrize("name", SETS)
 def test_k2_candidate_parallel_equals_warp_per_spectrum(mini, param_sets, indexes, name, torch_cuda):
-    """vk_k2_cands (a thread per candidate, peaks read in global memory) == vk_k2_spectra (a warp per spectrum,
+    """vk_k2_cands (a thread per candidate, its CTA's peak masses staged) == vk_k2_spectra (a warp per spectrum,
     staged peaks, bucket table) bit for bit on the exhaustive path's candidate lists."""
     import dataclasses
     from vulcan.gpu import engine as E
@@ -231,6 +231,95 @@ def test_k2_candidate_parallel_equals_warp_per_spectrum(mini, param_sets, indexe
         a, b = out["k2"][key][:nc], k2[key][:nc]
         assert torch_cuda.equal(a, b) or (a.is_floating_point() and torch_cuda.equal(a.isnan(), b.isnan()) and
                                           torch_cuda.equal(a[~a.isnan()], b[~b.isnan()])), (name, key)
+
+
+@pytest.mark.parametrize("unit", ("da", "ppm"))
+def test_k2_sparse_long_rows_and_high_charges_equal_warp_per_spectrum(unit, torch_cuda):
+    """vk_k2_cands == vk_k2_spectra bit for bit on synthetic rows of 2-60 residues with fragment charges up to 5,
+    N-terminal and per-position variable modifications, peaks planted on the candidates' own b/y ladders, repeated
+    masses and equal intensities, spectra above the 512-peak limit (whose CTAs read their peaks in global memory),
+    empty spectra and spectra without candidates."""
+    from vulcan.gpu import _lib as K
+    from vulcan.gpu import engine as E
+    torch = torch_cuda
+    f32 = np.float32
+    rng = np.random.default_rng(11)
+    aa = np.frombuffer(b"ACDEFGHIKLMNPQRSTVWY", np.uint8)
+    fp = E.frag_params({"C": 57.021464}, {"M": 15.994915, "^": 42.010565}, unit)
+    mono, stat, var = (np.array(list(getattr(fp, k)), f32) for k in ("mono", "stat", "var"))
+    n_rows = 400
+    lens = rng.integers(2, 61, n_rows).astype(np.uint8)
+    seq_off = np.concatenate([[0], np.cumsum(lens.astype(np.int64))])
+    res = rng.choice(aa, int(seq_off[-1])).astype(np.uint8)
+    mask = rng.integers(0, 2 ** 62, n_rows, dtype=np.int64).astype(np.uint64) & np.uint64(0x0000_0F0F_0F0F_0F0F)
+    mask[rng.random(n_rows) < 0.3] |= np.uint64(1 << 63)
+    mass32 = rng.uniform(300.0, 6000.0, n_rows).astype(f32)
+
+    def ladder(r, maxfz):
+        """m/z of the row's b and y ions at fragment charges 1..maxfz-1, in the kernels' f32 arithmetic"""
+        mk = int(mask[r])
+        nt = f32(fp.nterm) if mk >> 63 else f32(0.0)
+        b, y, out = nt, f32(mass32[r] - nt), []
+        for k in range(int(lens[r]) - 1):
+            i = int(res[seq_off[r] + k]) - 65
+            rm = f32(mono[i] + (var[i] if (mk >> k) & 1 else stat[i]))
+            b, y = f32(b + rm), f32(y - rm)
+            out += [f32(v / f32(z)) for v in (b, y) for z in range(1, maxfz)]
+        return np.array(out, f32)
+
+    n_spec = 300
+    offs, masses, ints, cand_off, c_row, c_maxfz = [0], [], [], [0], [], []
+    for s in range(n_spec):
+        nc = int(rng.choice([0, 1, 3, 4, 5, 9, 17]))
+        rows = rng.integers(0, n_rows, nc)
+        mfz = rng.integers(2, 7, nc)
+        npk = int(rng.choice([0, 5, 60, 150, 700]))
+        m = [rng.uniform(100.0, 3000.0, npk).astype(f32)]
+        for r, z in zip(rows[:2], mfz[:2]):
+            if npk:
+                lad = ladder(int(r), int(z))
+                lad = lad[rng.random(len(lad)) < 0.6]
+                tol = 0.015 if unit == "da" else lad * 1.5e-5
+                m.append((lad + rng.uniform(-1, 1, len(lad)) * tol).astype(f32))
+        m = np.concatenate(m)
+        rep = m[0::7][:len(m[1::7])]
+        m[1::7][:len(rep)] = rep                                  # repeated masses
+        m = np.sort(m)
+        it = rng.lognormal(3.0, 1.0, len(m)).astype(f32)
+        eq = it[3::9][:len(it[2::9])]
+        it[2::9][:len(eq)] = eq                                   # equal intensities
+        masses.append(m)
+        ints.append(it)
+        offs.append(offs[-1] + len(m))
+        c_row.append(rows)
+        c_maxfz.append(mfz)
+        cand_off.append(cand_off[-1] + nc)
+    dev = torch.device("cuda:0")
+    t = lambda a, dt: torch.as_tensor(np.ascontiguousarray(a), dtype=dt, device=dev)   # noqa: E731
+    pk_off, pk_mass, pk_int = t(offs, torch.int64), t(np.concatenate(masses), torch.float32), \
+        t(np.concatenate(ints), torch.float32)
+    c_off = t(cand_off, torch.int64)
+    rows = t(np.concatenate(c_row), torch.int32)
+    mfz = t(np.concatenate(c_maxfz), torch.int8)
+    tab = (t(seq_off, torch.int64), t(lens, torch.uint8), t(mask.view(np.int64), torch.int64),
+           t(mass32, torch.float32), t(res, torch.uint8))
+    tol = (-0.02, 0.02) if unit == "da" else (-20.0, 20.0)
+    nc = int(cand_off[-1])
+    L = K.lib()
+    outs = []
+    for fn in ("vk_k2_cands", "vk_k2_spectra"):
+        o = E._k2_outputs(nc, dev)
+        args = [C.byref(fp), n_spec, K.ptr(c_off), K.ptr(rows), K.ptr(mfz), K.ptr(pk_off), K.ptr(pk_mass),
+                K.ptr(pk_int), *[K.ptr(x) for x in tab], tol[0], tol[1]]
+        if fn == "vk_k2_spectra":
+            args.append(None)
+        K.check(getattr(L, fn)(*args, *E._k2_ptrs(o), K.stream()), fn)
+        outs.append(o)
+    torch.cuda.synchronize()
+    assert int((outs[1]["matched_b"] > 5).sum()) > 50 and int((outs[1]["longest_y"] > 3).sum()) > 20
+    for key in outs[0]:
+        a, b = outs[0][key], outs[1][key]
+        assert torch.equal(a.isnan(), b.isnan()) and torch.equal(a[~a.isnan()], b[~b.isnan()]), (unit, key)
 
 
 @pytest.mark.parametrize("name", SETS)

@@ -71,19 +71,24 @@ __global__ void cand_features_k(int64_t n, const int64_t* n_dev, const int64_t* 
 }
 
 // The hit-list shortlist's per-spectrum slots compacted (as vk_compact_hits does) and every hit's features written
-// on the way, one warp per spectrum: the features kernel's second read of the compacted hits is saved.
-constexpr int CF_WARPS = 8;
+// on the way: the features kernel's second read of the compacted hits is saved.  A group of 2^g_log lanes per
+// spectrum (the smallest power of two >= cap, at most 32): with the short lists the pruner sees (cap = the shortlist
+// cap, e.g. 8) a warp per spectrum would leave most lanes idle on this latency-bound gather.
+constexpr int CF_THREADS = 256;
 
-__global__ void __launch_bounds__(CF_WARPS * 32)
-compact_features_k(int n_spec, int cap, const int64_t* n_cand, const int64_t* cand_off, const int64_t* s_hyp,
-                   const int64_t* s_row, const int64_t* s_cnt, const uint32_t* s_isum, const int8_t* h_maxfz,
-                   int64_t* c_hyp, int64_t* c_row, int64_t* c_cnt, int32_t* c_row32, int8_t* c_maxfz,
-                   uint32_t* c_isum, const float* h_M, const int8_t* h_z, const float* mass32, const uint8_t* len,
-                   const uint8_t* missed, const float* mu, const float* sd, __nv_bfloat16* feat) {
-  const int s = blockIdx.x * CF_WARPS + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+__global__ void __launch_bounds__(CF_THREADS)
+compact_features_k(int n_spec, int cap, int g_log, const int64_t* n_cand, const int64_t* cand_off,
+                   const int64_t* s_hyp, const int64_t* s_row, const int64_t* s_cnt, const uint32_t* s_isum,
+                   const int8_t* h_maxfz, int64_t* c_hyp, int64_t* c_row, int64_t* c_cnt, int32_t* c_row32,
+                   int8_t* c_maxfz, uint32_t* c_isum, const float* h_M, const int8_t* h_z, const float* mass32,
+                   const uint8_t* len, const uint8_t* missed, const float* mu, const float* sd,
+                   __nv_bfloat16* feat) {
+  const int64_t t = blockIdx.x * (int64_t)CF_THREADS + threadIdx.x;
+  const int64_t s = t >> g_log;
   if (s >= n_spec) return;
-  const int64_t m = min(n_cand[s], (int64_t)cap), dst0 = cand_off[s], src0 = (int64_t)s * cap;
-  for (int64_t j = lane; j < m; j += 32) {
+  const int g = 1 << g_log;
+  const int64_t m = min(n_cand[s], (int64_t)cap), dst0 = cand_off[s], src0 = s * cap;
+  for (int64_t j = t & (g - 1); j < m; j += g) {
     const int64_t src = src0 + j, dst = dst0 + j;
     const int64_t h = s_hyp[src], r = s_row[src], c = s_cnt[src];
     const uint32_t is = s_isum[src];
@@ -392,9 +397,13 @@ int vk_compact_hits_features(int n_spec, int cap, const int64_t* n_cand, const i
                              const float* sd, void* feat_bf16, void* stream) {
   if (n_spec == 0) return 0;
   if (!s_isum || !c_isum || !mu || !sd || !feat_bf16 || ((uintptr_t)feat_bf16 & 15)) return VK_E_ARG;
-  compact_features_k<<<(unsigned)((n_spec + CF_WARPS - 1) / CF_WARPS), CF_WARPS * 32, 0, (cudaStream_t)stream>>>(
-      n_spec, cap, n_cand, cand_off, s_hyp, s_row, s_cnt, s_isum, h_maxfz, c_hyp, c_row, c_cnt, c_row32, c_maxfz,
-      c_isum, h_M, h_z, mass32, len, missed, mu, sd, reinterpret_cast<__nv_bfloat16*>(feat_bf16));
+  if (cap < 1) return VK_E_ARG;
+  int g_log = 0;
+  while ((1 << g_log) < cap && g_log < 5) ++g_log;
+  const int64_t n_thr = (int64_t)n_spec << g_log;
+  compact_features_k<<<(unsigned)((n_thr + CF_THREADS - 1) / CF_THREADS), CF_THREADS, 0, (cudaStream_t)stream>>>(
+      n_spec, cap, g_log, n_cand, cand_off, s_hyp, s_row, s_cnt, s_isum, h_maxfz, c_hyp, c_row, c_cnt, c_row32,
+      c_maxfz, c_isum, h_M, h_z, mass32, len, missed, mu, sd, reinterpret_cast<__nv_bfloat16*>(feat_bf16));
   return vk_launch_status();
 }
 
