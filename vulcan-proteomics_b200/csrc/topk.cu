@@ -604,11 +604,13 @@ select_hits_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo, cons
 }
 
 // select_hits_k for a short list without pair closure (topk <= 32), one warp per spectrum, with no per-warp key
-// buffer: the running top topk (by the same 63-bit keys) is held in the registers of lanes 0 .. topk-1 and merged
-// with every batch of 32 hits as they are read -- each key's rank among the batch and the running list is counted
-// with shuffles, and lane r takes the key of rank r.  The kept hits are then ordered by (row, hypothesis) and rows
-// reached by several hypotheses merged (lowest hypothesis and its intensity sum, highest count): the outputs of
-// select_hits_k, bit for bit, from shared memory for the hit reader alone (more warps per SM).
+// buffer: the running top (by the same 63-bit keys) is held in registers of the first lanes and merged with every
+// batch of 32 hits as they are read.  topk <= 16: the batch is sorted across the lanes by a bitonic network of
+// shuffles and its best tpow (the power of two >= topk) are merged with the running tpow by one bitonic merge;
+// topk 17-32: each key's rank among the batch and the running list is counted with shuffles and lane r takes the
+// key of rank r.  The kept hits are then ordered by (row, hypothesis) and rows reached by several hypotheses merged
+// (lowest hypothesis and its intensity sum, highest count): the outputs of select_hits_k, bit for bit, from shared
+// memory for the hit reader alone (more warps per SM).
 __global__ void __launch_bounds__(TK_WARPS * 32)
 select_hits_small_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo, const int64_t* h_hi,
                     const int64_t* win_off, const int8_t* hyp_shift, const uint32_t* seg_cnt, const uint64_t* rc,
@@ -633,9 +635,12 @@ select_hits_small_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo
     spec_scored[s] = sc;
     spec_matched[s] = mt;
   }
-  // running list: lane r < topk holds the key of rank r (0 = empty: a hit's key has its count >= 1 in the top bits)
+  // running list: lane r < topk holds the key of rank r (0 = empty: a hit's key has its count >= 1 in the top bits);
+  // for topk <= 16 the running list is the best tpow (the power of two >= topk), descending, in lanes 0 .. tpow-1
   uint64_t tk = 0ull;
   int64_t tp = 0;
+  int tpow = 1;
+  while (tpow < topk) tpow <<= 1;
   for (int g0 = 0; g0 < nhs; g0 += 32) {
     __syncwarp();
     if (lane < min(32, nhs - g0)) S.hyp[lane] = g0 + lane;
@@ -643,6 +648,42 @@ select_hits_small_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo
     gather_hits(S, min(32, nhs - g0), hb, h_lo, h_hi, win_off, hyp_shift, seg_cnt, rc, lane,
                 [&](bool ok, int64_t pos, uint64_t v, int hl_) {
       const uint64_t nk = ok ? sel_key(hit_count(v), hit_row(v), hl_) : 0ull;
+      if (tpow <= 16) {
+        // sort the batch descending across the lanes (bitonic, in registers; o = the lane the key came from), then
+        // merge its first tpow with the running list (lanes 0 .. tpow-1, descending) brought in reversed behind
+        // them: the first tpow lanes of the merged 2 x tpow hold the running list again
+        uint64_t k = nk;
+        uint32_t o = (uint32_t)lane;
+        for (int size = 2; size <= 32; size <<= 1)
+          for (int st = size >> 1; st > 0; st >>= 1) {
+            const uint64_t ok2 = __shfl_xor_sync(VK_FULL, k, st);
+            const uint32_t oo = __shfl_xor_sync(VK_FULL, o, st);
+            const bool want_max = ((lane & size) == 0) == ((lane & st) == 0);
+            if (want_max ? ok2 > k : ok2 < k) {
+              k = ok2;
+              o = oo;
+            }
+          }
+        const int rl = 2 * tpow - 1 - lane;   // running key that lands in this lane, reversed
+        const uint64_t rk = __shfl_sync(VK_FULL, tk, rl & 31);
+        if (lane >= tpow) {
+          k = lane < 2 * tpow ? rk : 0ull;
+          o = 32u + (uint32_t)(rl & 31);
+        }
+        for (int st = tpow; st > 0; st >>= 1) {
+          const uint64_t ok2 = __shfl_xor_sync(VK_FULL, k, st);
+          const uint32_t oo = __shfl_xor_sync(VK_FULL, o, st);
+          if (((lane & st) == 0) ? ok2 > k : ok2 < k) {
+            k = ok2;
+            o = oo;
+          }
+        }
+        const int64_t pb = __shfl_sync(VK_FULL, pos, (int)(o & 31u));
+        const int64_t pr = __shfl_sync(VK_FULL, tp, (int)(o & 31u));
+        tk = lane < tpow ? k : 0ull;
+        tp = lane < tpow ? (o < 32u ? pb : pr) : 0;
+        return;
+      }
       int rn = 0, rt = 0;   // ranks of this lane's new key and of its running key among all 32 + topk keys
 #pragma unroll 4
       for (int j = 0; j < 32; ++j) {
@@ -673,6 +714,7 @@ select_hits_small_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo
     });
   }
   // the kept hits ordered by (row, hypothesis); a row reached by several hypotheses keeps its lowest one
+  if (lane >= topk) tk = 0ull;   // (tpow > topk: the list's tail beyond the first topk)
   const bool have = tk != 0ull;
   const int hl = have ? (1 << 18) - 1 - (int)(tk & 0x3ffff) : 0;
   const uint64_t v = have ? rc[tp] : 0ull;
