@@ -179,6 +179,17 @@ int vk_k0_fill(int n_spec, const int64_t* raw_off, const float* raw_mz, const fl
                float fmax, int max_peaks, int min_peaks, const int64_t* pk_off, float* pk_mass, float* pk_int,
                float* tic, uint8_t* valid, int max_raw, const uint8_t* easy, const int32_t* hard_list,
                const int32_t* n_hard, void* stream);
+/* vk_k0_fill in two halves with its arguments: vk_k0_fill_easy writes the code 1 and 2 spectra, vk_k0_fill_hard the
+ * code 0 and 3 spectra.  They write disjoint outputs, so a caller may run them on two streams (both after
+ * vk_k0_count and the scan); vk_k0_fill runs one after the other. */
+int vk_k0_fill_easy(int n_spec, const int64_t* raw_off, const float* raw_mz, const float* raw_int, float fmin,
+                    float fmax, int max_peaks, int min_peaks, const int64_t* pk_off, float* pk_mass, float* pk_int,
+                    float* tic, uint8_t* valid, int max_raw, const uint8_t* easy, const int32_t* hard_list,
+                    const int32_t* n_hard, void* stream);
+int vk_k0_fill_hard(int n_spec, const int64_t* raw_off, const float* raw_mz, const float* raw_int, float fmin,
+                    float fmax, int max_peaks, int min_peaks, const int64_t* pk_off, float* pk_mass, float* pk_int,
+                    float* tic, uint8_t* valid, int max_raw, const uint8_t* easy, const int32_t* hard_list,
+                    const int32_t* n_hard, void* stream);
 
 /* K0 peak view in the window peak mode (reference vulcan/gpu/engine.py:182-183, peak_mode "window"), the same two
  * calls and buffers: the top window_k peaks (intensity desc, mass desc) of every window w = floor(mz * (1.0f /

@@ -457,6 +457,35 @@ int vk_k0_count(int n_spec, const int64_t* raw_off, const float* raw_mz, const f
   return vk_launch_status();
 }
 
+static int k0_fill_easy(int n_spec, const int64_t* raw_off, const float* raw_mz, const float* raw_int, float fmin,
+                        float fmax, int min_peaks, const int64_t* pk_off, float* pk_mass, float* pk_int, float* tic,
+                        uint8_t* valid, const uint8_t* easy, cudaStream_t st) {
+  int64_t threads = (int64_t)n_spec * 32;
+  k0_easy_k<<<(unsigned)((threads + KE_WARPS * 32 - 1) / (KE_WARPS * 32)), KE_WARPS * 32, 0, st>>>(
+      n_spec, raw_off, raw_mz, raw_int, fmin, fmax, min_peaks, pk_off, pk_mass, pk_int, tic, valid, easy);
+  return vk_launch_status();
+}
+
+// hard spectra (unsorted or NaN: sorted; in order with more than max_peaks in range and more than K0_WARP_SELECT raw
+// peaks: selected): one CTA each, keys in shared memory
+static int k0_fill_hard(int n_spec, const int64_t* raw_off, const float* raw_mz, const float* raw_int, float fmin,
+                        float fmax, int max_peaks, int min_peaks, const int64_t* pk_off, float* pk_mass,
+                        float* pk_int, float* tic, uint8_t* valid, int max_raw, const uint8_t* easy,
+                        const int32_t* hard_list, const int32_t* n_hard, cudaStream_t st) {
+  int dev = 0, n_sm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+  int n_pow2 = 32;
+  while (n_pow2 < max_raw) n_pow2 <<= 1;
+  size_t sh = (size_t)n_pow2 * sizeof(uint64_t);
+  cudaError_t e = cudaFuncSetAttribute(k0_fill_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  if (e != cudaSuccess) return vk_err(e);
+  const int grid = (int)min((int64_t)n_sm * 8, (int64_t)n_spec);
+  k0_fill_k<<<grid, K0_THREADS, sh, st>>>(hard_list, n_hard, raw_off, raw_mz, raw_int, fmin, fmax, max_peaks,
+                                          min_peaks, pk_off, pk_mass, pk_int, tic, valid, easy);
+  return vk_launch_status();
+}
+
 int vk_k0_fill(int n_spec, const int64_t* raw_off, const float* raw_mz, const float* raw_int, float fmin,
                float fmax, int max_peaks, int min_peaks, const int64_t* pk_off, float* pk_mass, float* pk_int,
                float* tic, uint8_t* valid, int max_raw, const uint8_t* easy, const int32_t* hard_list,
@@ -464,25 +493,34 @@ int vk_k0_fill(int n_spec, const int64_t* raw_off, const float* raw_mz, const fl
   if (n_spec == 0) return 0;
   if (max_raw < 0 || max_raw > 16384) return VK_E_ARG;
   cudaStream_t st = (cudaStream_t)stream;
-  int64_t threads = (int64_t)n_spec * 32;
-  k0_easy_k<<<(unsigned)((threads + KE_WARPS * 32 - 1) / (KE_WARPS * 32)), KE_WARPS * 32, 0, st>>>(
-      n_spec, raw_off, raw_mz, raw_int, fmin, fmax, min_peaks, pk_off, pk_mass, pk_int, tic, valid, easy);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return vk_err(e);
-  int dev = 0, n_sm = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-  // hard spectra (unsorted or NaN: sorted; in order with more than max_peaks in range and more than
-  // K0_WARP_SELECT raw peaks: selected): one CTA each, keys in shared memory
-  int n_pow2 = 32;
-  while (n_pow2 < max_raw) n_pow2 <<= 1;
-  size_t sh = (size_t)n_pow2 * sizeof(uint64_t);
-  e = cudaFuncSetAttribute(k0_fill_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
-  if (e != cudaSuccess) return vk_err(e);
-  const int grid = (int)min((int64_t)n_sm * 8, (int64_t)n_spec);
-  k0_fill_k<<<grid, K0_THREADS, sh, st>>>(hard_list, n_hard, raw_off, raw_mz, raw_int, fmin, fmax, max_peaks,
-                                          min_peaks, pk_off, pk_mass, pk_int, tic, valid, easy);
-  return vk_launch_status();
+  const int r = k0_fill_easy(n_spec, raw_off, raw_mz, raw_int, fmin, fmax, min_peaks, pk_off, pk_mass, pk_int, tic,
+                             valid, easy, st);
+  if (r != 0) return r;
+  return k0_fill_hard(n_spec, raw_off, raw_mz, raw_int, fmin, fmax, max_peaks, min_peaks, pk_off, pk_mass, pk_int,
+                      tic, valid, max_raw, easy, hard_list, n_hard, st);
+}
+
+int vk_k0_fill_easy(int n_spec, const int64_t* raw_off, const float* raw_mz, const float* raw_int, float fmin,
+                    float fmax, int max_peaks, int min_peaks, const int64_t* pk_off, float* pk_mass, float* pk_int,
+                    float* tic, uint8_t* valid, int max_raw, const uint8_t* easy, const int32_t* hard_list,
+                    const int32_t* n_hard, void* stream) {
+  (void)max_peaks;
+  (void)hard_list;
+  (void)n_hard;
+  if (n_spec == 0) return 0;
+  if (max_raw < 0 || max_raw > 16384) return VK_E_ARG;
+  return k0_fill_easy(n_spec, raw_off, raw_mz, raw_int, fmin, fmax, min_peaks, pk_off, pk_mass, pk_int, tic, valid,
+                      easy, (cudaStream_t)stream);
+}
+
+int vk_k0_fill_hard(int n_spec, const int64_t* raw_off, const float* raw_mz, const float* raw_int, float fmin,
+                    float fmax, int max_peaks, int min_peaks, const int64_t* pk_off, float* pk_mass, float* pk_int,
+                    float* tic, uint8_t* valid, int max_raw, const uint8_t* easy, const int32_t* hard_list,
+                    const int32_t* n_hard, void* stream) {
+  if (n_spec == 0) return 0;
+  if (max_raw < 0 || max_raw > 16384) return VK_E_ARG;
+  return k0_fill_hard(n_spec, raw_off, raw_mz, raw_int, fmin, fmax, max_peaks, min_peaks, pk_off, pk_mass, pk_int,
+                      tic, valid, max_raw, easy, hard_list, n_hard, (cudaStream_t)stream);
 }
 
 int vk_hyp_count(int n_spec, const uint8_t* valid, const double* precursor_mz, const int8_t* charge, int z_lo,

@@ -135,11 +135,26 @@ mlp_infer_tc_k(int64_t n, const int64_t* n_dev, const __nv_bfloat16* __restrict_
   uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(tc_raw) + 127) & ~uintptr_t(127));
   const int tid = threadIdx.x, warp = tid >> 5;
   if (n_dev) n = min(n, *n_dev);
-  // weights into the canonical layouts (16-byte chunks), biases and w3
-  for (int c = tid; c < TC_H * TC_H / 8; c += TC_THREADS) {
-    const int r = c / (TC_H / 8), k = (c % (TC_H / 8)) * 8;
-    *reinterpret_cast<uint4*>(sm + OFF_W2 + canon_off(r, k, TC_H)) =
-        *reinterpret_cast<const uint4*>(W2 + (size_t)r * TC_H + k);
+  // weights into the canonical layouts (16-byte chunks), biases and w3; W2's 16 chunks per thread are loaded in two
+  // batches of 8 independent loads before they are stored (one chunk at a time, every load waited for its
+  // predecessor's store: ~30 us of prologue per launch)
+  constexpr int W2_PER = TC_H * TC_H / 8 / TC_THREADS;   // 16
+  static_assert(W2_PER % 8 == 0, "W2 chunks per thread");
+#pragma unroll
+  for (int u0 = 0; u0 < W2_PER; u0 += 8) {
+    uint4 v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int c = tid + (u0 + u) * TC_THREADS;
+      const int r = c / (TC_H / 8), k = (c % (TC_H / 8)) * 8;
+      v[u] = __ldg(reinterpret_cast<const uint4*>(W2 + (size_t)r * TC_H + k));
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int c = tid + (u0 + u) * TC_THREADS;
+      const int r = c / (TC_H / 8), k = (c % (TC_H / 8)) * 8;
+      *reinterpret_cast<uint4*>(sm + OFF_W2 + canon_off(r, k, TC_H)) = v[u];
+    }
   }
   for (int c = tid; c < TC_H * TC_IN / 8; c += TC_THREADS) {
     const int r = c / (TC_IN / 8), k = (c % (TC_IN / 8)) * 8;

@@ -86,6 +86,8 @@ _SIGS_B200 = {
     "vk_scan_i64_noalloc": [P, I64, P, P],
     "vk_k0_count": [I32, P, P, P, F32, F32, I32, P, P, P, P, P],
     "vk_k0_fill": [I32, P, P, P, F32, F32, I32, I32, P, P, P, P, P, I32, P, P, P, P],
+    "vk_k0_fill_easy": [I32, P, P, P, F32, F32, I32, I32, P, P, P, P, P, I32, P, P, P, P],
+    "vk_k0_fill_hard": [I32, P, P, P, F32, F32, I32, I32, P, P, P, P, P, I32, P, P, P, P],
     "vk_k0w_count": [I32, P, P, P, F32, F32, F32, I32, P, P, P, P, P],
     "vk_k0w_fill": [I32, P, P, P, F32, F32, F32, I32, I32, P, P, P, P, P, I32, P, P, P, P],
     "vk_hyp_count": [I32, P, P, P, I32, I32, I32, I32, P, P],

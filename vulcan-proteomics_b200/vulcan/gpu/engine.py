@@ -80,6 +80,38 @@ def frag_params(static_mods: dict, var_mods: dict, fragment_unit: str = "ppm") -
     return fp
 
 
+_SIDE: dict = {}
+
+
+def _side_stream(dev) -> torch.cuda.Stream:
+    """A second stream per device for launches that may overlap the pass's own (one per process)."""
+    d = torch.device(dev).index or 0
+    s = _SIDE.get(d)
+    if s is None:
+        s = _SIDE[d] = torch.cuda.Stream(device=torch.device("cuda", d))
+    return s
+
+
+class _Forked:
+    """Work launched on the side stream after everything queued so far on the current stream (``fn`` launches on
+    ``K.stream()`` and allocates nothing); ``get()`` makes the current stream wait for it and returns fn's value.
+    Under CUDA-graph capture the two streams become parallel branches of the graph."""
+
+    def __init__(self, dev, fn):
+        main = torch.cuda.current_stream(dev)
+        self.side = _side_stream(dev)
+        self.side.wait_stream(main)
+        with torch.cuda.stream(self.side):
+            self.value = fn()
+        self.joined = False
+
+    def get(self):
+        if not self.joined:
+            torch.cuda.current_stream(self.side.device).wait_stream(self.side)
+            self.joined = True
+        return self.value
+
+
 def _scan(x: torch.Tensor) -> torch.Tensor:
     """Exclusive scan (n+1 entries) of an int64 device vector, on the device."""
     L = K.lib()
@@ -377,10 +409,14 @@ def _k0_device(run: DeviceRun, p: SearchParams, dev):
                               K.ptr(inten), K.ptr(tic), K.ptr(valid), run.max_raw, K.ptr(easy), K.ptr(hard),
                               K.ptr(n_hard), K.stream()), "k0w_fill")
     else:
-        K.check(L.vk_k0_fill(n, K.ptr(run.offsets), K.ptr(run.mz), K.ptr(run.intensity), p.fragment_min_mz,
-                             p.fragment_max_mz, p.max_peaks, p.min_peaks, K.ptr(off), K.ptr(mass), K.ptr(inten),
-                             K.ptr(tic), K.ptr(valid), run.max_raw, K.ptr(easy), K.ptr(hard), K.ptr(n_hard),
-                             K.stream()), "k0_fill")
+        # the few spectra a CTA selects or sorts (more than max_peaks in range, or out of order) on the side stream,
+        # beside the warp-per-spectrum copy of the others: disjoint outputs
+        args = (n, K.ptr(run.offsets), K.ptr(run.mz), K.ptr(run.intensity), p.fragment_min_mz, p.fragment_max_mz,
+                p.max_peaks, p.min_peaks, K.ptr(off), K.ptr(mass), K.ptr(inten), K.ptr(tic), K.ptr(valid),
+                run.max_raw, K.ptr(easy), K.ptr(hard), K.ptr(n_hard))
+        hard_fill = _Forked(dev, lambda: K.check(L.vk_k0_fill_hard(*args, K.stream()), "k0_fill_hard"))
+        K.check(L.vk_k0_fill_easy(*args, K.stream()), "k0_fill_easy")
+        hard_fill.get()
     return {"off": off, "mass": mass, "int": inten, "tic": tic[:n], "valid_d": valid[:n]}
 
 
@@ -485,18 +521,29 @@ def key_charges(p: SearchParams) -> int:
     return mfc if mfc > 0 else 2
 
 
-def peak_keys(gi: GpuIndex, peaks, p: SearchParams, tix=None):
+def peak_keys(gi: GpuIndex, peaks, p: SearchParams, tix=None, forked: bool = False):
     """Window keys and filter words of every kept peak (vk_k1_peak_keys): (keys, filt, n_kz, kstride), computed once
     per pass for all the (tile, hypothesis) items of K1; the filter words are bitmap positions of the tiling
-    ``tix`` (default: the index's own)."""
+    ``tix`` (default: the index's own).  ``forked``: launched on the side stream (they need only K0's peaks, so they
+    overlap the hypotheses and the K1 planning) and returned as a ``_Forked`` whose ``get()`` joins."""
     n_kz = key_charges(p)
     kstride = int(peaks["mass"].numel())
     keys = torch.empty(max(n_kz * kstride * 2, 2), dtype=torch.int32, device=gi.dev)
     filt = torch.empty(max(n_kz * kstride, 1), dtype=torch.int32, device=gi.dev)
-    K.check(K.lib().vk_k1_peak_keys(C.byref(tix or gi.tix), C.byref(gi.fp), float(p.fragment_ppm[0]),
-                                    float(p.fragment_ppm[1]), K.ptr(peaks["off"][-1:]), K.ptr(peaks["mass"]), n_kz,
-                                    kstride, K.ptr(keys), K.ptr(filt), K.stream()), "k1_peak_keys")
-    return keys, filt, n_kz, kstride
+    last = peaks["off"][-1:]
+
+    def launch():
+        K.check(K.lib().vk_k1_peak_keys(C.byref(tix or gi.tix), C.byref(gi.fp), float(p.fragment_ppm[0]),
+                                        float(p.fragment_ppm[1]), K.ptr(last), K.ptr(peaks["mass"]), n_kz,
+                                        kstride, K.ptr(keys), K.ptr(filt), K.stream()), "k1_peak_keys")
+        return keys, filt, n_kz, kstride
+    return _Forked(gi.dev, launch) if forked else launch()
+
+
+def early_peak_keys(gi: GpuIndex, peaks, p: SearchParams):
+    """The window keys of a pass with one K1 shape, forked right after K0 (None with per-bucket shapes, whose
+    tilings each get their own keys when planned)."""
+    return peak_keys(gi, peaks, p, forked=True) if len(k1_shape_list(gi, p)) == 1 else None
 
 
 def k1_shape_list(gi: GpuIndex, p: SearchParams) -> list:
@@ -510,17 +557,20 @@ def k1_shape_list(gi: GpuIndex, p: SearchParams) -> list:
     return out
 
 
-def _k1_passes(gi: GpuIndex, dh, peaks, p: SearchParams, n_hyp: int, caps: tuple | None = None):
+def _k1_passes(gi: GpuIndex, dh, peaks, p: SearchParams, n_hyp: int, caps: tuple | None = None, keys=None):
     """The K1 launches of a pass: per shape (``k1_shape_list``) its work items -- the hypotheses of the spectra in
     the shape's peak-count bucket, planned on the shape's tiling -- with the window keys of that tiling.  Yields
     (tix, warps, plan, keys, filt, n_kz, kstride); every plan shares one ``win_off`` (the windows of all the
-    hypotheses) and one ``status``."""
+    hypotheses) and one ``status``.  ``keys``: the single shape's keys forked earlier (``early_peak_keys``)."""
     shapes = k1_shape_list(gi, p)
     if len(shapes) == 1:
         tl, warps, _, _ = shapes[0]
         pl = _k1_plan(gi, dh, p, n_hyp, caps, tiling=tl)
-        yield (tl["tix"], warps, pl) + peak_keys(gi, peaks, p, tl["tix"])
+        kt = keys.get() if keys is not None else peak_keys(gi, peaks, p, tl["tix"])
+        yield (tl["tix"], warps, pl) + kt
         return
+    if keys is not None:
+        keys.get()
     lo, hi = dh["lo"][:n_hyp], dh["hi"][:n_hyp]
     win_off = _scan((hi - lo).clamp(min=0))
     status = torch.zeros(1, dtype=torch.int32, device=gi.dev)
@@ -537,7 +587,7 @@ def _k1_passes(gi: GpuIndex, dh, peaks, p: SearchParams, n_hyp: int, caps: tuple
 
 
 def _k1_dense(gi: GpuIndex, dh, peaks, p: SearchParams, n_hyp: int, stats: Stats | None = None,
-              isum: bool = False):
+              isum: bool = False, keys=None):
     """Tiled K1: dense counts of every window row.  Returns (win_off, cnt, status), plus the summed matched
     intensity of every window row (u32, 2^24 = the spectrum's TIC) when ``isum``.  The buffers are sized by the
     index's window bound (``GpuIndex.window_bound``), so nothing is read back from the device: cnt / isum hold
@@ -546,7 +596,7 @@ def _k1_dense(gi: GpuIndex, dh, peaks, p: SearchParams, n_hyp: int, stats: Stats
     L = K.lib()
     dev = gi.dev
     cnt = isw = pl = None
-    for tix, warps, pl, keys, filt, n_kz, kstride in _k1_passes(gi, dh, peaks, p, n_hyp):
+    for tix, warps, pl, kk, filt, n_kz, kstride in _k1_passes(gi, dh, peaks, p, n_hyp, keys=keys):
         if cnt is None:
             cnt = torch.empty(pl["cnt_cap"], dtype=torch.int32, device=dev)
             isw = torch.empty(pl["cnt_cap"], dtype=torch.int32, device=dev) if isum else None
@@ -555,7 +605,7 @@ def _k1_dense(gi: GpuIndex, dh, peaks, p: SearchParams, n_hyp: int, stats: Stats
                               K.ptr(dh["spec"]), K.ptr(dh["maxfz"]), K.ptr(dh["lo"]), K.ptr(dh["hi"]),
                               K.ptr(pl["win_off"]), pl["cnt_cap"], K.ptr(peaks["off"]), K.ptr(peaks["mass"]),
                               K.ptr(cnt), K.ptr(pl["status"]), K.ptr(peaks["int"]) if isum else None,
-                              K.ptr(peaks["tic"]) if isum else None, K.ptr(isw) if isum else None, K.ptr(keys),
+                              K.ptr(peaks["tic"]) if isum else None, K.ptr(isw) if isum else None, K.ptr(kk),
                               K.ptr(filt), n_kz, kstride, K.stream()), "k1_tiles")
     if isum:
         return pl["win_off"], cnt, pl["status"], isw
@@ -599,7 +649,7 @@ def _k1_plan(gi: GpuIndex, dh, p: SearchParams, n_hyp: int, caps: tuple | None =
 
 
 def _k1_hits(gi: GpuIndex, dh, peaks, p: SearchParams, n_hyp: int, thr: int, isum: bool = True,
-             h_thr: torch.Tensor | None = None, caps: tuple | None = None):
+             h_thr: torch.Tensor | None = None, caps: tuple | None = None, keys=None):
     """K1 in hit-list form (``vk_k1_hits``): per hypothesis the rows with count >= thr (``h_thr``: a device i32
     threshold per hypothesis instead) -- count << 32 | row, and the summed matched intensity -- in its window's
     region, their number, and the per-hypothesis scored / matched totals.  No dense per-row output.  ``caps``:
@@ -613,7 +663,7 @@ def _k1_hits(gi: GpuIndex, dh, peaks, p: SearchParams, n_hyp: int, thr: int, isu
     hyp_matched = z[nh:2 * nh]
     hyp_shift = z[2 * nh:].view(torch.int8)[:nh]
     rc = hisum = pl = None
-    for tix, warps, pl, keys, filt, n_kz, kstride in _k1_passes(gi, dh, peaks, p, n_hyp, caps):
+    for tix, warps, pl, kk, filt, n_kz, kstride in _k1_passes(gi, dh, peaks, p, n_hyp, caps, keys=keys):
         cap = pl["cnt_cap"]
         if rc is None:
             rc = torch.empty(cap, dtype=torch.int64, device=dev)
@@ -627,7 +677,7 @@ def _k1_hits(gi: GpuIndex, dh, peaks, p: SearchParams, n_hyp: int, thr: int, isu
                              K.ptr(hisum) if isum else None, K.ptr(seg_cnt), K.ptr(hyp_shift), K.ptr(hyp_scored),
                              K.ptr(hyp_matched),
                              K.ptr(pl["status"]), K.ptr(peaks["int"]) if isum else None,
-                             K.ptr(peaks["tic"]) if isum else None, K.ptr(keys), K.ptr(filt), n_kz, kstride,
+                             K.ptr(peaks["tic"]) if isum else None, K.ptr(kk), K.ptr(filt), n_kz, kstride,
                              K.stream()), "k1_hits")
     return {"win_off": pl["win_off"], "status": pl["status"], "rc": rc, "isum": hisum, "seg_cnt": seg_cnt,
             "hyp_shift": hyp_shift,
@@ -963,11 +1013,12 @@ def _search_device(run: DeviceRun, gi: GpuIndex, p: SearchParams, report: int, s
         return Timer(st, name) if timers else _NoTimer()
     with phase("k0"):
         peaks = _k0_device(run, p, dev)
+    keys = early_peak_keys(gi, peaks, p)
     with phase("hyp"):
         dh = _hyp_device(run, peaks, gi, p)
     n_h = dh["n_max"]
     with phase("k1"):
-        win_off, cnt, status = _k1_dense(gi, dh, peaks, p, n_h, st)
+        win_off, cnt, status = _k1_dense(gi, dh, peaks, p, n_h, st, keys=keys)
     with phase("topk"):
         cand, sums = _shortlist(gi, p, n, dh, win_off, cnt, p.topk, bool(p.pair_closure))
     with phase("k2"):

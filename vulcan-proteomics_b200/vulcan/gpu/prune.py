@@ -303,17 +303,18 @@ def _front(run: E.DeviceRun, gi: E.GpuIndex, p: SearchParams, st: E.Stats, timer
         return E.Timer(st, name) if timers else E._NoTimer()
     with phase("k0"):
         peaks = E._k0_device(run, p, dev)
+    keys = E.early_peak_keys(gi, peaks, p)
     with phase("hyp"):
         dh = E._hyp_device(run, peaks, gi, p)
     if dense:
         with phase("k1"):
-            win_off, cnt, status, isum = E._k1_dense(gi, dh, peaks, p, dh["n_max"], st, isum=True)
+            win_off, cnt, status, isum = E._k1_dense(gi, dh, peaks, p, dh["n_max"], st, isum=True, keys=keys)
         with phase("topk"):
             hits, sums = E._shortlist(gi, p, n, dh, win_off, cnt, p.topk, False, thr)
         return {"peaks": peaks, "dh": dh, "win_off": win_off, "cnt": cnt, "status": status, "isum": isum,
                 "hits": hits, **sums}
     with phase("k1"):
-        k1h = E._k1_hits(gi, dh, peaks, p, dh["n_max"], thr, isum=True)
+        k1h = E._k1_hits(gi, dh, peaks, p, dh["n_max"], thr, isum=True, keys=keys)
     k = p.topk if pr is None or pr.shortlist_k <= 0 else min(p.topk, pr.shortlist_k)
     with phase("topk"):
         hits, sums = E._shortlist_hits(gi, p, n, dh, k1h, k, features=(gi, pr.mu, pr.sd) if pr is not None else None)
