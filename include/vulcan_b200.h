@@ -139,9 +139,12 @@ int vk_tindex_bitmap(const vk_tindex* ix, uint32_t* bitmap, void* stream);
 int64_t vk_tindex_bitmap_bytes(const vk_tindex* ix);
 
 /* Exclusive scan of n int64 values: out[0] = 0, out[i+1] = sum(in[0..i]) (out has n+1 entries; in == out+1
- * is allowed).  Uses `tmp` of vk_scan_tmp_bytes(n) bytes. */
+ * is allowed).  Uses `tmp` of vk_scan_tmp_bytes(n) bytes.  vk_scan_kernels(n) = the kernels one scan of n values
+ * launches: 1 up to 4,096 values, 2 up to 8,388,608 (block sums, then each block adds the sums before it), 3
+ * beyond (the block sums scanned by a kernel of their own); n == 0 launches none (a memset). */
 int64_t vk_scan_tmp_bytes(int64_t n);
 int vk_scan_i64(const int64_t* in, int64_t n, int64_t* out, void* tmp, void* stream);
+int vk_scan_kernels(int64_t n);
 
 /* The same exclusive scan without the caller's scratch buffer; it allocates nothing.  No counterpart in the
  * reference.  For callers that cannot allocate device memory on this path: a foreign-language binding (cgo, JNI,

@@ -947,3 +947,26 @@ def test_short_hit_lists_with_overlapping_windows(mini, param_sets, torch_cuda, 
                       for a in range(so[s], so[s + 1]) for b in range(a + 1, so[s + 1]))
         assert overlap, name
         _assert_same_shortlist(fh, fd, sp, (name, topk))
+
+
+def test_scan_equals_cumsum_on_every_launch_shape(torch_cuda):
+    """vk_scan_i64 == torch.cumsum (exclusive) at the sizes where its launch shape changes: one block of 4,096
+    values (one kernel), up to 2,048 blocks (block sums + an apply kernel that adds the sums before its block),
+    beyond (a third kernel scans the block sums); also in place (in == out + 1)."""
+    from vulcan.gpu import _lib as K
+    from vulcan.gpu import engine as E
+    torch = torch_cuda
+    L = K.lib()
+    g = torch.Generator(device="cuda").manual_seed(5)
+    for n in (1, 7, 4096, 4097, 3 * 4096 + 5, 2048 * 4096, 2048 * 4096 + 1, 3_000_001):
+        x = torch.randint(-1000, 1 << 20, (n,), device="cuda", dtype=torch.int64, generator=g)
+        want = torch.zeros(n + 1, dtype=torch.int64, device="cuda")
+        want[1:] = torch.cumsum(x, 0)
+        assert torch.equal(E._scan(x), want), n
+        kern = L.vk_scan_kernels(n)
+        assert kern == (1 if n <= 4096 else (2 if n <= 2048 * 4096 else 3)), (n, kern)
+        buf = torch.empty(n + 1, dtype=torch.int64, device="cuda")
+        buf[1:] = x
+        tmp = torch.empty((L.vk_scan_tmp_bytes(n) + 7) // 8, dtype=torch.int64, device="cuda")
+        K.check(L.vk_scan_i64(K.ptr(buf[1:]), n, K.ptr(buf), K.ptr(tmp), K.stream()), "scan")
+        assert torch.equal(buf, want), ("in place", n)

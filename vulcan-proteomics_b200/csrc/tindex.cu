@@ -203,6 +203,11 @@ __global__ void __launch_bounds__(SCAN_THREADS) scan_blocks_k(int64_t* block_sum
 }
 
 // in may alias out + 1: every element is read before the block's barrier and written after it.
+// FOLD: block_sums holds the blocks' plain sums (scan_reduce_k's output, no scan_blocks_k), and each block adds up
+// those before it itself (at most SCAN_FOLD_MAX_BLOCKS of them); with a single block nothing is read.
+constexpr int64_t SCAN_FOLD_MAX_BLOCKS = 4 * SCAN_THREADS;
+
+template <bool FOLD>
 __global__ void __launch_bounds__(SCAN_THREADS)
 scan_apply_k(const int64_t* in, int64_t n, const int64_t* block_sums, int64_t* out) {
   __shared__ long long tot;
@@ -214,7 +219,16 @@ scan_apply_k(const int64_t* in, int64_t n, const int64_t* block_sums, int64_t* o
     v[i] = j < n ? in[j] : 0;
     s += v[i];
   }
-  long long e = block_excl_scan(s, &tot) + block_sums[blockIdx.x];
+  long long base;
+  if (FOLD) {
+    long long pre = 0;
+    for (int64_t j = threadIdx.x; j < (int64_t)blockIdx.x; j += SCAN_THREADS) pre += block_sums[j];
+    block_excl_scan(pre, &tot);
+    base = tot;   // read before the next scan's barriers (block_excl_scan ends with one)
+  } else {
+    base = block_sums[blockIdx.x];
+  }
+  long long e = block_excl_scan(s, &tot) + base;
   // grid-wide: the last element of the next block is read by that block only, so in/out aliasing is safe when
   // every block reads its own inputs before writing (done above, and out[j+1] belongs to in[j+1]'s block
   // except at the block edge, which is written by this block after its own reads only).
@@ -253,6 +267,27 @@ int scan_scratch_address(int64_t** out) {
   }
   *out = g_scan_scratch_dev[dev];
   return 0;
+}
+
+// Kernels of one scan of n > 0 values: one block -> the apply kernel alone; up to SCAN_FOLD_MAX_BLOCKS blocks ->
+// block sums, then the apply kernel adding up the sums before its block; more -> block sums, their scan, apply.
+int scan_kernels(int64_t n) {
+  if (n <= 0) return 0;
+  const int64_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;
+  return nb == 1 ? 1 : (nb <= SCAN_FOLD_MAX_BLOCKS ? 2 : 3);
+}
+
+int scan_launch(const int64_t* in, int64_t n, int64_t* out, int64_t* bs, cudaStream_t st) {
+  const int64_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;
+  const int k = scan_kernels(n);
+  if (k >= 2) scan_reduce_k<<<(unsigned)nb, SCAN_THREADS, 0, st>>>(in, n, bs);
+  if (k == 3) {
+    scan_blocks_k<<<1, SCAN_THREADS, 0, st>>>(bs, nb);
+    scan_apply_k<false><<<(unsigned)nb, SCAN_THREADS, 0, st>>>(in, n, bs, out);
+  } else {
+    scan_apply_k<true><<<(unsigned)nb, SCAN_THREADS, 0, st>>>(in, n, bs, out);
+  }
+  return vk_launch_status();
 }
 
 }  // namespace
@@ -338,11 +373,7 @@ int vk_scan_i64_noalloc(const int64_t* in, int64_t n, int64_t* out, void* stream
   int rc = scan_scratch_address(&bs);
   if (rc != 0) return rc;
   // every block sum is written by scan_reduce_k before it is read: nothing in the scratch has to start at zero
-  int64_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;
-  scan_reduce_k<<<(unsigned)nb, SCAN_THREADS, 0, st>>>(in, n, bs);
-  scan_blocks_k<<<1, SCAN_THREADS, 0, st>>>(bs, nb);
-  scan_apply_k<<<(unsigned)nb, SCAN_THREADS, 0, st>>>(in, n, bs, out);
-  return vk_launch_status();
+  return scan_launch(in, n, out, bs, st);
 }
 
 int64_t vk_scan_tmp_bytes(int64_t n) { return ((n + SCAN_TILE - 1) / SCAN_TILE + 1) * (int64_t)sizeof(int64_t); }
@@ -351,12 +382,9 @@ int vk_scan_i64(const int64_t* in, int64_t n, int64_t* out, void* tmp, void* str
   cudaStream_t st = (cudaStream_t)stream;
   if (n < 0) return VK_E_ARG;
   if (n == 0) return vk_err(cudaMemsetAsync(out, 0, sizeof(int64_t), st));
-  int64_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;
-  int64_t* bs = (int64_t*)tmp;
-  scan_reduce_k<<<(unsigned)nb, SCAN_THREADS, 0, st>>>(in, n, bs);
-  scan_blocks_k<<<1, SCAN_THREADS, 0, st>>>(bs, nb);
-  scan_apply_k<<<(unsigned)nb, SCAN_THREADS, 0, st>>>(in, n, bs, out);
-  return vk_launch_status();
+  return scan_launch(in, n, out, (int64_t*)tmp, st);
 }
+
+int vk_scan_kernels(int64_t n) { return scan_kernels(n); }
 
 }  // extern "C"

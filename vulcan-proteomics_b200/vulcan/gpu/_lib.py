@@ -141,6 +141,8 @@ def lib():
         f.restype = C.c_int
     L.vk_scan_tmp_bytes.argtypes = [I64]
     L.vk_scan_tmp_bytes.restype = I64
+    L.vk_scan_kernels.argtypes = [I64]
+    L.vk_scan_kernels.restype = C.c_int
     L.vk_scan_noalloc_max_n.argtypes = []
     L.vk_scan_noalloc_max_n.restype = I64
     L.vk_mlp_infer_smem.argtypes = []
@@ -175,8 +177,9 @@ _KERNELS_PER_CALL = {"scan": 3, "set_params": 0, "set_nterm": 0, "set_tol_da": 0
 LAUNCHES = {"n": 0}
 
 
-def check(code: int, what: str):
-    LAUNCHES["n"] += _KERNELS_PER_CALL.get(what, 1) if code == 0 else 0
+def check(code: int, what: str, kernels: int | None = None):
+    """Raise on a nonzero return code; count the call's kernels (``kernels``, else the entry point's usual number)."""
+    LAUNCHES["n"] += (_KERNELS_PER_CALL.get(what, 1) if kernels is None else kernels) if code == 0 else 0
     if code != 0:
         raise RuntimeError(f"{what}: CUDA error {code}" if code > 0 else f"{what}: rejected argument ({code})")
     if _TRACE:   # debugging aid: finish every launch and report the stage before the next one

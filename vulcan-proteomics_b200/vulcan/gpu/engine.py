@@ -118,7 +118,7 @@ def _scan(x: torch.Tensor) -> torch.Tensor:
     n = x.numel()
     out = torch.empty(n + 1, dtype=torch.int64, device=x.device)
     tmp = torch.empty((L.vk_scan_tmp_bytes(n) + 7) // 8, dtype=torch.int64, device=x.device)
-    K.check(L.vk_scan_i64(K.ptr(x), n, K.ptr(out), K.ptr(tmp), K.stream()), "scan")
+    K.check(L.vk_scan_i64(K.ptr(x), n, K.ptr(out), K.ptr(tmp), K.stream()), "scan", L.vk_scan_kernels(n))
     return out
 
 
