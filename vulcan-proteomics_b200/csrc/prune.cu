@@ -344,13 +344,45 @@ select_pruned_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* hit_off,
     n_list = 2 * n_keep;
   }
   __syncwarp();
+  const int64_t slot = (int64_t)s * cap;
+  if (n_list <= 32) {
+    // the usual short list: sorted across the lanes by a bitonic network of shuffles (ascending), each row's run
+    // reduced to its highest count by a log-step segmented max (a row's entries are adjacent once sorted), and the
+    // heads (lowest hypothesis of each row) written in order -- the shared-memory path's outputs
+    uint64_t k = lane < n_list ? lst[lane] : ~0ull;
+    for (int size = 2; size <= 32; size <<= 1)
+      for (int st = size >> 1; st > 0; st >>= 1) {
+        const uint64_t o = __shfl_xor_sync(VK_FULL, k, st);
+        const bool want_min = ((lane & size) == 0) == ((lane & st) == 0);
+        if (want_min ? o < k : o > k) k = o;
+      }
+    const bool valid = lane < n_list;
+    const int64_t r = (int64_t)(k >> 34);
+    const uint64_t kp = __shfl_up_sync(VK_FULL, k, 1);
+    const bool head = valid && (lane == 0 || (int64_t)(kp >> 34) != r);
+    int best = valid ? lcnt[k & 0xffff] : INT_MIN;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int b2 = __shfl_down_sync(VK_FULL, best, o);
+      const uint64_t k2 = __shfl_down_sync(VK_FULL, k, o);
+      if (lane + o < n_list && (int64_t)(k2 >> 34) == r) best = max(best, b2);
+    }
+    const unsigned hb = __ballot_sync(VK_FULL, head);
+    if (head) {
+      const int pos = __popc(hb & lt);
+      c_hyp[slot + pos] = h0 + (int64_t)((k >> 16) & 0x3ffff);
+      c_row[slot + pos] = r;
+      c_cnt[slot + pos] = best;
+    }
+    if (lane == 0) n_cand[s] = __popc(hb);
+    return;
+  }
   int n_pow2 = 1;
   while (n_pow2 < n_list) n_pow2 <<= 1;
   for (int i = n_list + lane; i < n_pow2; i += 32) lst[i] = ~0ull;
   __syncwarp();
   warp_bitonic_u64(lst, n_pow2, lane);
   int n_out = 0;
-  const int64_t slot = (int64_t)s * cap;
   for (int i0 = 0; i0 < n_list; i0 += 32) {
     const int i = i0 + lane;
     bool head = false;
