@@ -750,26 +750,50 @@ select_hits_small_k(int n_spec, const int64_t* spec_hyp_off, const int64_t* h_lo
   if (lane == 0) n_cand[s] = __popc(heads);
 }
 
-// One warp per spectrum: its n_cand[s] (<= cap) slots to [cand_off[s], ...).  A thread per slot of n_spec x cap
-// would launch mostly idle threads (cap is a bound; a few slots per spectrum are filled after the pruner).
+// Each spectrum's n_cand[s] (<= cap) slots to [cand_off[s], ...).  A warp takes CP_GROUPS spectra: when each has
+// at most 32 / CP_GROUPS candidates (the pruned lists) a group of 32 / CP_GROUPS lanes copies each one's, otherwise
+// (the exhaustive top-k lists) the whole warp copies them one spectrum after the other.  A thread per slot of
+// n_spec x cap would launch mostly idle threads (cap is a bound).
 constexpr int CP_WARPS = 8;
+constexpr int CP_GROUPS = 4;
+
+__device__ __forceinline__ void compact_slot(int64_t src, int64_t dst, const int64_t* s_hyp, const int64_t* s_row,
+                                             const int64_t* s_cnt, const int8_t* h_maxfz, int64_t* c_hyp,
+                                             int64_t* c_row, int64_t* c_cnt, int32_t* c_row32, int8_t* c_maxfz,
+                                             const uint32_t* s_isum, uint32_t* c_isum) {
+  const int64_t h = s_hyp[src];
+  c_hyp[dst] = h;
+  c_row[dst] = s_row[src];
+  c_cnt[dst] = s_cnt[src];
+  c_row32[dst] = (int32_t)s_row[src];
+  c_maxfz[dst] = h_maxfz[h];
+  if (c_isum) c_isum[dst] = s_isum[src];
+}
 
 __global__ void __launch_bounds__(CP_WARPS * 32)
 compact_k(int n_spec, int cap, const int64_t* n_cand, const int64_t* cand_off, const int64_t* s_hyp,
           const int64_t* s_row, const int64_t* s_cnt, const int8_t* h_maxfz, int64_t* c_hyp, int64_t* c_row,
           int64_t* c_cnt, int32_t* c_row32, int8_t* c_maxfz, const uint32_t* s_isum, uint32_t* c_isum) {
-  const int s = blockIdx.x * CP_WARPS + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-  if (s >= n_spec) return;
-  const int64_t m = min(n_cand[s], (int64_t)cap), dst0 = cand_off[s], src0 = (int64_t)s * cap;
-  for (int64_t j = lane; j < m; j += 32) {
-    const int64_t src = src0 + j, dst = dst0 + j;
-    const int64_t h = s_hyp[src];
-    c_hyp[dst] = h;
-    c_row[dst] = s_row[src];
-    c_cnt[dst] = s_cnt[src];
-    c_row32[dst] = (int32_t)s_row[src];
-    c_maxfz[dst] = h_maxfz[h];
-    if (c_isum) c_isum[dst] = s_isum[src];
+  constexpr int G = 32 / CP_GROUPS;
+  const int lane = threadIdx.x & 31;
+  const int64_t s0 = ((int64_t)blockIdx.x * CP_WARPS + (threadIdx.x >> 5)) * CP_GROUPS;
+  if (s0 >= n_spec) return;   // uniform over the warp
+  const int64_t s = s0 + lane / G;
+  const int64_t m = s < n_spec ? min(n_cand[s], (int64_t)cap) : 0;
+  if (__all_sync(VK_FULL, m <= G)) {
+    if (lane % G < m) {
+      const int64_t j = lane % G;
+      compact_slot(s * cap + j, cand_off[s] + j, s_hyp, s_row, s_cnt, h_maxfz, c_hyp, c_row, c_cnt, c_row32, c_maxfz,
+                   s_isum, c_isum);
+    }
+    return;
+  }
+  for (int g = 0; g < CP_GROUPS && s0 + g < n_spec; ++g) {
+    const int64_t sg = s0 + g;
+    const int64_t mg = __shfl_sync(VK_FULL, m, g * G), dst0 = cand_off[sg], src0 = sg * cap;
+    for (int64_t j = lane; j < mg; j += 32)
+      compact_slot(src0 + j, dst0 + j, s_hyp, s_row, s_cnt, h_maxfz, c_hyp, c_row, c_cnt, c_row32, c_maxfz, s_isum,
+                   c_isum);
   }
 }
 
@@ -805,9 +829,9 @@ int vk_compact_cands(int n_spec, int cap, const int64_t* n_cand, const int64_t* 
                      const int64_t* s_row, const int64_t* s_cnt, const int8_t* h_maxfz, int64_t* c_hyp,
                      int64_t* c_row, int64_t* c_cnt, int32_t* c_row32, int8_t* c_maxfz, void* stream) {
   if (n_spec == 0) return 0;
-  compact_k<<<(unsigned)((n_spec + CP_WARPS - 1) / CP_WARPS), CP_WARPS * 32, 0, (cudaStream_t)stream>>>(
-      n_spec, cap, n_cand, cand_off, s_hyp, s_row, s_cnt, h_maxfz, c_hyp, c_row, c_cnt, c_row32, c_maxfz, nullptr,
-      nullptr);
+  compact_k<<<(unsigned)((n_spec + CP_WARPS * CP_GROUPS - 1) / (CP_WARPS * CP_GROUPS)), CP_WARPS * 32, 0,
+              (cudaStream_t)stream>>>(n_spec, cap, n_cand, cand_off, s_hyp, s_row, s_cnt, h_maxfz, c_hyp, c_row, c_cnt,
+                                      c_row32, c_maxfz, nullptr, nullptr);
   return vk_launch_status();
 }
 
@@ -817,9 +841,9 @@ int vk_compact_hits(int n_spec, int cap, const int64_t* n_cand, const int64_t* c
                     uint32_t* c_isum, void* stream) {
   if (n_spec == 0) return 0;
   if ((s_isum != nullptr) != (c_isum != nullptr)) return VK_E_ARG;
-  compact_k<<<(unsigned)((n_spec + CP_WARPS - 1) / CP_WARPS), CP_WARPS * 32, 0, (cudaStream_t)stream>>>(
-      n_spec, cap, n_cand, cand_off, s_hyp, s_row, s_cnt, h_maxfz, c_hyp, c_row, c_cnt, c_row32, c_maxfz, s_isum,
-      c_isum);
+  compact_k<<<(unsigned)((n_spec + CP_WARPS * CP_GROUPS - 1) / (CP_WARPS * CP_GROUPS)), CP_WARPS * 32, 0,
+              (cudaStream_t)stream>>>(n_spec, cap, n_cand, cand_off, s_hyp, s_row, s_cnt, h_maxfz, c_hyp, c_row, c_cnt,
+                                      c_row32, c_maxfz, s_isum, c_isum);
   return vk_launch_status();
 }
 
