@@ -718,7 +718,7 @@ def _kernel_table(a, p, gi, run, flush, pr, dev):
 
 
 BATCH_SETUPS = {   # workload -> (index workload, runs, smallest, largest run, spectra per batch, description)
-    "batch64": ("human", 64, 5000, 60000, 131072, "configuration 2: 64 runs, batched, graph-captured"),
+    "batch64": ("human", 64, 5000, 60000, 262144, "configuration 2: 64 runs, batched, graph-captured"),
     "phospho": ("phospho", 32, 20000, 50000, 65536,
                 "configuration 4: phospho S/T/Y <= 3 + Met-ox <= 1 index, 32 runs, batched, graph-captured"),
 }
