@@ -98,6 +98,17 @@ def test_window_peak_mode_arguments_are_checked_before_any_device_call():
                              None, None) == vk_e_arg
 
 
+def test_scan_launch_shape_is_a_host_rule():
+    """vk_scan_kernels (host only, callable without a GPU): 0 kernels for an empty input, 1 up to one block of 4,096
+    values, 2 up to 2,048 blocks (each block adds up the block sums before it), 3 beyond."""
+    from vulcan import _native
+    L = _native._load(_native.GPU_SO, "CUDA kernel library")
+    L.vk_scan_kernels.argtypes = [C.c_int64]
+    L.vk_scan_kernels.restype = C.c_int
+    for n, k in ((0, 0), (1, 1), (4096, 1), (4097, 2), (2048 * 4096, 2), (2048 * 4096 + 1, 3), (1 << 40, 3)):
+        assert L.vk_scan_kernels(n) == k, n
+
+
 def test_header_compiles_as_c_and_links(tmp_path):
     """A C binding (cgo, JNI, N-API) includes the header as C99 and links the library: a program that takes the
     address of every declared entry point compiles, links and loads (it calls none of them)."""
