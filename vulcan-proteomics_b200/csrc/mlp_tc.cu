@@ -136,8 +136,7 @@ mlp_infer_tc_k(int64_t n, const int64_t* n_dev, const __nv_bfloat16* __restrict_
   const int tid = threadIdx.x, warp = tid >> 5;
   if (n_dev) n = min(n, *n_dev);
   // weights into the canonical layouts (16-byte chunks), biases and w3; W2's 16 chunks per thread are loaded in two
-  // batches of 8 independent loads before they are stored (one chunk at a time, every load waited for its
-  // predecessor's store: ~30 us of prologue per launch)
+  // batches of 8 independent loads before they are stored, so that the loads of a batch are in flight together
   constexpr int W2_PER = TC_H * TC_H / 8 / TC_THREADS;   // 16
   static_assert(W2_PER % 8 == 0, "W2 chunks per thread");
 #pragma unroll
