@@ -159,6 +159,13 @@ def cpu_oracle_pass(l1, sp_sub, p, var=None):
 _ARR = {}
 
 
+def _oracle_index(l1, p, var=None):
+    """The oracle's fragment index of l1 (built once per process, before any timed sample)."""
+    from oracle import oracle as O
+    P = O.make_params(STATIC, VAR if var is None else var, p.fragment_unit)
+    O.frag_index(l1, p, P, arrays=_ARR.get(id(l1)))
+
+
 def _subset(sp, n):
     from vulcan.gpu.host import Spectra
     n = min(n, len(sp))
@@ -172,6 +179,7 @@ def cpu_rate(l1, sp, p, budget_s: float, var=None):
     from oracle import oracle as O
     _ARR[id(l1)] = {k: np.ascontiguousarray(getattr(l1, k)) for k in ("seq_off", "length", "mask", "mass32",
                                                                          "residues")}
+    _oracle_index(l1, p, var)   # index-time work, outside the timed samples (as the device index)
     n = 500
     t0 = time.perf_counter()
     cpu_oracle_pass(l1, _subset(sp, n), p, var)
@@ -377,8 +385,8 @@ def run_b200(a):
     if rank == 0 and world == 1:
         rate, n_cpu, t_s, cores, cpu_ref = cpu_rate(l1, sp, p, a.cpu_budget, w.var_mods)
         cpu = {"value": round(rate, 1), "unit": "spectra/s", "cores": cores, "kind": "port",
-               "sample": f"first {n_cpu} spectra of the run through the oracle's plain path K0->hypotheses->K1->"
-                         f"top-k->K2->ranking ({t_s:.1f} s)"}
+               "sample": f"first {n_cpu} spectra of the run through the oracle's plain path K0->hypotheses->K1 (its "
+                         f"fragment index, built before)->top-k->K2->ranking ({t_s:.1f} s)"}
 
     def step_plain():
         if p.search_method == "fused":
@@ -920,6 +928,7 @@ def run_reference(a):
     p = w.search_params()
     _ARR[id(l1)] = {k: np.ascontiguousarray(getattr(l1, k)) for k in ("seq_off", "length", "mask", "mass32",
                                                                          "residues")}
+    _oracle_index(l1, p, w.var_mods)   # index-time work, before any timed sample
     # per-step sample sized so warmup + steps take about a.cpu_total seconds
     t0 = time.perf_counter()
     cpu_oracle_pass(l1, _subset(sp, 300), p, w.var_mods)
@@ -939,7 +948,8 @@ def run_reference(a):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
         "config": _config(w, p, {"spectra_per_step": n_step}),
         "cpu_baseline": {"value": round(value, 1), "unit": "spectra/s", "cores": cores, "kind": "port",
-                         "sample": f"{n_step} spectra per step of the same simulated run"},
+                         "sample": f"{n_step} spectra per step of the same simulated run (K1 over the oracle's "
+                                   f"fragment index, built before the timed steps)"},
         "e2e": {"value": round(value, 1), "unit": "spectra/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)

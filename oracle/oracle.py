@@ -128,6 +128,28 @@ def k0_view(sp, p):
     return {"off": off, "mass": mass, "int": it, "tic": tic.astype(np.float32), "valid": cnt >= p.min_peaks}
 
 
+def k0_view_c(sp, p, nthreads=None):
+    """``k0_view`` for the global peak mode in C, per spectrum on all cores (the same outputs; the tests check
+    them against ``k0_view``).  Other peak modes: ``k0_view`` itself."""
+    if p.peak_mode != "global":
+        return k0_view(sp, p)
+    n = len(sp.offsets) - 1
+    raw_off = _c(sp.offsets, np.int64)
+    mz = _c(sp.mz, np.float32)
+    it = _c(sp.intensity, np.float32)
+    off = np.empty(n + 1, np.int64)
+    mass = np.empty(max(len(mz), 1), np.float32)
+    inten = np.empty(max(len(mz), 1), np.float32)
+    tic = np.empty(max(n, 1), np.float32)
+    valid = np.empty(max(n, 1), np.uint8)
+    lib().or_k0_global(C.c_int64(n), _p(raw_off), _p(mz), _p(it), C.c_float(p.fragment_min_mz),
+                       C.c_float(p.fragment_max_mz), C.c_int(p.max_peaks), C.c_int(p.min_peaks), _p(off), _p(mass),
+                       _p(inten), _p(tic), _p(valid), C.c_int(nthreads or n_threads()))
+    k = int(off[-1])
+    return {"off": off, "mass": mass[:k].copy(), "int": inten[:k].copy(), "tic": tic[:n].copy(),
+            "valid": valid[:n].astype(bool)}
+
+
 # ---------------------------------------------------------------------------------------------------- hypotheses
 def make_hypotheses(sp, valid, idx_mass32, p):
     """host.py:64-91, written with the reference's own concatenate-then-lexsort structure."""
@@ -215,6 +237,69 @@ def k1_windows(l1, hyp, peaks, p, P, nthreads=None, arrays=None, tic=None):
     return win_off, cnt, scored, matched
 
 
+FRAG_BIN_TH = 0.02   # m/z bin width of the oracle's fragment index (Th)
+_FRAG_INDEX = {}
+
+
+def frag_index(l1, p, P, arrays=None, nthreads=None):
+    """The index fragments of every row of ``l1`` (kernels.cu:53-71 arithmetic, ion index > min_ion_index, fmin <= f
+    <= fmax) binned by m/z from fmin in FRAG_BIN_TH bins, rows ascending within a bin: (bin_off, mass, row, n_bins).
+    Built once per index and fragment setting (the reference's K1 searches such an index, kernels.cu:112-190)."""
+    a = arrays or {k: getattr(l1, k) for k in ("seq_off", "length", "mask", "mass32", "residues")}
+    key = (id(l1), len(a["mass32"]), p.min_ion_index, float(p.fragment_min_mz), float(p.fragment_max_mz),
+           bytes(P.mono), bytes(P.stat), bytes(P.var), float(P.nterm))
+    hit = _FRAG_INDEX.get(key)
+    if hit is not None:
+        return hit
+    arr = {k: _c(a[k], dt) for k, dt in (("seq_off", np.int64), ("length", np.uint8), ("mask", np.uint64),
+                                         ("mass32", np.float32), ("residues", np.uint8))}
+    n = len(arr["mass32"])
+    cnt = np.empty(n, np.int32)
+    lib().or_frag_count(C.c_int64(n), _p(arr["seq_off"]), _p(arr["length"]), _p(arr["mask"]), _p(arr["mass32"]),
+                        _p(arr["residues"]), C.c_int(p.min_ion_index), C.c_float(p.fragment_min_mz),
+                        C.c_float(p.fragment_max_mz), _p(cnt), C.byref(P))
+    total = int(cnt.sum(dtype=np.int64))
+    n_bins = max(1, int(np.ceil((float(np.float32(p.fragment_max_mz)) - float(np.float32(p.fragment_min_mz)))
+                               / FRAG_BIN_TH)) + 1)
+    bin_off = np.empty(n_bins + 1, np.int64)
+    mass = np.empty(max(total, 1), np.float32)
+    row = np.empty(max(total, 1), np.int32)
+    lib().or_frag_index_build(C.c_int64(n), _p(arr["seq_off"]), _p(arr["length"]), _p(arr["mask"]),
+                              _p(arr["mass32"]), _p(arr["residues"]), C.c_int(p.min_ion_index),
+                              C.c_float(p.fragment_min_mz), C.c_float(p.fragment_max_mz), C.c_double(FRAG_BIN_TH),
+                              C.c_int64(n_bins), _p(bin_off), _p(mass), _p(row), C.byref(P),
+                              C.c_int(nthreads or n_threads()))
+    _FRAG_INDEX.clear()   # one index at a time (the human index's is about 1.2 GB)
+    _FRAG_INDEX[key] = (bin_off, mass, row, n_bins)
+    return _FRAG_INDEX[key]
+
+
+def k1_index(l1, hyp, peaks, p, P, nthreads=None, arrays=None, tic=None):
+    """``k1_windows``' outputs (the same counts, statistics and intensity sums) from the fragment index
+    (``frag_index``): per peak window the bins it touches, and in each bin the rows of the hypothesis' window."""
+    bin_off, mass, row, n_bins = frag_index(l1, p, P, arrays, nthreads)
+    lo = _c(hyp["lo"], np.int64)
+    hi = _c(hyp["hi"], np.int64)
+    n_h = len(lo)
+    win_off = np.zeros(n_h + 1, np.int64)
+    np.cumsum(hi - lo, out=win_off[1:])
+    cnt = np.empty(int(win_off[-1]), np.int32)
+    scored = np.zeros(n_h, np.uint32)
+    matched = np.zeros(n_h, np.uint64)
+    isum = np.zeros(len(cnt), np.uint32) if tic is not None else None
+    lib().or_k1_index(C.c_int64(n_h), _p(_c(hyp["spec"], np.int32)), _p(_c(hyp["maxfz"], np.int8)), _p(lo), _p(hi),
+                      _p(win_off), _p(_c(peaks["off"], np.int64)), _p(_c(peaks["mass"], np.float32)), _p(bin_off),
+                      _p(mass), _p(row), C.c_float(p.fragment_min_mz), C.c_float(p.fragment_max_mz),
+                      C.c_double(FRAG_BIN_TH), C.c_int64(n_bins), C.c_float(p.fragment_ppm[0]),
+                      C.c_float(p.fragment_ppm[1]), _p(cnt), _p(scored), _p(matched),
+                      _p(_c(peaks["int"], np.float32)) if tic is not None else None,
+                      _p(_c(tic, np.float32)) if tic is not None else None,
+                      _p(isum) if tic is not None else None, C.byref(P), C.c_int(nthreads or n_threads()))
+    if tic is not None:
+        return win_off, cnt, scored, matched, isum
+    return win_off, cnt, scored, matched
+
+
 def k1_appended(hyp, win_off, cnt, thr):
     """(hyp, row, count) of every window row with count >= thr, sorted by (hyp, row) (kernels.cu:170-180)."""
     lo = hyp["lo"]
@@ -253,6 +338,25 @@ def select_topk(o_h, o_r, o_c, hyp_spec, partner, topk, pair_closure=True):
     cc = np.full(len(uk), -1, np.int64)
     np.maximum.at(cc, inv, c)
     return hh, uk & (2 ** ROW_BITS - 1), cc
+
+
+def topk_windows(hyp, win_off, cnt, thr, partner, topk, pair_closure=True, nthreads=None):
+    """``select_topk(*k1_appended(hyp, win_off, cnt, thr), hyp["spec"], partner, topk, pair_closure)`` in C, per
+    spectrum on all cores (the same (hyp, row, count) lists; the tests check them against the numpy chain)."""
+    spec = np.asarray(hyp["spec"], np.int64)
+    n_spec = int(spec.max()) + 1 if len(spec) else 0
+    spec_hyp_off = np.searchsorted(spec, np.arange(n_spec + 1), side="left").astype(np.int64)
+    cap = max(1, (2 if pair_closure else 1) * int(topk))
+    o_h = np.empty(max(n_spec * cap, 1), np.int64)
+    o_r = np.empty_like(o_h)
+    o_c = np.empty_like(o_h)
+    o_n = np.zeros(max(n_spec, 1), np.int32)
+    lib().or_topk_windows(C.c_int64(n_spec), _p(spec_hyp_off), _p(_c(hyp["lo"], np.int64)), _p(_c(hyp["hi"], np.int64)),
+                          _p(_c(win_off, np.int64)), _p(_c(cnt, np.int32)), C.c_int(int(thr)), C.c_int(int(topk)),
+                          C.c_int(int(bool(pair_closure))), _p(_c(partner, np.int64)), C.c_int(cap), _p(o_h), _p(o_r),
+                          _p(o_c), _p(o_n), C.c_int(nthreads or n_threads()))
+    sel = (np.arange(cap)[None, :] < o_n[:n_spec, None]).ravel()
+    return o_h[:n_spec * cap][sel], o_r[:n_spec * cap][sel], o_c[:n_spec * cap][sel]
 
 
 def _ord_f32(x):

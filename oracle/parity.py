@@ -9,7 +9,8 @@ first ``n`` spectra with the oracle's chain on those spectra (reference order: `
 
   k0        peak offsets, masses, intensities and validity bit-identical (engine.py:171-210)
   hyp       hypotheses and row windows bit-identical (host.py:64-91)
-  k1        dense counts of every window row, per-hypothesis scored / matched (kernels.cu:112-190, 195-232)
+  k1        dense counts of every window row, per-hypothesis scored / matched (kernels.cu:112-190, 195-232),
+            from the oracle's fragment index
   topk      candidate (hypothesis, row, count) lists after pair closure (engine.py:284-312)
   k2        f32 sums, ppm and integer outputs bit-identical, f64 hyperscore within 1e-12 of the oracle's
             (device log vs host libm) (kernels.cu:263-376)
@@ -37,12 +38,14 @@ def _np(t):
 
 
 def oracle_plain(l1, sp, p, P, arrays=None, f64=True):
-    """The oracle's plain search chain on run ``sp``: every intermediate the device pass has."""
-    pk = O.k0_view(sp, p)
+    """The oracle's plain search chain on run ``sp``: every intermediate the device pass has.  Its C stages: the K0
+    view (``O.k0_view_c``), K1 over the oracle's fragment index (``O.k1_index``, the reference's K1 search on the
+    host), the top-K with closure (``O.topk_windows``) and K2; the tests check each against the numpy restatements
+    and the window counts of ``O.k1_windows``, which are pinned to the reference's own code."""
+    pk = O.k0_view_c(sp, p)
     hyp = O.make_hypotheses(sp, pk["valid"], l1.mass32, p)
-    win_off, cnt, sc, mt = O.k1_windows(l1, hyp, pk, p, P, arrays=arrays)
-    oh, orr, oc = O.k1_appended(hyp, win_off, cnt, p.k1_threshold)
-    h, r, c = O.select_topk(oh, orr, oc, hyp["spec"], l1.partner, p.topk, p.pair_closure)
+    win_off, cnt, sc, mt = O.k1_index(l1, hyp, pk, p, P, arrays=arrays)
+    h, r, c = O.topk_windows(hyp, win_off, cnt, p.k1_threshold, l1.partner, p.topk, p.pair_closure)
     k2 = O.k2(l1, hyp, pk, h, r, p, P)
     k2f = O.k2_f64(l1, hyp, pk, h, r, p, P) if f64 else None
     rk = O.psm_rank(k2, r, p.min_matched_peaks, 1)

@@ -9,6 +9,9 @@
  *   - index fragment count / emit keys    vulcan/gpu/kernels.cu:53-101
  *   - K1 brute-force counts               vulcan/gpu/kernels.cu:195-232
  *   - K1 per-hypothesis window counts     same semantics, faster search (sorted fragments per row)
+ *   - K1 over a fragment index            vulcan/gpu/kernels.cu:112-190 (m/z-binned fragments, rows within a bin)
+ *   - K0 view, global peak mode           vulcan/gpu/engine.py:171-210 (oracle.k0_view per spectrum)
+ *   - top-K + pair closure over counts    vulcan/gpu/kernels.cu:170-180, engine.py:284-312 (oracle.select_topk)
  *   - K2 exact rescoring (+ shift mode)   vulcan/gpu/kernels.cu:240-376
  *   - K2 with FP64 accumulation           same matches, intensity sums and hyperscore in double (hyperscore oracle)
  *
@@ -231,6 +234,304 @@ void or_k1_windows(int64_t n_hyp, const int32_t* hyp_spec, const int8_t* hyp_max
     free(wa);
     free(wb);
     free(wg);
+  }
+}
+
+/* ------------------------------------------------------------------------------------------ K1 over a fragment index
+ * The reference's K1 (kernels.cu:112-190) searches a fragment index: every row's index fragments (row_fragments)
+ * binned by m/z, each bin's entries in row order, and for a peak window the bins it touches, then the rows of the
+ * hypothesis' window inside each bin.  This is that search on the host: bins of bin_w Th from fmin (bin(f) =
+ * floor((f - fmin) / bin_w), monotone in f), entries (f32 mass, row) stored bin after bin, rows ascending within a
+ * bin.  The counts are those of or_k1_windows (the same (peak, charge, fragment) triples with a <= f <= bd). */
+static inline int64_t frag_bin(double f, double fmin, double inv_w, int64_t n_bins) {
+  int64_t b = (int64_t)floor((f - fmin) * inv_w);
+  return b < 0 ? 0 : (b >= n_bins ? n_bins - 1 : b);
+}
+
+/* bin_off[n_bins + 1] (entries before each bin), ent_mass / ent_row[bin_off[n_bins]] (the caller sizes them by the
+ * sum of or_frag_count's counts).  Parallel over contiguous row blocks, each block's entries placed after the
+ * lower blocks' in every bin, so rows stay ascending within a bin. */
+void or_frag_index_build(int64_t n, const int64_t* seq_off, const uint8_t* len, const uint64_t* mask,
+                         const float* mass32, const uint8_t* res, int min_ion_index, float fmin, float fmax,
+                         double bin_w, int64_t n_bins, int64_t* bin_off, float* ent_mass, int32_t* ent_row,
+                         const or_params* P, int nthreads) {
+  set_threads(nthreads);
+  int nt = 1;
+#ifdef _OPENMP
+  nt = omp_get_max_threads();
+#endif
+  const double inv_w = 1.0 / bin_w;
+  int64_t* hist = (int64_t*)calloc((size_t)nt * (size_t)(n_bins + 1), sizeof(int64_t));
+#pragma omp parallel num_threads(nt)
+  {
+    int t = 0;
+#ifdef _OPENMP
+    t = omp_get_thread_num();
+#endif
+    int64_t r0 = n * t / nt, r1 = n * (t + 1) / nt;
+    int64_t* hc = hist + (size_t)t * (size_t)(n_bins + 1);
+    float fr[512];   /* 2 (L - 1) fragments at most, L < 256 */
+    for (int64_t r = r0; r < r1; ++r) {
+      int nf = row_fragments(P, seq_off, len, mask, mass32, res, r, min_ion_index, fmin, fmax, fr);
+      for (int i = 0; i < nf; ++i) ++hc[frag_bin(fr[i], fmin, inv_w, n_bins)];
+    }
+#pragma omp barrier
+#pragma omp single
+    {
+      int64_t run = 0;
+      for (int64_t b = 0; b < n_bins; ++b) {
+        bin_off[b] = run;
+        for (int u = 0; u < nt; ++u) {   /* hist becomes each block's first slot in the bin */
+          int64_t c = hist[(size_t)u * (size_t)(n_bins + 1) + b];
+          hist[(size_t)u * (size_t)(n_bins + 1) + b] = run;
+          run += c;
+        }
+      }
+      bin_off[n_bins] = run;
+    }
+    for (int64_t r = r0; r < r1; ++r) {
+      int nf = row_fragments(P, seq_off, len, mask, mass32, res, r, min_ion_index, fmin, fmax, fr);
+      for (int i = 0; i < nf; ++i) {
+        int64_t at = hc[frag_bin(fr[i], fmin, inv_w, n_bins)]++;
+        ent_mass[at] = fr[i];
+        ent_row[at] = (int32_t)r;
+      }
+    }
+  }
+  free(hist);
+}
+
+/* First index in the row-sorted v[0,n) with v[i] >= x. */
+static int64_t lower_bound_i32(const int32_t* v, int64_t n, int64_t x) {
+  int64_t lo = 0, hi = n;
+  while (lo < hi) {
+    int64_t m = (lo + hi) >> 1;
+    if ((int64_t)v[m] < x) lo = m + 1; else hi = m;
+  }
+  return lo;
+}
+
+/* or_k1_windows' outputs (dense counts of every window row, scored / matched per hypothesis, optional intensity
+ * sums) from the fragment index of or_frag_index_build. */
+void or_k1_index(int64_t n_hyp, const int32_t* hyp_spec, const int8_t* hyp_maxfz, const int64_t* hyp_lo,
+                 const int64_t* hyp_hi, const int64_t* win_off, const int64_t* pk_off, const float* pk_mass,
+                 const int64_t* bin_off, const float* ent_mass, const int32_t* ent_row, float fmin, float fmax,
+                 double bin_w, int64_t n_bins, float tol_lo, float tol_hi, int32_t* cnt, uint32_t* scored,
+                 uint64_t* matched, const float* pk_int, const float* tic, uint32_t* isum, const or_params* P,
+                 int nthreads) {
+  set_threads(nthreads);
+  const double inv_w = 1.0 / bin_w;
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int64_t h = 0; h < n_hyp; ++h) {
+    const int s = hyp_spec[h], maxfz = hyp_maxfz[h];
+    const int64_t lo = hyp_lo[h], hi = hyp_hi[h], w0 = win_off[h];
+    if (hi <= lo) {
+      scored[h] = 0;
+      matched[h] = 0;
+      continue;
+    }
+    int32_t* c = cnt + w0;
+    uint32_t* is = isum ? isum + w0 : NULL;
+    memset(c, 0, sizeof(int32_t) * (size_t)(hi - lo));
+    if (is) memset(is, 0, sizeof(uint32_t) * (size_t)(hi - lo));
+    const float wscale = (isum && tic[s] > 0.f) ? 16777216.0f / tic[s] : 0.f;
+    for (int64_t p = pk_off[s]; p < pk_off[s + 1]; ++p) {
+      const uint32_t wg = isum ? (uint32_t)lrintf(pk_int[p] * wscale) : 0u;
+      for (int z = 1; z < maxfz; ++z) {
+        const float m = pk_mass[p] * (float)z;
+        const float a = tol_bound(P, m, tol_lo), bd = tol_bound(P, m, tol_hi);
+        if (!(bd >= fmin && a <= fmax)) continue;   /* every index fragment lies in [fmin, fmax] */
+        const int64_t ba = frag_bin(a < fmin ? fmin : a, fmin, inv_w, n_bins);
+        const int64_t bb = frag_bin(bd > fmax ? fmax : bd, fmin, inv_w, n_bins);
+        for (int64_t b = ba; b <= bb; ++b) {
+          const int64_t e0 = bin_off[b], e1 = bin_off[b + 1];
+          for (int64_t e = e0 + lower_bound_i32(ent_row + e0, e1 - e0, lo); e < e1 && ent_row[e] < hi; ++e) {
+            const float f = ent_mass[e];
+            if (f >= a && f <= bd) {
+              ++c[ent_row[e] - lo];
+              if (is) is[ent_row[e] - lo] += wg;
+            }
+          }
+        }
+      }
+    }
+    uint32_t sc = 0;
+    uint64_t mt = 0;
+    for (int64_t r = 0; r < hi - lo; ++r)
+      if (c[r] > 0) {
+        ++sc;
+        mt += (uint64_t)c[r];
+      }
+    scored[h] = sc;
+    matched[h] = mt;
+  }
+}
+
+/* ------------------------------------------------------------------------------------------ K0 view (global mode)
+ * oracle.k0_view (engine.py:171-210) per spectrum: the peaks with fmin <= mz <= fmax (not NaN), mass = mz - PROTON
+ * in f32, the top max_peaks by (intensity desc, mass desc, input order) -- NaN intensities after all others, as a
+ * descending lexsort puts them -- then mass ascending (ties in that ranking order); TIC = the f64 sum of the kept
+ * intensities in output order, as f32; valid = kept >= min_peaks.  out_off[n + 1] gets the offsets; out_mass /
+ * out_int hold at most raw_off[n] peaks. */
+typedef struct { float mass, it; int64_t idx; int32_t rank; } k0_peak;
+
+static int k0_rank_cmp(const void* pa, const void* pb) {
+  const k0_peak* a = (const k0_peak*)pa;
+  const k0_peak* b = (const k0_peak*)pb;
+  const int na = isnan(a->it), nb = isnan(b->it);
+  if (na != nb) return na - nb;                      /* NaN intensities last */
+  if (!na && a->it != b->it) return a->it > b->it ? -1 : 1;
+  if (a->mass != b->mass) return a->mass > b->mass ? -1 : 1;
+  return (a->idx > b->idx) - (a->idx < b->idx);
+}
+
+static int k0_mass_cmp(const void* pa, const void* pb) {
+  const k0_peak* a = (const k0_peak*)pa;
+  const k0_peak* b = (const k0_peak*)pb;
+  if (a->mass != b->mass) return a->mass < b->mass ? -1 : 1;
+  return (a->rank > b->rank) - (a->rank < b->rank);
+}
+
+void or_k0_global(int64_t n, const int64_t* raw_off, const float* raw_mz, const float* raw_int, float fmin,
+                  float fmax, int max_peaks, int min_peaks, int64_t* out_off, float* out_mass, float* out_int,
+                  float* tic, uint8_t* valid, int nthreads) {
+  set_threads(nthreads);
+  int32_t* kept = (int32_t*)malloc(sizeof(int32_t) * (size_t)(n > 0 ? n : 1));
+#pragma omp parallel
+  {
+    k0_peak* buf = NULL;
+    int64_t cap = 0;
+#pragma omp for schedule(dynamic, 64)
+    for (int64_t s = 0; s < n; ++s) {
+      int64_t c = 0;
+      for (int64_t i = raw_off[s]; i < raw_off[s + 1]; ++i)
+        if (raw_mz[i] >= fmin && raw_mz[i] <= fmax) ++c;   /* false for NaN */
+      kept[s] = (int32_t)(c < max_peaks ? c : max_peaks);
+    }
+    /* offsets (one thread), then every spectrum's selection into its slot */
+#pragma omp single
+    {
+      out_off[0] = 0;
+      for (int64_t s = 0; s < n; ++s) out_off[s + 1] = out_off[s] + kept[s];
+    }
+#pragma omp for schedule(dynamic, 64)
+    for (int64_t s = 0; s < n; ++s) {
+      const int64_t r0 = raw_off[s], r1 = raw_off[s + 1];
+      if (r1 - r0 > cap) {
+        cap = (r1 - r0) * 2 + 16;
+        buf = (k0_peak*)realloc(buf, sizeof(k0_peak) * (size_t)cap);
+      }
+      int64_t m = 0;
+      for (int64_t i = r0; i < r1; ++i)
+        if (raw_mz[i] >= fmin && raw_mz[i] <= fmax) {
+          buf[m].mass = raw_mz[i] - 1.0072764f;
+          buf[m].it = raw_int[i];
+          buf[m].idx = i;
+          ++m;
+        }
+      qsort(buf, (size_t)m, sizeof(k0_peak), k0_rank_cmp);
+      const int64_t k = kept[s];
+      for (int64_t j = 0; j < k; ++j) buf[j].rank = (int32_t)j;
+      qsort(buf, (size_t)k, sizeof(k0_peak), k0_mass_cmp);
+      double t = 0.0;
+      const int64_t o = out_off[s];
+      for (int64_t j = 0; j < k; ++j) {
+        out_mass[o + j] = buf[j].mass;
+        out_int[o + j] = buf[j].it;
+        t += (double)buf[j].it;
+      }
+      tic[s] = (float)t;
+      valid[s] = k >= min_peaks;
+    }
+    free(buf);
+  }
+  free(kept);
+}
+
+/* ------------------------------------------------------------------------------------------ top-K over window counts
+ * oracle.k1_appended + oracle.select_topk (kernels.cu:170-180, engine.py:284-312) per spectrum: the window rows of
+ * its hypotheses [spec_hyp_off[s], spec_hyp_off[s+1]) with count >= thr, the topk by (min(count, 32767) desc, row
+ * desc, hypothesis asc), with pair closure the partner rows (same hypothesis, count -1), then one entry per row:
+ * the lowest hypothesis and the highest count, rows ascending.  Spectrum s's list goes to slots [s * cap, ...),
+ * its length to o_n[s] (cap >= topk, 2 topk with closure). */
+typedef struct { int64_t h, r, c; } tk_ent;
+
+static int tk_rank_cmp(const void* pa, const void* pb) {
+  const tk_ent* a = (const tk_ent*)pa;
+  const tk_ent* b = (const tk_ent*)pb;
+  const int64_t ca = a->c < 32767 ? a->c : 32767, cb = b->c < 32767 ? b->c : 32767;
+  if (ca != cb) return ca > cb ? -1 : 1;
+  if (a->r != b->r) return a->r > b->r ? -1 : 1;
+  return (a->h > b->h) - (a->h < b->h);
+}
+
+static int tk_row_cmp(const void* pa, const void* pb) {
+  const tk_ent* a = (const tk_ent*)pa;
+  const tk_ent* b = (const tk_ent*)pb;
+  if (a->r != b->r) return a->r < b->r ? -1 : 1;
+  return (a->h > b->h) - (a->h < b->h);
+}
+
+void or_topk_windows(int64_t n_spec, const int64_t* spec_hyp_off, const int64_t* hyp_lo, const int64_t* hyp_hi,
+                     const int64_t* win_off, const int32_t* cnt, int thr, int topk, int closure,
+                     const int64_t* partner, int cap, int64_t* o_h, int64_t* o_r, int64_t* o_c, int32_t* o_n,
+                     int nthreads) {
+  set_threads(nthreads);
+#pragma omp parallel
+  {
+    tk_ent* buf = NULL;
+    int64_t bcap = 0;
+#pragma omp for schedule(dynamic, 64)
+    for (int64_t s = 0; s < n_spec; ++s) {
+      int64_t m = 0;
+      for (int64_t h = spec_hyp_off[s]; h < spec_hyp_off[s + 1]; ++h) {
+        const int64_t nw = hyp_hi[h] - hyp_lo[h];
+        if (m + nw + 2 * (int64_t)topk > bcap) {
+          bcap = (m + nw + 2 * (int64_t)topk) * 2 + 64;
+          buf = (tk_ent*)realloc(buf, sizeof(tk_ent) * (size_t)bcap);
+        }
+        for (int64_t j = 0; j < nw; ++j) {
+          const int32_t c = cnt[win_off[h] + j];
+          if (c >= thr) {
+            buf[m].h = h;
+            buf[m].r = hyp_lo[h] + j;
+            buf[m].c = c;
+            ++m;
+          }
+        }
+      }
+      if (m + 2 * (int64_t)topk > bcap) {
+        bcap = (m + 2 * (int64_t)topk) * 2 + 64;
+        buf = (tk_ent*)realloc(buf, sizeof(tk_ent) * (size_t)bcap);
+      }
+      qsort(buf, (size_t)m, sizeof(tk_ent), tk_rank_cmp);
+      int64_t k = m < topk ? m : topk;
+      if (closure) {
+        for (int64_t j = 0; j < k; ++j) {
+          buf[k + j].h = buf[j].h;
+          buf[k + j].r = partner[buf[j].r];
+          buf[k + j].c = -1;
+        }
+        k *= 2;
+      }
+      qsort(buf, (size_t)k, sizeof(tk_ent), tk_row_cmp);
+      int32_t w = 0;
+      int64_t* oh = o_h + s * (int64_t)cap;
+      int64_t* orr = o_r + s * (int64_t)cap;
+      int64_t* oc = o_c + s * (int64_t)cap;
+      for (int64_t j = 0; j < k; ++j) {
+        if (w > 0 && orr[w - 1] == buf[j].r) {   /* same row: the lowest hypothesis came first; highest count */
+          if (buf[j].c > oc[w - 1]) oc[w - 1] = buf[j].c;
+          continue;
+        }
+        oh[w] = buf[j].h;
+        orr[w] = buf[j].r;
+        oc[w] = buf[j].c;
+        ++w;
+      }
+      o_n[s] = w;
+    }
+    free(buf);
   }
 }
 

@@ -1,6 +1,8 @@
 """The CPU oracle against the reference: its own Python code (golden_ref_py.npz, made by
 tests/golden/make_golden.py) and its own CUDA kernels (golden_ref_kernels.npz, made by
 tests/golden/make_golden_ref.py on a B200).  These pins make the oracle trustworthy before it judges the kernels."""
+import os
+
 import numpy as np
 import pytest
 
@@ -148,6 +150,87 @@ def test_k1_windows_equal_reference_k1(mini, golden_py, golden_kernels, param_se
     nz = bc > 0
     bkey = (g[f"{name}/win_h"][nz].astype(np.int64) << 32) | g[f"{name}/win_r"][nz]
     assert np.array_equal(np.sort(bkey), golden_kernels[f"{name}/k1_key"])
+
+
+@pytest.mark.parametrize("name", SETS)
+def test_k1_over_fragment_index_equals_window_counts_and_reference_k1(mini, golden_py, golden_kernels, param_sets,
+                                                                       name):
+    """The fragment-index K1 (m/z-binned index fragments, rows ascending in a bin -- the reference's K1 search) ==
+    the window counts bit for bit (counts, scored, matched and the intensity sums), and so the reference's K1."""
+    l1, _, _ = mini
+    g = golden_py
+    p = param_sets[name]
+    hyp = _hyp(g, name)
+    pk = _peaks(g, name)
+    P = O.make_params(STATIC, VAR, p.fragment_unit)
+    a = O.k1_windows(l1, hyp, pk, p, P, tic=pk["tic"])
+    b = O.k1_index(l1, hyp, pk, p, P, tic=pk["tic"])
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y), name
+    oh, orr, oc = O.k1_appended(hyp, b[0], b[1], p.k1_threshold)
+    key = (oh << 32) | orr
+    o = np.argsort(key)
+    assert np.array_equal(key[o], golden_kernels[f"{name}/k1_key"])
+    assert np.array_equal(oc[o], golden_kernels[f"{name}/k1_cnt"])
+
+
+@pytest.mark.parametrize("name", SETS)
+def test_c_k0_view_and_topk_equal_the_numpy_restatement(mini, golden_py, param_sets, name):
+    """The oracle's C K0 view (global peak mode) and C top-K + closure over the window counts == its numpy
+    restatements (pinned to the reference's own code) on the mini fixture."""
+    l1, sp, _ = mini
+    g = golden_py
+    p = param_sets[name]
+    P = O.make_params(STATIC, VAR, p.fragment_unit)
+    a, b = O.k0_view(sp, p), O.k0_view_c(sp, p)
+    for k in ("off", "mass", "int", "tic", "valid"):
+        assert np.array_equal(a[k], b[k]), (name, k)
+    hyp = _hyp(g, name)
+    win_off, cnt, _, _ = O.k1_index(l1, hyp, _peaks(g, name), p, P)
+    for closure in (True, False):
+        for topk in (1, 3, p.topk):
+            want = O.select_topk(*O.k1_appended(hyp, win_off, cnt, p.k1_threshold), hyp["spec"], l1.partner, topk,
+                                 closure)
+            got = O.topk_windows(hyp, win_off, cnt, p.k1_threshold, l1.partner, topk, closure)
+            for x, y in zip(want, got):
+                assert np.array_equal(x, y), (name, closure, topk)
+
+
+def test_k1_over_fragment_index_on_a_larger_run():
+    """The same equality on 400 spectra of the small synthetic workload (configuration 0's index: 2,000 proteins),
+    with precursor windows widened to +-2000 ppm so that windows span many rows of a bin, single-threaded and on all
+    cores, and for two fragment settings (the cached index is rebuilt for the second)."""
+    import dataclasses
+    import tempfile
+    from vulcan import synth
+    from vulcan.index.build import L1Index, read_labels
+    w = synth.WORKLOADS["small"]
+    d = synth.build_index(w, os.environ.get("VULCAN_BENCH_CACHE", os.path.join(tempfile.gettempdir(),
+                                                                                 "vulcan_bench_cache")))
+    l1 = L1Index(d)
+    sp, _ = synth.simulate_run(l1, read_labels(d), w, n_spectra=400, seed=5)
+    for tol, unit, ppm, mfc in (((-0.02, 0.02), "da", (-10.0, 10.0), 1),
+                                ((-20.0, 20.0), "ppm", (-2000.0, 2000.0), None)):
+        p = dataclasses.replace(w.search_params(), fragment_ppm=tol, fragment_unit=unit, precursor_ppm=ppm,
+                                max_fragment_charge=mfc)
+        P = O.make_params(STATIC, w.var_mods, p.fragment_unit)
+        pk = O.k0_view(sp, p)
+        hyp = O.make_hypotheses(sp, pk["valid"], l1.mass32, p)
+        a = O.k1_windows(l1, hyp, pk, p, P, tic=pk["tic"])
+        for nt in (1, None):
+            b = O.k1_index(l1, hyp, pk, p, P, nthreads=nt, tic=pk["tic"])
+            for x, y in zip(a, b):
+                assert np.array_equal(x, y), (unit, nt)
+        assert int(a[1].max()) >= 3
+        # the C K0 view and top-K of the oracle chain on the same run
+        pc = O.k0_view_c(sp, p, nthreads=3)
+        for k in ("off", "mass", "int", "tic", "valid"):
+            assert np.array_equal(pk[k], pc[k]), (unit, k)
+        for topk in (5, 50):
+            want = O.select_topk(*O.k1_appended(hyp, a[0], a[1], 2), hyp["spec"], l1.partner, topk, True)
+            got = O.topk_windows(hyp, a[0], a[1], 2, l1.partner, topk, True)
+            for x, y in zip(want, got):
+                assert np.array_equal(x, y), (unit, topk)
 
 
 @pytest.mark.parametrize("name", SETS)
