@@ -19,6 +19,7 @@ Pieces (each cites the reference lines it restates):
 from __future__ import annotations
 
 import ctypes as C
+import hashlib
 import os
 import subprocess
 
@@ -246,8 +247,15 @@ def frag_index(l1, p, P, arrays=None, nthreads=None):
     <= fmax) binned by m/z from fmin in FRAG_BIN_TH bins, rows ascending within a bin: (bin_off, mass, row, n_bins).
     Built once per index and fragment setting (the reference's K1 searches such an index, kernels.cu:112-190)."""
     a = arrays or {k: getattr(l1, k) for k in ("seq_off", "length", "mask", "mass32", "residues")}
-    key = (id(l1), len(a["mass32"]), p.min_ion_index, float(p.fragment_min_mz), float(p.fragment_max_mz),
-           bytes(P.mono), bytes(P.stat), bytes(P.var), float(P.nterm))
+    m32 = np.asarray(a["mass32"])
+    so = np.asarray(a["seq_off"])
+    # the index's content (an id can be reused once an index object is freed): length, every 256th mass and the
+    # residue total, with the fragment settings
+    fp = hashlib.blake2b(np.ascontiguousarray(m32[::max(1, len(m32) // 256)]).tobytes() +
+                         np.asarray([len(m32), int(so[-1]) if len(so) else 0], np.int64).tobytes(),
+                         digest_size=16).hexdigest()
+    key = (fp, p.min_ion_index, float(p.fragment_min_mz), float(p.fragment_max_mz), bytes(P.mono), bytes(P.stat),
+           bytes(P.var), float(P.nterm))
     hit = _FRAG_INDEX.get(key)
     if hit is not None:
         return hit
